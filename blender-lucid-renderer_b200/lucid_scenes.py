@@ -1,0 +1,351 @@
+"""Seeded synthetic scenes in the Lucid scene-JSON schema.
+
+The schema is the one `PyRenderer::loadSceneFromJsonString` reads
+(LucidRenderer/cpp_renderer/include/pybind_renderer.hpp:1258-1542) and that
+the Blender exporter writes (LucidRenderer/scene_export.py): ``meshes`` with
+``vertices``, ``triangles``, optional ``triangle_normals`` + ``smooth``,
+``material`` {base_color, metallic, roughness, emission, transmission, ior,
+node_tree, use_nodes, volume}, ``native_lights`` (POINT/SUN/SPOT/AREA) and
+``environment``.  Volumes reference a raw float32 sidecar grid file.
+
+Every generator returns ``(scene_dict, camera)`` where camera is the
+``set_camera`` argument tuple (pos, dir, up, fov_deg) flattened to 10 floats.
+No public dataset is used: every scene is procedural and seeded.
+"""
+from __future__ import annotations
+
+import math
+import os
+
+import numpy as np
+
+F32 = np.float32
+
+
+def _fmt_array(a: np.ndarray) -> str:
+    """JSON text of a float array with 9 significant digits (float32 round-trip)."""
+    a = np.asarray(a, dtype=np.float64)
+    if a.ndim == 1:
+        return "[" + ",".join("%.9g" % v for v in a) + "]"
+    return "[" + ",".join(_fmt_array(r) for r in a) + "]"
+
+
+def _fmt_int_array(a: np.ndarray) -> str:
+    a = np.asarray(a, dtype=np.int64)
+    if a.ndim == 1:
+        return "[" + ",".join(str(int(v)) for v in a) + "]"
+    return "[" + ",".join(_fmt_int_array(r) for r in a) + "]"
+
+
+def _fmt_value(v) -> str:
+    import json
+    if isinstance(v, np.ndarray):
+        return _fmt_int_array(v) if v.dtype.kind in "iu" else _fmt_array(v)
+    if isinstance(v, dict):
+        return "{" + ",".join(json.dumps(k) + ":" + _fmt_value(x) for k, x in v.items()) + "}"
+    if isinstance(v, (list, tuple)):
+        return "[" + ",".join(_fmt_value(x) for x in v) + "]"
+    if isinstance(v, (float, np.floating)):
+        return "%.9g" % float(v)
+    return json.dumps(v)
+
+
+def to_json(scene: dict) -> str:
+    """Serialise a scene dict (numpy arrays allowed) to the reference JSON schema."""
+    return _fmt_value(scene)
+
+
+def material(base=(0.8, 0.8, 0.8), metallic=0.0, roughness=0.5, emission=(0.0, 0.0, 0.0),
+             transmission=0.0, ior=1.45) -> dict:
+    return {"base_color": [float(x) for x in base], "metallic": float(metallic),
+            "roughness": float(roughness), "emission": [float(x) for x in emission],
+            "transmission": float(transmission), "ior": float(ior)}
+
+
+def quad(p0, p1, p2, p3):
+    """Two triangles (p0,p1,p2), (p0,p2,p3)."""
+    v = np.array([p0, p1, p2, p3], dtype=np.float64)
+    t = np.array([[0, 1, 2], [0, 2, 3]], dtype=np.int64)
+    return v, t
+
+
+def box(size, center, rot_y_deg=0.0):
+    """Axis-aligned box (12 triangles) rotated about y and placed with its base at center.y."""
+    sx, sy, sz = size
+    c = np.array([[x, y, z] for x in (-sx / 2, sx / 2) for y in (0.0, sy) for z in (-sz / 2, sz / 2)])
+    a = math.radians(rot_y_deg)
+    R = np.array([[math.cos(a), 0, math.sin(a)], [0, 1, 0], [-math.sin(a), 0, math.cos(a)]])
+    v = c @ R.T + np.asarray(center, dtype=np.float64)
+    # corner index = 4*ix + 2*iy + iz
+    faces = [(0, 1, 3, 2), (4, 6, 7, 5), (0, 4, 5, 1), (2, 3, 7, 6), (0, 2, 6, 4), (1, 5, 7, 3)]
+    t = []
+    for f in faces:
+        t += [[f[0], f[1], f[2]], [f[0], f[2], f[3]]]
+    return v, np.array(t, dtype=np.int64)
+
+
+def mesh(v, t, mat, normals=None, smooth=False) -> dict:
+    m = {"vertices": np.asarray(v, dtype=np.float64), "triangles": np.asarray(t, dtype=np.int64),
+         "material": mat}
+    if normals is not None:
+        m["triangle_normals"] = np.asarray(normals, dtype=np.float64)
+        m["smooth"] = bool(smooth)
+    return m
+
+
+# ---------------------------------------------------------------------------
+# Config 1: Cornell box, 36 triangles
+# ---------------------------------------------------------------------------
+def cornell_box():
+    """Unit-cube room (10 triangles, front open), two boxes of 12 triangles
+    (0.3 and 0.6 high, rotated -17 and +17 degrees about y) and a 0.25 x 0.2
+    ceiling quad light (2 triangles, emission 17 warm white).  Walls are
+    Principled diffuse (roughness 1, metallic 0).  Camera: 40 degree vertical
+    fov looking down -z into the room."""
+    white, red, green = (0.73, 0.73, 0.73), (0.63, 0.065, 0.05), (0.14, 0.45, 0.09)
+    meshes = []
+    wall = lambda col: material(col, 0.0, 1.0)
+    meshes.append(mesh(*quad((0, 0, 0), (0, 0, 1), (1, 0, 1), (1, 0, 0)), wall(white)))      # floor
+    meshes.append(mesh(*quad((0, 1, 0), (1, 1, 0), (1, 1, 1), (0, 1, 1)), wall(white)))      # ceiling
+    meshes.append(mesh(*quad((0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0)), wall(white)))      # back
+    meshes.append(mesh(*quad((0, 0, 0), (0, 1, 0), (0, 1, 1), (0, 0, 1)), wall(red)))        # left
+    meshes.append(mesh(*quad((1, 0, 0), (1, 0, 1), (1, 1, 1), (1, 1, 0)), wall(green)))      # right
+    meshes.append(mesh(*box((0.3, 0.3, 0.3), (0.66, 0.0, 0.62), -17.0), wall(white)))        # short box
+    meshes.append(mesh(*box((0.3, 0.6, 0.3), (0.34, 0.0, 0.36), 17.0), wall(white)))         # tall box
+    lv, lt = quad((0.375, 0.999, 0.4), (0.625, 0.999, 0.4), (0.625, 0.999, 0.6), (0.375, 0.999, 0.6))
+    meshes.append(mesh(lv, lt, material((0.78, 0.78, 0.78), 0.0, 1.0, emission=(17.0, 12.0, 4.0))))
+    scene = {"meshes": meshes, "native_lights": [],
+             "environment": {"color": [0.0, 0.0, 0.0], "strength": 1.0}}
+    camera = (0.5, 0.5, 1.95, 0.0, 0.0, -1.0, 0.0, 1.0, 0.0, 40.0)
+    return scene, camera
+
+
+# ---------------------------------------------------------------------------
+# Icospheres and value-noise fBm
+# ---------------------------------------------------------------------------
+def icosphere(levels: int):
+    """Unit icosphere with 20 * 4**levels triangles (Blender's 'subdivisions'
+    = levels + 1)."""
+    p = (1.0 + 5 ** 0.5) / 2.0
+    v = [(-1, p, 0), (1, p, 0), (-1, -p, 0), (1, -p, 0), (0, -1, p), (0, 1, p), (0, -1, -p), (0, 1, -p),
+         (p, 0, -1), (p, 0, 1), (-p, 0, -1), (-p, 0, 1)]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+         (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11),
+         (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    verts = np.array(v, dtype=np.float64)
+    verts /= np.linalg.norm(verts, axis=1, keepdims=True)
+    faces = np.array(f, dtype=np.int64)
+    for _ in range(levels):
+        e = np.concatenate([faces[:, [0, 1]], faces[:, [1, 2]], faces[:, [2, 0]]])
+        e.sort(axis=1)
+        uniq, inv = np.unique(e, axis=0, return_inverse=True)
+        inv = inv.reshape(-1)
+        mid = verts[uniq[:, 0]] + verts[uniq[:, 1]]
+        mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+        base = len(verts)
+        verts = np.concatenate([verts, mid])
+        n = len(faces)
+        a, b, c = faces[:, 0], faces[:, 1], faces[:, 2]
+        ab, bc, ca = inv[:n] + base, inv[n:2 * n] + base, inv[2 * n:] + base
+        faces = np.concatenate([np.stack([a, ab, ca], 1), np.stack([b, bc, ab], 1),
+                                np.stack([c, ca, bc], 1), np.stack([ab, bc, ca], 1)])
+    return verts, faces
+
+
+def _value_noise(p: np.ndarray, seed: int) -> np.ndarray:
+    """Trilinear value noise in [-1, 1] on the integer lattice (hash-based)."""
+    i = np.floor(p).astype(np.int64)
+    f = p - i
+    f = f * f * (3 - 2 * f)
+
+    def h(ix, iy, iz):
+        x = (ix * 73856093) ^ (iy * 19349663) ^ (iz * 83492791) ^ (seed * 2654435761)
+        x = (x ^ (x >> 13)) * 1274126177
+        x = x ^ (x >> 16)
+        return (x & 0xFFFF).astype(np.float64) / 32767.5 - 1.0
+
+    out = 0.0
+    for dx in (0, 1):
+        for dy in (0, 1):
+            for dz in (0, 1):
+                w = ((f[:, 0] if dx else 1 - f[:, 0]) * (f[:, 1] if dy else 1 - f[:, 1]) *
+                     (f[:, 2] if dz else 1 - f[:, 2]))
+                out = out + w * h(i[:, 0] + dx, i[:, 1] + dy, i[:, 2] + dz)
+    return out
+
+
+def fbm(p: np.ndarray, seed: int, octaves: int = 4) -> np.ndarray:
+    out, amp, freq, norm = 0.0, 1.0, 1.0, 0.0
+    for o in range(octaves):
+        out = out + amp * _value_noise(p * freq, seed + o)
+        norm += amp
+        amp *= 0.5
+        freq *= 2.0
+    return out / norm
+
+
+def vertex_normals(v: np.ndarray, t: np.ndarray) -> np.ndarray:
+    fn = np.cross(v[t[:, 1]] - v[t[:, 0]], v[t[:, 2]] - v[t[:, 0]])
+    vn = np.zeros_like(v)
+    for k in range(3):
+        np.add.at(vn, t[:, k], fn)
+    vn /= np.maximum(np.linalg.norm(vn, axis=1, keepdims=True), 1e-12)
+    return vn
+
+
+def displaced_sphere(levels, radius, center, amp_frac, seed):
+    v, t = icosphere(levels)
+    d = fbm(v * 2.5, seed)
+    v = v * (radius * (1.0 + amp_frac * d))[:, None] + np.asarray(center)
+    vn = vertex_normals(v, t)
+    return v, t, vn[t]
+
+
+def write_constant_grid(path: str, dims=(8, 8, 8), value: float = 1.0) -> None:
+    np.full(int(np.prod(dims)), value, dtype=np.float32).tofile(path)
+
+
+def volume_box_mesh(bmin, bmax, density, color, anisotropy, sidecar, dims=(8, 8, 8)) -> dict:
+    """A volume-boundary-only cube (Material Output Surface unlinked, Volume
+    linked) carrying a constant-density grid that fills its bbox."""
+    size = np.asarray(bmax, dtype=np.float64) - np.asarray(bmin, dtype=np.float64)
+    v, t = box(tuple(size), (bmin[0] + size[0] / 2, bmin[1], bmin[2] + size[2] / 2), 0.0)
+    node_tree = {"nodes": [
+        {"name": "Material Output", "type": "ShaderNodeOutputMaterial",
+         "inputs": [{"name": "Surface", "type": "SHADER"}, {"name": "Volume", "type": "SHADER"}]},
+        {"name": "Principled Volume", "type": "ShaderNodeVolumePrincipled", "inputs": []}],
+        "links": [{"from_node": "Principled Volume", "from_socket": "Volume",
+                   "to_node": "Material Output", "to_socket": "Volume"}]}
+    mat = material((0.8, 0.8, 0.8), 0.0, 0.5)
+    mat["node_tree"] = node_tree
+    mat["use_nodes"] = False
+    mat["volume"] = {"color": [float(c) for c in color], "absorption_color": [0.0, 0.0, 0.0],
+                     "density": float(density), "anisotropy": float(anisotropy),
+                     "smoke_grid": {"dims": list(dims), "world_min": [float(x) for x in bmin],
+                                    "world_max": [float(x) for x in bmax], "sidecar_path": sidecar}}
+    return mesh(v, t, mat)
+
+
+# ---------------------------------------------------------------------------
+# Config 2: ~1M-triangle procedural scene
+# ---------------------------------------------------------------------------
+def procedural_scene(seed: int = 2, n_spheres: int = 200, levels: int = 4, emissive_levels: int = 3,
+                     workdir: str | None = None, extent: float = 30.0):
+    """200 fBm-displaced icospheres (5120 triangles each, Blender subdivision
+    5; displacement 5% of radius; radii U[0.2, 1.5] m) on a 2-triangle 100 m
+    ground; per-object Principled params (base U[0.05,0.95]^3, roughness
+    U[0.02,1], metallic Bern(0.3), IOR 1.45, transmission Bern(0.1));
+    16 point, 4 spot (30 degree cone, 5 degree blend), 1 sun, 8 rectangle area
+    lights and 2 emissive icospheres (1280 triangles each); one homogeneous
+    volume box (sigma_t 0.5/m, albedo 0.8, g 0.3) encoded as a constant 8^3
+    grid inside a volume-boundary-only cube.  The sun is a delta light: the
+    reference ignores Blender's sun angle."""
+    rng = np.random.default_rng(seed)
+    meshes = [mesh(*quad((-50, 0, -50), (-50, 0, 50), (50, 0, 50), (50, 0, -50)),
+                   material((0.5, 0.5, 0.5), 0.0, 0.8))]
+    centers = []
+    for i in range(n_spheres):
+        r = rng.uniform(0.2, 1.5)
+        for _ in range(100):
+            c = np.array([rng.uniform(-extent, extent), r, rng.uniform(-extent, extent)])
+            if all(np.linalg.norm(c - c2) > r + r2 for c2, r2 in centers):
+                break
+        centers.append((c, r))
+        v, t, tn = displaced_sphere(levels, r, c, 0.05, seed * 1000 + i)
+        base = rng.uniform(0.05, 0.95, 3)
+        rough = rng.uniform(0.02, 1.0)
+        metal = float(rng.random() < 0.3)
+        trans = float(rng.random() < 0.1)
+        meshes.append(mesh(v, t, material(base, metal, rough, transmission=trans, ior=1.45), tn, True))
+    for k in range(2):
+        c = np.array([rng.uniform(-extent / 2, extent / 2), 4.0 + 2.0 * k, rng.uniform(-extent / 2, extent / 2)])
+        v, t = icosphere(emissive_levels)
+        v = v * 0.6 + c
+        meshes.append(mesh(v, t, material((0.9, 0.9, 0.9), 0.0, 1.0, emission=(12.0, 10.0, 8.0)),
+                           vertex_normals(v, t)[t], True))
+    workdir = workdir or os.getcwd()
+    sidecar = os.path.join(workdir, "procedural_volume_grid_%d.f32" % seed)
+    write_constant_grid(sidecar, (8, 8, 8), 1.0)
+    meshes.append(volume_box_mesh((-4.0, 0.0, -4.0), (4.0, 3.0, 4.0), 0.5, (0.8, 0.8, 0.8), 0.3, sidecar))
+    lights = []
+    for i in range(16):
+        lights.append({"type": "POINT", "name": "Point.%03d" % i,
+                       "position": [rng.uniform(-extent, extent), rng.uniform(1.5, 6.0), rng.uniform(-extent, extent)],
+                       "color": list(rng.uniform(0.6, 1.0, 3)), "energy": float(rng.uniform(200, 800)),
+                       "radius": 0.0})
+    for i in range(4):
+        pos = np.array([rng.uniform(-extent / 2, extent / 2), 8.0, rng.uniform(-extent / 2, extent / 2)])
+        lights.append({"type": "SPOT", "name": "Spot.%03d" % i, "position": list(pos),
+                       "direction": [0.0, -1.0, 0.0], "color": [1.0, 0.95, 0.9],
+                       "energy": 2000.0, "spot_size": math.radians(30.0), "spot_blend": 5.0 / 30.0, "radius": 0.0})
+    sd = np.array([-0.4, -1.0, -0.3])
+    lights.append({"type": "SUN", "name": "Sun", "direction": list(sd / np.linalg.norm(sd)),
+                   "color": [1.0, 0.95, 0.85], "energy": 3.0, "angle": math.radians(0.5)})
+    for i in range(8):
+        pos = np.array([rng.uniform(-extent, extent), rng.uniform(3.0, 7.0), rng.uniform(-extent, extent)])
+        lights.append({"type": "AREA", "name": "Area.%03d" % i, "position": list(pos),
+                       "direction": [0.0, -1.0, 0.0], "right": [1.0, 0.0, 0.0], "up": [0.0, 0.0, 1.0],
+                       "shape": "RECTANGLE", "size": float(rng.uniform(0.5, 2.0)), "size_y": float(rng.uniform(0.5, 2.0)),
+                       "color": [1.0, 1.0, 1.0], "energy": float(rng.uniform(300, 1500))})
+    scene = {"meshes": meshes, "native_lights": lights,
+             "environment": {"color": [0.25, 0.32, 0.45], "strength": 1.0}}
+    camera = (0.0, 9.0, 42.0, 0.0, -0.22, -1.0, 0.0, 1.0, 0.0, 45.0)
+    return scene, camera
+
+
+# ---------------------------------------------------------------------------
+# Small scenes for targeted parity cases
+# ---------------------------------------------------------------------------
+def all_lights_scene(workdir: str | None = None, with_volume: bool = True):
+    """A floor, a glass sphere, a near-mirror metal sphere, a rough metal box
+    and every native light type (soft and hard point, spot, sun, square /
+    rectangle / disk / ellipse area lights) plus an emissive triangle and,
+    optionally, a volume box — every light, BSDF and volume branch of the
+    reference integrators is reachable."""
+    meshes = [mesh(*quad((-5, 0, -5), (-5, 0, 5), (5, 0, 5), (5, 0, -5)), material((0.6, 0.6, 0.6), 0.0, 0.7))]
+    v, t = icosphere(2)
+    meshes.append(mesh(v * 0.5 + np.array([-1.0, 0.5, 0.0]), t, material((1, 1, 1), 0.0, 0.05, transmission=1.0, ior=1.5),
+                       vertex_normals(v, t)[t], True))
+    meshes.append(mesh(v * 0.45 + np.array([0.3, 0.45, -0.5]), t, material((0.95, 0.8, 0.5), 1.0, 0.02)))
+    meshes.append(mesh(*box((0.6, 0.6, 0.6), (1.3, 0.0, 0.6), 30.0), material((0.3, 0.5, 0.8), 0.7, 0.35)))
+    meshes.append(mesh(np.array([[-2.0, 0.01, 1.5], [-1.2, 0.01, 1.5], [-1.6, 0.8, 1.6]]), np.array([[0, 1, 2]]),
+                       material((0.9, 0.9, 0.9), 0.0, 1.0, emission=(6.0, 3.0, 1.0))))
+    if with_volume:
+        workdir = workdir or os.getcwd()
+        sidecar = os.path.join(workdir, "all_lights_grid.f32")
+        write_constant_grid(sidecar, (4, 4, 4), 1.0)
+        meshes.append(volume_box_mesh((0.2, 0.0, 0.8), (1.2, 1.0, 1.8), 1.5, (0.9, 0.7, 0.5), 0.3, sidecar, (4, 4, 4)))
+    lights = [
+        {"type": "POINT", "position": [0.0, 2.5, 1.0], "color": [1.0, 0.9, 0.8], "energy": 120.0, "radius": 0.0},
+        {"type": "POINT", "position": [-1.5, 1.8, -1.0], "color": [0.8, 0.9, 1.0], "energy": 80.0, "radius": 0.2},
+        {"type": "SPOT", "position": [1.5, 3.0, -0.5], "direction": [-0.3, -1.0, 0.1], "color": [1.0, 1.0, 0.9],
+         "energy": 300.0, "spot_size": math.radians(40.0), "spot_blend": 0.2},
+        {"type": "SUN", "direction": [0.3, -1.0, -0.4], "color": [1.0, 0.95, 0.9], "energy": 1.5},
+        {"type": "AREA", "position": [0.0, 3.0, 0.0], "direction": [0.0, -1.0, 0.0], "right": [1, 0, 0], "up": [0, 0, 1],
+         "shape": "SQUARE", "size": 0.8, "color": [1, 1, 1], "energy": 60.0},
+        {"type": "AREA", "position": [2.5, 1.5, 1.5], "direction": [-1.0, 0.0, 0.0], "right": [0, 0, 1], "up": [0, 1, 0],
+         "shape": "RECTANGLE", "size": 1.0, "size_y": 0.5, "color": [1, 0.7, 0.7], "energy": 40.0},
+        {"type": "AREA", "position": [-2.5, 1.5, 0.5], "direction": [1.0, 0.0, 0.0], "right": [0, 0, 1], "up": [0, 1, 0],
+         "shape": "DISK", "size": 0.7, "color": [0.7, 1, 0.7], "energy": 40.0},
+        {"type": "AREA", "position": [0.0, 1.2, -2.5], "direction": [0.0, 0.0, 1.0], "right": [1, 0, 0], "up": [0, 1, 0],
+         "shape": "ELLIPSE", "size": 1.2, "size_y": 0.6, "color": [0.7, 0.7, 1], "energy": 40.0},
+    ]
+    scene = {"meshes": meshes, "native_lights": lights,
+             "environment": {"color": [0.1, 0.12, 0.15], "strength": 1.0}}
+    camera = (0.0, 1.6, 5.0, 0.0, -0.25, -1.0, 0.0, 1.0, 0.0, 45.0)
+    return scene, camera
+
+
+def mirror_point_light_scene():
+    """Mirror floor + diffuse back wall + a point light (the reference's
+    createMirrorPointLightScene regression shape, test_utils.hpp:277-330)."""
+    meshes = [mesh(*quad((-2, 0, -2), (-2, 0, 2), (2, 0, 2), (2, 0, -2)), material((0.9, 0.9, 0.9), 1.0, 0.0)),
+              mesh(*quad((-2, 0, -2), (2, 0, -2), (2, 3, -2), (-2, 3, -2)), material((0.7, 0.7, 0.7), 0.0, 1.0))]
+    lights = [{"type": "POINT", "position": [0.0, 1.5, 0.0], "color": [1, 1, 1], "energy": 100.0, "radius": 0.0}]
+    scene = {"meshes": meshes, "native_lights": lights, "environment": {"color": [0, 0, 0], "strength": 1.0}}
+    camera = (0.0, 1.0, 4.0, 0.0, -0.2, -1.0, 0.0, 1.0, 0.0, 50.0)
+    return scene, camera
+
+
+def scene_triangle_count(scene: dict) -> int:
+    return int(sum(len(m["triangles"]) for m in scene["meshes"]))
