@@ -1,0 +1,151 @@
+// lucid_capi.cpp — extern "C" entry points of liblucid_cuda.so.
+// Exceptions never cross the boundary: every call returns a status code and
+// records its message for lucid_cuda_last_error().
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "../../include/lucid_cuda.h"
+#include "lucid_engine.h"
+#include "lucid_host.h"
+
+struct LucidCudaCtx {
+    lucid::Engine* engine;
+};
+
+namespace {
+template <class F>
+int guarded(LucidCudaCtx* ctx, F&& f) {
+    if (!ctx || !ctx->engine) return LUCID_ERR_INVALID;
+    try {
+        return f(*ctx->engine);
+    } catch (const std::bad_alloc&) {
+        return ctx->engine->fail(LUCID_ERR_OOM, "host allocation failed");
+    } catch (const std::exception& e) {
+        return ctx->engine->fail(LUCID_ERR_INVALID, e.what());
+    } catch (...) {
+        return ctx->engine->fail(LUCID_ERR_INVALID, "unknown error");
+    }
+}
+}  // namespace
+
+extern "C" {
+
+int lucid_cuda_create(int device, LucidCudaCtx** out) {
+    if (!out) return LUCID_ERR_INVALID;
+    *out = nullptr;
+    try {
+        LucidCudaCtx* c = new LucidCudaCtx;
+        c->engine = new lucid::Engine(device);
+        *out = c;
+        return LUCID_OK;
+    } catch (...) {
+        return LUCID_ERR_OOM;
+    }
+}
+
+void lucid_cuda_destroy(LucidCudaCtx* ctx) {
+    if (!ctx) return;
+    delete ctx->engine;
+    delete ctx;
+}
+
+const char* lucid_cuda_last_error(LucidCudaCtx* ctx) {
+    if (!ctx || !ctx->engine) return "invalid context";
+    return ctx->engine->last_error().c_str();
+}
+
+int lucid_cuda_device_info(LucidCudaCtx* ctx, char* buf, size_t cap) {
+    if (!buf || cap == 0) return LUCID_ERR_INVALID;
+    return guarded(ctx, [&](lucid::Engine& e) { return e.device_info(buf, cap); });
+}
+
+int lucid_cuda_load_scene_json(LucidCudaCtx* ctx, const char* json, size_t len) {
+    if (!json) return LUCID_ERR_INVALID;
+    return guarded(ctx, [&](lucid::Engine& e) { return e.load_scene_json(json, len); });
+}
+
+int lucid_cuda_set_camera(LucidCudaCtx* ctx, float px, float py, float pz, float dx, float dy, float dz, float ux,
+                          float uy, float uz, float fov_deg) {
+    return guarded(ctx, [&](lucid::Engine& e) { return e.set_camera(px, py, pz, dx, dy, dz, ux, uy, uz, fov_deg); });
+}
+
+int lucid_cuda_set_algorithm(LucidCudaCtx* ctx, const char* name) {
+    return guarded(ctx, [&](lucid::Engine& e) { return e.set_algorithm(name); });
+}
+
+int lucid_cuda_scene_stats(LucidCudaCtx* ctx, int out8[8]) {
+    if (!out8) return LUCID_ERR_INVALID;
+    return guarded(ctx, [&](lucid::Engine& e) { return e.scene_stats(out8); });
+}
+
+int lucid_cuda_inspect_scene(const char* json, size_t len, int counts8[8], float* cdf, float* area,
+                             float* emission_rgb, int cap) {
+    if (!json || !counts8) return LUCID_ERR_INVALID;
+    try {
+        lucid::HostScene hs;
+        std::string err;
+        if (!lucid::parse_scene_json(json, len, hs, err)) return LUCID_ERR_INVALID;
+        counts8[0] = hs.num_meshes; counts8[1] = hs.num_prims; counts8[2] = hs.num_native;
+        counts8[3] = (int)hs.lights.size(); counts8[4] = hs.num_boundary_meshes; counts8[5] = (int)hs.volumes.size();
+        counts8[6] = 0; counts8[7] = 0;
+        for (int i = 0; i < (int)hs.lights.size() && i < cap; ++i) {
+            if (cdf) cdf[i] = hs.cdf[i];
+            if (area) area[i] = hs.lights[i].normal_area.w;
+            if (emission_rgb) {
+                emission_rgb[3 * i] = hs.lights[i].emission_radius.x;
+                emission_rgb[3 * i + 1] = hs.lights[i].emission_radius.y;
+                emission_rgb[3 * i + 2] = hs.lights[i].emission_radius.z;
+            }
+        }
+        return (int)hs.lights.size();
+    } catch (...) {
+        return LUCID_ERR_INVALID;
+    }
+}
+
+int lucid_cuda_render(LucidCudaCtx* ctx, const LucidRenderParams* params, float* out_rgba, LucidSampleRecord* records) {
+    if (!params || !out_rgba) return LUCID_ERR_INVALID;
+    return guarded(ctx, [&](lucid::Engine& e) { return e.render(*params, out_rgba, records, nullptr); });
+}
+
+int lucid_cuda_render_device(LucidCudaCtx* ctx, const LucidRenderParams* params, float* d_out_rgba) {
+    if (!params || !d_out_rgba) return LUCID_ERR_INVALID;
+    return guarded(ctx, [&](lucid::Engine& e) { return e.render(*params, nullptr, nullptr, d_out_rgba); });
+}
+
+int lucid_cuda_render_debug(LucidCudaCtx* ctx, int tile_x, int tile_y, int tile_w, int tile_h, int full_w, int full_h,
+                            const char* mode, float* out_rgba) {
+    if (!out_rgba) return LUCID_ERR_INVALID;
+    return guarded(ctx, [&](lucid::Engine& e) {
+        return e.render_debug(tile_x, tile_y, tile_w, tile_h, full_w, full_h, mode, out_rgba);
+    });
+}
+
+int lucid_cuda_get_stats(LucidCudaCtx* ctx, LucidRenderStats* out) {
+    if (!out) return LUCID_ERR_INVALID;
+    return guarded(ctx, [&](lucid::Engine& e) { return e.stats(out); });
+}
+
+int lucid_cuda_set_wave_capacity(LucidCudaCtx* ctx, long long paths) {
+    return guarded(ctx, [&](lucid::Engine& e) { return e.set_wave_capacity(paths); });
+}
+
+int lucid_cuda_cancel(LucidCudaCtx* ctx) {
+    if (!ctx || !ctx->engine) return LUCID_ERR_INVALID;
+    ctx->engine->cancel();
+    return LUCID_OK;
+}
+
+int lucid_cuda_is_cancelled(LucidCudaCtx* ctx) {
+    if (!ctx || !ctx->engine) return LUCID_ERR_INVALID;
+    return ctx->engine->is_cancelled() ? 1 : 0;
+}
+
+int lucid_cuda_reset_cancel(LucidCudaCtx* ctx) {
+    if (!ctx || !ctx->engine) return LUCID_ERR_INVALID;
+    ctx->engine->reset_cancel();
+    return LUCID_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1223 @@
+// lucid_engine.cu — B200 wavefront path tracer: device LBVH build, persistent
+// traversal, shading, shadow rays, film; host orchestration.
+//
+// Pipeline per wave (a block of (pixel, sample) paths, sample-major):
+//   k_raygen                      seed PCG32 per (x, y, sample), jitter, primary ray
+//   for depth in [0, max_depth):
+//     k_trace   (persistent)      closest hit + native lights      -> hit SoA
+//     k_shade   (persistent)      volume / emission / NEE / BSDF   -> next queue,
+//                                                                     shadow queue
+//     k_shadow  (persistent)      any-hit, adds unoccluded NEE
+//   k_film                        per-pixel sum in sample order (deterministic)
+// Queues are compacted with warp ballots + one atomic per warp.  Work counts
+// stay on the device; the host enqueues a whole wave without synchronising.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <cub/cub.cuh>
+#include <string>
+#include <vector>
+
+#include "lucid_engine.h"
+#include "lucid_kernels.cuh"
+
+namespace lucid {
+
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) return fail(e_ == cudaErrorMemoryAllocation ? LUCID_ERR_OOM     \
+                                                                           : LUCID_ERR_CUDA,  \
+                                           std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// ---------------------------------------------------------------- buffers
+template <class T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    ~DBuf() { release(); }
+    cudaError_t alloc(size_t count) {
+        release();
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        if (e == cudaSuccess) n = count; else p = nullptr;
+        return e;
+    }
+    void release() { if (p) cudaFree(p); p = nullptr; n = 0; }
+};
+
+struct DeviceScene {
+    DBuf<float4> bvh_tris, bnd_tris, prim_fn, prim_vn;
+    DBuf<int4> prim_info;
+    DBuf<DevNode> nodes;
+    DBuf<DevMaterial> materials;
+    DBuf<DevLight> lights;
+    DBuf<float> cdf, grid;
+    DBuf<DevVolume> volumes;
+    DevScene view{};
+    void release() {
+        bvh_tris.release(); bnd_tris.release(); prim_fn.release(); prim_vn.release(); prim_info.release();
+        nodes.release(); materials.release(); lights.release(); cdf.release(); grid.release(); volumes.release();
+    }
+};
+
+// Per-path SoA state, indexed by path id (sample-major within a wave).
+struct PathView {
+    ulonglong2* rng;   // PCG state, increment
+    float4* ray_o;     // origin, tMin
+    float4* ray_d;     // direction, depth (int bits)
+    float4* thr;       // throughput rgb, pdf of the sampler that chose the ray
+    float4* rad;       // accumulated radiance
+    float4* hit;       // t, u, v, prim (int bits, -1 = miss)
+    float2* lhit;      // native light index (int bits, -1 = none), t
+    float4* sh_o;      // shadow ray origin, length
+    float4* sh_d;      // shadow ray direction
+    float4* sh_c;      // radiance added when unoccluded
+    int* q0;
+    int* q1;
+    int* qs;
+    int* counters;     // per depth: [0] active, [1] shadow, [2..4] fetch cursors
+    int* errors;       // [0] traversal stack overflow
+    int2* rec_prim;
+    int4* rec_cnt;     // bounces, nee tests, nee occluded
+    unsigned long long* rec_hash;
+};
+constexpr int kCountersPerDepth = 8;
+constexpr int kMaxDepth = 1024;
+
+struct PathPool {
+    long long cap = 0;
+    bool records = false;
+    DBuf<ulonglong2> rng;
+    DBuf<float4> ray_o, ray_d, thr, rad, hit, sh_o, sh_d, sh_c;
+    DBuf<float2> lhit;
+    DBuf<int> q0, q1, qs, counters, errors;
+    DBuf<int2> rec_prim;
+    DBuf<int4> rec_cnt;
+    DBuf<unsigned long long> rec_hash;
+    DBuf<float4> film;
+    DBuf<float4> out;
+    size_t film_n = 0;
+    PathView view{};
+    void release() {
+        rng.release(); ray_o.release(); ray_d.release(); thr.release(); rad.release(); hit.release();
+        sh_o.release(); sh_d.release(); sh_c.release(); lhit.release(); q0.release(); q1.release(); qs.release();
+        counters.release(); errors.release(); rec_prim.release(); rec_cnt.release(); rec_hash.release();
+        film.release(); out.release();
+    }
+};
+
+struct FrameParams {
+    float pos[3], fwd[3], right[3], up[3];
+    float aspect, scale;
+    int tile_x, tile_y, tile_w, tile_h, full_w, full_h;
+    int samples, sample_offset, max_depth, algo;
+    int npix;
+    int s0;          // first sample (within the call) of this wave
+    int n_wave;      // paths in this wave
+    int records;
+};
+
+// ---------------------------------------------------------------- warp helpers
+LD unsigned lane_id() { return threadIdx.x & 31u; }
+
+// Warp-aggregated append: one atomic per warp, ranks from the ballot.
+LD void warp_append(int* queue, int* counter, int value, bool pred) {
+    unsigned mask = __ballot_sync(0xffffffffu, pred);
+    if (mask == 0) return;
+    int leader = __ffs(mask) - 1;
+    int base = 0;
+    if ((int)lane_id() == leader) base = atomicAdd(counter, __popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (pred) queue[base + __popc(mask & ((1u << lane_id()) - 1u))] = value;
+}
+
+// Persistent-thread work fetch: a warp claims 32 consecutive items.
+LD int warp_fetch(int* cursor) {
+    int base = 0;
+    if (lane_id() == 0) base = atomicAdd(cursor, 32);
+    return __shfl_sync(0xffffffffu, base, 0);
+}
+
+// ---------------------------------------------------------------- raygen
+LD V3 primary_dir(const FrameParams& f, float nx, float ny) {
+    V3 v = v3(f.fwd[0] + f.right[0] * (nx * f.scale) + f.up[0] * (ny * f.scale),
+              f.fwd[1] + f.right[1] * (nx * f.scale) + f.up[1] * (ny * f.scale),
+              f.fwd[2] + f.right[2] * (nx * f.scale) + f.up[2] * (ny * f.scale));
+    return make_dir_or(v, v3(f.fwd[0], f.fwd[1], f.fwd[2]));
+}
+
+// Primary rays (pybind_renderer.hpp:250-293): NDC, seed (x, y, offset + s),
+// two jitter draws when the call has more than one sample.
+__global__ void k_raygen(FrameParams f, PathView pv) {
+    int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id == 0) pv.counters[0] = f.n_wave;
+    if (id >= f.n_wave) return;
+    int p = id % f.npix, sl = id / f.npix;
+    int gx = f.tile_x + p % f.tile_w, gy = f.tile_y + p / f.tile_w;
+    float nx = (2.0f * ((float)gx + 0.5f) / (float)f.full_w - 1.0f) * f.aspect;
+    float ny = 1.0f - 2.0f * ((float)gy + 0.5f) / (float)f.full_h;
+    Rng rng = seed_xyz((uint32_t)gx, (uint32_t)gy, (uint32_t)(f.sample_offset + f.s0 + sl));
+    V3 d;
+    if (f.samples > 1) {
+        float jx = (randf(rng) - 0.5f) / (float)f.full_w;
+        float jy = (randf(rng) - 0.5f) / (float)f.full_h;
+        d = primary_dir(f, nx + jx, ny + jy);
+    } else {
+        d = primary_dir(f, nx, ny);
+    }
+    pv.rng[id] = make_ulonglong2(rng.state, rng.inc);
+    pv.ray_o[id] = make_float4(f.pos[0], f.pos[1], f.pos[2], 0.0f);
+    pv.ray_d[id] = make_float4(d.x, d.y, d.z, __int_as_float(0));
+    pv.thr[id] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    pv.rad[id] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (f.records) {
+        pv.rec_prim[id] = make_int2(-1, -1);
+        pv.rec_cnt[id] = make_int4(0, 0, 0, 0);
+        pv.rec_hash[id] = 1469598103934665603ULL;
+    }
+}
+
+// ---------------------------------------------------------------- trace
+__global__ void __launch_bounds__(128) k_trace(DevScene sc, PathView pv, int* cnt, int identity, int records) {
+    const int n = *(volatile int*)&cnt[0];
+    const int* q = identity ? nullptr : pv.q0;
+    bool ok = true;
+    for (;;) {
+        int base = warp_fetch(&cnt[2]);
+        if (base >= n) break;
+        int i = base + (int)lane_id();
+        if (i >= n) continue;
+        int id = q ? q[i] : i;
+        float4 ro = pv.ray_o[id], rd = pv.ray_d[id];
+        V3 o = f3(ro), d = f3(rd);
+        int depth = __float_as_int(rd.w);
+        HitRec h = closest_skip_boundaries(sc, o, d, ro.w, ok);
+        float lt = 1e30f;
+        int li = (depth == 0) ? -1 : native_lights_closest(sc, o, d, lt);
+        pv.hit[id] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
+        pv.lhit[id] = make_float2(__int_as_float(li), lt);
+        if (records) {
+            int4 pi = h.prim >= 0 ? sc.prim_info[h.prim] : make_int4(-1, -1, -1, 0);
+            if (depth == 0) pv.rec_prim[id] = make_int2(pi.x, pi.y);
+            pv.rec_cnt[id].x += 1;
+            unsigned long long hs = pv.rec_hash[id];
+            hs = hpush(hs, (uint32_t)pi.x);
+            hs = hpush(hs, (uint32_t)pi.y);
+            hs = hpush(hs, (uint32_t)li);
+            pv.rec_hash[id] = hs;
+        }
+    }
+    if (!ok) atomicAdd(&pv.errors[0], 1);
+}
+
+// ---------------------------------------------------------------- shade
+struct ShadeResult {
+    bool cont, shadow;
+};
+
+LD ShadeResult shade_path(const DevScene& sc, const FrameParams& f, const PathView& pv, int id) {
+    ShadeResult out;
+    out.cont = false;
+    out.shadow = false;
+    const int algo = f.algo;
+    const bool nee = algo == ALGO_NEE || algo == ALGO_MIS || algo == ALGO_VOLUME_MIS;
+    const bool mis = algo == ALGO_MIS || algo == ALGO_VOLUME_MIS;
+    float4 ro = pv.ray_o[id], rd = pv.ray_d[id];
+    V3 o = f3(ro), d = f3(rd);
+    int depth = __float_as_int(rd.w);
+    float4 th = pv.thr[id];
+    RGB T = c3(th);
+    float last_pdf = th.w;
+    RGB result = c3(pv.rad[id]);
+    ulonglong2 rs = pv.rng[id];
+    Rng rng;
+    rng.state = rs.x;
+    rng.inc = rs.y;
+    float4 hh = pv.hit[id];
+    int prim = __float_as_int(hh.w);
+    bool has_hit = prim >= 0;
+    float2 lh = pv.lhit[id];
+    int lidx = __float_as_int(lh.x);
+    bool has_lh = lidx >= 0;
+    V3 new_o = o, new_d = d;
+    V3 sh_o = o, sh_d = d;
+    float sh_len = 0.0f;
+    RGB sh_inc = rgb(0.f, 0.f, 0.f);
+
+    do {
+        if (algo == ALGO_VOLUME_SIMPLE) {
+            float ts = 1e6f;
+            if (has_hit) ts = smin(ts, hh.x);
+            if (has_lh) ts = smin(ts, lh.y);
+            T = mul(T, volume_transmittance(sc, o, d, ts, false));
+        }
+        if (algo == ALGO_VOLUME_MIS) {
+            float ts = 1e6f;
+            if (has_hit) ts = smin(ts, hh.x);
+            if (has_lh) ts = smin(ts, lh.y);
+            float vt = 0.0f;
+            int vi = sample_volume_distance(sc, o, d, ts, rng, vt);
+            if (f.records) pv.rec_hash[id] = hpush(pv.rec_hash[id], vi >= 0 ? 1u : 0u);
+            if (vi >= 0) {
+                // scatter event (path_tracer.hpp:616-700)
+                const DevVolume& v = sc.volumes[vi];
+                T = mul(T, rgb(v.color[0] / (1.0f + v.absorption[0]), v.color[1] / (1.0f + v.absorption[1]),
+                               v.color[2] / (1.0f + v.absorption[2])));
+                V3 x = o + d * vt;
+                V3 wo = -d;
+                float g = v.anisotropy;
+                if (sc.num_lights > 0) {
+                    float usel = randf(rng);
+                    int li = 0;
+                    {
+                        int lo = 0, hi = sc.num_lights;
+                        while (lo < hi) { int mid = (lo + hi) >> 1; if (sc.light_cdf[mid] < usel) lo = mid + 1; else hi = mid; }
+                        li = min(lo, sc.num_lights - 1);
+                    }
+                    const DevLight& L = sc.lights[li];
+                    float lsp = area_ratio(L.normal_area.w, sc.total_light_area);
+                    if (lsp > 1e-6f) {
+                        float u1 = randf(rng), u2 = randf(rng);
+                        LightSample ls = sample_light(L, x, u1, u2);
+                        if (ls.pdf > MIN_PDF) {
+                            RGB Tsh = volume_transmittance(sc, x, ls.dir, ls.dist, true);
+                            float ct = dot(wo, ls.dir);
+                            float pe = hg_eval(g, ct);
+                            float pl = ls.pdf * lsp;
+                            float mw = mis_power(pl, pe);
+                            RGB pw = bsdf_weight(rgb(pe, pe, pe), 1.0f, pl);
+                            RGB c = mul(pw * mw, mul(Tsh, ls.emission));
+                            sh_inc = mul(T, c);
+                            sh_o = x; sh_d = ls.dir; sh_len = ls.dist;
+                            out.shadow = true;
+                        }
+                    }
+                }
+                float u1 = randf(rng), u2 = randf(rng);
+                float ppdf;
+                V3 wi = hg_sample(g, wo, u1, u2, ppdf);
+                last_pdf = ppdf;
+                new_o = x; new_d = wi;
+                if (depth >= 3) {
+                    float rr = smin(smax3(T.r, T.g, T.b), 0.95f);
+                    if (randf(rng) > rr) break;
+                    T = T * (1.0f / rr);
+                }
+                if (!rgb_valid(T)) break;
+                out.cont = true;
+                break;
+            }
+        }
+        if (has_lh && (!has_hit || lh.y < hh.x)) {
+            // native light hit (path_tracer.hpp:429-452)
+            const DevLight& L = sc.lights[sc.native_start + lidx];
+            RGB em = c3(L.emission_radius);
+            if (mis) {
+                float lpdf = 0.0f;
+                if (sc.num_lights > 0) {
+                    float sp = area_ratio(L.normal_area.w, sc.total_light_area);
+                    if (sp > 0.0f) {
+                        V3 lp = o + d * lh.y;
+                        V3 ln = (__float_as_int(L.pos_type.w) == LIGHT_POINT) ? normalize_nz(lp - f3(L.pos_type))
+                                                                              : f3(L.normal_area);
+                        lpdf = pdf_light(L.normal_area.w, o, lp, ln) * sp;
+                    }
+                }
+                float mw = (last_pdf > MIN_PDF && lpdf > MIN_PDF) ? mis_power(last_pdf, lpdf) : 1.0f;
+                result = result + mul(T, em) * mw;
+            } else {
+                result = result + mul(T, em);
+            }
+            break;
+        }
+        if (!has_hit) {
+            result = result + mul(T, rgb(sc.env[0], sc.env[1], sc.env[2]));
+            break;
+        }
+        // surface hit: point and normal from (t, u, v, prim) as in bvh.hpp:108-128
+        V3 p = o + d * hh.x;
+        int4 pi = sc.prim_info[prim];
+        V3 fn = f3(sc.prim_fn[prim]);
+        V3 n = fn;
+        if (pi.w) {
+            float u = hh.y, v = hh.z;
+            float w = 1.0f - u - v;
+            V3 ni = f3(sc.prim_vn[3 * prim]) * w + f3(sc.prim_vn[3 * prim + 1]) * u + f3(sc.prim_vn[3 * prim + 2]) * v;
+            n = make_dir_or(ni, fn);
+        }
+        const DevMaterial& dm = sc.materials[pi.x];
+        Mat m;
+        m.albedo = c3(dm.albedo_metallic);
+        m.metallic = dm.albedo_metallic.w;
+        m.roughness = smax(dm.rough_trans_ior_flags.x, MIN_ROUGHNESS);
+        m.transmission = dm.rough_trans_ior_flags.y;
+        m.ior = dm.rough_trans_ior_flags.z;
+        RGB em = c3(dm.emission);
+        bool has_em = dm.emission.w != 0.0f;
+        V3 wo = -d;
+        bool front = dot(wo, n) > 0;
+        V3 sn = n;
+        if (m.transmission < 0.5f && !front) sn = -n;
+        if (!nee) {
+            result = result + mul(T, em);
+        } else if (!mis) {
+            if (has_em && depth == 0) result = result + mul(T, em);
+        } else if (has_em) {
+            float mw = 1.0f;
+            if (sc.num_lights > 0 && last_pdf > MIN_PDF && pi.z >= 0) {
+                const DevLight& L = sc.lights[pi.z];
+                float sp = area_ratio(L.normal_area.w, sc.total_light_area);
+                if (sp > 0.0f) {
+                    float lpdf = pdf_light(L.normal_area.w, o, p, n) * sp;
+                    if (lpdf > MIN_PDF) mw = mis_power(last_pdf, lpdf);
+                }
+            }
+            result = result + mul(T, em) * mw;
+        }
+        bool transmissive = m.transmission > 0.5f;
+        if (nee && sc.num_lights > 0 && !has_em && !transmissive) {
+            float usel = randf(rng);
+            int li;
+            {
+                int lo = 0, hi = sc.num_lights;
+                while (lo < hi) { int mid = (lo + hi) >> 1; if (sc.light_cdf[mid] < usel) lo = mid + 1; else hi = mid; }
+                li = min(lo, sc.num_lights - 1);
+            }
+            const DevLight& L = sc.lights[li];
+            float lsp = area_ratio(L.normal_area.w, sc.total_light_area);
+            if (lsp > 1e-6f) {
+                float u1 = randf(rng), u2 = randf(rng);
+                LightSample ls = sample_light(L, p, u1, u2);
+                if (ls.pdf > MIN_PDF) {
+                    float nl = dot(sn, ls.dir);
+                    if (nl > 1e-6f) {
+                        RGB fb = eval_bsdf(m, wo, ls.dir, sn);
+                        float pl = ls.pdf * lsp;
+                        RGB c;
+                        if (mis) {
+                            float pb = pdf_bsdf(m, wo, ls.dir, sn);
+                            float mw = mis_power(pl, pb);
+                            RGB bw = bsdf_weight(fb, nl, pl);
+                            if (algo == ALGO_VOLUME_MIS) {
+                                RGB Tsh = volume_transmittance(sc, p, ls.dir, ls.dist, true);
+                                c = mul(bw * mw, mul(Tsh, ls.emission));
+                            } else {
+                                c = mul(bw * mw, ls.emission);
+                            }
+                        } else {
+                            c = mul(bsdf_weight(fb, nl, pl), ls.emission);
+                        }
+                        sh_inc = mul(T, c);
+                        sh_o = p; sh_d = ls.dir; sh_len = ls.dist;
+                        out.shadow = true;
+                    }
+                }
+            }
+        }
+        V3 smp_n = (m.transmission > 0.5f) ? n : sn;
+        float u1 = randf(rng), u2 = randf(rng), u3 = randf(rng);
+        BsdfSample bs = sample_bsdf(m, wo, smp_n, u1, u2, u3, rng);
+        if (!(bs.kind == BS_PRECOMP || bs.pdf > MIN_PDF)) break;
+        RGB w;
+        if (bs.kind == BS_PRECOMP) {
+            w = bs.f;
+        } else {
+            float c = fabsf(dot(smp_n, bs.wi));
+            if (c <= 1e-6f || bs.pdf < MIN_PDF) break;
+            w = bsdf_weight(bs.f, c, bs.pdf);
+        }
+        T = mul(T, w);
+        if (mis) last_pdf = (bs.kind == BS_EVAL) ? bs.pdf : 0.0f;
+        if (depth >= 3) {
+            float rr = smin(smax3(T.r, T.g, T.b), 0.95f);
+            if (randf(rng) > rr) break;
+            T = T * (1.0f / rr);
+        }
+        if (!rgb_valid(T)) break;
+        new_o = p; new_d = bs.wi;
+        out.cont = true;
+    } while (0);
+
+    if (out.cont && depth + 1 >= f.max_depth) out.cont = false;
+    pv.rng[id] = make_ulonglong2(rng.state, rng.inc);
+    pv.rad[id] = make_float4(result.r, result.g, result.b, 0.0f);
+    if (out.cont) {
+        pv.thr[id] = make_float4(T.r, T.g, T.b, last_pdf);
+        pv.ray_o[id] = make_float4(new_o.x, new_o.y, new_o.z, RAY_T_MIN);
+        pv.ray_d[id] = make_float4(new_d.x, new_d.y, new_d.z, __int_as_float(depth + 1));
+    }
+    if (out.shadow) {
+        pv.sh_o[id] = make_float4(sh_o.x, sh_o.y, sh_o.z, sh_len);
+        pv.sh_d[id] = make_float4(sh_d.x, sh_d.y, sh_d.z, 0.0f);
+        pv.sh_c[id] = make_float4(sh_inc.r, sh_inc.g, sh_inc.b, 0.0f);
+    }
+    return out;
+}
+
+__global__ void __launch_bounds__(128) k_shade(DevScene sc, FrameParams f, PathView pv, int* cnt, int* cnt_next,
+                                               int identity, int* qin, int* qout) {
+    const int n = *(volatile int*)&cnt[0];
+    for (;;) {
+        int base = warp_fetch(&cnt[3]);
+        if (base >= n) break;
+        int i = base + (int)lane_id();
+        int id = -1;
+        ShadeResult r;
+        r.cont = false;
+        r.shadow = false;
+        if (i < n) {
+            id = identity ? i : qin[i];
+            r = shade_path(sc, f, pv, id);
+        }
+        warp_append(qout, &cnt_next[0], id, r.cont);
+        warp_append(pv.qs, &cnt[1], id, r.shadow);
+    }
+}
+
+// ---------------------------------------------------------------- shadow
+__global__ void __launch_bounds__(128) k_shadow(DevScene sc, PathView pv, int* cnt, int records) {
+    const int n = *(volatile int*)&cnt[1];
+    bool ok = true;
+    for (;;) {
+        int base = warp_fetch(&cnt[4]);
+        if (base >= n) break;
+        int i = base + (int)lane_id();
+        if (i >= n) continue;
+        int id = pv.qs[i];
+        float4 so = pv.sh_o[id], sd = pv.sh_d[id];
+        bool occ = shadowed_skip_boundaries(sc, f3(so), f3(sd), so.w, ok);
+        if (!occ) {
+            float4 r = pv.rad[id], c = pv.sh_c[id];
+            pv.rad[id] = make_float4(r.x + c.x, r.y + c.y, r.z + c.z, 0.0f);
+        }
+        if (records) {
+            int4 rc = pv.rec_cnt[id];
+            rc.y += 1;
+            rc.z += occ ? 1 : 0;
+            pv.rec_cnt[id] = rc;
+            pv.rec_hash[id] = hpush(pv.rec_hash[id], 0x5EED0000u | (occ ? 1u : 0u));
+        }
+    }
+    if (!ok) atomicAdd(&pv.errors[0], 1);
+}
+
+// ---------------------------------------------------------------- film
+// Per-pixel radiance sum in sample order: film += rad(s0), rad(s0+1), ...
+// (the reference's `radiance = radiance + sample_radiance`, :318-327).
+__global__ void k_film(int npix, int spw, const float4* rad, float4* film) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npix) return;
+    float4 a = film[p];
+    for (int s = 0; s < spw; ++s) {
+        float4 r = rad[(size_t)s * npix + p];
+        a.x = a.x + r.x; a.y = a.y + r.y; a.z = a.z + r.z;
+    }
+    film[p] = a;
+}
+
+// Camera sensitivity (EV 0 => 1), clamp >= 0 keeping NaN, alpha 1, Y flip
+// (pybind_renderer.hpp:330-360).
+__global__ void k_output(int tw, int th, const float4* film, float4* out) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= tw * th) return;
+    int x = p % tw, y = p / tw;
+    float4 a = film[p];
+    float r = a.x * 1.0f, g = a.y * 1.0f, b = a.z * 1.0f;
+    out[(size_t)(th - 1 - y) * tw + x] = make_float4(smax(r, 0.0f), smax(g, 0.0f), smax(b, 0.0f), 1.0f);
+}
+
+__global__ void k_records(FrameParams f, PathView pv, LucidSampleRecord* out) {
+    int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= f.n_wave) return;
+    int p = id % f.npix, sl = id / f.npix;
+    LucidSampleRecord r;
+    float4 ra = pv.rad[id];
+    r.rgb[0] = ra.x; r.rgb[1] = ra.y; r.rgb[2] = ra.z;
+    int2 pp = pv.rec_prim[id];
+    int4 c = pv.rec_cnt[id];
+    r.primary_mesh = pp.x; r.primary_tri = pp.y;
+    r.bounces = (uint32_t)c.x; r.nee_tests = (uint32_t)c.y; r.nee_occluded = (uint32_t)c.z;
+    r.hash = pv.rec_hash[id];
+    out[(size_t)p * f.samples + f.s0 + sl] = r;
+}
+
+// ---------------------------------------------------------------- debug passes
+// render_debug (renderer.hpp:59-93): intersectScene from t = 0 over every
+// triangle (boundary meshes included), no jitter.
+__global__ void k_debug(DevScene sc, FrameParams f, int mode, float4* out, int* errors) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= f.npix) return;
+    int px = p % f.tile_w, py = p / f.tile_w;
+    int gx = f.tile_x + px, gy = f.tile_y + py;
+    float nx = (2.0f * ((float)gx + 0.5f) / (float)f.full_w - 1.0f) * f.aspect;
+    float ny = 1.0f - 2.0f * ((float)gy + 0.5f) / (float)f.full_h;
+    V3 d = primary_dir(f, nx, ny);
+    bool ok = true;
+    HitRec h = scene_closest(sc, v3(f.pos[0], f.pos[1], f.pos[2]), d, 0.0f, 1e30f, ok);
+    if (!ok) atomicAdd(&errors[0], 1);
+    float4 c = make_float4(0.f, 0.f, 0.f, 1.f);
+    if (h.prim >= 0) {
+        int4 pi = sc.prim_info[h.prim];
+        V3 fn = f3(sc.prim_fn[h.prim]);
+        V3 n = fn;
+        if (pi.w) {
+            float w = 1.0f - h.u - h.v;
+            V3 ni = f3(sc.prim_vn[3 * h.prim]) * w + f3(sc.prim_vn[3 * h.prim + 1]) * h.u +
+                    f3(sc.prim_vn[3 * h.prim + 2]) * h.v;
+            n = make_dir_or(ni, fn);
+        }
+        const DevMaterial& dm = sc.materials[pi.x];
+        if (mode == 0) c = make_float4(n.x * 0.5f + 0.5f, n.y * 0.5f + 0.5f, n.z * 0.5f + 0.5f, 1.0f);
+        else if (mode == 1) c = make_float4(dm.albedo_metallic.x, dm.albedo_metallic.y, dm.albedo_metallic.z, 1.0f);
+        else c = make_float4(dm.emission.x * 1.0f, dm.emission.y * 1.0f, dm.emission.z * 1.0f, 1.0f);
+    }
+    out[(size_t)(f.tile_h - 1 - py) * f.tile_w + px] = c;
+}
+
+// ---------------------------------------------------------------- LBVH build
+// Karras 2012 ("Maximizing parallelism in the construction of BVHs"):
+// 63-bit Morton codes of triangle centroids, radix sort, one thread per
+// internal node, bottom-up refit with arrival counters; subtrees of at most
+// four triangles are collapsed into leaves when the nodes are flattened.
+LD int ord_f(float f) { int i = __float_as_int(f); return i >= 0 ? i : i ^ 0x7fffffff; }
+LD float unord_f(int i) { return __int_as_float(i >= 0 ? i : i ^ 0x7fffffff); }
+LD V3 centroid(const float4* verts, int prim) {
+    V3 a = f3(verts[3 * prim]), b = f3(verts[3 * prim + 1]), c = f3(verts[3 * prim + 2]);
+    return (a + b + c) * (1.0f / 3.0f);
+}
+
+__global__ void k_centroid_bounds(const float4* verts, const int* ids, int n, int* bounds) {
+    __shared__ int s[6][128];
+    int t = threadIdx.x;
+    int mn[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, mx[3] = {(int)0x80000000, (int)0x80000000, (int)0x80000000};
+    for (int i = blockIdx.x * blockDim.x + t; i < n; i += gridDim.x * blockDim.x) {
+        V3 c = centroid(verts, ids[i]);
+        int o[3] = {ord_f(c.x), ord_f(c.y), ord_f(c.z)};
+        for (int k = 0; k < 3; ++k) { mn[k] = min(mn[k], o[k]); mx[k] = max(mx[k], o[k]); }
+    }
+    for (int k = 0; k < 3; ++k) { s[k][t] = mn[k]; s[3 + k][t] = mx[k]; }
+    __syncthreads();
+    for (int w = 64; w > 0; w >>= 1) {
+        if (t < w)
+            for (int k = 0; k < 3; ++k) {
+                s[k][t] = min(s[k][t], s[k][t + w]);
+                s[3 + k][t] = max(s[3 + k][t], s[3 + k][t + w]);
+            }
+        __syncthreads();
+    }
+    if (t == 0)
+        for (int k = 0; k < 3; ++k) { atomicMin(&bounds[k], s[k][0]); atomicMax(&bounds[3 + k], s[3 + k][0]); }
+}
+
+LD unsigned long long expand21(unsigned long long v) {
+    v &= 0x1fffffULL;
+    v = (v | v << 32) & 0x1f00000000ffffULL;
+    v = (v | v << 16) & 0x1f0000ff0000ffULL;
+    v = (v | v << 8) & 0x100f00f00f00f00fULL;
+    v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
+    v = (v | v << 2) & 0x1249249249249249ULL;
+    return v;
+}
+
+__global__ void k_morton(const float4* verts, const int* ids, int n, const int* bounds, unsigned long long* keys,
+                         int* vals) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    V3 c = centroid(verts, ids[i]);
+    float lo[3] = {unord_f(bounds[0]), unord_f(bounds[1]), unord_f(bounds[2])};
+    float hi[3] = {unord_f(bounds[3]), unord_f(bounds[4]), unord_f(bounds[5])};
+    float cc[3] = {c.x, c.y, c.z};
+    unsigned long long code = 0;
+    for (int k = 0; k < 3; ++k) {
+        float ext = hi[k] - lo[k];
+        float u = ext > 0.0f ? (cc[k] - lo[k]) / ext : 0.5f;
+        unsigned long long q = (unsigned long long)fminf(fmaxf(u * 2097152.0f, 0.0f), 2097151.0f);
+        code |= expand21(q) << (2 - k);
+    }
+    keys[i] = code;
+    vals[i] = ids[i];
+}
+
+LD int delta_k(const unsigned long long* keys, int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    unsigned long long a = keys[i], b = keys[j];
+    if (a == b) return 64 + __clz(i ^ j);
+    return __clzll(a ^ b);
+}
+
+// children: code >= 0 internal node, < 0 ~leaf index
+__global__ void k_karras(const unsigned long long* keys, int n, int2* child, int* parent, int* leaf_parent,
+                         int2* range) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    int d = (delta_k(keys, n, i, i + 1) - delta_k(keys, n, i, i - 1)) >= 0 ? 1 : -1;
+    int dmin = delta_k(keys, n, i, i - d);
+    int lmax = 2;
+    while (delta_k(keys, n, i, i + lmax * d) > dmin) lmax <<= 1;
+    int l = 0;
+    for (int t = lmax >> 1; t >= 1; t >>= 1)
+        if (delta_k(keys, n, i, i + (l + t) * d) > dmin) l += t;
+    int j = i + l * d;
+    int dnode = delta_k(keys, n, i, j);
+    int s = 0, t = l;
+    do {
+        t = (t + 1) >> 1;
+        if (delta_k(keys, n, i, i + (s + t) * d) > dnode) s += t;
+    } while (t > 1);
+    int gamma = i + s * d + min(d, 0);
+    int first = min(i, j), last = max(i, j);
+    int cl = (first == gamma) ? ~gamma : gamma;
+    int cr = (last == gamma + 1) ? ~(gamma + 1) : gamma + 1;
+    child[i] = make_int2(cl, cr);
+    range[i] = make_int2(first, last);
+    if (cl >= 0) parent[cl] = i; else leaf_parent[~cl] = i;
+    if (cr >= 0) parent[cr] = i; else leaf_parent[~cr] = i;
+}
+
+LD void leaf_box(const float4* verts, int prim, float* b) {
+    V3 a = f3(verts[3 * prim]), c = f3(verts[3 * prim + 1]), e = f3(verts[3 * prim + 2]);
+    b[0] = fminf(fminf(a.x, c.x), e.x); b[1] = fminf(fminf(a.y, c.y), e.y); b[2] = fminf(fminf(a.z, c.z), e.z);
+    b[3] = fmaxf(fmaxf(a.x, c.x), e.x); b[4] = fmaxf(fmaxf(a.y, c.y), e.y); b[5] = fmaxf(fmaxf(a.z, c.z), e.z);
+}
+
+__global__ void k_refit(const float4* verts, const int* sorted_ids, int n, const int2* child, const int* parent,
+                        const int* leaf_parent, int* arrive, float* nbox) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int node = leaf_parent[k];
+    // A Karras tree is at most 64 + log2(n) levels deep; the bound only
+    // guards against a malformed hierarchy.
+    for (int level = 0; node >= 0 && level < 256; ++level) {
+        __threadfence();
+        if (atomicAdd(&arrive[node], 1) == 0) return;   // the sibling subtree finishes this node
+        __threadfence();
+        int2 c = child[node];
+        float b[6], bb[6];
+        if (c.x < 0) leaf_box(verts, sorted_ids[~c.x], b);
+        else for (int q = 0; q < 6; ++q) b[q] = __ldcg(&nbox[6 * c.x + q]);
+        if (c.y < 0) leaf_box(verts, sorted_ids[~c.y], bb);
+        else for (int q = 0; q < 6; ++q) bb[q] = __ldcg(&nbox[6 * c.y + q]);
+        for (int q = 0; q < 3; ++q) {
+            __stcg(&nbox[6 * node + q], fminf(b[q], bb[q]));
+            __stcg(&nbox[6 * node + 3 + q], fmaxf(b[3 + q], bb[3 + q]));
+        }
+        node = parent[node];
+    }
+}
+
+__host__ __device__ __forceinline__ int leaf_code(int start, int count) { return ~((start << 3) | (count - 1)); }
+
+__global__ void k_flatten(const float4* verts, const int* sorted_ids, int n, const int2* child, const int2* range,
+                          const float* nbox, float pad, DevNode* nodes) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    int2 c = child[i];
+    int cc[2] = {c.x, c.y};
+    float bx[2][6];
+    int code[2];
+    for (int s = 0; s < 2; ++s) {
+        int ch = cc[s];
+        if (ch < 0) {
+            leaf_box(verts, sorted_ids[~ch], bx[s]);
+            code[s] = leaf_code(~ch, 1);
+        } else {
+            for (int q = 0; q < 6; ++q) bx[s][q] = nbox[6 * ch + q];
+            int2 r = range[ch];
+            int cnt = r.y - r.x + 1;
+            code[s] = cnt <= 4 ? leaf_code(r.x, cnt) : ch;
+        }
+        for (int q = 0; q < 3; ++q) { bx[s][q] -= pad; bx[s][3 + q] += pad; }
+    }
+    DevNode nd;
+    nd.lmin_lc = make_float4(bx[0][0], bx[0][1], bx[0][2], __int_as_float(code[0]));
+    nd.lmax_rc = make_float4(bx[0][3], bx[0][4], bx[0][5], __int_as_float(code[1]));
+    nd.rmin = make_float4(bx[1][0], bx[1][1], bx[1][2], 0.0f);
+    nd.rmax = make_float4(bx[1][3], bx[1][4], bx[1][5], 0.0f);
+    nodes[i] = nd;
+}
+
+__global__ void k_gather_tris(const float4* tri, const int* sorted_ids, int n, float4* out) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int prim = sorted_ids[k];
+    out[3 * k] = tri[3 * prim];
+    out[3 * k + 1] = tri[3 * prim + 1];
+    out[3 * k + 2] = tri[3 * prim + 2];
+}
+
+// ---------------------------------------------------------------- Engine
+static inline cudaStream_t S(void* s) { return (cudaStream_t)s; }
+
+Engine::Engine(int device) : device_(device) {
+    ds_ = new DeviceScene();
+    pool_ = new PathPool();
+}
+
+Engine::~Engine() {
+    cudaSetDevice(device_);
+    if (ds_) { ds_->release(); delete ds_; }
+    if (pool_) { pool_->release(); delete pool_; }
+    if (stream_) cudaStreamDestroy(S(stream_));
+}
+
+int Engine::device_info(char* buf, size_t cap) const {
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device_) != cudaSuccess) return LUCID_ERR_CUDA;
+    snprintf(buf, cap, "%s (sm_%d%d, %d SMs)", prop.name, prop.major, prop.minor, prop.multiProcessorCount);
+    return LUCID_OK;
+}
+
+int Engine::set_camera(float px, float py, float pz, float dx, float dy, float dz, float ux, float uy, float uz,
+                       float fov_deg) {
+    make_camera(cam_, px, py, pz, dx, dy, dz, ux, uy, uz, fov_deg);
+    camera_set_ = true;
+    return LUCID_OK;
+}
+
+int Engine::set_algorithm(const char* name) {
+    std::string a = name ? name : "";
+    if (a == "simple") algo_ = ALGO_SIMPLE;
+    else if (a == "mis") algo_ = ALGO_MIS;
+    else if (a == "volume_simple") algo_ = ALGO_VOLUME_SIMPLE;
+    else if (a == "volume_mis") algo_ = ALGO_VOLUME_MIS;
+    else algo_ = ALGO_NEE;   // the reference's dispatch falls through to traceNEE
+    return LUCID_OK;
+}
+
+int Engine::set_wave_capacity(long long paths) {
+    if (paths < 0) return fail(LUCID_ERR_INVALID, "wave capacity must be >= 0");
+    wave_cap_ = paths;
+    return LUCID_OK;
+}
+
+int Engine::scene_stats(int out8[8]) const {
+    if (!scene_loaded_) return LUCID_ERR_NO_SCENE;
+    int nvol = (int)host_.volumes.size();
+    out8[0] = host_.num_meshes; out8[1] = host_.num_prims; out8[2] = host_.num_native;
+    out8[3] = (int)host_.lights.size(); out8[4] = host_.num_boundary_meshes; out8[5] = nvol;
+    out8[6] = bvh_nodes_; out8[7] = bvh_leaves_;
+    return LUCID_OK;
+}
+
+int Engine::stats(LucidRenderStats* out) const { *out = stats_; return LUCID_OK; }
+
+void Engine::free_scene() { ds_->release(); scene_loaded_ = false; }
+
+int Engine::load_scene_json(const char* json, size_t len) {
+    CK(cudaSetDevice(device_));
+    if (!stream_) {
+        cudaStream_t s;
+        CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        stream_ = s;
+        cudaDeviceProp prop;
+        CK(cudaGetDeviceProperties(&prop, device_));
+        num_sms_ = prop.multiProcessorCount;
+    }
+    HostScene hs;
+    std::string err;
+    free_scene();
+    if (!parse_scene_json(json, len, hs, err)) return fail(LUCID_ERR_INVALID, err);
+    host_ = std::move(hs);
+    DeviceScene& D = *ds_;
+    const HostScene& H = host_;
+    // boundary triangles (brute force list) and per-prim shading data
+    std::vector<float4> bnd;
+    for (int p = 0; p < H.num_prims; ++p)
+        if (H.prim_boundary[p])
+            for (int k = 0; k < 3; ++k) bnd.push_back(H.tri[3 * p + k]);
+    auto up = [&](auto& buf, const auto& vec) -> cudaError_t {
+        cudaError_t e = buf.alloc(vec.size());
+        if (e != cudaSuccess) return e;
+        if (vec.empty()) return cudaSuccess;
+        return cudaMemcpyAsync(buf.p, vec.data(), vec.size() * sizeof(vec[0]), cudaMemcpyHostToDevice, S(stream_));
+    };
+    CK(up(D.bnd_tris, bnd));
+    CK(up(D.prim_info, H.prim_info));
+    CK(up(D.prim_fn, H.prim_fn));
+    CK(up(D.prim_vn, H.prim_vn));
+    CK(up(D.materials, H.materials));
+    CK(up(D.lights, H.lights));
+    CK(up(D.cdf, H.cdf));
+    CK(up(D.volumes, H.volumes));
+    CK(up(D.grid, H.grid));
+    DevScene& v = D.view;
+    v = DevScene{};
+    v.bnd_tris = D.bnd_tris.p;
+    v.num_bnd_tris = (int)(bnd.size() / 3);
+    v.prim_info = D.prim_info.p;
+    v.prim_fn = D.prim_fn.p;
+    v.prim_vn = D.prim_vn.p;
+    v.materials = D.materials.p;
+    v.lights = D.lights.p;
+    v.light_cdf = D.cdf.p;
+    v.num_lights = (int)H.lights.size();
+    v.native_start = H.native_start;
+    v.num_native = H.num_native;
+    v.total_light_area = H.total_light_area;
+    for (int k = 0; k < 3; ++k) v.env[k] = H.env[k];
+    v.volumes = D.volumes.p;
+    v.num_volumes = (int)H.volumes.size();
+    v.grid = D.grid.p;
+    v.has_boundary = v.num_bnd_tris > 0;
+    int rc = build_bvh();
+    if (rc != LUCID_OK) return rc;
+    CK(cudaStreamSynchronize(S(stream_)));
+    scene_loaded_ = true;
+    return LUCID_OK;
+}
+
+int Engine::build_bvh() {
+    DeviceScene& D = *ds_;
+    const HostScene& H = host_;
+    std::vector<int> real;
+    real.reserve(H.num_prims);
+    float maxabs = 0.0f;
+    for (int p = 0; p < H.num_prims; ++p) {
+        if (H.prim_boundary[p]) continue;
+        real.push_back(p);
+        for (int k = 0; k < 3; ++k) {
+            const float4& q = H.verts[3 * p + k];
+            maxabs = std::max(maxabs, std::max(std::fabs(q.x), std::max(std::fabs(q.y), std::fabs(q.z))));
+        }
+    }
+    int n = (int)real.size();
+    DevScene& v = D.view;
+    v.num_bvh_tris = n;
+    bvh_nodes_ = 0; bvh_leaves_ = 0; bvh_depth_ = 0;
+    if (n == 0) { v.root = 0; v.nodes = nullptr; v.bvh_tris = nullptr; return LUCID_OK; }
+    cudaStream_t st = S(stream_);
+    DBuf<float4> d_tri, d_verts;
+    DBuf<int> d_ids, d_vals, d_vals_sorted, d_parent, d_leaf_parent, d_arrive, d_bounds;
+    DBuf<unsigned long long> d_keys, d_keys_sorted;
+    DBuf<int2> d_child, d_range;
+    DBuf<float> d_nbox;
+    CK(d_tri.alloc(H.tri.size()));
+    CK(cudaMemcpyAsync(d_tri.p, H.tri.data(), H.tri.size() * sizeof(float4), cudaMemcpyHostToDevice, st));
+    CK(d_verts.alloc(H.verts.size()));
+    CK(cudaMemcpyAsync(d_verts.p, H.verts.data(), H.verts.size() * sizeof(float4), cudaMemcpyHostToDevice, st));
+    CK(d_ids.alloc(n));
+    CK(cudaMemcpyAsync(d_ids.p, real.data(), n * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(d_bounds.alloc(6));
+    int init[6] = {0x7fffffff, 0x7fffffff, 0x7fffffff, (int)0x80000000, (int)0x80000000, (int)0x80000000};
+    CK(cudaMemcpyAsync(d_bounds.p, init, sizeof(init), cudaMemcpyHostToDevice, st));
+    k_centroid_bounds<<<std::max(1, std::min(4 * num_sms_, (n + 127) / 128)), 128, 0, st>>>(d_verts.p, d_ids.p, n,
+                                                                                             d_bounds.p);
+    CK(d_keys.alloc(n)); CK(d_keys_sorted.alloc(n)); CK(d_vals.alloc(n)); CK(d_vals_sorted.alloc(n));
+    k_morton<<<(n + 255) / 256, 256, 0, st>>>(d_verts.p, d_ids.p, n, d_bounds.p, d_keys.p, d_vals.p);
+    size_t temp = 0;
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, temp, d_keys.p, d_keys_sorted.p, d_vals.p, d_vals_sorted.p, n, 0, 63,
+                                       st));
+    DBuf<unsigned char> d_temp;
+    CK(d_temp.alloc(temp));
+    CK(cub::DeviceRadixSort::SortPairs(d_temp.p, temp, d_keys.p, d_keys_sorted.p, d_vals.p, d_vals_sorted.p, n, 0, 63,
+                                       st));
+    CK(D.bvh_tris.alloc((size_t)3 * n));
+    k_gather_tris<<<(n + 255) / 256, 256, 0, st>>>(d_tri.p, d_vals_sorted.p, n, D.bvh_tris.p);
+    v.bvh_tris = D.bvh_tris.p;
+    if (n <= 4) {
+        v.root = leaf_code(0, n);
+        v.nodes = nullptr;
+        bvh_leaves_ = 1;
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(st));
+        return LUCID_OK;
+    }
+    CK(d_child.alloc(n - 1)); CK(d_range.alloc(n - 1)); CK(d_parent.alloc(n - 1)); CK(d_leaf_parent.alloc(n));
+    CK(d_arrive.alloc(n - 1)); CK(d_nbox.alloc((size_t)6 * (n - 1)));
+    CK(cudaMemsetAsync(d_parent.p, 0xff, (n - 1) * sizeof(int), st));   // root's parent = -1
+    CK(cudaMemsetAsync(d_arrive.p, 0, (n - 1) * sizeof(int), st));
+    k_karras<<<(n - 1 + 255) / 256, 256, 0, st>>>(d_keys_sorted.p, n, d_child.p, d_parent.p, d_leaf_parent.p,
+                                                  d_range.p);
+    k_refit<<<(n + 255) / 256, 256, 0, st>>>(d_verts.p, d_vals_sorted.p, n, d_child.p, d_parent.p, d_leaf_parent.p,
+                                            d_arrive.p, d_nbox.p);
+    CK(D.nodes.alloc(n - 1));
+    float pad = maxabs * 9.5367431640625e-07f + 1e-30f;   // 2^-20 of the scene's coordinate magnitude
+    k_flatten<<<(n - 1 + 255) / 256, 256, 0, st>>>(d_verts.p, d_vals_sorted.p, n, d_child.p, d_range.p, d_nbox.p, pad,
+                                                  D.nodes.p);
+    CK(cudaGetLastError());
+    v.nodes = D.nodes.p;
+    v.root = 0;
+    // Reachable node count, leaves and depth (the traversal stack bound).
+    std::vector<DevNode> hn(n - 1);
+    CK(cudaMemcpyAsync(hn.data(), D.nodes.p, (n - 1) * sizeof(DevNode), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    // The walk also validates the hierarchy before any traversal kernel uses
+    // it: child indices in range, leaf ranges inside the triangle array, and
+    // no node reached twice.
+    std::vector<std::pair<int, int>> stack{{0, 1}};
+    std::vector<unsigned char> seen(n - 1, 0);
+    int nodes = 0, leaves = 0, depth = 0;
+    long long leaf_tris = 0;
+    while (!stack.empty()) {
+        auto [nd, dep] = stack.back();
+        stack.pop_back();
+        if (nd < 0 || nd >= n - 1 || seen[nd]) return fail(LUCID_ERR_CUDA, "BVH build produced an invalid hierarchy");
+        seen[nd] = 1;
+        ++nodes;
+        depth = std::max(depth, dep);
+        int c[2];
+        std::memcpy(&c[0], &hn[nd].lmin_lc.w, 4);
+        std::memcpy(&c[1], &hn[nd].lmax_rc.w, 4);
+        for (int s = 0; s < 2; ++s) {
+            if (c[s] < 0) {
+                int w = ~c[s], start = w >> 3, count = (w & 7) + 1;
+                if (start < 0 || start + count > n) return fail(LUCID_ERR_CUDA, "BVH leaf out of range");
+                leaf_tris += count;
+                ++leaves;
+                depth = std::max(depth, dep + 1);
+            } else {
+                stack.push_back({c[s], dep + 1});
+            }
+        }
+    }
+    if (leaf_tris != n) return fail(LUCID_ERR_CUDA, "BVH leaves do not cover every triangle");
+    bvh_nodes_ = nodes; bvh_leaves_ = leaves; bvh_depth_ = depth;
+    if (depth >= kStack)
+        return fail(LUCID_ERR_OVERFLOW, "BVH depth " + std::to_string(depth) + " exceeds the traversal stack");
+    return LUCID_OK;
+}
+
+int Engine::ensure_pool(long long paths, bool records) {
+    PathPool& P = *pool_;
+    if (P.cap >= paths && (!records || P.records)) return LUCID_OK;
+    long long cap = std::max(paths, P.cap);
+    P.release();
+    CK(P.rng.alloc(cap)); CK(P.ray_o.alloc(cap)); CK(P.ray_d.alloc(cap)); CK(P.thr.alloc(cap)); CK(P.rad.alloc(cap));
+    CK(P.hit.alloc(cap)); CK(P.lhit.alloc(cap)); CK(P.sh_o.alloc(cap)); CK(P.sh_d.alloc(cap)); CK(P.sh_c.alloc(cap));
+    CK(P.q0.alloc(cap)); CK(P.q1.alloc(cap)); CK(P.qs.alloc(cap));
+    CK(P.counters.alloc((size_t)kCountersPerDepth * (kMaxDepth + 1)));
+    CK(P.errors.alloc(4));
+    if (records) { CK(P.rec_prim.alloc(cap)); CK(P.rec_cnt.alloc(cap)); CK(P.rec_hash.alloc(cap)); }
+    P.cap = cap;
+    P.records = records;
+    PathView& v = P.view;
+    v.rng = P.rng.p; v.ray_o = P.ray_o.p; v.ray_d = P.ray_d.p; v.thr = P.thr.p; v.rad = P.rad.p; v.hit = P.hit.p;
+    v.lhit = P.lhit.p; v.sh_o = P.sh_o.p; v.sh_d = P.sh_d.p; v.sh_c = P.sh_c.p; v.q0 = P.q0.p; v.q1 = P.q1.p;
+    v.qs = P.qs.p; v.counters = P.counters.p; v.errors = P.errors.p;
+    v.rec_prim = P.rec_prim.p; v.rec_cnt = P.rec_cnt.p; v.rec_hash = P.rec_hash.p;
+    return LUCID_OK;
+}
+
+namespace {
+// Algorithmic bytes per unit of work (compulsory SoA traffic; BVH node and
+// triangle fetches are scene-dependent and excluded):
+//   trace : ray 32 + queue id 4 + hit 16 + light hit 8                  = 60 / ray
+//   shade : queue 4 + hit 24 + ray 32 + throughput 16 + radiance 16 + rng 16
+//           + prim info/normal 32 + material 48  (reads)
+//           + rng 16 + radiance 16 + throughput 16 + ray 32 + queue 4
+//           + shadow record 48 + shadow queue 4  (writes)           = 340 / path
+//   shadow: queue 4 + shadow record 48 + radiance 16 read + 16 write  = 84 / ray
+//   raygen: rng 16 + ray 32 + throughput 16 + radiance 16            = 80 / path
+//   film  : radiance 16 / path + film 32 / pixel
+constexpr double kBytesTrace = 60, kBytesShade = 340, kBytesShadow = 84, kBytesRaygen = 80, kBytesFilm = 16;
+enum Kind { K_RAYGEN, K_TRACE, K_SHADE, K_SHADOW, K_FILM, K_NUM };
+const char* kKindNames[K_NUM] = {"k_raygen", "k_trace", "k_shade", "k_shadow", "k_film"};
+const double kKindBytes[K_NUM] = {kBytesRaygen, kBytesTrace, kBytesShade, kBytesShadow, kBytesFilm};
+}  // namespace
+
+int Engine::render(const LucidRenderParams& p, float* out_host, LucidSampleRecord* recs, float* out_device) {
+    CK(cudaSetDevice(device_));
+    reset_cancel();
+    if (p.tile_w <= 0 || p.tile_h <= 0 || p.full_w <= 0 || p.full_h <= 0)
+        return fail(LUCID_ERR_INVALID, "tile and image sizes must be positive");
+    size_t np = (size_t)p.tile_w * p.tile_h;
+    if (out_host) std::fill(out_host, out_host + np * 4, 0.0f);
+    if (!scene_loaded_ || !camera_set_) return fail(LUCID_ERR_NO_SCENE, "scene or camera not set");
+    if (p.samples <= 0) return fail(LUCID_ERR_INVALID, "samples must be >= 1");
+    if (p.max_depth > kMaxDepth) return fail(LUCID_ERR_INVALID, "max_depth too large");
+    if (np > (size_t)0x7fffffff / 2) return fail(LUCID_ERR_INVALID, "tile too large");
+    cudaStream_t st = S(stream_);
+    const bool profile = (p.flags & LUCID_RENDER_PROFILE) != 0;
+    const bool records = recs != nullptr;
+    long long cap = wave_cap_ > 0 ? wave_cap_ : (long long)1 << 22;
+    int spw = (int)std::max<long long>(1, std::min<long long>(p.samples, cap / (long long)np));
+    long long wave_paths = (long long)spw * (long long)np;
+    int rc = ensure_pool(wave_paths, records);
+    if (rc != LUCID_OK) return rc;
+    PathPool& P = *pool_;
+    if (P.film_n < np) {
+        CK(P.film.alloc(np));
+        CK(P.out.alloc(np));
+        P.film_n = np;
+    }
+    CK(cudaMemsetAsync(P.film.p, 0, np * sizeof(float4), st));
+    CK(cudaMemsetAsync(P.errors.p, 0, 4 * sizeof(int), st));
+    DBuf<LucidSampleRecord> d_recs;
+    if (records) CK(d_recs.alloc(np * (size_t)p.samples));
+
+    FrameParams f;
+    for (int k = 0; k < 3; ++k) { f.pos[k] = cam_.pos[k]; f.fwd[k] = cam_.forward[k]; f.right[k] = cam_.right[k]; f.up[k] = cam_.up[k]; }
+    f.aspect = (float)p.full_w / (float)p.full_h;
+    f.scale = std::tan(cam_.fov * 0.5f);
+    f.tile_x = p.tile_x; f.tile_y = p.tile_y; f.tile_w = p.tile_w; f.tile_h = p.tile_h;
+    f.full_w = p.full_w; f.full_h = p.full_h;
+    f.samples = p.samples; f.sample_offset = p.sample_offset; f.max_depth = p.max_depth; f.algo = algo_;
+    f.npix = (int)np;
+    f.records = records ? 1 : 0;
+
+    // persistent grids: a whole number of CTAs per SM
+    int occ_t = 1, occ_s = 1, occ_h = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t, k_trace, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, k_shade, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, k_shadow, 128, 0);
+    const int g_trace = num_sms_ * std::max(1, occ_t), g_shade = num_sms_ * std::max(1, occ_s),
+              g_shadow = num_sms_ * std::max(1, occ_h);
+
+    struct Launch { int kind; cudaEvent_t a, b; int depth; };
+    std::vector<Launch> launches;
+    auto ev_begin = [&](int kind, int depth) -> int {
+        if (!profile) return -1;
+        Launch l{kind, nullptr, nullptr, depth};
+        cudaEventCreate(&l.a);
+        cudaEventCreate(&l.b);
+        cudaEventRecord(l.a, st);
+        launches.push_back(l);
+        return (int)launches.size() - 1;
+    };
+    auto ev_end = [&](int idx) { if (idx >= 0) cudaEventRecord(launches[idx].b, st); };
+
+    stats_ = LucidRenderStats{};
+    double seg = 0, shadows = 0;
+    std::vector<int> hcnt((size_t)kCountersPerDepth * (p.max_depth + 1));
+    std::vector<double> kind_units(K_NUM, 0.0);
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    cudaEventRecord(t0, st);
+    int status = LUCID_OK;
+    int waves = 0;
+    for (int s0 = 0; s0 < p.samples; s0 += spw) {
+        if (is_cancelled()) { status = LUCID_ERR_CANCELLED; break; }
+        int this_spw = std::min(spw, p.samples - s0);
+        f.s0 = s0;
+        f.n_wave = (int)((long long)this_spw * (long long)np);
+        CK(cudaMemsetAsync(P.counters.p, 0, sizeof(int) * kCountersPerDepth * (p.max_depth + 1), st));
+        int e = ev_begin(K_RAYGEN, 0);
+        k_raygen<<<(f.n_wave + 255) / 256, 256, 0, st>>>(f, P.view);
+        ev_end(e);
+        for (int depth = 0; depth < p.max_depth; ++depth) {
+            int* cnt = P.counters.p + kCountersPerDepth * depth;
+            int* cnt_next = P.counters.p + kCountersPerDepth * (depth + 1);
+            PathView pv = P.view;
+            // queue ping-pong: depth d reads q[d&1] and writes q[(d+1)&1]
+            int* qin = (depth & 1) ? P.q1.p : P.q0.p;
+            int* qout = (depth & 1) ? P.q0.p : P.q1.p;
+            pv.q0 = qin;
+            e = ev_begin(K_TRACE, depth);
+            k_trace<<<g_trace, 128, 0, st>>>(ds_->view, pv, cnt, depth == 0, f.records);
+            ev_end(e);
+            e = ev_begin(K_SHADE, depth);
+            k_shade<<<g_shade, 128, 0, st>>>(ds_->view, f, pv, cnt, cnt_next, depth == 0, qin, qout);
+            ev_end(e);
+            e = ev_begin(K_SHADOW, depth);
+            k_shadow<<<g_shadow, 128, 0, st>>>(ds_->view, pv, cnt, f.records);
+            ev_end(e);
+        }
+        e = ev_begin(K_FILM, 0);
+        k_film<<<(f.npix + 255) / 256, 256, 0, st>>>(f.npix, this_spw, P.rad.p, P.film.p);
+        ev_end(e);
+        if (records) k_records<<<(f.n_wave + 255) / 256, 256, 0, st>>>(f, P.view, d_recs.p);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(hcnt.data(), P.counters.p, hcnt.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (int d = 0; d < p.max_depth; ++d) {
+            seg += hcnt[kCountersPerDepth * d];
+            shadows += hcnt[kCountersPerDepth * d + 1];
+        }
+        if (profile) {
+            kind_units[K_RAYGEN] += f.n_wave;
+            kind_units[K_FILM] += f.n_wave;
+            for (int d = 0; d < p.max_depth; ++d) {
+                kind_units[K_TRACE] += hcnt[kCountersPerDepth * d];
+                kind_units[K_SHADE] += hcnt[kCountersPerDepth * d];
+                kind_units[K_SHADOW] += hcnt[kCountersPerDepth * d + 1];
+            }
+        }
+        ++waves;
+    }
+    int np_i = (int)np;
+    k_output<<<(np_i + 255) / 256, 256, 0, st>>>(p.tile_w, p.tile_h, P.film.p, out_device ? (float4*)out_device : P.out.p);
+    cudaEventRecord(t1, st);
+    int herr[4] = {0, 0, 0, 0};
+    CK(cudaMemcpyAsync(herr, P.errors.p, sizeof(herr), cudaMemcpyDeviceToHost, st));
+    if (out_host && !out_device)
+        CK(cudaMemcpyAsync(out_host, P.out.p, np * sizeof(float4), cudaMemcpyDeviceToHost, st));
+    if (records)
+        CK(cudaMemcpyAsync(recs, d_recs.p, np * (size_t)p.samples * sizeof(LucidSampleRecord), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    float tot = 0.0f;
+    cudaEventElapsedTime(&tot, t0, t1);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    stats_.total_ms = tot;
+    stats_.paths = (double)np * p.samples;
+    stats_.segments = seg;
+    stats_.shadow_rays = shadows;
+    stats_.waves = waves;
+    if (profile) {
+        stats_.num_kinds = K_NUM;
+        for (int k = 0; k < K_NUM; ++k) {
+            std::snprintf(stats_.kinds[k].name, sizeof(stats_.kinds[k].name), "%s", kKindNames[k]);
+            stats_.kinds[k].units = kind_units[k];
+            stats_.kinds[k].algo_bytes = kind_units[k] * kKindBytes[k];
+        }
+        for (auto& l : launches) {
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, l.a, l.b);
+            stats_.kinds[l.kind].launches += 1;
+            stats_.kinds[l.kind].total_ms += ms;
+            cudaEventDestroy(l.a);
+            cudaEventDestroy(l.b);
+        }
+        stats_.kinds[K_FILM].algo_bytes += (double)np * 32.0 * waves;
+    }
+    if (herr[0] != 0) return fail(LUCID_ERR_OVERFLOW, "BVH traversal stack overflow");
+    if (status == LUCID_ERR_CANCELLED) return fail(LUCID_ERR_CANCELLED, "render cancelled");
+    return LUCID_OK;
+}
+
+int Engine::render_debug(int tx, int ty, int tw, int th, int fw, int fh, const char* mode, float* out_host) {
+    CK(cudaSetDevice(device_));
+    reset_cancel();
+    if (tw <= 0 || th <= 0 || fw <= 0 || fh <= 0) return fail(LUCID_ERR_INVALID, "tile and image sizes must be positive");
+    size_t np = (size_t)tw * th;
+    std::fill(out_host, out_host + np * 4, 0.0f);
+    if (!scene_loaded_ || !camera_set_) return fail(LUCID_ERR_NO_SCENE, "scene or camera not set");
+    std::string m = mode ? mode : "";
+    int md;
+    if (m == "normal") md = 0;
+    else if (m == "albedo") md = 1;
+    else if (m == "emission") md = 2;
+    else {
+        // unknown mode: magenta, as render_debug does (pybind_renderer.hpp:420-422)
+        for (size_t i = 0; i < np; ++i) { out_host[4 * i] = 1.0f; out_host[4 * i + 1] = 0.0f; out_host[4 * i + 2] = 1.0f; out_host[4 * i + 3] = 1.0f; }
+        return LUCID_OK;
+    }
+    cudaStream_t st = S(stream_);
+    PathPool& P = *pool_;
+    if (P.film_n < np) { CK(P.film.alloc(np)); CK(P.out.alloc(np)); P.film_n = np; }
+    if (!P.errors.p) CK(P.errors.alloc(4));
+    CK(cudaMemsetAsync(P.errors.p, 0, 4 * sizeof(int), st));
+    FrameParams f{};
+    for (int k = 0; k < 3; ++k) { f.pos[k] = cam_.pos[k]; f.fwd[k] = cam_.forward[k]; f.right[k] = cam_.right[k]; f.up[k] = cam_.up[k]; }
+    f.aspect = (float)fw / (float)fh;
+    f.scale = std::tan(cam_.fov * 0.5f);
+    f.tile_x = tx; f.tile_y = ty; f.tile_w = tw; f.tile_h = th; f.full_w = fw; f.full_h = fh; f.npix = (int)np;
+    k_debug<<<((int)np + 255) / 256, 256, 0, st>>>(ds_->view, f, md, P.out.p, P.errors.p);
+    CK(cudaGetLastError());
+    int herr[4];
+    CK(cudaMemcpyAsync(herr, P.errors.p, sizeof(herr), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(out_host, P.out.p, np * sizeof(float4), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (herr[0]) return fail(LUCID_ERR_OVERFLOW, "BVH traversal stack overflow");
+    return LUCID_OK;
+}
+
+}  // namespace lucid

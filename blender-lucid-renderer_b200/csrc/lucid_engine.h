@@ -1,0 +1,61 @@
+// lucid_engine.h — host orchestration of the wavefront path tracer.
+#pragma once
+
+#include <atomic>
+#include <string>
+#include <vector>
+
+#include "../../include/lucid_cuda.h"
+#include "lucid_host.h"
+#include "lucid_types.h"
+
+namespace lucid {
+
+struct DeviceScene;   // device allocations of one uploaded scene
+struct PathPool;      // wavefront SoA path state
+
+class Engine {
+public:
+    explicit Engine(int device);
+    ~Engine();
+
+    int load_scene_json(const char* json, size_t len);
+    int set_camera(float px, float py, float pz, float dx, float dy, float dz, float ux, float uy, float uz,
+                   float fov_deg);
+    int set_algorithm(const char* name);
+    int render(const LucidRenderParams& p, float* out_host, LucidSampleRecord* recs, float* out_device);
+    int render_debug(int tx, int ty, int tw, int th, int fw, int fh, const char* mode, float* out_host);
+    int scene_stats(int out8[8]) const;
+    int stats(LucidRenderStats* out) const;
+    int set_wave_capacity(long long paths);
+    int device_info(char* buf, size_t cap) const;
+
+    void cancel() { cancel_.store(true); }
+    bool is_cancelled() const { return cancel_.load(); }
+    void reset_cancel() { cancel_.store(false); }
+
+    const std::string& last_error() const { return err_; }
+    int fail(int code, const std::string& msg) { err_ = msg; return code; }
+
+private:
+    int ensure_pool(long long paths, bool records);
+    int build_bvh();
+    void free_scene();
+
+    int device_ = 0;
+    void* stream_ = nullptr;   // cudaStream_t
+    int num_sms_ = 0;
+    HostScene host_;
+    HostCamera cam_;
+    bool scene_loaded_ = false, camera_set_ = false;
+    int algo_ = 1;            // "nee": PyRenderer's default (pybind_renderer.hpp:68)
+    DeviceScene* ds_ = nullptr;
+    PathPool* pool_ = nullptr;
+    long long wave_cap_ = 0;  // 0 = automatic
+    std::atomic<bool> cancel_{false};
+    std::string err_;
+    LucidRenderStats stats_{};
+    int bvh_nodes_ = 0, bvh_leaves_ = 0, bvh_depth_ = 0;
+};
+
+}  // namespace lucid

@@ -1,0 +1,52 @@
+// lucid_host.h — host-side scene and camera of the CUDA engine.
+#pragma once
+
+#include <array>
+#include <string>
+#include <vector>
+
+#include "lucid_types.h"
+
+namespace lucid {
+
+// Flattened scene ready for upload.  Triangles are numbered globally in
+// mesh-major order ("prim id"), which is also the reference's hit-order
+// tie-break (later mesh wins on equal distance, geometry/bvh.hpp:167-174).
+struct HostScene {
+    int num_meshes = 0;
+    int num_prims = 0;
+    // per prim
+    std::vector<float4> tri;        // 3 per prim: v0 | prim id bits, e1 = v1 - v0, e2 = v2 - v0
+    std::vector<float4> verts;      // 3 per prim: v0, v1, v2 (bounds for the BVH build)
+    std::vector<int4> prim_info;    // mesh, local tri, light index, smooth
+    std::vector<float4> prim_fn;    // face normal
+    std::vector<float4> prim_vn;    // 3 per prim: vertex normals
+    std::vector<unsigned char> prim_boundary;
+    std::vector<DevMaterial> materials;
+    std::vector<DevLight> lights;
+    std::vector<float> cdf;
+    float total_light_area = 0.0f;
+    int native_start = 0;
+    int num_native = 0;
+    std::vector<DevVolume> volumes;
+    std::vector<float> grid;
+    float env[3] = {0.05f, 0.05f, 0.05f};
+    int num_boundary_meshes = 0;
+};
+
+// Parses the reference's scene JSON (pybind_renderer.hpp:1258-1746).
+// Returns false and sets err on malformed input.
+bool parse_scene_json(const char* json, size_t len, HostScene& out, std::string& err);
+
+struct HostCamera {
+    float pos[3] = {0, 0, 0};
+    float forward[3] = {0, 0, 1};
+    float right[3] = {1, 0, 0};
+    float up[3] = {0, 1, 0};
+    float fov = 1.04719758f;   // 60 degrees (ray.hpp:54)
+};
+// PyRenderer::set_camera (pybind_renderer.hpp:131-160).
+void make_camera(HostCamera& c, float px, float py, float pz, float dx, float dy, float dz, float ux, float uy,
+                 float uz, float fov_deg);
+
+}  // namespace lucid

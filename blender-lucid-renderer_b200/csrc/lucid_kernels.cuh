@@ -1,0 +1,293 @@
+// lucid_kernels.cuh — ray/primitive intersection and BVH traversal (device).
+//
+// Triangle and native-light intersection reproduce the reference's float
+// sequences (geometry/intersection.hpp:58-396) so accepted hits and their
+// (t, u, v) are identical to the CPU renderer.  BVH box tests are
+// conservative instead of exact: boxes are padded and the far distance is
+// widened by 2^-20, so the BVH never culls a triangle the exact triangle test
+// accepts (the reference's own per-mesh slab test, intersection.hpp:257-302,
+// can miss grazing hits; this traversal cannot).
+#pragma once
+
+#include "lucid_device.cuh"
+
+namespace lucid {
+
+// Möller–Trumbore (intersection.hpp:335-396) on a triangle stored as
+// (v0, e1 = v1 - v0, e2 = v2 - v0); identical operation order.
+LD bool isect_tri(V3 o, V3 d, V3 v0, V3 e1, V3 e2, float tmin, float tmax, float& t, float& u, float& v) {
+    V3 pvec = cross(d, e2);
+    float det = dot(e1, pvec);
+    const float eps = 1e-6f * 1e-6f;
+    if (det > -eps && det < eps) return false;
+    V3 tvec = o - v0;
+    float uu = dot(tvec, pvec) / det;
+    if (uu < 0.0f || uu > 1.0f) return false;
+    V3 qvec = cross(tvec, e1);
+    float vv = dot(d, qvec) / det;
+    if (vv < 0.0f || uu + vv > 1.0f) return false;
+    float tt = dot(e2, qvec) / det;
+    if (tt >= tmin && tt <= tmax) { t = tt; u = uu; v = vv; return true; }
+    return false;
+}
+
+struct HitRec {
+    float t, u, v;
+    int prim;
+};
+
+LD void load_tri(const float4* tris, int k, V3& v0, V3& e1, V3& e2, int& prim) {
+    float4 a = __ldg(&tris[3 * k]);
+    float4 b = __ldg(&tris[3 * k + 1]);
+    float4 c = __ldg(&tris[3 * k + 2]);
+    v0 = f3(a); e1 = f3(b); e2 = f3(c);
+    prim = __float_as_int(a.w);
+}
+
+// Closest-hit tie rule: on equal t the larger global prim id wins.  Global
+// ids are mesh-major, so across meshes this is the reference's "later mesh
+// wins" (bvh.hpp:167-174 passes the running t as an inclusive bound).
+LD void test_leaf_closest(const float4* tris, int code, V3 o, V3 d, float tmin, HitRec& h) {
+    int w = ~code;
+    int start = w >> 3, count = (w & 7) + 1;
+    for (int k = start; k < start + count; ++k) {
+        V3 v0, e1, e2;
+        int prim;
+        load_tri(tris, k, v0, e1, e2, prim);
+        float t, u, v;
+        if (isect_tri(o, d, v0, e1, e2, tmin, h.t, t, u, v)) {
+            if (t < h.t || prim > h.prim) { h.t = t; h.u = u; h.v = v; h.prim = prim; }
+        }
+    }
+}
+LD bool test_leaf_any(const float4* tris, int code, V3 o, V3 d, float tmin, float tmax) {
+    int w = ~code;
+    int start = w >> 3, count = (w & 7) + 1;
+    for (int k = start; k < start + count; ++k) {
+        V3 v0, e1, e2;
+        int prim;
+        load_tri(tris, k, v0, e1, e2, prim);
+        float t, u, v;
+        if (isect_tri(o, d, v0, e1, e2, tmin, tmax, t, u, v)) return true;
+    }
+    return false;
+}
+
+// Conservative slab test of one box; returns entry distance in tn.
+LD bool box_hit(float4 bmin, float4 bmax, V3 o, V3 inv, float tmin, float tfar_lim, float& tn) {
+    float tx0 = (bmin.x - o.x) * inv.x, tx1 = (bmax.x - o.x) * inv.x;
+    float ty0 = (bmin.y - o.y) * inv.y, ty1 = (bmax.y - o.y) * inv.y;
+    float tz0 = (bmin.z - o.z) * inv.z, tz1 = (bmax.z - o.z) * inv.z;
+    float t0 = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
+    float t1 = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tfar_lim));
+    tn = t0;
+    return t0 <= t1 * 1.00000095367431640625f;   // widen by 2^-20
+}
+
+constexpr int kStack = 64;
+
+// Closest hit over the BVH (non-boundary triangles) in [tmin, h.t].
+// Returns false when the traversal stack overflowed (a hit may be missed).
+LD bool bvh_closest(const DevScene& sc, V3 o, V3 d, float tmin, HitRec& h) {
+    if (sc.num_bvh_tris == 0) return true;
+    if (sc.root < 0) { test_leaf_closest(sc.bvh_tris, sc.root, o, d, tmin, h); return true; }
+    V3 inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    int stack[kStack];
+    int sp = 0;
+    int node = sc.root;
+    bool ok = true;
+    while (true) {
+        const DevNode* n = sc.nodes + node;
+        float4 a = __ldg(&n->lmin_lc), b = __ldg(&n->lmax_rc), c = __ldg(&n->rmin), e = __ldg(&n->rmax);
+        int cl = __float_as_int(a.w), cr = __float_as_int(b.w);
+        float tl, tr;
+        bool hl = box_hit(a, b, o, inv, tmin, h.t, tl);
+        bool hr = box_hit(c, e, o, inv, tmin, h.t, tr);
+        if (hl && cl < 0) { test_leaf_closest(sc.bvh_tris, cl, o, d, tmin, h); hl = false; }
+        if (hr && cr < 0) { test_leaf_closest(sc.bvh_tris, cr, o, d, tmin, h); hr = false; }
+        if (hl && hr) {
+            int nearc = (tl <= tr) ? cl : cr, farc = (tl <= tr) ? cr : cl;
+            if (sp < kStack) stack[sp++] = farc; else ok = false;
+            node = nearc;
+        } else if (hl) {
+            node = cl;
+        } else if (hr) {
+            node = cr;
+        } else {
+            if (sp == 0) break;
+            node = stack[--sp];
+        }
+    }
+    return ok;
+}
+
+// Any hit over the BVH in [tmin, tmax]; overflow reported through ok.
+LD bool bvh_any(const DevScene& sc, V3 o, V3 d, float tmin, float tmax, bool& ok) {
+    if (sc.num_bvh_tris == 0) return false;
+    if (sc.root < 0) return test_leaf_any(sc.bvh_tris, sc.root, o, d, tmin, tmax);
+    V3 inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    int stack[kStack];
+    int sp = 0;
+    int node = sc.root;
+    while (true) {
+        const DevNode* n = sc.nodes + node;
+        float4 a = __ldg(&n->lmin_lc), b = __ldg(&n->lmax_rc), c = __ldg(&n->rmin), e = __ldg(&n->rmax);
+        int cl = __float_as_int(a.w), cr = __float_as_int(b.w);
+        float tl, tr;
+        bool hl = box_hit(a, b, o, inv, tmin, tmax, tl);
+        bool hr = box_hit(c, e, o, inv, tmin, tmax, tr);
+        if (hl && cl < 0) { if (test_leaf_any(sc.bvh_tris, cl, o, d, tmin, tmax)) return true; hl = false; }
+        if (hr && cr < 0) { if (test_leaf_any(sc.bvh_tris, cr, o, d, tmin, tmax)) return true; hr = false; }
+        if (hl && hr) {
+            int nearc = (tl <= tr) ? cl : cr, farc = (tl <= tr) ? cr : cl;
+            if (sp < kStack) stack[sp++] = farc; else ok = false;
+            node = nearc;
+        } else if (hl) {
+            node = cl;
+        } else if (hr) {
+            node = cr;
+        } else {
+            if (sp == 0) break;
+            node = stack[--sp];
+        }
+    }
+    return false;
+}
+
+// Closest boundary-only triangle in [tmin, h.t] by brute force (these are the
+// few triangles of volume-domain cubes).
+LD void boundary_closest(const DevScene& sc, V3 o, V3 d, float tmin, HitRec& h) {
+    for (int k = 0; k < sc.num_bnd_tris; ++k) {
+        V3 v0, e1, e2;
+        int prim;
+        load_tri(sc.bnd_tris, k, v0, e1, e2, prim);
+        float t, u, v;
+        if (isect_tri(o, d, v0, e1, e2, tmin, h.t, t, u, v)) {
+            if (t < h.t || prim > h.prim) { h.t = t; h.u = u; h.v = v; h.prim = prim; }
+        }
+    }
+}
+
+// intersectScene over every triangle (geometry/bvh.hpp:155-177).
+LD HitRec scene_closest(const DevScene& sc, V3 o, V3 d, float tmin, float tmax, bool& ok) {
+    HitRec h;
+    h.t = tmax; h.u = 0.0f; h.v = 0.0f; h.prim = -1;
+    ok &= bvh_closest(sc, o, d, tmin, h);
+    if (sc.num_bnd_tris) boundary_closest(sc, o, d, tmin, h);
+    return h;
+}
+
+// intersect_skipping_volume_boundaries (path_tracer.hpp:82-95): the closest
+// non-boundary hit after skipping at most 8 boundary hits, each skip moving
+// the search start 1 mm past the boundary.  The real-surface BVH query is
+// reused while its hit stays beyond the advanced search start.
+LD HitRec closest_skip_boundaries(const DevScene& sc, V3 o, V3 d, float tmin, bool& ok) {
+    HitRec real;
+    real.t = 1e30f; real.u = 0.0f; real.v = 0.0f; real.prim = -1;
+    ok &= bvh_closest(sc, o, d, tmin, real);
+    if (!sc.num_bnd_tris) return real;
+    float search = tmin;
+    HitRec none;
+    none.t = 1e30f; none.u = 0.0f; none.v = 0.0f; none.prim = -1;
+    for (int peek = 0; peek < 8; ++peek) {
+        if (real.prim >= 0 && real.t < search) {
+            real = none;
+            ok &= bvh_closest(sc, o, d, search, real);
+        }
+        HitRec b;
+        b.t = (real.prim >= 0) ? real.t : 1e30f; b.u = 0.0f; b.v = 0.0f;
+        b.prim = (real.prim >= 0) ? real.prim : -1;
+        int real_prim = b.prim;
+        boundary_closest(sc, o, d, search, b);
+        if (b.prim < 0) return none;                 // no hit at all
+        if (b.prim == real_prim) return real;        // the real surface is closest
+        search = b.t + 1e-3f;                        // skip the boundary hit
+    }
+    return none;
+}
+
+// is_shadowed_skipping_volume_boundaries (path_tracer.hpp:103-119).
+LD bool shadowed_skip_boundaries(const DevScene& sc, V3 o, V3 d, float tmax, bool& ok) {
+    if (!sc.num_bnd_tris) {
+        if (tmax <= 0.0f) return false;
+        return bvh_any(sc, o, d, RAY_T_MIN, tmax, ok);
+    }
+    V3 po = o;
+    float off = 0.0f;
+    for (int peek = 0; peek < 8; ++peek) {
+        float rem = tmax - off;
+        if (rem <= 0.0f) return false;
+        HitRec b;
+        b.t = rem; b.u = 0.0f; b.v = 0.0f; b.prim = -1;
+        boundary_closest(sc, po, d, RAY_T_MIN, b);
+        if (b.prim < 0) return bvh_any(sc, po, d, RAY_T_MIN, rem, ok);
+        if (bvh_any(sc, po, d, RAY_T_MIN, b.t, ok)) return true;
+        float skip = b.t + 1e-3f;
+        off += skip;
+        po = po + d * skip;
+    }
+    return false;
+}
+
+// ---- native-light shapes (intersection.hpp:58-236) ----
+LD bool isect_sphere(V3 o, V3 d, V3 c, float radius, float& th) {
+    V3 oc = o - c;
+    float b = 2.0f * dot(oc, d);
+    float cc = len2(oc) - radius * radius;
+    float disc = b * b - 4.0f * cc;
+    if (disc < 0.0f) return false;
+    float sq = sqrtf(smax(0.0f, disc));
+    float t = (-b - sq) / 2.0f;
+    if (t < RAY_T_MIN) {
+        t = (-b + sq) / 2.0f;
+        if (t < RAY_T_MIN) return false;
+    }
+    th = t;
+    return true;
+}
+LD bool isect_planar(V3 o, V3 d, V3 c, V3 n, V3 right, V3 up, float& t, float& x, float& y) {
+    float den = dot(d, n);
+    if (fabsf(den) < 1e-6f) return false;
+    float num = dot(c - o, n);
+    t = num / den;
+    if (t < RAY_T_MIN) return false;
+    V3 lh = (o + d * t) - c;
+    x = dot(lh, right);
+    y = dot(lh, up);
+    return true;
+}
+
+// intersectNativeLights (scene_lights.hpp:176-246): index into the native
+// light list and distance, or -1.
+LD int native_lights_closest(const DevScene& sc, V3 o, V3 d, float& t_out) {
+    int best = -1;
+    float bt = 1e30f;
+    for (int i = 0; i < sc.num_native; ++i) {
+        const DevLight& L = sc.lights[sc.native_start + i];
+        int type = __float_as_int(L.pos_type.w);
+        float t;
+        if (type == LIGHT_POINT) {
+            float radius = L.emission_radius.w;
+            if (radius > MIN_LENGTH && isect_sphere(o, d, f3(L.pos_type), radius, t) && t < bt) { bt = t; best = i; }
+        } else if (type == LIGHT_AREA) {
+            int shape = __float_as_int(L.v0_shape.w);
+            float x, y;
+            V3 n = f3(L.normal_area);
+            bool h = isect_planar(o, d, f3(L.pos_type), n, f3(L.right_sx), f3(L.up_sy), t, x, y);
+            if (h) {
+                if (shape == AREA_DISK || shape == AREA_ELLIPSE) {
+                    float nx = x / (L.right_sx.w * 0.5f), ny = y / (L.up_sy.w * 0.5f);
+                    h = !(nx * nx + ny * ny > 1.0f);
+                } else {
+                    float hx = L.right_sx.w * 0.5f, hy = L.up_sy.w * 0.5f;
+                    h = !(x * x > hx * hx || y * y > hy * hy);
+                }
+            }
+            if (h && t < bt && dot(n, d) < 0) { bt = t; best = i; }
+        }
+    }
+    t_out = bt;
+    return best;
+}
+
+}  // namespace lucid

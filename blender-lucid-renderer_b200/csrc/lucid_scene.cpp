@@ -1,0 +1,370 @@
+// lucid_scene.cpp — JSON scene → flattened device-ready arrays.
+//
+// Semantics follow PyRenderer::loadSceneFromJsonString
+// (include/pybind_renderer.hpp:1258-1542), parseNativeLights (:1544-1746),
+// finalizeMeshBounds (core/scene.hpp:191-227) and SceneLights::buildFromScene
+// (light/scene_lights.hpp:56-122): the same keys, defaults and float
+// conversions, so the uploaded lights, CDF and normals equal the CPU
+// renderer's bit for bit.  Compiled with -ffp-contract=off.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <nlohmann/json.hpp>
+#include <stdexcept>
+
+#include "lucid_host.h"
+#include "lucid_math.h"
+
+namespace lucid {
+namespace {
+
+using json = nlohmann::json;
+
+struct F3 {
+    float x, y, z;
+};
+inline F3 sub(F3 a, F3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline F3 cross3(F3 a, F3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+inline float len2(F3 a) { return a.x * a.x + a.y * a.y + a.z * a.z; }
+// make_direction_or_default / make_normal_or_default (render_units.hpp:485-503, 776-791)
+inline F3 dir_or(F3 v, F3 fb) {
+    float l2 = len2(v);
+    if (l2 < 1e-6f * 1e-6f) return fb;
+    float l = std::sqrt(l2);
+    return {v.x / l, v.y / l, v.z / l};
+}
+inline float4 f4(F3 v, float w) { float4 r; r.x = v.x; r.y = v.y; r.z = v.z; r.w = w; return r; }
+inline float ibits(int i) { float f; std::memcpy(&f, &i, 4); return f; }
+inline F3 arr3(const json& a) { return {a[0].get<float>(), a[1].get<float>(), a[2].get<float>()}; }
+
+// Is the Material Output's Surface input linked?  (node_evaluator.cpp:82-163
+// builds the links map; pybind_renderer.hpp:1377-1388 reads the socket.)
+bool surface_linked(const json& nt, bool& valid) {
+    valid = false;
+    if (!nt.contains("nodes") || !nt.is_object()) return true;
+    const auto& nodes = nt["nodes"];
+    valid = !nodes.empty();
+    if (!valid) return true;
+    std::map<std::pair<std::string, std::string>, bool> links;
+    if (nt.contains("links"))
+        for (const auto& l : nt["links"])
+            links[{l["to_node"].get<std::string>(), l["to_socket"].get<std::string>()}] = true;
+    for (const auto& n : nodes) {
+        if (n.value("type", "") != "ShaderNodeOutputMaterial") continue;
+        const std::string name = n.value("name", "");
+        if (!n.contains("inputs")) return false;
+        for (const auto& in : n["inputs"])
+            if (in.value("name", "") == "Surface") return links.count({name, "Surface"}) > 0;
+        return false;
+    }
+    return true;
+}
+
+struct NativeLight {
+    int type = LIGHT_POINT;
+    F3 pos{0, 0, 0}, normal{0, 0, 1};
+    float em[3] = {0, 0, 0};
+    float area = 0, radius = 0, spot_angle = 0, spot_blend = 0;
+    F3 right{1, 0, 0}, up{0, 1, 0};
+    float sx = 1, sy = 1;
+    int shape = AREA_SQUARE;
+};
+
+// parseNativeLights (pybind_renderer.hpp:1544-1746), W -> radiance conversions.
+void parse_lights(const json& arr, std::vector<NativeLight>& out) {
+    const double PI = M_PI;
+    const float EPS = 1e-6f;
+    for (const auto& lj : arr) {
+        NativeLight L;
+        std::string type = lj.value("type", "POINT");
+        if (lj.contains("position")) L.pos = arr3(lj["position"]);
+        if (lj.contains("direction")) L.normal = dir_or(arr3(lj["direction"]), F3{0, 0, -1});
+        float cr = 1, cg = 1, cb = 1;
+        if (lj.contains("color")) { F3 c = arr3(lj["color"]); cr = c.x; cg = c.y; cb = c.z; }
+        float energy = lj.value("energy", 1.0f);
+        if (type == "POINT") {
+            L.type = LIGHT_POINT;
+            float radius = lj.value("radius", 0.0f);
+            L.radius = radius;
+            float area = 4.0f * PI * radius * radius;
+            if (area < EPS) area = 1.0f;
+            L.area = area;
+            if (radius > EPS) {
+                L.em[0] = (float)(cr * (energy / (PI * area)));
+                L.em[1] = (float)(cg * (energy / (PI * area)));
+                L.em[2] = (float)(cb * (energy / (PI * area)));
+            } else {
+                float factor = energy / (4.0f * PI);
+                L.em[0] = cr * factor; L.em[1] = cg * factor; L.em[2] = cb * factor;
+            }
+        } else if (type == "SUN") {
+            L.type = LIGHT_SUN;
+            L.area = 1.0f;
+            L.em[0] = cr * energy; L.em[1] = cg * energy; L.em[2] = cb * energy;
+        } else if (type == "SPOT") {
+            L.type = LIGHT_SPOT;
+            L.radius = lj.value("radius", 0.0f);
+            float sa = lj.value("spot_size", static_cast<float>(M_PI / 4.0f));
+            L.spot_angle = sa;
+            L.spot_blend = lj.value("spot_blend", 0.0f);
+            L.area = 1.0f;
+            float half = sa * 0.5f;
+            float solid = 2.0f * PI * (1.0f - std::cos(half));
+            float factor = energy / solid;
+            L.em[0] = cr * factor; L.em[1] = cg * factor; L.em[2] = cb * factor;
+        } else if (type == "AREA") {
+            L.type = LIGHT_AREA;
+            float sx = lj.value("size", 1.0f);
+            float sy = lj.value("size_y", sx);
+            L.sx = sx; L.sy = sy;
+            float area;
+            std::string shape = lj.value("shape", "SQUARE");
+            if (shape == "DISK") { L.shape = AREA_DISK; float r = sx * 0.5f; area = PI * r * r; }
+            else if (shape == "ELLIPSE") { L.shape = AREA_ELLIPSE; float rx = sx * 0.5f, ry = sy * 0.5f; area = PI * rx * ry; }
+            else if (shape == "RECTANGLE") { L.shape = AREA_RECTANGLE; area = sx * sy; }
+            else { L.shape = AREA_SQUARE; area = sx * sy; }
+            L.area = area;
+            if (lj.contains("right")) L.right = dir_or(arr3(lj["right"]), F3{1, 0, 0});
+            if (lj.contains("up")) L.up = dir_or(arr3(lj["up"]), F3{0, 1, 0});
+            float factor = energy / (PI * area);
+            L.em[0] = cr * factor; L.em[1] = cg * factor; L.em[2] = cb * factor;
+        } else {
+            // An unknown type keeps the reference's default-constructed Light
+            // (EMISSIVE_MESH with zero area and emission).
+            L.type = LIGHT_EMISSIVE;
+            L.area = 0.0f;
+        }
+        out.push_back(L);
+    }
+}
+
+DevLight pack_native(const NativeLight& L) {
+    DevLight d;
+    std::memset(&d, 0, sizeof(d));
+    d.pos_type = f4(L.pos, ibits(L.type));
+    // point-like lights get 1 m^2 in the CDF (scene_lights.hpp:106-108)
+    float area = L.area < 1e-6f ? 1.0f : L.area;
+    d.normal_area = f4(L.normal, area);
+    d.emission_radius = f4(F3{L.em[0], L.em[1], L.em[2]}, L.radius);
+    d.v0_shape = f4(F3{0, 0, 0}, ibits(L.shape));
+    d.v1_cosc = f4(F3{0, 0, 0}, lucid_math::lm_cosf(L.spot_angle * 0.5f));
+    d.v2_blend = f4(F3{0, 0, 0}, L.spot_blend);
+    d.right_sx = f4(L.right, L.sx);
+    d.up_sy = f4(L.up, L.sy);
+    return d;
+}
+
+}  // namespace
+
+bool parse_scene_json(const char* text, size_t length, HostScene& S, std::string& err) {
+    S = HostScene();
+    json j;
+    try {
+        j = json::parse(text, text + length);
+    } catch (const std::exception& e) {
+        err = std::string("scene JSON parse error: ") + e.what();
+        return false;
+    }
+    try {
+        std::vector<DevLight> emissive_lights;
+        float total = 0.0f;
+        if (j.contains("meshes")) {
+            int mesh_index = 0;
+            for (const auto& mj : j["meshes"]) {
+                std::vector<F3> verts;
+                if (mj.contains("vertices"))
+                    for (const auto& v : mj["vertices"]) verts.push_back(arr3(v));
+                std::vector<std::array<F3, 3>> tn;
+                bool has_tn = false;
+                if (mj.contains("triangle_normals")) {
+                    has_tn = true;
+                    for (const auto& t : mj["triangle_normals"]) {
+                        std::array<F3, 3> a;
+                        for (int k = 0; k < 3; ++k)
+                            a[k] = dir_or(F3{static_cast<float>(t[k][0]), static_cast<float>(t[k][1]),
+                                             static_cast<float>(t[k][2])}, F3{0, 0, 1});
+                        tn.push_back(a);
+                    }
+                }
+                bool smooth = mj.contains("smooth") && mj["smooth"].get<bool>();
+                std::vector<std::array<int, 3>> tris;
+                if (mj.contains("triangles"))
+                    for (const auto& t : mj["triangles"]) tris.push_back({t[0].get<int>(), t[1].get<int>(), t[2].get<int>()});
+                for (const auto& t : tris)
+                    for (int k = 0; k < 3; ++k)
+                        if (t[k] < 0 || t[k] >= (int)verts.size())
+                            throw std::runtime_error("mesh " + std::to_string(mesh_index) + ": triangle index out of range");
+
+                // material (pybind_renderer.hpp:1346-1503)
+                float alb[3] = {0.8f, 0.8f, 0.8f}, metallic = 0.0f, roughness = 0.5f, em[3] = {0, 0, 0};
+                float transmission = 0.0f, ior = 1.45f;
+                bool boundary = false;
+                DevVolume vol;
+                std::memset(&vol, 0, sizeof(vol));
+                vol.color[0] = vol.color[1] = vol.color[2] = 1.0f;
+                bool vol_has_grid = false;
+                std::vector<float> grid;
+                if (mj.contains("material")) {
+                    const auto& mat = mj["material"];
+                    if (mat.contains("base_color")) { F3 c = arr3(mat["base_color"]); alb[0] = c.x; alb[1] = c.y; alb[2] = c.z; }
+                    if (mat.contains("metallic")) metallic = mat["metallic"];
+                    if (mat.contains("roughness")) roughness = mat["roughness"];
+                    if (mat.contains("emission")) { F3 c = arr3(mat["emission"]); em[0] = c.x; em[1] = c.y; em[2] = c.z; }
+                    if (mat.contains("transmission")) transmission = mat["transmission"];
+                    if (mat.contains("ior")) ior = mat["ior"];
+                    bool nt_valid = false, surf = true;
+                    if (mat.contains("node_tree") && !mat["node_tree"].is_null()) {
+                        surf = surface_linked(mat["node_tree"], nt_valid);
+                        if (!nt_valid) surf = true;
+                    }
+                    if (mat.contains("volume") && !mat["volume"].is_null()) {
+                        const auto& v = mat["volume"];
+                        if (v.contains("color") && v["color"].is_array() && v["color"].size() >= 3) {
+                            F3 c = arr3(v["color"]); vol.color[0] = c.x; vol.color[1] = c.y; vol.color[2] = c.z;
+                        }
+                        if (v.contains("absorption_color") && v["absorption_color"].is_array() && v["absorption_color"].size() >= 3) {
+                            F3 c = arr3(v["absorption_color"]); vol.absorption[0] = c.x; vol.absorption[1] = c.y; vol.absorption[2] = c.z;
+                        }
+                        if (v.contains("density")) vol.density = v["density"].get<float>();
+                        if (v.contains("anisotropy")) vol.anisotropy = v["anisotropy"].get<float>();
+                        if (v.contains("smoke_grid") && v["smoke_grid"].is_object()) {
+                            const auto& sg = v["smoke_grid"];
+                            if (sg.contains("dims") && sg["dims"].is_array() && sg["dims"].size() == 3 && sg.contains("world_min") &&
+                                sg["world_min"].is_array() && sg.contains("world_max") && sg["world_max"].is_array() &&
+                                sg.contains("sidecar_path")) {
+                                for (int i = 0; i < 3; ++i) vol.dims[i] = sg["dims"][i].get<int>();
+                                for (int i = 0; i < 3; ++i) {
+                                    vol.wmin[i] = sg["world_min"][i].get<float>();
+                                    vol.wmax[i] = sg["world_max"][i].get<float>();
+                                }
+                                if (vol.dims[0] < 2 || vol.dims[1] < 2 || vol.dims[2] < 2)
+                                    throw std::runtime_error("volume grid dims must be >= 2 per axis");
+                                size_t n = (size_t)vol.dims[0] * vol.dims[1] * vol.dims[2];
+                                std::ifstream f(sg["sidecar_path"].get<std::string>(), std::ios::binary);
+                                if (f) {
+                                    grid.resize(n);
+                                    f.read(reinterpret_cast<char*>(grid.data()), n * sizeof(float));
+                                    float mx = 0.0f;
+                                    for (float d : grid) if (d > mx) mx = d;
+                                    vol.grid_max = mx;
+                                    vol_has_grid = true;
+                                } else {
+                                    vol.dims[0] = vol.dims[1] = vol.dims[2] = 0;
+                                }
+                            }
+                        }
+                    }
+                    bool present = vol.density > 0.0f || vol_has_grid;
+                    if (present && !surf) boundary = true;
+                }
+                if (vol_has_grid) {
+                    vol.grid_offset = (long long)S.grid.size();
+                    S.grid.insert(S.grid.end(), grid.begin(), grid.end());
+                    S.volumes.push_back(vol);
+                }
+                S.num_boundary_meshes += boundary;
+                bool emissive = (0.2126f * em[0] + 0.7152f * em[1] + 0.0722f * em[2]) > 1e-6f;
+                DevMaterial dm;
+                dm.albedo_metallic = f4(F3{alb[0], alb[1], alb[2]}, metallic);
+                dm.rough_trans_ior_flags.x = roughness;
+                dm.rough_trans_ior_flags.y = transmission;
+                dm.rough_trans_ior_flags.z = ior;
+                dm.rough_trans_ior_flags.w = ibits((emissive ? MAT_EMISSIVE : 0) | (boundary ? MAT_BOUNDARY_ONLY : 0));
+                dm.emission = f4(F3{em[0], em[1], em[2]}, emissive ? 1.0f : 0.0f);
+                S.materials.push_back(dm);
+
+                // triangles: face normals (scene.hpp:214-222) and emissive lights
+                for (size_t ti = 0; ti < tris.size(); ++ti) {
+                    const auto& t = tris[ti];
+                    F3 a = verts[t[0]], b = verts[t[1]], c = verts[t[2]];
+                    F3 e1 = sub(b, a), e2 = sub(c, a);
+                    F3 fn = dir_or(cross3(e1, e2), F3{0, 1, 0});
+                    int prim = S.num_prims++;
+                    S.tri.push_back(f4(a, ibits(prim)));
+                    S.tri.push_back(f4(e1, 0.0f));
+                    S.tri.push_back(f4(e2, 0.0f));
+                    S.verts.push_back(f4(a, 0.0f));
+                    S.verts.push_back(f4(b, 0.0f));
+                    S.verts.push_back(f4(c, 0.0f));
+                    bool sm = has_tn && ti < tn.size() && smooth;
+                    int light_index = -1;
+                    if (emissive) {
+                        // SceneLights::buildFromScene emissive triangles (scene_lights.hpp:79-101)
+                        float area = std::sqrt(len2(cross3(e1, e2))) * 0.5f;
+                        if (area > 1e-6f) {
+                            DevLight d;
+                            std::memset(&d, 0, sizeof(d));
+                            d.pos_type = f4(F3{0, 0, 0}, ibits(LIGHT_EMISSIVE));
+                            d.normal_area = f4(fn, area);
+                            d.emission_radius = f4(F3{em[0], em[1], em[2]}, 0.0f);
+                            d.v0_shape = f4(a, ibits(0));
+                            d.v1_cosc = f4(b, 0.0f);
+                            d.v2_blend = f4(c, 0.0f);
+                            light_index = (int)emissive_lights.size();
+                            emissive_lights.push_back(d);
+                            total += area;
+                        }
+                    }
+                    int4 pi;
+                    pi.x = mesh_index; pi.y = (int)ti; pi.z = light_index; pi.w = sm ? 1 : 0;
+                    S.prim_info.push_back(pi);
+                    S.prim_fn.push_back(f4(fn, 0.0f));
+                    for (int k = 0; k < 3; ++k) S.prim_vn.push_back(sm ? f4(tn[ti][k], 0.0f) : f4(fn, 0.0f));
+                    S.prim_boundary.push_back(boundary ? 1 : 0);
+                }
+                ++mesh_index;
+            }
+            S.num_meshes = mesh_index;
+        }
+        std::vector<NativeLight> native;
+        if (j.contains("native_lights") && j["native_lights"].is_array()) parse_lights(j["native_lights"], native);
+        else if (j.contains("lights") && j["lights"].is_array()) parse_lights(j["lights"], native);
+        if (j.contains("environment") && j["environment"].is_object()) {
+            const auto& e = j["environment"];
+            float col[3] = {0.05f, 0.05f, 0.05f}, strength = 1.0f;
+            if (e.contains("color") && e["color"].is_array()) { F3 c = arr3(e["color"]); col[0] = c.x; col[1] = c.y; col[2] = c.z; }
+            if (e.contains("strength")) strength = e["strength"].get<float>();
+            for (int k = 0; k < 3; ++k) S.env[k] = col[k] * strength;
+        } else {
+            for (int k = 0; k < 3; ++k) S.env[k] = 0.05f * 1.0f;
+        }
+        // SceneLights: emissive triangles, then native lights; CDF by
+        // cumulative area / total (scene_lights.hpp:103-121).
+        S.lights = emissive_lights;
+        S.native_start = (int)S.lights.size();
+        S.num_native = (int)native.size();
+        for (const auto& L : native) {
+            DevLight d = pack_native(L);
+            S.lights.push_back(d);
+            total += d.normal_area.w;
+        }
+        S.total_light_area = total;
+        S.cdf.resize(S.lights.size());
+        float cum = 0.0f;
+        for (size_t i = 0; i < S.lights.size(); ++i) {
+            cum += S.lights[i].normal_area.w;
+            S.cdf[i] = (total < 1e-6f) ? 0.0f : cum / total;
+        }
+    } catch (const std::exception& e) {
+        err = std::string("malformed scene: ") + e.what();
+        return false;
+    }
+    return true;
+}
+
+void make_camera(HostCamera& c, float px, float py, float pz, float dx, float dy, float dz, float ux, float uy,
+                 float uz, float fov_deg) {
+    c.pos[0] = px; c.pos[1] = py; c.pos[2] = pz;
+    F3 dir = dir_or(F3{dx, dy, dz}, F3{0, 0, -1});
+    F3 up = dir_or(F3{ux, uy, uz}, F3{0, 1, 0});
+    c.fov = fov_deg * (3.14159274101257324219f / 180.0f);
+    F3 right = dir_or(cross3(dir, up), F3{1, 0, 0});
+    F3 upc = dir_or(cross3(right, dir), F3{0, 1, 0});
+    c.forward[0] = dir.x; c.forward[1] = dir.y; c.forward[2] = dir.z;
+    c.right[0] = right.x; c.right[1] = right.y; c.right[2] = right.z;
+    c.up[0] = upc.x; c.up[1] = upc.y; c.up[2] = upc.z;
+}
+
+}  // namespace lucid

@@ -1,0 +1,216 @@
+"""ctypes binding of liblucid_cuda.so (the C ABI in include/lucid_cuda.h).
+
+This is the reference-facing boundary as a non-pybind caller sees it (the
+same stub a ctypes/cffi integration would use).  Importing it fails loudly
+when the CUDA library has not been built: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblucid_cuda.so")
+
+LUCID_OK = 0
+LUCID_ERR_NO_SCENE = -1
+LUCID_ERR_OOM = -2
+LUCID_ERR_TIMEOUT = -3
+LUCID_ERR_CANCELLED = -4
+LUCID_ERR_INVALID = -5
+LUCID_ERR_CUDA = -6
+LUCID_ERR_OVERFLOW = -7
+LUCID_RENDER_PROFILE = 1
+
+
+class RenderParams(ctypes.Structure):
+    _fields_ = [("tile_x", ctypes.c_int), ("tile_y", ctypes.c_int), ("tile_w", ctypes.c_int),
+                ("tile_h", ctypes.c_int), ("full_w", ctypes.c_int), ("full_h", ctypes.c_int),
+                ("samples", ctypes.c_int), ("sample_offset", ctypes.c_int), ("max_depth", ctypes.c_int),
+                ("flags", ctypes.c_int)]
+
+
+class SampleRecord(ctypes.Structure):
+    _fields_ = [("rgb", ctypes.c_float * 3), ("primary_mesh", ctypes.c_int32), ("primary_tri", ctypes.c_int32),
+                ("bounces", ctypes.c_uint32), ("nee_tests", ctypes.c_uint32), ("nee_occluded", ctypes.c_uint32),
+                ("hash", ctypes.c_uint64)]
+
+
+RECORD_DTYPE = np.dtype([("rgb", np.float32, 3), ("primary_mesh", np.int32), ("primary_tri", np.int32),
+                         ("bounces", np.uint32), ("nee_tests", np.uint32), ("nee_occluded", np.uint32),
+                         ("hash", np.uint64)], align=True)
+assert RECORD_DTYPE.itemsize == ctypes.sizeof(SampleRecord)
+
+
+class KernelStat(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 32), ("launches", ctypes.c_int), ("total_ms", ctypes.c_double),
+                ("algo_bytes", ctypes.c_double), ("units", ctypes.c_double)]
+
+
+class RenderStats(ctypes.Structure):
+    _fields_ = [("total_ms", ctypes.c_double), ("paths", ctypes.c_double), ("segments", ctypes.c_double),
+                ("shadow_rays", ctypes.c_double), ("waves", ctypes.c_int), ("num_kinds", ctypes.c_int),
+                ("kinds", KernelStat * 8)]
+
+
+# Every symbol include/lucid_cuda.h declares, with its ctypes signature.
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_F = ctypes.c_float
+SIGNATURES = {
+    "lucid_cuda_create": (_I, [_I, ctypes.POINTER(_P)]),
+    "lucid_cuda_destroy": (None, [_P]),
+    "lucid_cuda_last_error": (ctypes.c_char_p, [_P]),
+    "lucid_cuda_device_info": (_I, [_P, ctypes.c_char_p, ctypes.c_size_t]),
+    "lucid_cuda_load_scene_json": (_I, [_P, ctypes.c_char_p, ctypes.c_size_t]),
+    "lucid_cuda_set_camera": (_I, [_P] + [_F] * 10),
+    "lucid_cuda_set_algorithm": (_I, [_P, ctypes.c_char_p]),
+    "lucid_cuda_scene_stats": (_I, [_P, ctypes.POINTER(_I)]),
+    "lucid_cuda_inspect_scene": (_I, [ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(_I), _P, _P, _P, _I]),
+    "lucid_cuda_render": (_I, [_P, ctypes.POINTER(RenderParams), _P, _P]),
+    "lucid_cuda_render_device": (_I, [_P, ctypes.POINTER(RenderParams), _P]),
+    "lucid_cuda_render_debug": (_I, [_P, _I, _I, _I, _I, _I, _I, ctypes.c_char_p, _P]),
+    "lucid_cuda_get_stats": (_I, [_P, ctypes.POINTER(RenderStats)]),
+    "lucid_cuda_set_wave_capacity": (_I, [_P, ctypes.c_longlong]),
+    "lucid_cuda_cancel": (_I, [_P]),
+    "lucid_cuda_is_cancelled": (_I, [_P]),
+    "lucid_cuda_reset_cancel": (_I, [_P]),
+}
+
+_lib = None
+
+
+def load_library() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("liblucid_cuda.so is not built (run blender-lucid-renderer_b200/build_ext.py); "
+                               "the renderer has no CPU fallback")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+class LucidError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"lucid error {code}: {msg}")
+        self.code = code
+
+
+def inspect_scene(json_text: str, cap: int = 1 << 16):
+    """Host-only parse: (counts[8], cdf, area, emission[n,3]) — no GPU needed."""
+    lib = load_library()
+    b = json_text.encode()
+    counts = (ctypes.c_int * 8)()
+    cdf = np.zeros(cap, np.float32)
+    area = np.zeros(cap, np.float32)
+    em = np.zeros((cap, 3), np.float32)
+    n = lib.lucid_cuda_inspect_scene(b, len(b), counts, cdf.ctypes.data, area.ctypes.data, em.ctypes.data, cap)
+    if n < 0:
+        raise LucidError(n, "scene parse failed")
+    n = min(n, cap)
+    return list(counts), cdf[:n].copy(), area[:n].copy(), em[:n].copy()
+
+
+class Context:
+    """One renderer context on a CUDA device."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        rc = self.lib.lucid_cuda_create(device, ctypes.byref(h))
+        if rc != LUCID_OK:
+            raise LucidError(rc, "create failed")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.lucid_cuda_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int) -> int:
+        if rc != LUCID_OK:
+            raise LucidError(rc, self.lib.lucid_cuda_last_error(self.h).decode())
+        return rc
+
+    def load_scene_json(self, text: str) -> None:
+        b = text.encode()
+        self._check(self.lib.lucid_cuda_load_scene_json(self.h, b, len(b)))
+
+    def set_camera(self, *cam) -> None:
+        self._check(self.lib.lucid_cuda_set_camera(self.h, *[float(c) for c in cam]))
+
+    def set_algorithm(self, name: str) -> None:
+        self._check(self.lib.lucid_cuda_set_algorithm(self.h, name.encode()))
+
+    def set_wave_capacity(self, paths: int) -> None:
+        self._check(self.lib.lucid_cuda_set_wave_capacity(self.h, int(paths)))
+
+    def scene_stats(self):
+        out = (ctypes.c_int * 8)()
+        self._check(self.lib.lucid_cuda_scene_stats(self.h, out))
+        return list(out)
+
+    def device_info(self) -> str:
+        buf = ctypes.create_string_buffer(256)
+        self._check(self.lib.lucid_cuda_device_info(self.h, buf, 256))
+        return buf.value.decode()
+
+    def render(self, tile_w, tile_h, full_w=None, full_h=None, samples=1, sample_offset=0, max_depth=8,
+               tile_x=0, tile_y=0, records=False, profile=False, out=None, check=True):
+        """Render into a host float32 RGBA array (tile_h, tile_w, 4).  Returns
+        (image, records-or-None, status)."""
+        full_w = tile_w if full_w is None else full_w
+        full_h = tile_h if full_h is None else full_h
+        p = RenderParams(tile_x, tile_y, tile_w, tile_h, full_w, full_h, samples, sample_offset, max_depth,
+                         LUCID_RENDER_PROFILE if profile else 0)
+        img = out if out is not None else np.zeros((tile_h, tile_w, 4), np.float32)
+        recs = np.zeros(tile_w * tile_h * samples, RECORD_DTYPE) if records else None
+        rc = self.lib.lucid_cuda_render(self.h, ctypes.byref(p), img.ctypes.data,
+                                        recs.ctypes.data if recs is not None else None)
+        if check:
+            self._check(rc)
+        return img, recs, rc
+
+    def render_device(self, d_out_ptr: int, tile_w, tile_h, samples=1, sample_offset=0, max_depth=8,
+                      profile=False):
+        p = RenderParams(0, 0, tile_w, tile_h, tile_w, tile_h, samples, sample_offset, max_depth,
+                         LUCID_RENDER_PROFILE if profile else 0)
+        return self._check(self.lib.lucid_cuda_render_device(self.h, ctypes.byref(p), ctypes.c_void_p(d_out_ptr)))
+
+    def render_debug(self, mode: str, tile_w, tile_h, full_w=None, full_h=None, tile_x=0, tile_y=0):
+        full_w = tile_w if full_w is None else full_w
+        full_h = tile_h if full_h is None else full_h
+        img = np.zeros((tile_h, tile_w, 4), np.float32)
+        self._check(self.lib.lucid_cuda_render_debug(self.h, tile_x, tile_y, tile_w, tile_h, full_w, full_h,
+                                                     mode.encode(), img.ctypes.data))
+        return img
+
+    def stats(self) -> dict:
+        s = RenderStats()
+        self._check(self.lib.lucid_cuda_get_stats(self.h, ctypes.byref(s)))
+        kinds = {}
+        for k in range(s.num_kinds):
+            ks = s.kinds[k]
+            kinds[ks.name.decode()] = {"launches": ks.launches, "total_ms": ks.total_ms,
+                                       "algo_bytes": ks.algo_bytes, "units": ks.units}
+        return {"total_ms": s.total_ms, "paths": s.paths, "segments": s.segments, "shadow_rays": s.shadow_rays,
+                "waves": s.waves, "kernels": kinds}
+
+    def cancel(self):
+        self.lib.lucid_cuda_cancel(self.h)
+
+    def is_cancelled(self) -> bool:
+        return self.lib.lucid_cuda_is_cancelled(self.h) == 1

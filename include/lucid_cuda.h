@@ -1,0 +1,154 @@
+/*
+ * lucid_cuda.h — C ABI of the B200 (sm_100a) wavefront path tracer.
+ *
+ * This is the drop-in boundary for the Lucid renderer's progressive render
+ * entry point.  Each entry point replaces one method of the reference's
+ * PyRenderer façade (LucidRenderer/cpp_renderer/include/pybind_renderer.hpp),
+ * which the pybind11 module (src/pybind_module.cpp) exposes to Blender.  All
+ * signatures use plain C types, caller-owned host buffers and integer status
+ * codes; no C++ type or exception crosses the boundary.
+ *
+ * Threading: a context may be used from one thread at a time, except
+ * lucid_cuda_cancel(), which may be called from any thread (the reference's
+ * std::atomic cancel flag, pybind_renderer.hpp:86-102).
+ */
+#ifndef LUCID_CUDA_H
+#define LUCID_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference reports scene-load failure as `false` and
+ * silently returns zero buffers otherwise (pybind_renderer.hpp:121-125,
+ * 200-203); this ABI returns explicit codes instead and never falls back to
+ * a CPU path. */
+#define LUCID_OK 0
+#define LUCID_ERR_NO_SCENE (-1)   /* render before load_scene_json / set_camera */
+#define LUCID_ERR_OOM (-2)        /* device allocation failed                    */
+#define LUCID_ERR_TIMEOUT (-3)    /* a bounded device wait gave up               */
+#define LUCID_ERR_CANCELLED (-4)  /* lucid_cuda_cancel() observed; partial image */
+#define LUCID_ERR_INVALID (-5)    /* bad argument or malformed scene             */
+#define LUCID_ERR_CUDA (-6)       /* CUDA runtime error (see last_error)         */
+#define LUCID_ERR_OVERFLOW (-7)   /* a traversal stack or queue bound was hit    */
+
+typedef struct LucidCudaCtx LucidCudaCtx;
+
+/* Render parameters of PyRenderer::render_tile / render_tile_gpu
+ * (pybind_renderer.hpp:185-194, 538-547). */
+typedef struct LucidRenderParams {
+    int tile_x, tile_y, tile_w, tile_h;
+    int full_w, full_h;
+    int samples;        /* samples in this call (jitter only when > 1) */
+    int sample_offset;  /* RNG sample index offset                      */
+    int max_depth;
+    int flags;          /* LUCID_RENDER_* bits                          */
+} LucidRenderParams;
+
+#define LUCID_RENDER_PROFILE 1   /* time every kernel launch (lucid_cuda_get_stats) */
+
+/* One record per (pixel, sample) for parity checking against a CPU
+ * implementation of the same integrator.  hash = FNV-1a 64 over the path's
+ * event words: per bounce [hit mesh, hit tri, native light] (-1 when absent),
+ * [scatter flag] under volume_mis, and [0x5EED0000 | occluded] per shadow
+ * ray. */
+typedef struct LucidSampleRecord {
+    float rgb[3];
+    int32_t primary_mesh, primary_tri;
+    uint32_t bounces;
+    uint32_t nee_tests, nee_occluded;
+    uint64_t hash;
+} LucidSampleRecord;
+
+/* Per-render statistics (the last render call with LUCID_RENDER_PROFILE). */
+#define LUCID_MAX_KERNEL_KINDS 8
+typedef struct LucidKernelStat {
+    char name[32];
+    int launches;
+    double total_ms;          /* sum of CUDA-event durations on the render stream */
+    double algo_bytes;        /* algorithmic bytes moved by all launches           */
+    double units;             /* rays / paths / pixels processed                    */
+} LucidKernelStat;
+
+typedef struct LucidRenderStats {
+    double total_ms;
+    double paths;             /* (pixel, sample) pairs traced          */
+    double segments;          /* extension rays traced (path segments) */
+    double shadow_rays;
+    int waves;
+    int num_kinds;
+    LucidKernelStat kinds[LUCID_MAX_KERNEL_KINDS];
+} LucidRenderStats;
+
+/* ---- context -------------------------------------------------------- */
+/* Replaces PyRenderer::PyRenderer (pybind_renderer.hpp:64-76). */
+int lucid_cuda_create(int device, LucidCudaCtx** out);
+void lucid_cuda_destroy(LucidCudaCtx* ctx);
+/* Message of the last failing call on this context ("" when none). */
+const char* lucid_cuda_last_error(LucidCudaCtx* ctx);
+/* Device name and compute capability, e.g. "NVIDIA B200 (sm_100)". */
+int lucid_cuda_device_info(LucidCudaCtx* ctx, char* buf, size_t cap);
+
+/* ---- scene / camera / algorithm ------------------------------------- */
+/* Replaces PyRenderer::load_scene_json (pybind_renderer.hpp:111-126) and
+ * loadSceneFromJsonString (:1258-1746): parses the JSON scene, builds the
+ * light CDF, uploads geometry and builds the device BVH. */
+int lucid_cuda_load_scene_json(LucidCudaCtx* ctx, const char* json, size_t len);
+/* Replaces PyRenderer::set_camera (pybind_renderer.hpp:131-160). */
+int lucid_cuda_set_camera(LucidCudaCtx* ctx, float pos_x, float pos_y, float pos_z, float dir_x, float dir_y,
+                          float dir_z, float up_x, float up_y, float up_z, float fov_deg);
+/* Replaces PyRenderer::set_algorithm (pybind_renderer.hpp:165-167):
+ * "simple", "nee", "mis", "volume_simple", "volume_mis" (others act as
+ * "nee", as in the reference's dispatch at :296-328). */
+int lucid_cuda_set_algorithm(LucidCudaCtx* ctx, const char* name);
+/* Scene statistics: meshes, triangles, native lights, scene lights,
+ * boundary-only meshes, volumes, BVH nodes, BVH leaves. */
+int lucid_cuda_scene_stats(LucidCudaCtx* ctx, int out8[8]);
+
+/* Host-only scene inspection (no GPU needed): parses the JSON exactly as
+ * lucid_cuda_load_scene_json does and reports counts (meshes, triangles,
+ * native lights, scene lights, boundary-only meshes, volumes, 0, 0) and, for
+ * up to `cap` scene lights in SceneLights order (scene_lights.hpp:56-122),
+ * the CDF value, area and emission rgb.  Returns the scene light count or a
+ * negative status. */
+int lucid_cuda_inspect_scene(const char* json, size_t len, int counts8[8], float* cdf, float* area,
+                             float* emission_rgb, int cap);
+
+/* ---- rendering ------------------------------------------------------- */
+/* Replaces PyRenderer::render_tile / render_tile_gpu
+ * (pybind_renderer.hpp:185-361, 538-666).  out_rgba: host buffer of
+ * tile_w*tile_h*4 floats: the SUM over the call's samples of each pixel's
+ * radiance, camera sensitivity applied, clamped >= 0, alpha 1, rows
+ * Y-flipped.  records (optional, may be NULL): tile_w*tile_h*samples entries
+ * in (row-major unflipped pixel, sample) order. */
+int lucid_cuda_render(LucidCudaCtx* ctx, const LucidRenderParams* params, float* out_rgba,
+                      LucidSampleRecord* records);
+/* Same render with the image left in device memory (d_out_rgba: a device
+ * pointer of tile_w*tile_h*4 floats); no host copies. */
+int lucid_cuda_render_device(LucidCudaCtx* ctx, const LucidRenderParams* params, float* d_out_rgba);
+/* Replaces PyRenderer::render_debug / render_debug_gpu
+ * (pybind_renderer.hpp:371-525): mode "normal", "albedo" or "emission" at
+ * the primary hit, no jitter, Y-flipped RGBA. */
+int lucid_cuda_render_debug(LucidCudaCtx* ctx, int tile_x, int tile_y, int tile_w, int tile_h, int full_w,
+                            int full_h, const char* mode, float* out_rgba);
+/* Statistics of the last render (kernel times need LUCID_RENDER_PROFILE). */
+int lucid_cuda_get_stats(LucidCudaCtx* ctx, LucidRenderStats* out);
+/* Path-pool capacity in paths (0 = automatic).  A render processes
+ * samples in waves of at most this many paths. */
+int lucid_cuda_set_wave_capacity(LucidCudaCtx* ctx, long long paths);
+
+/* ---- cancellation ---------------------------------------------------- */
+/* Replaces PyRenderer::cancel / is_cancelled / reset_cancel
+ * (pybind_renderer.hpp:86-102).  Thread-safe. */
+int lucid_cuda_cancel(LucidCudaCtx* ctx);
+int lucid_cuda_is_cancelled(LucidCudaCtx* ctx);
+int lucid_cuda_reset_cancel(LucidCudaCtx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LUCID_CUDA_H */
