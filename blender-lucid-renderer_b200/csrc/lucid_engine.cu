@@ -110,6 +110,8 @@ struct PathPool {
         sh_o.release(); sh_d.release(); sh_c.release(); lhit.release(); q0.release(); q1.release(); qs.release();
         counters.release(); errors.release(); rec_prim.release(); rec_cnt.release(); rec_hash.release();
         film.release(); out.release();
+        film_n = 0;
+        cap = 0;
     }
 };
 

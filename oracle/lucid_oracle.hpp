@@ -1395,6 +1395,7 @@ inline RGB render_pixel(const Scene& s, const SceneLights& sl, const Camera& cam
             r.d = primary_dir(cam, ndc_x + jx, ndc_y + jy, scale);
         }
         SampleRec* rec = recs ? &recs[si] : nullptr;
+        if (rec) *rec = SampleRec();
         RGB sr = trace(s, sl, r, max_depth, algo, rng, rec);
         if (rec) { rec->rgb[0] = sr.r; rec->rgb[1] = sr.g; rec->rgb[2] = sr.b; }
         rad = rad + sr;
