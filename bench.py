@@ -1,0 +1,313 @@
+"""Benchmark: progressive path tracing of the ~1M-triangle procedural scene.
+
+Workload (one "step" = one full render call): seeded procedural scene of
+1,026,574 triangles (200 fBm-displaced icospheres + ground + 2 emissive
+spheres + a homogeneous volume box), 16 point / 4 spot / 1 sun / 8 rectangle
+lights, 1920x1080, 64 samples per pixel in one call, max depth 16, the
+reference's `volume_mis` integrator.  Synthetic data: no public dataset.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+value   : samples/s over the whole job, device-timed (CUDA events on the
+          renderer's stream) with the image left in device memory.
+e2e     : samples/s through the C ABI call lucid_cuda_render with a host
+          output buffer (device->host copy of the image inside the timing).
+roofline: the dominant kernel's algorithmic bytes / its measured time,
+          against the measured HBM copy bandwidth.
+cpu_baseline: the CPU oracle (a restatement of the reference CPU path) on a
+          stratified 2% pixel crop at full spp, all host cores.
+Multi-GPU (torchrun): each rank renders the frame with its own sample range
+(sample_offset = rank * 64); no collective on the data path ("weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "blender-lucid-renderer_b200")
+sys.path.insert(0, PKG)
+
+W, H, SPP, DEPTH, ALGO = 1920, 1080, 64, 16, "volume_mis"
+SCENE_SEED = 2
+WORKLOAD = "procedural_1M_tris_1920x1080_64spp_depth16_volume_mis"
+CPU_TILES = (5, 4, 64, 33)   # 5x4 tiles of 64x33 px = 42,240 px (2.04%)
+
+
+def set_frame(w: int, h: int, spp: int) -> None:
+    global W, H, SPP, WORKLOAD
+    if (w, h, spp) != (W, H, SPP):
+        W, H, SPP = w, h, spp
+        WORKLOAD = f"procedural_1M_tris_{W}x{H}_{SPP}spp_depth{DEPTH}_{ALGO}"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def scene_json(cache_dir: str) -> tuple[str, tuple]:
+    import lucid_scenes as ls
+    os.makedirs(cache_dir, exist_ok=True)
+    path = os.path.join(cache_dir, f"procedural_seed{SCENE_SEED}.json")
+    sc, cam = ls.procedural_scene(seed=SCENE_SEED, workdir=cache_dir)   # also (re)writes the volume sidecar
+    if not os.path.exists(path):
+        with open(path + ".tmp", "w") as f:
+            f.write(ls.to_json(sc))
+        os.replace(path + ".tmp", path)
+    with open(path) as f:
+        return f.read(), cam
+
+
+def measured_peak():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(kernel: str):
+    """DRAM bytes per unit of work of `kernel` from the committed ncu summary
+    (profiles/*.md lines 'traffic_bytes_per_unit <kernel> <bytes>')."""
+    d = os.path.join(REPO, "profiles")
+    if not os.path.isdir(d):
+        return None
+    for fn in sorted(os.listdir(d)):
+        if not fn.endswith(".md"):
+            continue
+        with open(os.path.join(d, fn)) as f:
+            for line in f:
+                parts = line.strip().strip("`").split()
+                if len(parts) == 3 and parts[0] == "traffic_bytes_per_unit" and parts[1] == kernel:
+                    return float(parts[2])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"lucid_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines()]
+            rows = [[x.strip() for x in r] for r in rows if len(r) >= 7]
+        except Exception:
+            rows = []
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(rows[0][1]) if rows[0][1].replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(js: str, cam, steps: int = 1):
+    """Oracle (CPU restatement of the reference path) on the stratified crop."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    from oracle_ctypes import Oracle
+    o = Oracle(device_math=False, canonical_ties=False)   # libm + literal traversal order, as the reference
+    assert o.load_scene_json(js)
+    o.set_camera(*cam)
+    o.set_algorithm(ALGO)
+    nx, ny, tw, th = CPU_TILES
+    threads = os.cpu_count() or 1
+    vals = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        for j in range(ny):
+            for i in range(nx):
+                tx = (i * W) // nx + (W // nx - tw) // 2
+                ty = (j * H) // ny + (H // ny - th) // 2
+                o.render(tw, th, W, H, SPP, 0, DEPTH, tile_x=tx, tile_y=ty, threads=threads)
+        dt = time.perf_counter() - t0
+        vals.append(nx * ny * tw * th * SPP / dt)
+    sample = f"{nx * ny} stratified tiles of {tw}x{th} px ({nx * ny * tw * th} px, " \
+             f"{100.0 * nx * ny * tw * th / (W * H):.2f}% of the frame) at {SPP} spp, depth {DEPTH}, {ALGO}"
+    return vals, threads, sample
+
+
+def run_reference(args, rank: int):
+    if rank != 0:
+        return 0
+    js, cam = scene_json(args.cache)
+    cpu_baseline(js, cam, steps=max(0, min(args.warmup, 1)))   # warm caches (bounded)
+    vals, threads, sample = cpu_baseline(js, cam, steps=args.steps)
+    v = float(np.mean(vals))
+    line = {"impl": "reference", "metric": "samples/s", "value": v, "unit": "samples/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * (42240 * SPP) / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded procedural scene)",
+            "config": {"workload": WORKLOAD, "triangles": 1026574, "width": W, "height": H, "spp": SPP,
+                       "max_depth": DEPTH, "integrator": ALGO, "cpu_sample": sample},
+            "cpu_baseline": {"value": v, "unit": "samples/s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="lucid", choices=["lucid", "reference"])
+    ap.add_argument("--cache", default="/tmp/lucid_bench")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--width", type=int, default=W, help="smaller frames for profiling captures")
+    ap.add_argument("--height", type=int, default=H)
+    ap.add_argument("--spp", type=int, default=SPP)
+    args = ap.parse_args()
+    set_frame(args.width, args.height, args.spp)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank)
+
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local_rank))
+
+    import lucid_capi
+    js, cam = scene_json(args.cache)
+    ctx = lucid_capi.Context(local_rank)
+    t0 = time.perf_counter()
+    ctx.load_scene_json(js)
+    load_s = time.perf_counter() - t0
+    ctx.set_camera(*cam)
+    ctx.set_algorithm(ALGO)
+    stats0 = ctx.scene_stats()
+    log(f"[rank {rank}] {ctx.device_info()} scene {stats0} load {load_s:.2f}s")
+    dev = torch.device("cuda", local_rank)
+    d_out = torch.empty((H, W, 4), dtype=torch.float32, device=dev)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # 512 MB > L2
+    offset = rank * SPP
+
+    for _ in range(args.warmup):
+        ctx.render_device(d_out.data_ptr(), W, H, SPP, offset, DEPTH)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+    # timed: value (device events inside the library, per step, L2 flushed between steps)
+    per_step_ms, kern = [], {}
+    launches = 0
+    with ClockSampler(local_rank) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            ctx.render_device(d_out.data_ptr(), W, H, SPP, offset, DEPTH, profile=True)
+            st = ctx.stats()
+            per_step_ms.append(st["total_ms"])
+            for k, v in st["kernels"].items():
+                a = kern.setdefault(k, {"launches": 0, "total_ms": 0.0, "algo_bytes": 0.0, "units": 0.0})
+                for f in a:
+                    a[f] += v[f]
+                launches += v["launches"]
+            launches += 1   # k_output
+            segs, shadows = st["segments"], st["shadow_rays"]
+    torch.cuda.synchronize()
+    total_ms = float(np.sum(per_step_ms))
+    if dist:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+
+    # e2e: the reference-facing C ABI call with a host output buffer
+    host = np.zeros((H, W, 4), np.float32)
+    if dist:
+        dist.barrier()
+    e2e_ms = []
+    for _ in range(max(1, args.steps)):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.render(W, H, W, H, SPP, offset, DEPTH, out=host)
+        e2e_ms.append(1000.0 * (time.perf_counter() - t0))
+    e2e_total = float(np.sum(e2e_ms))
+    if dist:
+        t = torch.tensor([e2e_total], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+
+    samples_per_step = W * H * SPP
+    value = world * samples_per_step * args.steps / (total_ms / 1000.0)
+    e2e_value = world * samples_per_step * len(e2e_ms) / (e2e_total / 1000.0)
+    top = max(kern.items(), key=lambda kv: kv[1]["total_ms"])
+    peak, peak_kind = measured_peak()
+    achieved = top[1]["algo_bytes"] / (top[1]["total_ms"] / 1000.0) / 1e9
+    tpu = profile_traffic(top[0])
+    traffic = None if tpu is None else tpu * top[1]["units"] / max(1, top[1]["launches"])
+    mrays = (segs + shadows) / (per_step_ms[-1] / 1000.0) / 1e6
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        vals, threads, sample = cpu_baseline(js, cam, steps=1)
+        cpu = {"value": float(vals[0]), "unit": "samples/s", "cores": threads, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        line = {
+            "metric": "samples/s", "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+            "config": {"workload": WORKLOAD, "triangles": stats0[1], "width": W, "height": H, "spp": SPP,
+                       "max_depth": DEPTH, "integrator": ALGO, "scene_lights": stats0[3],
+                       "bvh_nodes": stats0[6], "parallelism": f"replicas{world} (sample ranges)",
+                       "l2": "512 MB buffer written between timed steps; scene + path state > L2",
+                       "scene_load_s": round(load_s, 3)},
+            "e2e": {"value": e2e_value, "unit": "samples/s", "h2d_bytes_per_step": 40,
+                    "d2h_bytes_per_step": W * H * 16},
+            "roofline": {"bound": "hbm", "kernel": top[0], "achieved": achieved, "peak": peak,
+                         "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic},
+            "kernels": {k: {"launches": v["launches"], "ms": round(v["total_ms"], 3),
+                            "share": round(v["total_ms"] / sum(x["total_ms"] for x in kern.values()), 4)}
+                        for k, v in kern.items()},
+            "mrays_per_s": mrays, "segments_per_step": segs, "shadow_rays_per_step": shadows,
+            "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

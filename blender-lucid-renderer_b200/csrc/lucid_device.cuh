@@ -463,6 +463,20 @@ LD float pdf_light(float area, V3 sp, V3 lp, V3 ln) {
 }
 LD float area_ratio(float num, float den) { return (den < MIN_AREA) ? 0.0f : num / den; }
 
+// SceneLights::selectLight's index (scene_lights.hpp:130-144):
+// min(std::lower_bound(cdf, u), n - 1).  The guide table narrows the binary
+// search to the entries between two bucket boundaries; the result is the
+// same index.  u is a multiple of 2^-23, so u * kLightGuide is exact.
+LD int select_light(const DevScene& sc, float u) {
+    int k = min((int)(u * (float)kLightGuide), kLightGuide - 1);
+    int lo = __ldg(&sc.light_guide[k]), hi = __ldg(&sc.light_guide[k + 1]);
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (__ldg(&sc.light_cdf[mid]) < u) lo = mid + 1; else hi = mid;
+    }
+    return min(lo, sc.num_lights - 1);
+}
+
 // ---------------------------------------------------------------- volumes
 constexpr float HG_INV_4PI = 1.0f / (4.0f * kPI);
 LD float hg_eval(float g, float c) {

@@ -53,8 +53,9 @@ struct DBuf {
 };
 
 struct DeviceScene {
-    DBuf<float4> bvh_tris, bnd_tris, prim_fn, prim_vn;
+    DBuf<float4> bvh_tris, bnd_tris, big_tris, prim_fn, prim_vn;
     DBuf<int4> prim_info;
+    DBuf<int> guide;
     DBuf<DevNode> nodes;
     DBuf<DevMaterial> materials;
     DBuf<DevLight> lights;
@@ -62,8 +63,8 @@ struct DeviceScene {
     DBuf<DevVolume> volumes;
     DevScene view{};
     void release() {
-        bvh_tris.release(); bnd_tris.release(); prim_fn.release(); prim_vn.release(); prim_info.release();
-        nodes.release(); materials.release(); lights.release(); cdf.release(); grid.release(); volumes.release();
+        bvh_tris.release(); bnd_tris.release(); big_tris.release(); prim_fn.release(); prim_vn.release(); prim_info.release();
+        nodes.release(); guide.release(); materials.release(); lights.release(); cdf.release(); grid.release(); volumes.release();
     }
 };
 
@@ -187,26 +188,110 @@ __global__ void k_raygen(FrameParams f, PathView pv) {
 }
 
 // ---------------------------------------------------------------- trace
-__global__ void __launch_bounds__(128) k_trace(DevScene sc, PathView pv, int* cnt, int identity, int records) {
+constexpr int kRounds = 4;         // closest hit: descend/test rounds per lane between refills
+constexpr int kShadowSteps = 12;   // any hit: node visits per lane between refills
+
+LD unsigned lanemask_lt() { return (1u << lane_id()) - 1u; }
+
+// Per-lane dynamic refill: lanes without a ray claim new ones together (one
+// atomic per warp per round); `exhausted` stops claiming once the queue is
+// drained.  Returns the claimed index or -1.
+LD int refill(int* cursor, int n, bool need, bool& exhausted) {
+    unsigned m = __ballot_sync(0xffffffffu, need && !exhausted);
+    if (m == 0) return -1;
+    int leader = __ffs(m) - 1;
+    int base = 0;
+    if ((int)lane_id() == leader) base = atomicAdd(cursor, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (!(need && !exhausted)) return -1;
+    int r = base + __popc(m & lanemask_lt());
+    if (r >= n) { exhausted = true; return -1; }
+    return r;
+}
+
+// Closest hit of camera rays: neighbouring pixels trace similar paths, so a
+// warp claims 32 consecutive rays at a time and keeps them together.
+__global__ void __launch_bounds__(128) k_trace_primary(DevScene sc, PathView pv, int* cnt, int records) {
     const int n = *(volatile int*)&cnt[0];
-    const int* q = identity ? nullptr : pv.q0;
     bool ok = true;
     for (;;) {
         int base = warp_fetch(&cnt[2]);
         if (base >= n) break;
-        int i = base + (int)lane_id();
-        if (i >= n) continue;
-        int id = q ? q[i] : i;
+        int id = base + (int)lane_id();
+        if (id >= n) continue;
         float4 ro = pv.ray_o[id], rd = pv.ray_d[id];
         V3 o = f3(ro), d = f3(rd);
-        int depth = __float_as_int(rd.w);
         HitRec h = closest_skip_boundaries(sc, o, d, ro.w, ok);
-        float lt = 1e30f;
-        int li = (depth == 0) ? -1 : native_lights_closest(sc, o, d, lt);
+        if (h.prim < 0) { h.t = 1e30f; h.u = 0.0f; h.v = 0.0f; }
         pv.hit[id] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
-        pv.lhit[id] = make_float2(__int_as_float(li), lt);
+        pv.lhit[id] = make_float2(__int_as_float(-1), 1e30f);   // native lights are invisible to camera rays
         if (records) {
             int4 pi = h.prim >= 0 ? sc.prim_info[h.prim] : make_int4(-1, -1, -1, 0);
+            pv.rec_prim[id] = make_int2(pi.x, pi.y);
+            pv.rec_cnt[id].x += 1;
+            unsigned long long hs = pv.rec_hash[id];
+            hs = hpush(hs, (uint32_t)pi.x);
+            hs = hpush(hs, (uint32_t)pi.y);
+            hs = hpush(hs, 0xffffffffu);
+            pv.rec_hash[id] = hs;
+        }
+    }
+    if (!ok) atomicAdd(&pv.errors[0], 1);
+}
+
+// Closest hit of extension rays (persistent, dynamic refill), including the
+// skip-volume-boundary rule (path_tracer.hpp:82-95) and native lights.
+__global__ void __launch_bounds__(128) k_trace(DevScene sc, PathView pv, int* cnt, int identity, int records) {
+    const int n = *(volatile int*)&cnt[0];
+    const int* q = identity ? nullptr : pv.q0;
+    int stack[kStack];
+    float stack_t[kStack];
+    Trav s;
+    bool active = false, exhausted = false, ok = true;
+    int id = 0, depth = 0, peek = 0;
+    float search = 0.0f;
+    for (;;) {
+        int r = refill(&cnt[2], n, !active, exhausted);
+        if (r >= 0) {
+            id = q ? q[r] : r;
+            float4 ro = pv.ray_o[id], rd = pv.ray_d[id];
+            depth = __float_as_int(rd.w);
+            trav_begin<false>(s, sc, f3(ro), f3(rd), ro.w, 1e30f);
+            search = ro.w;
+            peek = 0;
+            active = true;
+        }
+        if (__ballot_sync(0xffffffffu, active) == 0) break;
+        if (!active) continue;
+        if (!trav_run<false>(s, stack, stack_t, sc, ok, kRounds)) continue;
+        HitRec res = s.h;
+        if (sc.num_bnd_tris) {
+            // resolve the closest real surface against boundary-only hits
+            bool restart = false;
+            for (;;) {
+                HitRec real = s.h;
+                HitRec b = real;
+                if (real.prim < 0) b.t = 1e30f;
+                boundary_closest(sc, s.o, s.d, search, b);
+                if (b.prim < 0) { res.prim = -1; res.t = 1e30f; break; }
+                if (b.prim == real.prim) { res = real; break; }
+                search = b.t + 1e-3f;
+                if (++peek == 8) { res.prim = -1; res.t = 1e30f; break; }
+                if (real.prim >= 0 && real.t < search) {
+                    trav_begin<false>(s, sc, s.o, s.d, search, 1e30f);
+                    restart = true;
+                    break;
+                }
+            }
+            if (restart) continue;
+        }
+        if (res.prim < 0) { res.t = 1e30f; res.u = 0.0f; res.v = 0.0f; }
+        float lt = 1e30f;
+        int li = (depth == 0) ? -1 : native_lights_closest(sc, s.o, s.d, lt);
+        pv.hit[id] = make_float4(res.t, res.u, res.v, __int_as_float(res.prim));
+        pv.lhit[id] = make_float2(__int_as_float(li), lt);
+        if (records) {
+            int4 pi = res.prim >= 0 ? sc.prim_info[res.prim] : make_int4(-1, -1, -1, 0);
             if (depth == 0) pv.rec_prim[id] = make_int2(pi.x, pi.y);
             pv.rec_cnt[id].x += 1;
             unsigned long long hs = pv.rec_hash[id];
@@ -215,6 +300,7 @@ __global__ void __launch_bounds__(128) k_trace(DevScene sc, PathView pv, int* cn
             hs = hpush(hs, (uint32_t)li);
             pv.rec_hash[id] = hs;
         }
+        active = false;
     }
     if (!ok) atomicAdd(&pv.errors[0], 1);
 }
@@ -277,12 +363,7 @@ LD ShadeResult shade_path(const DevScene& sc, const FrameParams& f, const PathVi
                 float g = v.anisotropy;
                 if (sc.num_lights > 0) {
                     float usel = randf(rng);
-                    int li = 0;
-                    {
-                        int lo = 0, hi = sc.num_lights;
-                        while (lo < hi) { int mid = (lo + hi) >> 1; if (sc.light_cdf[mid] < usel) lo = mid + 1; else hi = mid; }
-                        li = min(lo, sc.num_lights - 1);
-                    }
+                    int li = select_light(sc, usel);
                     const DevLight& L = sc.lights[li];
                     float lsp = area_ratio(L.normal_area.w, sc.total_light_area);
                     if (lsp > 1e-6f) {
@@ -386,12 +467,7 @@ LD ShadeResult shade_path(const DevScene& sc, const FrameParams& f, const PathVi
         bool transmissive = m.transmission > 0.5f;
         if (nee && sc.num_lights > 0 && !has_em && !transmissive) {
             float usel = randf(rng);
-            int li;
-            {
-                int lo = 0, hi = sc.num_lights;
-                while (lo < hi) { int mid = (lo + hi) >> 1; if (sc.light_cdf[mid] < usel) lo = mid + 1; else hi = mid; }
-                li = min(lo, sc.num_lights - 1);
-            }
+            int li = select_light(sc, usel);
             const DevLight& L = sc.lights[li];
             float lsp = area_ratio(L.normal_area.w, sc.total_light_area);
             if (lsp > 1e-6f) {
@@ -484,20 +560,70 @@ __global__ void __launch_bounds__(128) k_shade(DevScene sc, FrameParams f, PathV
 }
 
 // ---------------------------------------------------------------- shadow
+// Shadow rays (persistent, dynamic refill): is_shadowed_skipping_volume_
+// boundaries (path_tracer.hpp:103-119) with any-hit BVH queries; a segment
+// ends at the nearest boundary-only hit, past which the probe advances 1 mm.
 __global__ void __launch_bounds__(128) k_shadow(DevScene sc, PathView pv, int* cnt, int records) {
     const int n = *(volatile int*)&cnt[1];
-    bool ok = true;
+    int stack[kStack];
+    Trav s;
+    bool active = false, exhausted = false, ok = true;
+    int id = 0, peek = 0;
+    float tmax = 0.0f, off = 0.0f, bt = -1.0f;
+    V3 po = v3(0.f, 0.f, 0.f), d = v3(0.f, 0.f, 1.f);
     for (;;) {
-        int base = warp_fetch(&cnt[4]);
-        if (base >= n) break;
-        int i = base + (int)lane_id();
-        if (i >= n) continue;
-        int id = pv.qs[i];
-        float4 so = pv.sh_o[id], sd = pv.sh_d[id];
-        bool occ = shadowed_skip_boundaries(sc, f3(so), f3(sd), so.w, ok);
+        int r = refill(&cnt[4], n, !active, exhausted);
+        int outcome = -1;   // -1 running, 0 unoccluded, 1 occluded
+        if (r >= 0) {
+            id = pv.qs[r];
+            float4 so = pv.sh_o[id], sd = pv.sh_d[id];
+            po = f3(so); d = f3(sd); tmax = so.w; off = 0.0f; peek = 0;
+            active = true;
+            // first segment
+            float rem = tmax - off;
+            if (rem <= 0.0f) outcome = 0;
+            else {
+                bt = -1.0f;
+                if (sc.num_bnd_tris) {
+                    HitRec b; b.t = rem; b.u = 0.f; b.v = 0.f; b.prim = -1;
+                    boundary_closest(sc, po, d, RAY_T_MIN, b);
+                    if (b.prim >= 0) bt = b.t;
+                }
+                trav_begin<true>(s, sc, po, d, RAY_T_MIN, bt >= 0.0f ? bt : rem);
+                if (s.any_hit) outcome = 1;
+            }
+        }
+        if (__ballot_sync(0xffffffffu, active) == 0) break;
+        if (!active) continue;
+        if (outcome < 0) {
+            if (!trav_run_any(s, stack, sc, ok, kShadowSteps)) continue;
+            if (s.any_hit) outcome = 1;
+            else if (bt < 0.0f) outcome = 0;
+            else {
+                // skip past the boundary hit and start the next segment
+                float skip = bt + 1e-3f;
+                off += skip;
+                po = po + d * skip;
+                if (++peek == 8) outcome = 0;
+                else {
+                    float rem = tmax - off;
+                    if (rem <= 0.0f) outcome = 0;
+                    else {
+                        bt = -1.0f;
+                        HitRec b; b.t = rem; b.u = 0.f; b.v = 0.f; b.prim = -1;
+                        boundary_closest(sc, po, d, RAY_T_MIN, b);
+                        if (b.prim >= 0) bt = b.t;
+                        trav_begin<true>(s, sc, po, d, RAY_T_MIN, bt >= 0.0f ? bt : rem);
+                        if (s.any_hit) outcome = 1;
+                    }
+                }
+            }
+            if (outcome < 0) continue;
+        }
+        bool occ = outcome == 1;
         if (!occ) {
-            float4 r = pv.rad[id], c = pv.sh_c[id];
-            pv.rad[id] = make_float4(r.x + c.x, r.y + c.y, r.z + c.z, 0.0f);
+            float4 ra = pv.rad[id], c = pv.sh_c[id];
+            pv.rad[id] = make_float4(ra.x + c.x, ra.y + c.y, ra.z + c.z, 0.0f);
         }
         if (records) {
             int4 rc = pv.rec_cnt[id];
@@ -506,6 +632,7 @@ __global__ void __launch_bounds__(128) k_shadow(DevScene sc, PathView pv, int* c
             pv.rec_cnt[id] = rc;
             pv.rec_hash[id] = hpush(pv.rec_hash[id], 0x5EED0000u | (occ ? 1u : 0u));
         }
+        active = false;
     }
     if (!ok) atomicAdd(&pv.errors[0], 1);
 }
@@ -847,6 +974,7 @@ int Engine::load_scene_json(const char* json, size_t len) {
     CK(up(D.materials, H.materials));
     CK(up(D.lights, H.lights));
     CK(up(D.cdf, H.cdf));
+    CK(up(D.guide, H.light_guide));
     CK(up(D.volumes, H.volumes));
     CK(up(D.grid, H.grid));
     DevScene& v = D.view;
@@ -859,6 +987,7 @@ int Engine::load_scene_json(const char* json, size_t len) {
     v.materials = D.materials.p;
     v.lights = D.lights.p;
     v.light_cdf = D.cdf.p;
+    v.light_guide = D.guide.p;
     v.num_lights = (int)H.lights.size();
     v.native_start = H.native_start;
     v.num_native = H.num_native;
@@ -878,19 +1007,69 @@ int Engine::load_scene_json(const char* json, size_t len) {
 int Engine::build_bvh() {
     DeviceScene& D = *ds_;
     const HostScene& H = host_;
-    std::vector<int> real;
-    real.reserve(H.num_prims);
+    // Scene bounds, then split off the largest triangles: at most kMaxBig
+    // whose bounding-box diagonal exceeds a quarter of the scene's.
+    float lo[3] = {1e30f, 1e30f, 1e30f}, hi[3] = {-1e30f, -1e30f, -1e30f};
     float maxabs = 0.0f;
+    std::vector<float> diag(H.num_prims, 0.0f);
     for (int p = 0; p < H.num_prims; ++p) {
         if (H.prim_boundary[p]) continue;
-        real.push_back(p);
+        float pl[3] = {1e30f, 1e30f, 1e30f}, ph[3] = {-1e30f, -1e30f, -1e30f};
         for (int k = 0; k < 3; ++k) {
             const float4& q = H.verts[3 * p + k];
-            maxabs = std::max(maxabs, std::max(std::fabs(q.x), std::max(std::fabs(q.y), std::fabs(q.z))));
+            const float c[3] = {q.x, q.y, q.z};
+            for (int a = 0; a < 3; ++a) {
+                pl[a] = std::min(pl[a], c[a]); ph[a] = std::max(ph[a], c[a]);
+                maxabs = std::max(maxabs, std::fabs(c[a]));
+            }
         }
+        for (int a = 0; a < 3; ++a) { lo[a] = std::min(lo[a], pl[a]); hi[a] = std::max(hi[a], ph[a]); }
+        diag[p] = std::sqrt((ph[0] - pl[0]) * (ph[0] - pl[0]) + (ph[1] - pl[1]) * (ph[1] - pl[1]) +
+                            (ph[2] - pl[2]) * (ph[2] - pl[2]));
     }
+    // secondary-ray origins lie on triangles (boundary ones included) or
+    // inside volume boxes: all of them bound the FMA slab test's error
+    for (int p = 0; p < H.num_prims; ++p)
+        if (H.prim_boundary[p])
+            for (int k = 0; k < 3; ++k) {
+                const float4& q = H.verts[3 * p + k];
+                maxabs = std::max(maxabs, std::max(std::fabs(q.x), std::max(std::fabs(q.y), std::fabs(q.z))));
+            }
+    for (const DevVolume& vol : H.volumes)
+        for (int a = 0; a < 3; ++a)
+            maxabs = std::max(maxabs, std::max(std::fabs(vol.wmin[a]), std::fabs(vol.wmax[a])));
+    float sdiag = std::sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
+                            (hi[2] - lo[2]) * (hi[2] - lo[2]));
+    const int kMaxBig = 32;
+    std::vector<int> bigc;
+    for (int p = 0; p < H.num_prims; ++p)
+        if (!H.prim_boundary[p] && diag[p] > 0.25f * sdiag) bigc.push_back(p);
+    std::sort(bigc.begin(), bigc.end(), [&](int a, int b) { return diag[a] > diag[b] || (diag[a] == diag[b] && a < b); });
+    if ((int)bigc.size() > kMaxBig) bigc.resize(kMaxBig);
+    // keep at least one triangle in the BVH so tiny scenes still build one
+    int nonbnd = 0;
+    for (int p = 0; p < H.num_prims; ++p) nonbnd += !H.prim_boundary[p];
+    if ((int)bigc.size() == nonbnd) bigc.clear();
+    std::vector<unsigned char> is_big(H.num_prims, 0);
+    std::vector<float4> big;
+    for (int p : bigc) is_big[p] = 1;
+    for (int p = 0; p < H.num_prims; ++p)
+        if (is_big[p]) for (int k = 0; k < 3; ++k) big.push_back(H.tri[3 * p + k]);
+    std::vector<int> real;
+    real.reserve(H.num_prims);
+    for (int p = 0; p < H.num_prims; ++p)
+        if (!H.prim_boundary[p] && !is_big[p]) real.push_back(p);
     int n = (int)real.size();
     DevScene& v = D.view;
+    {
+        cudaError_t e = D.big_tris.alloc(big.size());
+        if (e != cudaSuccess) return fail(LUCID_ERR_OOM, "big triangle list allocation failed");
+        if (!big.empty())
+            CK(cudaMemcpyAsync(D.big_tris.p, big.data(), big.size() * sizeof(float4), cudaMemcpyHostToDevice, S(stream_)));
+        v.big_tris = D.big_tris.p;
+        v.num_big_tris = (int)(big.size() / 3);
+        num_big_ = v.num_big_tris;
+    }
     v.num_bvh_tris = n;
     bvh_nodes_ = 0; bvh_leaves_ = 0; bvh_depth_ = 0;
     if (n == 0) { v.root = 0; v.nodes = nullptr; v.bvh_tris = nullptr; return LUCID_OK; }
@@ -1019,19 +1198,19 @@ namespace {
 //   raygen: rng 16 + ray 32 + throughput 16 + radiance 16            = 80 / path
 //   film  : radiance 16 / path + film 32 / pixel
 constexpr double kBytesTrace = 60, kBytesShade = 340, kBytesShadow = 84, kBytesRaygen = 80, kBytesFilm = 16;
-enum Kind { K_RAYGEN, K_TRACE, K_SHADE, K_SHADOW, K_FILM, K_NUM };
-const char* kKindNames[K_NUM] = {"k_raygen", "k_trace", "k_shade", "k_shadow", "k_film"};
-const double kKindBytes[K_NUM] = {kBytesRaygen, kBytesTrace, kBytesShade, kBytesShadow, kBytesFilm};
+enum Kind { K_RAYGEN, K_TRACE0, K_TRACE, K_SHADE, K_SHADOW, K_FILM, K_NUM };
+const char* kKindNames[K_NUM] = {"k_raygen", "k_trace_primary", "k_trace", "k_shade", "k_shadow", "k_film"};
+const double kKindBytes[K_NUM] = {kBytesRaygen, kBytesTrace, kBytesTrace, kBytesShade, kBytesShadow, kBytesFilm};
 }  // namespace
 
 int Engine::render(const LucidRenderParams& p, float* out_host, LucidSampleRecord* recs, float* out_device) {
-    CK(cudaSetDevice(device_));
     reset_cancel();
     if (p.tile_w <= 0 || p.tile_h <= 0 || p.full_w <= 0 || p.full_h <= 0)
         return fail(LUCID_ERR_INVALID, "tile and image sizes must be positive");
     size_t np = (size_t)p.tile_w * p.tile_h;
     if (out_host) std::fill(out_host, out_host + np * 4, 0.0f);
     if (!scene_loaded_ || !camera_set_) return fail(LUCID_ERR_NO_SCENE, "scene or camera not set");
+    CK(cudaSetDevice(device_));
     if (p.samples <= 0) return fail(LUCID_ERR_INVALID, "samples must be >= 1");
     if (p.max_depth > kMaxDepth) return fail(LUCID_ERR_INVALID, "max_depth too large");
     if (np > (size_t)0x7fffffff / 2) return fail(LUCID_ERR_INVALID, "tile too large");
@@ -1065,10 +1244,12 @@ int Engine::render(const LucidRenderParams& p, float* out_host, LucidSampleRecor
     f.records = records ? 1 : 0;
 
     // persistent grids: a whole number of CTAs per SM
-    int occ_t = 1, occ_s = 1, occ_h = 1;
+    int occ_t = 1, occ_s = 1, occ_h = 1, occ_t0 = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t0, k_trace_primary, 128, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t, k_trace, 128, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, k_shade, 128, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, k_shadow, 128, 0);
+    const int g_trace0 = num_sms_ * std::max(1, occ_t0);
     const int g_trace = num_sms_ * std::max(1, occ_t), g_shade = num_sms_ * std::max(1, occ_s),
               g_shadow = num_sms_ * std::max(1, occ_h);
 
@@ -1112,8 +1293,13 @@ int Engine::render(const LucidRenderParams& p, float* out_host, LucidSampleRecor
             int* qin = (depth & 1) ? P.q1.p : P.q0.p;
             int* qout = (depth & 1) ? P.q0.p : P.q1.p;
             pv.q0 = qin;
-            e = ev_begin(K_TRACE, depth);
-            k_trace<<<g_trace, 128, 0, st>>>(ds_->view, pv, cnt, depth == 0, f.records);
+            if (depth == 0) {
+                e = ev_begin(K_TRACE0, depth);
+                k_trace_primary<<<g_trace0, 128, 0, st>>>(ds_->view, pv, cnt, f.records);
+            } else {
+                e = ev_begin(K_TRACE, depth);
+                k_trace<<<g_trace, 128, 0, st>>>(ds_->view, pv, cnt, 0, f.records);
+            }
             ev_end(e);
             e = ev_begin(K_SHADE, depth);
             k_shade<<<g_shade, 128, 0, st>>>(ds_->view, f, pv, cnt, cnt_next, depth == 0, qin, qout);
@@ -1137,7 +1323,7 @@ int Engine::render(const LucidRenderParams& p, float* out_host, LucidSampleRecor
             kind_units[K_RAYGEN] += f.n_wave;
             kind_units[K_FILM] += f.n_wave;
             for (int d = 0; d < p.max_depth; ++d) {
-                kind_units[K_TRACE] += hcnt[kCountersPerDepth * d];
+                kind_units[d == 0 ? K_TRACE0 : K_TRACE] += hcnt[kCountersPerDepth * d];
                 kind_units[K_SHADE] += hcnt[kCountersPerDepth * d];
                 kind_units[K_SHADOW] += hcnt[kCountersPerDepth * d + 1];
             }
@@ -1186,7 +1372,6 @@ int Engine::render(const LucidRenderParams& p, float* out_host, LucidSampleRecor
 }
 
 int Engine::render_debug(int tx, int ty, int tw, int th, int fw, int fh, const char* mode, float* out_host) {
-    CK(cudaSetDevice(device_));
     reset_cancel();
     if (tw <= 0 || th <= 0 || fw <= 0 || fh <= 0) return fail(LUCID_ERR_INVALID, "tile and image sizes must be positive");
     size_t np = (size_t)tw * th;
@@ -1202,6 +1387,7 @@ int Engine::render_debug(int tx, int ty, int tw, int th, int fw, int fh, const c
         for (size_t i = 0; i < np; ++i) { out_host[4 * i] = 1.0f; out_host[4 * i + 1] = 0.0f; out_host[4 * i + 2] = 1.0f; out_host[4 * i + 3] = 1.0f; }
         return LUCID_OK;
     }
+    CK(cudaSetDevice(device_));
     cudaStream_t st = S(stream_);
     PathPool& P = *pool_;
     if (P.film_n < np) { CK(P.film.alloc(np)); CK(P.out.alloc(np)); P.film_n = np; }

@@ -55,7 +55,7 @@ private:
     std::atomic<bool> cancel_{false};
     std::string err_;
     LucidRenderStats stats_{};
-    int bvh_nodes_ = 0, bvh_leaves_ = 0, bvh_depth_ = 0;
+    int bvh_nodes_ = 0, bvh_leaves_ = 0, bvh_depth_ = 0, num_big_ = 0;
 };
 
 }  // namespace lucid

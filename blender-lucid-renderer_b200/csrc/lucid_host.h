@@ -25,6 +25,7 @@ struct HostScene {
     std::vector<DevMaterial> materials;
     std::vector<DevLight> lights;
     std::vector<float> cdf;
+    std::vector<int> light_guide;   // kLightGuide + 1 entries
     float total_light_area = 0.0f;
     int native_start = 0;
     int num_native = 0;

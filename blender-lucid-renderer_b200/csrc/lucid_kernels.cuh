@@ -14,19 +14,40 @@
 namespace lucid {
 
 // Möller–Trumbore (intersection.hpp:335-396) on a triangle stored as
-// (v0, e1 = v1 - v0, e2 = v2 - v0); identical operation order.
+// (v0, e1 = v1 - v0, e2 = v2 - v0); identical operation order, so accepted
+// hits and their (t, u, v) equal the reference's bit for bit.
+//
+// The three IEEE divisions are deferred behind a conservative prefilter on
+// the undivided numerators: with D = |det| and s = sign(det), a triangle is
+// rejected early only when s*num lies outside the accepted interval by a
+// relative margin of 2^-20 (or 2^-18 for u + v), far above the few-ulp
+// rounding of the quotients.  Every triangle the prefilter passes is then
+// decided by the exact divided test, so the result is unchanged.
 LD bool isect_tri(V3 o, V3 d, V3 v0, V3 e1, V3 e2, float tmin, float tmax, float& t, float& u, float& v) {
     V3 pvec = cross(d, e2);
     float det = dot(e1, pvec);
     const float eps = 1e-6f * 1e-6f;
     if (det > -eps && det < eps) return false;
     V3 tvec = o - v0;
-    float uu = dot(tvec, pvec) / det;
-    if (uu < 0.0f || uu > 1.0f) return false;
+    float un = dot(tvec, pvec);
+    float D = fabsf(det);
+    float sg = det < 0.0f ? -1.0f : 1.0f;
+    float a = un * sg;
+    const float lo = -D * 9.5367431640625e-07f;            // -D * 2^-20 (exact)
+    if (a < lo || a > D * 1.00000095367431640625f) return false;
     V3 qvec = cross(tvec, e1);
-    float vv = dot(d, qvec) / det;
+    float vn = dot(d, qvec);
+    float b = vn * sg;
+    if (b < lo || a + b > D * 1.000003814697265625f) return false;   // 1 + 2^-18
+    float tn = dot(e2, qvec);
+    float c = tn * sg;
+    if (c > D * tmax * 1.00000095367431640625f) return false;
+    if (c < D * tmin * 0.99999904632568359375f + lo) return false;
+    float uu = un / det;
+    if (uu < 0.0f || uu > 1.0f) return false;
+    float vv = vn / det;
     if (vv < 0.0f || uu + vv > 1.0f) return false;
-    float tt = dot(e2, qvec) / det;
+    float tt = tn / det;
     if (tt >= tmin && tt <= tmax) { t = tt; u = uu; v = vv; return true; }
     return false;
 }
@@ -84,11 +105,51 @@ LD bool box_hit(float4 bmin, float4 bmax, V3 o, V3 inv, float tmin, float tfar_l
     return t0 <= t1 * 1.00000095367431640625f;   // widen by 2^-20
 }
 
+// Brute-force closest / any over a short triangle list (same tie rule).
+LD void list_closest(const float4* tris, int count, V3 o, V3 d, float tmin, HitRec& h) {
+    for (int k = 0; k < count; ++k) {
+        V3 v0, e1, e2;
+        int prim;
+        load_tri(tris, k, v0, e1, e2, prim);
+        float t, u, v;
+        if (isect_tri(o, d, v0, e1, e2, tmin, h.t, t, u, v)) {
+            if (t < h.t || prim > h.prim) { h.t = t; h.u = u; h.v = v; h.prim = prim; }
+        }
+    }
+}
+LD bool list_any(const float4* tris, int count, V3 o, V3 d, float tmin, float tmax) {
+    for (int k = 0; k < count; ++k) {
+        V3 v0, e1, e2;
+        int prim;
+        load_tri(tris, k, v0, e1, e2, prim);
+        float t, u, v;
+        if (isect_tri(o, d, v0, e1, e2, tmin, tmax, t, u, v)) return true;
+    }
+    return false;
+}
+
+// FMA slab test for rays whose origin lies inside the scene bounds (every
+// secondary and shadow ray): t = b*inv - o*inv with one fused rounding.  Its
+// absolute error, about 5 * max|coordinate| * 2^-24 in distance units, is
+// 16x below the 2^-20 * max|coordinate| padding of every BVH box, so the
+// test stays conservative.  Camera rays, whose origin can be far outside the
+// scene, use box_hit above.
+LD bool box_hit_fma(float4 bmin, float4 bmax, V3 ooi, V3 inv, float tmin, float tfar_lim, float& tn) {
+    float tx0 = __fmaf_rn(bmin.x, inv.x, ooi.x), tx1 = __fmaf_rn(bmax.x, inv.x, ooi.x);
+    float ty0 = __fmaf_rn(bmin.y, inv.y, ooi.y), ty1 = __fmaf_rn(bmax.y, inv.y, ooi.y);
+    float tz0 = __fmaf_rn(bmin.z, inv.z, ooi.z), tz1 = __fmaf_rn(bmax.z, inv.z, ooi.z);
+    float t0 = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
+    float t1 = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tfar_lim));
+    tn = t0;
+    return t0 <= t1 * 1.00000095367431640625f;
+}
+
 constexpr int kStack = 64;
 
 // Closest hit over the BVH (non-boundary triangles) in [tmin, h.t].
 // Returns false when the traversal stack overflowed (a hit may be missed).
 LD bool bvh_closest(const DevScene& sc, V3 o, V3 d, float tmin, HitRec& h) {
+    if (sc.num_big_tris) list_closest(sc.big_tris, sc.num_big_tris, o, d, tmin, h);
     if (sc.num_bvh_tris == 0) return true;
     if (sc.root < 0) { test_leaf_closest(sc.bvh_tris, sc.root, o, d, tmin, h); return true; }
     V3 inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
@@ -123,6 +184,7 @@ LD bool bvh_closest(const DevScene& sc, V3 o, V3 d, float tmin, HitRec& h) {
 
 // Any hit over the BVH in [tmin, tmax]; overflow reported through ok.
 LD bool bvh_any(const DevScene& sc, V3 o, V3 d, float tmin, float tmax, bool& ok) {
+    if (sc.num_big_tris && list_any(sc.big_tris, sc.num_big_tris, o, d, tmin, tmax)) return true;
     if (sc.num_bvh_tris == 0) return false;
     if (sc.root < 0) return test_leaf_any(sc.bvh_tris, sc.root, o, d, tmin, tmax);
     V3 inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
@@ -150,6 +212,155 @@ LD bool bvh_any(const DevScene& sc, V3 o, V3 d, float tmin, float tmax, bool& ok
             if (sp == 0) break;
             node = stack[--sp];
         }
+    }
+    return false;
+}
+
+// ---- resumable while-while traversal for the persistent kernels ----
+// Aila & Laine ("Understanding the efficiency of ray traversal on GPUs",
+// HPG 2009): each lane descends internal nodes until it has found a leaf,
+// postponing the leaf; the warp leaves the descent loop once every lane holds
+// a leaf (or is done), then all lanes test their leaves together.  The stack
+// keeps each entry's entry distance so closest-hit queries skip entries that
+// a nearer hit has made unreachable.  A lane runs a bounded number of
+// descend/test rounds between work refills.
+struct Trav {
+    V3 o, d, inv, ooi;   // ooi = -o * inv
+    float tmin;
+    HitRec h;        // closest: running best; any: h.t is the fixed limit
+    int node;        // next entry (internal node index or leaf code), or kTravDone
+    int leaf;        // postponed leaf code, 0 when none
+    int sp;
+    bool any_hit;
+};
+constexpr int kTravDone = 0x7fffffff;
+
+template <bool ANY>
+LD void trav_begin(Trav& s, const DevScene& sc, V3 o, V3 d, float tmin, float tmax) {
+    s.o = o; s.d = d;
+    s.inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    s.ooi = v3(-o.x * s.inv.x, -o.y * s.inv.y, -o.z * s.inv.z);
+    s.tmin = tmin;
+    s.h.t = tmax; s.h.u = 0.0f; s.h.v = 0.0f; s.h.prim = -1;
+    s.sp = 0;
+    s.leaf = 0;
+    s.any_hit = false;
+    s.node = kTravDone;
+    if (sc.num_big_tris) {
+        if (ANY) {
+            if (list_any(sc.big_tris, sc.num_big_tris, o, d, tmin, tmax)) { s.any_hit = true; return; }
+        } else {
+            list_closest(sc.big_tris, sc.num_big_tris, o, d, tmin, s.h);
+        }
+    }
+    if (sc.num_bvh_tris == 0) return;
+    s.node = sc.root;   // a leaf code when the whole BVH is one leaf
+}
+
+LD int trav_pop(Trav& s, const int* stack, const float* stack_t) {
+    while (s.sp > 0) {
+        --s.sp;
+        if (stack_t[s.sp] <= s.h.t * 1.00000095367431640625f) return stack[s.sp];
+    }
+    return kTravDone;
+}
+
+// Any-hit stepping for shadow rays: leaves are tested as soon as their box
+// is hit (an occluder found early ends the ray), one node per step.
+LD bool trav_run_any(Trav& s, int* stack, const DevScene& sc, bool& ok, int steps) {
+    for (int k = 0; k < steps; ++k) {
+        if (s.node == kTravDone) return true;
+        if (s.node < 0) {   // the whole BVH is a single leaf
+            s.any_hit = test_leaf_any(sc.bvh_tris, s.node, s.o, s.d, s.tmin, s.h.t);
+            s.node = kTravDone;
+            return true;
+        }
+        const DevNode* n = sc.nodes + s.node;
+        float4 a = __ldg(&n->lmin_lc), b = __ldg(&n->lmax_rc), c = __ldg(&n->rmin), e = __ldg(&n->rmax);
+        int cl = __float_as_int(a.w), cr = __float_as_int(b.w);
+        float tl, tr;
+        bool hl = box_hit_fma(a, b, s.ooi, s.inv, s.tmin, s.h.t, tl);
+        bool hr = box_hit_fma(c, e, s.ooi, s.inv, s.tmin, s.h.t, tr);
+        if (hl && cl < 0) {
+            if (test_leaf_any(sc.bvh_tris, cl, s.o, s.d, s.tmin, s.h.t)) { s.any_hit = true; s.node = kTravDone; return true; }
+            hl = false;
+        }
+        if (hr && cr < 0) {
+            if (test_leaf_any(sc.bvh_tris, cr, s.o, s.d, s.tmin, s.h.t)) { s.any_hit = true; s.node = kTravDone; return true; }
+            hr = false;
+        }
+        if (hl && hr) {
+            bool lfirst = tl <= tr;
+            if (s.sp < kStack) stack[s.sp++] = lfirst ? cr : cl; else ok = false;
+            s.node = lfirst ? cl : cr;
+        } else if (hl) {
+            s.node = cl;
+        } else if (hr) {
+            s.node = cr;
+        } else if (s.sp == 0) {
+            s.node = kTravDone;
+            return true;
+        } else {
+            s.node = stack[--s.sp];
+        }
+    }
+    return false;
+}
+
+// Runs up to `rounds` descend/test rounds; returns true when finished.
+template <bool ANY>
+LD bool trav_run(Trav& s, int* stack, float* stack_t, const DevScene& sc, bool& ok, int rounds) {
+    for (int r = 0; r < rounds; ++r) {
+        // descend until this lane holds a leaf (speculatively with its warp)
+        while (s.node != kTravDone && s.leaf == 0) {
+            if (s.node < 0) {                      // a leaf reached by popping
+                s.leaf = s.node;
+                s.node = trav_pop(s, stack, stack_t);
+                break;
+            }
+            const DevNode* n = sc.nodes + s.node;
+            float4 a = __ldg(&n->lmin_lc), b = __ldg(&n->lmax_rc), c = __ldg(&n->rmin), e = __ldg(&n->rmax);
+            int cl = __float_as_int(a.w), cr = __float_as_int(b.w);
+            float tl, tr;
+            bool hl = box_hit_fma(a, b, s.ooi, s.inv, s.tmin, s.h.t, tl);
+            bool hr = box_hit_fma(c, e, s.ooi, s.inv, s.tmin, s.h.t, tr);
+            if (hl && hr) {
+                bool lfirst = tl <= tr;
+                if (s.sp < kStack) {
+                    stack[s.sp] = lfirst ? cr : cl;
+                    stack_t[s.sp] = lfirst ? tr : tl;
+                    ++s.sp;
+                } else {
+                    ok = false;
+                }
+                s.node = lfirst ? cl : cr;
+            } else if (hl) {
+                s.node = cl;
+            } else if (hr) {
+                s.node = cr;
+            } else {
+                s.node = trav_pop(s, stack, stack_t);
+            }
+            if (s.node != kTravDone && s.node < 0) {   // postpone the leaf, keep descending
+                s.leaf = s.node;
+                s.node = trav_pop(s, stack, stack_t);
+            }
+            if (!__any_sync(__activemask(), s.leaf == 0 && s.node != kTravDone)) break;
+        }
+        if (s.leaf != 0) {
+            if (ANY) {
+                if (test_leaf_any(sc.bvh_tris, s.leaf, s.o, s.d, s.tmin, s.h.t)) {
+                    s.any_hit = true;
+                    s.node = kTravDone;
+                    s.leaf = 0;
+                    return true;
+                }
+            } else {
+                test_leaf_closest(sc.bvh_tris, s.leaf, s.o, s.d, s.tmin, s.h);
+            }
+            s.leaf = 0;
+        }
+        if (s.node == kTravDone) return true;
     }
     return false;
 }

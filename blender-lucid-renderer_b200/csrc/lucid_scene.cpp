@@ -6,6 +6,7 @@
 // (light/scene_lights.hpp:56-122): the same keys, defaults and float
 // conversions, so the uploaded lights, CDF and normals equal the CPU
 // renderer's bit for bit.  Compiled with -ffp-contract=off.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -346,6 +347,11 @@ bool parse_scene_json(const char* text, size_t length, HostScene& S, std::string
         for (size_t i = 0; i < S.lights.size(); ++i) {
             cum += S.lights[i].normal_area.w;
             S.cdf[i] = (total < 1e-6f) ? 0.0f : cum / total;
+        }
+        S.light_guide.resize(kLightGuide + 1);
+        for (int k = 0; k <= kLightGuide; ++k) {
+            float x = (float)k / (float)kLightGuide;   // exact: power-of-two denominator
+            S.light_guide[k] = (int)(std::lower_bound(S.cdf.begin(), S.cdf.end(), x) - S.cdf.begin());
         }
     } catch (const std::exception& e) {
         err = std::string("malformed scene: ") + e.what();

@@ -11,6 +11,7 @@ namespace lucid {
 
 enum LightTypeId { LIGHT_EMISSIVE = 0, LIGHT_POINT = 1, LIGHT_SUN = 2, LIGHT_SPOT = 3, LIGHT_AREA = 4 };
 enum AreaShapeId { AREA_SQUARE = 0, AREA_RECTANGLE = 1, AREA_DISK = 2, AREA_ELLIPSE = 3 };
+constexpr int kLightGuide = 1024;
 enum AlgoId { ALGO_SIMPLE = 0, ALGO_NEE = 1, ALGO_MIS = 2, ALGO_VOLUME_SIMPLE = 3, ALGO_VOLUME_MIS = 4 };
 
 // One scene light in SceneLights order (emissive triangles, then native
@@ -64,6 +65,12 @@ struct DevScene {
     // boundary-only triangles (tested by brute force): 3 float4 each
     const float4* bnd_tris;
     int num_bnd_tris;
+    // the few triangles whose bounds span a large part of the scene (ground
+    // planes, walls) are kept out of the BVH and tested first by brute force:
+    // in a Morton-ordered hierarchy they would inflate every box on their
+    // root path
+    const float4* big_tris;
+    int num_big_tris;
     // per global prim (mesh-major order)
     const int4* prim_info;          // mesh, local tri, light index (-1), smooth flag
     const float4* prim_fn;          // face normal
@@ -72,6 +79,9 @@ struct DevScene {
     // lights
     const DevLight* lights;
     const float* light_cdf;
+    // guide[k] = lower_bound(cdf, k / kLightGuide) for k = 0..kLightGuide:
+    // brackets std::lower_bound(cdf, u) for u in [k, k+1) / kLightGuide
+    const int* light_guide;
     int num_lights;
     int native_start;
     int num_native;
