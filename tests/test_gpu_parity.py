@@ -75,3 +75,17 @@ def test_debug_passes_match_oracle(ctx, workdir):
         g = ctx.render_debug(name, 40, 30)
         c = o.render_debug(mode, 40, 30)
         assert np.array_equal(g, c), name
+
+
+@pytest.mark.parametrize("name", ["cornell_mis", "cornell_nee", "all_lights_volume_mis", "mirror_mis"])
+def test_against_golden_fixtures(ctx, workdir, name):
+    """The CUDA tracer reproduces the committed oracle fixtures
+    (tests/golden/make_golden.py) without running the oracle."""
+    from golden_cases import GOLDEN, load_golden
+    scene, algo, w, h, spp, depth, off = GOLDEN[name]
+    sc, cam = scene_and_camera(scene, workdir)
+    gimg, grec = render_gpu(ctx, sc, cam, algo, w, h, spp, depth, offset=off)
+    fimg, frec = load_golden(name)
+    r = compare_records(grec, frec)
+    assert r["primary"] == 0 and r["hash"] == 0 and r["counts"] == 0 and r["rgb"] == 0, r
+    np.testing.assert_allclose(gimg, fimg, rtol=1e-4, atol=1e-5)
