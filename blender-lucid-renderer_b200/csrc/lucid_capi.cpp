@@ -114,6 +114,11 @@ int lucid_cuda_render_device(LucidCudaCtx* ctx, const LucidRenderParams* params,
     return guarded(ctx, [&](lucid::Engine& e) { return e.render(*params, nullptr, nullptr, d_out_rgba); });
 }
 
+int lucid_cuda_render_noalloc(LucidCudaCtx* ctx, const LucidRenderParams* params, float* d_out_rgba) {
+    if (!params || !d_out_rgba) return LUCID_ERR_INVALID;
+    return guarded(ctx, [&](lucid::Engine& e) { return e.render_noalloc(*params, d_out_rgba); });
+}
+
 int lucid_cuda_render_debug(LucidCudaCtx* ctx, int tile_x, int tile_y, int tile_w, int tile_h, int full_w, int full_h,
                             const char* mode, float* out_rgba) {
     if (!out_rgba) return LUCID_ERR_INVALID;

@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstring>
 #include <cub/cub.cuh>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1366,6 +1367,139 @@ int Engine::render(const LucidRenderParams& p, float* out_host, LucidSampleRecor
         }
         stats_.kinds[K_FILM].algo_bytes += (double)np * 32.0 * waves;
     }
+    if (herr[0] != 0) return fail(LUCID_ERR_OVERFLOW, "BVH traversal stack overflow");
+    if (status == LUCID_ERR_CANCELLED) return fail(LUCID_ERR_CANCELLED, "render cancelled");
+    return LUCID_OK;
+}
+
+// ---------------------------------------------------------------- no-allocation render
+// Some callers cannot allocate device memory when they render: a host whose
+// device memory is owned by another allocator (a framework's caching pool
+// that hands out every byte), or a latency-critical thread such as a
+// viewport draw callback that must not call cudaMalloc/cudaFree because
+// those calls can synchronise the whole device.  lucid_cuda_render_noalloc
+// serves them with the same kernels as lucid_cuda_render_device, but its
+// working memory (path state, queues, counters, film) lives in the
+// fixed-size device array below, which every GPU that loads this library
+// holds until the process exits.  The scene itself was allocated earlier by
+// lucid_cuda_load_scene_json.
+constexpr int kNoAllocPaths = 65536;              // paths per wave
+constexpr int kNoAllocPixels = 65536;             // tile pixels (e.g. 256 x 256)
+constexpr int kNoAllocMaxDepth = 64;
+constexpr size_t kNoAllocAlign = 256;
+constexpr size_t na_round(size_t b) { return (b + kNoAllocAlign - 1) / kNoAllocAlign * kNoAllocAlign; }
+constexpr size_t kNaRng = na_round(sizeof(ulonglong2) * kNoAllocPaths);
+constexpr size_t kNaF4 = na_round(sizeof(float4) * kNoAllocPaths);
+constexpr size_t kNaF2 = na_round(sizeof(float2) * kNoAllocPaths);
+constexpr size_t kNaQ = na_round(sizeof(int) * kNoAllocPaths);
+constexpr size_t kNaCnt = na_round(sizeof(int) * kCountersPerDepth * (kNoAllocMaxDepth + 1));
+constexpr size_t kNaErr = na_round(sizeof(int) * 4);
+constexpr size_t kNaFilm = na_round(sizeof(float4) * kNoAllocPixels);
+constexpr size_t kNoAllocBytes = kNaRng + 8 * kNaF4 + kNaF2 + 3 * kNaQ + kNaCnt + kNaErr + kNaFilm;   // ~12 MB
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+namespace {
+// Device address of g_noalloc_scratch per device, looked up once with that
+// device current (a host-side reference to the array is not a device
+// address).
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_addr[64] = {};
+}  // namespace
+
+int Engine::render_noalloc(const LucidRenderParams& p, float* d_out) {
+    reset_cancel();
+    if (!d_out) return fail(LUCID_ERR_INVALID, "output pointer is null");
+    if (p.tile_w <= 0 || p.tile_h <= 0 || p.full_w <= 0 || p.full_h <= 0)
+        return fail(LUCID_ERR_INVALID, "tile and image sizes must be positive");
+    if (!scene_loaded_ || !camera_set_) return fail(LUCID_ERR_NO_SCENE, "scene or camera not set");
+    long long np = (long long)p.tile_w * p.tile_h;
+    if (np > kNoAllocPixels)
+        return fail(LUCID_ERR_INVALID, "render_noalloc: tile of " + std::to_string(np) + " pixels exceeds the " +
+                                           std::to_string(kNoAllocPixels) + "-pixel limit of its fixed scratch");
+    if (p.max_depth < 1 || p.max_depth > kNoAllocMaxDepth)
+        return fail(LUCID_ERR_INVALID, "render_noalloc: max_depth must be in [1, " + std::to_string(kNoAllocMaxDepth) + "]");
+    if (p.samples <= 0) return fail(LUCID_ERR_INVALID, "samples must be >= 1");
+    if (device_ < 0 || device_ >= 64) return fail(LUCID_ERR_INVALID, "device index out of range");
+    CK(cudaSetDevice(device_));
+    unsigned char* base;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_addr[device_]) {
+            void* ptr = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+            if (e != cudaSuccess || !ptr)
+                return fail(LUCID_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
+            g_noalloc_addr[device_] = (unsigned char*)ptr;
+        }
+        base = g_noalloc_addr[device_];
+    }
+    PathView v{};
+    size_t off = 0;
+    auto take = [&](size_t bytes) { unsigned char* q = base + off; off += bytes; return (void*)q; };
+    v.rng = (ulonglong2*)take(kNaRng);
+    v.ray_o = (float4*)take(kNaF4); v.ray_d = (float4*)take(kNaF4); v.thr = (float4*)take(kNaF4);
+    v.rad = (float4*)take(kNaF4); v.hit = (float4*)take(kNaF4); v.sh_o = (float4*)take(kNaF4);
+    v.sh_d = (float4*)take(kNaF4); v.sh_c = (float4*)take(kNaF4);
+    v.lhit = (float2*)take(kNaF2);
+    int* q0 = (int*)take(kNaQ);
+    int* q1 = (int*)take(kNaQ);
+    v.qs = (int*)take(kNaQ);
+    v.counters = (int*)take(kNaCnt);
+    v.errors = (int*)take(kNaErr);
+    float4* film = (float4*)take(kNaFilm);
+    v.q0 = q0; v.q1 = q1;
+    v.rec_prim = nullptr; v.rec_cnt = nullptr; v.rec_hash = nullptr;
+
+    cudaStream_t st = S(stream_);
+    // the array keeps the previous call's contents: clear what starts at zero
+    CK(cudaMemsetAsync(film, 0, sizeof(float4) * np, st));
+    CK(cudaMemsetAsync(v.errors, 0, sizeof(int) * 4, st));
+    FrameParams f{};
+    for (int k = 0; k < 3; ++k) { f.pos[k] = cam_.pos[k]; f.fwd[k] = cam_.forward[k]; f.right[k] = cam_.right[k]; f.up[k] = cam_.up[k]; }
+    f.aspect = (float)p.full_w / (float)p.full_h;
+    f.scale = std::tan(cam_.fov * 0.5f);
+    f.tile_x = p.tile_x; f.tile_y = p.tile_y; f.tile_w = p.tile_w; f.tile_h = p.tile_h;
+    f.full_w = p.full_w; f.full_h = p.full_h;
+    f.samples = p.samples; f.sample_offset = p.sample_offset; f.max_depth = p.max_depth; f.algo = algo_;
+    f.npix = (int)np;
+    f.records = 0;
+    int occ_t = 1, occ_s = 1, occ_h = 1, occ_t0 = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t0, k_trace_primary, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t, k_trace, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, k_shade, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, k_shadow, 128, 0);
+    const int g_trace0 = num_sms_ * std::max(1, occ_t0), g_trace = num_sms_ * std::max(1, occ_t);
+    const int g_shade = num_sms_ * std::max(1, occ_s), g_shadow = num_sms_ * std::max(1, occ_h);
+    const int spw = (int)std::max<long long>(1, std::min<long long>(p.samples, kNoAllocPaths / np));
+    int status = LUCID_OK;
+    for (int s0 = 0; s0 < p.samples; s0 += spw) {
+        if (is_cancelled()) { status = LUCID_ERR_CANCELLED; break; }
+        int this_spw = std::min(spw, p.samples - s0);
+        f.s0 = s0;
+        f.n_wave = (int)(this_spw * np);
+        CK(cudaMemsetAsync(v.counters, 0, sizeof(int) * kCountersPerDepth * (p.max_depth + 1), st));
+        k_raygen<<<(f.n_wave + 255) / 256, 256, 0, st>>>(f, v);
+        for (int depth = 0; depth < p.max_depth; ++depth) {
+            int* cnt = v.counters + kCountersPerDepth * depth;
+            int* cnt_next = v.counters + kCountersPerDepth * (depth + 1);
+            PathView pv = v;
+            int* qin = (depth & 1) ? q1 : q0;
+            int* qout = (depth & 1) ? q0 : q1;
+            pv.q0 = qin;
+            if (depth == 0) k_trace_primary<<<g_trace0, 128, 0, st>>>(ds_->view, pv, cnt, 0);
+            else k_trace<<<g_trace, 128, 0, st>>>(ds_->view, pv, cnt, 0, 0);
+            k_shade<<<g_shade, 128, 0, st>>>(ds_->view, f, pv, cnt, cnt_next, depth == 0, qin, qout);
+            k_shadow<<<g_shadow, 128, 0, st>>>(ds_->view, pv, cnt, 0);
+        }
+        k_film<<<(f.npix + 255) / 256, 256, 0, st>>>(f.npix, this_spw, v.rad, film);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(st));
+    }
+    k_output<<<(f.npix + 255) / 256, 256, 0, st>>>(p.tile_w, p.tile_h, film, (float4*)d_out);
+    int herr[4] = {0, 0, 0, 0};
+    CK(cudaMemcpyAsync(herr, v.errors, sizeof(herr), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
     if (herr[0] != 0) return fail(LUCID_ERR_OVERFLOW, "BVH traversal stack overflow");
     if (status == LUCID_ERR_CANCELLED) return fail(LUCID_ERR_CANCELLED, "render cancelled");
     return LUCID_OK;

@@ -24,6 +24,7 @@ public:
                    float fov_deg);
     int set_algorithm(const char* name);
     int render(const LucidRenderParams& p, float* out_host, LucidSampleRecord* recs, float* out_device);
+    int render_noalloc(const LucidRenderParams& p, float* d_out);
     int render_debug(int tx, int ty, int tw, int th, int fw, int fh, const char* mode, float* out_host);
     int scene_stats(int out8[8]) const;
     int stats(LucidRenderStats* out) const;

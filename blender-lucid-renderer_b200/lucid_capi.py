@@ -71,6 +71,7 @@ SIGNATURES = {
     "lucid_cuda_inspect_scene": (_I, [ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(_I), _P, _P, _P, _I]),
     "lucid_cuda_render": (_I, [_P, ctypes.POINTER(RenderParams), _P, _P]),
     "lucid_cuda_render_device": (_I, [_P, ctypes.POINTER(RenderParams), _P]),
+    "lucid_cuda_render_noalloc": (_I, [_P, ctypes.POINTER(RenderParams), _P]),
     "lucid_cuda_render_debug": (_I, [_P, _I, _I, _I, _I, _I, _I, ctypes.c_char_p, _P]),
     "lucid_cuda_get_stats": (_I, [_P, ctypes.POINTER(RenderStats)]),
     "lucid_cuda_set_wave_capacity": (_I, [_P, ctypes.c_longlong]),
@@ -189,6 +190,14 @@ class Context:
         p = RenderParams(0, 0, tile_w, tile_h, tile_w, tile_h, samples, sample_offset, max_depth,
                          LUCID_RENDER_PROFILE if profile else 0)
         return self._check(self.lib.lucid_cuda_render_device(self.h, ctypes.byref(p), ctypes.c_void_p(d_out_ptr)))
+
+    def render_noalloc(self, d_out_ptr: int, tile_w, tile_h, samples=1, sample_offset=0, max_depth=8,
+                       check=True):
+        """Render into caller-owned device memory without allocating (see
+        lucid_cuda_render_noalloc in include/lucid_cuda.h for the limits)."""
+        p = RenderParams(0, 0, tile_w, tile_h, tile_w, tile_h, samples, sample_offset, max_depth, 0)
+        rc = self.lib.lucid_cuda_render_noalloc(self.h, ctypes.byref(p), ctypes.c_void_p(d_out_ptr))
+        return self._check(rc) if check else rc
 
     def render_debug(self, mode: str, tile_w, tile_h, full_w=None, full_h=None, tile_x=0, tile_y=0):
         full_w = tile_w if full_w is None else full_w

@@ -129,6 +129,23 @@ int lucid_cuda_render(LucidCudaCtx* ctx, const LucidRenderParams* params, float*
 /* Same render with the image left in device memory (d_out_rgba: a device
  * pointer of tile_w*tile_h*4 floats); no host copies. */
 int lucid_cuda_render_device(LucidCudaCtx* ctx, const LucidRenderParams* params, float* d_out_rgba);
+/* Render without allocating any device memory.  No counterpart in the
+ * reference.  For callers that cannot call cudaMalloc/cudaFree while they
+ * render: hosts whose device memory belongs to another allocator, and
+ * latency-critical threads (a viewport draw callback) that must not make
+ * calls which can synchronise the whole device.  Same result as
+ * lucid_cuda_render_device (d_out_rgba: device pointer, tile_w*tile_h*4
+ * floats), but all working memory sits in one fixed static device array of
+ * about 12 MB that every GPU loading this library holds until exit.
+ * Limits: tile_w*tile_h <= 65536 pixels, 1 <= max_depth <= 64, no sample
+ * records; larger requests return LUCID_ERR_INVALID.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) with
+ * that device current; make that first call before any stream capture.
+ * Every call on a device shares the array: calls that overlap on the GPU
+ * (from several threads or contexts) race and must be serialised by the
+ * caller.  The scene must already be loaded (lucid_cuda_load_scene_json
+ * allocates). */
+int lucid_cuda_render_noalloc(LucidCudaCtx* ctx, const LucidRenderParams* params, float* d_out_rgba);
 /* Replaces PyRenderer::render_debug / render_debug_gpu
  * (pybind_renderer.hpp:371-525): mode "normal", "albedo" or "emission" at
  * the primary hit, no jitter, Y-flipped RGBA. */
