@@ -136,6 +136,31 @@ int lucid_cuda_set_wave_capacity(LucidCudaCtx* ctx, long long paths) {
     return guarded(ctx, [&](lucid::Engine& e) { return e.set_wave_capacity(paths); });
 }
 
+int lucid_cuda_async_start(LucidCudaCtx* ctx, int width, int height, int max_depth) {
+    return guarded(ctx, [&](lucid::Engine& e) { return e.async_start(width, height, max_depth); });
+}
+
+int lucid_cuda_async_poll(LucidCudaCtx* ctx, int* samples, float* out_rgba, size_t cap_floats) {
+    if (!samples) return LUCID_ERR_INVALID;
+    return guarded(ctx, [&](lucid::Engine& e) { return e.async_poll(samples, out_rgba, cap_floats); });
+}
+
+int lucid_cuda_async_revision(LucidCudaCtx* ctx) {
+    return guarded(ctx, [&](lucid::Engine& e) { return e.async_revision(); });
+}
+
+int lucid_cuda_async_reset(LucidCudaCtx* ctx, int width, int height, int max_depth) {
+    return guarded(ctx, [&](lucid::Engine& e) { return e.async_reset(width, height, max_depth); });
+}
+
+int lucid_cuda_async_stop(LucidCudaCtx* ctx) {
+    return guarded(ctx, [&](lucid::Engine& e) { return e.async_stop(); });
+}
+
+int lucid_cuda_async_running(LucidCudaCtx* ctx) {
+    return guarded(ctx, [&](lucid::Engine& e) { return e.async_running() ? 1 : 0; });
+}
+
 int lucid_cuda_cancel(LucidCudaCtx* ctx) {
     if (!ctx || !ctx->engine) return LUCID_ERR_INVALID;
     ctx->engine->cancel();

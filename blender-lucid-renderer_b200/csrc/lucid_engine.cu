@@ -16,8 +16,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <chrono>
 #include <cub/cub.cuh>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -891,7 +893,10 @@ Engine::Engine(int device) : device_(device) {
 }
 
 Engine::~Engine() {
+    async_stop();
     cudaSetDevice(device_);
+    if (async_acc_) cudaFree(async_acc_);
+    if (async_pinned_) cudaFreeHost(async_pinned_);
     if (ds_) { ds_->release(); delete ds_; }
     if (pool_) { pool_->release(); delete pool_; }
     if (stream_) cudaStreamDestroy(S(stream_));
@@ -906,12 +911,14 @@ int Engine::device_info(char* buf, size_t cap) const {
 
 int Engine::set_camera(float px, float py, float pz, float dx, float dy, float dz, float ux, float uy, float uz,
                        float fov_deg) {
+    std::lock_guard<std::mutex> gl(gpu_mu_);
     make_camera(cam_, px, py, pz, dx, dy, dz, ux, uy, uz, fov_deg);
     camera_set_ = true;
     return LUCID_OK;
 }
 
 int Engine::set_algorithm(const char* name) {
+    std::lock_guard<std::mutex> gl(gpu_mu_);
     std::string a = name ? name : "";
     if (a == "simple") algo_ = ALGO_SIMPLE;
     else if (a == "mis") algo_ = ALGO_MIS;
@@ -941,6 +948,7 @@ int Engine::stats(LucidRenderStats* out) const { *out = stats_; return LUCID_OK;
 void Engine::free_scene() { ds_->release(); scene_loaded_ = false; }
 
 int Engine::load_scene_json(const char* json, size_t len) {
+    std::lock_guard<std::mutex> gl(gpu_mu_);
     CK(cudaSetDevice(device_));
     if (!stream_) {
         cudaStream_t s;
@@ -1205,7 +1213,21 @@ const double kKindBytes[K_NUM] = {kBytesRaygen, kBytesTrace, kBytesTrace, kBytes
 }  // namespace
 
 int Engine::render(const LucidRenderParams& p, float* out_host, LucidSampleRecord* recs, float* out_device) {
-    reset_cancel();
+    std::lock_guard<std::mutex> lk(gpu_mu_);
+    return render_impl(p, out_host, recs, out_device, nullptr, false);
+}
+
+// Adds one render's film into the async accumulator (float4 sum per pixel).
+__global__ void k_accumulate(int npix, const float4* film, float4* acc) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npix) return;
+    float4 a = acc[p], f = film[p];
+    acc[p] = make_float4(a.x + f.x, a.y + f.y, a.z + f.z, 0.0f);
+}
+
+int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSampleRecord* recs, float* out_device,
+                        void* accumulate, bool from_async) {
+    if (!from_async) reset_cancel();
     if (p.tile_w <= 0 || p.tile_h <= 0 || p.full_w <= 0 || p.full_h <= 0)
         return fail(LUCID_ERR_INVALID, "tile and image sizes must be positive");
     size_t np = (size_t)p.tile_w * p.tile_h;
@@ -1278,7 +1300,7 @@ int Engine::render(const LucidRenderParams& p, float* out_host, LucidSampleRecor
     int status = LUCID_OK;
     int waves = 0;
     for (int s0 = 0; s0 < p.samples; s0 += spw) {
-        if (is_cancelled()) { status = LUCID_ERR_CANCELLED; break; }
+        if (!from_async && is_cancelled()) { status = LUCID_ERR_CANCELLED; break; }
         int this_spw = std::min(spw, p.samples - s0);
         f.s0 = s0;
         f.n_wave = (int)((long long)this_spw * (long long)np);
@@ -1332,7 +1354,11 @@ int Engine::render(const LucidRenderParams& p, float* out_host, LucidSampleRecor
         ++waves;
     }
     int np_i = (int)np;
-    k_output<<<(np_i + 255) / 256, 256, 0, st>>>(p.tile_w, p.tile_h, P.film.p, out_device ? (float4*)out_device : P.out.p);
+    if (accumulate)
+        k_accumulate<<<(np_i + 255) / 256, 256, 0, st>>>(np_i, P.film.p, (float4*)accumulate);
+    else
+        k_output<<<(np_i + 255) / 256, 256, 0, st>>>(p.tile_w, p.tile_h, P.film.p,
+                                                     out_device ? (float4*)out_device : P.out.p);
     cudaEventRecord(t1, st);
     int herr[4] = {0, 0, 0, 0};
     CK(cudaMemcpyAsync(herr, P.errors.p, sizeof(herr), cudaMemcpyDeviceToHost, st));
@@ -1372,6 +1398,123 @@ int Engine::render(const LucidRenderParams& p, float* out_host, LucidSampleRecor
     return LUCID_OK;
 }
 
+// ---------------------------------------------------------------- async accumulator
+// The viewport's progressive mode (PyRenderer::render_start_async ..
+// render_stop_async, pybind_renderer.hpp:689-856; the Dawn worker it drives,
+// gpu/path_tracer.cpp:838-1090): a worker thread adds one 1-spp render per
+// iteration (sample offset n, so iteration n seeds (x, y, n)) into a device
+// accumulator and publishes an averaged snapshot after 1, 2, 4, 8 and then
+// every 16 samples.  reset() wipes the accumulator without stopping.
+int Engine::async_start(int w, int h, int max_depth) {
+    async_stop();
+    if (w <= 0 || h <= 0) return fail(LUCID_ERR_INVALID, "async: size must be positive");
+    if (!scene_loaded_ || !camera_set_) return fail(LUCID_ERR_NO_SCENE, "scene or camera not set");
+    {
+        std::lock_guard<std::mutex> gl(gpu_mu_);
+        CK(cudaSetDevice(device_));
+        size_t n = (size_t)w * h;
+        if (async_acc_n_ < n) {
+            if (async_acc_) cudaFree(async_acc_);
+            if (async_pinned_) cudaFreeHost(async_pinned_);
+            async_acc_ = nullptr;
+            async_pinned_ = nullptr;
+            async_acc_n_ = 0;
+            CK(cudaMalloc(&async_acc_, n * sizeof(float4)));
+            CK(cudaMallocHost((void**)&async_pinned_, n * sizeof(float4)));
+            async_acc_n_ = n;
+        }
+        CK(cudaMemset(async_acc_, 0, n * sizeof(float4)));
+        async_w_ = w; async_h_ = h; async_depth_ = std::max(1, max_depth);
+    }
+    {
+        std::lock_guard<std::mutex> sl(snap_mu_);
+        snap_.clear();
+        snap_samples_ = 0;
+    }
+    async_reset_ = false;
+    async_run_ = true;
+    async_thread_ = std::thread([this] { async_worker(); });
+    return LUCID_OK;
+}
+
+int Engine::async_reset(int w, int h, int max_depth) {
+    if (!async_run_) return LUCID_OK;
+    if ((size_t)w * h > async_acc_n_ || w <= 0 || h <= 0)
+        return fail(LUCID_ERR_INVALID, "async reset: a larger resolution needs stop + start");
+    {
+        std::lock_guard<std::mutex> gl(gpu_mu_);
+        async_w_ = w; async_h_ = h; async_depth_ = std::max(1, max_depth);
+    }
+    async_reset_ = true;
+    return LUCID_OK;
+}
+
+int Engine::async_stop() {
+    async_run_ = false;
+    if (async_thread_.joinable()) async_thread_.join();
+    return LUCID_OK;
+}
+
+int Engine::async_poll(int* samples, float* out, size_t cap_floats) {
+    std::lock_guard<std::mutex> sl(snap_mu_);
+    *samples = snap_samples_;
+    if (snap_samples_ == 0) return LUCID_OK;
+    if (!out || cap_floats < snap_.size()) return fail(LUCID_ERR_INVALID, "async poll: output buffer too small");
+    std::copy(snap_.begin(), snap_.end(), out);
+    return LUCID_OK;
+}
+
+void Engine::async_worker() {
+    cudaSetDevice(device_);
+    long long n = 0;
+    int w = 0, h = 0, depth = 8;
+    while (async_run_) {
+        bool wipe = async_reset_.exchange(false);
+        {
+            std::lock_guard<std::mutex> gl(gpu_mu_);
+            if (wipe || w != async_w_ || h != async_h_) {
+                w = async_w_; h = async_h_;
+                cudaMemsetAsync(async_acc_, 0, (size_t)w * h * sizeof(float4), S(stream_));
+                n = 0;
+            }
+            depth = async_depth_;
+            LucidRenderParams p{0, 0, w, h, w, h, 1, (int)n, depth, 0};
+            int rc = render_impl(p, nullptr, nullptr, nullptr, async_acc_, true);
+            if (rc != LUCID_OK) {
+                async_err_ = err_;
+            } else {
+                ++n;
+                if (n <= 8 ? ((n & (n - 1)) == 0) : (n % 16 == 0)) {
+                    size_t np = (size_t)w * h;
+                    cudaMemcpyAsync(async_pinned_, async_acc_, np * sizeof(float4), cudaMemcpyDeviceToHost, S(stream_));
+                    cudaStreamSynchronize(S(stream_));
+                    // average, camera sensitivity (EV 0 -> 1), clamp >= 0, alpha 1, Y flip
+                    std::vector<float> img(np * 4);
+                    const float inv = (float)n;
+                    for (int y = 0; y < h; ++y)
+                        for (int x = 0; x < w; ++x) {
+                            const float* a = async_pinned_ + 4 * ((size_t)y * w + x);
+                            float* o = img.data() + 4 * ((size_t)(h - 1 - y) * w + x);
+                            for (int c = 0; c < 3; ++c) {
+                                float v = (a[c] / inv) * 1.0f;
+                                o[c] = (v < 0.0f) ? 0.0f : v;
+                            }
+                            o[3] = 1.0f;
+                        }
+                    std::lock_guard<std::mutex> sl(snap_mu_);
+                    snap_.swap(img);
+                    snap_samples_ = (int)n;
+                    async_revision_.fetch_add(1);
+                }
+            }
+        }
+        if (async_err_.size()) {
+            std::this_thread::sleep_for(std::chrono::milliseconds(2));   // the reference backs off 2 ms
+            async_err_.clear();
+        }
+    }
+}
+
 // ---------------------------------------------------------------- no-allocation render
 // Some callers cannot allocate device memory when they render: a host whose
 // device memory is owned by another allocator (a framework's caching pool
@@ -1408,6 +1551,7 @@ unsigned char* g_noalloc_addr[64] = {};
 }  // namespace
 
 int Engine::render_noalloc(const LucidRenderParams& p, float* d_out) {
+    std::lock_guard<std::mutex> gl(gpu_mu_);
     reset_cancel();
     if (!d_out) return fail(LUCID_ERR_INVALID, "output pointer is null");
     if (p.tile_w <= 0 || p.tile_h <= 0 || p.full_w <= 0 || p.full_h <= 0)
@@ -1506,6 +1650,7 @@ int Engine::render_noalloc(const LucidRenderParams& p, float* d_out) {
 }
 
 int Engine::render_debug(int tx, int ty, int tw, int th, int fw, int fh, const char* mode, float* out_host) {
+    std::lock_guard<std::mutex> gl(gpu_mu_);
     reset_cancel();
     if (tw <= 0 || th <= 0 || fw <= 0 || fh <= 0) return fail(LUCID_ERR_INVALID, "tile and image sizes must be positive");
     size_t np = (size_t)tw * th;

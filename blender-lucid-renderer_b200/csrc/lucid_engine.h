@@ -2,7 +2,9 @@
 #pragma once
 
 #include <atomic>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/lucid_cuda.h"
@@ -24,6 +26,13 @@ public:
                    float fov_deg);
     int set_algorithm(const char* name);
     int render(const LucidRenderParams& p, float* out_host, LucidSampleRecord* recs, float* out_device);
+    // Progressive accumulator (PyRenderer render_*_async, pybind_renderer.hpp:689-856).
+    int async_start(int w, int h, int max_depth);
+    int async_poll(int* samples, float* out, size_t cap_floats);
+    int async_reset(int w, int h, int max_depth);
+    int async_stop();
+    int async_revision() const { return async_revision_.load(); }
+    bool async_running() const { return async_run_.load(); }
     int render_noalloc(const LucidRenderParams& p, float* d_out);
     int render_debug(int tx, int ty, int tw, int th, int fw, int fh, const char* mode, float* out_host);
     int scene_stats(int out8[8]) const;
@@ -39,6 +48,9 @@ public:
     int fail(int code, const std::string& msg) { err_ = msg; return code; }
 
 private:
+    int render_impl(const LucidRenderParams& p, float* out_host, LucidSampleRecord* recs, float* out_device,
+                    void* accumulate, bool from_async);
+    void async_worker();
     int ensure_pool(long long paths, bool records);
     int build_bvh();
     void free_scene();
@@ -57,6 +69,20 @@ private:
     std::string err_;
     LucidRenderStats stats_{};
     int bvh_nodes_ = 0, bvh_leaves_ = 0, bvh_depth_ = 0, num_big_ = 0;
+    // one GPU call at a time per context (the reference's gpu_mutex_)
+    std::mutex gpu_mu_;
+    // async accumulator
+    std::thread async_thread_;
+    std::atomic<bool> async_run_{false}, async_reset_{false};
+    std::atomic<int> async_revision_{0};
+    int async_w_ = 0, async_h_ = 0, async_depth_ = 8;
+    void* async_acc_ = nullptr;       // device float4[w*h] sum of samples
+    size_t async_acc_n_ = 0;
+    float* async_pinned_ = nullptr;   // pinned host copy of the accumulator
+    std::mutex snap_mu_;
+    std::vector<float> snap_;
+    int snap_samples_ = 0;
+    std::string async_err_;
 };
 
 }  // namespace lucid

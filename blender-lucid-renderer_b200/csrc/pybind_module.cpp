@@ -109,6 +109,29 @@ public:
         return path + " \xe2\x86\x92 Camera";
     }
 
+    // async accumulator (pybind_renderer.hpp:689-856)
+    void start_async(int w, int h, int depth) {
+        int rc = lucid_cuda_async_start(ctx_, w, h, depth);
+        if (rc == LUCID_OK) { async_w_ = w; async_h_ = h; }
+        else if (rc != LUCID_ERR_NO_SCENE)
+            std::fprintf(stderr, "[lucidrenderer] start_async failed: %s\n", lucid_cuda_last_error(ctx_));
+    }
+    std::pair<int, std::vector<float>> poll_async() {
+        int n = 0;
+        std::vector<float> px((size_t)async_w_ * async_h_ * 4);
+        if (lucid_cuda_async_running(ctx_) != 1 && lucid_cuda_async_revision(ctx_) <= 0) return {0, {}};
+        if (lucid_cuda_async_poll(ctx_, &n, px.data(), px.size()) != LUCID_OK || n == 0) return {0, {}};
+        return {n, std::move(px)};
+    }
+    void reset_async(int w, int h, int depth) {
+        if (lucid_cuda_async_reset(ctx_, w, h, depth) != LUCID_OK)
+            std::fprintf(stderr, "[lucidrenderer] reset_async failed: %s\n", lucid_cuda_last_error(ctx_));
+        else { async_w_ = w; async_h_ = h; }
+    }
+    void stop_async() { lucid_cuda_async_stop(ctx_); }
+    bool async_running() { return lucid_cuda_async_running(ctx_) == 1; }
+    int async_revision() { int r = lucid_cuda_async_revision(ctx_); return r < 0 ? 0 : r; }
+
     LucidCudaCtx* ctx() { return ctx_; }
 
 private:
@@ -117,6 +140,7 @@ private:
     int mesh_count_ = 0;
     std::string algorithm_ = "nee";
     std::vector<std::string> names_;
+    int async_w_ = 0, async_h_ = 0;
 };
 
 std::string adapter_info() {
@@ -170,6 +194,25 @@ PYBIND11_MODULE(lucidrenderer, m) {
         .def("render_debug_gpu", &Renderer::render_debug, py::call_guard<py::gil_scoped_release>(), py::arg("tile_x"),
              py::arg("tile_y"), py::arg("tile_w"), py::arg("tile_h"), py::arg("full_w"), py::arg("full_h"),
              py::arg("mode"))
+        .def("render_start_async", &Renderer::start_async, py::call_guard<py::gil_scoped_release>(),
+             py::arg("width"), py::arg("height"), py::arg("max_depth") = 8)
+        .def("render_poll_async",
+             [](Renderer& self) {
+                 std::pair<int, std::vector<float>> r;
+                 {
+                     py::gil_scoped_release release;
+                     r = self.poll_async();
+                 }
+                 py::array_t<float> arr(static_cast<py::ssize_t>(r.second.size()));
+                 if (!r.second.empty()) std::memcpy(arr.mutable_data(), r.second.data(), r.second.size() * sizeof(float));
+                 return py::make_tuple(r.first, arr);
+             },
+             "(samples, RGBA numpy): averaged over samples, Y-flipped; samples == 0 means no snapshot yet")
+        .def("render_snapshot_revision_async", &Renderer::async_revision, py::call_guard<py::gil_scoped_release>())
+        .def("render_stop_async", &Renderer::stop_async, py::call_guard<py::gil_scoped_release>())
+        .def("render_reset_async", &Renderer::reset_async, py::call_guard<py::gil_scoped_release>(),
+             py::arg("width"), py::arg("height"), py::arg("max_depth") = 8)
+        .def("is_render_async_running", &Renderer::async_running, py::call_guard<py::gil_scoped_release>())
         .def("is_scene_loaded", &Renderer::is_scene_loaded)
         .def("is_camera_set", &Renderer::is_camera_set)
         .def("get_algorithm", &Renderer::get_algorithm)

@@ -75,6 +75,12 @@ SIGNATURES = {
     "lucid_cuda_render_debug": (_I, [_P, _I, _I, _I, _I, _I, _I, ctypes.c_char_p, _P]),
     "lucid_cuda_get_stats": (_I, [_P, ctypes.POINTER(RenderStats)]),
     "lucid_cuda_set_wave_capacity": (_I, [_P, ctypes.c_longlong]),
+    "lucid_cuda_async_start": (_I, [_P, _I, _I, _I]),
+    "lucid_cuda_async_poll": (_I, [_P, ctypes.POINTER(_I), _P, ctypes.c_size_t]),
+    "lucid_cuda_async_revision": (_I, [_P]),
+    "lucid_cuda_async_reset": (_I, [_P, _I, _I, _I]),
+    "lucid_cuda_async_stop": (_I, [_P]),
+    "lucid_cuda_async_running": (_I, [_P]),
     "lucid_cuda_cancel": (_I, [_P]),
     "lucid_cuda_is_cancelled": (_I, [_P]),
     "lucid_cuda_reset_cancel": (_I, [_P]),
@@ -217,6 +223,30 @@ class Context:
                                        "algo_bytes": ks.algo_bytes, "units": ks.units}
         return {"total_ms": s.total_ms, "paths": s.paths, "segments": s.segments, "shadow_rays": s.shadow_rays,
                 "waves": s.waves, "kernels": kinds}
+
+    # progressive accumulator (viewport)
+    def async_start(self, w, h, max_depth=8):
+        self._check(self.lib.lucid_cuda_async_start(self.h, w, h, max_depth))
+        self._async_shape = (h, w)
+
+    def async_poll(self):
+        h, w = getattr(self, "_async_shape", (0, 0))
+        n = ctypes.c_int(0)
+        img = np.zeros((h, w, 4), np.float32)
+        self._check(self.lib.lucid_cuda_async_poll(self.h, ctypes.byref(n), img.ctypes.data, img.size))
+        return n.value, (img if n.value > 0 else None)
+
+    def async_revision(self) -> int:
+        return self.lib.lucid_cuda_async_revision(self.h)
+
+    def async_reset(self, w, h, max_depth=8):
+        self._check(self.lib.lucid_cuda_async_reset(self.h, w, h, max_depth))
+
+    def async_stop(self):
+        self._check(self.lib.lucid_cuda_async_stop(self.h))
+
+    def async_running(self) -> bool:
+        return self.lib.lucid_cuda_async_running(self.h) == 1
 
     def cancel(self):
         self.lib.lucid_cuda_cancel(self.h)

@@ -157,6 +157,27 @@ int lucid_cuda_get_stats(LucidCudaCtx* ctx, LucidRenderStats* out);
  * samples in waves of at most this many paths. */
 int lucid_cuda_set_wave_capacity(LucidCudaCtx* ctx, long long paths);
 
+/* ---- progressive accumulator (viewport) -------------------------------- */
+/* Replaces PyRenderer::render_start_async / render_poll_async /
+ * render_snapshot_revision_async / render_reset_async / render_stop_async /
+ * is_render_async_running (pybind_renderer.hpp:689-856).  A worker thread
+ * adds one 1-spp render per iteration (iteration n uses sample offset n)
+ * into a device accumulator and publishes an averaged snapshot after 1, 2,
+ * 4, 8 and then every 16 samples. */
+int lucid_cuda_async_start(LucidCudaCtx* ctx, int width, int height, int max_depth);
+/* Latest snapshot: *samples = samples averaged (0 = none yet); out_rgba gets
+ * width*height*4 floats (averaged, exposure applied, clamped >= 0, alpha 1,
+ * Y-flipped) when *samples > 0. */
+int lucid_cuda_async_poll(LucidCudaCtx* ctx, int* samples, float* out_rgba, size_t cap_floats);
+/* Monotonic snapshot counter (>= 0). */
+int lucid_cuda_async_revision(LucidCudaCtx* ctx);
+/* Non-blocking wipe of the accumulator; picks up the current camera.  A
+ * larger resolution needs stop + start. */
+int lucid_cuda_async_reset(LucidCudaCtx* ctx, int width, int height, int max_depth);
+int lucid_cuda_async_stop(LucidCudaCtx* ctx);
+/* 1 while the worker runs, else 0. */
+int lucid_cuda_async_running(LucidCudaCtx* ctx);
+
 /* ---- cancellation ---------------------------------------------------- */
 /* Replaces PyRenderer::cancel / is_cancelled / reset_cancel
  * (pybind_renderer.hpp:86-102).  Thread-safe. */
