@@ -295,7 +295,7 @@ def main():
                     "d2h_bytes_per_step": W * H * 16},
             "roofline": {"bound": "hbm", "kernel": top[0], "achieved": achieved, "peak": peak,
                          "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic},
-            "kernels": {k: {"launches": v["launches"], "ms": round(v["total_ms"], 3),
+            "kernels": {k: {"launches": v["launches"], "ms": round(v["total_ms"], 3), "units": v["units"],
                             "share": round(v["total_ms"] / sum(x["total_ms"] for x in kern.values()), 4)}
                         for k, v in kern.items()},
             "mrays_per_s": mrays, "segments_per_step": segs, "shadow_rays_per_step": shadows,

@@ -161,6 +161,42 @@ int lucid_cuda_async_running(LucidCudaCtx* ctx) {
     return guarded(ctx, [&](lucid::Engine& e) { return e.async_running() ? 1 : 0; });
 }
 
+int lucid_cuda_diag_enable(LucidCudaCtx* ctx, const LucidDiagConfig* config) {
+    return guarded(ctx, [&](lucid::Engine& e) { return e.diag_enable(config); });
+}
+
+int lucid_cuda_diag_disable(LucidCudaCtx* ctx) {
+    return guarded(ctx, [&](lucid::Engine& e) { return e.diag_disable(); });
+}
+
+int lucid_cuda_diag_enabled(LucidCudaCtx* ctx) {
+    return guarded(ctx, [&](lucid::Engine& e) { return e.diag_enabled() ? 1 : 0; });
+}
+
+int lucid_cuda_diag_clear(LucidCudaCtx* ctx) {
+    return guarded(ctx, [&](lucid::Engine& e) { return e.diag_clear(); });
+}
+
+int lucid_cuda_diag_stats(LucidCudaCtx* ctx, LucidDiagStats* out) {
+    if (!out) return LUCID_ERR_INVALID;
+    return guarded(ctx, [&](lucid::Engine& e) { return e.diag_stats(out); });
+}
+
+int lucid_cuda_diag_pixel(LucidCudaCtx* ctx, int x, int y, int sort_by_mean, LucidDiagPixel* info,
+                          LucidDiagGroup* groups, int cap) {
+    if (!info) return LUCID_ERR_INVALID;
+    return guarded(ctx, [&](lucid::Engine& e) { return e.diag_pixel(x, y, sort_by_mean != 0, info, groups, cap); });
+}
+
+int lucid_cuda_diag_variance_map(LucidCudaCtx* ctx, float* out, size_t cap) {
+    if (!out) return LUCID_ERR_INVALID;
+    return guarded(ctx, [&](lucid::Engine& e) { return e.diag_variance_map(out, cap); });
+}
+
+int lucid_cuda_diag_top_groups(LucidCudaCtx* ctx, int n, int by_mean, LucidDiagGroup* groups, int32_t* xy, int cap) {
+    return guarded(ctx, [&](lucid::Engine& e) { return e.diag_top(n, by_mean != 0, groups, xy, cap); });
+}
+
 int lucid_cuda_cancel(LucidCudaCtx* ctx) {
     if (!ctx || !ctx->engine) return LUCID_ERR_INVALID;
     ctx->engine->cancel();

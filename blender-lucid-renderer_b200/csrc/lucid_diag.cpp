@@ -1,0 +1,235 @@
+// lucid_diag.cpp — host DiagnosticFilm: ordered replay of the GPU's completed
+// path records (see lucid_diag.h).  Compiled with -ffp-contract=off.
+#include "lucid_diag.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace lucid {
+
+void DiagStats::add(const float* v) {   // path_stats.hpp:63-100
+    ++count;
+    if (count == 1) {
+        for (int c = 0; c < 3; ++c) { mean[c] = v[c]; m2[c] = 0.0f; var[c] = 0.0f; }
+        return;
+    }
+    float d[3], d2[3];
+    for (int c = 0; c < 3; ++c) d[c] = v[c] - mean[c];
+    for (int c = 0; c < 3; ++c) mean[c] += d[c] / (float)count;
+    for (int c = 0; c < 3; ++c) d2[c] = v[c] - mean[c];
+    for (int c = 0; c < 3; ++c) m2[c] += d[c] * d2[c];
+    float nm1 = (float)(count - 1);
+    for (int c = 0; c < 3; ++c) var[c] = m2[c] / nm1;
+}
+
+// PathTrace::hash (path_types.hpp:321-343): FNV-1a over the depth and every
+// vertex's (object id, material id 0 or -1, BSDF class, flags), with the
+// signed ids sign-extended to 64 bits.
+uint64_t DiagFilm::hash(const DiagRecord& r) {
+    uint64_t h = 14695981039346656037ULL;
+    h ^= (uint64_t)r.depth;
+    h *= 1099511628211ULL;
+    for (int i = 0; i < r.depth; ++i) {
+        const int16_t material = r.bsdf[i] == 4 ? -1 : 0;   // only the final light vertex is Emission
+        h ^= (uint64_t)(int64_t)r.object_id[i];
+        h *= 1099511628211ULL;
+        h ^= (uint64_t)(int64_t)material;
+        h *= 1099511628211ULL;
+        h ^= (uint64_t)r.bsdf[i];
+        h *= 1099511628211ULL;
+        h ^= (uint64_t)r.flags[i];
+        h *= 1099511628211ULL;
+    }
+    return h;
+}
+
+uint8_t DiagFilm::coarse_type(const DiagRecord& r) {   // path_types.hpp:354-372
+    uint8_t t = 0;
+    for (int i = 0; i < r.depth; ++i) {
+        if (r.flags[i] & 2) t |= 1;
+        if (r.flags[i] & 1) t |= 2;
+    }
+    if (r.depth > 2) t |= 4;
+    return t;
+}
+
+// PixelPathData::record_path (pixel_path_data.hpp:53-89).
+void DiagPixel::record(const DiagRecord& r, uint64_t h, uint8_t coarse_t) {
+    ++total;
+    total_stats.add(r.contrib);
+    coarse[coarse_t].add(r.contrib);
+    if (total >= 10) {   // is_outlier (:172-192)
+        const float th = 3.0f;
+        bool out = false;
+        for (int c = 0; c < 3; ++c) {
+            float sd = std::sqrt(total_stats.var[c] + 1e-10f);
+            float dv = std::fabs(r.contrib[c] - total_stats.mean[c]);
+            out = out || (dv > th * sd);
+        }
+        if (out) {
+            size_t i = num_outliers % kOutliers;
+            outlier_hash[i] = h;
+            for (int c = 0; c < 3; ++c) outlier_c[i][c] = r.contrib[c];
+            ++num_outliers;
+        }
+    }
+    for (size_t i = 0; i < num_groups; ++i)
+        if (groups[i].hash == h) { groups[i].stats.add(r.contrib); return; }
+    auto init_from = [&](DiagGroup& g) {   // PathGroup::init_from (path_stats.hpp:161-178)
+        g.hash = h;
+        g.depth = (uint8_t)std::min<int>(r.depth, kDiagMaxDepth);
+        g.coarse = coarse_t;
+        g.light_type = r.light_type;
+        g.strategy = r.strategy;
+        for (int k = 0; k < g.depth; ++k) {
+            g.object_id[k] = r.object_id[k]; g.bsdf[k] = r.bsdf[k]; g.flags[k] = r.flags[k];
+            for (int c = 0; c < 3; ++c) { g.pos[k][c] = r.pos[k][c]; g.nrm[k][c] = r.nrm[k][c]; }
+        }
+        g.stats = DiagStats();
+        g.stats.add(r.contrib);
+    };
+    if (num_groups < (size_t)kGroups) { init_from(groups[num_groups++]); return; }
+    // evict_and_add (:203-220)
+    size_t mi = 0;
+    float mv = groups[0].stats.total_variance();
+    for (size_t i = 1; i < num_groups; ++i) {
+        float var = groups[i].stats.total_variance();
+        float adj = var * std::log2((float)(groups[i].stats.count + 1));
+        float madj = mv * std::log2((float)(groups[mi].stats.count + 1));
+        if (adj < madj) { mi = i; mv = var; }
+    }
+    ++overflow;
+    init_from(groups[mi]);
+}
+
+void DiagFilm::init(int tile_w, int tile_h, int subsample) {
+    w_ = tile_w; h_ = tile_h; sf_ = std::max(1, subsample);
+    sw_ = w_ / sf_; sh_ = h_ / sf_;
+    px_.assign((size_t)sw_ * sh_, DiagPixel());
+    recorded_ = 0;
+    valid_ = true;
+}
+
+void DiagFilm::clear() {
+    for (auto& p : px_) p = DiagPixel();
+    recorded_ = 0;
+}
+
+void DiagFilm::replay(std::vector<DiagRecord>& recs, int tile_w) {
+    // the reference's single-threaded loop order: 8x8 micro-tiles row-major,
+    // pixels row-major inside one, samples, records along the path
+    const int nmx = (tile_w + 7) / 8;
+    auto key = [&](const DiagRecord& r) {
+        int x = (int)(r.pixel % (uint32_t)tile_w), y = (int)(r.pixel / (uint32_t)tile_w);
+        uint64_t order = (uint64_t)((y / 8) * nmx + x / 8) * 64u + (uint64_t)((y % 8) * 8 + (x % 8));
+        return (order << 40) | ((uint64_t)r.sample << 16) | (uint64_t)r.seq;
+    };
+    std::vector<std::pair<uint64_t, uint32_t>> idx(recs.size());
+    for (size_t i = 0; i < recs.size(); ++i) idx[i] = {key(recs[i]), (uint32_t)i};
+    std::sort(idx.begin(), idx.end());
+    for (const auto& e : idx) {
+        const DiagRecord& r = recs[e.second];
+        int x = (int)(r.pixel % (uint32_t)tile_w), y = (int)(r.pixel / (uint32_t)tile_w);
+        int sx = x / sf_, sy = y / sf_;
+        if (sx >= sw_ || sy >= sh_) continue;
+        px_[(size_t)sy * sw_ + sx].record(r, hash(r), coarse_type(r));
+        ++recorded_;
+    }
+}
+
+const DiagPixel* DiagFilm::at(int x, int y) const {
+    if (!valid_ || x < 0 || y < 0) return nullptr;
+    int sx = x / sf_, sy = y / sf_;
+    if (sx >= sw_ || sy >= sh_) return nullptr;
+    return &px_[(size_t)sy * sw_ + sx];
+}
+DiagPixel* DiagFilm::at_mut(int x, int y) { return const_cast<DiagPixel*>(at(x, y)); }
+
+void DiagFilm::stats(LucidDiagStats* out) const {
+    std::memset(out, 0, sizeof(*out));
+    for (const auto& p : px_)
+        if (p.total > 0) {
+            ++out->active_pixels;
+            out->total_samples += p.total;
+            out->total_groups += p.num_groups;
+            out->total_overflow += p.overflow;
+        }
+    out->paths_recorded = recorded_;
+}
+
+void DiagFilm::variance_map(float* out) const {
+    for (int y = 0; y < h_; ++y)
+        for (int x = 0; x < w_; ++x) {
+            const DiagPixel* p = at(x, y);
+            out[(size_t)y * w_ + x] = p ? p->total_stats.total_variance() : 0.0f;
+        }
+}
+
+void DiagFilm::export_group(const DiagGroup& g, LucidDiagGroup* o) {
+    std::memset(o, 0, sizeof(*o));
+    o->hash = g.hash; o->count = g.stats.count; o->depth = g.depth; o->coarse_type = g.coarse;
+    o->light_type = g.light_type; o->strategy = g.strategy;
+    for (int c = 0; c < 3; ++c) { o->mean_rgb[c] = g.stats.mean[c]; o->variance_rgb[c] = g.stats.var[c]; }
+    o->mean_luminance = g.stats.mean_luminance();
+    o->total_variance = g.stats.total_variance();
+    for (int k = 0; k < g.depth; ++k) {
+        o->object_ids[k] = g.object_id[k]; o->bsdf[k] = g.bsdf[k]; o->flags[k] = g.flags[k];
+        for (int c = 0; c < 3; ++c) { o->positions[k][c] = g.pos[k][c]; o->normals[k][c] = g.nrm[k][c]; }
+    }
+}
+
+// get_pixel_diagnostic (pybind_renderer.hpp:1008-1102).
+int DiagFilm::export_pixel(int x, int y, bool sort_by_mean, LucidDiagPixel* info, LucidDiagGroup* groups, int cap) {
+    std::memset(info, 0, sizeof(*info));
+    DiagPixel* p = at_mut(x, y);
+    if (!p) return 0;
+    if (sort_by_mean)
+        std::sort(p->groups, p->groups + p->num_groups, [](const DiagGroup& a, const DiagGroup& b) {
+            return a.stats.mean_luminance() > b.stats.mean_luminance();
+        });
+    else
+        std::sort(p->groups, p->groups + p->num_groups, [](const DiagGroup& a, const DiagGroup& b) {
+            return a.stats.total_variance() > b.stats.total_variance();
+        });
+    info->valid = 1;
+    info->sample_count = (uint32_t)p->total;
+    info->group_count = (uint32_t)p->num_groups;
+    info->outlier_count = (uint32_t)p->num_outliers;
+    info->overflow_count = (uint32_t)p->overflow;
+    info->variance = p->total_stats.total_variance();
+    for (int c = 0; c < 3; ++c) info->mean_rgb[c] = p->total_stats.mean[c];
+    int n = (int)std::min<size_t>(p->num_groups, (size_t)std::max(cap, 0));
+    for (int i = 0; i < n; ++i) export_group(p->groups[i], groups + i);
+    return n;
+}
+
+// top_groups_by_variance / top_groups_by_mean (diagnostic_film.hpp:160-222):
+// cells in row-major order, groups in cell order, std::partial_sort.
+int DiagFilm::export_top(int n, bool by_mean, LucidDiagGroup* groups, int32_t* xy, int cap) const {
+    struct Ref { int x, y; const DiagGroup* g; };
+    std::vector<Ref> all;
+    for (int sy = 0; sy < sh_; ++sy)
+        for (int sx = 0; sx < sw_; ++sx) {
+            const DiagPixel& px = px_[(size_t)sy * sw_ + sx];
+            for (size_t i = 0; i < px.num_groups; ++i)
+                if (px.groups[i].stats.count >= (by_mean ? 1u : 2u)) all.push_back({sx * sf_, sy * sf_, &px.groups[i]});
+        }
+    size_t limit = std::min((size_t)std::max(n, 0), all.size());
+    if (by_mean)
+        std::partial_sort(all.begin(), all.begin() + limit, all.end(), [](const Ref& a, const Ref& b) {
+            return a.g->stats.mean_luminance() > b.g->stats.mean_luminance();
+        });
+    else
+        std::partial_sort(all.begin(), all.begin() + limit, all.end(), [](const Ref& a, const Ref& b) {
+            return a.g->stats.total_variance() > b.g->stats.total_variance();
+        });
+    int m = (int)std::min(limit, (size_t)std::max(cap, 0));
+    for (int i = 0; i < m; ++i) {
+        export_group(*all[i].g, groups + i);
+        if (xy) { xy[2 * i] = all[i].x; xy[2 * i + 1] = all[i].y; }
+    }
+    return m;
+}
+
+}  // namespace lucid

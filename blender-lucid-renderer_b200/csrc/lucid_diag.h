@@ -1,0 +1,99 @@
+// lucid_diag.h — DiagnosticFilm for the CUDA tracer (host side).
+//
+// The diagnostic kernels append one record per completed path (a path that
+// reached a light, the environment or an emitter; diagnostic_integrator.hpp:
+// 349-389) to a device buffer with warp-aggregated atomics.  After the render
+// the records are sorted into the single-threaded order of the reference's
+// tile loop (micro-tiles, pixels, samples, records along the path) and
+// replayed into the per-pixel statistics below: Welford mean/variance,
+// coarse-type stats, a 3-sigma outlier ring and up to 16 path groups per film
+// cell keyed by the FNV-1a path hash, with the reference's log2-weighted
+// variance eviction (diagnostics/pixel_path_data.hpp:53-220).
+#pragma once
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "../../include/lucid_cuda.h"
+
+namespace lucid {
+
+constexpr int kDiagMaxDepth = 16;
+
+// One completed path as the kernels write it (512 B).
+struct DiagRecord {
+    uint32_t pixel;      // tile-local pixel index (y * tile_w + x)
+    uint32_t sample;     // sample index within the call
+    uint32_t seq;        // bounce at which the path completed
+    uint8_t strategy, light_type, depth, pad;
+    float contrib[3];
+    int32_t object_id[kDiagMaxDepth];
+    uint8_t bsdf[kDiagMaxDepth];
+    uint8_t flags[kDiagMaxDepth];
+    float pos[kDiagMaxDepth][3];
+    float nrm[kDiagMaxDepth][3];
+    uint32_t pad2;
+};
+static_assert(sizeof(DiagRecord) == 512, "DiagRecord layout");
+
+struct DiagStats {   // PathStatistics (path_stats.hpp:63-100)
+    uint32_t count = 0;
+    float mean[3] = {0, 0, 0}, m2[3] = {0, 0, 0}, var[3] = {0, 0, 0};
+    void add(const float* v);
+    float total_variance() const { return var[0] + var[1] + var[2]; }
+    float mean_luminance() const { return 0.2126f * mean[0] + 0.7152f * mean[1] + 0.0722f * mean[2]; }
+};
+
+struct DiagGroup {   // PathGroup (path_stats.hpp:142-232)
+    uint64_t hash = 0;
+    DiagStats stats;
+    uint8_t depth = 0, coarse = 0, light_type = 0, strategy = 0;
+    int32_t object_id[kDiagMaxDepth] = {};
+    uint8_t bsdf[kDiagMaxDepth] = {};
+    uint8_t flags[kDiagMaxDepth] = {};
+    float pos[kDiagMaxDepth][3] = {};
+    float nrm[kDiagMaxDepth][3] = {};
+};
+
+struct DiagPixel {   // PixelPathData<16, 4>
+    static constexpr int kGroups = 16, kOutliers = 4;
+    DiagGroup groups[kGroups];
+    DiagStats coarse[8];
+    uint64_t outlier_hash[kOutliers] = {};
+    float outlier_c[kOutliers][3] = {};
+    size_t num_groups = 0, num_outliers = 0, total = 0, overflow = 0;
+    DiagStats total_stats;
+    void record(const DiagRecord& r, uint64_t hash, uint8_t coarse_type);
+};
+
+class DiagFilm {
+public:
+    void init(int tile_w, int tile_h, int subsample);
+    void clear();
+    void reset() { px_.clear(); valid_ = false; w_ = h_ = sw_ = sh_ = 0; recorded_ = 0; }
+    // Sorts the records into the reference's loop order and replays them.
+    void replay(std::vector<DiagRecord>& records, int tile_w);
+    const DiagPixel* at(int x, int y) const;
+    DiagPixel* at_mut(int x, int y);
+    void stats(LucidDiagStats* out) const;
+    void variance_map(float* out) const;   // tile_w * tile_h floats, cell variance per pixel
+    // get_pixel_diagnostic's export: sorts the cell's groups in place.
+    int export_pixel(int x, int y, bool sort_by_mean, LucidDiagPixel* info, LucidDiagGroup* groups, int cap);
+    int export_top(int n, bool by_mean, LucidDiagGroup* groups, int32_t* xy, int cap) const;
+    static void export_group(const DiagGroup& g, LucidDiagGroup* o);
+    int width() const { return w_; }
+    int height() const { return h_; }
+    bool valid() const { return valid_; }
+    static uint64_t hash(const DiagRecord& r);
+    static uint8_t coarse_type(const DiagRecord& r);
+
+private:
+    int w_ = 0, h_ = 0, sf_ = 2, sw_ = 0, sh_ = 0;
+    bool valid_ = false;
+    size_t recorded_ = 0;
+    std::vector<DiagPixel> px_;
+};
+
+}  // namespace lucid

@@ -23,6 +23,7 @@
 #include <string>
 #include <vector>
 
+#include "lucid_diag.h"
 #include "lucid_engine.h"
 #include "lucid_kernels.cuh"
 
@@ -117,6 +118,12 @@ struct PathPool {
         film_n = 0;
         cap = 0;
     }
+};
+
+// Completed-path records of the path diagnostics and their count.
+struct DiagDevice {
+    DBuf<DiagRecord> recs;
+    DBuf<unsigned long long> count;
 };
 
 struct FrameParams {
@@ -680,6 +687,255 @@ __global__ void k_records(FrameParams f, PathView pv, LucidSampleRecord* out) {
     out[(size_t)p * f.samples + f.s0 + sl] = r;
 }
 
+// ---------------------------------------------------------------- path diagnostics
+// trace{Simple,NEE,MIS}WithDiagnostics (integrator/path_tracer.hpp:880-1514)
+// with the PathDiagnosticRecorder (diagnostics/diagnostic_integrator.hpp:
+// 87-389): one thread follows one (pixel, sample) path through every bounce;
+// intersectScene covers every triangle (no volume-boundary skipping), shadow
+// rays are any-hit queries over every triangle, volumes are ignored.  Each
+// completed path (light, environment or emitter reached) is appended to the
+// record buffer; the host replays the records into the DiagnosticFilm.
+enum DiagBsdf { DB_DIFFUSE = 0, DB_GLOSSY = 1, DB_MIRROR = 2, DB_GLASS = 3, DB_EMISSION = 4 };
+enum DiagLight { DL_UNKNOWN = 0, DL_POINT = 1, DL_AREA = 2, DL_DIRECTIONAL = 3, DL_SPOT = 4, DL_ENV = 5, DL_EMISSIVE = 6 };
+enum DiagStrategy { DS_BSDF = 0, DS_NEE = 1, DS_MIS_BSDF = 2, DS_MIS_NEE = 3 };
+
+LD uint8_t diag_light_type(int type) {   // to_light_source_type (diagnostics/path_types.hpp)
+    switch (type) {
+        case LIGHT_EMISSIVE: return DL_AREA;
+        case LIGHT_POINT: return DL_POINT;
+        case LIGHT_SUN: return DL_DIRECTIONAL;
+        case LIGHT_SPOT: return DL_SPOT;
+        case LIGHT_AREA: return DL_AREA;
+    }
+    return DL_UNKNOWN;
+}
+
+struct DiagPath {   // the recorder's current PathTrace
+    int depth;
+    int32_t obj[kDiagMaxDepth];
+    uint8_t bsdf[kDiagMaxDepth], flags[kDiagMaxDepth];
+    V3 pos[kDiagMaxDepth], nrm[kDiagMaxDepth];
+};
+
+struct DiagOut {
+    DiagRecord* recs;
+    unsigned long long* count;
+    long long cap;
+};
+
+LD void diag_vertex(DiagPath& P, int32_t obj, uint8_t type, bool delta, V3 p, V3 n) {
+    if (P.depth >= kDiagMaxDepth) return;
+    P.obj[P.depth] = obj; P.bsdf[P.depth] = type; P.flags[P.depth] = delta ? 1 : 0;
+    P.pos[P.depth] = p; P.nrm[P.depth] = n;
+    ++P.depth;
+}
+
+// record_completed_path_with_geometry (diagnostic_integrator.hpp:349-389):
+// the path plus a final Emission vertex (object -1 for the environment, else
+// -(light + 2)) when there is room.
+LD void diag_complete(const DiagOut& o, const DiagPath& P, uint32_t pixel, uint32_t sample, uint32_t seq,
+                      uint8_t strategy, int light_id, uint8_t ltype, RGB c, V3 lpos) {
+    unsigned long long slot = atomicAdd(o.count, 1ull);
+    if ((long long)slot >= o.cap) return;   // the host grows the buffer and runs the wave again
+    DiagRecord* r = o.recs + slot;
+    int d = P.depth;
+    for (int k = 0; k < d; ++k) {
+        r->object_id[k] = P.obj[k]; r->bsdf[k] = P.bsdf[k]; r->flags[k] = P.flags[k];
+        r->pos[k][0] = P.pos[k].x; r->pos[k][1] = P.pos[k].y; r->pos[k][2] = P.pos[k].z;
+        r->nrm[k][0] = P.nrm[k].x; r->nrm[k][1] = P.nrm[k].y; r->nrm[k][2] = P.nrm[k].z;
+    }
+    if (d < kDiagMaxDepth) {
+        r->object_id[d] = (ltype == DL_ENV) ? -1 : -(light_id + 2);
+        r->bsdf[d] = DB_EMISSION; r->flags[d] = 0;
+        r->pos[d][0] = lpos.x; r->pos[d][1] = lpos.y; r->pos[d][2] = lpos.z;
+        r->nrm[d][0] = 0.0f; r->nrm[d][1] = 0.0f; r->nrm[d][2] = 0.0f;
+        ++d;
+    }
+    r->pixel = pixel; r->sample = sample; r->seq = seq;
+    r->strategy = strategy; r->light_type = ltype; r->depth = (uint8_t)d; r->pad = 0;
+    r->contrib[0] = c.r; r->contrib[1] = c.g; r->contrib[2] = c.b;
+}
+
+__global__ void __launch_bounds__(128) k_diag_paths(DevScene sc, FrameParams f, PathView pv, DiagOut out,
+                                                    int pixel_base) {
+    int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= f.n_wave) return;
+    const int algo = f.algo;   // ALGO_SIMPLE, ALGO_MIS, else NEE (pybind_renderer.hpp:300-309)
+    const bool simple = algo == ALGO_SIMPLE, mis = algo == ALGO_MIS, nee_only = !simple && !mis;
+    const uint32_t pixel = (uint32_t)(pixel_base + id % f.npix);
+    const uint32_t sample = (uint32_t)(f.s0 + id / f.npix);
+    ulonglong2 rs = pv.rng[id];
+    Rng rng;
+    rng.state = rs.x;
+    rng.inc = rs.y;
+    float4 ro = pv.ray_o[id], rd = pv.ray_d[id];
+    V3 o = f3(ro), d = f3(rd);
+    float tmin = 0.0f;
+    RGB result = rgb(0.f, 0.f, 0.f), T = rgb(1.f, 1.f, 1.f);
+    float last_pdf = 0.0f;
+    bool ok = true;
+    DiagPath P;
+    P.depth = 0;
+    for (int depth = 0; depth < f.max_depth; ++depth) {
+        const uint32_t seq = (uint32_t)depth * 2u;
+        HitRec h = scene_closest(sc, o, d, tmin, 1e30f, ok);
+        float lt = 1e30f;
+        int li = (depth == 0) ? -1 : native_lights_closest(sc, o, d, lt);
+        if (li >= 0 && (h.prim < 0 || lt < h.t)) {
+            if (!nee_only || depth == 0) {
+                const DevLight& L = sc.lights[sc.native_start + li];
+                uint8_t ltype = diag_light_type(__float_as_int(L.pos_type.w));
+                V3 lp = o + d * lt;
+                float mw = 1.0f;
+                if (mis) {
+                    float lpdf = 0.0f;
+                    if (sc.num_lights > 0) {
+                        float sp = area_ratio(L.normal_area.w, sc.total_light_area);
+                        if (sp > 0.0f) {
+                            V3 ln = (__float_as_int(L.pos_type.w) == LIGHT_POINT) ? normalize_nz(lp - f3(L.pos_type))
+                                                                                  : f3(L.normal_area);
+                            lpdf = pdf_light(L.normal_area.w, o, lp, ln) * sp;
+                        }
+                    }
+                    mw = (last_pdf > MIN_PDF && lpdf > MIN_PDF) ? mis_power(last_pdf, lpdf) : 1.0f;
+                }
+                RGB em = c3(L.emission_radius);
+                RGB pc = mis ? mul(T, em) * mw : mul(T, em);
+                diag_complete(out, P, pixel, sample, seq, mis ? DS_MIS_BSDF : DS_BSDF, li, ltype, pc, lp);
+                result = result + pc;
+            }
+            break;
+        }
+        if (h.prim < 0) {
+            if (!nee_only || depth == 0) {
+                RGB env = mul(T, rgb(sc.env[0], sc.env[1], sc.env[2]));
+                diag_complete(out, P, pixel, sample, seq, mis ? DS_MIS_BSDF : DS_BSDF, -1, DL_ENV, env,
+                              o + d * 1000.0f);
+                result = result + env;
+            }
+            break;
+        }
+        V3 p = o + d * h.t;
+        int4 pi = sc.prim_info[h.prim];
+        V3 fn = f3(sc.prim_fn[h.prim]);
+        V3 n = fn;
+        if (pi.w) {
+            float w = 1.0f - h.u - h.v;
+            V3 ni = f3(sc.prim_vn[3 * h.prim]) * w + f3(sc.prim_vn[3 * h.prim + 1]) * h.u +
+                    f3(sc.prim_vn[3 * h.prim + 2]) * h.v;
+            n = make_dir_or(ni, fn);
+        }
+        const DevMaterial& dm = sc.materials[pi.x];
+        Mat m;
+        m.albedo = c3(dm.albedo_metallic);
+        m.metallic = dm.albedo_metallic.w;
+        m.roughness = smax(dm.rough_trans_ior_flags.x, MIN_ROUGHNESS);
+        m.transmission = dm.rough_trans_ior_flags.y;
+        m.ior = dm.rough_trans_ior_flags.z;
+        RGB em = c3(dm.emission);
+        const bool has_em = dm.emission.w != 0.0f;
+        // classify_bsdf / is_delta_bsdf (diagnostic_integrator.hpp:25-60)
+        uint8_t bt = m.transmission > 0.5f                       ? DB_GLASS
+                     : (m.roughness < 0.01f && m.metallic > 0.5f) ? DB_MIRROR
+                     : (m.metallic > 0.5f || m.roughness < 0.5f)  ? DB_GLOSSY
+                                                                  : DB_DIFFUSE;
+        bool delta = (m.transmission > 0.5f && m.roughness < 0.01f) || (m.metallic > 0.5f && m.roughness < 0.01f);
+        V3 wo = -d;
+        bool front = dot(wo, n) > 0;
+        V3 sn = n;
+        if (m.transmission < 0.5f && !front) sn = -n;
+        if (simple) {
+            if (has_em) {
+                RGB ec = mul(T, em);
+                diag_complete(out, P, pixel, sample, seq, DS_BSDF, pi.x, DL_EMISSIVE, ec, p);
+                result = result + ec;
+                break;
+            }
+            diag_vertex(P, pi.x, bt, delta, p, n);
+        } else {
+            bool do_nee = false;
+            if (has_em && (mis || depth == 0)) {
+                float mw = 1.0f;
+                if (mis && sc.num_lights > 0 && last_pdf > MIN_PDF && pi.z >= 0) {
+                    const DevLight& L = sc.lights[pi.z];
+                    float sp = area_ratio(L.normal_area.w, sc.total_light_area);
+                    if (sp > 0.0f) {
+                        float lpdf = pdf_light(L.normal_area.w, o, p, n) * sp;
+                        if (lpdf > MIN_PDF) mw = mis_power(last_pdf, lpdf);
+                    }
+                }
+                RGB ec = mis ? mul(T, em) * mw : mul(T, em);
+                diag_complete(out, P, pixel, sample, seq, mis ? DS_MIS_BSDF : DS_BSDF, pi.x, DL_EMISSIVE, ec, p);
+                result = result + ec;
+            } else if (!has_em) {
+                diag_vertex(P, pi.x, bt, delta, p, n);
+                do_nee = true;
+            }
+            const bool transmissive = m.transmission > 0.5f;
+            if (do_nee && sc.num_lights > 0 && !transmissive) {
+                float usel = randf(rng);
+                int sli = select_light(sc, usel);
+                const DevLight& L = sc.lights[sli];
+                float lsp = area_ratio(L.normal_area.w, sc.total_light_area);
+                if (lsp > 1e-6f) {
+                    float u1 = randf(rng), u2 = randf(rng);
+                    LightSample ls = sample_light(L, p, u1, u2);
+                    if (ls.pdf > MIN_PDF) {
+                        float nl = dot(sn, ls.dir);
+                        if (nl > 1e-6f) {
+                            bool occ = bvh_any(sc, p, ls.dir, RAY_T_MIN, ls.dist, ok) ||
+                                       (sc.num_bnd_tris &&
+                                        list_any(sc.bnd_tris, sc.num_bnd_tris, p, ls.dir, RAY_T_MIN, ls.dist));
+                            if (!occ) {
+                                RGB fb = eval_bsdf(m, wo, ls.dir, sn);
+                                float pl = ls.pdf * lsp;
+                                RGB nr;
+                                if (mis) {
+                                    float pb = pdf_bsdf(m, wo, ls.dir, sn);
+                                    float mw = mis_power(pl, pb);
+                                    nr = mul(bsdf_weight(fb, nl, pl) * mw, ls.emission);
+                                } else {
+                                    nr = mul(bsdf_weight(fb, nl, pl), ls.emission);
+                                }
+                                RGB tot = mul(T, nr);
+                                diag_complete(out, P, pixel, sample, seq + 1u, mis ? DS_MIS_NEE : DS_NEE,
+                                              sli - sc.native_start, diag_light_type(__float_as_int(L.pos_type.w)),
+                                              tot, ls.pos);
+                                result = result + tot;
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        V3 smp_n = (m.transmission > 0.5f) ? n : sn;
+        float u1 = randf(rng), u2 = randf(rng), u3 = randf(rng);
+        BsdfSample bs = sample_bsdf(m, wo, smp_n, u1, u2, u3, rng);
+        if (!(bs.kind == BS_PRECOMP || bs.pdf > MIN_PDF)) break;
+        RGB w;
+        if (bs.kind == BS_PRECOMP) {
+            w = bs.f;
+        } else {
+            float c = fabsf(dot(smp_n, bs.wi));
+            if (c <= 1e-6f || bs.pdf < MIN_PDF) break;
+            w = bsdf_weight(bs.f, c, bs.pdf);
+        }
+        T = mul(T, w);
+        if (mis) last_pdf = (bs.kind == BS_EVAL) ? bs.pdf : 0.0f;
+        if (depth >= 3) {
+            float rr = smin(smax3(T.r, T.g, T.b), 0.95f);
+            if (randf(rng) > rr) break;
+            T = T * (1.0f / rr);
+        }
+        if (!rgb_valid(T)) break;
+        o = p;
+        d = bs.wi;
+        tmin = RAY_T_MIN;
+    }
+    pv.rad[id] = make_float4(result.r, result.g, result.b, 0.0f);
+    if (!ok) atomicAdd(&pv.errors[0], 1);
+}
+
 // ---------------------------------------------------------------- debug passes
 // render_debug (renderer.hpp:59-93): intersectScene from t = 0 over every
 // triangle (boundary meshes included), no jitter.
@@ -899,6 +1155,7 @@ Engine::~Engine() {
     if (async_pinned_) cudaFreeHost(async_pinned_);
     if (ds_) { ds_->release(); delete ds_; }
     if (pool_) { pool_->release(); delete pool_; }
+    delete diag_dev_;
     if (stream_) cudaStreamDestroy(S(stream_));
 }
 
@@ -1214,7 +1471,174 @@ const double kKindBytes[K_NUM] = {kBytesRaygen, kBytesTrace, kBytesTrace, kBytes
 
 int Engine::render(const LucidRenderParams& p, float* out_host, LucidSampleRecord* recs, float* out_device) {
     std::lock_guard<std::mutex> lk(gpu_mu_);
+    if (diag_enabled_) {
+        if (recs) return fail(LUCID_ERR_INVALID, "per-sample records are not produced while diagnostics are enabled");
+        return render_diag_impl(p, out_host, out_device);
+    }
     return render_impl(p, out_host, recs, out_device, nullptr, false);
+}
+
+// ---------------------------------------------------------------- path diagnostics (host)
+constexpr long long kDiagWavePaths = 1LL << 20;   // paths per diagnostic wave
+
+// render_tile with diagnostics enabled (pybind_renderer.hpp:205-316): a
+// fresh DiagnosticFilm per call.  The tile is processed in bands of whole
+// 8-row micro-tile rows, so replaying each band's records (sorted into the
+// reference's loop order) band after band gives the order of the whole tile.
+int Engine::render_diag_impl(const LucidRenderParams& p, float* out_host, float* out_device) {
+    reset_cancel();
+    if (p.tile_w <= 0 || p.tile_h <= 0 || p.full_w <= 0 || p.full_h <= 0)
+        return fail(LUCID_ERR_INVALID, "tile and image sizes must be positive");
+    const size_t np = (size_t)p.tile_w * p.tile_h;
+    if (out_host) std::fill(out_host, out_host + np * 4, 0.0f);
+    if (!scene_loaded_ || !camera_set_) return fail(LUCID_ERR_NO_SCENE, "scene or camera not set");
+    CK(cudaSetDevice(device_));
+    if (p.samples <= 0) return fail(LUCID_ERR_INVALID, "samples must be >= 1");
+    if (p.max_depth > kMaxDepth) return fail(LUCID_ERR_INVALID, "max_depth too large");
+    if (np > (size_t)0x7fffffff / 2) return fail(LUCID_ERR_INVALID, "tile too large");
+    diag_film_.init(p.tile_w, p.tile_h, diag_cfg_.subsample_factor);
+    cudaStream_t st = S(stream_);
+    const long long wave = wave_cap_ > 0 ? std::min(wave_cap_, kDiagWavePaths) : kDiagWavePaths;
+    const long long row_paths = (long long)p.tile_w * p.samples;
+    int band_rows = 8 * (int)std::max<long long>(1, wave / (8 * row_paths));
+    band_rows = std::min(band_rows, (p.tile_h + 7) / 8 * 8);
+    const long long band_np = (long long)band_rows * p.tile_w;
+    const int spw = (int)std::max<long long>(1, std::min<long long>(p.samples, wave / band_np));
+    int rc = ensure_pool((long long)spw * band_np, false);
+    if (rc != LUCID_OK) return rc;
+    PathPool& P = *pool_;
+    if (P.film_n < np) {
+        CK(P.film.alloc(np));
+        CK(P.out.alloc(np));
+        P.film_n = np;
+    }
+    if (!diag_dev_) diag_dev_ = new DiagDevice();
+    DiagDevice& D = *diag_dev_;
+    const long long want = diag_cfg_.record_capacity > 0 ? diag_cfg_.record_capacity : (1LL << 20);
+    if ((long long)D.recs.n < want) CK(D.recs.alloc((size_t)want));
+    if (!D.count.p) CK(D.count.alloc(1));
+    CK(cudaMemsetAsync(P.film.p, 0, np * sizeof(float4), st));
+    CK(cudaMemsetAsync(P.errors.p, 0, 4 * sizeof(int), st));
+
+    FrameParams f;
+    for (int k = 0; k < 3; ++k) { f.pos[k] = cam_.pos[k]; f.fwd[k] = cam_.forward[k]; f.right[k] = cam_.right[k]; f.up[k] = cam_.up[k]; }
+    f.aspect = (float)p.full_w / (float)p.full_h;
+    f.scale = std::tan(cam_.fov * 0.5f);
+    f.tile_x = p.tile_x; f.tile_w = p.tile_w; f.full_w = p.full_w; f.full_h = p.full_h;
+    f.samples = p.samples; f.sample_offset = p.sample_offset; f.max_depth = p.max_depth; f.algo = algo_;
+    f.records = 0;
+
+    stats_ = LucidRenderStats{};
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    cudaEventRecord(t0, st);
+    int status = LUCID_OK;
+    int waves = 0;
+    std::vector<DiagRecord> band;
+    for (int y0 = 0; y0 < p.tile_h && status == LUCID_OK; y0 += band_rows) {
+        const int bh = std::min(band_rows, p.tile_h - y0);
+        f.tile_y = p.tile_y + y0;
+        f.tile_h = bh;
+        f.npix = bh * p.tile_w;
+        band.clear();
+        for (int s0 = 0; s0 < p.samples; s0 += spw) {
+            if (is_cancelled()) { status = LUCID_ERR_CANCELLED; break; }
+            const int this_spw = std::min(spw, p.samples - s0);
+            f.s0 = s0;
+            f.n_wave = this_spw * f.npix;
+            unsigned long long produced = 0;
+            for (;;) {
+                CK(cudaMemsetAsync(D.count.p, 0, sizeof(unsigned long long), st));
+                k_raygen<<<(f.n_wave + 255) / 256, 256, 0, st>>>(f, P.view);
+                DiagOut o{D.recs.p, D.count.p, (long long)D.recs.n};
+                k_diag_paths<<<(f.n_wave + 127) / 128, 128, 0, st>>>(ds_->view, f, P.view, o, y0 * p.tile_w);
+                CK(cudaGetLastError());
+                CK(cudaMemcpyAsync(&produced, D.count.p, sizeof(produced), cudaMemcpyDeviceToHost, st));
+                CK(cudaStreamSynchronize(st));
+                if (produced <= (unsigned long long)D.recs.n) break;
+                // the wave is deterministic: grow the buffer and run it again
+                CK(D.recs.alloc((size_t)(produced + produced / 4)));
+            }
+            k_film<<<(f.npix + 255) / 256, 256, 0, st>>>(f.npix, this_spw, P.rad.p, P.film.p + (size_t)y0 * p.tile_w);
+            const size_t old = band.size();
+            band.resize(old + (size_t)produced);
+            if (produced)
+                CK(cudaMemcpyAsync(band.data() + old, D.recs.p, (size_t)produced * sizeof(DiagRecord),
+                                   cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            ++waves;
+        }
+        if (status == LUCID_OK) diag_film_.replay(band, p.tile_w);
+    }
+    const int np_i = (int)np;
+    k_output<<<(np_i + 255) / 256, 256, 0, st>>>(p.tile_w, p.tile_h, P.film.p, out_device ? (float4*)out_device : P.out.p);
+    CK(cudaGetLastError());
+    cudaEventRecord(t1, st);
+    int herr[4] = {0, 0, 0, 0};
+    CK(cudaMemcpyAsync(herr, P.errors.p, sizeof(herr), cudaMemcpyDeviceToHost, st));
+    if (out_host && !out_device)
+        CK(cudaMemcpyAsync(out_host, P.out.p, np * sizeof(float4), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    float tot = 0.0f;
+    cudaEventElapsedTime(&tot, t0, t1);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    stats_.total_ms = tot;
+    stats_.paths = (double)np * p.samples;
+    stats_.waves = waves;
+    if (herr[0] != 0) return fail(LUCID_ERR_OVERFLOW, "BVH traversal stack overflow");
+    if (status == LUCID_ERR_CANCELLED) return fail(LUCID_ERR_CANCELLED, "render cancelled");
+    return LUCID_OK;
+}
+
+// PathRecordingConfig::standard() (diagnostics/path_stats_config.hpp).
+int Engine::diag_enable(const LucidDiagConfig* cfg) {
+    std::lock_guard<std::mutex> lk(gpu_mu_);
+    LucidDiagConfig c{2, 16, 4, 16, 0.001f, 3.0f, 0};
+    if (cfg) c = *cfg;
+    if (c.subsample_factor < 1) return fail(LUCID_ERR_INVALID, "subsample_factor must be >= 1");
+    diag_cfg_ = c;
+    diag_enabled_ = true;
+    diag_film_.reset();
+    return LUCID_OK;
+}
+int Engine::diag_disable() {
+    std::lock_guard<std::mutex> lk(gpu_mu_);
+    diag_enabled_ = false;
+    diag_film_.reset();
+    if (diag_dev_) { delete diag_dev_; diag_dev_ = nullptr; }
+    return LUCID_OK;
+}
+int Engine::diag_clear() {
+    std::lock_guard<std::mutex> lk(gpu_mu_);
+    if (diag_film_.valid()) diag_film_.clear();
+    return LUCID_OK;
+}
+int Engine::diag_stats(LucidDiagStats* out) {
+    std::lock_guard<std::mutex> lk(gpu_mu_);
+    std::memset(out, 0, sizeof(*out));
+    if (diag_film_.valid()) diag_film_.stats(out);
+    return LUCID_OK;
+}
+int Engine::diag_pixel(int x, int y, bool by_mean, LucidDiagPixel* info, LucidDiagGroup* groups, int cap) {
+    std::lock_guard<std::mutex> lk(gpu_mu_);
+    std::memset(info, 0, sizeof(*info));
+    if (!diag_film_.valid()) return 0;
+    return diag_film_.export_pixel(x, y, by_mean, info, groups, groups ? cap : 0);
+}
+int Engine::diag_variance_map(float* out, size_t cap) {
+    std::lock_guard<std::mutex> lk(gpu_mu_);
+    if (!diag_film_.valid()) return 0;
+    size_t n = (size_t)diag_film_.width() * diag_film_.height();
+    if (cap < n) return fail(LUCID_ERR_INVALID, "variance map buffer too small");
+    diag_film_.variance_map(out);
+    return (int)n;
+}
+int Engine::diag_top(int n, bool by_mean, LucidDiagGroup* groups, int32_t* xy, int cap) {
+    std::lock_guard<std::mutex> lk(gpu_mu_);
+    if (!diag_film_.valid()) return 0;
+    return diag_film_.export_top(n, by_mean, groups, xy, groups ? cap : 0);
 }
 
 // Adds one render's film into the async accumulator (float4 sum per pixel).

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "../../include/lucid_cuda.h"
+#include "lucid_diag.h"
 #include "lucid_host.h"
 #include "lucid_types.h"
 
@@ -15,6 +16,7 @@ namespace lucid {
 
 struct DeviceScene;   // device allocations of one uploaded scene
 struct PathPool;      // wavefront SoA path state
+struct DiagDevice;    // device record buffer of the path diagnostics
 
 class Engine {
 public:
@@ -35,6 +37,15 @@ public:
     bool async_running() const { return async_run_.load(); }
     int render_noalloc(const LucidRenderParams& p, float* d_out);
     int render_debug(int tx, int ty, int tw, int th, int fw, int fh, const char* mode, float* out_host);
+    // Path diagnostics (PyRenderer's diagnostics API, pybind_renderer.hpp:893-1102).
+    int diag_enable(const LucidDiagConfig* cfg);
+    int diag_disable();
+    bool diag_enabled() const { return diag_enabled_; }
+    int diag_clear();
+    int diag_stats(LucidDiagStats* out);
+    int diag_pixel(int x, int y, bool by_mean, LucidDiagPixel* info, LucidDiagGroup* groups, int cap);
+    int diag_variance_map(float* out, size_t cap);
+    int diag_top(int n, bool by_mean, LucidDiagGroup* groups, int32_t* xy, int cap);
     int scene_stats(int out8[8]) const;
     int stats(LucidRenderStats* out) const;
     int set_wave_capacity(long long paths);
@@ -50,6 +61,7 @@ public:
 private:
     int render_impl(const LucidRenderParams& p, float* out_host, LucidSampleRecord* recs, float* out_device,
                     void* accumulate, bool from_async);
+    int render_diag_impl(const LucidRenderParams& p, float* out_host, float* out_device);
     void async_worker();
     int ensure_pool(long long paths, bool records);
     int build_bvh();
@@ -71,6 +83,11 @@ private:
     int bvh_nodes_ = 0, bvh_leaves_ = 0, bvh_depth_ = 0, num_big_ = 0;
     // one GPU call at a time per context (the reference's gpu_mutex_)
     std::mutex gpu_mu_;
+    // path diagnostics
+    bool diag_enabled_ = false;
+    LucidDiagConfig diag_cfg_{};
+    DiagFilm diag_film_;
+    DiagDevice* diag_dev_ = nullptr;
     // async accumulator
     std::thread async_thread_;
     std::atomic<bool> async_run_{false}, async_reset_{false};

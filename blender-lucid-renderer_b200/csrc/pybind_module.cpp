@@ -10,6 +10,8 @@
 #include <pybind11/pybind11.h>
 #include <pybind11/stl.h>
 
+#include <algorithm>
+#include <array>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -22,6 +24,100 @@
 namespace py = pybind11;
 
 namespace {
+
+// ---- diagnostics value types (diagnostics/path_stats_config.hpp,
+// diagnostic_export.hpp:26-49, pybind_renderer.hpp:971-981) ----
+struct PathRecordingConfig {
+    int subsample_factor = 2, max_groups_per_pixel = 16, max_outliers_per_pixel = 4, max_depth = 16;
+    float variance_threshold = 0.001f, outlier_threshold = 3.0f;
+    static PathRecordingConfig minimal() { return {4, 8, 2, 8, 0.01f, 5.0f}; }
+    static PathRecordingConfig standard() { return {}; }
+    static PathRecordingConfig detailed() { return {1, 32, 8, 16, 0.0001f, 2.0f}; }
+    // sampled pixels x (8 coarse stats + groups + outliers + 32 B) + 1 MiB
+    size_t estimate_memory_bytes(size_t w, size_t h) const {
+        size_t sf = (size_t)std::max(1, subsample_factor);
+        size_t pixels = (w / sf) * (h / sf);
+        size_t stats = 4 + 9 * sizeof(float);
+        size_t group = 8 + stats + 16 * 8 + 2 * 16 * 12 + 4;
+        size_t per_pixel = 8 * stats + (size_t)max_groups_per_pixel * group +
+                           (size_t)max_outliers_per_pixel * (8 + 12) + 32;
+        return pixels * per_pixel + 1024 * 1024;
+    }
+};
+
+struct ExportedGroupInfo {
+    size_t pixel_x = 0, pixel_y = 0;
+    std::string signature, signature_heckbert;
+    std::vector<int32_t> object_ids;
+    std::string object_path;
+    uint32_t sample_count = 0;
+    float mean_luminance = 0.0f, variance_luminance = 0.0f;
+    std::array<float, 3> mean_rgb{}, variance_rgb{};
+    uint8_t depth = 0, coarse_type = 0;
+    std::string coarse_type_name, strategy_name;
+    std::vector<std::array<float, 3>> positions, normals;
+};
+
+enum class TopGroupSortBy { Variance, Mean };
+
+struct PixelDiagnosticInfo {
+    bool valid = false;
+    size_t sample_count = 0;
+    float variance = 0.0f;
+    size_t group_count = 0, outlier_count = 0;
+    std::array<float, 3> mean_rgb{};
+    std::vector<ExportedGroupInfo> top_groups;
+};
+
+struct GlobalDiagnosticStats {
+    size_t total_samples = 0, active_pixels = 0, total_groups = 0, total_overflow = 0;
+    float total_variance = 0.0f;
+};
+
+// bsdf_type_short / bsdf_type_heckbert / light_source_heckbert
+// (diagnostics/path_types.hpp:56-157), coarse_type_name (path_stats.hpp:26-40).
+char bsdf_short(uint8_t t) { return t < 6 ? "DGMTLE"[t] : '?'; }
+char bsdf_heckbert(uint8_t t) { return t < 6 ? "DSSSEE"[t] : '?'; }
+const char* light_heckbert(uint8_t t) {
+    switch (t) {
+        case 1: case 3: case 4: return "LSD";
+        case 2: return "LDD";
+        case 5: return "LDE";
+    }
+    return "L??";
+}
+const char* coarse_name(uint8_t t) {
+    static const char* n[8] = {"Direct-NoDelta-BSDF",   "Direct-NoDelta-NEE",   "Direct-Delta-BSDF",
+                               "Direct-Delta-NEE",      "Indirect-NoDelta-BSDF", "Indirect-NoDelta-NEE",
+                               "Indirect-Delta-BSDF",   "Indirect-Delta-NEE"};
+    return n[t & 7];
+}
+const char* strategy_name(uint8_t s) {
+    static const char* n[4] = {"BSDF", "NEE", "MIS_BSDF", "MIS_NEE"};
+    return s < 4 ? n[s] : "Unknown";
+}
+std::string signature_of(const LucidDiagGroup& g) {
+    std::string sig;
+    for (int i = 0; i < g.depth; ++i) sig += bsdf_short(g.bsdf[i]);
+    return sig;
+}
+std::string heckbert_of(const LucidDiagGroup& g) {   // PathGroup::signature_heckbert (path_stats.hpp:210-238)
+    std::string sig = light_heckbert(g.light_type);
+    int end = g.depth;
+    while (end > 0 && (g.bsdf[end - 1] == 4 || g.bsdf[end - 1] == 5)) --end;
+    if (end > 0) {
+        sig += ' ';
+        for (int i = 0; i < end; ++i) {
+            sig += bsdf_heckbert(g.bsdf[i]);
+            if (i + 1 < end) sig += ' ';
+        }
+    }
+    return sig + " DSE";
+}
+float variance_luminance(const LucidDiagGroup& g) {   // PathStatistics::variance_luminance (path_stats.hpp:117-123)
+    return 0.2126f * 0.2126f * g.variance_rgb[0] + 0.7152f * 0.7152f * g.variance_rgb[1] +
+           0.0722f * 0.0722f * g.variance_rgb[2];
+}
 
 class Renderer {
 public:
@@ -56,6 +152,7 @@ public:
                     float fov) {
         lucid_cuda_set_camera(ctx_, px, py, pz, dx, dy, dz, ux, uy, uz, fov);
         camera_set_ = true;
+        cam_pos_[0] = px; cam_pos_[1] = py; cam_pos_[2] = pz;
     }
     void set_algorithm(const std::string& a) {
         algorithm_ = a;
@@ -71,6 +168,7 @@ public:
         std::vector<float> px((size_t)tw * th * 4, 0.0f);
         LucidRenderParams p{tx, ty, tw, th, fw, fh, samples, offset, depth, 0};
         int rc = lucid_cuda_render(ctx_, &p, px.data(), nullptr);
+        if (rc != LUCID_ERR_NO_SCENE) { last_tile_w_ = tw; last_tile_h_ = th; }
         if (rc == LUCID_ERR_NO_SCENE) {
             // the reference returns a zero buffer (pybind_renderer.hpp:200-203)
             std::fprintf(stderr, "[lucidrenderer] Scene or camera not set\n");
@@ -109,6 +207,132 @@ public:
         return path + " \xe2\x86\x92 Camera";
     }
 
+    // object_path_string with the light type (pybind_renderer.hpp:1198-1268)
+    std::string object_path_typed(const std::vector<int32_t>& ids, uint8_t light_type) const {
+        if (ids.empty()) return "Camera";
+        std::string path;
+        size_t start = ids.size();
+        int32_t last = ids[start - 1];
+        if (light_type == 5) {
+            path = "Environment";
+            if (last == -1) --start;
+        } else if (light_type == 6) {
+            path = get_object_name(last);
+            --start;
+        } else if (light_type >= 1 && light_type <= 4) {
+            static const char* names[5] = {"", "PointLight", "AreaLight", "SunLight", "SpotLight"};
+            path = names[light_type];
+            if (last <= -2) --start;
+        } else if (last <= -2) { path = "Light(?)"; --start; }
+        else if (last == -1) { path = "Environment(?)"; --start; }
+        else path = "(terminated)";
+        for (size_t i = start; i > 0; --i) path += " \xe2\x86\x92 " + get_object_name(ids[i - 1]);
+        return path + " \xe2\x86\x92 Camera";
+    }
+
+    // ---- path diagnostics (pybind_renderer.hpp:893-1102) ----
+    void enable_diagnostics(const PathRecordingConfig& c) {
+        LucidDiagConfig cfg{c.subsample_factor, c.max_groups_per_pixel, c.max_outliers_per_pixel, c.max_depth,
+                            c.variance_threshold, c.outlier_threshold, 0};
+        if (lucid_cuda_diag_enable(ctx_, &cfg) != LUCID_OK)
+            throw std::invalid_argument(std::string("enable_diagnostics: ") + lucid_cuda_last_error(ctx_));
+        diag_cfg_ = c;
+    }
+    void disable_diagnostics() { lucid_cuda_diag_disable(ctx_); }
+    bool is_diagnostics_enabled() { return lucid_cuda_diag_enabled(ctx_) == 1; }
+    void clear_diagnostics() { lucid_cuda_diag_clear(ctx_); }
+    GlobalDiagnosticStats get_diagnostic_stats() {
+        LucidDiagStats st{};
+        GlobalDiagnosticStats out;
+        if (lucid_cuda_diag_stats(ctx_, &st) != LUCID_OK) return out;
+        out.total_samples = st.total_samples; out.active_pixels = st.active_pixels;
+        out.total_groups = st.total_groups; out.total_overflow = st.total_overflow;
+        return out;
+    }
+    size_t diag_paths_recorded() {
+        LucidDiagStats st{};
+        return lucid_cuda_diag_stats(ctx_, &st) == LUCID_OK ? (size_t)st.paths_recorded : 0;
+    }
+    std::vector<float> get_diagnostic_variance_map() {
+        std::vector<float> v((size_t)last_tile_w_ * last_tile_h_);
+        int n = v.empty() ? 0 : lucid_cuda_diag_variance_map(ctx_, v.data(), v.size());
+        v.resize(n > 0 ? (size_t)n : 0);
+        return v;
+    }
+    // DiagnosticFilm::metadata_json (diagnostic_film.hpp:230-243)
+    std::string export_diagnostic_json() {
+        if (lucid_cuda_diag_enabled(ctx_) != 1 || last_tile_w_ == 0) return "{}";
+        int sf = std::max(1, diag_cfg_.subsample_factor);
+        std::string j = "{\n";
+        j += "  \"width\": " + std::to_string(last_tile_w_) + ",\n";
+        j += "  \"height\": " + std::to_string(last_tile_h_) + ",\n";
+        j += "  \"sampled_width\": " + std::to_string(last_tile_w_ / sf) + ",\n";
+        j += "  \"sampled_height\": " + std::to_string(last_tile_h_ / sf) + ",\n";
+        j += "  \"subsample_factor\": " + std::to_string(sf) + ",\n";
+        j += "  \"max_groups\": " + std::to_string(diag_cfg_.max_groups_per_pixel) + ",\n";
+        j += "  \"max_outliers\": " + std::to_string(diag_cfg_.max_outliers_per_pixel) + ",\n";
+        j += "  \"total_samples\": " + std::to_string(diag_paths_recorded()) + "\n";
+        j += "}\n";
+        return j;
+    }
+    // DiagnosticExporter::convert_refs (diagnostic_export.hpp:257-285)
+    std::vector<ExportedGroupInfo> get_top_variance_groups(size_t count) {
+        std::vector<LucidDiagGroup> g(std::max<size_t>(count, 1));
+        std::vector<int32_t> xy(2 * g.size());
+        int n = lucid_cuda_diag_top_groups(ctx_, (int)count, 0, g.data(), xy.data(), (int)g.size());
+        std::vector<ExportedGroupInfo> out;
+        for (int i = 0; i < n; ++i) {
+            ExportedGroupInfo e;
+            e.pixel_x = (size_t)xy[2 * i]; e.pixel_y = (size_t)xy[2 * i + 1];
+            e.signature = signature_of(g[i]);
+            e.sample_count = g[i].count;
+            e.mean_luminance = g[i].mean_luminance;
+            e.variance_luminance = variance_luminance(g[i]);
+            for (int c = 0; c < 3; ++c) { e.mean_rgb[c] = g[i].mean_rgb[c]; e.variance_rgb[c] = g[i].variance_rgb[c]; }
+            e.depth = g[i].depth; e.coarse_type = g[i].coarse_type;
+            e.coarse_type_name = coarse_name(g[i].coarse_type);
+            out.push_back(std::move(e));
+        }
+        return out;
+    }
+    // get_pixel_diagnostic (pybind_renderer.hpp:1008-1102)
+    PixelDiagnosticInfo get_pixel_diagnostic(size_t x, size_t y, TopGroupSortBy sort_by) {
+        PixelDiagnosticInfo info;
+        LucidDiagPixel px{};
+        std::vector<LucidDiagGroup> g(64);
+        int n = lucid_cuda_diag_pixel(ctx_, (int)x, (int)y, sort_by == TopGroupSortBy::Mean, &px, g.data(), (int)g.size());
+        if (n < 0 || !px.valid) return info;
+        info.valid = true;
+        info.sample_count = px.sample_count;
+        info.variance = px.variance;
+        info.group_count = px.group_count;
+        info.outlier_count = px.outlier_count;
+        for (int c = 0; c < 3; ++c) info.mean_rgb[c] = px.mean_rgb[c];
+        for (int i = 0; i < n; ++i) {
+            const LucidDiagGroup& gi = g[i];
+            ExportedGroupInfo e;
+            e.pixel_x = x; e.pixel_y = y;
+            e.signature = signature_of(gi);
+            e.signature_heckbert = heckbert_of(gi);
+            e.object_ids.assign(gi.object_ids, gi.object_ids + gi.depth);
+            e.sample_count = gi.count;
+            e.mean_luminance = gi.mean_luminance;
+            e.variance_luminance = gi.total_variance;
+            for (int c = 0; c < 3; ++c) { e.mean_rgb[c] = gi.mean_rgb[c]; e.variance_rgb[c] = gi.variance_rgb[c]; }
+            e.depth = gi.depth; e.coarse_type = gi.coarse_type;
+            e.coarse_type_name = coarse_name(gi.coarse_type);
+            e.strategy_name = strategy_name(gi.strategy);
+            e.object_path = object_path_typed(e.object_ids, gi.light_type);
+            e.positions.push_back({cam_pos_[0], cam_pos_[1], cam_pos_[2]});
+            for (int k = 0; k < gi.depth; ++k) {
+                e.positions.push_back({gi.positions[k][0], gi.positions[k][1], gi.positions[k][2]});
+                e.normals.push_back({gi.normals[k][0], gi.normals[k][1], gi.normals[k][2]});
+            }
+            info.top_groups.push_back(std::move(e));
+        }
+        return info;
+    }
+
     // async accumulator (pybind_renderer.hpp:689-856)
     void start_async(int w, int h, int depth) {
         int rc = lucid_cuda_async_start(ctx_, w, h, depth);
@@ -141,6 +365,9 @@ private:
     std::string algorithm_ = "nee";
     std::vector<std::string> names_;
     int async_w_ = 0, async_h_ = 0;
+    float cam_pos_[3] = {0.0f, 0.0f, 0.0f};
+    int last_tile_w_ = 0, last_tile_h_ = 0;
+    PathRecordingConfig diag_cfg_;
 };
 
 std::string adapter_info() {
@@ -213,6 +440,29 @@ PYBIND11_MODULE(lucidrenderer, m) {
         .def("render_reset_async", &Renderer::reset_async, py::call_guard<py::gil_scoped_release>(),
              py::arg("width"), py::arg("height"), py::arg("max_depth") = 8)
         .def("is_render_async_running", &Renderer::async_running, py::call_guard<py::gil_scoped_release>())
+        .def("enable_diagnostics", &Renderer::enable_diagnostics, py::arg("config"),
+             "Enable diagnostic path recording with given configuration")
+        .def("disable_diagnostics", &Renderer::disable_diagnostics)
+        .def("is_diagnostics_enabled", &Renderer::is_diagnostics_enabled)
+        .def("clear_diagnostics", &Renderer::clear_diagnostics)
+        .def("get_diagnostic_stats", &Renderer::get_diagnostic_stats)
+        .def("get_diagnostic_variance_map",
+             [](Renderer& self) {
+                 std::vector<float> v = self.get_diagnostic_variance_map();
+                 py::array_t<float> arr(static_cast<py::ssize_t>(v.size()));
+                 if (!v.empty()) std::memcpy(arr.mutable_data(), v.data(), v.size() * sizeof(float));
+                 return arr;
+             },
+             "Per-pixel variance as a 1D numpy array (width * height)")
+        .def("export_diagnostic_json", &Renderer::export_diagnostic_json)
+        .def("get_top_variance_groups", &Renderer::get_top_variance_groups, py::arg("count") = 10)
+        .def("get_pixel_diagnostic",
+             [](Renderer& self, size_t x, size_t y, const std::string& sort_by) {
+                 return self.get_pixel_diagnostic(x, y, sort_by == "mean" ? TopGroupSortBy::Mean
+                                                                          : TopGroupSortBy::Variance);
+             },
+             py::arg("x"), py::arg("y"), py::arg("sort_by") = "variance",
+             "Diagnostic data of one pixel, groups sorted by 'variance' (default) or 'mean'")
         .def("is_scene_loaded", &Renderer::is_scene_loaded)
         .def("is_camera_set", &Renderer::is_camera_set)
         .def("get_algorithm", &Renderer::get_algorithm)
@@ -221,6 +471,72 @@ PYBIND11_MODULE(lucidrenderer, m) {
             return "<lucidrenderer.Renderer scene_loaded=" + std::string(r.is_scene_loaded() ? "True" : "False") +
                    " meshes=" + std::to_string(r.get_mesh_count()) + " algorithm='" + r.get_algorithm() + "'>";
         });
+    py::class_<PathRecordingConfig>(m, "PathRecordingConfig")
+        .def(py::init<>())
+        .def_readwrite("subsample_factor", &PathRecordingConfig::subsample_factor)
+        .def_readwrite("max_groups_per_pixel", &PathRecordingConfig::max_groups_per_pixel)
+        .def_readwrite("max_outliers_per_pixel", &PathRecordingConfig::max_outliers_per_pixel)
+        .def_readwrite("max_depth", &PathRecordingConfig::max_depth)
+        .def_readwrite("variance_threshold", &PathRecordingConfig::variance_threshold)
+        .def_readwrite("outlier_threshold", &PathRecordingConfig::outlier_threshold)
+        .def_static("minimal", &PathRecordingConfig::minimal)
+        .def_static("standard", &PathRecordingConfig::standard)
+        .def_static("detailed", &PathRecordingConfig::detailed)
+        .def("estimate_memory_bytes", &PathRecordingConfig::estimate_memory_bytes, py::arg("width"), py::arg("height"))
+        .def("__repr__", [](const PathRecordingConfig& c) {
+            return "<PathRecordingConfig subsample=" + std::to_string(c.subsample_factor) +
+                   " max_groups=" + std::to_string(c.max_groups_per_pixel) + ">";
+        });
+    py::class_<ExportedGroupInfo>(m, "ExportedGroupInfo")
+        .def(py::init<>())
+        .def_readonly("pixel_x", &ExportedGroupInfo::pixel_x)
+        .def_readonly("pixel_y", &ExportedGroupInfo::pixel_y)
+        .def_readonly("signature", &ExportedGroupInfo::signature)
+        .def_readonly("signature_heckbert", &ExportedGroupInfo::signature_heckbert)
+        .def_readonly("object_ids", &ExportedGroupInfo::object_ids)
+        .def_readonly("object_path", &ExportedGroupInfo::object_path)
+        .def_readonly("sample_count", &ExportedGroupInfo::sample_count)
+        .def_readonly("mean_luminance", &ExportedGroupInfo::mean_luminance)
+        .def_readonly("variance_luminance", &ExportedGroupInfo::variance_luminance)
+        .def_readonly("mean_rgb", &ExportedGroupInfo::mean_rgb)
+        .def_readonly("variance_rgb", &ExportedGroupInfo::variance_rgb)
+        .def_readonly("depth", &ExportedGroupInfo::depth)
+        .def_readonly("coarse_type", &ExportedGroupInfo::coarse_type)
+        .def_readonly("coarse_type_name", &ExportedGroupInfo::coarse_type_name)
+        .def_readonly("strategy_name", &ExportedGroupInfo::strategy_name)
+        .def_readonly("positions", &ExportedGroupInfo::positions, "camera first, then the path vertices")
+        .def_readonly("normals", &ExportedGroupInfo::normals)
+        .def("__repr__", [](const ExportedGroupInfo& g) {
+            return "<ExportedGroupInfo signature='" + g.signature + "' heckbert='" + g.signature_heckbert + "'" +
+                   " path='" + g.object_path + "'" + " strategy='" + g.strategy_name + "'" +
+                   " mean=" + std::to_string(g.mean_luminance) + " var=" + std::to_string(g.variance_luminance) +
+                   " positions=" + std::to_string(g.positions.size()) + ">";
+        });
+    py::enum_<TopGroupSortBy>(m, "TopGroupSortBy")
+        .value("Variance", TopGroupSortBy::Variance)
+        .value("Mean", TopGroupSortBy::Mean)
+        .export_values();
+    py::class_<PixelDiagnosticInfo>(m, "PixelDiagnosticInfo")
+        .def(py::init<>())
+        .def_readonly("valid", &PixelDiagnosticInfo::valid)
+        .def_readonly("sample_count", &PixelDiagnosticInfo::sample_count)
+        .def_readonly("variance", &PixelDiagnosticInfo::variance)
+        .def_readonly("group_count", &PixelDiagnosticInfo::group_count)
+        .def_readonly("outlier_count", &PixelDiagnosticInfo::outlier_count)
+        .def_readonly("mean_rgb", &PixelDiagnosticInfo::mean_rgb)
+        .def_readonly("top_groups", &PixelDiagnosticInfo::top_groups)
+        .def("__repr__", [](const PixelDiagnosticInfo& p) {
+            if (!p.valid) return std::string("<PixelDiagnosticInfo invalid>");
+            return "<PixelDiagnosticInfo samples=" + std::to_string(p.sample_count) +
+                   " variance=" + std::to_string(p.variance) + " groups=" + std::to_string(p.group_count) + ">";
+        });
+    py::class_<GlobalDiagnosticStats>(m, "GlobalDiagnosticStats")
+        .def(py::init<>())
+        .def_readonly("total_samples", &GlobalDiagnosticStats::total_samples)
+        .def_readonly("active_pixels", &GlobalDiagnosticStats::active_pixels)
+        .def_readonly("total_groups", &GlobalDiagnosticStats::total_groups)
+        .def_readonly("total_overflow", &GlobalDiagnosticStats::total_overflow)
+        .def_readonly("total_variance", &GlobalDiagnosticStats::total_variance);
     m.attr("__version__") = "1.0.0";
     m.attr("openmp_enabled") = false;
     m.attr("dawn_enabled") = false;

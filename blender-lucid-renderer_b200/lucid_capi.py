@@ -55,6 +55,26 @@ class RenderStats(ctypes.Structure):
                 ("kinds", KernelStat * 8)]
 
 
+class DiagConfig(ctypes.Structure):
+    _fields_ = [("subsample_factor", ctypes.c_int), ("max_groups_per_pixel", ctypes.c_int),
+                ("max_outliers_per_pixel", ctypes.c_int), ("max_depth", ctypes.c_int),
+                ("variance_threshold", ctypes.c_float), ("outlier_threshold", ctypes.c_float),
+                ("record_capacity", ctypes.c_longlong)]
+
+
+# LucidDiagGroup / LucidDiagPixel / LucidDiagStats (include/lucid_cuda.h).
+DIAG_GROUP_DTYPE = np.dtype([("hash", np.uint64), ("count", np.uint32), ("depth", np.uint8),
+                             ("coarse_type", np.uint8), ("light_type", np.uint8), ("strategy", np.uint8),
+                             ("mean_rgb", np.float32, 3), ("variance_rgb", np.float32, 3),
+                             ("mean_luminance", np.float32), ("total_variance", np.float32),
+                             ("object_ids", np.int32, 16), ("bsdf", np.uint8, 16), ("flags", np.uint8, 16),
+                             ("positions", np.float32, (16, 3)), ("normals", np.float32, (16, 3))], align=True)
+DIAG_PIXEL_DTYPE = np.dtype([("valid", np.int32), ("sample_count", np.uint32), ("group_count", np.uint32),
+                             ("outlier_count", np.uint32), ("overflow_count", np.uint32), ("variance", np.float32),
+                             ("mean_rgb", np.float32, 3)], align=True)
+DIAG_STATS_FIELDS = ("total_samples", "active_pixels", "total_groups", "total_overflow", "paths_recorded")
+
+
 # Every symbol include/lucid_cuda.h declares, with its ctypes signature.
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -81,6 +101,14 @@ SIGNATURES = {
     "lucid_cuda_async_reset": (_I, [_P, _I, _I, _I]),
     "lucid_cuda_async_stop": (_I, [_P]),
     "lucid_cuda_async_running": (_I, [_P]),
+    "lucid_cuda_diag_enable": (_I, [_P, ctypes.POINTER(DiagConfig)]),
+    "lucid_cuda_diag_disable": (_I, [_P]),
+    "lucid_cuda_diag_enabled": (_I, [_P]),
+    "lucid_cuda_diag_clear": (_I, [_P]),
+    "lucid_cuda_diag_stats": (_I, [_P, _P]),
+    "lucid_cuda_diag_pixel": (_I, [_P, _I, _I, _I, _P, _P, _I]),
+    "lucid_cuda_diag_variance_map": (_I, [_P, _P, ctypes.c_size_t]),
+    "lucid_cuda_diag_top_groups": (_I, [_P, _I, _I, _P, _P, _I]),
     "lucid_cuda_cancel": (_I, [_P]),
     "lucid_cuda_is_cancelled": (_I, [_P]),
     "lucid_cuda_reset_cancel": (_I, [_P]),
@@ -253,3 +281,41 @@ class Context:
 
     def is_cancelled(self) -> bool:
         return self.lib.lucid_cuda_is_cancelled(self.h) == 1
+
+    # ---- path diagnostics ----
+    def diag_enable(self, subsample=2, record_capacity=0):
+        cfg = DiagConfig(subsample, 16, 4, 16, 0.001, 3.0, record_capacity)
+        self._check(self.lib.lucid_cuda_diag_enable(self.h, ctypes.byref(cfg)))
+
+    def diag_disable(self):
+        self._check(self.lib.lucid_cuda_diag_disable(self.h))
+
+    def diag_enabled(self) -> bool:
+        return self.lib.lucid_cuda_diag_enabled(self.h) == 1
+
+    def diag_clear(self):
+        self._check(self.lib.lucid_cuda_diag_clear(self.h))
+
+    def diag_stats(self) -> list:
+        out = np.zeros(5, np.uint64)
+        self._check(self.lib.lucid_cuda_diag_stats(self.h, out.ctypes.data))
+        return out.tolist()
+
+    def diag_pixel(self, x, y, sort_by_mean=False, cap=32):
+        info = np.zeros(1, DIAG_PIXEL_DTYPE)
+        groups = np.zeros(cap, DIAG_GROUP_DTYPE)
+        n = self._check(self.lib.lucid_cuda_diag_pixel(self.h, x, y, int(sort_by_mean), info.ctypes.data,
+                                                       groups.ctypes.data, cap))
+        return info[0], groups[:n]
+
+    def diag_variance_map(self, w, h):
+        out = np.zeros(w * h, np.float32)
+        n = self._check(self.lib.lucid_cuda_diag_variance_map(self.h, out.ctypes.data, out.size))
+        return out[:n]
+
+    def diag_top_groups(self, n, by_mean=False):
+        groups = np.zeros(max(n, 1), DIAG_GROUP_DTYPE)
+        xy = np.zeros((max(n, 1), 2), np.int32)
+        m = self._check(self.lib.lucid_cuda_diag_top_groups(self.h, n, int(by_mean), groups.ctypes.data,
+                                                            xy.ctypes.data, groups.size))
+        return groups[:m], xy[:m]

@@ -178,6 +178,73 @@ int lucid_cuda_async_stop(LucidCudaCtx* ctx);
 /* 1 while the worker runs, else 0. */
 int lucid_cuda_async_running(LucidCudaCtx* ctx);
 
+/* ---- path diagnostics (DiagnosticFilm) ---------------------------------- */
+/* PathRecordingConfig (diagnostics/path_stats_config.hpp:24-105).  The film
+ * uses subsample_factor; the others are carried for the caller, as in the
+ * reference.  record_capacity bounds the device record buffer (completed
+ * paths per render call; 0 = 1,048,576). */
+typedef struct LucidDiagConfig {
+    int subsample_factor, max_groups_per_pixel, max_outliers_per_pixel, max_depth;
+    float variance_threshold, outlier_threshold;
+    long long record_capacity;
+} LucidDiagConfig;
+
+/* GlobalDiagnosticStats (diagnostic_film.hpp:124-154) + paths recorded. */
+typedef struct LucidDiagStats {
+    uint64_t total_samples, active_pixels, total_groups, total_overflow, paths_recorded;
+} LucidDiagStats;
+
+/* PixelDiagnosticInfo (pybind_renderer.hpp:971-981). */
+typedef struct LucidDiagPixel {
+    int32_t valid;
+    uint32_t sample_count, group_count, outlier_count, overflow_count;
+    float variance;
+    float mean_rgb[3];
+} LucidDiagPixel;
+
+/* One path group (PathGroup, path_stats.hpp:142-232): hash, Welford stats,
+ * vertex list (object id: mesh index, -1 environment, -(light+2) lights),
+ * BSDF class and flags per vertex, representative positions and normals. */
+typedef struct LucidDiagGroup {
+    uint64_t hash;
+    uint32_t count;
+    uint8_t depth, coarse_type, light_type, strategy;
+    float mean_rgb[3], variance_rgb[3];
+    float mean_luminance, total_variance;
+    int32_t object_ids[16];
+    uint8_t bsdf[16];
+    uint8_t flags[16];
+    float positions[16][3];
+    float normals[16][3];
+} LucidDiagGroup;
+
+/* Replaces PyRenderer::enable_diagnostics / disable_diagnostics /
+ * is_diagnostics_enabled / clear_diagnostics (pybind_renderer.hpp:893-937).
+ * While enabled, lucid_cuda_render uses the diagnostic integrators
+ * (path_tracer.hpp:880-1514: "simple", "mis", everything else as "nee") and
+ * rebuilds the film for each call.  config may be NULL (standard preset). */
+int lucid_cuda_diag_enable(LucidCudaCtx* ctx, const LucidDiagConfig* config);
+int lucid_cuda_diag_disable(LucidCudaCtx* ctx);
+int lucid_cuda_diag_enabled(LucidCudaCtx* ctx);
+int lucid_cuda_diag_clear(LucidCudaCtx* ctx);
+/* get_diagnostic_stats (pybind_renderer.hpp:939-946). */
+int lucid_cuda_diag_stats(LucidCudaCtx* ctx, LucidDiagStats* out);
+/* get_pixel_diagnostic (pybind_renderer.hpp:1008-1102): tile-local pixel
+ * (x, y); the cell's groups are sorted in place by variance (or by mean
+ * luminance when sort_by_mean) and up to cap are copied; returns the number
+ * copied. */
+int lucid_cuda_diag_pixel(LucidCudaCtx* ctx, int x, int y, int sort_by_mean, LucidDiagPixel* info,
+                          LucidDiagGroup* groups, int cap);
+/* get_diagnostic_variance_map (pybind_renderer.hpp:952-972): film width *
+ * height floats; returns the number written. */
+int lucid_cuda_diag_variance_map(LucidCudaCtx* ctx, float* out, size_t cap);
+/* get_top_variance_groups / top mean groups (diagnostic_film.hpp:160-222,
+ * diagnostic_export.hpp:94-105): the n groups of the whole film with the
+ * largest variance (groups with >= 2 samples) or mean luminance (>= 1),
+ * with the film position (x, y) of their cell in xy[2 * i].  Returns the
+ * number copied. */
+int lucid_cuda_diag_top_groups(LucidCudaCtx* ctx, int n, int by_mean, LucidDiagGroup* groups, int32_t* xy, int cap);
+
 /* ---- cancellation ---------------------------------------------------- */
 /* Replaces PyRenderer::cancel / is_cancelled / reset_cancel
  * (pybind_renderer.hpp:86-102).  Thread-safe. */

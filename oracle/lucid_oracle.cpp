@@ -436,3 +436,201 @@ float orc_lm(int fn, float x) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------ diagnostics
+#include "oracle_diag.hpp"
+
+namespace orc {
+struct DiagState {
+    DiagFilm film;
+    bool has = false;
+};
+static DiagState& diag_of(void* h) {
+    static std::map<void*, DiagState> m;
+    return m[h];
+}
+}  // namespace orc
+
+extern "C" {
+
+// One exported path group (layout shared with LucidDiagGroup in
+// include/lucid_cuda.h).
+struct OrcDiagGroup {
+    uint64_t hash;
+    uint32_t count;
+    uint8_t depth, coarse_type, light_type, strategy;
+    float mean_rgb[3], variance_rgb[3];
+    float mean_luminance, total_variance;
+    int32_t object_ids[16];
+    uint8_t bsdf[16];
+    uint8_t flags[16];
+    float positions[16][3];
+    float normals[16][3];
+};
+struct OrcDiagPixel {
+    int32_t valid;
+    uint32_t sample_count, group_count, outlier_count, overflow_count;
+    float variance;
+    float mean_rgb[3];
+};
+
+// render_tile with diagnostics enabled (pybind_renderer.hpp:205-316): the
+// diagnostic integrators render every pixel; completed paths go to a fresh
+// DiagnosticFilm(tile_w, tile_h, subsample) in the single-threaded loop order.
+int orc_render_tile_diag(void* h, int tile_x, int tile_y, int tile_w, int tile_h, int full_w, int full_h, int samples,
+                         int sample_offset, int max_depth, int subsample, float* out_rgba, int nthreads) {
+    Renderer* r = static_cast<Renderer*>(h);
+    size_t np = (size_t)tile_w * tile_h;
+    std::fill(out_rgba, out_rgba + np * 4, 0.0f);
+    if (!r->scene_loaded || !r->camera_set) return -1;
+    DiagState& ds = diag_of(h);
+    ds.film.init(tile_w, tile_h, subsample);
+    ds.has = true;
+    r->cam.aspect = (float)full_w / (float)full_h;
+    float scale = std::tan(r->cam.fov * 0.5f);
+    SceneLights sl = build_lights(r->scene);
+    DiagAlgo algo = diag_algo_from(algo_from_string(r->algorithm));
+    std::vector<std::vector<PTrace>> per_pixel(np);
+    std::vector<float> px(np * 4, 0.0f);
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nthreads)
+#endif
+    for (long long idx = 0; idx < (long long)np; ++idx) {
+        int py_ = (int)(idx / tile_w), px_ = (int)(idx % tile_w);
+        int gx = tile_x + px_, gy = tile_y + py_;
+        float ndc_x = (2.0f * ((float)gx + 0.5f) / (float)full_w - 1.0f) * r->cam.aspect;
+        float ndc_y = 1.0f - 2.0f * ((float)gy + 0.5f) / (float)full_h;
+        V3 wd = primary_dir(r->cam, ndc_x, ndc_y, scale);
+        RGB rad(0, 0, 0);
+        Recorder rec;
+        for (int si = 0; si < samples; ++si) {
+            Rng rng;
+            seed_xyz(rng, (uint32_t)gx, (uint32_t)gy, (uint32_t)(sample_offset + si));
+            Ray ray{r->cam.pos, wd};
+            if (samples > 1) {
+                float jx = (randf(rng) - 0.5f) / (float)full_w;
+                float jy = (randf(rng) - 0.5f) / (float)full_h;
+                ray.d = primary_dir(r->cam, ndc_x + jx, ndc_y + jy, scale);
+            }
+            rec.begin();
+            rad = rad + trace_diag(r->scene, sl, ray, max_depth, algo, rng, rec);
+            for (const PTrace& t : rec.completed) per_pixel[idx].push_back(t);
+        }
+        float* o = &px[(size_t)idx * 4];
+        o[0] = smax(rad.r * 1.0f, 0.0f); o[1] = smax(rad.g * 1.0f, 0.0f); o[2] = smax(rad.b * 1.0f, 0.0f); o[3] = 1.0f;
+    }
+    // film in the single-threaded loop order: 8x8 micro-tiles, pixels, samples, records
+    for (int my = 0; my < tile_h; my += 8)
+        for (int mx = 0; mx < tile_w; mx += 8)
+            for (int j = 0; j < std::min(8, tile_h - my); ++j)
+                for (int i = 0; i < std::min(8, tile_w - mx); ++i) {
+                    int pxx = mx + i, pyy = my + j;
+                    for (const PTrace& t : per_pixel[(size_t)pyy * tile_w + pxx]) ds.film.record(pxx, pyy, t);
+                }
+    for (int y = 0; y < tile_h; ++y)
+        std::copy(px.begin() + (size_t)y * tile_w * 4, px.begin() + (size_t)(y + 1) * tile_w * 4,
+                  out_rgba + (size_t)(tile_h - 1 - y) * tile_w * 4);
+    return 0;
+}
+
+// get_pixel_diagnostic (pybind_renderer.hpp:1008-1102): sorts the cell's
+// groups in place (by variance, or by mean when sort_by_mean) and exports them.
+int orc_diag_pixel(void* h, int x, int y, int sort_by_mean, OrcDiagPixel* info, OrcDiagGroup* groups, int cap) {
+    DiagState& ds = diag_of(h);
+    info->valid = 0;
+    if (!ds.has) return 0;
+    PixelData* p = const_cast<PixelData*>(ds.film.at(x, y));
+    if (!p) return 0;
+    if (sort_by_mean)
+        std::sort(p->groups, p->groups + p->num_groups,
+                  [](const PGroup& a, const PGroup& b) { return a.stats.mean_luminance() > b.stats.mean_luminance(); });
+    else
+        std::sort(p->groups, p->groups + p->num_groups,
+                  [](const PGroup& a, const PGroup& b) { return a.stats.total_variance() > b.stats.total_variance(); });
+    info->valid = 1;
+    info->sample_count = (uint32_t)p->total;
+    info->group_count = (uint32_t)p->num_groups;
+    info->outlier_count = (uint32_t)p->num_outliers;
+    info->overflow_count = (uint32_t)p->overflow;
+    info->variance = p->total_stats.total_variance();
+    info->mean_rgb[0] = p->total_stats.mean.r; info->mean_rgb[1] = p->total_stats.mean.g; info->mean_rgb[2] = p->total_stats.mean.b;
+    int n = (int)std::min<size_t>(p->num_groups, (size_t)cap);
+    for (int i = 0; i < n; ++i) {
+        const PGroup& g = p->groups[i];
+        OrcDiagGroup& o = groups[i];
+        std::memset(&o, 0, sizeof(o));
+        o.hash = g.hash; o.count = g.stats.count; o.depth = g.depth; o.coarse_type = g.coarse;
+        o.light_type = g.light_type; o.strategy = g.strategy;
+        o.mean_rgb[0] = g.stats.mean.r; o.mean_rgb[1] = g.stats.mean.g; o.mean_rgb[2] = g.stats.mean.b;
+        o.variance_rgb[0] = g.stats.variance.r; o.variance_rgb[1] = g.stats.variance.g; o.variance_rgb[2] = g.stats.variance.b;
+        o.mean_luminance = g.stats.mean_luminance();
+        o.total_variance = g.stats.total_variance();
+        for (int k = 0; k < g.depth; ++k) {
+            o.object_ids[k] = g.v[k].object_id; o.bsdf[k] = g.v[k].bsdf; o.flags[k] = g.v[k].flags;
+            o.positions[k][0] = g.pos[k].x; o.positions[k][1] = g.pos[k].y; o.positions[k][2] = g.pos[k].z;
+            o.normals[k][0] = g.nrm[k].x; o.normals[k][1] = g.nrm[k].y; o.normals[k][2] = g.nrm[k].z;
+        }
+    }
+    return n;
+}
+
+static void export_group(const PGroup& g, OrcDiagGroup& o) {
+    std::memset(&o, 0, sizeof(o));
+    o.hash = g.hash; o.count = g.stats.count; o.depth = g.depth; o.coarse_type = g.coarse;
+    o.light_type = g.light_type; o.strategy = g.strategy;
+    o.mean_rgb[0] = g.stats.mean.r; o.mean_rgb[1] = g.stats.mean.g; o.mean_rgb[2] = g.stats.mean.b;
+    o.variance_rgb[0] = g.stats.variance.r; o.variance_rgb[1] = g.stats.variance.g; o.variance_rgb[2] = g.stats.variance.b;
+    o.mean_luminance = g.stats.mean_luminance();
+    o.total_variance = g.stats.total_variance();
+    for (int k = 0; k < g.depth; ++k) {
+        o.object_ids[k] = g.v[k].object_id; o.bsdf[k] = g.v[k].bsdf; o.flags[k] = g.v[k].flags;
+        o.positions[k][0] = g.pos[k].x; o.positions[k][1] = g.pos[k].y; o.positions[k][2] = g.pos[k].z;
+        o.normals[k][0] = g.nrm[k].x; o.normals[k][1] = g.nrm[k].y; o.normals[k][2] = g.nrm[k].z;
+    }
+}
+
+// top_groups_by_variance / top_groups_by_mean (diagnostic_film.hpp:160-222):
+// every cell's groups (>= 2 samples for variance, >= 1 for mean) in cell
+// order, then std::partial_sort of the first n.
+int orc_diag_top_groups(void* h, int n, int by_mean, OrcDiagGroup* out, int32_t* xy, int cap) {
+    DiagState& ds = diag_of(h);
+    if (!ds.has) return 0;
+    struct Ref { size_t x, y; const PGroup* g; };
+    std::vector<Ref> all;
+    const DiagFilm& f = ds.film;
+    for (size_t sy = 0; sy < f.shh; ++sy)
+        for (size_t sx = 0; sx < f.sw; ++sx) {
+            const PixelData& px = f.px[sy * f.sw + sx];
+            for (size_t i = 0; i < px.num_groups; ++i)
+                if (px.groups[i].stats.count >= (by_mean ? 1u : 2u)) all.push_back({sx * f.sf, sy * f.sf, &px.groups[i]});
+        }
+    size_t limit = std::min((size_t)std::max(n, 0), all.size());
+    if (by_mean)
+        std::partial_sort(all.begin(), all.begin() + limit, all.end(), [](const Ref& a, const Ref& b) {
+            return a.g->stats.mean_luminance() > b.g->stats.mean_luminance();
+        });
+    else
+        std::partial_sort(all.begin(), all.begin() + limit, all.end(), [](const Ref& a, const Ref& b) {
+            return a.g->stats.total_variance() > b.g->stats.total_variance();
+        });
+    int m = (int)std::min(limit, (size_t)std::max(cap, 0));
+    for (int i = 0; i < m; ++i) {
+        export_group(*all[i].g, out[i]);
+        xy[2 * i] = (int32_t)all[i].x;
+        xy[2 * i + 1] = (int32_t)all[i].y;
+    }
+    return m;
+}
+
+// GlobalDiagnosticStats (diagnostic_film.hpp:124-154): total samples, active
+// pixels, groups, overflow, paths recorded.
+void orc_diag_stats(void* h, uint64_t* out5) {
+    DiagState& ds = diag_of(h);
+    uint64_t ts = 0, act = 0, grp = 0, ovf = 0;
+    for (const PixelData& p : ds.film.px)
+        if (p.total > 0) { ++act; ts += p.total; grp += p.num_groups; ovf += p.overflow; }
+    out5[0] = ts; out5[1] = act; out5[2] = grp; out5[3] = ovf; out5[4] = ds.film.recorded;
+}
+
+}  // extern "C"

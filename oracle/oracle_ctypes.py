@@ -50,6 +50,9 @@ def load() -> ctypes.CDLL:
             "orc_isect_aabb": (i, [p, p, p, p]), "orc_isect_sphere": (i, [p, p, p, f, p]),
             "orc_eval_bsdf": (None, [p, p, p, p, p, p]),
             "orc_sample_bsdf": (i, [p, p, p, f, f, f, u, u, u, p, p, p, p, p]), "orc_lm": (f, [i, f]),
+            "orc_render_tile_diag": (i, [p, i, i, i, i, i, i, i, i, i, i, p, i]),
+            "orc_diag_pixel": (i, [p, i, i, i, p, p, i]), "orc_diag_stats": (None, [p, p]),
+            "orc_diag_top_groups": (i, [p, i, i, p, p, i]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -58,6 +61,18 @@ def load() -> ctypes.CDLL:
         assert lib.orc_sizeof_record() == RECORD_DTYPE.itemsize
         _lib = lib
     return _lib
+
+
+# Same layouts as LucidDiagGroup / LucidDiagPixel (include/lucid_cuda.h).
+DIAG_GROUP_DTYPE = np.dtype([("hash", np.uint64), ("count", np.uint32), ("depth", np.uint8),
+                             ("coarse_type", np.uint8), ("light_type", np.uint8), ("strategy", np.uint8),
+                             ("mean_rgb", np.float32, 3), ("variance_rgb", np.float32, 3),
+                             ("mean_luminance", np.float32), ("total_variance", np.float32),
+                             ("object_ids", np.int32, 16), ("bsdf", np.uint8, 16), ("flags", np.uint8, 16),
+                             ("positions", np.float32, (16, 3)), ("normals", np.float32, (16, 3))], align=True)
+DIAG_PIXEL_DTYPE = np.dtype([("valid", np.int32), ("sample_count", np.uint32), ("group_count", np.uint32),
+                             ("outlier_count", np.uint32), ("overflow_count", np.uint32), ("variance", np.float32),
+                             ("mean_rgb", np.float32, 3)], align=True)
 
 
 def fptr(a: np.ndarray):
@@ -107,6 +122,32 @@ class Oracle:
         img = np.zeros((tile_h, tile_w, 4), np.float32)
         self.lib.orc_render_debug(self.h, tile_x, tile_y, tile_w, tile_h, full_w, full_h, mode, fptr(img))
         return img
+
+    def render_diag(self, tile_w, tile_h, full_w=None, full_h=None, samples=1, sample_offset=0, max_depth=8,
+                    tile_x=0, tile_y=0, subsample=2, threads=0):
+        full_w = tile_w if full_w is None else full_w
+        full_h = tile_h if full_h is None else full_h
+        img = np.zeros((tile_h, tile_w, 4), np.float32)
+        rc = self.lib.orc_render_tile_diag(self.h, tile_x, tile_y, tile_w, tile_h, full_w, full_h, samples,
+                                           sample_offset, max_depth, subsample, fptr(img), threads)
+        return img, rc
+
+    def diag_pixel(self, x, y, sort_by_mean=False, cap=32):
+        info = np.zeros(1, DIAG_PIXEL_DTYPE)
+        groups = np.zeros(cap, DIAG_GROUP_DTYPE)
+        n = self.lib.orc_diag_pixel(self.h, x, y, int(sort_by_mean), fptr(info), fptr(groups), cap)
+        return info[0], groups[:n]
+
+    def diag_top_groups(self, n, by_mean=False):
+        groups = np.zeros(max(n, 1), DIAG_GROUP_DTYPE)
+        xy = np.zeros((max(n, 1), 2), np.int32)
+        m = self.lib.orc_diag_top_groups(self.h, n, int(by_mean), fptr(groups), fptr(xy), groups.size)
+        return groups[:m], xy[:m]
+
+    def diag_stats(self):
+        out = np.zeros(5, np.uint64)
+        self.lib.orc_diag_stats(self.h, fptr(out))
+        return out.tolist()
 
     def scene_stats(self):
         out = np.zeros(6, np.int32)
