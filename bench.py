@@ -294,7 +294,9 @@ def main():
             "e2e": {"value": e2e_value, "unit": "samples/s", "h2d_bytes_per_step": 40,
                     "d2h_bytes_per_step": W * H * 16},
             "roofline": {"bound": "hbm", "kernel": top[0], "achieved": achieved, "peak": peak,
-                         "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic},
+                         "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "dram_gbs": None if traffic is None else
+                         traffic / (top[1]["total_ms"] / max(1, top[1]["launches"]) / 1000.0) / 1e9},
             "kernels": {k: {"launches": v["launches"], "ms": round(v["total_ms"], 3), "units": v["units"],
                             "share": round(v["total_ms"] / sum(x["total_ms"] for x in kern.values()), 4)}
                         for k, v in kern.items()},

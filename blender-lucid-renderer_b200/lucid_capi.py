@@ -180,6 +180,12 @@ class Context:
             raise LucidError(rc, self.lib.lucid_cuda_last_error(self.h).decode())
         return rc
 
+    def _count(self, rc: int) -> int:
+        """Calls that return a count on success and a negative status on failure."""
+        if rc < 0:
+            raise LucidError(rc, self.lib.lucid_cuda_last_error(self.h).decode())
+        return rc
+
     def load_scene_json(self, text: str) -> None:
         b = text.encode()
         self._check(self.lib.lucid_cuda_load_scene_json(self.h, b, len(b)))
@@ -304,18 +310,18 @@ class Context:
     def diag_pixel(self, x, y, sort_by_mean=False, cap=32):
         info = np.zeros(1, DIAG_PIXEL_DTYPE)
         groups = np.zeros(cap, DIAG_GROUP_DTYPE)
-        n = self._check(self.lib.lucid_cuda_diag_pixel(self.h, x, y, int(sort_by_mean), info.ctypes.data,
+        n = self._count(self.lib.lucid_cuda_diag_pixel(self.h, x, y, int(sort_by_mean), info.ctypes.data,
                                                        groups.ctypes.data, cap))
         return info[0], groups[:n]
 
     def diag_variance_map(self, w, h):
         out = np.zeros(w * h, np.float32)
-        n = self._check(self.lib.lucid_cuda_diag_variance_map(self.h, out.ctypes.data, out.size))
+        n = self._count(self.lib.lucid_cuda_diag_variance_map(self.h, out.ctypes.data, out.size))
         return out[:n]
 
     def diag_top_groups(self, n, by_mean=False):
         groups = np.zeros(max(n, 1), DIAG_GROUP_DTYPE)
         xy = np.zeros((max(n, 1), 2), np.int32)
-        m = self._check(self.lib.lucid_cuda_diag_top_groups(self.h, n, int(by_mean), groups.ctypes.data,
+        m = self._count(self.lib.lucid_cuda_diag_top_groups(self.h, n, int(by_mean), groups.ctypes.data,
                                                             xy.ctypes.data, groups.size))
         return groups[:m], xy[:m]
