@@ -156,6 +156,29 @@ def cpu_baseline(js: str, cam, steps: int = 1):
     return vals, threads, sample
 
 
+def c1_quality(device: int) -> dict:
+    """Cornell box (256x256, mis, depth 8): a 16-spp render's relMSE against
+    an independent FP64-accumulated 4096-spp GPU reference, and the rate."""
+    import lucid_capi
+    import lucid_quality as lq
+    import lucid_scenes as ls
+    scene, cam = ls.cornell_box()
+    c = lucid_capi.Context(device)
+    c.load_scene_json(ls.to_json(scene))
+    c.set_camera(*cam)
+    c.set_algorithm("mis")
+    t0 = time.perf_counter()
+    ref = lq.render_reference(c, 256, 256, spp=lq.REFERENCE_SPP, max_depth=8, sample_offset=1 << 20)
+    ref_s = time.perf_counter() - t0
+    c.render(256, 256, 256, 256, 16, 0, 8)   # warm
+    img, _, _ = c.render(256, 256, 256, 256, 16, 0, 8, profile=True)
+    ms = c.stats()["total_ms"]
+    c.close()
+    return {"scene": "cornell 256x256, mis, depth 8", "spp": 16, "relmse": lq.relmse(lq.mean_image(img, 16), ref),
+            "reference": f"FP64-accumulated {lq.REFERENCE_SPP} spp on the GPU (sample offset 2^20)",
+            "reference_s": round(ref_s, 3), "samples_per_s": 256 * 256 * 16 / (ms / 1000.0)}
+
+
 def run_reference(args, rank: int):
     if rank != 0:
         return 0
@@ -183,6 +206,7 @@ def main():
     ap.add_argument("--impl", default="lucid", choices=["lucid", "reference"])
     ap.add_argument("--cache", default="/tmp/lucid_bench")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-quality", action="store_true", help="skip the Cornell relMSE measurement")
     ap.add_argument("--width", type=int, default=W, help="smaller frames for profiling captures")
     ap.add_argument("--height", type=int, default=H)
     ap.add_argument("--spp", type=int, default=SPP)
@@ -276,6 +300,8 @@ def main():
     traffic = None if tpu is None else tpu * top[1]["units"] / max(1, top[1]["launches"])
     mrays = (segs + shadows) / (per_step_ms[-1] / 1000.0) / 1e6
 
+    quality = c1_quality(local_rank) if rank == 0 and not args.no_quality else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         vals, threads, sample = cpu_baseline(js, cam, steps=1)
@@ -301,7 +327,7 @@ def main():
                             "share": round(v["total_ms"] / sum(x["total_ms"] for x in kern.values()), 4)}
                         for k, v in kern.items()},
             "mrays_per_s": mrays, "segments_per_step": segs, "shadow_rays_per_step": shadows,
-            "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": cpu,
+            "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": cpu, "quality": quality,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -161,6 +161,11 @@ int lucid_cuda_async_running(LucidCudaCtx* ctx) {
     return guarded(ctx, [&](lucid::Engine& e) { return e.async_running() ? 1 : 0; });
 }
 
+int lucid_cuda_render_f64(LucidCudaCtx* ctx, const LucidRenderParams* params, double* out_rgba) {
+    if (!params || !out_rgba) return LUCID_ERR_INVALID;
+    return guarded(ctx, [&](lucid::Engine& e) { return e.render_f64(*params, out_rgba); });
+}
+
 int lucid_cuda_diag_enable(LucidCudaCtx* ctx, const LucidDiagConfig* config) {
     return guarded(ctx, [&](lucid::Engine& e) { return e.diag_enable(config); });
 }

@@ -109,13 +109,16 @@ struct PathPool {
     DBuf<float4> film;
     DBuf<float4> out;
     size_t film_n = 0;
+    DBuf<double> film64, out64;   // FP64 accumulation (converged references)
+    size_t film64_n = 0;
     PathView view{};
     void release() {
         rng.release(); ray_o.release(); ray_d.release(); thr.release(); rad.release(); hit.release();
         sh_o.release(); sh_d.release(); sh_c.release(); lhit.release(); q0.release(); q1.release(); qs.release();
         counters.release(); errors.release(); rec_prim.release(); rec_cnt.release(); rec_hash.release();
-        film.release(); out.release();
+        film.release(); out.release(); film64.release(); out64.release();
         film_n = 0;
+        film64_n = 0;
         cap = 0;
     }
 };
@@ -659,6 +662,30 @@ __global__ void k_film(int npix, int spw, const float4* rad, float4* film) {
         a.x = a.x + r.x; a.y = a.y + r.y; a.z = a.z + r.z;
     }
     film[p] = a;
+}
+
+// FP64 accumulation for converged references: the same per-sample FP32
+// radiance, summed per pixel in double in sample order.
+__global__ void k_film_f64(int npix, int spw, const float4* rad, double* film) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npix) return;
+    double a0 = film[3 * (size_t)p], a1 = film[3 * (size_t)p + 1], a2 = film[3 * (size_t)p + 2];
+    for (int s = 0; s < spw; ++s) {
+        float4 r = rad[(size_t)s * npix + p];
+        a0 += (double)r.x; a1 += (double)r.y; a2 += (double)r.z;
+    }
+    film[3 * (size_t)p] = a0; film[3 * (size_t)p + 1] = a1; film[3 * (size_t)p + 2] = a2;
+}
+__global__ void k_output_f64(int tw, int th, const double* film, double* out) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= tw * th) return;
+    int x = p % tw, y = p / tw;
+    double* o = out + ((size_t)(th - 1 - y) * tw + x) * 4;
+    for (int c = 0; c < 3; ++c) {
+        double v = film[3 * (size_t)p + c];
+        o[c] = (v < 0.0) ? 0.0 : v;
+    }
+    o[3] = 1.0;
 }
 
 // Camera sensitivity (EV 0 => 1), clamp >= 0 keeping NaN, alpha 1, Y flip
@@ -1478,6 +1505,12 @@ int Engine::render(const LucidRenderParams& p, float* out_host, LucidSampleRecor
     return render_impl(p, out_host, recs, out_device, nullptr, false);
 }
 
+int Engine::render_f64(const LucidRenderParams& p, double* out_host) {
+    std::lock_guard<std::mutex> lk(gpu_mu_);
+    if (diag_enabled_) return fail(LUCID_ERR_INVALID, "FP64 references are not rendered while diagnostics are enabled");
+    return render_impl(p, nullptr, nullptr, nullptr, nullptr, false, out_host);
+}
+
 // ---------------------------------------------------------------- path diagnostics (host)
 constexpr long long kDiagWavePaths = 1LL << 20;   // paths per diagnostic wave
 
@@ -1650,12 +1683,13 @@ __global__ void k_accumulate(int npix, const float4* film, float4* acc) {
 }
 
 int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSampleRecord* recs, float* out_device,
-                        void* accumulate, bool from_async) {
+                        void* accumulate, bool from_async, double* out_f64) {
     if (!from_async) reset_cancel();
     if (p.tile_w <= 0 || p.tile_h <= 0 || p.full_w <= 0 || p.full_h <= 0)
         return fail(LUCID_ERR_INVALID, "tile and image sizes must be positive");
     size_t np = (size_t)p.tile_w * p.tile_h;
     if (out_host) std::fill(out_host, out_host + np * 4, 0.0f);
+    if (out_f64) std::fill(out_f64, out_f64 + np * 4, 0.0);
     if (!scene_loaded_ || !camera_set_) return fail(LUCID_ERR_NO_SCENE, "scene or camera not set");
     CK(cudaSetDevice(device_));
     if (p.samples <= 0) return fail(LUCID_ERR_INVALID, "samples must be >= 1");
@@ -1677,6 +1711,14 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
     }
     CK(cudaMemsetAsync(P.film.p, 0, np * sizeof(float4), st));
     CK(cudaMemsetAsync(P.errors.p, 0, 4 * sizeof(int), st));
+    if (out_f64) {
+        if (P.film64_n < np) {
+            CK(P.film64.alloc(np * 3));
+            CK(P.out64.alloc(np * 4));
+            P.film64_n = np;
+        }
+        CK(cudaMemsetAsync(P.film64.p, 0, np * 3 * sizeof(double), st));
+    }
     DBuf<LucidSampleRecord> d_recs;
     if (records) CK(d_recs.alloc(np * (size_t)p.samples));
 
@@ -1756,7 +1798,10 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
             ev_end(e);
         }
         e = ev_begin(K_FILM, 0);
-        k_film<<<(f.npix + 255) / 256, 256, 0, st>>>(f.npix, this_spw, P.rad.p, P.film.p);
+        if (out_f64)
+            k_film_f64<<<(f.npix + 255) / 256, 256, 0, st>>>(f.npix, this_spw, P.rad.p, P.film64.p);
+        else
+            k_film<<<(f.npix + 255) / 256, 256, 0, st>>>(f.npix, this_spw, P.rad.p, P.film.p);
         ev_end(e);
         if (records) k_records<<<(f.n_wave + 255) / 256, 256, 0, st>>>(f, P.view, d_recs.p);
         CK(cudaGetLastError());
@@ -1780,6 +1825,8 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
     int np_i = (int)np;
     if (accumulate)
         k_accumulate<<<(np_i + 255) / 256, 256, 0, st>>>(np_i, P.film.p, (float4*)accumulate);
+    else if (out_f64)
+        k_output_f64<<<(np_i + 255) / 256, 256, 0, st>>>(p.tile_w, p.tile_h, P.film64.p, P.out64.p);
     else
         k_output<<<(np_i + 255) / 256, 256, 0, st>>>(p.tile_w, p.tile_h, P.film.p,
                                                      out_device ? (float4*)out_device : P.out.p);
@@ -1788,6 +1835,8 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
     CK(cudaMemcpyAsync(herr, P.errors.p, sizeof(herr), cudaMemcpyDeviceToHost, st));
     if (out_host && !out_device)
         CK(cudaMemcpyAsync(out_host, P.out.p, np * sizeof(float4), cudaMemcpyDeviceToHost, st));
+    if (out_f64)
+        CK(cudaMemcpyAsync(out_f64, P.out64.p, np * 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
     if (records)
         CK(cudaMemcpyAsync(recs, d_recs.p, np * (size_t)p.samples * sizeof(LucidSampleRecord), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));

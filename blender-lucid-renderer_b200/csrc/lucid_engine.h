@@ -28,6 +28,8 @@ public:
                    float fov_deg);
     int set_algorithm(const char* name);
     int render(const LucidRenderParams& p, float* out_host, LucidSampleRecord* recs, float* out_device);
+    // Converged references: the per-pixel sum of the samples in FP64.
+    int render_f64(const LucidRenderParams& p, double* out_host);
     // Progressive accumulator (PyRenderer render_*_async, pybind_renderer.hpp:689-856).
     int async_start(int w, int h, int max_depth);
     int async_poll(int* samples, float* out, size_t cap_floats);
@@ -60,7 +62,7 @@ public:
 
 private:
     int render_impl(const LucidRenderParams& p, float* out_host, LucidSampleRecord* recs, float* out_device,
-                    void* accumulate, bool from_async);
+                    void* accumulate, bool from_async, double* out_f64 = nullptr);
     int render_diag_impl(const LucidRenderParams& p, float* out_host, float* out_device);
     void async_worker();
     int ensure_pool(long long paths, bool records);

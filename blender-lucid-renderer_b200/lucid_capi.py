@@ -101,6 +101,7 @@ SIGNATURES = {
     "lucid_cuda_async_reset": (_I, [_P, _I, _I, _I]),
     "lucid_cuda_async_stop": (_I, [_P]),
     "lucid_cuda_async_running": (_I, [_P]),
+    "lucid_cuda_render_f64": (_I, [_P, ctypes.POINTER(RenderParams), _P]),
     "lucid_cuda_diag_enable": (_I, [_P, ctypes.POINTER(DiagConfig)]),
     "lucid_cuda_diag_disable": (_I, [_P]),
     "lucid_cuda_diag_enabled": (_I, [_P]),
@@ -287,6 +288,17 @@ class Context:
 
     def is_cancelled(self) -> bool:
         return self.lib.lucid_cuda_is_cancelled(self.h) == 1
+
+    def render_f64(self, tile_w, tile_h, full_w=None, full_h=None, samples=1, sample_offset=0, max_depth=8,
+                   tile_x=0, tile_y=0):
+        """Per-pixel FP64 sum of the samples' FP32 radiance (a converged reference
+        is this divided by samples)."""
+        full_w = tile_w if full_w is None else full_w
+        full_h = tile_h if full_h is None else full_h
+        p = RenderParams(tile_x, tile_y, tile_w, tile_h, full_w, full_h, samples, sample_offset, max_depth, 0)
+        img = np.zeros((tile_h, tile_w, 4), np.float64)
+        self._check(self.lib.lucid_cuda_render_f64(self.h, ctypes.byref(p), img.ctypes.data))
+        return img
 
     # ---- path diagnostics ----
     def diag_enable(self, subsample=2, record_capacity=0):

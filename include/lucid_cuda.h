@@ -178,6 +178,14 @@ int lucid_cuda_async_stop(LucidCudaCtx* ctx);
 /* 1 while the worker runs, else 0. */
 int lucid_cuda_async_running(LucidCudaCtx* ctx);
 
+/* ---- converged references ---------------------------------------------- */
+/* No reference counterpart (the reference sums in FP32 only).  Renders like
+ * lucid_cuda_render but sums each pixel's per-sample FP32 radiance in FP64,
+ * in sample order, for the 4096-spp references that relMSE is measured
+ * against.  out_rgba: tile_w * tile_h * 4 doubles, clamp >= 0, alpha 1,
+ * Y-flipped (the layout of lucid_cuda_render). */
+int lucid_cuda_render_f64(LucidCudaCtx* ctx, const LucidRenderParams* params, double* out_rgba);
+
 /* ---- path diagnostics (DiagnosticFilm) ---------------------------------- */
 /* PathRecordingConfig (diagnostics/path_stats_config.hpp:24-105).  The film
  * uses subsample_factor; the others are carried for the caller, as in the

@@ -309,6 +309,35 @@ int orc_render_tile(void* h, int tile_x, int tile_y, int tile_w, int tile_h, int
     return 0;
 }
 
+// FP64-accumulated render for converged references: every sample's FP32
+// radiance (the same values render_tile sums in FP32) is summed per pixel in
+// double, in sample order; clamp >= 0, alpha 1, Y-flipped like render_tile.
+int orc_render_tile_f64(void* h, int tile_x, int tile_y, int tile_w, int tile_h, int full_w, int full_h, int samples,
+                        int sample_offset, int max_depth, double* out_rgba, int nthreads) {
+    Renderer* r = static_cast<Renderer*>(h);
+    size_t np = (size_t)tile_w * tile_h;
+    std::fill(out_rgba, out_rgba + np * 4, 0.0);
+    if (!r->scene_loaded || !r->camera_set) return -1;
+    r->cam.aspect = (float)full_w / (float)full_h;
+    float scale = std::tan(r->cam.fov * 0.5f);
+    SceneLights sl = build_lights(r->scene);
+    Algo algo = algo_from_string(r->algorithm);
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nthreads)
+#endif
+    for (long long idx = 0; idx < (long long)np; ++idx) {
+        int py_ = (int)(idx / tile_w), px_ = (int)(idx % tile_w);
+        double acc[3] = {0.0, 0.0, 0.0};
+        render_pixel(r->scene, sl, r->cam, tile_x + px_, tile_y + py_, full_w, full_h, samples, sample_offset,
+                     max_depth, algo, scale, nullptr, acc);
+        double* o = out_rgba + ((size_t)(tile_h - 1 - py_) * tile_w + px_) * 4;
+        for (int c = 0; c < 3; ++c) o[c] = (acc[c] < 0.0) ? 0.0 : acc[c];
+        o[3] = 1.0;
+    }
+    return 0;
+}
+
 // render_debug (pybind_renderer.hpp:371-439): mode 0 normal, 1 albedo, 2 emission.
 int orc_render_debug(void* h, int tile_x, int tile_y, int tile_w, int tile_h, int full_w, int full_h, int mode,
                      float* out) {

@@ -1380,7 +1380,7 @@ inline V3 primary_dir(const Camera& c, float ndc_x, float ndc_y, float scale) {
 // exposure/clamp/Y-flip, returning the radiance sum over the call's samples.
 inline RGB render_pixel(const Scene& s, const SceneLights& sl, const Camera& cam, int gx, int gy, int full_w,
                         int full_h, int samples, int sample_offset, int max_depth, Algo algo, float scale,
-                        SampleRec* recs) {
+                        SampleRec* recs, double* acc64 = nullptr) {
     float ndc_x = (2.0f * ((float)gx + 0.5f) / (float)full_w - 1.0f) * cam.aspect;
     float ndc_y = 1.0f - 2.0f * ((float)gy + 0.5f) / (float)full_h;
     V3 wd = primary_dir(cam, ndc_x, ndc_y, scale);
@@ -1399,6 +1399,7 @@ inline RGB render_pixel(const Scene& s, const SceneLights& sl, const Camera& cam
         RGB sr = trace(s, sl, r, max_depth, algo, rng, rec);
         if (rec) { rec->rgb[0] = sr.r; rec->rgb[1] = sr.g; rec->rgb[2] = sr.b; }
         rad = rad + sr;
+        if (acc64) { acc64[0] += (double)sr.r; acc64[1] += (double)sr.g; acc64[2] += (double)sr.b; }
     }
     return rad;
 }

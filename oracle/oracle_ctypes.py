@@ -53,6 +53,7 @@ def load() -> ctypes.CDLL:
             "orc_render_tile_diag": (i, [p, i, i, i, i, i, i, i, i, i, i, p, i]),
             "orc_diag_pixel": (i, [p, i, i, i, p, p, i]), "orc_diag_stats": (None, [p, p]),
             "orc_diag_top_groups": (i, [p, i, i, p, p, i]),
+            "orc_render_tile_f64": (i, [p, i, i, i, i, i, i, i, i, i, p, i]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -115,6 +116,16 @@ class Oracle:
                                       sample_offset, max_depth, fptr(img),
                                       fptr(recs) if recs is not None else None, threads)
         return img, recs, rc
+
+    def render_f64(self, tile_w, tile_h, full_w=None, full_h=None, samples=1, sample_offset=0, max_depth=8,
+                   tile_x=0, tile_y=0, threads=0):
+        """Per-pixel FP64 sum of the samples' FP32 radiance (clamp >= 0, Y-flipped)."""
+        full_w = tile_w if full_w is None else full_w
+        full_h = tile_h if full_h is None else full_h
+        img = np.zeros((tile_h, tile_w, 4), np.float64)
+        rc = self.lib.orc_render_tile_f64(self.h, tile_x, tile_y, tile_w, tile_h, full_w, full_h, samples,
+                                          sample_offset, max_depth, fptr(img), threads)
+        return img, rc
 
     def render_debug(self, mode: int, tile_w, tile_h, full_w=None, full_h=None, tile_x=0, tile_y=0):
         full_w = tile_w if full_w is None else full_w
