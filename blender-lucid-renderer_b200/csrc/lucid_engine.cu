@@ -15,6 +15,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <chrono>
 #include <cub/cub.cuh>
@@ -1158,6 +1160,129 @@ __global__ void k_flatten(const float4* verts, const int* sorted_ids, int n, con
     nodes[i] = nd;
 }
 
+// ---------------------------------------------------------------- PLOC build
+// Parallel locally-ordered clustering (Meister & Bittner, "Parallel Locally-
+// Ordered Clustering for Bounding Volume Hierarchy Construction", IEEE TVCG
+// 2018): clusters start as the Morton-sorted triangles; each round every
+// cluster finds the neighbour within +-kPlocRadius positions whose merged box
+// has the smallest surface area, mutual nearest neighbours merge into a new
+// node, and the cluster array is compacted in order.  Ties prefer the lower
+// index, which totally orders candidate pairs, so the best pair of a round
+// is always mutual and every round merges at least one pair.  Node ids follow
+// creation order (root last); a top-down pass then gives every subtree a
+// contiguous range of triangle slots so that k_flatten can collapse small
+// subtrees into leaves exactly as for the Karras tree.
+constexpr int kPlocRadius = 16;
+constexpr int kPlocBlock = 256;
+
+struct PlocBox { float lo[3], hi[3]; };
+
+LD float ploc_area(const float* a, const float* b) {
+    float dx = fmaxf(a[3], b[3]) - fminf(a[0], b[0]);
+    float dy = fmaxf(a[4], b[4]) - fminf(a[1], b[1]);
+    float dz = fmaxf(a[5], b[5]) - fminf(a[2], b[2]);
+    return dx * dy + dy * dz + dz * dx;
+}
+
+// Initial clusters: leaf i (Morton order) with its triangle's box.
+__global__ void k_ploc_init(const float4* verts, const int* sorted_ids, int n, int* cl, float* cbox, int* cnt_leaf) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    cl[i] = ~i;
+    leaf_box(verts, sorted_ids[i], cbox + 6 * (size_t)i);
+    cnt_leaf[i] = 1;
+}
+
+// Nearest neighbour of every cluster within the window (boxes staged in
+// shared memory with a halo of kPlocRadius on both sides).
+__global__ void __launch_bounds__(kPlocBlock) k_ploc_nn(const float* cbox, int count, int* nn) {
+    __shared__ float sb[(kPlocBlock + 2 * kPlocRadius) * 6];
+    const int b0 = blockIdx.x * kPlocBlock;
+    for (int t = threadIdx.x; t < (kPlocBlock + 2 * kPlocRadius) * 6; t += kPlocBlock) {
+        int j = b0 - kPlocRadius + t / 6;
+        sb[t] = (j >= 0 && j < count) ? cbox[6 * (size_t)j + t % 6] : 0.0f;
+    }
+    __syncthreads();
+    int i = b0 + threadIdx.x;
+    if (i >= count) return;
+    const float* bi = sb + 6 * (threadIdx.x + kPlocRadius);
+    float best = 3.0e38f;
+    int bj = -1;
+    int lo = max(0, i - kPlocRadius), hi = min(count - 1, i + kPlocRadius);
+    for (int j = lo; j <= hi; ++j) {
+        if (j == i) continue;
+        float d = ploc_area(bi, sb + 6 * (j - b0 + kPlocRadius));
+        if (d < best) { best = d; bj = j; }   // ascending j: ties keep the lower index
+    }
+    nn[i] = bj;
+}
+
+// flag[i]: 1 = creates a node (mutual pair, lower index), keep[i]: cluster
+// survives (unmerged, or the lower index of a merged pair).
+__global__ void k_ploc_flags(const int* nn, int count, int* create, int* keep) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    int j = nn[i];
+    bool mutual = j >= 0 && nn[j] == i;
+    create[i] = (mutual && i < j) ? 1 : 0;
+    keep[i] = (!mutual || i < j) ? 1 : 0;
+}
+
+// Merges (node id = base + exclusive scan of create) and compacts the
+// clusters (position = exclusive scan of keep) into the other buffers.
+__global__ void k_ploc_merge(const int* cl, const float* cbox, const int* nn, const int* create, const int* keep,
+                             const int* create_pos, const int* keep_pos, int count, int base, int2* child,
+                             float* nbox, int* cnt_node, const int* cnt_leaf, int* cl_out, float* cbox_out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count || !keep[i]) return;
+    int o = keep_pos[i];
+    if (!create[i]) {
+        cl_out[o] = cl[i];
+        for (int q = 0; q < 6; ++q) cbox_out[6 * (size_t)o + q] = cbox[6 * (size_t)i + q];
+        return;
+    }
+    int j = nn[i];
+    int id = base + create_pos[i];
+    int a = cl[i], b = cl[j];
+    child[id] = make_int2(a, b);
+    float m[6];
+    for (int q = 0; q < 3; ++q) {
+        m[q] = fminf(cbox[6 * (size_t)i + q], cbox[6 * (size_t)j + q]);
+        m[3 + q] = fmaxf(cbox[6 * (size_t)i + 3 + q], cbox[6 * (size_t)j + 3 + q]);
+    }
+    for (int q = 0; q < 6; ++q) { nbox[6 * (size_t)id + q] = m[q]; cbox_out[6 * (size_t)o + q] = m[q]; }
+    cnt_node[id] = (a >= 0 ? cnt_node[a] : cnt_leaf[~a]) + (b >= 0 ? cnt_node[b] : cnt_leaf[~b]);
+    cl_out[o] = id;
+}
+
+// Top-down slot assignment for the nodes created in one round (processed in
+// reverse creation order, so a node's own offset is already known).
+__global__ void k_ploc_offsets(const int2* child, const int* cnt_node, int base, int m, int* off_node, int* leaf_pos) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    int id = base + k;
+    int2 c = child[id];
+    int o = off_node[id];
+    int ca = c.x >= 0 ? cnt_node[c.x] : 1;
+    if (c.x >= 0) off_node[c.x] = o; else leaf_pos[~c.x] = o;
+    if (c.y >= 0) off_node[c.y] = o + ca; else leaf_pos[~c.y] = o + ca;
+}
+
+// Children re-coded to triangle slots, subtree slot ranges, triangle ids in
+// slot order.
+__global__ void k_ploc_finish(const int* sorted_ids, const int* leaf_pos, int n, int2* child, const int* off_node,
+                              const int* cnt_node, int2* range, int* slot_ids) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) slot_ids[leaf_pos[i]] = sorted_ids[i];
+    if (i < n - 1) {
+        int2 c = child[i];
+        if (c.x < 0) c.x = ~leaf_pos[~c.x];
+        if (c.y < 0) c.y = ~leaf_pos[~c.y];
+        child[i] = c;
+        range[i] = make_int2(off_node[i], off_node[i] + cnt_node[i] - 1);
+    }
+}
+
 __global__ void k_gather_tris(const float4* tri, const int* sorted_ids, int n, float4* out) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
@@ -1297,6 +1422,69 @@ int Engine::load_scene_json(const char* json, size_t len) {
     return LUCID_OK;
 }
 
+// PLOC rounds on the device; the host reads four integers per round to know
+// the surviving cluster count.  Returns LUCID_OK with root = -1 when the
+// clustering needs more than kPlocMaxRounds rounds (the caller then builds
+// the Karras tree instead).
+int Engine::build_ploc(const float4* verts, const int* sorted_ids, int n, int2* child, int2* range, float* nbox,
+                       int* slot_ids, int& root) {
+    constexpr int kPlocMaxRounds = 4096;
+    cudaStream_t st = S(stream_);
+    root = -1;
+    DBuf<int> cl0, cl1, nn, create, keep, create_pos, keep_pos, cnt_leaf, cnt_node, off_node, leaf_pos;
+    DBuf<float> cb0, cb1;
+    CK(cl0.alloc(n)); CK(cl1.alloc(n)); CK(nn.alloc(n)); CK(create.alloc(n)); CK(keep.alloc(n));
+    CK(create_pos.alloc(n)); CK(keep_pos.alloc(n)); CK(cnt_leaf.alloc(n)); CK(cnt_node.alloc(n - 1));
+    CK(off_node.alloc(n - 1)); CK(leaf_pos.alloc(n)); CK(cb0.alloc((size_t)6 * n)); CK(cb1.alloc((size_t)6 * n));
+    size_t temp = 0;
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, temp, create.p, create_pos.p, n, st));
+    DBuf<unsigned char> d_temp;
+    CK(d_temp.alloc(temp));
+    k_ploc_init<<<(n + 255) / 256, 256, 0, st>>>(verts, sorted_ids, n, cl0.p, cb0.p, cnt_leaf.p);
+    int* cl[2] = {cl0.p, cl1.p};
+    float* cb[2] = {cb0.p, cb1.p};
+    int cur = 0, count = n, base = 0;
+    std::vector<std::pair<int, int>> rounds;
+    int h[4];
+    while (count > 1) {
+        if ((int)rounds.size() >= kPlocMaxRounds) return LUCID_OK;
+        k_ploc_nn<<<(count + kPlocBlock - 1) / kPlocBlock, kPlocBlock, 0, st>>>(cb[cur], count, nn.p);
+        k_ploc_flags<<<(count + 255) / 256, 256, 0, st>>>(nn.p, count, create.p, keep.p);
+        size_t t1 = temp;
+        CK(cub::DeviceScan::ExclusiveSum(d_temp.p, t1, create.p, create_pos.p, count, st));
+        t1 = temp;
+        CK(cub::DeviceScan::ExclusiveSum(d_temp.p, t1, keep.p, keep_pos.p, count, st));
+        k_ploc_merge<<<(count + 255) / 256, 256, 0, st>>>(cl[cur], cb[cur], nn.p, create.p, keep.p, create_pos.p,
+                                                         keep_pos.p, count, base, child, nbox, cnt_node.p,
+                                                         cnt_leaf.p, cl[cur ^ 1], cb[cur ^ 1]);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(&h[0], create_pos.p + count - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&h[1], create.p + count - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&h[2], keep_pos.p + count - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&h[3], keep.p + count - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        int m = h[0] + h[1], survivors = h[2] + h[3];
+        if (m <= 0 || survivors != count - m) return fail(LUCID_ERR_CUDA, "BVH clustering made no progress");
+        rounds.push_back({base, m});
+        base += m;
+        count = survivors;
+        cur ^= 1;
+    }
+    if (base != n - 1) return fail(LUCID_ERR_CUDA, "BVH clustering produced a wrong node count");
+    const int r = n - 2;   // the last node created is the root
+    CK(cudaMemsetAsync(off_node.p + r, 0, sizeof(int), st));
+    for (auto it = rounds.rbegin(); it != rounds.rend(); ++it)
+        k_ploc_offsets<<<(it->second + 255) / 256, 256, 0, st>>>(child, cnt_node.p, it->first, it->second, off_node.p,
+                                                                 leaf_pos.p);
+    k_ploc_finish<<<(n + 255) / 256, 256, 0, st>>>(sorted_ids, leaf_pos.p, n, child, off_node.p, cnt_node.p, range,
+                                                  slot_ids);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));
+    ploc_rounds_ = (int)rounds.size();
+    root = r;
+    return LUCID_OK;
+}
+
 int Engine::build_bvh() {
     DeviceScene& D = *ds_;
     const HostScene& H = host_;
@@ -1393,9 +1581,9 @@ int Engine::build_bvh() {
     CK(cub::DeviceRadixSort::SortPairs(d_temp.p, temp, d_keys.p, d_keys_sorted.p, d_vals.p, d_vals_sorted.p, n, 0, 63,
                                        st));
     CK(D.bvh_tris.alloc((size_t)3 * n));
-    k_gather_tris<<<(n + 255) / 256, 256, 0, st>>>(d_tri.p, d_vals_sorted.p, n, D.bvh_tris.p);
     v.bvh_tris = D.bvh_tris.p;
     if (n <= 4) {
+        k_gather_tris<<<(n + 255) / 256, 256, 0, st>>>(d_tri.p, d_vals_sorted.p, n, D.bvh_tris.p);
         v.root = leaf_code(0, n);
         v.nodes = nullptr;
         bvh_leaves_ = 1;
@@ -1403,21 +1591,34 @@ int Engine::build_bvh() {
         CK(cudaStreamSynchronize(st));
         return LUCID_OK;
     }
-    CK(d_child.alloc(n - 1)); CK(d_range.alloc(n - 1)); CK(d_parent.alloc(n - 1)); CK(d_leaf_parent.alloc(n));
-    CK(d_arrive.alloc(n - 1)); CK(d_nbox.alloc((size_t)6 * (n - 1)));
-    CK(cudaMemsetAsync(d_parent.p, 0xff, (n - 1) * sizeof(int), st));   // root's parent = -1
-    CK(cudaMemsetAsync(d_arrive.p, 0, (n - 1) * sizeof(int), st));
-    k_karras<<<(n - 1 + 255) / 256, 256, 0, st>>>(d_keys_sorted.p, n, d_child.p, d_parent.p, d_leaf_parent.p,
-                                                  d_range.p);
-    k_refit<<<(n + 255) / 256, 256, 0, st>>>(d_verts.p, d_vals_sorted.p, n, d_child.p, d_parent.p, d_leaf_parent.p,
-                                            d_arrive.p, d_nbox.p);
+    CK(d_child.alloc(n - 1)); CK(d_range.alloc(n - 1)); CK(d_nbox.alloc((size_t)6 * (n - 1)));
+    const char* builder = std::getenv("LUCID_BVH");
+    int root = -1;
+    DBuf<int> d_slot;
+    if (!(builder && std::string(builder) == "lbvh")) {
+        CK(d_slot.alloc(n));
+        int rc = build_ploc(d_verts.p, d_vals_sorted.p, n, d_child.p, d_range.p, d_nbox.p, d_slot.p, root);
+        if (rc != LUCID_OK) return rc;
+    }
+    const int* slot_ids = root >= 0 ? d_slot.p : d_vals_sorted.p;
+    if (root < 0) {   // Karras LBVH (also the fallback when clustering does not converge)
+        CK(d_parent.alloc(n - 1)); CK(d_leaf_parent.alloc(n)); CK(d_arrive.alloc(n - 1));
+        CK(cudaMemsetAsync(d_parent.p, 0xff, (n - 1) * sizeof(int), st));   // root's parent = -1
+        CK(cudaMemsetAsync(d_arrive.p, 0, (n - 1) * sizeof(int), st));
+        k_karras<<<(n - 1 + 255) / 256, 256, 0, st>>>(d_keys_sorted.p, n, d_child.p, d_parent.p, d_leaf_parent.p,
+                                                      d_range.p);
+        k_refit<<<(n + 255) / 256, 256, 0, st>>>(d_verts.p, d_vals_sorted.p, n, d_child.p, d_parent.p,
+                                                d_leaf_parent.p, d_arrive.p, d_nbox.p);
+        root = 0;
+    }
+    k_gather_tris<<<(n + 255) / 256, 256, 0, st>>>(d_tri.p, slot_ids, n, D.bvh_tris.p);
     CK(D.nodes.alloc(n - 1));
     float pad = maxabs * 9.5367431640625e-07f + 1e-30f;   // 2^-20 of the scene's coordinate magnitude
-    k_flatten<<<(n - 1 + 255) / 256, 256, 0, st>>>(d_verts.p, d_vals_sorted.p, n, d_child.p, d_range.p, d_nbox.p, pad,
+    k_flatten<<<(n - 1 + 255) / 256, 256, 0, st>>>(d_verts.p, slot_ids, n, d_child.p, d_range.p, d_nbox.p, pad,
                                                   D.nodes.p);
     CK(cudaGetLastError());
     v.nodes = D.nodes.p;
-    v.root = 0;
+    v.root = root;
     // Reachable node count, leaves and depth (the traversal stack bound).
     std::vector<DevNode> hn(n - 1);
     CK(cudaMemcpyAsync(hn.data(), D.nodes.p, (n - 1) * sizeof(DevNode), cudaMemcpyDeviceToHost, st));
@@ -1425,10 +1626,25 @@ int Engine::build_bvh() {
     // The walk also validates the hierarchy before any traversal kernel uses
     // it: child indices in range, leaf ranges inside the triangle array, and
     // no node reached twice.
-    std::vector<std::pair<int, int>> stack{{0, 1}};
+    // The same walk sums the surface-area cost (node visits + triangle tests
+    // weighted by box area relative to the root's) reported as bvh_sah_.
+    std::vector<std::pair<int, int>> stack{{root, 1}};
     std::vector<unsigned char> seen(n - 1, 0);
     int nodes = 0, leaves = 0, depth = 0;
     long long leaf_tris = 0;
+    auto area = [](const float4& lo, const float4& hi) {
+        double dx = (double)hi.x - lo.x, dy = (double)hi.y - lo.y, dz = (double)hi.z - lo.z;
+        return dx * dy + dy * dz + dz * dx;
+    };
+    double sah = 1.0, root_area = 0.0;
+    {
+        const DevNode& r = hn[root];
+        float4 lo = make_float4(std::min(r.lmin_lc.x, r.rmin.x), std::min(r.lmin_lc.y, r.rmin.y),
+                                std::min(r.lmin_lc.z, r.rmin.z), 0.0f);
+        float4 hi = make_float4(std::max(r.lmax_rc.x, r.rmax.x), std::max(r.lmax_rc.y, r.rmax.y),
+                                std::max(r.lmax_rc.z, r.rmax.z), 0.0f);
+        root_area = std::max(area(lo, hi), 1e-30);
+    }
     while (!stack.empty()) {
         auto [nd, dep] = stack.back();
         stack.pop_back();
@@ -1439,6 +1655,7 @@ int Engine::build_bvh() {
         int c[2];
         std::memcpy(&c[0], &hn[nd].lmin_lc.w, 4);
         std::memcpy(&c[1], &hn[nd].lmax_rc.w, 4);
+        const double ca[2] = {area(hn[nd].lmin_lc, hn[nd].lmax_rc) / root_area, area(hn[nd].rmin, hn[nd].rmax) / root_area};
         for (int s = 0; s < 2; ++s) {
             if (c[s] < 0) {
                 int w = ~c[s], start = w >> 3, count = (w & 7) + 1;
@@ -1446,13 +1663,18 @@ int Engine::build_bvh() {
                 leaf_tris += count;
                 ++leaves;
                 depth = std::max(depth, dep + 1);
+                sah += ca[s] * count;
             } else {
                 stack.push_back({c[s], dep + 1});
+                sah += ca[s];
             }
         }
     }
     if (leaf_tris != n) return fail(LUCID_ERR_CUDA, "BVH leaves do not cover every triangle");
-    bvh_nodes_ = nodes; bvh_leaves_ = leaves; bvh_depth_ = depth;
+    bvh_nodes_ = nodes; bvh_leaves_ = leaves; bvh_depth_ = depth; bvh_sah_ = sah;
+    if (std::getenv("LUCID_VERBOSE"))
+        std::fprintf(stderr, "[lucid] BVH %s: %d nodes, %d leaves, depth %d, SAH cost %.2f\n",
+                     slot_ids == d_vals_sorted.p ? "lbvh" : "ploc", nodes, leaves, depth, sah);
     if (depth >= kStack)
         return fail(LUCID_ERR_OVERFLOW, "BVH depth " + std::to_string(depth) + " exceeds the traversal stack");
     return LUCID_OK;

@@ -67,6 +67,8 @@ private:
     void async_worker();
     int ensure_pool(long long paths, bool records);
     int build_bvh();
+    int build_ploc(const float4* verts, const int* sorted_ids, int n, int2* child, int2* range, float* nbox,
+                   int* slot_ids, int& root);
     void free_scene();
 
     int device_ = 0;
@@ -82,7 +84,8 @@ private:
     std::atomic<bool> cancel_{false};
     std::string err_;
     LucidRenderStats stats_{};
-    int bvh_nodes_ = 0, bvh_leaves_ = 0, bvh_depth_ = 0, num_big_ = 0;
+    int bvh_nodes_ = 0, bvh_leaves_ = 0, bvh_depth_ = 0, num_big_ = 0, ploc_rounds_ = 0;
+    double bvh_sah_ = 0.0;
     // one GPU call at a time per context (the reference's gpu_mutex_)
     std::mutex gpu_mu_;
     // path diagnostics
