@@ -1166,9 +1166,9 @@ __global__ void k_flatten(const float4* verts, const int* sorted_ids, int n, con
 // 2018): clusters start as the Morton-sorted triangles; each round every
 // cluster finds the neighbour within +-kPlocRadius positions whose merged box
 // has the smallest surface area, mutual nearest neighbours merge into a new
-// node, and the cluster array is compacted in order.  Ties prefer the lower
-// index, which totally orders candidate pairs, so the best pair of a round
-// is always mutual and every round merges at least one pair.  Node ids follow
+// node, and the cluster array is compacted in order.  Candidate pairs are
+// totally ordered (area, then a tie key of the pair), so the best pair of a
+// round is always mutual and every round merges at least one pair.  Node ids follow
 // creation order (root last); a top-down pass then gives every subtree a
 // contiguous range of triangle slots so that k_flatten can collapse small
 // subtrees into leaves exactly as for the Karras tree.
@@ -1207,12 +1207,19 @@ __global__ void __launch_bounds__(kPlocBlock) k_ploc_nn(const float* cbox, int c
     if (i >= count) return;
     const float* bi = sb + 6 * (threadIdx.x + kPlocRadius);
     float best = 3.0e38f;
-    int bj = -1;
+    int bj = -1, bgap = 0, ba = 0;
     int lo = max(0, i - kPlocRadius), hi = min(count - 1, i + kPlocRadius);
     for (int j = lo; j <= hi; ++j) {
         if (j == i) continue;
         float d = ploc_area(bi, sb + 6 * (j - b0 + kPlocRadius));
-        if (d < best) { best = d; bj = j; }   // ascending j: ties keep the lower index
+        // pair key (area, index gap, parity of the lower index, lower index):
+        // it depends on the pair only, so the best pair is mutual; on equal
+        // areas neighbours pair up (0,1), (2,3), ... instead of chaining
+        int a = min(i, j), gap = abs(i - j);
+        bool better = bj < 0 || d < best ||
+                      (d == best && (gap < bgap || (gap == bgap && ((a & 1) < (ba & 1) ||
+                                                                    ((a & 1) == (ba & 1) && a < ba)))));
+        if (better) { best = d; bj = j; bgap = gap; ba = a; }
     }
     nn[i] = bj;
 }
@@ -1673,8 +1680,9 @@ int Engine::build_bvh() {
     if (leaf_tris != n) return fail(LUCID_ERR_CUDA, "BVH leaves do not cover every triangle");
     bvh_nodes_ = nodes; bvh_leaves_ = leaves; bvh_depth_ = depth; bvh_sah_ = sah;
     if (std::getenv("LUCID_VERBOSE"))
-        std::fprintf(stderr, "[lucid] BVH %s: %d nodes, %d leaves, depth %d, SAH cost %.2f\n",
-                     slot_ids == d_vals_sorted.p ? "lbvh" : "ploc", nodes, leaves, depth, sah);
+        std::fprintf(stderr, "[lucid] BVH %s (%d rounds): %d nodes, %d leaves, depth %d, SAH cost %.2f\n",
+                     slot_ids == d_vals_sorted.p ? "lbvh" : "ploc", slot_ids == d_vals_sorted.p ? 0 : ploc_rounds_,
+                     nodes, leaves, depth, sah);
     if (depth >= kStack)
         return fail(LUCID_ERR_OVERFLOW, "BVH depth " + std::to_string(depth) + " exceeds the traversal stack");
     return LUCID_OK;
