@@ -325,22 +325,18 @@ struct ShadeResult {
     bool cont, shadow;
 };
 
-// One path segment.  A volume scatter event and a surface hit share the NEE
-// block (light selection, sampling, transmittance, weight) and the Russian
-// roulette; only the directional factor (phase function or BSDF) and the
-// continuation sample differ.  ALGO is a compile-time integrator id, so each
-// integrator's kernel carries only its own branches.  RNG draws per event
-// keep the reference's order: scatter = light select, 2 light draws, 2 phase
-// draws, RR; surface = light select, 2 light draws, 3 BSDF draws (+1 glass),
-// RR (path_tracer.hpp:496-554, 616-700).
+// One path segment: volume sampling, native-light / environment / emission
+// terms, NEE, BSDF sampling and Russian roulette.  ALGO is the integrator as
+// a compile-time constant, so each integrator's kernel carries only its own
+// branches.
 template <int ALGO>
 LD ShadeResult shade_path(const DevScene& sc, const FrameParams& f, const PathView& pv, int id) {
     ShadeResult out;
     out.cont = false;
     out.shadow = false;
-    constexpr bool nee = ALGO == ALGO_NEE || ALGO == ALGO_MIS || ALGO == ALGO_VOLUME_MIS;
-    constexpr bool mis = ALGO == ALGO_MIS || ALGO == ALGO_VOLUME_MIS;
-    constexpr bool vmis = ALGO == ALGO_VOLUME_MIS;
+    constexpr int algo = ALGO;
+    constexpr bool nee = algo == ALGO_NEE || algo == ALGO_MIS || algo == ALGO_VOLUME_MIS;
+    constexpr bool mis = algo == ALGO_MIS || algo == ALGO_VOLUME_MIS;
     float4 ro = pv.ray_o[id], rd = pv.ray_d[id];
     V3 o = f3(ro), d = f3(rd);
     int depth = __float_as_int(rd.w);
@@ -364,19 +360,13 @@ LD ShadeResult shade_path(const DevScene& sc, const FrameParams& f, const PathVi
     RGB sh_inc = rgb(0.f, 0.f, 0.f);
 
     do {
-        if (ALGO == ALGO_VOLUME_SIMPLE) {
+        if (algo == ALGO_VOLUME_SIMPLE) {
             float ts = 1e6f;
             if (has_hit) ts = smin(ts, hh.x);
             if (has_lh) ts = smin(ts, lh.y);
             T = mul(T, volume_transmittance(sc, o, d, ts, false));
         }
-        bool scatter = false;
-        V3 x = o;          // the event point
-        V3 wo = -d;
-        float g = 0.0f;    // phase anisotropy (scatter)
-        Mat m;             // material, shading normal, geometric normal (surface)
-        V3 n = d, sn = d;
-        if (vmis) {
+        if (algo == ALGO_VOLUME_MIS) {
             float ts = 1e6f;
             if (has_hit) ts = smin(ts, hh.x);
             if (has_lh) ts = smin(ts, lh.y);
@@ -388,151 +378,168 @@ LD ShadeResult shade_path(const DevScene& sc, const FrameParams& f, const PathVi
                 const DevVolume& v = sc.volumes[vi];
                 T = mul(T, rgb(v.color[0] / (1.0f + v.absorption[0]), v.color[1] / (1.0f + v.absorption[1]),
                                v.color[2] / (1.0f + v.absorption[2])));
-                x = o + d * vt;
-                g = v.anisotropy;
-                scatter = true;
-            }
-        }
-        bool want_nee;
-        if (!scatter) {
-            if (has_lh && (!has_hit || lh.y < hh.x)) {
-                // native light hit (path_tracer.hpp:429-452)
-                const DevLight& L = sc.lights[sc.native_start + lidx];
-                RGB em = c3(L.emission_radius);
-                if (mis) {
-                    float lpdf = 0.0f;
-                    if (sc.num_lights > 0) {
-                        float sp = area_ratio(L.normal_area.w, sc.total_light_area);
-                        if (sp > 0.0f) {
-                            V3 lp = o + d * lh.y;
-                            V3 ln = (__float_as_int(L.pos_type.w) == LIGHT_POINT) ? normalize_nz(lp - f3(L.pos_type))
-                                                                                  : f3(L.normal_area);
-                            lpdf = pdf_light(L.normal_area.w, o, lp, ln) * sp;
+                V3 x = o + d * vt;
+                V3 wo = -d;
+                float g = v.anisotropy;
+                if (sc.num_lights > 0) {
+                    float usel = randf(rng);
+                    int li = select_light(sc, usel);
+                    const DevLight& L = sc.lights[li];
+                    float lsp = area_ratio(L.normal_area.w, sc.total_light_area);
+                    if (lsp > 1e-6f) {
+                        float u1 = randf(rng), u2 = randf(rng);
+                        LightSample ls = sample_light(L, x, u1, u2);
+                        if (ls.pdf > MIN_PDF) {
+                            RGB Tsh = volume_transmittance(sc, x, ls.dir, ls.dist, true);
+                            float ct = dot(wo, ls.dir);
+                            float pe = hg_eval(g, ct);
+                            float pl = ls.pdf * lsp;
+                            float mw = mis_power(pl, pe);
+                            RGB pw = bsdf_weight(rgb(pe, pe, pe), 1.0f, pl);
+                            RGB c = mul(pw * mw, mul(Tsh, ls.emission));
+                            sh_inc = mul(T, c);
+                            sh_o = x; sh_d = ls.dir; sh_len = ls.dist;
+                            out.shadow = true;
                         }
                     }
-                    float mw = (last_pdf > MIN_PDF && lpdf > MIN_PDF) ? mis_power(last_pdf, lpdf) : 1.0f;
-                    result = result + mul(T, em) * mw;
-                } else {
-                    result = result + mul(T, em);
                 }
+                float u1 = randf(rng), u2 = randf(rng);
+                float ppdf;
+                V3 wi = hg_sample(g, wo, u1, u2, ppdf);
+                last_pdf = ppdf;
+                new_o = x; new_d = wi;
+                if (depth >= 3) {
+                    float rr = smin(smax3(T.r, T.g, T.b), 0.95f);
+                    if (randf(rng) > rr) break;
+                    T = T * (1.0f / rr);
+                }
+                if (!rgb_valid(T)) break;
+                out.cont = true;
                 break;
             }
-            if (!has_hit) {
-                result = result + mul(T, rgb(sc.env[0], sc.env[1], sc.env[2]));
-                break;
-            }
-            // surface hit: point and normal from (t, u, v, prim) as in bvh.hpp:108-128
-            x = o + d * hh.x;
-            int4 pi = sc.prim_info[prim];
-            V3 fn = f3(sc.prim_fn[prim]);
-            n = fn;
-            if (pi.w) {
-                float u = hh.y, vv = hh.z;
-                float w = 1.0f - u - vv;
-                V3 ni = f3(sc.prim_vn[3 * prim]) * w + f3(sc.prim_vn[3 * prim + 1]) * u + f3(sc.prim_vn[3 * prim + 2]) * vv;
-                n = make_dir_or(ni, fn);
-            }
-            const DevMaterial& dm = sc.materials[pi.x];
-            m.albedo = c3(dm.albedo_metallic);
-            m.metallic = dm.albedo_metallic.w;
-            m.roughness = smax(dm.rough_trans_ior_flags.x, MIN_ROUGHNESS);
-            m.transmission = dm.rough_trans_ior_flags.y;
-            m.ior = dm.rough_trans_ior_flags.z;
-            RGB em = c3(dm.emission);
-            bool has_em = dm.emission.w != 0.0f;
-            bool front = dot(wo, n) > 0;
-            sn = n;
-            if (m.transmission < 0.5f && !front) sn = -n;
-            if (!nee) {
-                result = result + mul(T, em);
-            } else if (!mis) {
-                if (has_em && depth == 0) result = result + mul(T, em);
-            } else if (has_em) {
-                float mw = 1.0f;
-                if (sc.num_lights > 0 && last_pdf > MIN_PDF && pi.z >= 0) {
-                    const DevLight& L = sc.lights[pi.z];
+        }
+        if (has_lh && (!has_hit || lh.y < hh.x)) {
+            // native light hit (path_tracer.hpp:429-452)
+            const DevLight& L = sc.lights[sc.native_start + lidx];
+            RGB em = c3(L.emission_radius);
+            if (mis) {
+                float lpdf = 0.0f;
+                if (sc.num_lights > 0) {
                     float sp = area_ratio(L.normal_area.w, sc.total_light_area);
                     if (sp > 0.0f) {
-                        float lpdf = pdf_light(L.normal_area.w, o, x, n) * sp;
-                        if (lpdf > MIN_PDF) mw = mis_power(last_pdf, lpdf);
+                        V3 lp = o + d * lh.y;
+                        V3 ln = (__float_as_int(L.pos_type.w) == LIGHT_POINT) ? normalize_nz(lp - f3(L.pos_type))
+                                                                              : f3(L.normal_area);
+                        lpdf = pdf_light(L.normal_area.w, o, lp, ln) * sp;
                     }
                 }
+                float mw = (last_pdf > MIN_PDF && lpdf > MIN_PDF) ? mis_power(last_pdf, lpdf) : 1.0f;
                 result = result + mul(T, em) * mw;
+            } else {
+                result = result + mul(T, em);
             }
-            want_nee = nee && !has_em && !(m.transmission > 0.5f);
-        } else {
-            want_nee = true;
+            break;
         }
-        if (want_nee && sc.num_lights > 0) {
+        if (!has_hit) {
+            result = result + mul(T, rgb(sc.env[0], sc.env[1], sc.env[2]));
+            break;
+        }
+        // surface hit: point and normal from (t, u, v, prim) as in bvh.hpp:108-128
+        V3 p = o + d * hh.x;
+        int4 pi = sc.prim_info[prim];
+        V3 fn = f3(sc.prim_fn[prim]);
+        V3 n = fn;
+        if (pi.w) {
+            float u = hh.y, v = hh.z;
+            float w = 1.0f - u - v;
+            V3 ni = f3(sc.prim_vn[3 * prim]) * w + f3(sc.prim_vn[3 * prim + 1]) * u + f3(sc.prim_vn[3 * prim + 2]) * v;
+            n = make_dir_or(ni, fn);
+        }
+        const DevMaterial& dm = sc.materials[pi.x];
+        Mat m;
+        m.albedo = c3(dm.albedo_metallic);
+        m.metallic = dm.albedo_metallic.w;
+        m.roughness = smax(dm.rough_trans_ior_flags.x, MIN_ROUGHNESS);
+        m.transmission = dm.rough_trans_ior_flags.y;
+        m.ior = dm.rough_trans_ior_flags.z;
+        RGB em = c3(dm.emission);
+        bool has_em = dm.emission.w != 0.0f;
+        V3 wo = -d;
+        bool front = dot(wo, n) > 0;
+        V3 sn = n;
+        if (m.transmission < 0.5f && !front) sn = -n;
+        if (!nee) {
+            result = result + mul(T, em);
+        } else if (!mis) {
+            if (has_em && depth == 0) result = result + mul(T, em);
+        } else if (has_em) {
+            float mw = 1.0f;
+            if (sc.num_lights > 0 && last_pdf > MIN_PDF && pi.z >= 0) {
+                const DevLight& L = sc.lights[pi.z];
+                float sp = area_ratio(L.normal_area.w, sc.total_light_area);
+                if (sp > 0.0f) {
+                    float lpdf = pdf_light(L.normal_area.w, o, p, n) * sp;
+                    if (lpdf > MIN_PDF) mw = mis_power(last_pdf, lpdf);
+                }
+            }
+            result = result + mul(T, em) * mw;
+        }
+        bool transmissive = m.transmission > 0.5f;
+        if (nee && sc.num_lights > 0 && !has_em && !transmissive) {
             float usel = randf(rng);
             int li = select_light(sc, usel);
             const DevLight& L = sc.lights[li];
             float lsp = area_ratio(L.normal_area.w, sc.total_light_area);
             if (lsp > 1e-6f) {
                 float u1 = randf(rng), u2 = randf(rng);
-                LightSample ls = sample_light(L, x, u1, u2);
+                LightSample ls = sample_light(L, p, u1, u2);
                 if (ls.pdf > MIN_PDF) {
-                    float pl = ls.pdf * lsp;
-                    RGB wgt = rgb(0.f, 0.f, 0.f);
-                    bool ok = true;
-                    if (scatter) {
-                        float pe = hg_eval(g, dot(wo, ls.dir));
-                        float mw = mis_power(pl, pe);
-                        wgt = bsdf_weight(rgb(pe, pe, pe), 1.0f, pl) * mw;
-                    } else {
-                        float nl = dot(sn, ls.dir);
-                        ok = nl > 1e-6f;
-                        if (ok) {
-                            RGB fb = eval_bsdf(m, wo, ls.dir, sn);
-                            if (mis) {
-                                float pb = pdf_bsdf(m, wo, ls.dir, sn);
-                                float mw = mis_power(pl, pb);
-                                wgt = bsdf_weight(fb, nl, pl) * mw;
+                    float nl = dot(sn, ls.dir);
+                    if (nl > 1e-6f) {
+                        RGB fb = eval_bsdf(m, wo, ls.dir, sn);
+                        float pl = ls.pdf * lsp;
+                        RGB c;
+                        if (mis) {
+                            float pb = pdf_bsdf(m, wo, ls.dir, sn);
+                            float mw = mis_power(pl, pb);
+                            RGB bw = bsdf_weight(fb, nl, pl);
+                            if (algo == ALGO_VOLUME_MIS) {
+                                RGB Tsh = volume_transmittance(sc, p, ls.dir, ls.dist, true);
+                                c = mul(bw * mw, mul(Tsh, ls.emission));
                             } else {
-                                wgt = bsdf_weight(fb, nl, pl);
+                                c = mul(bw * mw, ls.emission);
                             }
+                        } else {
+                            c = mul(bsdf_weight(fb, nl, pl), ls.emission);
                         }
-                    }
-                    if (ok) {
-                        RGB le = ls.emission;
-                        if (vmis) le = mul(volume_transmittance(sc, x, ls.dir, ls.dist, true), le);
-                        sh_inc = mul(T, mul(wgt, le));
-                        sh_o = x; sh_d = ls.dir; sh_len = ls.dist;
+                        sh_inc = mul(T, c);
+                        sh_o = p; sh_d = ls.dir; sh_len = ls.dist;
                         out.shadow = true;
                     }
                 }
             }
         }
-        if (scatter) {
-            float u1 = randf(rng), u2 = randf(rng);
-            float ppdf;
-            V3 wi = hg_sample(g, wo, u1, u2, ppdf);
-            last_pdf = ppdf;
-            new_d = wi;
+        V3 smp_n = (m.transmission > 0.5f) ? n : sn;
+        float u1 = randf(rng), u2 = randf(rng), u3 = randf(rng);
+        BsdfSample bs = sample_bsdf(m, wo, smp_n, u1, u2, u3, rng);
+        if (!(bs.kind == BS_PRECOMP || bs.pdf > MIN_PDF)) break;
+        RGB w;
+        if (bs.kind == BS_PRECOMP) {
+            w = bs.f;
         } else {
-            V3 smp_n = (m.transmission > 0.5f) ? n : sn;
-            float u1 = randf(rng), u2 = randf(rng), u3 = randf(rng);
-            BsdfSample bs = sample_bsdf(m, wo, smp_n, u1, u2, u3, rng);
-            if (!(bs.kind == BS_PRECOMP || bs.pdf > MIN_PDF)) break;
-            RGB w;
-            if (bs.kind == BS_PRECOMP) {
-                w = bs.f;
-            } else {
-                float c = fabsf(dot(smp_n, bs.wi));
-                if (c <= 1e-6f || bs.pdf < MIN_PDF) break;
-                w = bsdf_weight(bs.f, c, bs.pdf);
-            }
-            T = mul(T, w);
-            if (mis) last_pdf = (bs.kind == BS_EVAL) ? bs.pdf : 0.0f;
-            new_d = bs.wi;
+            float c = fabsf(dot(smp_n, bs.wi));
+            if (c <= 1e-6f || bs.pdf < MIN_PDF) break;
+            w = bsdf_weight(bs.f, c, bs.pdf);
         }
-        new_o = x;
+        T = mul(T, w);
+        if (mis) last_pdf = (bs.kind == BS_EVAL) ? bs.pdf : 0.0f;
         if (depth >= 3) {
             float rr = smin(smax3(T.r, T.g, T.b), 0.95f);
             if (randf(rng) > rr) break;
             T = T * (1.0f / rr);
         }
         if (!rgb_valid(T)) break;
+        new_o = p; new_d = bs.wi;
         out.cont = true;
     } while (0);
 
@@ -552,8 +559,11 @@ LD ShadeResult shade_path(const DevScene& sc, const FrameParams& f, const PathVi
     return out;
 }
 
+// Six resident CTAs per SM (at most 80 registers per thread): the extra
+// warps hide more of the shading kernel's instruction-fetch and memory
+// latency than the registers they cost (measured on the 1M-triangle scene).
 template <int ALGO>
-__global__ void __launch_bounds__(128) k_shade(DevScene sc, FrameParams f, PathView pv, int* cnt, int* cnt_next,
+__global__ void __launch_bounds__(128, 6) k_shade(DevScene sc, FrameParams f, PathView pv, int* cnt, int* cnt_next,
                                                int identity, int* qin, int* qout) {
     const int n = *(volatile int*)&cnt[0];
     for (;;) {
