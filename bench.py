@@ -207,6 +207,7 @@ def main():
     ap.add_argument("--cache", default="/tmp/lucid_bench")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-quality", action="store_true", help="skip the Cornell relMSE measurement")
+    ap.add_argument("--wave", type=int, default=0, help="paths per wave (0: the engine's default)")
     ap.add_argument("--width", type=int, default=W, help="smaller frames for profiling captures")
     ap.add_argument("--height", type=int, default=H)
     ap.add_argument("--spp", type=int, default=SPP)
@@ -235,6 +236,8 @@ def main():
     load_s = time.perf_counter() - t0
     ctx.set_camera(*cam)
     ctx.set_algorithm(ALGO)
+    if args.wave:
+        ctx.set_wave_capacity(args.wave)
     stats0 = ctx.scene_stats()
     log(f"[rank {rank}] {ctx.device_info()} scene {stats0} load {load_s:.2f}s")
     dev = torch.device("cuda", local_rank)

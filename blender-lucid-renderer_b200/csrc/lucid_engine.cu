@@ -559,11 +559,12 @@ LD ShadeResult shade_path(const DevScene& sc, const FrameParams& f, const PathVi
     return out;
 }
 
-// Six resident CTAs per SM (at most 80 registers per thread): the extra
-// warps hide more of the shading kernel's instruction-fetch and memory
-// latency than the registers they cost (measured on the 1M-triangle scene).
+// Eight resident CTAs per SM (at most 64 registers per thread, a few
+// hundred bytes of spills): the extra warps hide more of the shading
+// kernel's instruction-fetch and memory latency than the spills cost
+// (measured on the 1M-triangle scene: 4, 5, 6, 7, 8 CTAs per SM).
 template <int ALGO>
-__global__ void __launch_bounds__(128, 6) k_shade(DevScene sc, FrameParams f, PathView pv, int* cnt, int* cnt_next,
+__global__ void __launch_bounds__(128, 8) k_shade(DevScene sc, FrameParams f, PathView pv, int* cnt, int* cnt_next,
                                                int identity, int* qin, int* qout) {
     const int n = *(volatile int*)&cnt[0];
     for (;;) {
