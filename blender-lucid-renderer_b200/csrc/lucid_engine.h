@@ -66,6 +66,7 @@ private:
     int render_diag_impl(const LucidRenderParams& p, float* out_host, float* out_device);
     void async_worker();
     int ensure_pool(long long paths, bool records);
+    long long default_wave_paths(bool records) const;
     int build_bvh();
     int build_ploc(const float4* verts, const int* sorted_ids, int n, int2* child, int2* range, float* nbox,
                    int* slot_ids, int& root);
