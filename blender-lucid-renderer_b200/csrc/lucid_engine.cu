@@ -89,13 +89,17 @@ struct PathView {
     int* q0;
     int* q1;
     int* qs;
-    int* counters;     // per depth: [0] active, [1] shadow, [2..4] fetch cursors
+    int* qb;           // shading queue binned by event / material class
+    unsigned char* cls;   // class of each path's pending event
+    int* counters;     // per depth: [0] active, [1] shadow, [2..4] fetch cursors,
+                       // [8..23] class counts, [24..39] class cursors
     int* errors;       // [0] traversal stack overflow
     int2* rec_prim;
     int4* rec_cnt;     // bounces, nee tests, nee occluded
     unsigned long long* rec_hash;
 };
-constexpr int kCountersPerDepth = 8;
+constexpr int kCountersPerDepth = 48;
+constexpr int kBins = 16;
 constexpr int kMaxDepth = 1024;
 
 struct PathPool {
@@ -104,7 +108,8 @@ struct PathPool {
     DBuf<ulonglong2> rng;
     DBuf<float4> ray_o, ray_d, thr, rad, hit, sh_o, sh_d, sh_c;
     DBuf<float2> lhit;
-    DBuf<int> q0, q1, qs, counters, errors;
+    DBuf<int> q0, q1, qs, qb, counters, errors;
+    DBuf<unsigned char> cls;
     DBuf<int2> rec_prim;
     DBuf<int4> rec_cnt;
     DBuf<unsigned long long> rec_hash;
@@ -117,6 +122,7 @@ struct PathPool {
     void release() {
         rng.release(); ray_o.release(); ray_d.release(); thr.release(); rad.release(); hit.release();
         sh_o.release(); sh_d.release(); sh_c.release(); lhit.release(); q0.release(); q1.release(); qs.release();
+        qb.release(); cls.release();
         counters.release(); errors.release(); rec_prim.release(); rec_cnt.release(); rec_hash.release();
         film.release(); out.release(); film64.release(); out64.release();
         film_n = 0;
@@ -592,6 +598,77 @@ static ShadeKernel shade_kernel(int algo) {
         case ALGO_VOLUME_SIMPLE: return k_shade<ALGO_VOLUME_SIMPLE>;
         case ALGO_VOLUME_MIS: return k_shade<ALGO_VOLUME_MIS>;
         default: return k_shade<ALGO_NEE>;
+    }
+}
+
+// ---------------------------------------------------------------- shading bins
+// The shading kernel is limited by instruction fetch: divergent warps run
+// different parts of it (light/environment hits, emitters, glass, near-delta
+// metal, general Principled lobes, volume delta tracking).  Before each
+// shading launch the queue is binned by that class (a counting sort: one
+// histogram pass, one scatter pass with one atomic per class per warp), so
+// neighbouring warps shade the same kind of event.  The order of paths in a
+// queue does not change any result.
+LD int shade_bin(const DevScene& sc, const PathView& pv, int id, bool vol) {
+    float4 hh = pv.hit[id];
+    int prim = __float_as_int(hh.w);
+    float2 lh = pv.lhit[id];
+    int li = __float_as_int(lh.x);
+    int c = 0;   // light or environment reached
+    if (prim >= 0 && !(li >= 0 && lh.y < hh.x)) {
+        const DevMaterial& dm = sc.materials[sc.prim_info[prim].x];
+        float rough = dm.rough_trans_ior_flags.x, trans = dm.rough_trans_ior_flags.y, metal = dm.albedo_metallic.w;
+        c = dm.emission.w != 0.0f ? 1 : trans > 0.5f ? 2 : (metal > 0.5f && rough < 0.05f) ? 3 : (metal > 0.5f ? 4 : 5);
+    }
+    if (vol && sc.num_volumes > 0) {
+        float ts = 1e6f;
+        if (prim >= 0) ts = smin(ts, hh.x);
+        if (li >= 0) ts = smin(ts, lh.y);
+        V3 o = f3(pv.ray_o[id]), d = f3(pv.ray_d[id]);
+        for (int k = 0; k < sc.num_volumes && k < 4; ++k) {
+            float te, tx;
+            if (ray_aabb_segment(o, d, ts, sc.volumes[k], te, tx)) { c += 8; break; }
+        }
+    }
+    return c;
+}
+
+__global__ void __launch_bounds__(256) k_bin_count(DevScene sc, PathView pv, int* cnt, int identity, const int* qin,
+                                                   int vol) {
+    __shared__ int h[kBins];
+    if (threadIdx.x < kBins) h[threadIdx.x] = 0;
+    __syncthreads();
+    const int n = *(volatile int*)&cnt[0];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int id = identity ? i : qin[i];
+        int c = shade_bin(sc, pv, id, vol != 0);
+        pv.cls[id] = (unsigned char)c;
+        atomicAdd(&h[c], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < kBins && h[threadIdx.x]) atomicAdd(&cnt[8 + threadIdx.x], h[threadIdx.x]);
+}
+
+__global__ void __launch_bounds__(256) k_bin_scatter(PathView pv, int* cnt, int identity, const int* qin, int* qb) {
+    __shared__ int base[kBins];
+    if (threadIdx.x == 0) {
+        int sum = 0;
+        for (int c = 0; c < kBins; ++c) { base[c] = sum; sum += cnt[8 + c]; }
+    }
+    __syncthreads();
+    const int n = *(volatile int*)&cnt[0];
+    // whole warps iterate together (match/shuffle below need every lane)
+    for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+        int i = i0 + (int)threadIdx.x;
+        bool act = i < n;
+        int id = act ? (identity ? i : qin[i]) : 0;
+        int c = act ? (int)pv.cls[id] : -1;
+        unsigned peers = __match_any_sync(0xffffffffu, c);
+        int leader = __ffs(peers) - 1;
+        int pos = 0;
+        if (act && (int)lane_id() == leader) pos = atomicAdd(&cnt[24 + c], __popc(peers));
+        pos = __shfl_sync(0xffffffffu, pos, leader);
+        if (act) qb[base[c] + pos + __popc(peers & lanemask_lt())] = id;
     }
 }
 
@@ -1348,14 +1425,14 @@ int Engine::device_info(char* buf, size_t cap) const {
 
 int Engine::set_camera(float px, float py, float pz, float dx, float dy, float dz, float ux, float uy, float uz,
                        float fov_deg) {
-    std::lock_guard<std::mutex> gl(gpu_mu_);
+    GpuLock gl(*this);
     make_camera(cam_, px, py, pz, dx, dy, dz, ux, uy, uz, fov_deg);
     camera_set_ = true;
     return LUCID_OK;
 }
 
 int Engine::set_algorithm(const char* name) {
-    std::lock_guard<std::mutex> gl(gpu_mu_);
+    GpuLock gl(*this);
     std::string a = name ? name : "";
     if (a == "simple") algo_ = ALGO_SIMPLE;
     else if (a == "mis") algo_ = ALGO_MIS;
@@ -1385,7 +1462,7 @@ int Engine::stats(LucidRenderStats* out) const { *out = stats_; return LUCID_OK;
 void Engine::free_scene() { ds_->release(); scene_loaded_ = false; }
 
 int Engine::load_scene_json(const char* json, size_t len) {
-    std::lock_guard<std::mutex> gl(gpu_mu_);
+    GpuLock gl(*this);
     CK(cudaSetDevice(device_));
     if (!stream_) {
         cudaStream_t s;
@@ -1716,7 +1793,7 @@ int Engine::ensure_pool(long long paths, bool records) {
     P.release();
     CK(P.rng.alloc(cap)); CK(P.ray_o.alloc(cap)); CK(P.ray_d.alloc(cap)); CK(P.thr.alloc(cap)); CK(P.rad.alloc(cap));
     CK(P.hit.alloc(cap)); CK(P.lhit.alloc(cap)); CK(P.sh_o.alloc(cap)); CK(P.sh_d.alloc(cap)); CK(P.sh_c.alloc(cap));
-    CK(P.q0.alloc(cap)); CK(P.q1.alloc(cap)); CK(P.qs.alloc(cap));
+    CK(P.q0.alloc(cap)); CK(P.q1.alloc(cap)); CK(P.qs.alloc(cap)); CK(P.qb.alloc(cap)); CK(P.cls.alloc(cap));
     CK(P.counters.alloc((size_t)kCountersPerDepth * (kMaxDepth + 1)));
     CK(P.errors.alloc(4));
     if (records) { CK(P.rec_prim.alloc(cap)); CK(P.rec_cnt.alloc(cap)); CK(P.rec_hash.alloc(cap)); }
@@ -1725,7 +1802,7 @@ int Engine::ensure_pool(long long paths, bool records) {
     PathView& v = P.view;
     v.rng = P.rng.p; v.ray_o = P.ray_o.p; v.ray_d = P.ray_d.p; v.thr = P.thr.p; v.rad = P.rad.p; v.hit = P.hit.p;
     v.lhit = P.lhit.p; v.sh_o = P.sh_o.p; v.sh_d = P.sh_d.p; v.sh_c = P.sh_c.p; v.q0 = P.q0.p; v.q1 = P.q1.p;
-    v.qs = P.qs.p; v.counters = P.counters.p; v.errors = P.errors.p;
+    v.qs = P.qs.p; v.qb = P.qb.p; v.cls = P.cls.p; v.counters = P.counters.p; v.errors = P.errors.p;
     v.rec_prim = P.rec_prim.p; v.rec_cnt = P.rec_cnt.p; v.rec_hash = P.rec_hash.p;
     return LUCID_OK;
 }
@@ -1741,10 +1818,14 @@ namespace {
 //   shadow: queue 4 + shadow record 48 + radiance 16 read + 16 write  = 84 / ray
 //   raygen: rng 16 + ray 32 + throughput 16 + radiance 16            = 80 / path
 //   film  : radiance 16 / path + film 32 / pixel
-constexpr double kBytesTrace = 60, kBytesShade = 340, kBytesShadow = 84, kBytesRaygen = 80, kBytesFilm = 16;
-enum Kind { K_RAYGEN, K_TRACE0, K_TRACE, K_SHADE, K_SHADOW, K_FILM, K_NUM };
-const char* kKindNames[K_NUM] = {"k_raygen", "k_trace_primary", "k_trace", "k_shade", "k_shadow", "k_film"};
-const double kKindBytes[K_NUM] = {kBytesRaygen, kBytesTrace, kBytesTrace, kBytesShade, kBytesShadow, kBytesFilm};
+//   bin   : queue id 2 x 4 + hit 16 + light hit 8 + class 1 w + 1 r
+//           + binned id 4                                            = 38 / path
+constexpr double kBytesTrace = 60, kBytesShade = 340, kBytesShadow = 84, kBytesRaygen = 80, kBytesFilm = 16,
+                 kBytesBin = 38;
+enum Kind { K_RAYGEN, K_TRACE0, K_TRACE, K_SHADE, K_SHADOW, K_FILM, K_BIN, K_NUM };
+const char* kKindNames[K_NUM] = {"k_raygen", "k_trace_primary", "k_trace", "k_shade", "k_shadow", "k_film", "k_bin"};
+const double kKindBytes[K_NUM] = {kBytesRaygen, kBytesTrace, kBytesTrace, kBytesShade, kBytesShadow, kBytesFilm,
+                                  kBytesBin};
 }  // namespace
 
 // Default paths per wave: large waves keep every depth's launches full and
@@ -1762,7 +1843,7 @@ long long Engine::default_wave_paths(bool records) const {
 }
 
 int Engine::render(const LucidRenderParams& p, float* out_host, LucidSampleRecord* recs, float* out_device) {
-    std::lock_guard<std::mutex> lk(gpu_mu_);
+    GpuLock gl(*this);
     if (diag_enabled_) {
         if (recs) return fail(LUCID_ERR_INVALID, "per-sample records are not produced while diagnostics are enabled");
         return render_diag_impl(p, out_host, out_device);
@@ -1771,7 +1852,7 @@ int Engine::render(const LucidRenderParams& p, float* out_host, LucidSampleRecor
 }
 
 int Engine::render_f64(const LucidRenderParams& p, double* out_host) {
-    std::lock_guard<std::mutex> lk(gpu_mu_);
+    GpuLock gl(*this);
     if (diag_enabled_) return fail(LUCID_ERR_INVALID, "FP64 references are not rendered while diagnostics are enabled");
     return render_impl(p, nullptr, nullptr, nullptr, nullptr, false, out_host);
 }
@@ -1892,7 +1973,7 @@ int Engine::render_diag_impl(const LucidRenderParams& p, float* out_host, float*
 
 // PathRecordingConfig::standard() (diagnostics/path_stats_config.hpp).
 int Engine::diag_enable(const LucidDiagConfig* cfg) {
-    std::lock_guard<std::mutex> lk(gpu_mu_);
+    GpuLock gl(*this);
     LucidDiagConfig c{2, 16, 4, 16, 0.001f, 3.0f, 0};
     if (cfg) c = *cfg;
     if (c.subsample_factor < 1) return fail(LUCID_ERR_INVALID, "subsample_factor must be >= 1");
@@ -1902,31 +1983,31 @@ int Engine::diag_enable(const LucidDiagConfig* cfg) {
     return LUCID_OK;
 }
 int Engine::diag_disable() {
-    std::lock_guard<std::mutex> lk(gpu_mu_);
+    GpuLock gl(*this);
     diag_enabled_ = false;
     diag_film_.reset();
     if (diag_dev_) { delete diag_dev_; diag_dev_ = nullptr; }
     return LUCID_OK;
 }
 int Engine::diag_clear() {
-    std::lock_guard<std::mutex> lk(gpu_mu_);
+    GpuLock gl(*this);
     if (diag_film_.valid()) diag_film_.clear();
     return LUCID_OK;
 }
 int Engine::diag_stats(LucidDiagStats* out) {
-    std::lock_guard<std::mutex> lk(gpu_mu_);
+    GpuLock gl(*this);
     std::memset(out, 0, sizeof(*out));
     if (diag_film_.valid()) diag_film_.stats(out);
     return LUCID_OK;
 }
 int Engine::diag_pixel(int x, int y, bool by_mean, LucidDiagPixel* info, LucidDiagGroup* groups, int cap) {
-    std::lock_guard<std::mutex> lk(gpu_mu_);
+    GpuLock gl(*this);
     std::memset(info, 0, sizeof(*info));
     if (!diag_film_.valid()) return 0;
     return diag_film_.export_pixel(x, y, by_mean, info, groups, groups ? cap : 0);
 }
 int Engine::diag_variance_map(float* out, size_t cap) {
-    std::lock_guard<std::mutex> lk(gpu_mu_);
+    GpuLock gl(*this);
     if (!diag_film_.valid()) return 0;
     size_t n = (size_t)diag_film_.width() * diag_film_.height();
     if (cap < n) return fail(LUCID_ERR_INVALID, "variance map buffer too small");
@@ -1934,7 +2015,7 @@ int Engine::diag_variance_map(float* out, size_t cap) {
     return (int)n;
 }
 int Engine::diag_top(int n, bool by_mean, LucidDiagGroup* groups, int32_t* xy, int cap) {
-    std::lock_guard<std::mutex> lk(gpu_mu_);
+    GpuLock gl(*this);
     if (!diag_film_.valid()) return 0;
     return diag_film_.export_top(n, by_mean, groups, xy, groups ? cap : 0);
 }
@@ -2007,6 +2088,10 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
     const int g_trace0 = num_sms_ * std::max(1, occ_t0);
     const int g_trace = num_sms_ * std::max(1, occ_t), g_shade = num_sms_ * std::max(1, occ_s),
               g_shadow = num_sms_ * std::max(1, occ_h);
+    const int g_bin = num_sms_ * 8;
+    const char* sort_env = std::getenv("LUCID_SHADE_BINS");
+    const bool bin = !(sort_env && sort_env[0] == '0');
+    const int vol_bins = (algo_ == ALGO_VOLUME_MIS || algo_ == ALGO_VOLUME_SIMPLE) ? 1 : 0;
 
     struct Launch { int kind; cudaEvent_t a, b; int depth; };
     std::vector<Launch> launches;
@@ -2056,8 +2141,17 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
                 k_trace<<<g_trace, 128, 0, st>>>(ds_->view, pv, cnt, 0, f.records);
             }
             ev_end(e);
+            if (bin) {
+                e = ev_begin(K_BIN, depth);
+                k_bin_count<<<g_bin, 256, 0, st>>>(ds_->view, pv, cnt, depth == 0, qin, vol_bins);
+                k_bin_scatter<<<g_bin, 256, 0, st>>>(pv, cnt, depth == 0, qin, P.qb.p);
+                ev_end(e);
+            }
             e = ev_begin(K_SHADE, depth);
-            shade<<<g_shade, 128, 0, st>>>(ds_->view, f, pv, cnt, cnt_next, depth == 0, qin, qout);
+            if (bin)
+                shade<<<g_shade, 128, 0, st>>>(ds_->view, f, pv, cnt, cnt_next, 0, P.qb.p, qout);
+            else
+                shade<<<g_shade, 128, 0, st>>>(ds_->view, f, pv, cnt, cnt_next, depth == 0, qin, qout);
             ev_end(e);
             e = ev_begin(K_SHADOW, depth);
             k_shadow<<<g_shadow, 128, 0, st>>>(ds_->view, pv, cnt, f.records);
@@ -2083,6 +2177,7 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
             for (int d = 0; d < p.max_depth; ++d) {
                 kind_units[d == 0 ? K_TRACE0 : K_TRACE] += hcnt[kCountersPerDepth * d];
                 kind_units[K_SHADE] += hcnt[kCountersPerDepth * d];
+                if (bin) kind_units[K_BIN] += hcnt[kCountersPerDepth * d];
                 kind_units[K_SHADOW] += hcnt[kCountersPerDepth * d + 1];
             }
         }
@@ -2149,7 +2244,7 @@ int Engine::async_start(int w, int h, int max_depth) {
     if (w <= 0 || h <= 0) return fail(LUCID_ERR_INVALID, "async: size must be positive");
     if (!scene_loaded_ || !camera_set_) return fail(LUCID_ERR_NO_SCENE, "scene or camera not set");
     {
-        std::lock_guard<std::mutex> gl(gpu_mu_);
+        GpuLock gl(*this);
         CK(cudaSetDevice(device_));
         size_t n = (size_t)w * h;
         if (async_acc_n_ < n) {
@@ -2181,7 +2276,7 @@ int Engine::async_reset(int w, int h, int max_depth) {
     if ((size_t)w * h > async_acc_n_ || w <= 0 || h <= 0)
         return fail(LUCID_ERR_INVALID, "async reset: a larger resolution needs stop + start");
     {
-        std::lock_guard<std::mutex> gl(gpu_mu_);
+        GpuLock gl(*this);
         async_w_ = w; async_h_ = h; async_depth_ = std::max(1, max_depth);
     }
     async_reset_ = true;
@@ -2209,6 +2304,10 @@ void Engine::async_worker() {
     int w = 0, h = 0, depth = 8;
     while (async_run_) {
         bool wipe = async_reset_.exchange(false);
+        // std::mutex is not fair: back off while an API call waits for the
+        // GPU, or a set_camera / reset from the UI thread could wait for
+        // minutes behind the worker's back-to-back iterations
+        while (gpu_waiters_.load() > 0 && async_run_) std::this_thread::sleep_for(std::chrono::microseconds(100));
         {
             std::lock_guard<std::mutex> gl(gpu_mu_);
             if (wipe || w != async_w_ || h != async_h_) {
@@ -2290,7 +2389,7 @@ unsigned char* g_noalloc_addr[64] = {};
 }  // namespace
 
 int Engine::render_noalloc(const LucidRenderParams& p, float* d_out) {
-    std::lock_guard<std::mutex> gl(gpu_mu_);
+    GpuLock gl(*this);
     reset_cancel();
     if (!d_out) return fail(LUCID_ERR_INVALID, "output pointer is null");
     if (p.tile_w <= 0 || p.tile_h <= 0 || p.full_w <= 0 || p.full_h <= 0)
@@ -2390,7 +2489,7 @@ int Engine::render_noalloc(const LucidRenderParams& p, float* d_out) {
 }
 
 int Engine::render_debug(int tx, int ty, int tw, int th, int fw, int fh, const char* mode, float* out_host) {
-    std::lock_guard<std::mutex> gl(gpu_mu_);
+    GpuLock gl(*this);
     reset_cancel();
     if (tw <= 0 || th <= 0 || fw <= 0 || fh <= 0) return fail(LUCID_ERR_INVALID, "tile and image sizes must be positive");
     size_t np = (size_t)tw * th;

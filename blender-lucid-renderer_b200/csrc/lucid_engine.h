@@ -87,8 +87,21 @@ private:
     LucidRenderStats stats_{};
     int bvh_nodes_ = 0, bvh_leaves_ = 0, bvh_depth_ = 0, num_big_ = 0, ploc_rounds_ = 0;
     double bvh_sah_ = 0.0;
-    // one GPU call at a time per context (the reference's gpu_mutex_)
+    // one GPU call at a time per context (the reference's gpu_mutex_); API
+    // calls take it through GpuLock, which the async worker yields to
     std::mutex gpu_mu_;
+    std::atomic<int> gpu_waiters_{0};
+    struct GpuLock {
+        Engine& e;
+        explicit GpuLock(Engine& en) : e(en) {
+            e.gpu_waiters_.fetch_add(1);
+            e.gpu_mu_.lock();
+            e.gpu_waiters_.fetch_sub(1);
+        }
+        ~GpuLock() { e.gpu_mu_.unlock(); }
+        GpuLock(const GpuLock&) = delete;
+        GpuLock& operator=(const GpuLock&) = delete;
+    };
     // path diagnostics
     bool diag_enabled_ = false;
     LucidDiagConfig diag_cfg_{};

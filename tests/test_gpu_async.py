@@ -48,8 +48,11 @@ def test_async_snapshot_equals_average_of_one_sample_renders():
     # reset wipes the accumulator: the sample count restarts
     ctx.async_start(W, H, DEPTH)
     assert _wait(lambda: ctx.async_poll()[0] >= 64)
+    # calls from another thread get the GPU promptly while the worker runs
+    t0 = time.time()
     ctx.set_camera(0.5, 0.5, 1.9, 0.0, 0.0, -1.0, 0.0, 1.0, 0.0, 35.0)
     ctx.async_reset(W, H, DEPTH)
+    assert time.time() - t0 < 2.0
     assert _wait(lambda: 0 < ctx.async_poll()[0] < 64 or ctx.async_revision() > 0)
     ctx.async_stop()
     ctx.close()
