@@ -62,7 +62,8 @@ struct DeviceScene {
     DBuf<float4> bvh_tris, bnd_tris, big_tris, prim_fn, prim_vn;
     DBuf<int4> prim_info;
     DBuf<int> guide;
-    DBuf<DevNode> nodes;
+    DBuf<DevNode4> nodes;
+    DBuf<DevNode> nodes2;
     DBuf<DevMaterial> materials;
     DBuf<DevLight> lights;
     DBuf<float> cdf, grid;
@@ -70,7 +71,7 @@ struct DeviceScene {
     DevScene view{};
     void release() {
         bvh_tris.release(); bnd_tris.release(); big_tris.release(); prim_fn.release(); prim_vn.release(); prim_info.release();
-        nodes.release(); guide.release(); materials.release(); lights.release(); cdf.release(); grid.release(); volumes.release();
+        nodes.release(); nodes2.release(); guide.release(); materials.release(); lights.release(); cdf.release(); grid.release(); volumes.release();
     }
 };
 
@@ -1270,7 +1271,7 @@ __global__ void k_flatten(const float4* verts, const int* sorted_ids, int n, con
 // creation order (root last); a top-down pass then gives every subtree a
 // contiguous range of triangle slots so that k_flatten can collapse small
 // subtrees into leaves exactly as for the Karras tree.
-constexpr int kPlocRadius = 16;
+constexpr int kPlocRadius = 32;
 constexpr int kPlocBlock = 256;
 
 struct PlocBox { float lo[3], hi[3]; };
@@ -1658,7 +1659,7 @@ int Engine::build_bvh() {
     }
     v.num_bvh_tris = n;
     bvh_nodes_ = 0; bvh_leaves_ = 0; bvh_depth_ = 0;
-    if (n == 0) { v.root = 0; v.nodes = nullptr; v.bvh_tris = nullptr; return LUCID_OK; }
+    if (n == 0) { v.root = v.root2 = 0; v.nodes = nullptr; v.nodes2 = nullptr; v.bvh_tris = nullptr; return LUCID_OK; }
     cudaStream_t st = S(stream_);
     DBuf<float4> d_tri, d_verts;
     DBuf<int> d_ids, d_vals, d_vals_sorted, d_parent, d_leaf_parent, d_arrive, d_bounds;
@@ -1690,7 +1691,9 @@ int Engine::build_bvh() {
     if (n <= 4) {
         k_gather_tris<<<(n + 255) / 256, 256, 0, st>>>(d_tri.p, d_vals_sorted.p, n, D.bvh_tris.p);
         v.root = leaf_code(0, n);
+        v.root2 = v.root;
         v.nodes = nullptr;
+        v.nodes2 = nullptr;
         bvh_leaves_ = 1;
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(st));
@@ -1717,16 +1720,15 @@ int Engine::build_bvh() {
         root = 0;
     }
     k_gather_tris<<<(n + 255) / 256, 256, 0, st>>>(d_tri.p, slot_ids, n, D.bvh_tris.p);
-    CK(D.nodes.alloc(n - 1));
+    DBuf<DevNode>& d_nodes2 = D.nodes2;
+    CK(d_nodes2.alloc(n - 1));
     float pad = maxabs * 9.5367431640625e-07f + 1e-30f;   // 2^-20 of the scene's coordinate magnitude
     k_flatten<<<(n - 1 + 255) / 256, 256, 0, st>>>(d_verts.p, slot_ids, n, d_child.p, d_range.p, d_nbox.p, pad,
-                                                  D.nodes.p);
+                                                  d_nodes2.p);
     CK(cudaGetLastError());
-    v.nodes = D.nodes.p;
-    v.root = root;
     // Reachable node count, leaves and depth (the traversal stack bound).
     std::vector<DevNode> hn(n - 1);
-    CK(cudaMemcpyAsync(hn.data(), D.nodes.p, (n - 1) * sizeof(DevNode), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(hn.data(), d_nodes2.p, (n - 1) * sizeof(DevNode), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     // The walk also validates the hierarchy before any traversal kernel uses
     // it: child indices in range, leaf ranges inside the triangle array, and
@@ -1776,12 +1778,83 @@ int Engine::build_bvh() {
         }
     }
     if (leaf_tris != n) return fail(LUCID_ERR_CUDA, "BVH leaves do not cover every triangle");
-    bvh_nodes_ = nodes; bvh_leaves_ = leaves; bvh_depth_ = depth; bvh_sah_ = sah;
+    // Collapse the binary tree into 4-wide nodes: starting from a node's two
+    // children, the internal child with the largest box is replaced by its
+    // own two children until there are four (or only leaves).
+    std::vector<DevNode4> n4;
+    n4.reserve((size_t)nodes / 2 + 1);
+    std::vector<std::pair<int, int>> todo{{root, 0}};   // (binary node, index of its 4-wide node)
+    n4.push_back(DevNode4{});
+    int depth4 = 1;
+    std::vector<int> level4{1};
+    while (!todo.empty()) {
+        auto [bn, idx] = todo.back();
+        todo.pop_back();
+        struct Ch { float4 lo, hi; int code; };
+        Ch ch[4];
+        int cnt = 0;
+        auto children_of = [&](int b, Ch* out) {
+            int c0, c1;
+            std::memcpy(&c0, &hn[b].lmin_lc.w, 4);
+            std::memcpy(&c1, &hn[b].lmax_rc.w, 4);
+            out[0] = {hn[b].lmin_lc, hn[b].lmax_rc, c0};
+            out[1] = {hn[b].rmin, hn[b].rmax, c1};
+        };
+        children_of(bn, ch);
+        cnt = 2;
+        while (cnt < 4) {
+            int best = -1;
+            double ba = -1.0;
+            for (int k = 0; k < cnt; ++k)
+                if (ch[k].code >= 0 && area(ch[k].lo, ch[k].hi) > ba) { ba = area(ch[k].lo, ch[k].hi); best = k; }
+            if (best < 0) break;
+            Ch two[2];
+            children_of(ch[best].code, two);
+            ch[best] = two[0];
+            ch[cnt++] = two[1];
+        }
+        const int my_level = level4[idx];
+        DevNode4 q;
+        float* f[6] = {&q.xmin.x, &q.xmax.x, &q.ymin.x, &q.ymax.x, &q.zmin.x, &q.zmax.x};
+        int codes[4];
+        for (int k = 0; k < 4; ++k) {
+            if (k < cnt) {
+                f[0][k] = ch[k].lo.x; f[1][k] = ch[k].hi.x; f[2][k] = ch[k].lo.y; f[3][k] = ch[k].hi.y;
+                f[4][k] = ch[k].lo.z; f[5][k] = ch[k].hi.z;
+                if (ch[k].code >= 0) {
+                    int ni = (int)n4.size();
+                    n4.push_back(DevNode4{});
+                    level4.push_back(my_level + 1);
+                    depth4 = std::max(depth4, my_level + 1);
+                    todo.push_back({ch[k].code, ni});
+                    codes[k] = ni;
+                } else {
+                    codes[k] = ch[k].code;
+                    depth4 = std::max(depth4, my_level + 1);
+                }
+            } else {
+                for (int a = 0; a < 6; ++a) f[a][k] = 0.0f;
+                codes[k] = kEmptyChild;
+            }
+        }
+        q.child = make_int4(codes[0], codes[1], codes[2], codes[3]);
+        q.pad = make_int4(0, 0, 0, 0);
+        n4[idx] = q;
+    }
+    CK(D.nodes.alloc(n4.size()));
+    CK(cudaMemcpyAsync(D.nodes.p, n4.data(), n4.size() * sizeof(DevNode4), cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    v.nodes = D.nodes.p;
+    v.root = 0;
+    v.nodes2 = D.nodes2.p;
+    v.root2 = root;
+    bvh_nodes_ = (int)n4.size(); bvh_leaves_ = leaves; bvh_depth_ = depth4; bvh_sah_ = sah;
     if (std::getenv("LUCID_VERBOSE"))
-        std::fprintf(stderr, "[lucid] BVH %s (%d rounds): %d nodes, %d leaves, depth %d, SAH cost %.2f\n",
+        std::fprintf(stderr, "[lucid] BVH %s (%d rounds): %d binary nodes, %d leaves, depth %d, SAH cost %.2f; "
+                     "%d 4-wide nodes, depth %d\n",
                      slot_ids == d_vals_sorted.p ? "lbvh" : "ploc", slot_ids == d_vals_sorted.p ? 0 : ploc_rounds_,
-                     nodes, leaves, depth, sah);
-    if (depth >= kStack)
+                     nodes, leaves, depth, sah, (int)n4.size(), depth4);
+    if (3 * (depth4 - 1) >= kStack || depth >= kStack)
         return fail(LUCID_ERR_OVERFLOW, "BVH depth " + std::to_string(depth) + " exceeds the traversal stack");
     return LUCID_OK;
 }

@@ -56,10 +56,22 @@ struct alignas(16) DevNode {
     float4 rmax;      // right box max xyz
 };
 
+// 4-wide BVH node (128 B): the four children's boxes as x/y/z min/max lanes
+// and their codes (>= 0 node index, < 0 leaf ~(start << 3 | count - 1),
+// kEmptyChild for an unused slot).
+struct alignas(16) DevNode4 {
+    float4 xmin, xmax, ymin, ymax, zmin, zmax;
+    int4 child;
+    int4 pad;
+};
+constexpr int kEmptyChild = 0x7fffffff;
+
 struct DevScene {
     // geometry in BVH order: 3 float4 per triangle (v0 | prim id, e1, e2)
     const float4* bvh_tris;
-    const DevNode* nodes;
+    const DevNode4* nodes;    // 4-wide tree (any-hit queries), root `root`
+    const DevNode* nodes2;    // binary tree (closest-hit queries), root `root2`
+    int root2;
     int num_bvh_tris;
     int root;                       // root child code (node index or leaf code)
     // boundary-only triangles (tested by brute force): 3 float4 each
