@@ -179,6 +179,64 @@ def c1_quality(device: int) -> dict:
             "reference_s": round(ref_s, 3), "samples_per_s": 256 * 256 * 16 / (ms / 1000.0)}
 
 
+def serving(device: int, seed: int = 7) -> dict:
+    """The request loop on a seeded job trace: Poisson arrivals (mean 40 per
+    second for one second) of viewport sessions (800x600, 16 one-sample
+    ticks, interactive), material previews (256x256, 32 spp) and F12 renders
+    (1920x1080, 256 spp) of the Cornell box.  Latencies come from the trace
+    on 4 slots; aggregate samples/s from the same jobs submitted at once, on
+    4 slots and on 1 slot (one after another)."""
+    import lucid_capi
+    import lucid_scenes as ls
+    rng = np.random.default_rng(seed)
+    cornell, ccam = ls.cornell_box()
+    preview, pcam = ls.material_preview_scene(seed)
+    t, jobs = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / 40.0)
+        if t > 1.0:
+            break
+        u = rng.random()
+        if u < 0.6:
+            jobs.append((t, "cornell", 800, 600, 16, True))
+        elif u < 0.95:
+            jobs.append((t, "preview", 256, 256, 32, False))
+        else:
+            jobs.append((t, "cornell", 1920, 1080, 256, False))
+    if not any(j[2] == 1920 for j in jobs):
+        jobs.append((0.5, "cornell", 1920, 1080, 256, False))
+    cams = {"cornell": ccam, "preview": pcam}
+
+    def run(slots, timed):
+        srv = lucid_capi.Server(device, slots=slots)
+        ids = {"cornell": srv.add_scene(ls.to_json(cornell)), "preview": srv.add_scene(ls.to_json(preview))}
+        t0 = time.perf_counter()
+        jids = []
+        for (ta, name, w, h, spp, inter) in jobs:
+            if timed:
+                dt = ta - (time.perf_counter() - t0)
+                if dt > 0:
+                    time.sleep(dt)
+            jids.append(srv.submit(ids[name], cams[name], w, h, spp, 8, "mis", inter))
+        for j in jids:
+            srv.wait(j, -1)
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
+        return st, wall
+
+    total = sum(w * h * spp for (_, _, w, h, spp, _) in jobs)
+    st_trace, _ = run(4, True)
+    _, wall_mix = run(4, False)
+    _, wall_seq = run(1, False)
+    return {"trace": "Poisson 40/s for 1 s, seed %d: 60%% viewport 800x600x16 (interactive), 35%% preview "
+                     "256x256x32, 5%% F12 1920x1080x256, mis depth 8" % seed,
+            "jobs": len(jobs), "samples": total,
+            "latency_p50_ms": st_trace["latency_p50_ms"], "latency_p99_ms": st_trace["latency_p99_ms"],
+            "first_frame_p50_ms": st_trace["first_p50_ms"], "first_frame_p99_ms": st_trace["first_p99_ms"],
+            "samples_per_s_4_slots": total / wall_mix, "samples_per_s_sequential": total / wall_seq}
+
+
 def run_reference(args, rank: int):
     if rank != 0:
         return 0
@@ -207,6 +265,7 @@ def main():
     ap.add_argument("--cache", default="/tmp/lucid_bench")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-quality", action="store_true", help="skip the Cornell relMSE measurement")
+    ap.add_argument("--no-serving", action="store_true", help="skip the request-loop job trace")
     ap.add_argument("--wave", type=int, default=0, help="paths per wave (0: the engine's default)")
     ap.add_argument("--width", type=int, default=W, help="smaller frames for profiling captures")
     ap.add_argument("--height", type=int, default=H)
@@ -304,6 +363,7 @@ def main():
     mrays = (segs + shadows) / (per_step_ms[-1] / 1000.0) / 1e6
 
     quality = c1_quality(local_rank) if rank == 0 and not args.no_quality else None
+    serve = serving(local_rank) if rank == 0 and world == 1 and not args.no_serving else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -331,6 +391,7 @@ def main():
                         for k, v in kern.items()},
             "mrays_per_s": mrays, "segments_per_step": segs, "shadow_rays_per_step": shadows,
             "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": cpu, "quality": quality,
+            "serving": serve,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -8,9 +8,14 @@
 #include "../../include/lucid_cuda.h"
 #include "lucid_engine.h"
 #include "lucid_host.h"
+#include "lucid_server.h"
 
 struct LucidCudaCtx {
     lucid::Engine* engine;
+};
+
+struct LucidServer {
+    lucid::Server* server;
 };
 
 namespace {
@@ -25,6 +30,17 @@ int guarded(LucidCudaCtx* ctx, F&& f) {
         return ctx->engine->fail(LUCID_ERR_INVALID, e.what());
     } catch (...) {
         return ctx->engine->fail(LUCID_ERR_INVALID, "unknown error");
+    }
+}
+template <class F>
+int server_guarded(LucidServer* srv, F&& f) {
+    if (!srv || !srv->server) return LUCID_ERR_INVALID;
+    try {
+        return f(*srv->server);
+    } catch (const std::bad_alloc&) {
+        return srv->server->fail(LUCID_ERR_OOM, "host allocation failed");
+    } catch (const std::exception& e) {
+        return srv->server->fail(LUCID_ERR_INVALID, e.what());
     }
 }
 }  // namespace
@@ -200,6 +216,86 @@ int lucid_cuda_diag_variance_map(LucidCudaCtx* ctx, float* out, size_t cap) {
 
 int lucid_cuda_diag_top_groups(LucidCudaCtx* ctx, int n, int by_mean, LucidDiagGroup* groups, int32_t* xy, int cap) {
     return guarded(ctx, [&](lucid::Engine& e) { return e.diag_top(n, by_mean != 0, groups, xy, cap); });
+}
+
+// ---- request loop ----
+int lucid_server_create(int device, int slots, long long budget_bytes, LucidServer** out) {
+    if (!out || slots <= 0 || slots > 64) return LUCID_ERR_INVALID;
+    *out = nullptr;
+    try {
+        LucidServer* s = new LucidServer;
+        s->server = new lucid::Server(device, slots, budget_bytes);
+        *out = s;
+        return LUCID_OK;
+    } catch (...) {
+        return LUCID_ERR_OOM;
+    }
+}
+
+void lucid_server_destroy(LucidServer* srv) {
+    if (!srv) return;
+    delete srv->server;
+    delete srv;
+}
+
+const char* lucid_server_last_error(LucidServer* srv) {
+    if (!srv || !srv->server) return "invalid server";
+    return srv->server->last_error().c_str();
+}
+
+int lucid_server_add_scene(LucidServer* srv, const char* json, size_t len, int* scene_id) {
+    if (!json || !scene_id) return LUCID_ERR_INVALID;
+    return server_guarded(srv, [&](lucid::Server& s) { return s.add_scene(json, len, scene_id); });
+}
+
+int lucid_server_submit(LucidServer* srv, const LucidJobDesc* job, int* job_id) {
+    if (!job || !job_id) return LUCID_ERR_INVALID;
+    return server_guarded(srv, [&](lucid::Server& s) { return s.submit(*job, job_id); });
+}
+
+int lucid_server_job_state(LucidServer* srv, int job_id, int* samples_done) {
+    return server_guarded(srv, [&](lucid::Server& s) { return s.state(job_id, samples_done); });
+}
+
+int lucid_server_wait(LucidServer* srv, int job_id, int timeout_ms) {
+    return server_guarded(srv, [&](lucid::Server& s) { return s.wait(job_id, timeout_ms); });
+}
+
+int lucid_server_result(LucidServer* srv, int job_id, float* out_rgba, size_t cap_floats) {
+    if (!out_rgba) return LUCID_ERR_INVALID;
+    return server_guarded(srv, [&](lucid::Server& s) { return s.result(job_id, out_rgba, cap_floats); });
+}
+
+int lucid_server_cancel(LucidServer* srv, int job_id) {
+    return server_guarded(srv, [&](lucid::Server& s) { return s.cancel(job_id); });
+}
+
+int lucid_server_stats(LucidServer* srv, LucidServerStats* out) {
+    if (!out) return LUCID_ERR_INVALID;
+    return server_guarded(srv, [&](lucid::Server& s) { return s.stats(out); });
+}
+
+int lucid_admission_plan(long long budget, long long reserved, int slots, const long long* job_bytes, int n,
+                         int* decision) {
+    if (n < 0 || slots <= 0 || (n > 0 && (!job_bytes || !decision))) return LUCID_ERR_INVALID;
+    lucid::Admission a;
+    a.budget = budget;
+    a.reserved = reserved;
+    a.slots = slots;
+    std::vector<int> running;   // job indices in start order
+    int started = 0;
+    for (int i = 0; i < n; ++i) {
+        if (a.never_fits(job_bytes[i])) { decision[i] = -1; continue; }
+        while (!a.can_start(job_bytes[i])) {   // the earliest started job finishes first
+            int k = running.front();
+            running.erase(running.begin());
+            a.finish(job_bytes[k]);
+        }
+        a.start(job_bytes[i]);
+        running.push_back(i);
+        decision[i] = started++;
+    }
+    return LUCID_OK;
 }
 
 int lucid_cuda_cancel(LucidCudaCtx* ctx) {

@@ -147,6 +147,8 @@ struct FrameParams {
     int s0;          // first sample (within the call) of this wave
     int n_wave;      // paths in this wave
     int records;
+    int jitter;      // jitter camera rays even when `samples` is 1 (progressive jobs)
+    const int* dyn;  // when set, dyn[0] replaces sample_offset (graph-replayed iterations)
 };
 
 // ---------------------------------------------------------------- warp helpers
@@ -188,9 +190,10 @@ __global__ void k_raygen(FrameParams f, PathView pv) {
     int gx = f.tile_x + p % f.tile_w, gy = f.tile_y + p / f.tile_w;
     float nx = (2.0f * ((float)gx + 0.5f) / (float)f.full_w - 1.0f) * f.aspect;
     float ny = 1.0f - 2.0f * ((float)gy + 0.5f) / (float)f.full_h;
-    Rng rng = seed_xyz((uint32_t)gx, (uint32_t)gy, (uint32_t)(f.sample_offset + f.s0 + sl));
+    const int offset = f.dyn ? f.dyn[0] : f.sample_offset;
+    Rng rng = seed_xyz((uint32_t)gx, (uint32_t)gy, (uint32_t)(offset + f.s0 + sl));
     V3 d;
-    if (f.samples > 1) {
+    if (f.samples > 1 || f.jitter) {
         float jx = (randf(rng) - 0.5f) / (float)f.full_w;
         float jy = (randf(rng) - 0.5f) / (float)f.full_h;
         d = primary_dir(f, nx + jx, ny + jy);
@@ -1402,7 +1405,7 @@ __global__ void k_gather_tris(const float4* tri, const int* sorted_ids, int n, f
 static inline cudaStream_t S(void* s) { return (cudaStream_t)s; }
 
 Engine::Engine(int device) : device_(device) {
-    ds_ = new DeviceScene();
+    ds_ = std::make_shared<DeviceScene>();
     pool_ = new PathPool();
 }
 
@@ -1411,7 +1414,8 @@ Engine::~Engine() {
     cudaSetDevice(device_);
     if (async_acc_) cudaFree(async_acc_);
     if (async_pinned_) cudaFreeHost(async_pinned_);
-    if (ds_) { ds_->release(); delete ds_; }
+    job_end();
+    ds_.reset();   // the device scene is freed with its last sharing engine
     if (pool_) { pool_->release(); delete pool_; }
     delete diag_dev_;
     if (stream_) cudaStreamDestroy(S(stream_));
@@ -1451,28 +1455,65 @@ int Engine::set_wave_capacity(long long paths) {
 
 int Engine::scene_stats(int out8[8]) const {
     if (!scene_loaded_) return LUCID_ERR_NO_SCENE;
+    scene_stats_locked(out8);
+    return LUCID_OK;
+}
+
+void Engine::scene_stats_locked(int out8[8]) const {
+    if (shared_) { std::memcpy(out8, shared_stats_, 8 * sizeof(int)); return; }
     int nvol = (int)host_.volumes.size();
     out8[0] = host_.num_meshes; out8[1] = host_.num_prims; out8[2] = host_.num_native;
     out8[3] = (int)host_.lights.size(); out8[4] = host_.num_boundary_meshes; out8[5] = nvol;
     out8[6] = bvh_nodes_; out8[7] = bvh_leaves_;
-    return LUCID_OK;
 }
 
 int Engine::stats(LucidRenderStats* out) const { *out = stats_; return LUCID_OK; }
 
-void Engine::free_scene() { ds_->release(); scene_loaded_ = false; }
+void Engine::free_scene() {
+    if (ds_.use_count() > 1) ds_ = std::make_shared<DeviceScene>();   // still used by a sharing engine
+    else ds_->release();
+    scene_loaded_ = false;
+}
+
+int Engine::ensure_stream() {
+    if (stream_) return LUCID_OK;
+    cudaStream_t s;
+    CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    stream_ = s;
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, device_));
+    num_sms_ = prop.multiProcessorCount;
+    return LUCID_OK;
+}
+
+int Engine::share_scene(Engine& owner) {
+    std::shared_ptr<DeviceScene> ds;
+    int stats[8];
+    {
+        GpuLock ol(owner);
+        if (!owner.scene_loaded_) return fail(LUCID_ERR_NO_SCENE, "the sharing source has no scene");
+        ds = owner.ds_;
+        owner.scene_stats_locked(stats);
+    }
+    GpuLock gl(*this);
+    CK(cudaSetDevice(device_));
+    int rc = ensure_stream();
+    if (rc != LUCID_OK) return rc;
+    ds_ = ds;
+    std::memcpy(shared_stats_, stats, sizeof(stats));
+    shared_ = true;
+    scene_loaded_ = true;
+    return LUCID_OK;
+}
 
 int Engine::load_scene_json(const char* json, size_t len) {
     GpuLock gl(*this);
     CK(cudaSetDevice(device_));
-    if (!stream_) {
-        cudaStream_t s;
-        CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-        stream_ = s;
-        cudaDeviceProp prop;
-        CK(cudaGetDeviceProperties(&prop, device_));
-        num_sms_ = prop.multiProcessorCount;
+    {
+        int rc = ensure_stream();
+        if (rc != LUCID_OK) return rc;
     }
+    shared_ = false;
     HostScene hs;
     std::string err;
     free_scene();
@@ -1972,7 +2013,7 @@ int Engine::render_diag_impl(const LucidRenderParams& p, float* out_host, float*
     CK(cudaMemsetAsync(P.film.p, 0, np * sizeof(float4), st));
     CK(cudaMemsetAsync(P.errors.p, 0, 4 * sizeof(int), st));
 
-    FrameParams f;
+    FrameParams f{};
     for (int k = 0; k < 3; ++k) { f.pos[k] = cam_.pos[k]; f.fwd[k] = cam_.forward[k]; f.right[k] = cam_.right[k]; f.up[k] = cam_.up[k]; }
     f.aspect = (float)p.full_w / (float)p.full_h;
     f.scale = std::tan(cam_.fov * 0.5f);
@@ -2141,7 +2182,7 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
     DBuf<LucidSampleRecord> d_recs;
     if (records) CK(d_recs.alloc(np * (size_t)p.samples));
 
-    FrameParams f;
+    FrameParams f{};
     for (int k = 0; k < 3; ++k) { f.pos[k] = cam_.pos[k]; f.fwd[k] = cam_.forward[k]; f.right[k] = cam_.right[k]; f.up[k] = cam_.up[k]; }
     f.aspect = (float)p.full_w / (float)p.full_h;
     f.scale = std::tan(cam_.fov * 0.5f);
@@ -2303,6 +2344,217 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
     if (herr[0] != 0) return fail(LUCID_ERR_OVERFLOW, "BVH traversal stack overflow");
     if (status == LUCID_ERR_CANCELLED) return fail(LUCID_ERR_CANCELLED, "render cancelled");
     return LUCID_OK;
+}
+
+// ---------------------------------------------------------------- progressive jobs
+// A job renders one image progressively: each iteration adds n samples to a
+// film that keeps its sum across iterations, pixel by pixel in sample order,
+// so a job's image is bit-identical to one render call with all its samples
+// (camera rays are jittered whenever the job has more than one sample, as in
+// that call).  Iterations of `chunk` samples are captured once into a CUDA
+// graph and replayed; the sample offset comes from a device integer that a
+// one-thread kernel sets before each replay.  Nothing in an iteration waits
+// for the host, so iterations of jobs on different engines (streams) overlap
+// on the device.
+__global__ void k_set_int(int* p, int v) { *p = v; }
+
+struct JobState {
+    int w = 0, h = 0, spp = 0, depth = 8, chunk = 1;
+    bool active = false;
+    cudaGraphExec_t graph = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};   // iteration k records ev[k & 1]
+    long long issued = 0;
+    DBuf<int> dyn;
+    FrameParams f{};
+    int g_trace0 = 0, g_trace = 0, g_shade = 0, g_shadow = 0, g_bin = 0;
+};
+
+long long Engine::job_bytes(int w, int h, int chunk) {
+    const long long np = (long long)w * h;
+    return (long long)chunk * np * (168 + 5) + np * 32 + (1 << 20);
+}
+
+void Engine::enqueue_iteration(void* fp, int n) {
+    JobState& J = *job_;
+    FrameParams f = *static_cast<const FrameParams*>(fp);
+    PathPool& P = *pool_;
+    cudaStream_t st = S(stream_);
+    f.s0 = 0;
+    f.samples = n;
+    f.n_wave = n * f.npix;
+    const ShadeKernel shade = shade_kernel(algo_);
+    const int vol_bins = (algo_ == ALGO_VOLUME_MIS || algo_ == ALGO_VOLUME_SIMPLE) ? 1 : 0;
+    cudaMemsetAsync(P.counters.p, 0, sizeof(int) * kCountersPerDepth * (J.depth + 1), st);
+    k_raygen<<<(f.n_wave + 255) / 256, 256, 0, st>>>(f, P.view);
+    for (int depth = 0; depth < J.depth; ++depth) {
+        int* cnt = P.counters.p + kCountersPerDepth * depth;
+        int* cnt_next = P.counters.p + kCountersPerDepth * (depth + 1);
+        PathView pv = P.view;
+        int* qin = (depth & 1) ? P.q1.p : P.q0.p;
+        int* qout = (depth & 1) ? P.q0.p : P.q1.p;
+        pv.q0 = qin;
+        if (depth == 0) k_trace_primary<<<J.g_trace0, 128, 0, st>>>(ds_->view, pv, cnt, 0);
+        else k_trace<<<J.g_trace, 128, 0, st>>>(ds_->view, pv, cnt, 0, 0);
+        k_bin_count<<<J.g_bin, 256, 0, st>>>(ds_->view, pv, cnt, depth == 0, qin, vol_bins);
+        k_bin_scatter<<<J.g_bin, 256, 0, st>>>(pv, cnt, depth == 0, qin, P.qb.p);
+        shade<<<J.g_shade, 128, 0, st>>>(ds_->view, f, pv, cnt, cnt_next, 0, P.qb.p, qout);
+        k_shadow<<<J.g_shadow, 128, 0, st>>>(ds_->view, pv, cnt, 0);
+    }
+    k_film<<<(f.npix + 255) / 256, 256, 0, st>>>(f.npix, n, P.rad.p, P.film.p);
+}
+
+int Engine::job_begin(int w, int h, int spp, int max_depth, int chunk, bool use_graph) {
+    GpuLock gl(*this);
+    if (w <= 0 || h <= 0 || spp <= 0 || chunk <= 0) return fail(LUCID_ERR_INVALID, "job: sizes must be positive");
+    if (max_depth <= 0 || max_depth > kMaxDepth) return fail(LUCID_ERR_INVALID, "job: bad max_depth");
+    if (!scene_loaded_ || !camera_set_) return fail(LUCID_ERR_NO_SCENE, "scene or camera not set");
+    if ((long long)w * h * chunk > 0x7fffffffLL) return fail(LUCID_ERR_INVALID, "job: chunk too large");
+    CK(cudaSetDevice(device_));
+    job_end_locked();
+    if (!job_) job_ = new JobState();
+    JobState& J = *job_;
+    J.w = w; J.h = h; J.spp = spp; J.depth = max_depth; J.chunk = std::min(chunk, spp);
+    const size_t np = (size_t)w * h;
+    int rc = ensure_pool((long long)J.chunk * (long long)np, false);
+    if (rc != LUCID_OK) return rc;
+    PathPool& P = *pool_;
+    if (P.film_n < np) {
+        CK(P.film.alloc(np));
+        CK(P.out.alloc(np));
+        P.film_n = np;
+    }
+    cudaStream_t st = S(stream_);
+    CK(cudaMemsetAsync(P.film.p, 0, np * sizeof(float4), st));
+    CK(cudaMemsetAsync(P.errors.p, 0, 4 * sizeof(int), st));
+    if (!J.dyn.p) CK(J.dyn.alloc(1));
+    FrameParams& f = J.f;
+    f = FrameParams{};
+    for (int k = 0; k < 3; ++k) { f.pos[k] = cam_.pos[k]; f.fwd[k] = cam_.forward[k]; f.right[k] = cam_.right[k]; f.up[k] = cam_.up[k]; }
+    f.aspect = (float)w / (float)h;
+    f.scale = std::tan(cam_.fov * 0.5f);
+    f.tile_w = w; f.tile_h = h; f.full_w = w; f.full_h = h;
+    f.max_depth = max_depth; f.algo = algo_;
+    f.npix = (int)np;
+    f.jitter = spp > 1 ? 1 : 0;
+    int occ_t = 1, occ_s = 1, occ_h = 1, occ_t0 = 1;
+    const ShadeKernel shade = shade_kernel(algo_);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t0, k_trace_primary, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t, k_trace, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, shade, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, k_shadow, 128, 0);
+    J.g_trace0 = num_sms_ * std::max(1, occ_t0);
+    J.g_trace = num_sms_ * std::max(1, occ_t);
+    J.g_shade = num_sms_ * std::max(1, occ_s);
+    J.g_shadow = num_sms_ * std::max(1, occ_h);
+    J.g_bin = num_sms_ * 8;
+    for (int k = 0; k < 2; ++k)
+        if (!J.ev[k]) CK(cudaEventCreateWithFlags(&J.ev[k], cudaEventDisableTiming));
+    J.issued = 0;
+    J.active = true;
+    return use_graph ? capture_locked(J.chunk) : LUCID_OK;
+}
+
+// Captures one iteration of `chunk` samples into a graph (chunk <= the
+// chunk the job's path state was sized for).
+int Engine::capture_locked(int chunk) {
+    JobState& J = *job_;
+    cudaStream_t st = S(stream_);
+    if (J.graph) { cudaGraphExecDestroy(J.graph); J.graph = nullptr; }
+    FrameParams fg = J.f;
+    fg.dyn = J.dyn.p;
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    enqueue_iteration(&fg, chunk);
+    cudaError_t e = cudaStreamEndCapture(st, &graph);
+    if (e != cudaSuccess) return fail(LUCID_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&J.graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) { J.graph = nullptr; return fail(LUCID_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e)); }
+    J.chunk = chunk;
+    return LUCID_OK;
+}
+
+int Engine::job_set_chunk(int chunk, bool use_graph) {
+    GpuLock gl(*this);
+    if (!job_ || !job_->active) return fail(LUCID_ERR_INVALID, "no job");
+    if (chunk <= 0 || (long long)chunk * job_->w * job_->h > pool_->cap)
+        return fail(LUCID_ERR_INVALID, "job: chunk exceeds the job's path state");
+    CK(cudaSetDevice(device_));
+    if (use_graph) return capture_locked(chunk);
+    if (job_->graph) { cudaGraphExecDestroy(job_->graph); job_->graph = nullptr; }
+    job_->chunk = chunk;
+    return LUCID_OK;
+}
+
+int Engine::job_iterate(int sample_offset, int n) {
+    GpuLock gl(*this);
+    if (!job_ || !job_->active) return fail(LUCID_ERR_INVALID, "no job");
+    JobState& J = *job_;
+    if (n <= 0 || n > J.chunk) return fail(LUCID_ERR_INVALID, "job: iteration size must be in [1, chunk]");
+    CK(cudaSetDevice(device_));
+    cudaStream_t st = S(stream_);
+    // at most two iterations in flight per job: wait for iteration k - 2
+    if (J.issued >= 2) CK(cudaEventSynchronize(J.ev[J.issued & 1]));
+    if (J.graph && n == J.chunk) {
+        k_set_int<<<1, 1, 0, st>>>(J.dyn.p, sample_offset);
+        CK(cudaGraphLaunch(J.graph, st));
+    } else {
+        FrameParams f = J.f;
+        f.sample_offset = sample_offset;
+        enqueue_iteration(&f, n);
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(J.ev[J.issued & 1], st));
+    ++J.issued;
+    return LUCID_OK;
+}
+
+int Engine::job_wait() {
+    GpuLock gl(*this);
+    CK(cudaSetDevice(device_));
+    CK(cudaStreamSynchronize(S(stream_)));
+    int herr[4] = {0, 0, 0, 0};
+    CK(cudaMemcpy(herr, pool_->errors.p, sizeof(herr), cudaMemcpyDeviceToHost));
+    if (herr[0] != 0) return fail(LUCID_ERR_OVERFLOW, "BVH traversal stack overflow");
+    return LUCID_OK;
+}
+
+int Engine::job_output(float* out_host) {
+    GpuLock gl(*this);
+    if (!job_ || !job_->active) return fail(LUCID_ERR_INVALID, "no job");
+    JobState& J = *job_;
+    CK(cudaSetDevice(device_));
+    cudaStream_t st = S(stream_);
+    const int np = J.w * J.h;
+    k_output<<<(np + 255) / 256, 256, 0, st>>>(J.w, J.h, pool_->film.p, pool_->out.p);
+    CK(cudaMemcpyAsync(out_host, pool_->out.p, (size_t)np * sizeof(float4), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return LUCID_OK;
+}
+
+void Engine::job_end_locked() {
+    if (!job_) return;
+    if (stream_) cudaStreamSynchronize(S(stream_));
+    if (job_->graph) { cudaGraphExecDestroy(job_->graph); job_->graph = nullptr; }
+    job_->active = false;
+}
+
+void Engine::job_end() {
+    GpuLock gl(*this);
+    cudaSetDevice(device_);
+    job_end_locked();
+    if (job_)
+        for (int k = 0; k < 2; ++k)
+            if (job_->ev[k]) cudaEventDestroy(job_->ev[k]);
+    delete job_;
+    job_ = nullptr;
+}
+
+void Engine::release_pool() {
+    GpuLock gl(*this);
+    cudaSetDevice(device_);
+    if (stream_) cudaStreamSynchronize(S(stream_));
+    pool_->release();
 }
 
 // ---------------------------------------------------------------- async accumulator

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <atomic>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -17,6 +18,7 @@ namespace lucid {
 struct DeviceScene;   // device allocations of one uploaded scene
 struct PathPool;      // wavefront SoA path state
 struct DiagDevice;    // device record buffer of the path diagnostics
+struct JobState;      // progressive job (film, captured iteration graph)
 
 class Engine {
 public:
@@ -49,6 +51,17 @@ public:
     int diag_variance_map(float* out, size_t cap);
     int diag_top(int n, bool by_mean, LucidDiagGroup* groups, int32_t* xy, int cap);
     int scene_stats(int out8[8]) const;
+    // Uses `owner`'s uploaded scene (BVH, materials, lights) without a copy.
+    int share_scene(Engine& owner);
+    // Progressive jobs (the request loop's unit of work).
+    static long long job_bytes(int w, int h, int chunk);
+    int job_begin(int w, int h, int spp, int max_depth, int chunk, bool use_graph);
+    int job_set_chunk(int chunk, bool use_graph);
+    int job_iterate(int sample_offset, int n);
+    int job_wait();
+    int job_output(float* out_host);
+    void job_end();
+    void release_pool();
     int stats(LucidRenderStats* out) const;
     int set_wave_capacity(long long paths);
     int device_info(char* buf, size_t cap) const;
@@ -68,6 +81,11 @@ private:
     int ensure_pool(long long paths, bool records);
     long long default_wave_paths(bool records) const;
     int build_bvh();
+    int ensure_stream();
+    void scene_stats_locked(int out8[8]) const;
+    void enqueue_iteration(void* frame_params, int n);
+    void job_end_locked();
+    int capture_locked(int chunk);
     int build_ploc(const float4* verts, const int* sorted_ids, int n, int2* child, int2* range, float* nbox,
                    int* slot_ids, int& root);
     void free_scene();
@@ -79,7 +97,10 @@ private:
     HostCamera cam_;
     bool scene_loaded_ = false, camera_set_ = false;
     int algo_ = 1;            // "nee": PyRenderer's default (pybind_renderer.hpp:68)
-    DeviceScene* ds_ = nullptr;
+    std::shared_ptr<DeviceScene> ds_;
+    bool shared_ = false;         // ds_ belongs to another engine (share_scene)
+    int shared_stats_[8] = {};
+    JobState* job_ = nullptr;
     PathPool* pool_ = nullptr;
     long long wave_cap_ = 0;  // 0 = automatic
     std::atomic<bool> cancel_{false};

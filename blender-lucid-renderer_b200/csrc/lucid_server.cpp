@@ -1,0 +1,314 @@
+// lucid_server.cpp — the request loop (see lucid_server.h).
+#include "lucid_server.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+
+#include "lucid_engine.h"
+
+namespace lucid {
+
+namespace {
+// Largest wave a job may use (paths per iteration) and the iteration time
+// an interactive job aims for.
+constexpr long long kJobWavePaths = 1LL << 24;
+constexpr double kInteractiveMs = 33.0;
+
+double percentile(std::vector<double> v, double q) {
+    if (v.empty()) return 0.0;
+    std::sort(v.begin(), v.end());
+    double pos = q * (double)(v.size() - 1);
+    size_t lo = (size_t)pos, hi = std::min(lo + 1, v.size() - 1);
+    return v[lo] + (v[hi] - v[lo]) * (pos - (double)lo);
+}
+}  // namespace
+
+double Server::now() const {
+    using namespace std::chrono;
+    return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+Server::Server(int device, int slots, long long budget_bytes) : device_(device) {
+    slots = std::max(1, slots);
+    if (budget_bytes <= 0) {
+        size_t free_b = 0, total_b = 0;
+        cudaSetDevice(device);
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) budget_bytes = (long long)(free_b * 0.8);
+        else budget_bytes = 1LL << 30;
+    }
+    budget_ = budget_bytes;
+    adm_.budget = budget_bytes;
+    adm_.slots = slots;
+    t0_ = now();
+    for (int s = 0; s < slots; ++s) {
+        slot_eng_.emplace_back(new Engine(device));
+        slot_scene_.push_back(-1);
+    }
+    for (int s = 0; s < slots; ++s) threads_.emplace_back([this, s] { slot_loop(s); });
+}
+
+Server::~Server() {
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        stop_ = true;
+        for (auto& kv : jobs_) kv.second.cancel = true;
+    }
+    cv_.notify_all();
+    for (auto& t : threads_) t.join();
+    slot_eng_.clear();
+    scenes_.clear();
+}
+
+int Server::add_scene(const char* json, size_t len, int* scene_id) {
+    size_t f0 = 0, f1 = 0, tot = 0;
+    cudaSetDevice(device_);
+    cudaMemGetInfo(&f0, &tot);
+    std::unique_ptr<Engine> e(new Engine(device_));
+    int rc = e->load_scene_json(json, len);
+    if (rc != LUCID_OK) return fail(rc, e->last_error());
+    cudaMemGetInfo(&f1, &tot);
+    std::lock_guard<std::mutex> lk(mu_);
+    long long bytes = f0 > f1 ? (long long)(f0 - f1) : 0;
+    scenes_.push_back(std::move(e));
+    scene_bytes_.push_back(bytes);
+    adm_.reserved += bytes;
+    *scene_id = (int)scenes_.size() - 1;
+    return LUCID_OK;
+}
+
+int Server::submit(const LucidJobDesc& d, int* job_id) {
+    if (d.width <= 0 || d.height <= 0 || d.samples <= 0 || d.max_depth <= 0 || d.max_depth > 1024)
+        return fail(LUCID_ERR_INVALID, "job: sizes must be positive (max_depth <= 1024)");
+    std::unique_lock<std::mutex> lk(mu_);
+    if (d.scene < 0 || d.scene >= (int)scenes_.size()) return fail(LUCID_ERR_INVALID, "job: unknown scene");
+    int id = next_id_++;
+    Job& j = jobs_[id];
+    j.d = d;
+    j.d.algorithm[sizeof(j.d.algorithm) - 1] = 0;
+    j.t_submit = now();
+    const long long np = (long long)d.width * d.height;
+    // the largest samples per iteration within the wave limit and the budget
+    int cmax = (int)std::max(1LL, std::min<long long>(d.samples, kJobWavePaths / std::max(1LL, np)));
+    while (cmax > 1 && adm_.never_fits(Engine::job_bytes(d.width, d.height, cmax))) cmax /= 2;
+    j.chunk_max = cmax;
+    j.bytes = Engine::job_bytes(d.width, d.height, j.chunk_max);
+    *job_id = id;
+    if (adm_.never_fits(j.bytes)) {
+        j.state = LUCID_JOB_REFUSED;
+        j.t_end = now();
+        j.error = "job needs " + std::to_string(j.bytes) + " bytes; the budget leaves " +
+                  std::to_string(adm_.budget - adm_.reserved);
+        done_cv_.notify_all();
+        return fail(LUCID_ERR_OOM, j.error);
+    }
+    queue_.push_back(id);
+    lk.unlock();
+    cv_.notify_all();
+    return LUCID_OK;
+}
+
+void Server::slot_loop(int slot) {
+    for (;;) {
+        int id = -1;
+        Job* j = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(mu_);
+            cv_.wait(lk, [&] {
+                if (stop_) return true;
+                while (!queue_.empty() && jobs_[queue_.front()].cancel) {   // drop cancelled queued jobs
+                    Job& c = jobs_[queue_.front()];
+                    c.state = LUCID_JOB_CANCELLED;
+                    c.t_end = now();
+                    queue_.pop_front();
+                    done_cv_.notify_all();
+                }
+                return !queue_.empty() && adm_.can_start(jobs_[queue_.front()].bytes);
+            });
+            if (stop_) return;
+            id = queue_.front();
+            queue_.pop_front();
+            j = &jobs_[id];
+            adm_.start(j->bytes);
+            j->state = LUCID_JOB_RUNNING;
+            j->t_start = now();
+            if (busy_from_ < 0) busy_from_ = j->t_start;
+        }
+        cv_.notify_all();   // another slot may start the next job too
+        int rc = run_job(slot, *j, id);
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            adm_.finish(j->bytes);
+            j->t_end = now();
+            busy_to_ = std::max(busy_to_, j->t_end);
+            if (rc == LUCID_OK && !j->cancel) {
+                j->state = LUCID_JOB_DONE;
+                samples_done_ += (long long)j->d.samples * j->d.width * j->d.height;
+            } else {
+                j->state = j->cancel ? LUCID_JOB_CANCELLED : LUCID_JOB_FAILED;
+            }
+        }
+        cv_.notify_all();
+        done_cv_.notify_all();
+    }
+}
+
+// Autotuner: the first iterations of a job shape (scene, size, integrator,
+// depth, interactivity) try 1, 2, 4, ... samples per iteration; the size with
+// the most samples per second wins (for interactive jobs among those whose
+// iteration stays under kInteractiveMs) and is cached for the shape.  The
+// trial iterations are part of the job's own samples.
+int Server::pick_chunk(Engine& e, Job& j, int id, int& offset) {
+    const LucidJobDesc& d = j.d;
+    std::string key = std::to_string(d.scene) + ":" + std::to_string(d.width) + "x" + std::to_string(d.height) + ":" +
+                      d.algorithm + ":" + std::to_string(d.max_depth) + ":" + std::to_string(d.interactive);
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        auto it = tuned_.find(key);
+        if (it != tuned_.end()) return std::min(it->second, j.chunk_max);
+    }
+    int best = 1;
+    double best_rate = -1.0;
+    for (int c = 1; c <= j.chunk_max && offset + c <= d.samples; c *= 2) {
+        auto t = std::chrono::steady_clock::now();
+        int rc = e.job_iterate(offset, c);
+        if (rc == LUCID_OK) rc = e.job_wait();
+        if (rc != LUCID_OK) return -rc;
+        double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
+        offset += c;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            j.done = offset;
+            if (j.t_first == 0) j.t_first = now();
+        }
+        double rate = c / std::max(ms, 1e-3);
+        bool ok = !d.interactive || ms <= kInteractiveMs || c == 1;
+        if (ok && rate > best_rate) { best_rate = rate; best = c; }
+        if (d.interactive && ms > kInteractiveMs) break;
+    }
+    (void)id;
+    std::lock_guard<std::mutex> lk(mu_);
+    tuned_[key] = best;
+    return best;
+}
+
+int Server::run_job(int slot, Job& j, int id) {
+    Engine& e = *slot_eng_[slot];
+    const LucidJobDesc& d = j.d;
+    int rc = LUCID_OK;
+    if (slot_scene_[slot] != d.scene) {
+        rc = e.share_scene(*scenes_[d.scene]);
+        if (rc != LUCID_OK) { j.error = e.last_error(); return rc; }
+        slot_scene_[slot] = d.scene;
+    }
+    const float* c = d.camera;
+    e.set_camera(c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7], c[8], c[9]);
+    e.set_algorithm(d.algorithm);
+    rc = e.job_begin(d.width, d.height, d.samples, d.max_depth, j.chunk_max, false);
+    if (rc != LUCID_OK) { j.error = e.last_error(); e.job_end(); e.release_pool(); return rc; }
+    int offset = 0;
+    int chunk = pick_chunk(e, j, id, offset);
+    if (chunk < 0) { j.error = e.last_error(); e.job_end(); e.release_pool(); return -chunk; }
+    if (offset < d.samples) {
+        rc = e.job_set_chunk(chunk, d.samples - offset >= 2 * chunk);
+        while (rc == LUCID_OK && offset < d.samples) {
+            if (j.cancel) break;
+            int n = std::min(chunk, d.samples - offset);
+            rc = e.job_iterate(offset, n);
+            offset += n;
+            std::lock_guard<std::mutex> lk(mu_);
+            // iteration k returns once iteration k - 2 has finished
+            j.done = std::max(j.done, std::max(0, offset - 2 * chunk));
+            if (j.t_first == 0 && offset > 2 * chunk) j.t_first = now();
+        }
+    }
+    if (rc == LUCID_OK) rc = e.job_wait();
+    if (rc == LUCID_OK && !j.cancel) {
+        std::vector<float> img((size_t)d.width * d.height * 4);
+        rc = e.job_output(img.data());
+        std::lock_guard<std::mutex> lk(mu_);
+        if (rc == LUCID_OK) {
+            j.image.swap(img);
+            j.done = d.samples;
+            if (j.t_first == 0) j.t_first = now();
+        }
+    }
+    if (rc != LUCID_OK) j.error = e.last_error();
+    e.job_end();
+    e.release_pool();
+    return rc;
+}
+
+int Server::state(int job, int* samples_done) {
+    std::lock_guard<std::mutex> lk(mu_);
+    auto it = jobs_.find(job);
+    if (it == jobs_.end()) return fail(LUCID_ERR_INVALID, "unknown job");
+    if (samples_done) *samples_done = it->second.done;
+    return it->second.state;
+}
+
+int Server::wait(int job, int timeout_ms) {
+    std::unique_lock<std::mutex> lk(mu_);
+    auto it = jobs_.find(job);
+    if (it == jobs_.end()) return fail(LUCID_ERR_INVALID, "unknown job");
+    auto finished = [&] { int s = jobs_[job].state; return s != LUCID_JOB_QUEUED && s != LUCID_JOB_RUNNING; };
+    if (timeout_ms < 0) done_cv_.wait(lk, finished);
+    else done_cv_.wait_for(lk, std::chrono::milliseconds(timeout_ms), finished);
+    return jobs_[job].state;
+}
+
+int Server::result(int job, float* out, size_t cap_floats) {
+    std::lock_guard<std::mutex> lk(mu_);
+    auto it = jobs_.find(job);
+    if (it == jobs_.end()) return fail(LUCID_ERR_INVALID, "unknown job");
+    Job& j = it->second;
+    if (j.state != LUCID_JOB_DONE) return fail(LUCID_ERR_INVALID, "job has no image" + (j.error.empty() ? "" : ": " + j.error));
+    if (cap_floats < j.image.size()) return fail(LUCID_ERR_INVALID, "result buffer too small");
+    std::memcpy(out, j.image.data(), j.image.size() * sizeof(float));
+    return LUCID_OK;
+}
+
+int Server::cancel(int job) {
+    std::lock_guard<std::mutex> lk(mu_);
+    auto it = jobs_.find(job);
+    if (it == jobs_.end()) return fail(LUCID_ERR_INVALID, "unknown job");
+    it->second.cancel = true;
+    cv_.notify_all();
+    return LUCID_OK;
+}
+
+int Server::stats(LucidServerStats* out) {
+    std::lock_guard<std::mutex> lk(mu_);
+    std::memset(out, 0, sizeof(*out));
+    std::vector<double> lat, first;
+    for (auto& kv : jobs_) {
+        const Job& j = kv.second;
+        ++out->submitted;
+        switch (j.state) {
+            case LUCID_JOB_DONE:
+                ++out->done;
+                lat.push_back(j.t_end - j.t_submit);
+                first.push_back(j.t_first - j.t_submit);
+                break;
+            case LUCID_JOB_REFUSED: ++out->refused; break;
+            case LUCID_JOB_RUNNING: ++out->running; break;
+            case LUCID_JOB_QUEUED: ++out->queued; break;
+            default: break;
+        }
+    }
+    out->latency_p50_ms = percentile(lat, 0.50);
+    out->latency_p99_ms = percentile(lat, 0.99);
+    out->first_p50_ms = percentile(first, 0.50);
+    out->first_p99_ms = percentile(first, 0.99);
+    double busy = busy_to_ - busy_from_;
+    out->samples_per_s = (busy_from_ >= 0 && busy > 0) ? (double)samples_done_ / (busy / 1000.0) : 0.0;
+    out->bytes_reserved = adm_.reserved;
+    out->bytes_running = adm_.running;
+    out->budget_bytes = adm_.budget;
+    return LUCID_OK;
+}
+
+}  // namespace lucid

@@ -1,0 +1,95 @@
+// lucid_server.h — the device-resident request loop.
+//
+// Lucid's concurrent sessions (viewport, F12 render, material previews: one
+// Renderer each in the Blender add-on, render_session.py:77-106) become jobs
+// of one server.  A job renders a whole image progressively on one of a few
+// slots; each slot is an engine with its own CUDA stream sharing the
+// uploaded scenes, so iterations of different jobs overlap on the device.
+// Jobs are admitted in arrival order as slots and device memory free up
+// (HBM budget = uploaded scenes + every running job's path state and film);
+// a job that could never fit is refused at submission.  Each slot picks the
+// samples per iteration (the queue capacity of its waves) with a small
+// autotuner and replays the iteration as a CUDA graph.  A job's image
+// depends only on its own sample indices, so it is the same alone and in
+// any mix, bit for bit, and equals one render call with all its samples.
+#pragma once
+
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/lucid_cuda.h"
+
+namespace lucid {
+
+class Engine;
+
+// FIFO admission under a byte budget: the head job starts when a slot is
+// free and reserved + running + its bytes fit; a job larger than budget -
+// reserved is refused.  Shared by the server and by the host-only planner.
+struct Admission {
+    long long budget = 0, reserved = 0, running = 0;
+    int slots = 1, busy = 0;
+    bool never_fits(long long bytes) const { return reserved + bytes > budget; }
+    bool can_start(long long bytes) const { return busy < slots && reserved + running + bytes <= budget; }
+    void start(long long bytes) { running += bytes; ++busy; }
+    void finish(long long bytes) { running -= bytes; --busy; }
+};
+
+class Server {
+public:
+    Server(int device, int slots, long long budget_bytes);
+    ~Server();
+    int add_scene(const char* json, size_t len, int* scene_id);
+    int submit(const LucidJobDesc& d, int* job_id);
+    int state(int job, int* samples_done);
+    int wait(int job, int timeout_ms);
+    int result(int job, float* out, size_t cap_floats);
+    int cancel(int job);
+    int stats(LucidServerStats* out);
+    const std::string& last_error() const { return err_; }
+    int fail(int code, const std::string& m) { err_ = m; return code; }
+
+private:
+    struct Job {
+        LucidJobDesc d{};
+        int state = LUCID_JOB_QUEUED;
+        int done = 0;
+        long long bytes = 0;
+        int chunk_max = 1;
+        bool cancel = false;
+        double t_submit = 0, t_start = 0, t_first = 0, t_end = 0;
+        std::vector<float> image;
+        std::string error;
+    };
+    void slot_loop(int slot);
+    int run_job(int slot, Job& j, int id);
+    int pick_chunk(Engine& e, Job& j, int id, int& offset);
+    double now() const;
+
+    int device_;
+    long long budget_;
+    std::vector<std::unique_ptr<Engine>> scenes_;
+    std::vector<long long> scene_bytes_;
+    std::vector<std::unique_ptr<Engine>> slot_eng_;
+    std::vector<int> slot_scene_;
+    std::vector<std::thread> threads_;
+    std::mutex mu_;
+    std::condition_variable cv_, done_cv_;
+    std::deque<int> queue_;
+    std::map<int, Job> jobs_;
+    std::map<std::string, int> tuned_;   // autotuned samples per iteration
+    Admission adm_;
+    int next_id_ = 1;
+    bool stop_ = false;
+    double t0_ = 0, busy_from_ = -1, busy_to_ = 0;
+    long long samples_done_ = 0;
+    std::string err_;
+};
+
+}  // namespace lucid

@@ -75,6 +75,23 @@ DIAG_PIXEL_DTYPE = np.dtype([("valid", np.int32), ("sample_count", np.uint32), (
 DIAG_STATS_FIELDS = ("total_samples", "active_pixels", "total_groups", "total_overflow", "paths_recorded")
 
 
+class JobDesc(ctypes.Structure):
+    _fields_ = [("scene", ctypes.c_int), ("camera", ctypes.c_float * 10), ("algorithm", ctypes.c_char * 16),
+                ("width", ctypes.c_int), ("height", ctypes.c_int), ("samples", ctypes.c_int),
+                ("max_depth", ctypes.c_int), ("interactive", ctypes.c_int)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_int), ("done", ctypes.c_int), ("refused", ctypes.c_int),
+                ("running", ctypes.c_int), ("queued", ctypes.c_int),
+                ("latency_p50_ms", ctypes.c_double), ("latency_p99_ms", ctypes.c_double),
+                ("first_p50_ms", ctypes.c_double), ("first_p99_ms", ctypes.c_double),
+                ("samples_per_s", ctypes.c_double), ("bytes_reserved", ctypes.c_longlong),
+                ("bytes_running", ctypes.c_longlong), ("budget_bytes", ctypes.c_longlong)]
+
+
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_REFUSED, JOB_FAILED, JOB_CANCELLED = range(6)
+
 # Every symbol include/lucid_cuda.h declares, with its ctypes signature.
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -110,6 +127,17 @@ SIGNATURES = {
     "lucid_cuda_diag_pixel": (_I, [_P, _I, _I, _I, _P, _P, _I]),
     "lucid_cuda_diag_variance_map": (_I, [_P, _P, ctypes.c_size_t]),
     "lucid_cuda_diag_top_groups": (_I, [_P, _I, _I, _P, _P, _I]),
+    "lucid_server_create": (_I, [_I, _I, ctypes.c_longlong, ctypes.POINTER(_P)]),
+    "lucid_server_destroy": (None, [_P]),
+    "lucid_server_last_error": (ctypes.c_char_p, [_P]),
+    "lucid_server_add_scene": (_I, [_P, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(_I)]),
+    "lucid_server_submit": (_I, [_P, ctypes.POINTER(JobDesc), ctypes.POINTER(_I)]),
+    "lucid_server_job_state": (_I, [_P, _I, ctypes.POINTER(_I)]),
+    "lucid_server_wait": (_I, [_P, _I, _I]),
+    "lucid_server_result": (_I, [_P, _I, _P, ctypes.c_size_t]),
+    "lucid_server_cancel": (_I, [_P, _I]),
+    "lucid_server_stats": (_I, [_P, ctypes.POINTER(ServerStats)]),
+    "lucid_admission_plan": (_I, [ctypes.c_longlong, ctypes.c_longlong, _I, _P, _I, _P]),
     "lucid_cuda_cancel": (_I, [_P]),
     "lucid_cuda_is_cancelled": (_I, [_P]),
     "lucid_cuda_reset_cancel": (_I, [_P]),
@@ -337,3 +365,87 @@ class Context:
         m = self._count(self.lib.lucid_cuda_diag_top_groups(self.h, n, int(by_mean), groups.ctypes.data,
                                                             xy.ctypes.data, groups.size))
         return groups[:m], xy[:m]
+
+
+def admission_plan(budget: int, reserved: int, slots: int, job_bytes) -> list:
+    """The server's admission policy run on the host (no GPU): the start order
+    of each job when jobs finish in start order, or -1 when it is refused."""
+    lib = load_library()
+    b = np.asarray(job_bytes, np.int64)
+    out = np.zeros(len(b), np.int32)
+    rc = lib.lucid_admission_plan(int(budget), int(reserved), int(slots), b.ctypes.data, len(b), out.ctypes.data)
+    if rc != LUCID_OK:
+        raise LucidError(rc, "admission plan")
+    return out.tolist()
+
+
+class Server:
+    """Several progressive render jobs on one device (the request loop)."""
+
+    def __init__(self, device: int = 0, slots: int = 4, budget_bytes: int = 0):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        rc = self.lib.lucid_server_create(device, slots, budget_bytes, ctypes.byref(h))
+        if rc != LUCID_OK:
+            raise LucidError(rc, "server create failed")
+        self.h = h
+        self._sizes = {}
+
+    def close(self):
+        if self.h:
+            self.lib.lucid_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _err(self, rc):
+        raise LucidError(rc, self.lib.lucid_server_last_error(self.h).decode())
+
+    def add_scene(self, json_text: str) -> int:
+        b = json_text.encode()
+        sid = ctypes.c_int()
+        rc = self.lib.lucid_server_add_scene(self.h, b, len(b), ctypes.byref(sid))
+        if rc != LUCID_OK:
+            self._err(rc)
+        return sid.value
+
+    def submit(self, scene: int, camera, width: int, height: int, samples: int, max_depth: int = 8,
+               algorithm: str = "mis", interactive: bool = False, check: bool = True):
+        d = JobDesc(scene, (ctypes.c_float * 10)(*[float(c) for c in camera]), algorithm.encode(), width, height,
+                    samples, max_depth, int(interactive))
+        jid = ctypes.c_int()
+        rc = self.lib.lucid_server_submit(self.h, ctypes.byref(d), ctypes.byref(jid))
+        self._sizes[jid.value] = (height, width)
+        if rc != LUCID_OK and check:
+            self._err(rc)
+        return jid.value
+
+    def state(self, job: int):
+        n = ctypes.c_int()
+        st = self.lib.lucid_server_job_state(self.h, job, ctypes.byref(n))
+        return st, n.value
+
+    def wait(self, job: int, timeout_ms: int = -1) -> int:
+        return self.lib.lucid_server_wait(self.h, job, timeout_ms)
+
+    def result(self, job: int) -> np.ndarray:
+        h, w = self._sizes[job]
+        img = np.zeros((h, w, 4), np.float32)
+        rc = self.lib.lucid_server_result(self.h, job, img.ctypes.data, img.size)
+        if rc != LUCID_OK:
+            self._err(rc)
+        return img
+
+    def cancel(self, job: int):
+        self.lib.lucid_server_cancel(self.h, job)
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        rc = self.lib.lucid_server_stats(self.h, ctypes.byref(st))
+        if rc != LUCID_OK:
+            self._err(rc)
+        return {f: getattr(st, f) for f, _ in ServerStats._fields_}

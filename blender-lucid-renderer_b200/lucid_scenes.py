@@ -347,5 +347,22 @@ def mirror_point_light_scene():
     return scene, camera
 
 
+def material_preview_scene(seed: int = 0):
+    """A material-preview shot: a subdivision-4 icosphere (5,120 triangles,
+    smooth normals) with seeded random Principled parameters on a plane,
+    lit by a square area light and a dim environment."""
+    rng = np.random.default_rng(seed)
+    v, t = icosphere(4)
+    mat = material(tuple(rng.uniform(0.05, 0.95, 3)), float(rng.random() < 0.3), float(rng.uniform(0.02, 1.0)),
+                   transmission=float(rng.random() < 0.1))
+    meshes = [mesh(*quad((-3, 0, -3), (-3, 0, 3), (3, 0, 3), (3, 0, -3)), material((0.5, 0.5, 0.5), 0.0, 0.8)),
+              mesh(v * 0.8 + np.array([0.0, 0.8, 0.0]), t, mat, vertex_normals(v, t)[t], True)]
+    lights = [{"type": "AREA", "position": [1.5, 3.0, 2.0], "direction": [-0.4, -1.0, -0.5], "right": [1, 0, 0],
+               "up": [0, 0, 1], "shape": "SQUARE", "size": 1.5, "color": [1, 1, 1], "energy": 200.0}]
+    scene = {"meshes": meshes, "native_lights": lights, "environment": {"color": [0.2, 0.22, 0.25], "strength": 1.0}}
+    camera = (0.0, 1.2, 3.2, 0.0, -0.15, -1.0, 0.0, 1.0, 0.0, 40.0)
+    return scene, camera
+
+
 def scene_triangle_count(scene: dict) -> int:
     return int(sum(len(m["triangles"]) for m in scene["meshes"]))

@@ -253,6 +253,58 @@ int lucid_cuda_diag_variance_map(LucidCudaCtx* ctx, float* out, size_t cap);
  * number copied. */
 int lucid_cuda_diag_top_groups(LucidCudaCtx* ctx, int n, int by_mean, LucidDiagGroup* groups, int32_t* xy, int cap);
 
+/* ---- request loop (several jobs on one device) ------------------------- */
+/* No reference counterpart: the reference runs one Renderer per Blender
+ * session (viewport, F12 render, material preview; render_session.py:77-106),
+ * each rendering on its own.  Here those sessions submit jobs to one server:
+ * jobs are admitted in arrival order as slots and device memory free up,
+ * run concurrently on per-slot CUDA streams, and each job's image is the
+ * same, bit for bit, as one lucid_cuda_render call with all its samples. */
+typedef struct LucidServer LucidServer;
+
+typedef struct LucidJobDesc {
+    int scene;            /* id returned by lucid_server_add_scene */
+    float camera[10];     /* position, direction, up, vertical fov (degrees) */
+    char algorithm[16];   /* "simple", "nee", "mis", "volume_simple", "volume_mis" */
+    int width, height, samples, max_depth;
+    int interactive;      /* 1: keep each iteration short (viewport); 0: throughput */
+} LucidJobDesc;
+
+enum { LUCID_JOB_QUEUED = 0, LUCID_JOB_RUNNING = 1, LUCID_JOB_DONE = 2, LUCID_JOB_REFUSED = 3,
+       LUCID_JOB_FAILED = 4, LUCID_JOB_CANCELLED = 5 };
+
+typedef struct LucidServerStats {
+    int submitted, done, refused, running, queued;
+    double latency_p50_ms, latency_p99_ms;   /* submit -> image ready, finished jobs */
+    double first_p50_ms, first_p99_ms;       /* submit -> first iteration finished */
+    double samples_per_s;                    /* samples of finished jobs / busy wall time */
+    long long bytes_reserved, bytes_running, budget_bytes;
+} LucidServerStats;
+
+/* slots: concurrent jobs; budget_bytes: device memory the server may use
+ * (0 = 80 % of the free memory). */
+int lucid_server_create(int device, int slots, long long budget_bytes, LucidServer** out);
+void lucid_server_destroy(LucidServer* srv);
+const char* lucid_server_last_error(LucidServer* srv);
+/* Parses, uploads and builds the BVH once; jobs name the scene by its id. */
+int lucid_server_add_scene(LucidServer* srv, const char* json, size_t len, int* scene_id);
+/* Queues a job (LUCID_ERR_OOM and state REFUSED when it can never fit). */
+int lucid_server_submit(LucidServer* srv, const LucidJobDesc* job, int* job_id);
+/* Returns the job's LUCID_JOB_* state; samples_done may be NULL. */
+int lucid_server_job_state(LucidServer* srv, int job_id, int* samples_done);
+/* Waits until the job has finished (or timeout_ms, < 0 = no limit): returns its state. */
+int lucid_server_wait(LucidServer* srv, int job_id, int timeout_ms);
+/* The finished image: width * height * 4 floats, sum over samples, Y-flipped
+ * (the layout of lucid_cuda_render). */
+int lucid_server_result(LucidServer* srv, int job_id, float* out_rgba, size_t cap_floats);
+int lucid_server_cancel(LucidServer* srv, int job_id);
+int lucid_server_stats(LucidServer* srv, LucidServerStats* out);
+/* The server's admission policy on its own (host only, no GPU): n jobs of
+ * job_bytes[i] arrive in order; decision[i] = the start order of job i
+ * (0, 1, ...) when jobs finish in start order, or -1 when it is refused. */
+int lucid_admission_plan(long long budget, long long reserved, int slots, const long long* job_bytes, int n,
+                         int* decision);
+
 /* ---- cancellation ---------------------------------------------------- */
 /* Replaces PyRenderer::cancel / is_cancelled / reset_cancel
  * (pybind_renderer.hpp:86-102).  Thread-safe. */

@@ -15,7 +15,7 @@ def declared_symbols():
         if fn.endswith(".h"):
             text = open(os.path.join(REPO, "include", fn)).read()
             text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-            names |= set(re.findall(r"\b(lucid_cuda_\w+)\s*\(", text))
+            names |= set(re.findall(r"\b(lucid_\w+)\s*\(", text))
     return names
 
 

@@ -1,0 +1,117 @@
+"""The request loop: admission by device-memory budget (host-side policy,
+no GPU) and, on the GPU, jobs whose images are the same alone and in a mix
+of concurrent jobs, bit for bit, and equal to one render call with all
+their samples."""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+import pytest
+
+import lucid_capi
+import lucid_scenes as ls
+from parity_util import scene_and_camera
+
+
+def test_admission_refuses_jobs_that_never_fit():
+    assert lucid_capi.admission_plan(100, 20, 2, [30, 30, 50, 90, 10]) == [0, 1, 2, -1, 3]
+    assert lucid_capi.admission_plan(100, 0, 4, [101, 100, 1]) == [-1, 0, 1]
+    assert lucid_capi.admission_plan(10, 10, 1, [1]) == [-1]
+
+
+def test_admission_is_first_come_first_served_within_slots_and_budget():
+    # 3 slots, room for two 40-byte jobs at a time: arrival order is kept
+    assert lucid_capi.admission_plan(100, 20, 3, [40, 40, 40, 5, 40]) == [0, 1, 2, 3, 4]
+    # one slot: strictly sequential
+    assert lucid_capi.admission_plan(1 << 40, 0, 1, [1, 2, 3]) == [0, 1, 2]
+    assert lucid_capi.admission_plan(100, 0, 2, []) == []
+
+
+def test_server_rejects_bad_arguments_without_a_gpu():
+    lib = lucid_capi.load_library()
+    assert lib.lucid_server_create(0, 0, 0, None) == lucid_capi.LUCID_ERR_INVALID
+    assert lib.lucid_server_submit(None, None, None) == lucid_capi.LUCID_ERR_INVALID
+    assert lib.lucid_server_wait(None, 1, 0) == lucid_capi.LUCID_ERR_INVALID
+
+
+JOBS = [  # scene, algorithm, width, height, samples, depth, interactive
+    ("cornell", "mis", 64, 48, 16, 8, False),
+    ("all_lights_novol", "nee", 80, 60, 8, 6, False),
+    ("procedural_small", "mis", 96, 64, 24, 8, False),
+    ("cornell", "mis", 32, 32, 64, 8, True),
+    ("all_lights_novol", "mis", 40, 30, 1, 4, True),
+]
+
+
+def _single_call(workdir, name, algo, w, h, spp, depth):
+    scene, cam = scene_and_camera(name, workdir)
+    ctx = lucid_capi.Context(0)
+    ctx.load_scene_json(ls.to_json(scene))
+    ctx.set_camera(*cam)
+    ctx.set_algorithm(algo)
+    img, _, _ = ctx.render(w, h, w, h, spp, 0, depth)
+    ctx.close()
+    return img
+
+
+def _submit_all(srv, ids, workdir, jobs):
+    out = []
+    for name, algo, w, h, spp, depth, inter in jobs:
+        _, cam = scene_and_camera(name, workdir)
+        out.append(srv.submit(ids[name], cam, w, h, spp, depth, algo, inter))
+    return out
+
+
+@pytest.mark.gpu
+def test_jobs_equal_alone_in_a_mix_and_one_render_call(workdir):
+    names = sorted({j[0] for j in JOBS})
+    want = [_single_call(workdir, n, a, w, h, s, d) for n, a, w, h, s, d, _ in JOBS]
+
+    alone = []
+    srv = lucid_capi.Server(0, slots=1)
+    ids = {n: srv.add_scene(ls.to_json(scene_and_camera(n, workdir)[0])) for n in names}
+    for job in JOBS:
+        jid = _submit_all(srv, ids, workdir, [job])[0]
+        assert srv.wait(jid, 60000) == lucid_capi.JOB_DONE
+        alone.append(srv.result(jid))
+    srv.close()
+
+    srv = lucid_capi.Server(0, slots=3)
+    ids = {n: srv.add_scene(ls.to_json(scene_and_camera(n, workdir)[0])) for n in names}
+    jids = _submit_all(srv, ids, workdir, JOBS + JOBS)   # every job twice, all at once
+    for jid in jids:
+        assert srv.wait(jid, 60000) == lucid_capi.JOB_DONE
+    mixed = [srv.result(j) for j in jids]
+    st = srv.stats()
+    srv.close()
+
+    for k in range(len(JOBS)):
+        np.testing.assert_array_equal(alone[k], want[k])
+        np.testing.assert_array_equal(mixed[k], want[k])
+        np.testing.assert_array_equal(mixed[k + len(JOBS)], want[k])
+    assert st["done"] == 2 * len(JOBS) and st["refused"] == 0
+    assert st["latency_p99_ms"] >= st["latency_p50_ms"] > 0 and st["samples_per_s"] > 0
+    assert st["bytes_running"] == 0
+
+
+@pytest.mark.gpu
+def test_budget_refusal_and_cancel(workdir):
+    scene, cam = scene_and_camera("cornell", workdir)
+    srv = lucid_capi.Server(0, slots=1, budget_bytes=64 << 20)
+    sid = srv.add_scene(ls.to_json(scene))
+    # 4096 x 4096 needs far more than 64 MB of film and path state
+    big = srv.submit(sid, cam, 4096, 4096, 64, 8, "mis", check=False)
+    assert srv.state(big)[0] == lucid_capi.JOB_REFUSED
+    assert srv.wait(big, 0) == lucid_capi.JOB_REFUSED
+    with pytest.raises(lucid_capi.LucidError):
+        srv.result(big)
+    long_job = srv.submit(sid, cam, 256, 256, 100000, 8, "mis")
+    queued = srv.submit(sid, cam, 64, 64, 4, 8, "mis")
+    time.sleep(0.2)
+    srv.cancel(long_job)
+    assert srv.wait(long_job, 60000) == lucid_capi.JOB_CANCELLED
+    assert srv.wait(queued, 60000) == lucid_capi.JOB_DONE
+    st = srv.stats()
+    assert st["refused"] == 1 and st["done"] == 1
+    srv.close()
