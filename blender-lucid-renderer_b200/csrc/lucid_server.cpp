@@ -105,7 +105,14 @@ int Server::submit(const LucidJobDesc& d, int* job_id) {
         done_cv_.notify_all();
         return fail(LUCID_ERR_OOM, j.error);
     }
-    queue_.push_back(id);
+    // interactive jobs (viewport ticks) queue ahead of batch jobs; arrival
+    // order holds within each class
+    if (d.interactive) {
+        auto it = std::find_if(queue_.begin(), queue_.end(), [&](int q) { return !jobs_[q].d.interactive; });
+        queue_.insert(it, id);
+    } else {
+        queue_.push_back(id);
+    }
     lk.unlock();
     cv_.notify_all();
     return LUCID_OK;

@@ -5,7 +5,8 @@
 // of one server.  A job renders a whole image progressively on one of a few
 // slots; each slot is an engine with its own CUDA stream sharing the
 // uploaded scenes, so iterations of different jobs overlap on the device.
-// Jobs are admitted in arrival order as slots and device memory free up
+// Jobs are admitted in arrival order (interactive jobs ahead of batch jobs)
+// as slots and device memory free up
 // (HBM budget = uploaded scenes + every running job's path state and film);
 // a job that could never fit is refused at submission.  Each slot picks the
 // samples per iteration (the queue capacity of its waves) with a small
