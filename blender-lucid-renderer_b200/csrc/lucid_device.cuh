@@ -368,7 +368,7 @@ struct LightSample {
 // Not inlined: the shading kernel samples lights at two call sites (volume
 // scatter and surface NEE) and is limited by instruction fetch; one shared
 // copy measured 3.6 % faster on the 1M-triangle frame.
-__device__ __noinline__ LightSample sample_light(const DevLight& L, V3 sp, float u1, float u2) {
+static __device__ __noinline__ LightSample sample_light(const DevLight& L, V3 sp, float u1, float u2) {
     LightSample s;
     int type = __float_as_int(L.pos_type.w);
     s.emission = c3(L.emission_radius);

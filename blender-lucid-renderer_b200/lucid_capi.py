@@ -138,6 +138,16 @@ SIGNATURES = {
     "lucid_server_cancel": (_I, [_P, _I]),
     "lucid_server_stats": (_I, [_P, ctypes.POINTER(ServerStats)]),
     "lucid_admission_plan": (_I, [ctypes.c_longlong, ctypes.c_longlong, _I, _P, _I, _P]),
+    "lucid_guide_create": (_I, [_I, _I, ctypes.POINTER(_P)]),
+    "lucid_guide_destroy": (None, [_P]),
+    "lucid_guide_last_error": (ctypes.c_char_p, [_P]),
+    "lucid_guide_num_params": (_I, []),
+    "lucid_guide_get_params": (_I, [_P, _P, ctypes.c_size_t]),
+    "lucid_guide_set_params": (_I, [_P, _P, ctypes.c_size_t]),
+    "lucid_guide_forward": (_I, [_P, _P, _I, _P]),
+    "lucid_guide_encode": (_I, [_P, _P, _P, _P, _I, _P]),
+    "lucid_guide_gradient": (_I, [_P, _P, _I, _P]),
+    "lucid_guide_train": (_I, [_P, _P, _I, ctypes.c_float]),
     "lucid_cuda_cancel": (_I, [_P]),
     "lucid_cuda_is_cancelled": (_I, [_P]),
     "lucid_cuda_reset_cancel": (_I, [_P]),

@@ -305,6 +305,36 @@ int lucid_server_stats(LucidServer* srv, LucidServerStats* out);
 int lucid_admission_plan(long long budget, long long reserved, int slots, const long long* job_bytes, int n,
                          int* decision);
 
+/* ---- path-guiding network ------------------------------------------------ */
+/* No reference counterpart.  The guide of the `mis` integrator (see
+ * lucid_cuda_guide_enable) on its own: an MLP from 176 encoded inputs
+ * (position in [0,1]^3 of the scene box: sin/cos of pi 2^j x, j < 16, per
+ * axis; normal; one-blob(32) of (cos theta + 1)/2 and phi/(2 pi) + 1/2 of the
+ * outgoing direction; zero padding) through three 64-wide ReLU layers to 48
+ * raw outputs (8 lobe logits, 8 softplus concentrations, 8 x 3 mean
+ * directions, padding), BF16 on the tensor cores with FP32 accumulation and
+ * FP32 master weights.  Parameter layout: W1[64][176] b1[64] W2[64][64] b2[64]
+ * W3[64][64] b3[64] W4[48][64] b4[48].  A training record is 16 floats:
+ * position01[3], normal[3], wo[3], wi[3], pdf, radiance[3]; the loss is
+ * -sum_s c_s log q(wi_s) with c_s proportional to luminance / pdf, summing
+ * to 1 over the batch. */
+typedef struct LucidGuide LucidGuide;
+int lucid_guide_create(int device, int seed, LucidGuide** out);
+void lucid_guide_destroy(LucidGuide* guide);
+const char* lucid_guide_last_error(LucidGuide* guide);
+int lucid_guide_num_params(void);
+int lucid_guide_get_params(LucidGuide* guide, float* out, size_t cap);
+int lucid_guide_set_params(LucidGuide* guide, const float* params, size_t n);
+/* n x 176 inputs -> n x 48 raw outputs */
+int lucid_guide_forward(LucidGuide* guide, const float* inputs, int n, float* outputs);
+/* n (position01, normal, wo) triples -> n x 176 inputs */
+int lucid_guide_encode(LucidGuide* guide, const float* p01, const float* normal, const float* wo, int n,
+                       float* out);
+/* loss gradient of n records (parameter layout above); the network is unchanged */
+int lucid_guide_gradient(LucidGuide* guide, const float* records, int n, float* grad_out);
+/* one Adam step (beta 0.9 / 0.999, eps 1e-8) on n records */
+int lucid_guide_train(LucidGuide* guide, const float* records, int n, float lr);
+
 /* ---- cancellation ---------------------------------------------------- */
 /* Replaces PyRenderer::cancel / is_cancelled / reset_cancel
  * (pybind_renderer.hpp:86-102).  Thread-safe. */
