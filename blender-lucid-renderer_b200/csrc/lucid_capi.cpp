@@ -298,6 +298,14 @@ int lucid_admission_plan(long long budget, long long reserved, int slots, const 
     return LUCID_OK;
 }
 
+int lucid_cuda_guide_enable(LucidCudaCtx* ctx, int on, int seed) {
+    return guarded(ctx, [&](lucid::Engine& e) { return e.guide_enable(on != 0, seed); });
+}
+
+int lucid_cuda_guide_steps(LucidCudaCtx* ctx) {
+    return guarded(ctx, [&](lucid::Engine& e) { return e.guide_steps(); });
+}
+
 int lucid_cuda_cancel(LucidCudaCtx* ctx) {
     if (!ctx || !ctx->engine) return LUCID_ERR_INVALID;
     ctx->engine->cancel();

@@ -27,6 +27,8 @@
 
 #include "lucid_diag.h"
 #include "lucid_engine.h"
+#include "lucid_guide.cuh"
+#include "lucid_guide_host.h"
 #include "lucid_kernels.cuh"
 
 namespace lucid {
@@ -98,6 +100,15 @@ struct PathView {
     int2* rec_prim;
     int4* rec_cnt;     // bounces, nee tests, nee occluded
     unsigned long long* rec_hash;
+    // path guiding (null when off)
+    float* gmix;       // 40 raw network outputs per path (k_guide_infer)
+    int4* gslot;       // training records of the path's 3 latest guided vertices (-1: none)
+    float4* ginv;      // 3 per path: 1 / throughput after each of those vertices
+    GuideRec* grec;    // training records of this wave
+    int* gcount;       // [0] records written, [1] guided vertices
+    int gcap;
+    unsigned gkeep;    // a guided vertex is recorded when its hash < gkeep
+    float glo[3], gscale[3];   // scene box -> [0,1]^3
 };
 constexpr int kCountersPerDepth = 48;
 constexpr int kBins = 16;
@@ -130,6 +141,22 @@ struct PathPool {
         film64_n = 0;
         cap = 0;
     }
+};
+
+// Path guiding: the network and the per-path / per-wave buffers.
+constexpr int kGuideBatch = 1 << 18;   // training records per step
+constexpr long long kGuideWave = 1LL << 24;
+struct GuideState {
+    GuideNet net;
+    DBuf<float> gmix;
+    DBuf<int4> gslot;
+    DBuf<float4> ginv;
+    DBuf<GuideRec> recs;
+    DBuf<int> count;
+    long long cap = 0;
+    float keep = 1.0f;
+    float lr = 1e-2f;
+    bool on = false;
 };
 
 // Completed-path records of the path diagnostics and their count.
@@ -339,11 +366,34 @@ struct ShadeResult {
 // terms, NEE, BSDF sampling and Russian roulette.  ALGO is the integrator as
 // a compile-time constant, so each integrator's kernel carries only its own
 // branches.
-template <int ALGO>
+// Adds a radiance contribution c (already weighted by the path throughput)
+// to the training records of the path's guided vertices from slot `from` on
+// (c / throughput-after-vertex = radiance that arrived along its sample).
+LD void guide_credit(const PathView& pv, int id, RGB c, int from) {
+    int4 s = pv.gslot[id];
+    const int r[3] = {s.x, s.y, s.z};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        if (k < from || r[k] < 0) continue;
+        float4 iv = pv.ginv[3 * id + k];
+        GuideRec& g = pv.grec[r[k]];
+        g.L[0] += c.r * iv.x; g.L[1] += c.g * iv.y; g.L[2] += c.b * iv.z;
+    }
+}
+
+// A surface the guide may sample: no transmission lobe and not the
+// near-delta metal that sample_bsdf weights in closed form.
+LD bool guide_eligible(const DevMaterial& dm) {
+    float rough = smax(dm.rough_trans_ior_flags.x, MIN_ROUGHNESS);
+    return dm.rough_trans_ior_flags.y == 0.0f && !(rough < 0.05f && dm.albedo_metallic.w > 0.5f);
+}
+
+template <int ALGO, bool GUIDE = false>
 LD ShadeResult shade_path(const DevScene& sc, const FrameParams& f, const PathView& pv, int id) {
     ShadeResult out;
     out.cont = false;
     out.shadow = false;
+    int pushed = 0;
     constexpr int algo = ALGO;
     constexpr bool nee = algo == ALGO_NEE || algo == ALGO_MIS || algo == ALGO_VOLUME_MIS;
     constexpr bool mis = algo == ALGO_MIS || algo == ALGO_VOLUME_MIS;
@@ -445,6 +495,7 @@ LD ShadeResult shade_path(const DevScene& sc, const FrameParams& f, const PathVi
                 }
                 float mw = (last_pdf > MIN_PDF && lpdf > MIN_PDF) ? mis_power(last_pdf, lpdf) : 1.0f;
                 result = result + mul(T, em) * mw;
+                if (GUIDE) guide_credit(pv, id, mul(T, em) * mw, 0);
             } else {
                 result = result + mul(T, em);
             }
@@ -452,6 +503,7 @@ LD ShadeResult shade_path(const DevScene& sc, const FrameParams& f, const PathVi
         }
         if (!has_hit) {
             result = result + mul(T, rgb(sc.env[0], sc.env[1], sc.env[2]));
+            if (GUIDE) guide_credit(pv, id, mul(T, rgb(sc.env[0], sc.env[1], sc.env[2])), 0);
             break;
         }
         // surface hit: point and normal from (t, u, v, prim) as in bvh.hpp:108-128
@@ -493,8 +545,21 @@ LD ShadeResult shade_path(const DevScene& sc, const FrameParams& f, const PathVi
                 }
             }
             result = result + mul(T, em) * mw;
+            if (GUIDE) guide_credit(pv, id, mul(T, em) * mw, 0);
         }
         bool transmissive = m.transmission > 0.5f;
+        const bool guided = GUIDE && guide_eligible(dm);
+        GuideMix gm;
+        if (guided) {
+            float raw[kGOut];
+            const float4* src = reinterpret_cast<const float4*>(pv.gmix + (size_t)id * 40);
+#pragma unroll
+            for (int k = 0; k < 10; ++k) {
+                float4 v = src[k];
+                raw[4 * k] = v.x; raw[4 * k + 1] = v.y; raw[4 * k + 2] = v.z; raw[4 * k + 3] = v.w;
+            }
+            guide_mix_from_raw(raw, gm);
+        }
         if (nee && sc.num_lights > 0 && !has_em && !transmissive) {
             float usel = randf(rng);
             int li = select_light(sc, usel);
@@ -511,6 +576,7 @@ LD ShadeResult shade_path(const DevScene& sc, const FrameParams& f, const PathVi
                         RGB c;
                         if (mis) {
                             float pb = pdf_bsdf(m, wo, ls.dir, sn);
+                            if (guided) pb = 0.5f * pb + 0.5f * guide_pdf(gm, ls.dir);
                             float mw = mis_power(pl, pb);
                             RGB bw = bsdf_weight(fb, nl, pl);
                             if (algo == ALGO_VOLUME_MIS) {
@@ -530,27 +596,70 @@ LD ShadeResult shade_path(const DevScene& sc, const FrameParams& f, const PathVi
             }
         }
         V3 smp_n = (m.transmission > 0.5f) ? n : sn;
-        float u1 = randf(rng), u2 = randf(rng), u3 = randf(rng);
-        BsdfSample bs = sample_bsdf(m, wo, smp_n, u1, u2, u3, rng);
-        if (!(bs.kind == BS_PRECOMP || bs.pdf > MIN_PDF)) break;
-        RGB w;
-        if (bs.kind == BS_PRECOMP) {
-            w = bs.f;
+        V3 wi;
+        float gpdf = 0.0f;
+        if (guided) {
+            // one-sample MIS of BSDF and guide sampling, 1/2 each (balance heuristic)
+            float usel = randf(rng);
+            float u1 = randf(rng), u2 = randf(rng), u3 = randf(rng);
+            if (usel < 0.5f) wi = sample_bsdf(m, wo, smp_n, u1, u2, u3, rng).wi;
+            else wi = guide_sample(gm, u1, u2, u3);
+            float c = dot(smp_n, wi);
+            if (c <= 1e-6f) break;
+            gpdf = 0.5f * pdf_bsdf(m, wo, wi, smp_n) + 0.5f * guide_pdf(gm, wi);
+            if (!(gpdf > MIN_PDF)) break;
+            T = mul(T, bsdf_weight(eval_bsdf(m, wo, wi, smp_n), c, gpdf));
+            last_pdf = gpdf;
         } else {
-            float c = fabsf(dot(smp_n, bs.wi));
-            if (c <= 1e-6f || bs.pdf < MIN_PDF) break;
-            w = bsdf_weight(bs.f, c, bs.pdf);
+            float u1 = randf(rng), u2 = randf(rng), u3 = randf(rng);
+            BsdfSample bs = sample_bsdf(m, wo, smp_n, u1, u2, u3, rng);
+            if (!(bs.kind == BS_PRECOMP || bs.pdf > MIN_PDF)) break;
+            RGB w;
+            if (bs.kind == BS_PRECOMP) {
+                w = bs.f;
+            } else {
+                float c = fabsf(dot(smp_n, bs.wi));
+                if (c <= 1e-6f || bs.pdf < MIN_PDF) break;
+                w = bsdf_weight(bs.f, c, bs.pdf);
+            }
+            T = mul(T, w);
+            if (mis) last_pdf = (bs.kind == BS_EVAL) ? bs.pdf : 0.0f;
+            wi = bs.wi;
         }
-        T = mul(T, w);
-        if (mis) last_pdf = (bs.kind == BS_EVAL) ? bs.pdf : 0.0f;
         if (depth >= 3) {
             float rr = smin(smax3(T.r, T.g, T.b), 0.95f);
             if (randf(rng) > rr) break;
             T = T * (1.0f / rr);
         }
         if (!rgb_valid(T)) break;
-        new_o = p; new_d = bs.wi;
+        new_o = p; new_d = wi;
         out.cont = true;
+        if (guided) {
+            atomicAdd(&pv.gcount[1], 1);
+            unsigned hsh = murmur3_finalize((unsigned)id * 0x9E3779B9u ^ (unsigned)(depth + 1) * 0x85EBCA6Bu);
+            if (hsh < pv.gkeep) {
+                int r = atomicAdd(&pv.gcount[0], 1);
+                if (r < pv.gcap) {
+                    GuideRec g;
+                    g.p[0] = (p.x - pv.glo[0]) * pv.gscale[0];
+                    g.p[1] = (p.y - pv.glo[1]) * pv.gscale[1];
+                    g.p[2] = (p.z - pv.glo[2]) * pv.gscale[2];
+                    g.n[0] = n.x; g.n[1] = n.y; g.n[2] = n.z;
+                    g.wo[0] = wo.x; g.wo[1] = wo.y; g.wo[2] = wo.z;
+                    g.wi[0] = wi.x; g.wi[1] = wi.y; g.wi[2] = wi.z;
+                    g.pdf = gpdf;
+                    g.L[0] = g.L[1] = g.L[2] = 0.0f;
+                    pv.grec[r] = g;
+                    int4 sl = pv.gslot[id];
+                    pv.gslot[id] = make_int4(r, sl.x, sl.y, -1);
+                    pv.ginv[3 * id + 2] = pv.ginv[3 * id + 1];
+                    pv.ginv[3 * id + 1] = pv.ginv[3 * id];
+                    pv.ginv[3 * id] = make_float4(T.r > 0.0f ? 1.0f / T.r : 0.0f, T.g > 0.0f ? 1.0f / T.g : 0.0f,
+                                                  T.b > 0.0f ? 1.0f / T.b : 0.0f, 0.0f);
+                    pushed = 1;
+                }
+            }
+        }
     } while (0);
 
     if (out.cont && depth + 1 >= f.max_depth) out.cont = false;
@@ -563,7 +672,9 @@ LD ShadeResult shade_path(const DevScene& sc, const FrameParams& f, const PathVi
     }
     if (out.shadow) {
         pv.sh_o[id] = make_float4(sh_o.x, sh_o.y, sh_o.z, sh_len);
-        pv.sh_d[id] = make_float4(sh_d.x, sh_d.y, sh_d.z, 0.0f);
+        // w: the first guide slot the NEE contribution credits (a vertex's
+        // own light sample did not arrive along its sampled direction)
+        pv.sh_d[id] = make_float4(sh_d.x, sh_d.y, sh_d.z, __int_as_float(pushed));
         pv.sh_c[id] = make_float4(sh_inc.r, sh_inc.g, sh_inc.b, 0.0f);
     }
     return out;
@@ -573,7 +684,7 @@ LD ShadeResult shade_path(const DevScene& sc, const FrameParams& f, const PathVi
 // hundred bytes of spills): the extra warps hide more of the shading
 // kernel's instruction-fetch and memory latency than the spills cost
 // (measured on the 1M-triangle scene: 4, 5, 6, 7, 8 CTAs per SM).
-template <int ALGO>
+template <int ALGO, bool GUIDE = false>
 __global__ void __launch_bounds__(128, 8) k_shade(DevScene sc, FrameParams f, PathView pv, int* cnt, int* cnt_next,
                                                int identity, int* qin, int* qout) {
     const int n = *(volatile int*)&cnt[0];
@@ -587,7 +698,7 @@ __global__ void __launch_bounds__(128, 8) k_shade(DevScene sc, FrameParams f, Pa
         r.shadow = false;
         if (i < n) {
             id = identity ? i : qin[i];
-            r = shade_path<ALGO>(sc, f, pv, id);
+            r = shade_path<ALGO, GUIDE>(sc, f, pv, id);
         }
         warp_append(qout, &cnt_next[0], id, r.cont);
         warp_append(pv.qs, &cnt[1], id, r.shadow);
@@ -595,7 +706,8 @@ __global__ void __launch_bounds__(128, 8) k_shade(DevScene sc, FrameParams f, Pa
 }
 
 using ShadeKernel = void (*)(DevScene, FrameParams, PathView, int*, int*, int, int*, int*);
-static ShadeKernel shade_kernel(int algo) {
+static ShadeKernel shade_kernel(int algo, bool guide = false) {
+    if (guide && algo == ALGO_MIS) return k_shade<ALGO_MIS, true>;
     switch (algo) {
         case ALGO_SIMPLE: return k_shade<ALGO_SIMPLE>;
         case ALGO_MIS: return k_shade<ALGO_MIS>;
@@ -676,6 +788,71 @@ __global__ void __launch_bounds__(256) k_bin_scatter(PathView pv, int* cnt, int 
     }
 }
 
+// ---------------------------------------------------------------- guide inference
+// Raw guide outputs for every queued path whose next event is a guidable
+// surface hit: 16 paths per warp-tile through the BF16 tensor-core MLP, the
+// weights staged once per block in shared memory.
+constexpr size_t kInferSmem = sizeof(GuideSmemW) + 4 * sizeof(GuideTile);
+
+__global__ void __launch_bounds__(128) k_guide_infer(DevScene sc, PathView pv, int* cnt, int identity, const int* qin,
+                                                     const __nv_bfloat16* wq, const float* master) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    GuideSmemW& W = *reinterpret_cast<GuideSmemW*>(smem);
+    GuideTile* tiles = reinterpret_cast<GuideTile*>(smem + sizeof(GuideSmemW));
+    guide_load_weights(W, wq, master);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    GuideTile& T = tiles[warp];
+    const int n = *(volatile int*)&cnt[0];
+    const int ntiles = (n + 15) / 16;
+    for (int tile = blockIdx.x * 4 + warp; tile < ntiles; tile += gridDim.x * 4) {
+        int id = -1;
+        bool elig = false;
+        if (lane < 16) {
+            const int i = tile * 16 + lane;
+            __nv_bfloat16* row = T.x + lane * kLdIn;
+            if (i < n) {
+                id = identity ? i : qin[i];
+                float4 hh = pv.hit[id];
+                int prim = __float_as_int(hh.w);
+                float2 lh = pv.lhit[id];
+                int li = __float_as_int(lh.x);
+                if (prim >= 0 && !(li >= 0 && lh.y < hh.x)) {
+                    int4 pi = sc.prim_info[prim];
+                    elig = guide_eligible(sc.materials[pi.x]);
+                    if (elig) {
+                        float4 ro = pv.ray_o[id], rd = pv.ray_d[id];
+                        V3 o = f3(ro), d = f3(rd);
+                        V3 p = o + d * hh.x;
+                        V3 fn = f3(sc.prim_fn[prim]);
+                        V3 nn = fn;
+                        if (pi.w) {
+                            float w = 1.0f - hh.y - hh.z;
+                            V3 ni = f3(sc.prim_vn[3 * prim]) * w + f3(sc.prim_vn[3 * prim + 1]) * hh.y +
+                                    f3(sc.prim_vn[3 * prim + 2]) * hh.z;
+                            nn = make_dir_or(ni, fn);
+                        }
+                        V3 p01 = v3((p.x - pv.glo[0]) * pv.gscale[0], (p.y - pv.glo[1]) * pv.gscale[1],
+                                    (p.z - pv.glo[2]) * pv.gscale[2]);
+                        guide_encode(p01, nn, -d, [&](int k, float v) { row[k] = __float2bfloat16(v); });
+                    }
+                }
+            }
+            if (!elig)
+                for (int k = 0; k < kGIn; ++k) row[k] = __float2bfloat16(0.0f);
+        }
+        __syncwarp();
+        guide_forward_tile(W, T);
+        if (lane < 16 && elig) {
+            float4* dst = reinterpret_cast<float4*>(pv.gmix + (size_t)id * 40);
+            const float* r = T.raw + lane * kGOut;
+#pragma unroll
+            for (int k = 0; k < 10; ++k) dst[k] = make_float4(r[4 * k], r[4 * k + 1], r[4 * k + 2], r[4 * k + 3]);
+        }
+        __syncwarp();
+    }
+}
+
 // ---------------------------------------------------------------- shadow
 // Shadow rays (persistent, dynamic refill): is_shadowed_skipping_volume_
 // boundaries (path_tracer.hpp:103-119) with any-hit BVH queries; a segment
@@ -741,6 +918,7 @@ __global__ void __launch_bounds__(128) k_shadow(DevScene sc, PathView pv, int* c
         if (!occ) {
             float4 ra = pv.rad[id], c = pv.sh_c[id];
             pv.rad[id] = make_float4(ra.x + c.x, ra.y + c.y, ra.z + c.z, 0.0f);
+            if (pv.grec) guide_credit(pv, id, rgb(c.x, c.y, c.z), __float_as_int(pv.sh_d[id].w));
         }
         if (records) {
             int4 rc = pv.rec_cnt[id];
@@ -1415,6 +1593,7 @@ Engine::~Engine() {
     if (async_acc_) cudaFree(async_acc_);
     if (async_pinned_) cudaFreeHost(async_pinned_);
     job_end();
+    delete guide_;
     ds_.reset();   // the device scene is freed with its last sharing engine
     if (pool_) { pool_->release(); delete pool_; }
     delete diag_dev_;
@@ -1666,6 +1845,7 @@ int Engine::build_bvh() {
     for (const DevVolume& vol : H.volumes)
         for (int a = 0; a < 3; ++a)
             maxabs = std::max(maxabs, std::max(std::fabs(vol.wmin[a]), std::fabs(vol.wmax[a])));
+    for (int a = 0; a < 3; ++a) { scene_lo_[a] = lo[a]; scene_hi_[a] = hi[a]; }
     float sdiag = std::sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
                             (hi[2] - lo[2]) * (hi[2] - lo[2]));
     const int kMaxBig = 32;
@@ -1936,10 +2116,14 @@ namespace {
 //           + binned id 4                                            = 38 / path
 constexpr double kBytesTrace = 60, kBytesShade = 340, kBytesShadow = 84, kBytesRaygen = 80, kBytesFilm = 16,
                  kBytesBin = 38;
-enum Kind { K_RAYGEN, K_TRACE0, K_TRACE, K_SHADE, K_SHADOW, K_FILM, K_BIN, K_NUM };
-const char* kKindNames[K_NUM] = {"k_raygen", "k_trace_primary", "k_trace", "k_shade", "k_shadow", "k_film", "k_bin"};
+//   guide : queue 4 + hit 24 + ray 32 + raw outputs 160 w              = 220 / path
+//   train : one record 64 / record (weights are read from shared memory)
+enum Kind { K_RAYGEN, K_TRACE0, K_TRACE, K_SHADE, K_SHADOW, K_FILM, K_BIN, K_GUIDE, K_TRAIN, K_NUM };
+const char* kKindNames[K_NUM] = {"k_raygen", "k_trace_primary", "k_trace", "k_shade", "k_shadow", "k_film", "k_bin",
+                                 "k_guide_infer", "k_guide_train"};
 const double kKindBytes[K_NUM] = {kBytesRaygen, kBytesTrace, kBytesTrace, kBytesShade, kBytesShadow, kBytesFilm,
-                                  kBytesBin};
+                                  kBytesBin, 220, 64};
+static_assert(K_NUM <= LUCID_MAX_KERNEL_KINDS, "kernel kinds");
 }  // namespace
 
 // Default paths per wave: large waves keep every depth's launches full and
@@ -2158,7 +2342,9 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
     cudaStream_t st = S(stream_);
     const bool profile = (p.flags & LUCID_RENDER_PROFILE) != 0;
     const bool records = recs != nullptr;
+    const bool guide = guide_ && guide_->on && algo_ == ALGO_MIS && !from_async;
     long long cap = wave_cap_ > 0 ? wave_cap_ : default_wave_paths(records);
+    if (guide) cap = std::min(cap, kGuideWave);
     int spw = (int)std::max<long long>(1, std::min<long long>(p.samples, cap / (long long)np));
     long long wave_paths = (long long)spw * (long long)np;
     int rc = ensure_pool(wave_paths, records);
@@ -2196,13 +2382,31 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
     int occ_t = 1, occ_s = 1, occ_h = 1, occ_t0 = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t0, k_trace_primary, 128, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t, k_trace, 128, 0);
-    const ShadeKernel shade = shade_kernel(algo_);
+    const ShadeKernel shade = shade_kernel(algo_, guide);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, shade, 128, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, k_shadow, 128, 0);
     const int g_trace0 = num_sms_ * std::max(1, occ_t0);
     const int g_trace = num_sms_ * std::max(1, occ_t), g_shade = num_sms_ * std::max(1, occ_s),
               g_shadow = num_sms_ * std::max(1, occ_h);
     const int g_bin = num_sms_ * 8;
+    PathView gv = P.view;   // the path view with the guide's buffers when guiding
+    if (guide) {
+        int rc2 = guide_buffers(wave_paths);
+        if (rc2 != LUCID_OK) return rc2;
+        GuideState& G = *guide_;
+        gv.gmix = G.gmix.p; gv.gslot = G.gslot.p; gv.ginv = G.ginv.p; gv.grec = G.recs.p; gv.gcount = G.count.p;
+        gv.gcap = kGuideBatch;
+        for (int k = 0; k < 3; ++k) {
+            gv.glo[k] = scene_lo_[k];
+            float ext = scene_hi_[k] - scene_lo_[k];
+            gv.gscale[k] = ext > 0.0f ? 1.0f / ext : 0.0f;
+        }
+        static bool attr = false;
+        if (!attr) {
+            CK(cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInferSmem));
+            attr = true;
+        }
+    }
     const char* sort_env = std::getenv("LUCID_SHADE_BINS");
     const bool bin = !(sort_env && sort_env[0] == '0');
     const int vol_bins = (algo_ == ALGO_VOLUME_MIS || algo_ == ALGO_VOLUME_SIMPLE) ? 1 : 0;
@@ -2236,13 +2440,19 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
         f.s0 = s0;
         f.n_wave = (int)((long long)this_spw * (long long)np);
         CK(cudaMemsetAsync(P.counters.p, 0, sizeof(int) * kCountersPerDepth * (p.max_depth + 1), st));
+        if (guide) {
+            GuideState& G = *guide_;
+            gv.gkeep = (unsigned)std::min(4294967295.0, (double)G.keep * 4294967296.0);
+            CK(cudaMemsetAsync(G.gslot.p, 0xff, (size_t)f.n_wave * sizeof(int4), st));
+            CK(cudaMemsetAsync(G.count.p, 0, 2 * sizeof(int), st));
+        }
         int e = ev_begin(K_RAYGEN, 0);
         k_raygen<<<(f.n_wave + 255) / 256, 256, 0, st>>>(f, P.view);
         ev_end(e);
         for (int depth = 0; depth < p.max_depth; ++depth) {
             int* cnt = P.counters.p + kCountersPerDepth * depth;
             int* cnt_next = P.counters.p + kCountersPerDepth * (depth + 1);
-            PathView pv = P.view;
+            PathView pv = gv;
             // queue ping-pong: depth d reads q[d&1] and writes q[(d+1)&1]
             int* qin = (depth & 1) ? P.q1.p : P.q0.p;
             int* qout = (depth & 1) ? P.q0.p : P.q1.p;
@@ -2255,6 +2465,13 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
                 k_trace<<<g_trace, 128, 0, st>>>(ds_->view, pv, cnt, 0, f.records);
             }
             ev_end(e);
+            if (guide) {
+                e = ev_begin(K_GUIDE, depth);
+                k_guide_infer<<<num_sms_ * 2, 128, kInferSmem, st>>>(
+                    ds_->view, pv, cnt, depth == 0, qin, static_cast<const __nv_bfloat16*>(guide_->net.weights_bf16()),
+                    guide_->net.master());
+                ev_end(e);
+            }
             if (bin) {
                 e = ev_begin(K_BIN, depth);
                 k_bin_count<<<g_bin, 256, 0, st>>>(ds_->view, pv, cnt, depth == 0, qin, vol_bins);
@@ -2280,7 +2497,21 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
         if (records) k_records<<<(f.n_wave + 255) / 256, 256, 0, st>>>(f, P.view, d_recs.p);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(hcnt.data(), P.counters.p, hcnt.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
+        int gcnt[2] = {0, 0};
+        if (guide) CK(cudaMemcpyAsync(gcnt, guide_->count.p, sizeof(gcnt), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        if (guide) {
+            // one Adam step on this wave's records; next wave's sampling rate
+            // aims at 90 % of a training batch
+            GuideState& G = *guide_;
+            int nrec = std::min(gcnt[0], kGuideBatch);
+            e = ev_begin(K_TRAIN, 0);
+            if (nrec > 0 && G.net.train_step(G.recs.p, nrec, st, G.lr) != 0)
+                return fail(LUCID_ERR_CUDA, "guide training: " + G.net.error());
+            ev_end(e);
+            if (profile) kind_units[K_TRAIN] += nrec;
+            G.keep = (float)std::min(1.0, 0.9 * kGuideBatch / std::max(1.0, (double)gcnt[1]));
+        }
         for (int d = 0; d < p.max_depth; ++d) {
             seg += hcnt[kCountersPerDepth * d];
             shadows += hcnt[kCountersPerDepth * d + 1];
@@ -2292,6 +2523,7 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
                 kind_units[d == 0 ? K_TRACE0 : K_TRACE] += hcnt[kCountersPerDepth * d];
                 kind_units[K_SHADE] += hcnt[kCountersPerDepth * d];
                 if (bin) kind_units[K_BIN] += hcnt[kCountersPerDepth * d];
+                if (guide) kind_units[K_GUIDE] += hcnt[kCountersPerDepth * d];
                 kind_units[K_SHADOW] += hcnt[kCountersPerDepth * d + 1];
             }
         }
@@ -2345,6 +2577,39 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
     if (status == LUCID_ERR_CANCELLED) return fail(LUCID_ERR_CANCELLED, "render cancelled");
     return LUCID_OK;
 }
+
+// ---------------------------------------------------------------- path guiding (host)
+int Engine::guide_buffers(long long paths) {
+    GuideState& G = *guide_;
+    if (G.cap < paths) {
+        CK(G.gmix.alloc((size_t)paths * 40));
+        CK(G.gslot.alloc((size_t)paths));
+        CK(G.ginv.alloc((size_t)paths * 3));
+        G.cap = paths;
+    }
+    if (!G.recs.p) CK(G.recs.alloc(kGuideBatch));
+    if (!G.count.p) CK(G.count.alloc(2));
+    return LUCID_OK;
+}
+
+int Engine::guide_enable(bool on, int seed) {
+    GpuLock gl(*this);
+    CK(cudaSetDevice(device_));
+    if (!on) {
+        if (guide_) guide_->on = false;
+        return LUCID_OK;
+    }
+    int rc = ensure_stream();
+    if (rc != LUCID_OK) return rc;
+    if (!guide_) guide_ = new GuideState();
+    if (guide_->net.init(seed, S(stream_)) != 0) return fail(LUCID_ERR_CUDA, "guide init: " + guide_->net.error());
+    CK(cudaStreamSynchronize(S(stream_)));
+    guide_->keep = 1.0f;
+    guide_->on = true;
+    return LUCID_OK;
+}
+
+int Engine::guide_steps() const { return guide_ ? guide_->net.steps() : 0; }
 
 // ---------------------------------------------------------------- progressive jobs
 // A job renders one image progressively: each iteration adds n samples to a

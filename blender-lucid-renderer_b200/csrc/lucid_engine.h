@@ -19,6 +19,7 @@ struct DeviceScene;   // device allocations of one uploaded scene
 struct PathPool;      // wavefront SoA path state
 struct DiagDevice;    // device record buffer of the path diagnostics
 struct JobState;      // progressive job (film, captured iteration graph)
+struct GuideState;    // path-guiding network and its per-path buffers
 
 class Engine {
 public:
@@ -51,6 +52,9 @@ public:
     int diag_variance_map(float* out, size_t cap);
     int diag_top(int n, bool by_mean, LucidDiagGroup* groups, int32_t* xy, int cap);
     int scene_stats(int out8[8]) const;
+    // Online-trained path guiding for the `mis` integrator (reseeds the network).
+    int guide_enable(bool on, int seed);
+    int guide_steps() const;
     // Uses `owner`'s uploaded scene (BVH, materials, lights) without a copy.
     int share_scene(Engine& owner);
     // Progressive jobs (the request loop's unit of work).
@@ -82,6 +86,7 @@ private:
     long long default_wave_paths(bool records) const;
     int build_bvh();
     int ensure_stream();
+    int guide_buffers(long long paths);
     void scene_stats_locked(int out8[8]) const;
     void enqueue_iteration(void* frame_params, int n);
     void job_end_locked();
@@ -101,6 +106,8 @@ private:
     bool shared_ = false;         // ds_ belongs to another engine (share_scene)
     int shared_stats_[8] = {};
     JobState* job_ = nullptr;
+    GuideState* guide_ = nullptr;
+    float scene_lo_[3] = {0, 0, 0}, scene_hi_[3] = {1, 1, 1};
     PathPool* pool_ = nullptr;
     long long wave_cap_ = 0;  // 0 = automatic
     std::atomic<bool> cancel_{false};

@@ -52,7 +52,7 @@ class KernelStat(ctypes.Structure):
 class RenderStats(ctypes.Structure):
     _fields_ = [("total_ms", ctypes.c_double), ("paths", ctypes.c_double), ("segments", ctypes.c_double),
                 ("shadow_rays", ctypes.c_double), ("waves", ctypes.c_int), ("num_kinds", ctypes.c_int),
-                ("kinds", KernelStat * 8)]
+                ("kinds", KernelStat * 12)]
 
 
 class DiagConfig(ctypes.Structure):
@@ -148,6 +148,8 @@ SIGNATURES = {
     "lucid_guide_encode": (_I, [_P, _P, _P, _P, _I, _P]),
     "lucid_guide_gradient": (_I, [_P, _P, _I, _P]),
     "lucid_guide_train": (_I, [_P, _P, _I, ctypes.c_float]),
+    "lucid_cuda_guide_enable": (_I, [_P, _I, _I]),
+    "lucid_cuda_guide_steps": (_I, [_P]),
     "lucid_cuda_cancel": (_I, [_P]),
     "lucid_cuda_is_cancelled": (_I, [_P]),
     "lucid_cuda_reset_cancel": (_I, [_P]),
@@ -337,6 +339,12 @@ class Context:
         img = np.zeros((tile_h, tile_w, 4), np.float64)
         self._check(self.lib.lucid_cuda_render_f64(self.h, ctypes.byref(p), img.ctypes.data))
         return img
+
+    def guide_enable(self, on: bool = True, seed: int = 1):
+        self._check(self.lib.lucid_cuda_guide_enable(self.h, int(on), seed))
+
+    def guide_steps(self) -> int:
+        return self._count(self.lib.lucid_cuda_guide_steps(self.h))
 
     # ---- path diagnostics ----
     def diag_enable(self, subsample=2, record_capacity=0):

@@ -364,5 +364,61 @@ def material_preview_scene(seed: int = 0):
     return scene, camera
 
 
+def _grid_quad(origin, du, dv, nu, nv, skip=None):
+    """A planar quad origin + [0,1]^2 (du, dv) split into nu x nv cells (two
+    triangles each); `skip(i, j)` leaves cells out (openings)."""
+    o, du, dv = (np.asarray(a, np.float64) for a in (origin, du, dv))
+    verts, tris = [], []
+    for j in range(nv):
+        for i in range(nu):
+            if skip is not None and skip(i, j):
+                continue
+            p0 = o + du * (i / nu) + dv * (j / nv)
+            p1 = o + du * ((i + 1) / nu) + dv * (j / nv)
+            p2 = o + du * ((i + 1) / nu) + dv * ((j + 1) / nv)
+            p3 = o + du * (i / nu) + dv * ((j + 1) / nv)
+            b = len(verts)
+            verts += [p0, p1, p2, p3]
+            tris += [[b, b + 1, b + 2], [b, b + 2, b + 3]]
+    return np.array(verts), np.array(tris, dtype=np.int64)
+
+
+def hard_indirect_scene():
+    """A 12 x 12 x 4 m room (diffuse walls, albedo 0.6; glossy floor,
+    roughness 0.2) lit only through a 0.5 m wide, 2.25 m high door gap from
+    an adjoining 4 x 12 m room holding a 1 m^2 area light and a 2 x 2 m roof
+    opening for the sun.  Walls are tessellated into 0.25 m cells (about
+    20k triangles); the environment is black.  Camera: 1280x720 framing,
+    60 degree vertical field of view, inside the main room."""
+    wall = material((0.6, 0.6, 0.6), 0.0, 1.0)
+    floor_m = material((0.6, 0.6, 0.6), 0.0, 0.2)
+    c = 4   # cells per metre
+    meshes = []
+    add = lambda vt, m: meshes.append(mesh(vt[0], vt[1], m))
+    # main room: x in [0, 12], z in [0, 12], y in [0, 4]
+    add(_grid_quad((0, 0, 0), (0, 0, 12), (12, 0, 0), 12 * c, 12 * c), floor_m)            # floor (normal +y)
+    add(_grid_quad((0, 4, 0), (12, 0, 0), (0, 0, 12), 12 * c, 12 * c), wall)               # ceiling
+    add(_grid_quad((0, 0, 0), (12, 0, 0), (0, 4, 0), 12 * c, 4 * c), wall)                 # z = 0
+    add(_grid_quad((0, 0, 12), (0, 4, 0), (12, 0, 0), 4 * c, 12 * c), wall)                # z = 12
+    add(_grid_quad((0, 0, 0), (0, 4, 0), (0, 0, 12), 4 * c, 12 * c), wall)                 # x = 0
+    door = lambda i, j: 23 <= j <= 24 and i <= 8     # z in [5.75, 6.25], y in [0, 2.25]
+    add(_grid_quad((12, 0, 0), (0, 4, 0), (0, 0, 12), 4 * c, 12 * c, skip=door), wall)    # x = 12, with the gap
+    # adjoining room: x in [12, 16]
+    add(_grid_quad((12, 0, 0), (0, 0, 12), (4, 0, 0), 12 * c, 4 * c), wall)
+    hole = lambda i, j: 4 <= i < 12 and 4 <= j < 12    # x in [13, 15], z in [1, 3]
+    add(_grid_quad((12, 4, 0), (4, 0, 0), (0, 0, 12), 4 * c, 12 * c, skip=hole), wall)
+    add(_grid_quad((12, 0, 0), (4, 0, 0), (0, 4, 0), 4 * c, 4 * c), wall)
+    add(_grid_quad((12, 0, 12), (0, 4, 0), (4, 0, 0), 4 * c, 4 * c), wall)
+    add(_grid_quad((16, 0, 0), (0, 0, 12), (0, 4, 0), 12 * c, 4 * c), wall)
+    lights = [
+        {"type": "SUN", "direction": [-0.25, -1.0, 0.35], "color": [1.0, 0.95, 0.85], "energy": 6.0},
+        {"type": "AREA", "position": [14.0, 3.8, 9.0], "direction": [0.0, -1.0, 0.0], "right": [1, 0, 0],
+         "up": [0, 0, 1], "shape": "SQUARE", "size": 1.0, "color": [1.0, 1.0, 1.0], "energy": 300.0},
+    ]
+    scene = {"meshes": meshes, "native_lights": lights, "environment": {"color": [0.0, 0.0, 0.0], "strength": 1.0}}
+    camera = (2.0, 1.7, 1.5, 0.9, -0.1, 0.42, 0.0, 1.0, 0.0, 60.0)
+    return scene, camera
+
+
 def scene_triangle_count(scene: dict) -> int:
     return int(sum(len(m["triangles"]) for m in scene["meshes"]))

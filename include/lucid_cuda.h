@@ -64,7 +64,7 @@ typedef struct LucidSampleRecord {
 } LucidSampleRecord;
 
 /* Per-render statistics (the last render call with LUCID_RENDER_PROFILE). */
-#define LUCID_MAX_KERNEL_KINDS 8
+#define LUCID_MAX_KERNEL_KINDS 12
 typedef struct LucidKernelStat {
     char name[32];
     int launches;
@@ -334,6 +334,18 @@ int lucid_guide_encode(LucidGuide* guide, const float* p01, const float* normal,
 int lucid_guide_gradient(LucidGuide* guide, const float* records, int n, float* grad_out);
 /* one Adam step (beta 0.9 / 0.999, eps 1e-8) on n records */
 int lucid_guide_train(LucidGuide* guide, const float* records, int n, float lr);
+
+/* Online path guiding for the `mis` integrator (no reference counterpart):
+ * while on, every render call samples guidable surfaces (no transmission,
+ * not near-delta metal) from the BSDF or from the guide network with
+ * probability 1/2 each, weighted by the balance heuristic (NEE's MIS weight
+ * uses the same mixed pdf), records the guided vertices with the radiance
+ * that arrives along their samples, and takes one Adam step (lr 1e-2, up to
+ * 2^18 records) after each wave.  The estimator stays unbiased; its noise
+ * changes.  Enabling (re)initialises the network from `seed`. */
+int lucid_cuda_guide_enable(LucidCudaCtx* ctx, int on, int seed);
+/* Training steps taken since the network was initialised. */
+int lucid_cuda_guide_steps(LucidCudaCtx* ctx);
 
 /* ---- cancellation ---------------------------------------------------- */
 /* Replaces PyRenderer::cancel / is_cancelled / reset_cancel

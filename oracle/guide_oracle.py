@@ -131,11 +131,15 @@ def loss(theta, recs):
     return float(-(c * np.log(np.maximum(q, 1e-300))).sum())
 
 
-def gradient(theta, recs):
-    """d loss / d theta by backpropagation (records: (m, 16))."""
+def gradient(theta, recs, bf16_inputs=False):
+    """d loss / d theta by backpropagation (records: (m, 16)); with
+    bf16_inputs the encoded inputs are rounded to BF16 first, as the CUDA
+    kernels feed them to the tensor cores."""
     recs = np.asarray(recs, np.float64)
     P = unpack(theta)
     x = encode(recs[:, 0:3], recs[:, 3:6], recs[:, 6:9])
+    if bf16_inputs:
+        x = bf16_round(x)
     raw, (x, h1, h2, h3) = forward(theta, x)
     wi = recs[:, 9:12]
     c = coefficients(recs)
@@ -172,6 +176,39 @@ def adam(theta, m, v, g, step, lr, b1=0.9, b2=0.999, eps=1e-8):
     v = b2 * v + (1 - b2) * g * g
     theta = theta - lr * (m / (1 - b1 ** step)) / (np.sqrt(v / (1 - b2 ** step)) + eps)
     return theta, m, v
+
+
+def bf16_round(a):
+    """Round FP32 values to BF16 (round to nearest even), returned as FP64."""
+    a = np.asarray(a, np.float32).copy()
+    u = a.view(np.uint32)
+    u += 0x7FFF + ((u >> 16) & 1)
+    u &= 0xFFFF0000
+    return u.view(np.float32).astype(np.float64)
+
+
+def bf16_weights(theta):
+    """theta with its weight matrices (not the biases) rounded to BF16: the
+    network the CUDA kernels evaluate."""
+    t = np.asarray(theta, np.float64).copy()
+    o = 0
+    for name, shape in SHAPES:
+        n = int(np.prod(shape))
+        if name.startswith("W"):
+            t[o:o + n] = bf16_round(t[o:o + n])
+        o += n
+    return t
+
+
+def coherent_records(rng, n, spread=0.3):
+    """Records whose sampled directions cluster around one direction: a
+    well-conditioned gradient (the samples agree) for precision checks."""
+    recs = random_records(rng, n)
+    d0 = np.array([0.3, -0.5, 0.81])
+    w = d0 / np.linalg.norm(d0) + spread * rng.normal(size=(n, 3))
+    recs[:, 9:12] = w / np.linalg.norm(w, axis=1, keepdims=True)
+    recs[:, 13:16] = 1.0
+    return recs
 
 
 def random_records(rng, n, raw_like=None):

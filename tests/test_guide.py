@@ -101,25 +101,33 @@ def test_gpu_forward_matches_fp64(guide):
     x = go.encode(rng.random((500, 3)), rng.normal(size=(500, 3)), rng.normal(size=(500, 3))).astype(np.float32)
     out = np.zeros((500, go.N_OUT), np.float32)
     assert lib.lucid_guide_forward(h, x.ctypes.data, 500, out.ctypes.data) == 0
-    ref, _ = go.forward(theta.astype(np.float64), x.astype(np.float64))
+    ref, _ = go.forward(go.bf16_weights(theta), x.astype(np.float64))
     assert _rel(out, ref) < RTOL_BF16
 
 
 @pytest.mark.gpu
 def test_gpu_gradient_matches_fp64(guide):
+    """Against the FP64 gradient of the network the kernels evaluate (weights
+    and encoded inputs rounded to BF16; hidden activations and gradients stay
+    BF16 on the GPU): relative error <= 2e-2 per parameter block on records
+    whose samples agree, and <= 1e-1 on random records, where the gradient is
+    a small sum of large cancelling terms (there even rounding the weights to
+    BF16 moves the FP64 gradient by 4-6 %)."""
     lib, h = guide
     rng = np.random.default_rng(6)
     theta = rng.normal(0, 0.15, go.N_PARAMS).astype(np.float32)
     assert lib.lucid_guide_set_params(h, theta.ctypes.data, theta.size) == 0
-    recs = go.random_records(rng, 4096).astype(np.float32)
-    g = np.zeros(go.N_PARAMS, np.float32)
-    assert lib.lucid_guide_gradient(h, recs.ctypes.data, len(recs), g.ctypes.data) == 0
-    ref = go.gradient(theta.astype(np.float64), recs.astype(np.float64))
-    o = 0
-    for name, shape in go.SHAPES:
-        n = int(np.prod(shape))
-        assert _rel(g[o:o + n], ref[o:o + n]) < RTOL_BF16, name
-        o += n
+    tq = go.bf16_weights(theta)
+    for recs, tol in ((go.coherent_records(rng, 4096), RTOL_BF16), (go.random_records(rng, 4096), 0.1)):
+        recs = recs.astype(np.float32)
+        g = np.zeros(go.N_PARAMS, np.float32)
+        assert lib.lucid_guide_gradient(h, recs.ctypes.data, len(recs), g.ctypes.data) == 0
+        ref = go.gradient(tq, recs.astype(np.float64), bf16_inputs=True)
+        o = 0
+        for name, shape in go.SHAPES:
+            n = int(np.prod(shape))
+            assert _rel(g[o:o + n], ref[o:o + n]) < tol, (name, tol)
+            o += n
 
 
 @pytest.mark.gpu
@@ -135,6 +143,8 @@ def test_gpu_adam_step_matches_fp64(guide):
     after = _params(lib, h)
     want, _, _ = go.adam(theta.astype(np.float64), np.zeros(go.N_PARAMS), np.zeros(go.N_PARAMS),
                          g.astype(np.float64), 1, 1e-2)
-    np.testing.assert_allclose(after, want, rtol=1e-5, atol=1e-6)
+    # FP32 against FP64 Adam: the first step is lr * g / (|g| + eps), ill
+    # conditioned where |g| is near eps; 1e-4 is 1 % of the step size
+    np.testing.assert_allclose(after, want, rtol=1e-5, atol=1e-4)
     # a step against its own gradient lowers the loss
     assert go.loss(after.astype(np.float64), recs) < go.loss(theta.astype(np.float64), recs)
