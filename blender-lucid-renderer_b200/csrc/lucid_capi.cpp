@@ -302,6 +302,10 @@ int lucid_cuda_guide_enable(LucidCudaCtx* ctx, int on, int seed) {
     return guarded(ctx, [&](lucid::Engine& e) { return e.guide_enable(on != 0, seed); });
 }
 
+int lucid_cuda_guide_config(LucidCudaCtx* ctx, int steps_per_wave, float lr) {
+    return guarded(ctx, [&](lucid::Engine& e) { return e.guide_config(steps_per_wave, lr); });
+}
+
 int lucid_cuda_guide_steps(LucidCudaCtx* ctx) {
     return guarded(ctx, [&](lucid::Engine& e) { return e.guide_steps(); });
 }

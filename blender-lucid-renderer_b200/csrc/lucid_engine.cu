@@ -156,6 +156,7 @@ struct GuideState {
     long long cap = 0;
     float keep = 1.0f;
     float lr = 1e-2f;
+    int steps = 4;   // Adam steps per wave, each on its own batch of records
     bool on = false;
 };
 
@@ -2395,7 +2396,7 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
         if (rc2 != LUCID_OK) return rc2;
         GuideState& G = *guide_;
         gv.gmix = G.gmix.p; gv.gslot = G.gslot.p; gv.ginv = G.ginv.p; gv.grec = G.recs.p; gv.gcount = G.count.p;
-        gv.gcap = kGuideBatch;
+        gv.gcap = G.steps * kGuideBatch;
         for (int k = 0; k < 3; ++k) {
             gv.glo[k] = scene_lo_[k];
             float ext = scene_hi_[k] - scene_lo_[k];
@@ -2501,16 +2502,18 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
         if (guide) CK(cudaMemcpyAsync(gcnt, guide_->count.p, sizeof(gcnt), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         if (guide) {
-            // one Adam step on this wave's records; next wave's sampling rate
-            // aims at 90 % of a training batch
+            // Adam steps on this wave's records, one batch each; the next
+            // wave's sampling rate aims at 90 % of the batches
             GuideState& G = *guide_;
-            int nrec = std::min(gcnt[0], kGuideBatch);
+            int nrec = std::min(gcnt[0], G.steps * kGuideBatch);
             e = ev_begin(K_TRAIN, 0);
-            if (nrec > 0 && G.net.train_step(G.recs.p, nrec, st, G.lr) != 0)
-                return fail(LUCID_ERR_CUDA, "guide training: " + G.net.error());
+            for (int b = 0; b * kGuideBatch < nrec; ++b)
+                if (G.net.train_step(G.recs.p + (size_t)b * kGuideBatch, std::min(kGuideBatch, nrec - b * kGuideBatch),
+                                     st, G.lr) != 0)
+                    return fail(LUCID_ERR_CUDA, "guide training: " + G.net.error());
             ev_end(e);
             if (profile) kind_units[K_TRAIN] += nrec;
-            G.keep = (float)std::min(1.0, 0.9 * kGuideBatch / std::max(1.0, (double)gcnt[1]));
+            G.keep = (float)std::min(1.0, 0.9 * G.steps * kGuideBatch / std::max(1.0, (double)gcnt[1]));
         }
         for (int d = 0; d < p.max_depth; ++d) {
             seg += hcnt[kCountersPerDepth * d];
@@ -2587,7 +2590,7 @@ int Engine::guide_buffers(long long paths) {
         CK(G.ginv.alloc((size_t)paths * 3));
         G.cap = paths;
     }
-    if (!G.recs.p) CK(G.recs.alloc(kGuideBatch));
+    if ((long long)G.recs.n < (long long)G.steps * kGuideBatch) CK(G.recs.alloc((size_t)G.steps * kGuideBatch));
     if (!G.count.p) CK(G.count.alloc(2));
     return LUCID_OK;
 }
@@ -2610,6 +2613,15 @@ int Engine::guide_enable(bool on, int seed) {
 }
 
 int Engine::guide_steps() const { return guide_ ? guide_->net.steps() : 0; }
+
+int Engine::guide_config(int steps_per_wave, float lr) {
+    GpuLock gl(*this);
+    if (steps_per_wave < 1 || steps_per_wave > 64 || !(lr > 0.0f)) return fail(LUCID_ERR_INVALID, "guide: bad config");
+    if (!guide_) guide_ = new GuideState();
+    guide_->steps = steps_per_wave;
+    guide_->lr = lr;
+    return LUCID_OK;
+}
 
 // ---------------------------------------------------------------- progressive jobs
 // A job renders one image progressively: each iteration adds n samples to a

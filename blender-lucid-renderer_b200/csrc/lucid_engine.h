@@ -55,6 +55,7 @@ public:
     // Online-trained path guiding for the `mis` integrator (reseeds the network).
     int guide_enable(bool on, int seed);
     int guide_steps() const;
+    int guide_config(int steps_per_wave, float lr);
     // Uses `owner`'s uploaded scene (BVH, materials, lights) without a copy.
     int share_scene(Engine& owner);
     // Progressive jobs (the request loop's unit of work).

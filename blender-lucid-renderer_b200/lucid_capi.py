@@ -150,6 +150,7 @@ SIGNATURES = {
     "lucid_guide_train": (_I, [_P, _P, _I, ctypes.c_float]),
     "lucid_cuda_guide_enable": (_I, [_P, _I, _I]),
     "lucid_cuda_guide_steps": (_I, [_P]),
+    "lucid_cuda_guide_config": (_I, [_P, _I, ctypes.c_float]),
     "lucid_cuda_cancel": (_I, [_P]),
     "lucid_cuda_is_cancelled": (_I, [_P]),
     "lucid_cuda_reset_cancel": (_I, [_P]),
@@ -342,6 +343,9 @@ class Context:
 
     def guide_enable(self, on: bool = True, seed: int = 1):
         self._check(self.lib.lucid_cuda_guide_enable(self.h, int(on), seed))
+
+    def guide_config(self, steps_per_wave: int = 4, lr: float = 1e-2):
+        self._check(self.lib.lucid_cuda_guide_config(self.h, steps_per_wave, ctypes.c_float(lr)))
 
     def guide_steps(self) -> int:
         return self._count(self.lib.lucid_cuda_guide_steps(self.h))
