@@ -237,6 +237,43 @@ def serving(device: int, seed: int = 7) -> dict:
             "slots": 8, "samples_per_s": total / wall_mix, "samples_per_s_sequential": total / wall_seq}
 
 
+def guiding(device: int, budget_ms: float = 1000.0) -> dict:
+    """Equal-time relMSE on the hard-indirect room (1280x720, mis, depth 8)
+    against an independent FP64-accumulated 4096-spp reference: plain and
+    guided renders of 4 spp per call until each has used budget_ms of device
+    time (guided time includes inference and training)."""
+    import lucid_capi
+    import lucid_quality as lq
+    import lucid_scenes as ls
+    W, H, D, spp = 1280, 720, 8, 4
+    scene, cam = ls.hard_indirect_scene()
+    c = lucid_capi.Context(device)
+    c.load_scene_json(ls.to_json(scene))
+    c.set_camera(*cam)
+    c.set_algorithm("mis")
+    t0 = time.perf_counter()
+    ref = lq.render_reference(c, W, H, spp=lq.REFERENCE_SPP, max_depth=D, sample_offset=1 << 20)
+    ref_s = time.perf_counter() - t0
+    out = {}
+    for guided in (False, True):
+        c.guide_enable(guided, 1)
+        acc, ms, k = np.zeros((H, W, 4)), 0.0, 0
+        while ms < budget_ms:
+            img, _, _ = c.render(W, H, W, H, spp, spp * k, D, profile=True)
+            ms += c.stats()["total_ms"]
+            acc += img
+            k += 1
+        out["guided" if guided else "plain"] = {"relmse": lq.relmse(lq.mean_image(acc, k * spp), ref),
+                                                "spp": k * spp, "device_ms": ms}
+    out["training_steps"] = c.guide_steps()
+    c.guide_enable(False, 0)
+    c.close()
+    out.update({"scene": "hard-indirect room, 20,828 triangles, 1280x720, mis, depth 8",
+                "reference": f"FP64-accumulated {lq.REFERENCE_SPP} spp on the GPU", "reference_s": round(ref_s, 2),
+                "equal_time_relmse_ratio": out["guided"]["relmse"] / out["plain"]["relmse"]})
+    return out
+
+
 def run_reference(args, rank: int):
     if rank != 0:
         return 0
@@ -266,6 +303,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-quality", action="store_true", help="skip the Cornell relMSE measurement")
     ap.add_argument("--no-serving", action="store_true", help="skip the request-loop job trace")
+    ap.add_argument("--no-guiding", action="store_true", help="skip the guided-vs-plain equal-time comparison")
     ap.add_argument("--wave", type=int, default=0, help="paths per wave (0: the engine's default)")
     ap.add_argument("--width", type=int, default=W, help="smaller frames for profiling captures")
     ap.add_argument("--height", type=int, default=H)
@@ -364,6 +402,7 @@ def main():
 
     quality = c1_quality(local_rank) if rank == 0 and not args.no_quality else None
     serve = serving(local_rank) if rank == 0 and world == 1 and not args.no_serving else None
+    guide = guiding(local_rank) if rank == 0 and world == 1 and not args.no_guiding else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -391,7 +430,7 @@ def main():
                         for k, v in kern.items()},
             "mrays_per_s": mrays, "segments_per_step": segs, "shadow_rays_per_step": shadows,
             "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": cpu, "quality": quality,
-            "serving": serve,
+            "serving": serve, "guiding": guide,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
