@@ -179,13 +179,14 @@ def c1_quality(device: int) -> dict:
             "reference_s": round(ref_s, 3), "samples_per_s": 256 * 256 * 16 / (ms / 1000.0)}
 
 
-def serving(device: int, seed: int = 7) -> dict:
+def serving(device: int, seed: int = 7, slots: int = 2) -> dict:
     """The request loop on a seeded job trace: Poisson arrivals (mean 40 per
     second for one second) of viewport sessions (800x600, 16 one-sample
     ticks, interactive), material previews (256x256, 32 spp) and F12 renders
     (1920x1080, 256 spp) of the Cornell box.  Latencies come from the trace
-    on 8 slots; aggregate samples/s from the same jobs submitted at once, on
-    8 slots and on 1 slot (one after another)."""
+    on 2 slots; aggregate samples/s from the same jobs submitted at once, on
+    2 slots and on 1 slot (one after another).  (Measured: 2 slots beat 4
+    and 8, whose persistent kernels contend for the same SMs.)"""
     import lucid_capi
     import lucid_scenes as ls
     rng = np.random.default_rng(seed)
@@ -226,18 +227,18 @@ def serving(device: int, seed: int = 7) -> dict:
         return st, wall
 
     total = sum(w * h * spp for (_, _, w, h, spp, _) in jobs)
-    st_trace, _ = run(8, True)
-    _, wall_mix = run(8, False)
+    st_trace, _ = run(slots, True)
+    _, wall_mix = run(slots, False)
     _, wall_seq = run(1, False)
     return {"trace": "Poisson 40/s for 1 s, seed %d: 60%% viewport 800x600x16 (interactive), 35%% preview "
                      "256x256x32, 5%% F12 1920x1080x256, mis depth 8" % seed,
             "jobs": len(jobs), "samples": total,
             "latency_p50_ms": st_trace["latency_p50_ms"], "latency_p99_ms": st_trace["latency_p99_ms"],
             "first_frame_p50_ms": st_trace["first_p50_ms"], "first_frame_p99_ms": st_trace["first_p99_ms"],
-            "slots": 8, "samples_per_s": total / wall_mix, "samples_per_s_sequential": total / wall_seq}
+            "slots": slots, "samples_per_s": total / wall_mix, "samples_per_s_sequential": total / wall_seq}
 
 
-def guiding(device: int, budget_ms: float = 1000.0) -> dict:
+def guiding(device: int, budget_ms: float = 1000.0, width: int = 1280, height: int = 720) -> dict:
     """Equal-time relMSE on the hard-indirect room (1280x720, mis, depth 8)
     against an independent FP64-accumulated 4096-spp reference: plain and
     guided renders of 4 spp per call until each has used budget_ms of device
@@ -245,7 +246,7 @@ def guiding(device: int, budget_ms: float = 1000.0) -> dict:
     import lucid_capi
     import lucid_quality as lq
     import lucid_scenes as ls
-    W, H, D, spp = 1280, 720, 8, 4
+    W, H, D, spp = width, height, 8, 4
     scene, cam = ls.hard_indirect_scene()
     c = lucid_capi.Context(device)
     c.load_scene_json(ls.to_json(scene))
@@ -268,7 +269,7 @@ def guiding(device: int, budget_ms: float = 1000.0) -> dict:
     out["training_steps"] = c.guide_steps()
     c.guide_enable(False, 0)
     c.close()
-    out.update({"scene": "hard-indirect room, 20,828 triangles, 1280x720, mis, depth 8",
+    out.update({"scene": f"hard-indirect room, 20,828 triangles, {W}x{H}, mis, depth 8",
                 "reference": f"FP64-accumulated {lq.REFERENCE_SPP} spp on the GPU", "reference_s": round(ref_s, 2),
                 "equal_time_relmse_ratio": out["guided"]["relmse"] / out["plain"]["relmse"]})
     return out
@@ -304,6 +305,10 @@ def main():
     ap.add_argument("--no-quality", action="store_true", help="skip the Cornell relMSE measurement")
     ap.add_argument("--no-serving", action="store_true", help="skip the request-loop job trace")
     ap.add_argument("--no-guiding", action="store_true", help="skip the guided-vs-plain equal-time comparison")
+    ap.add_argument("--guiding-only", action="store_true", help="only the guided-vs-plain comparison")
+    ap.add_argument("--guide-budget-ms", type=float, default=1000.0)
+    ap.add_argument("--guide-width", type=int, default=1280)
+    ap.add_argument("--guide-height", type=int, default=720)
     ap.add_argument("--wave", type=int, default=0, help="paths per wave (0: the engine's default)")
     ap.add_argument("--width", type=int, default=W, help="smaller frames for profiling captures")
     ap.add_argument("--height", type=int, default=H)
@@ -316,6 +321,10 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank)
+    if args.guiding_only:
+        print(json.dumps(guiding(int(os.environ.get("LOCAL_RANK", "0")), args.guide_budget_ms, args.guide_width,
+                                 args.guide_height)), flush=True)
+        return 0
 
     import torch
     dist = None
@@ -402,7 +411,8 @@ def main():
 
     quality = c1_quality(local_rank) if rank == 0 and not args.no_quality else None
     serve = serving(local_rank) if rank == 0 and world == 1 and not args.no_serving else None
-    guide = guiding(local_rank) if rank == 0 and world == 1 and not args.no_guiding else None
+    guide = (guiding(local_rank, args.guide_budget_ms, args.guide_width, args.guide_height)
+             if rank == 0 and world == 1 and not args.no_guiding else None)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
