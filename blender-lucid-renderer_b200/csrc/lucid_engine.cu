@@ -95,7 +95,7 @@ struct PathView {
     int* qb;           // shading queue binned by event / material class
     unsigned char* cls;   // class of each path's pending event
     int* counters;     // per depth: [0] active, [1] shadow, [2..4] fetch cursors,
-                       // [8..23] class counts, [24..39] class cursors
+                       // [8, 8 + kBins) class counts, then kBins class cursors
     int* errors;       // [0] traversal stack overflow
     int2* rec_prim;
     int4* rec_cnt;     // bounces, nee tests, nee occluded
@@ -110,8 +110,8 @@ struct PathView {
     unsigned gkeep;    // a guided vertex is recorded when its hash < gkeep
     float glo[3], gscale[3];   // scene box -> [0,1]^3
 };
-constexpr int kCountersPerDepth = 48;
 constexpr int kBins = 16;
+constexpr int kCountersPerDepth = 8 + 2 * kBins;
 constexpr int kMaxDepth = 1024;
 
 struct PathPool {
@@ -783,7 +783,7 @@ __global__ void __launch_bounds__(256) k_bin_scatter(PathView pv, int* cnt, int 
         unsigned peers = __match_any_sync(0xffffffffu, c);
         int leader = __ffs(peers) - 1;
         int pos = 0;
-        if (act && (int)lane_id() == leader) pos = atomicAdd(&cnt[24 + c], __popc(peers));
+        if (act && (int)lane_id() == leader) pos = atomicAdd(&cnt[8 + kBins + c], __popc(peers));
         pos = __shfl_sync(0xffffffffu, pos, leader);
         if (act) qb[base[c] + pos + __popc(peers & lanemask_lt())] = id;
     }
