@@ -1,5 +1,6 @@
-// lucid_guide.cu — training of the path-guiding network (fused forward,
-// backward and weight gradients on the tensor cores; Adam on FP32 masters).
+// lucid_guide.cu — training of the path-guiding network (forward/backward
+// pass and split-K weight-gradient GEMMs on the tensor cores; Adam on FP32
+// masters).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -22,37 +23,6 @@ struct TrainTile {
     __nv_bfloat16 dout[16 * kLdH];   // dL/d(raw outputs), 48 used
     __nv_bfloat16 da[16 * kLdH], db[16 * kLdH];
 };
-constexpr int kTrainWarps = 3;
-constexpr size_t kTrainSmem = sizeof(GuideSmemW) + kTrainWarps * sizeof(TrainTile) + kGParams * sizeof(float);
-
-// grad[MOUT][KIN] += D^T H over the tile's 16 rows (D: 16 x MOUT, H: 16 x KIN).
-template <int MOUT, int KIN, int LDD, int LDH>
-LD void tile_wgrad(const __nv_bfloat16* D, const __nv_bfloat16* H, float* grad) {
-    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
-#pragma unroll 1
-    for (int mb = 0; mb < MOUT / 16; ++mb) {
-        const int m0 = mb * 16 + g;
-        unsigned a[4];
-        a[0] = pair2(D + (2 * q) * LDD + m0, D + (2 * q + 1) * LDD + m0);
-        a[1] = pair2(D + (2 * q) * LDD + m0 + 8, D + (2 * q + 1) * LDD + m0 + 8);
-        a[2] = pair2(D + (2 * q + 8) * LDD + m0, D + (2 * q + 9) * LDD + m0);
-        a[3] = pair2(D + (2 * q + 8) * LDD + m0 + 8, D + (2 * q + 9) * LDD + m0 + 8);
-#pragma unroll 2
-        for (int nb = 0; nb < KIN / 8; ++nb) {
-            const int n0 = nb * 8 + g;
-            unsigned b[2];
-            b[0] = pair2(H + (2 * q) * LDH + n0, H + (2 * q + 1) * LDH + n0);
-            b[1] = pair2(H + (2 * q + 8) * LDH + n0, H + (2 * q + 9) * LDH + n0);
-            float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-            mma16816(acc, a, b);
-            const int c = nb * 8 + 2 * q;
-            atomicAdd(&grad[m0 * KIN + c], acc[0]);
-            atomicAdd(&grad[m0 * KIN + c + 1], acc[1]);
-            atomicAdd(&grad[(m0 + 8) * KIN + c], acc[2]);
-            atomicAdd(&grad[(m0 + 8) * KIN + c + 1], acc[3]);
-        }
-    }
-}
 
 // out[16 x KIN] = (D[16 x MOUT] W[MOUT][KIN]) * (H > 0), as BF16 (ld kLdH);
 // the column sums go to gbias (the bias gradient of the layer below).
@@ -143,25 +113,53 @@ __global__ void k_guide_coeff_sum(const GuideRec* recs, int n, float* sum) {
     if ((threadIdx.x & 31) == 0) atomicAdd(sum, s);
 }
 
-// Fused forward + backward over tiles of 16 records; weight gradients are
-// summed in shared memory and added to `grad` once per block.  The loss is
-// sum_s c_s (-log q(wi_s)) with c_s = (F_s / pdf_s) / sum_t F_t / pdf_t.
-__global__ void __launch_bounds__(32 * kTrainWarps) k_guide_train(const GuideRec* recs, int n,
-                                                                 const __nv_bfloat16* wq, const float* master,
-                                                                 const float* csum, float* grad) {
+// The loss of a batch is sum_s c_s (-log q(wi_s)) with
+// c_s = (F_s / pdf_s) / sum_t F_t / pdf_t.
+
+// ---- training in two passes ---------------------------------------------------
+// Pass 1 (k_guide_fb): per warp tile of 16 records, forward, mixture
+// gradient and backpropagation of the gradients through the layers; the
+// layer inputs (x, h1..h3) and output gradients (d4..d1) go to global memory
+// as BF16 and the bias gradients are summed per block.  Pass 2
+// (k_guide_wgrad): each weight gradient dW = D^T H as a split-K GEMM over the
+// records, accumulated in registers over a slice of records and added to the
+// gradient once per block.
+constexpr int kFbWarps = 7;
+constexpr size_t kFbSmem = sizeof(GuideSmemW) + kFbWarps * sizeof(TrainTile) + 256 * sizeof(float);
+// per-record offsets (BF16 elements) in the pass-1 workspace
+constexpr int kWsX = 0, kWsH1 = kGIn, kWsH2 = kWsH1 + kGHid, kWsH3 = kWsH2 + kGHid, kWsD4 = kWsH3 + kGHid,
+              kWsD3 = kWsD4 + kGOut, kWsD2 = kWsD3 + kGHid, kWsD1 = kWsD2 + kGHid, kWsRow = kWsD1 + kGHid;
+
+// Copies a 16-row tile (ld `ld` in shared memory) to rows r0.. of a global
+// matrix of `cols` columns inside the record workspace (row stride kWsRow).
+LD void tile_store(const __nv_bfloat16* src, int ld, int cols, __nv_bfloat16* dst, int r0, int n) {
+    const int lane = threadIdx.x & 31;
+    for (int e = lane; e < 16 * (cols / 2); e += 32) {
+        int r = e / (cols / 2), c = 2 * (e % (cols / 2));
+        if (r0 + r < n)
+            *reinterpret_cast<unsigned*>(dst + (size_t)(r0 + r) * kWsRow + c) =
+                *reinterpret_cast<const unsigned*>(src + r * ld + c);
+    }
+}
+
+// Backpropagation without the weight gradient (tile_backprop's data part).
+__global__ void __launch_bounds__(32 * kFbWarps) k_guide_fb(const GuideRec* recs, int n, const __nv_bfloat16* wq,
+                                                           const float* master, const float* csum,
+                                                           __nv_bfloat16* ws, float* grad) {
     extern __shared__ __align__(16) unsigned char smem[];
     GuideSmemW& W = *reinterpret_cast<GuideSmemW*>(smem);
     TrainTile* tiles = reinterpret_cast<TrainTile*>(smem + sizeof(GuideSmemW));
-    float* sg = reinterpret_cast<float*>(smem + sizeof(GuideSmemW) + kTrainWarps * sizeof(TrainTile));
+    float* sb = reinterpret_cast<float*>(smem + sizeof(GuideSmemW) + kFbWarps * sizeof(TrainTile));
     guide_load_weights(W, wq, master);
-    for (int i = threadIdx.x; i < kGParams; i += blockDim.x) sg[i] = 0.0f;
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) sb[i] = 0.0f;
     __syncthreads();
+    // bias gradients in sb: b1 [0, 64), b2 [64, 128), b3 [128, 192), b4 [192, 240)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     TrainTile& T = tiles[warp];
     const float inv_sum = *csum > 0.0f ? 1.0f / *csum : 0.0f;
     const int ntiles = (n + 15) / 16;
-    for (int tile = blockIdx.x * kTrainWarps + warp; tile < ntiles; tile += gridDim.x * kTrainWarps) {
-        const int r = tile * 16 + lane;
+    for (int tile = blockIdx.x * kFbWarps + warp; tile < ntiles; tile += gridDim.x * kFbWarps) {
+        const int r0 = tile * 16, r = r0 + lane;
         GuideRec rec{};
         bool valid = lane < 16 && r < n;
         if (valid) rec = recs[r];
@@ -179,24 +177,96 @@ __global__ void __launch_bounds__(32 * kTrainWarps) k_guide_train(const GuideRec
             for (int i = 0; i < kGOut; i += 2)
                 *reinterpret_cast<unsigned*>(T.dout + lane * kLdH + i) = pack_bf16(d[i], d[i + 1]);
             for (int i = 0; i < kGOut; ++i)
-                if (d[i] != 0.0f) atomicAdd(&sg[kGB4 + i], d[i]);
+                if (d[i] != 0.0f) atomicAdd(&sb[192 + i], d[i]);
         }
         __syncwarp();
-        tile_wgrad<kGOut, kGHid, kLdH, kLdH>(T.dout, T.t.h3, sg + kGW4);
-        tile_backprop<kGOut, kGHid, kLdH, kLdH>(T.dout, W.w4, T.t.h3, T.da, sg + kGB3);
+        tile_backprop<kGOut, kGHid, kLdH, kLdH>(T.dout, W.w4, T.t.h3, T.da, sb + 128);
         __syncwarp();
-        tile_wgrad<kGHid, kGHid, kLdH, kLdH>(T.da, T.t.h2, sg + kGW3);
-        tile_backprop<kGHid, kGHid, kLdH, kLdH>(T.da, W.w3, T.t.h2, T.db, sg + kGB2);
+        tile_store(T.t.x, kLdIn, kGIn, ws + kWsX, r0, n);
+        tile_store(T.t.h1, kLdH, kGHid, ws + kWsH1, r0, n);
+        tile_store(T.t.h2, kLdH, kGHid, ws + kWsH2, r0, n);
+        tile_store(T.t.h3, kLdH, kGHid, ws + kWsH3, r0, n);
+        tile_store(T.dout, kLdH, kGOut, ws + kWsD4, r0, n);
+        tile_store(T.da, kLdH, kGHid, ws + kWsD3, r0, n);
+        tile_backprop<kGHid, kGHid, kLdH, kLdH>(T.da, W.w3, T.t.h2, T.db, sb + 64);
         __syncwarp();
-        tile_wgrad<kGHid, kGHid, kLdH, kLdH>(T.db, T.t.h1, sg + kGW2);
-        tile_backprop<kGHid, kGHid, kLdH, kLdH>(T.db, W.w2, T.t.h1, T.da, sg + kGB1);
+        tile_store(T.db, kLdH, kGHid, ws + kWsD2, r0, n);
+        tile_backprop<kGHid, kGHid, kLdH, kLdH>(T.db, W.w2, T.t.h1, T.da, sb);
         __syncwarp();
-        tile_wgrad<kGHid, kGIn, kLdH, kLdIn>(T.da, T.t.x, sg + kGW1);
+        tile_store(T.da, kLdH, kGHid, ws + kWsD1, r0, n);
         __syncwarp();
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < kGParams; i += blockDim.x)
-        if (sg[i] != 0.0f) atomicAdd(&grad[i], sg[i]);
+    for (int i = threadIdx.x; i < kGHid; i += blockDim.x) {
+        if (sb[i] != 0.0f) atomicAdd(&grad[kGB1 + i], sb[i]);
+        if (sb[64 + i] != 0.0f) atomicAdd(&grad[kGB2 + i], sb[64 + i]);
+        if (sb[128 + i] != 0.0f) atomicAdd(&grad[kGB3 + i], sb[128 + i]);
+    }
+    for (int i = threadIdx.x; i < kGOut; i += blockDim.x)
+        if (sb[192 + i] != 0.0f) atomicAdd(&grad[kGB4 + i], sb[192 + i]);
+}
+
+// grad[O][I] += sum over this block's records of D[s][o] H[s][i] (8 warps;
+// the (16 x 8) output fragments are split over the warps and accumulated in
+// registers over 32-record chunks staged in shared memory).
+constexpr int kWgChunk = 32, kWgSlice = 2048;
+template <int O, int I>
+__global__ void __launch_bounds__(256) k_guide_wgrad(const __nv_bfloat16* ws, int doff, int hoff, int n, float* grad) {
+    constexpr int LDD = O + 8, LDH = I + 8, NB = I / 8, FR = (O / 16) * NB, FPW = (FR + 7) / 8;
+    __shared__ __align__(16) __nv_bfloat16 Ds[kWgChunk * LDD];
+    __shared__ __align__(16) __nv_bfloat16 Hs[kWgChunk * LDH];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+    float acc[FPW][4];
+#pragma unroll
+    for (int j = 0; j < FPW; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
+    const int k0 = blockIdx.x * kWgSlice, k1 = min(n, k0 + kWgSlice);
+    for (int c0 = k0; c0 < k1; c0 += kWgChunk) {
+        __syncthreads();
+        for (int e = threadIdx.x; e < kWgChunk * (O / 2); e += blockDim.x) {
+            int r = e / (O / 2), c = 2 * (e % (O / 2));
+            unsigned v = 0;
+            if (c0 + r < k1) v = *reinterpret_cast<const unsigned*>(ws + (size_t)(c0 + r) * kWsRow + doff + c);
+            *reinterpret_cast<unsigned*>(Ds + r * LDD + c) = v;
+        }
+        for (int e = threadIdx.x; e < kWgChunk * (I / 2); e += blockDim.x) {
+            int r = e / (I / 2), c = 2 * (e % (I / 2));
+            unsigned v = 0;
+            if (c0 + r < k1) v = *reinterpret_cast<const unsigned*>(ws + (size_t)(c0 + r) * kWsRow + hoff + c);
+            *reinterpret_cast<unsigned*>(Hs + r * LDH + c) = v;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < FPW; ++j) {
+            const int f = warp + 8 * j;
+            if (f < FR) {
+                const int m0 = (f / NB) * 16 + g, n0 = (f % NB) * 8 + g;
+#pragma unroll
+                for (int ks = 0; ks < kWgChunk; ks += 16) {
+                    unsigned a[4], b[2];
+                    const __nv_bfloat16* D = Ds + ks * LDD;
+                    const __nv_bfloat16* H = Hs + ks * LDH;
+                    a[0] = pair2(D + (2 * q) * LDD + m0, D + (2 * q + 1) * LDD + m0);
+                    a[1] = pair2(D + (2 * q) * LDD + m0 + 8, D + (2 * q + 1) * LDD + m0 + 8);
+                    a[2] = pair2(D + (2 * q + 8) * LDD + m0, D + (2 * q + 9) * LDD + m0);
+                    a[3] = pair2(D + (2 * q + 8) * LDD + m0 + 8, D + (2 * q + 9) * LDD + m0 + 8);
+                    b[0] = pair2(H + (2 * q) * LDH + n0, H + (2 * q + 1) * LDH + n0);
+                    b[1] = pair2(H + (2 * q + 8) * LDH + n0, H + (2 * q + 9) * LDH + n0);
+                    mma16816(acc[j], a, b);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < FPW; ++j) {
+        const int f = warp + 8 * j;
+        if (f < FR) {
+            const int m0 = (f / NB) * 16 + g, c = (f % NB) * 8 + 2 * q;
+            atomicAdd(&grad[m0 * I + c], acc[j][0]);
+            atomicAdd(&grad[m0 * I + c + 1], acc[j][1]);
+            atomicAdd(&grad[(m0 + 8) * I + c], acc[j][2]);
+            atomicAdd(&grad[(m0 + 8) * I + c + 1], acc[j][3]);
+        }
+    }
 }
 
 __global__ void k_guide_adam(float* master, float* m, float* v, float* grad, __nv_bfloat16* wq, int n, float lr,
@@ -266,10 +336,11 @@ __global__ void k_guide_encode_rows(const float* p01, const float* nrm, const fl
 GuideNet::~GuideNet() { release(); }
 
 void GuideNet::release() {
-    for (void* p : {(void*)master_, (void*)m_, (void*)v_, (void*)grad_, (void*)wq_, (void*)csum_})
+    for (void* p : {(void*)master_, (void*)m_, (void*)v_, (void*)grad_, (void*)wq_, (void*)csum_, ws_})
         if (p) cudaFree(p);
     master_ = m_ = v_ = grad_ = csum_ = nullptr;
-    wq_ = nullptr;
+    wq_ = ws_ = nullptr;
+    ws_n_ = 0;
 }
 
 int GuideNet::init(int seed, cudaStream_t st) {
@@ -316,19 +387,31 @@ int GuideNet::get_params(float* w, cudaStream_t st) {
 }
 
 int GuideNet::gradient(const GuideRec* recs, int n, cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
-        GCK(cudaFuncSetAttribute(k_guide_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrainSmem));
-        attr = true;
-    }
     GCK(cudaMemsetAsync(csum_, 0, sizeof(float), st));
     if (n <= 0) return 0;
     k_guide_coeff_sum<<<std::min(1024, (n + 255) / 256), 256, 0, st>>>(recs, n, csum_);
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int blocks = std::max(1, std::min(sms, (n + 16 * kTrainWarps - 1) / (16 * kTrainWarps)));
-    k_guide_train<<<blocks, 32 * kTrainWarps, kTrainSmem, st>>>(recs, n, WQ(wq_), master_, csum_, grad_);
+    static bool attr_fb = false;
+    if (!attr_fb) {
+        GCK(cudaFuncSetAttribute(k_guide_fb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFbSmem));
+        attr_fb = true;
+    }
+    if (ws_n_ < n) {
+        if (ws_) cudaFree(ws_);
+        ws_ = nullptr;
+        GCK(cudaMalloc(&ws_, (size_t)n * kWsRow * sizeof(__nv_bfloat16)));
+        ws_n_ = n;
+    }
+    __nv_bfloat16* ws = WQ(ws_);
+    int blocks = std::max(1, std::min(sms, (n + 16 * kFbWarps - 1) / (16 * kFbWarps)));
+    k_guide_fb<<<blocks, 32 * kFbWarps, kFbSmem, st>>>(recs, n, WQ(wq_), master_, csum_, ws, grad_);
+    const int slices = (n + kWgSlice - 1) / kWgSlice;
+    k_guide_wgrad<kGHid, kGIn><<<slices, 256, 0, st>>>(ws, kWsD1, kWsX, n, grad_ + kGW1);
+    k_guide_wgrad<kGHid, kGHid><<<slices, 256, 0, st>>>(ws, kWsD2, kWsH1, n, grad_ + kGW2);
+    k_guide_wgrad<kGHid, kGHid><<<slices, 256, 0, st>>>(ws, kWsD3, kWsH2, n, grad_ + kGW3);
+    k_guide_wgrad<kGOut, kGHid><<<slices, 256, 0, st>>>(ws, kWsD4, kWsH3, n, grad_ + kGW4);
     GCK(cudaGetLastError());
     return 0;
 }

@@ -51,6 +51,8 @@ private:
     float* grad_ = nullptr;
     float* csum_ = nullptr;
     void* wq_ = nullptr;
+    void* ws_ = nullptr;   // per-record layer inputs and gradients of the last batch (BF16)
+    int ws_n_ = 0;
     int step_ = 0;
     std::string err_;
 };
