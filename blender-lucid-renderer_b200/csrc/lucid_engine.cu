@@ -2550,6 +2550,7 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
     if (records)
         CK(cudaMemcpyAsync(recs, d_recs.p, np * (size_t)p.samples * sizeof(LucidSampleRecord), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    if (guide && guide_->net.failed(st) != 0) return fail(LUCID_ERR_TIMEOUT, guide_->net.error());
     float tot = 0.0f;
     cudaEventElapsedTime(&tot, t0, t1);
     cudaEventDestroy(t0);

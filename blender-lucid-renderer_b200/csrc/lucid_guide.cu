@@ -24,11 +24,9 @@ struct TrainTile {
     __nv_bfloat16 da[16 * kLdH], db[16 * kLdH];
 };
 
-// out[16 x KIN] = (D[16 x MOUT] W[MOUT][KIN]) * (H > 0), as BF16 (ld kLdH);
-// the column sums go to gbias (the bias gradient of the layer below).
+// out[16 x KIN] = (D[16 x MOUT] W[MOUT][KIN]) * (H > 0), as BF16 (ld kLdH).
 template <int MOUT, int KIN, int LDD, int LDW>
-LD void tile_backprop(const __nv_bfloat16* D, const __nv_bfloat16* W, const __nv_bfloat16* H, __nv_bfloat16* out,
-                      float* gbias) {
+LD void tile_backprop(const __nv_bfloat16* D, const __nv_bfloat16* W, const __nv_bfloat16* H, __nv_bfloat16* out) {
     const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
     float acc[KIN / 8][4];
 #pragma unroll
@@ -60,8 +58,6 @@ LD void tile_backprop(const __nv_bfloat16* D, const __nv_bfloat16* W, const __nv
         v[3] = __bfloat162float(H[(g + 8) * kLdH + c + 1]) > 0.0f ? acc[nb][3] : 0.0f;
         *reinterpret_cast<unsigned*>(out + g * kLdH + c) = pack_bf16(v[0], v[1]);
         *reinterpret_cast<unsigned*>(out + (g + 8) * kLdH + c) = pack_bf16(v[2], v[3]);
-        atomicAdd(&gbias[c], v[0] + v[2]);
-        atomicAdd(&gbias[c + 1], v[1] + v[3]);
     }
 }
 
@@ -95,11 +91,13 @@ LD void mixture_grad(const float* raw, V3 wi, float c, float* d) {
     }
 }
 
-// Encodes one record's inputs into row `r` of the tile (lanes 0..15).
-LD void encode_row(__nv_bfloat16* x, int r, const GuideRec& rec) {
+// Encodes one record's inputs into row `r` of the tile: lane r the position
+// features, lane r + 16 the direction features.
+LD void encode_row(__nv_bfloat16* x, int r, bool position, const GuideRec& rec) {
     __nv_bfloat16* row = x + r * kLdIn;
-    guide_encode(v3(rec.p[0], rec.p[1], rec.p[2]), v3(rec.n[0], rec.n[1], rec.n[2]),
-                 v3(rec.wo[0], rec.wo[1], rec.wo[2]), [&](int i, float v) { row[i] = __float2bfloat16(v); });
+    auto st = [&](int i, float v) { row[i] = __float2bfloat16(v); };
+    if (position) guide_encode_position(v3(rec.p[0], rec.p[1], rec.p[2]), st);
+    else guide_encode_direction(v3(rec.n[0], rec.n[1], rec.n[2]), v3(rec.wo[0], rec.wo[1], rec.wo[2]), st);
 }
 
 __global__ void k_guide_coeff_sum(const GuideRec* recs, int n, float* sum) {
@@ -118,55 +116,56 @@ __global__ void k_guide_coeff_sum(const GuideRec* recs, int n, float* sum) {
 
 // ---- training in two passes ---------------------------------------------------
 // Pass 1 (k_guide_fb): per warp tile of 16 records, forward, mixture
-// gradient and backpropagation of the gradients through the layers; the
-// layer inputs (x, h1..h3) and output gradients (d4..d1) go to global memory
-// as BF16 and the bias gradients are summed per block.  Pass 2
-// (k_guide_wgrad): each weight gradient dW = D^T H as a split-K GEMM over the
-// records, accumulated in registers over a slice of records and added to the
-// gradient once per block.
+// gradient and backpropagation through the layers; the layer inputs
+// (x, h1..h3) and the gradients of the layer outputs (d4..d1) go to a
+// per-record BF16 workspace row.  Pass 2 (k_guide_wgrad): every weight and
+// bias gradient, dW = D^T H and db = D^T 1, as one split-K GEMM over the
+// records: each block streams chunks of workspace rows into shared memory
+// with bulk async copies (double-buffered) and keeps its share of the
+// gradient in registers; the per-block partial gradients are summed by
+// k_guide_reduce in block order.
 constexpr int kFbWarps = 7;
-constexpr size_t kFbSmem = sizeof(GuideSmemW) + kFbWarps * sizeof(TrainTile) + 256 * sizeof(float);
-// per-record offsets (BF16 elements) in the pass-1 workspace
+constexpr size_t kFbSmem = sizeof(GuideSmemW) + kFbWarps * sizeof(TrainTile);
+// per-record offsets (BF16 elements) in a workspace row; every block starts
+// on a 16-byte boundary and the row (616 elements, 1232 bytes) is padded so
+// that eight consecutive rows fall in different shared-memory banks
 constexpr int kWsX = 0, kWsH1 = kGIn, kWsH2 = kWsH1 + kGHid, kWsH3 = kWsH2 + kGHid, kWsD4 = kWsH3 + kGHid,
-              kWsD3 = kWsD4 + kGOut, kWsD2 = kWsD3 + kGHid, kWsD1 = kWsD2 + kGHid, kWsRow = kWsD1 + kGHid;
+              kWsD3 = kWsD4 + kGOut, kWsD2 = kWsD3 + kGHid, kWsD1 = kWsD2 + kGHid, kWsRow = kWsD1 + kGHid + 8;
+static_assert(kWsRow * 2 % 16 == 0 && kWsH1 % 8 == 0 && kWsD4 % 8 == 0 && kWsD1 % 8 == 0, "workspace alignment");
 
-// Copies a 16-row tile (ld `ld` in shared memory) to rows r0.. of a global
-// matrix of `cols` columns inside the record workspace (row stride kWsRow).
+// Copies a 16-row tile (ld `ld` in shared memory) to rows r0.. of the
+// workspace column block at `dst` (16-byte vectors).
 LD void tile_store(const __nv_bfloat16* src, int ld, int cols, __nv_bfloat16* dst, int r0, int n) {
-    const int lane = threadIdx.x & 31;
-    for (int e = lane; e < 16 * (cols / 2); e += 32) {
-        int r = e / (cols / 2), c = 2 * (e % (cols / 2));
+    const int lane = threadIdx.x & 31, vec = cols / 8;
+    for (int e = lane; e < 16 * vec; e += 32) {
+        int r = e / vec, c = 8 * (e % vec);
         if (r0 + r < n)
-            *reinterpret_cast<unsigned*>(dst + (size_t)(r0 + r) * kWsRow + c) =
-                *reinterpret_cast<const unsigned*>(src + r * ld + c);
+            *reinterpret_cast<uint4*>(dst + (size_t)(r0 + r) * kWsRow + c) =
+                *reinterpret_cast<const uint4*>(src + r * ld + c);
     }
 }
 
-// Backpropagation without the weight gradient (tile_backprop's data part).
 __global__ void __launch_bounds__(32 * kFbWarps) k_guide_fb(const GuideRec* recs, int n, const __nv_bfloat16* wq,
                                                            const float* master, const float* csum,
-                                                           __nv_bfloat16* ws, float* grad) {
+                                                           __nv_bfloat16* ws) {
     extern __shared__ __align__(16) unsigned char smem[];
     GuideSmemW& W = *reinterpret_cast<GuideSmemW*>(smem);
     TrainTile* tiles = reinterpret_cast<TrainTile*>(smem + sizeof(GuideSmemW));
-    float* sb = reinterpret_cast<float*>(smem + sizeof(GuideSmemW) + kFbWarps * sizeof(TrainTile));
     guide_load_weights(W, wq, master);
-    for (int i = threadIdx.x; i < 256; i += blockDim.x) sb[i] = 0.0f;
     __syncthreads();
-    // bias gradients in sb: b1 [0, 64), b2 [64, 128), b3 [128, 192), b4 [192, 240)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     TrainTile& T = tiles[warp];
     const float inv_sum = *csum > 0.0f ? 1.0f / *csum : 0.0f;
     const int ntiles = (n + 15) / 16;
     for (int tile = blockIdx.x * kFbWarps + warp; tile < ntiles; tile += gridDim.x * kFbWarps) {
-        const int r0 = tile * 16, r = r0 + lane;
+        const int r0 = tile * 16, row = lane & 15, r = r0 + row;
         GuideRec rec{};
-        bool valid = lane < 16 && r < n;
+        const bool valid = r < n;
         if (valid) rec = recs[r];
-        if (lane < 16) {
-            if (valid) encode_row(T.t.x, lane, rec);
-            else for (int i = 0; i < kGIn; ++i) T.t.x[lane * kLdIn + i] = __float2bfloat16(0.0f);
-        }
+        if (valid) encode_row(T.t.x, row, lane < 16, rec);
+        else
+            for (int i = (lane < 16 ? 0 : 96); i < (lane < 16 ? 96 : kGIn); ++i)
+                T.t.x[row * kLdIn + i] = __float2bfloat16(0.0f);
         __syncwarp();
         guide_forward_tile(W, T.t);
         if (lane < 16) {
@@ -176,11 +175,9 @@ __global__ void __launch_bounds__(32 * kFbWarps) k_guide_fb(const GuideRec* recs
             mixture_grad(T.t.raw + lane * kGOut, v3(rec.wi[0], rec.wi[1], rec.wi[2]), c, d);
             for (int i = 0; i < kGOut; i += 2)
                 *reinterpret_cast<unsigned*>(T.dout + lane * kLdH + i) = pack_bf16(d[i], d[i + 1]);
-            for (int i = 0; i < kGOut; ++i)
-                if (d[i] != 0.0f) atomicAdd(&sb[192 + i], d[i]);
         }
         __syncwarp();
-        tile_backprop<kGOut, kGHid, kLdH, kLdH>(T.dout, W.w4, T.t.h3, T.da, sb + 128);
+        tile_backprop<kGOut, kGHid, kLdH, kLdH>(T.dout, W.w4, T.t.h3, T.da);
         __syncwarp();
         tile_store(T.t.x, kLdIn, kGIn, ws + kWsX, r0, n);
         tile_store(T.t.h1, kLdH, kGHid, ws + kWsH1, r0, n);
@@ -188,84 +185,188 @@ __global__ void __launch_bounds__(32 * kFbWarps) k_guide_fb(const GuideRec* recs
         tile_store(T.t.h3, kLdH, kGHid, ws + kWsH3, r0, n);
         tile_store(T.dout, kLdH, kGOut, ws + kWsD4, r0, n);
         tile_store(T.da, kLdH, kGHid, ws + kWsD3, r0, n);
-        tile_backprop<kGHid, kGHid, kLdH, kLdH>(T.da, W.w3, T.t.h2, T.db, sb + 64);
+        tile_backprop<kGHid, kGHid, kLdH, kLdH>(T.da, W.w3, T.t.h2, T.db);
         __syncwarp();
         tile_store(T.db, kLdH, kGHid, ws + kWsD2, r0, n);
-        tile_backprop<kGHid, kGHid, kLdH, kLdH>(T.db, W.w2, T.t.h1, T.da, sb);
+        tile_backprop<kGHid, kGHid, kLdH, kLdH>(T.db, W.w2, T.t.h1, T.da);
         __syncwarp();
         tile_store(T.da, kLdH, kGHid, ws + kWsD1, r0, n);
         __syncwarp();
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < kGHid; i += blockDim.x) {
-        if (sb[i] != 0.0f) atomicAdd(&grad[kGB1 + i], sb[i]);
-        if (sb[64 + i] != 0.0f) atomicAdd(&grad[kGB2 + i], sb[64 + i]);
-        if (sb[128 + i] != 0.0f) atomicAdd(&grad[kGB3 + i], sb[128 + i]);
-    }
-    for (int i = threadIdx.x; i < kGOut; i += blockDim.x)
-        if (sb[192 + i] != 0.0f) atomicAdd(&grad[kGB4 + i], sb[192 + i]);
 }
 
-// grad[O][I] += sum over this block's records of D[s][o] H[s][i] (8 warps;
-// the (16 x 8) output fragments are split over the warps and accumulated in
-// registers over 32-record chunks staged in shared memory).
-constexpr int kWgChunk = 32, kWgSlice = 2048;
-template <int O, int I>
-__global__ void __launch_bounds__(256) k_guide_wgrad(const __nv_bfloat16* ws, int doff, int hoff, int n, float* grad) {
-    constexpr int LDD = O + 8, LDH = I + 8, NB = I / 8, FR = (O / 16) * NB, FPW = (FR + 7) / 8;
-    __shared__ __align__(16) __nv_bfloat16 Ds[kWgChunk * LDD];
-    __shared__ __align__(16) __nv_bfloat16 Hs[kWgChunk * LDH];
+// Pass 2 work units: a 16 x 16 block of one weight gradient (two m16n8
+// fragments) or a 16-row block of one bias gradient (one fragment against a
+// column of ones).  Units 0..87 are the weight blocks (W1 44, W2 16, W3 16,
+// W4 12), units 88..102 the bias blocks (b1 4, b2 4, b3 4, b4 3).
+constexpr int kWgRows = 64, kWgWarps = 16, kWgUnits = 103, kWgMaxUnits = (kWgUnits + kWgWarps - 1) / kWgWarps;
+constexpr size_t kWgChunkBytes = (size_t)kWgRows * kWsRow * 2;
+constexpr size_t kWgSmem = 2 * kWgChunkBytes;
+constexpr long long kWgSpin = 1ll << 24;   // bound on the polls of one chunk's arrival
+
+struct WgUnit {
+    int a_off, b_off;   // workspace column of the A block (D^T) and B block (H^T); b_off < 0: bias
+    int goff, cols;     // gradient offset of the block's first element and the row length
+};
+LD WgUnit wg_unit(int u) {
+    // per layer: D column, H column, weight offset, bias offset, outputs, inputs
+    const int dcol[4] = {kWsD1, kWsD2, kWsD3, kWsD4}, hcol[4] = {kWsX, kWsH1, kWsH2, kWsH3};
+    const int wofs[4] = {kGW1, kGW2, kGW3, kGW4}, bofs[4] = {kGB1, kGB2, kGB3, kGB4};
+    const int outs[4] = {kGHid, kGHid, kGHid, kGOut}, ins[4] = {kGIn, kGHid, kGHid, kGHid};
+    WgUnit w{};
+    if (u < 88) {
+        int l = 0;
+        while (u >= (outs[l] / 16) * (ins[l] / 16)) { u -= (outs[l] / 16) * (ins[l] / 16); ++l; }
+        const int pb = ins[l] / 16, m0 = (u / pb) * 16, n0 = (u % pb) * 16;
+        w.a_off = dcol[l] + m0; w.b_off = hcol[l] + n0;
+        w.goff = wofs[l] + m0 * ins[l] + n0; w.cols = ins[l];
+    } else {
+        u -= 88;
+        int l = 0;
+        while (u >= outs[l] / 16) { u -= outs[l] / 16; ++l; }
+        w.a_off = dcol[l] + u * 16; w.b_off = -1;
+        w.goff = bofs[l] + u * 16; w.cols = 1;
+    }
+    return w;
+}
+
+LD unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+LD void ldsm_x4_trans(unsigned addr, unsigned* r) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0, %1, %2, %3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(addr));
+}
+LD void mbar_init(unsigned bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count));
+}
+LD void bulk_load(unsigned dst, const void* src, unsigned bytes, unsigned bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+                 ::"r"(dst), "l"(src), "r"(bytes), "r"(bar) : "memory");
+}
+// Polls the barrier's phase `parity` at most kWgSpin times; false if it
+// never completed.
+LD bool mbar_wait(unsigned bar, unsigned parity) {
+    for (long long i = 0; i < kWgSpin; ++i) {
+        unsigned done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done) : "r"(bar), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__global__ void __launch_bounds__(32 * kWgWarps, 1) k_guide_wgrad(const __nv_bfloat16* ws, int chunks, float* part,
+                                                                  int* flag) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ __align__(8) unsigned long long bars[2];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
-    float acc[FPW][4];
+    const unsigned buf0 = smem_u32(smem), bar0 = smem_u32(&bars[0]);
+    if (threadIdx.x == 0) {
+        mbar_init(bar0, 1);
+        mbar_init(bar0 + 8, 1);
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    }
+    __syncthreads();
+    // this warp's units
+    const int u_lo = warp * kWgUnits / kWgWarps, u_hi = (warp + 1) * kWgUnits / kWgWarps;
+    int a_off[kWgMaxUnits], b_off[kWgMaxUnits];
 #pragma unroll
-    for (int j = 0; j < FPW; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
-    const int k0 = blockIdx.x * kWgSlice, k1 = min(n, k0 + kWgSlice);
-    for (int c0 = k0; c0 < k1; c0 += kWgChunk) {
-        __syncthreads();
-        for (int e = threadIdx.x; e < kWgChunk * (O / 2); e += blockDim.x) {
-            int r = e / (O / 2), c = 2 * (e % (O / 2));
-            unsigned v = 0;
-            if (c0 + r < k1) v = *reinterpret_cast<const unsigned*>(ws + (size_t)(c0 + r) * kWsRow + doff + c);
-            *reinterpret_cast<unsigned*>(Ds + r * LDD + c) = v;
-        }
-        for (int e = threadIdx.x; e < kWgChunk * (I / 2); e += blockDim.x) {
-            int r = e / (I / 2), c = 2 * (e % (I / 2));
-            unsigned v = 0;
-            if (c0 + r < k1) v = *reinterpret_cast<const unsigned*>(ws + (size_t)(c0 + r) * kWsRow + hoff + c);
-            *reinterpret_cast<unsigned*>(Hs + r * LDH + c) = v;
-        }
-        __syncthreads();
+    for (int j = 0; j < kWgMaxUnits; ++j) {
+        WgUnit w = wg_unit(min(u_lo + j, kWgUnits - 1));
+        a_off[j] = w.a_off; b_off[j] = w.b_off;
+    }
+    float acc[kWgMaxUnits][8];
 #pragma unroll
-        for (int j = 0; j < FPW; ++j) {
-            const int f = warp + 8 * j;
-            if (f < FR) {
-                const int m0 = (f / NB) * 16 + g, n0 = (f % NB) * 8 + g;
+    for (int j = 0; j < kWgMaxUnits; ++j)
 #pragma unroll
-                for (int ks = 0; ks < kWgChunk; ks += 16) {
-                    unsigned a[4], b[2];
-                    const __nv_bfloat16* D = Ds + ks * LDD;
-                    const __nv_bfloat16* H = Hs + ks * LDH;
-                    a[0] = pair2(D + (2 * q) * LDD + m0, D + (2 * q + 1) * LDD + m0);
-                    a[1] = pair2(D + (2 * q) * LDD + m0 + 8, D + (2 * q + 1) * LDD + m0 + 8);
-                    a[2] = pair2(D + (2 * q + 8) * LDD + m0, D + (2 * q + 9) * LDD + m0);
-                    a[3] = pair2(D + (2 * q + 8) * LDD + m0 + 8, D + (2 * q + 9) * LDD + m0 + 8);
-                    b[0] = pair2(H + (2 * q) * LDH + n0, H + (2 * q + 1) * LDH + n0);
-                    b[1] = pair2(H + (2 * q + 8) * LDH + n0, H + (2 * q + 9) * LDH + n0);
-                    mma16816(acc[j], a, b);
+        for (int i = 0; i < 8; ++i) acc[j][i] = 0.0f;
+    // ldmatrix row addresses: A = D^T blocks (matrices k0|m0, k0|m0+8,
+    // k0+8|m0, k0+8|m0+8), B = H^T blocks (k0|n0, k0+8|n0, k0|n0+8, k0+8|n0+8)
+    const int mi = lane >> 3, ri = lane & 7;
+    const int a_lane = (ri + ((mi >> 1) << 3)) * kWsRow + ((mi & 1) << 3);
+    const int b_lane = (ri + ((mi & 1) << 3)) * kWsRow + ((mi >> 1) << 3);
+    const unsigned ones = pack_bf16(1.0f, 1.0f);
+    bool ok = true;
+    if (threadIdx.x == 0 && (int)blockIdx.x < chunks)
+        bulk_load(buf0, ws + (size_t)blockIdx.x * kWgRows * kWsRow, (unsigned)kWgChunkBytes, bar0);
+    int it = 0;
+    for (int c = blockIdx.x; c < chunks; c += gridDim.x, ++it) {
+        const int b = it & 1;
+        const int nxt = c + gridDim.x;
+        if (threadIdx.x == 0 && nxt < chunks)
+            bulk_load(buf0 + (unsigned)((b ^ 1) * kWgChunkBytes), ws + (size_t)nxt * kWgRows * kWsRow,
+                      (unsigned)kWgChunkBytes, bar0 + 8 * (b ^ 1));
+        ok = mbar_wait(bar0 + 8 * b, (it >> 1) & 1);
+        if (!__syncthreads_and(ok)) break;
+        const unsigned base = buf0 + (unsigned)(b * kWgChunkBytes);
+#pragma unroll
+        for (int ks = 0; ks < kWgRows; ks += 16) {
+            const unsigned kb = base + 2u * (unsigned)(ks * kWsRow);
+            int a_cur = -1;
+            unsigned a[4] = {0, 0, 0, 0};
+#pragma unroll
+            for (int j = 0; j < kWgMaxUnits; ++j) {
+                if (u_lo + j < u_hi) {
+                    if (a_off[j] != a_cur) {
+                        ldsm_x4_trans(kb + 2u * (unsigned)(a_lane + a_off[j]), a);
+                        a_cur = a_off[j];
+                    }
+                    if (b_off[j] >= 0) {
+                        unsigned bb[4];
+                        ldsm_x4_trans(kb + 2u * (unsigned)(b_lane + b_off[j]), bb);
+                        mma16816(acc[j], a, bb);
+                        mma16816(acc[j] + 4, a, bb + 2);
+                    } else {
+                        const unsigned bo[2] = {ones, ones};
+                        mma16816(acc[j], a, bo);
+                    }
                 }
             }
         }
+        __syncthreads();
     }
-#pragma unroll
-    for (int j = 0; j < FPW; ++j) {
-        const int f = warp + 8 * j;
-        if (f < FR) {
-            const int m0 = (f / NB) * 16 + g, c = (f % NB) * 8 + 2 * q;
-            atomicAdd(&grad[m0 * I + c], acc[j][0]);
-            atomicAdd(&grad[m0 * I + c + 1], acc[j][1]);
-            atomicAdd(&grad[(m0 + 8) * I + c], acc[j][2]);
-            atomicAdd(&grad[(m0 + 8) * I + c + 1], acc[j][3]);
+    if (!ok) {
+        // give the copies still in flight (this chunk's, the prefetched
+        // one's) a bounded time to land before the shared memory goes away
+        if (threadIdx.x == 0) {
+            atomicExch(flag, 1);
+            const int c = blockIdx.x + it * gridDim.x;
+            mbar_wait(bar0 + 8 * (it & 1), (it >> 1) & 1);
+            if (c + (int)gridDim.x < chunks) mbar_wait(bar0 + 8 * ((it + 1) & 1), ((it + 1) >> 1) & 1);
         }
+        return;
+    }
+    float* dst = part + (size_t)blockIdx.x * kGParams;
+#pragma unroll
+    for (int j = 0; j < kWgMaxUnits; ++j) {
+        if (u_lo + j < u_hi) {
+            const WgUnit w = wg_unit(u_lo + j);
+            if (w.b_off >= 0) {
+                float* o = dst + w.goff;
+                o[g * w.cols + 2 * q] = acc[j][0];
+                o[g * w.cols + 2 * q + 1] = acc[j][1];
+                o[(g + 8) * w.cols + 2 * q] = acc[j][2];
+                o[(g + 8) * w.cols + 2 * q + 1] = acc[j][3];
+                o[g * w.cols + 8 + 2 * q] = acc[j][4];
+                o[g * w.cols + 8 + 2 * q + 1] = acc[j][5];
+                o[(g + 8) * w.cols + 8 + 2 * q] = acc[j][6];
+                o[(g + 8) * w.cols + 8 + 2 * q + 1] = acc[j][7];
+            } else if (q == 0) {
+                dst[w.goff + g] = acc[j][0];
+                dst[w.goff + g + 8] = acc[j][2];
+            }
+        }
+    }
+}
+
+// grad[i] += sum over blocks of part[block][i], in block order.
+__global__ void k_guide_reduce(const float* part, int blocks, float* grad) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kGParams; i += gridDim.x * blockDim.x) {
+        float s = 0.0f;
+        for (int b = 0; b < blocks; ++b) s += part[(size_t)b * kGParams + i];
+        grad[i] += s;
     }
 }
 
@@ -336,11 +437,13 @@ __global__ void k_guide_encode_rows(const float* p01, const float* nrm, const fl
 GuideNet::~GuideNet() { release(); }
 
 void GuideNet::release() {
-    for (void* p : {(void*)master_, (void*)m_, (void*)v_, (void*)grad_, (void*)wq_, (void*)csum_, ws_})
+    for (void* p : {(void*)master_, (void*)m_, (void*)v_, (void*)grad_, (void*)wq_, (void*)csum_, ws_, (void*)part_,
+                    (void*)flag_})
         if (p) cudaFree(p);
-    master_ = m_ = v_ = grad_ = csum_ = nullptr;
+    master_ = m_ = v_ = grad_ = csum_ = part_ = nullptr;
     wq_ = ws_ = nullptr;
-    ws_n_ = 0;
+    flag_ = nullptr;
+    ws_rows_ = part_blocks_ = 0;
 }
 
 int GuideNet::init(int seed, cudaStream_t st) {
@@ -350,6 +453,8 @@ int GuideNet::init(int seed, cudaStream_t st) {
     GCK(cudaMalloc(&v_, kGParams * sizeof(float)));
     GCK(cudaMalloc(&grad_, kGParams * sizeof(float)));
     GCK(cudaMalloc(&csum_, sizeof(float)));
+    GCK(cudaMalloc(&flag_, sizeof(int)));
+    GCK(cudaMemsetAsync(flag_, 0, sizeof(int), st));
     GCK(cudaMalloc(&wq_, kGParams * sizeof(__nv_bfloat16)));
     std::vector<float> w(kGParams, 0.0f);
     std::mt19937 rng((unsigned)seed);
@@ -393,26 +498,44 @@ int GuideNet::gradient(const GuideRec* recs, int n, cudaStream_t st) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    static bool attr_fb = false;
-    if (!attr_fb) {
+    static bool attr = false;
+    if (!attr) {
         GCK(cudaFuncSetAttribute(k_guide_fb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFbSmem));
-        attr_fb = true;
+        GCK(cudaFuncSetAttribute(k_guide_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWgSmem));
+        attr = true;
     }
-    if (ws_n_ < n) {
+    // workspace rows for whole chunks; rows past n stay zero
+    const int chunks = (n + kWgRows - 1) / kWgRows, rows = chunks * kWgRows;
+    const int wblocks = std::min(chunks, sms);
+    if (ws_rows_ < rows || part_blocks_ < wblocks) {
         if (ws_) cudaFree(ws_);
+        if (part_) cudaFree(part_);
         ws_ = nullptr;
-        GCK(cudaMalloc(&ws_, (size_t)n * kWsRow * sizeof(__nv_bfloat16)));
-        ws_n_ = n;
+        part_ = nullptr;
+        ws_rows_ = part_blocks_ = 0;
+        GCK(cudaMalloc(&ws_, (size_t)rows * kWsRow * sizeof(__nv_bfloat16)));
+        GCK(cudaMalloc(&part_, (size_t)sms * kGParams * sizeof(float)));
+        ws_rows_ = rows;
+        part_blocks_ = sms;
     }
     __nv_bfloat16* ws = WQ(ws_);
+    if (rows > n) GCK(cudaMemsetAsync(ws + (size_t)n * kWsRow, 0, (size_t)(rows - n) * kWsRow * sizeof(__nv_bfloat16), st));
     int blocks = std::max(1, std::min(sms, (n + 16 * kFbWarps - 1) / (16 * kFbWarps)));
-    k_guide_fb<<<blocks, 32 * kFbWarps, kFbSmem, st>>>(recs, n, WQ(wq_), master_, csum_, ws, grad_);
-    const int slices = (n + kWgSlice - 1) / kWgSlice;
-    k_guide_wgrad<kGHid, kGIn><<<slices, 256, 0, st>>>(ws, kWsD1, kWsX, n, grad_ + kGW1);
-    k_guide_wgrad<kGHid, kGHid><<<slices, 256, 0, st>>>(ws, kWsD2, kWsH1, n, grad_ + kGW2);
-    k_guide_wgrad<kGHid, kGHid><<<slices, 256, 0, st>>>(ws, kWsD3, kWsH2, n, grad_ + kGW3);
-    k_guide_wgrad<kGOut, kGHid><<<slices, 256, 0, st>>>(ws, kWsD4, kWsH3, n, grad_ + kGW4);
+    k_guide_fb<<<blocks, 32 * kFbWarps, kFbSmem, st>>>(recs, n, WQ(wq_), master_, csum_, ws);
+    k_guide_wgrad<<<wblocks, 32 * kWgWarps, kWgSmem, st>>>(ws, chunks, part_, flag_);
+    k_guide_reduce<<<(kGParams + 255) / 256, 256, 0, st>>>(part_, wblocks, grad_);
     GCK(cudaGetLastError());
+    return 0;
+}
+
+int GuideNet::failed(cudaStream_t st) {
+    int h = 0;
+    GCK(cudaMemcpyAsync(&h, flag_, sizeof(int), cudaMemcpyDeviceToHost, st));
+    GCK(cudaStreamSynchronize(st));
+    if (h) {
+        err_ = "guide training: a bounded wait for a workspace copy gave up";
+        return -3;
+    }
     return 0;
 }
 

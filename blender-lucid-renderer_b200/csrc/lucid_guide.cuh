@@ -47,8 +47,9 @@ LD float one_blob(float x, int b) {
     float d = (x - c) * (float)kGBins;
     return __expf(-0.5f * d * d);
 }
+// Features [0, 96): the position frequencies.
 template <class Store>
-LD void guide_encode(V3 p01, V3 n, V3 wo, Store&& st) {
+LD void guide_encode_position(V3 p01, Store&& st) {
     const float pc[3] = {p01.x, p01.y, p01.z};
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -60,6 +61,10 @@ LD void guide_encode(V3 p01, V3 n, V3 wo, Store&& st) {
             st(a * 2 * kGFreq + 2 * j + 1, c);
         }
     }
+}
+// Features [96, kGIn): normal, one-blob outgoing direction, zero padding.
+template <class Store>
+LD void guide_encode_direction(V3 n, V3 wo, Store&& st) {
     st(96, n.x); st(97, n.y); st(98, n.z);
     float u = sclamp(0.5f * (wo.z + 1.0f), 0.0f, 1.0f);
     float v = atan2f(wo.y, wo.x) * (0.5f * kINV_PI) + 0.5f;
@@ -68,6 +73,11 @@ LD void guide_encode(V3 p01, V3 n, V3 wo, Store&& st) {
         st(99 + kGBins + b, one_blob(v, b));
     }
     for (int i = kGInUsed; i < kGIn; ++i) st(i, 0.0f);
+}
+template <class Store>
+LD void guide_encode(V3 p01, V3 n, V3 wo, Store&& st) {
+    guide_encode_position(p01, st);
+    guide_encode_direction(n, wo, st);
 }
 
 // ---- vMF mixture ----------------------------------------------------------------

@@ -135,7 +135,9 @@ int lucid_guide_gradient(LucidGuide* g, const float* records, int n, float* grad
     e = cudaMemcpyAsync(grad_out, g->net.grad(), lucid::kGuideParams * sizeof(float), cudaMemcpyDeviceToHost, g->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync((void*)g->net.grad(), 0, lucid::kGuideParams * sizeof(float), g->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
-    return e == cudaSuccess ? LUCID_OK : cuda_fail(g, e, "gradient");
+    if (e != cudaSuccess) return cuda_fail(g, e, "gradient");
+    if (g->net.failed(g->stream) != 0) { g->err = g->net.error(); return LUCID_ERR_TIMEOUT; }
+    return LUCID_OK;
 }
 
 int lucid_guide_train(LucidGuide* g, const float* records, int n, float lr) {
@@ -146,7 +148,9 @@ int lucid_guide_train(LucidGuide* g, const float* records, int n, float lr) {
     if (rc != LUCID_OK) return rc;
     if (g->net.train_step((const lucid::GuideRec*)d.p, n, g->stream, lr) != 0) { g->err = g->net.error(); return LUCID_ERR_CUDA; }
     cudaError_t e = cudaStreamSynchronize(g->stream);
-    return e == cudaSuccess ? LUCID_OK : cuda_fail(g, e, "train");
+    if (e != cudaSuccess) return cuda_fail(g, e, "train");
+    if (g->net.failed(g->stream) != 0) { g->err = g->net.error(); return LUCID_ERR_TIMEOUT; }
+    return LUCID_OK;
 }
 
 }  // extern "C"

@@ -35,6 +35,9 @@ public:
     int gradient(const GuideRec* d_recs, int n, cudaStream_t st);
     int adam(cudaStream_t st, float lr);                 // one step; clears the gradient
     int train_step(const GuideRec* d_recs, int n, cudaStream_t st, float lr);
+    // Synchronises `st`; -3 (with error()) if a training kernel gave up a
+    // bounded wait since init.
+    int failed(cudaStream_t st);
     int forward_rows(const float* d_in, int n, float* d_out, cudaStream_t st);
     int encode_rows(const float* p01, const float* nrm, const float* wo, int n, float* out, cudaStream_t st);
     const void* weights_bf16() const { return wq_; }
@@ -51,8 +54,10 @@ private:
     float* grad_ = nullptr;
     float* csum_ = nullptr;
     void* wq_ = nullptr;
-    void* ws_ = nullptr;   // per-record layer inputs and gradients of the last batch (BF16)
-    int ws_n_ = 0;
+    void* ws_ = nullptr;       // per-record layer inputs and gradients of the last batch (BF16)
+    float* part_ = nullptr;    // per-block partial gradients
+    int* flag_ = nullptr;      // set when a bounded device wait gave up
+    int ws_rows_ = 0, part_blocks_ = 0;
     int step_ = 0;
     std::string err_;
 };
