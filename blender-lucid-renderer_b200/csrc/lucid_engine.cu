@@ -791,64 +791,67 @@ __global__ void __launch_bounds__(256) k_bin_scatter(PathView pv, int* cnt, int 
 
 // ---------------------------------------------------------------- guide inference
 // Raw guide outputs for every queued path whose next event is a guidable
-// surface hit: 16 paths per warp-tile through the BF16 tensor-core MLP, the
-// weights staged once per block in shared memory.
-constexpr size_t kInferSmem = sizeof(GuideSmemW) + 4 * sizeof(GuideTile);
+// surface hit: 16 paths per warp-tile through the BF16 tensor-core MLP
+// (16 warps per block, one block per SM), the weights staged once per block
+// in shared memory.  Two lanes encode each path (lanes r and r + 16, half of
+// the features each).
+constexpr int kInferWarps = 16;
+constexpr size_t kInferSmem = sizeof(GuideSmemW) + kInferWarps * sizeof(GuideLeanTile);
 
-__global__ void __launch_bounds__(128) k_guide_infer(DevScene sc, PathView pv, int* cnt, int identity, const int* qin,
-                                                     const __nv_bfloat16* wq, const float* master) {
+__global__ void __launch_bounds__(32 * kInferWarps, 1) k_guide_infer(DevScene sc, PathView pv, int* cnt, int identity,
+                                                                     const int* qin, const __nv_bfloat16* wq,
+                                                                     const float* master) {
     extern __shared__ __align__(16) unsigned char smem[];
     GuideSmemW& W = *reinterpret_cast<GuideSmemW*>(smem);
-    GuideTile* tiles = reinterpret_cast<GuideTile*>(smem + sizeof(GuideSmemW));
+    GuideLeanTile* tiles = reinterpret_cast<GuideLeanTile*>(smem + sizeof(GuideSmemW));
     guide_load_weights(W, wq, master);
     __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    GuideTile& T = tiles[warp];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, rl = lane & 15, half = lane >> 4;
+    GuideLeanTile& T = tiles[warp];
     const int n = *(volatile int*)&cnt[0];
     const int ntiles = (n + 15) / 16;
-    for (int tile = blockIdx.x * 4 + warp; tile < ntiles; tile += gridDim.x * 4) {
+    for (int tile = blockIdx.x * kInferWarps + warp; tile < ntiles; tile += gridDim.x * kInferWarps) {
         int id = -1;
         bool elig = false;
-        if (lane < 16) {
-            const int i = tile * 16 + lane;
-            __nv_bfloat16* row = T.x + lane * kLdIn;
-            if (i < n) {
-                id = identity ? i : qin[i];
-                float4 hh = pv.hit[id];
-                int prim = __float_as_int(hh.w);
-                float2 lh = pv.lhit[id];
-                int li = __float_as_int(lh.x);
-                if (prim >= 0 && !(li >= 0 && lh.y < hh.x)) {
-                    int4 pi = sc.prim_info[prim];
-                    elig = guide_eligible(sc.materials[pi.x]);
-                    if (elig) {
-                        float4 ro = pv.ray_o[id], rd = pv.ray_d[id];
-                        V3 o = f3(ro), d = f3(rd);
-                        V3 p = o + d * hh.x;
-                        V3 fn = f3(sc.prim_fn[prim]);
-                        V3 nn = fn;
-                        if (pi.w) {
-                            float w = 1.0f - hh.y - hh.z;
-                            V3 ni = f3(sc.prim_vn[3 * prim]) * w + f3(sc.prim_vn[3 * prim + 1]) * hh.y +
-                                    f3(sc.prim_vn[3 * prim + 2]) * hh.z;
-                            nn = make_dir_or(ni, fn);
-                        }
-                        V3 p01 = v3((p.x - pv.glo[0]) * pv.gscale[0], (p.y - pv.glo[1]) * pv.gscale[1],
-                                    (p.z - pv.glo[2]) * pv.gscale[2]);
-                        guide_encode(p01, nn, -d, [&](int k, float v) { row[k] = __float2bfloat16(v); });
+        __nv_bfloat16* row = T.x + rl * kLdIn;
+        const int i = tile * 16 + rl;
+        if (i < n) {
+            id = identity ? i : qin[i];
+            float4 hh = pv.hit[id];
+            int prim = __float_as_int(hh.w);
+            float2 lh = pv.lhit[id];
+            int li = __float_as_int(lh.x);
+            if (prim >= 0 && !(li >= 0 && lh.y < hh.x)) {
+                int4 pi = sc.prim_info[prim];
+                elig = guide_eligible(sc.materials[pi.x]);
+                if (elig) {
+                    float4 ro = pv.ray_o[id], rd = pv.ray_d[id];
+                    V3 o = f3(ro), d = f3(rd);
+                    V3 p = o + d * hh.x;
+                    V3 p01 = v3((p.x - pv.glo[0]) * pv.gscale[0], (p.y - pv.glo[1]) * pv.gscale[1],
+                                (p.z - pv.glo[2]) * pv.gscale[2]);
+                    V3 fn = f3(sc.prim_fn[prim]);
+                    V3 nn = fn;
+                    if (pi.w) {
+                        float w = 1.0f - hh.y - hh.z;
+                        V3 ni = f3(sc.prim_vn[3 * prim]) * w + f3(sc.prim_vn[3 * prim + 1]) * hh.y +
+                                f3(sc.prim_vn[3 * prim + 2]) * hh.z;
+                        nn = make_dir_or(ni, fn);
                     }
+                    guide_encode_half(p01, nn, -d, half, [&](int k, float v) { row[k] = __float2bfloat16(v); });
                 }
             }
-            if (!elig)
-                for (int k = 0; k < kGIn; ++k) row[k] = __float2bfloat16(0.0f);
         }
+        if (!elig)
+            for (int k = half * 88; k < half * 88 + 88; ++k) row[k] = __float2bfloat16(0.0f);
         __syncwarp();
-        guide_forward_tile(W, T);
-        if (lane < 16 && elig) {
-            float4* dst = reinterpret_cast<float4*>(pv.gmix + (size_t)id * 40);
-            const float* r = T.raw + lane * kGOut;
+        guide_forward_lean(W, T);
+        // 40 raw outputs per path, 20 by each of its two lanes
+        if (elig) {
+            float4* dst = reinterpret_cast<float4*>(pv.gmix + (size_t)id * 40) + 5 * half;
+            const float* r = T.raw() + rl * kGOut + 20 * half;
 #pragma unroll
-            for (int k = 0; k < 10; ++k) dst[k] = make_float4(r[4 * k], r[4 * k + 1], r[4 * k + 2], r[4 * k + 3]);
+            for (int k = 0; k < 5; ++k) dst[k] = make_float4(r[4 * k], r[4 * k + 1], r[4 * k + 2], r[4 * k + 3]);
         }
         __syncwarp();
     }
@@ -2468,7 +2471,7 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
             ev_end(e);
             if (guide) {
                 e = ev_begin(K_GUIDE, depth);
-                k_guide_infer<<<num_sms_ * 2, 128, kInferSmem, st>>>(
+                k_guide_infer<<<num_sms_, 32 * kInferWarps, kInferSmem, st>>>(
                     ds_->view, pv, cnt, depth == 0, qin, static_cast<const __nv_bfloat16*>(guide_->net.weights_bf16()),
                     guide_->net.master());
                 ev_end(e);

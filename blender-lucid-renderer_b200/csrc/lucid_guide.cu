@@ -18,11 +18,18 @@ static_assert(kGuideParams == kGParams && kGuideInputs == kGIn && kGuideOutputs 
 static inline __nv_bfloat16* WQ(void* p) { return static_cast<__nv_bfloat16*>(p); }
 
 // ---- training tile -----------------------------------------------------------------
+// One warp's 16 records (12.5 KB): the input rows are reused, once they are
+// stored, for the FP32 raw outputs, dL/d(raw) and one gradient buffer; the
+// other gradient buffer reuses h3 once backpropagation has passed it.
 struct TrainTile {
-    GuideTile t;
-    __nv_bfloat16 dout[16 * kLdH];   // dL/d(raw outputs), 48 used
-    __nv_bfloat16 da[16 * kLdH], db[16 * kLdH];
+    __nv_bfloat16 x[16 * kLdIn];
+    __nv_bfloat16 h1[16 * kLdH], h2[16 * kLdH], h3[16 * kLdH];
+    LD float* raw() { return reinterpret_cast<float*>(x); }              // bytes [0, 3072)
+    LD __nv_bfloat16* dout() { return x + 16 * kGOut * 2; }               // bytes [3072, 5376)
+    LD __nv_bfloat16* da() { return x; }                                  // bytes [0, 2304)
+    LD __nv_bfloat16* db() { return h3; }
 };
+static_assert(16 * kGOut * 4 + 16 * kLdH * 2 <= 16 * kLdIn * 2, "raw outputs and dL/d(raw) fit the input rows");
 
 // out[16 x KIN] = (D[16 x MOUT] W[MOUT][KIN]) * (H > 0), as BF16 (ld kLdH).
 template <int MOUT, int KIN, int LDD, int LDW>
@@ -31,21 +38,19 @@ LD void tile_backprop(const __nv_bfloat16* D, const __nv_bfloat16* W, const __nv
     float acc[KIN / 8][4];
 #pragma unroll
     for (int nb = 0; nb < KIN / 8; ++nb) acc[nb][0] = acc[nb][1] = acc[nb][2] = acc[nb][3] = 0.0f;
+    // B[k][n] = W[k][n]: transposed loads of (k0, n0), (k0 + 8, n0),
+    // (k0, n0 + 8), (k0 + 8, n0 + 8)
+    const unsigned d_base = smem_u32(D + ldsm_a_offset(LDD)), w_base = smem_u32(W + ldsm_a_offset(LDW));
 #pragma unroll
     for (int kb = 0; kb < MOUT / 16; ++kb) {
         unsigned a[4];
-        a[0] = ld_pair(D + g * LDD + kb * 16 + 2 * q);
-        a[1] = ld_pair(D + (g + 8) * LDD + kb * 16 + 2 * q);
-        a[2] = ld_pair(D + g * LDD + kb * 16 + 2 * q + 8);
-        a[3] = ld_pair(D + (g + 8) * LDD + kb * 16 + 2 * q + 8);
-        const int k0 = kb * 16 + 2 * q;
+        ldsm_x4(d_base + 32u * kb, a);
 #pragma unroll
-        for (int nb = 0; nb < KIN / 8; ++nb) {
-            const int n0 = nb * 8 + g;
-            unsigned b[2];
-            b[0] = pair2(W + k0 * LDW + n0, W + (k0 + 1) * LDW + n0);
-            b[1] = pair2(W + (k0 + 8) * LDW + n0, W + (k0 + 9) * LDW + n0);
+        for (int nb = 0; nb < KIN / 8; nb += 2) {
+            unsigned b[4];
+            ldsm_x4_trans(w_base + 2u * (unsigned)(kb * 16 * LDW + nb * 8), b);
             mma16816(acc[nb], a, b);
+            mma16816(acc[nb + 1], a, b + 2);
         }
     }
 #pragma unroll
@@ -61,43 +66,59 @@ LD void tile_backprop(const __nv_bfloat16* D, const __nv_bfloat16* W, const __nv
     }
 }
 
-// dL/d(raw) of L = -c log q(wi) for one row (kGOut values, padding zero).
-LD void mixture_grad(const float* raw, V3 wi, float c, float* d) {
-    for (int i = 0; i < kGOut; ++i) d[i] = 0.0f;
-    if (!(c > 0.0f)) return;
+// dL/d(raw) of L = -c log q(wi) for one row, split over two lanes (xor 16)
+// that run the same instructions: half h handles lobes 4h..4h+3 and half 1
+// also the zero padding.  st(i, value) receives every output once.
+template <class Store>
+LD void mixture_grad_half(const float* raw, V3 wi, float c, int half, Store&& st) {
     GuideMix gm;
     guide_mix_from_raw(raw, gm);
-    float p[kGLobes], qsum = 0.0f;
-    for (int k = 0; k < kGLobes; ++k) { p[k] = vmf_pdf(gm.k[k], gm.mu[k], wi); qsum += gm.w[k] * p[k]; }
-    if (!(qsum > 1e-30f)) return;
-    for (int k = 0; k < kGLobes; ++k) {
-        float gam = gm.w[k] * p[k] / qsum;
-        d[k] = c * (gm.w[k] - gam);
-        float r = raw[kGLobes + k];
-        float kap = gm.k[k];
-        if (kap < kGKappaMax) {
-            float e = __expf(-2.0f * kap);
-            float mw = dot(gm.mu[k], wi);
-            float dlogp = 1.0f / kap - 2.0f * e / (1.0f - e) + (mw - 1.0f);
-            d[kGLobes + k] = -c * gam * dlogp * sigmoidf(r);
-        }
-        V3 m = v3(raw[16 + 3 * k], raw[17 + 3 * k], raw[18 + 3 * k]);
-        float l = len(m);
-        if (l > 1e-6f) {
-            float mw = dot(gm.mu[k], wi);
-            V3 gdir = (wi - gm.mu[k] * mw) * (-c * gam * kap / l);
-            d[16 + 3 * k] = gdir.x; d[17 + 3 * k] = gdir.y; d[18 + 3 * k] = gdir.z;
-        }
+    const int k0 = half * (kGLobes / 2);
+    // this half's lobes, picked with constant indices (no local-memory arrays)
+    float w[kGLobes / 2], kp[kGLobes / 2], p[kGLobes / 2], own = 0.0f;
+    V3 mu[kGLobes / 2];
+#pragma unroll
+    for (int j = 0; j < kGLobes / 2; ++j) {
+        w[j] = half ? gm.w[kGLobes / 2 + j] : gm.w[j];
+        kp[j] = half ? gm.k[kGLobes / 2 + j] : gm.k[j];
+        mu[j] = half ? gm.mu[kGLobes / 2 + j] : gm.mu[j];
+        p[j] = vmf_pdf(kp[j], mu[j], wi);
+        own += w[j] * p[j];
     }
+    const float other = __shfl_xor_sync(0xffffffffu, own, 16);
+    const float qsum = half ? other + own : own + other;
+    const bool live = c > 0.0f && qsum > 1e-30f;
+#pragma unroll
+    for (int j = 0; j < kGLobes / 2; ++j) {
+        const int k = k0 + j;
+        float dl = 0.0f, dk = 0.0f;
+        V3 gdir = v3(0.0f, 0.0f, 0.0f);
+        if (live) {
+            const float gam = w[j] * p[j] / qsum;
+            dl = c * (w[j] - gam);
+            const float kap = kp[j], mw = dot(mu[j], wi);
+            if (kap < kGKappaMax) {
+                float e = __expf(-2.0f * kap);
+                float dlogp = 1.0f / kap - 2.0f * e / (1.0f - e) + (mw - 1.0f);
+                dk = -c * gam * dlogp * sigmoidf(raw[kGLobes + k]);
+            }
+            const float l = len(v3(raw[16 + 3 * k], raw[17 + 3 * k], raw[18 + 3 * k]));
+            if (l > 1e-6f) gdir = (wi - mu[j] * mw) * (-c * gam * kap / l);
+        }
+        st(k, dl);
+        st(kGLobes + k, dk);
+        st(16 + 3 * k, gdir.x); st(17 + 3 * k, gdir.y); st(18 + 3 * k, gdir.z);
+    }
+    if (half)
+        for (int i = 40; i < kGOut; ++i) st(i, 0.0f);
 }
 
-// Encodes one record's inputs into row `r` of the tile: lane r the position
-// features, lane r + 16 the direction features.
-LD void encode_row(__nv_bfloat16* x, int r, bool position, const GuideRec& rec) {
+// Encodes one record's inputs into row `r` of the tile, half of the
+// features per lane (lanes r and r + 16).
+LD void encode_row(__nv_bfloat16* x, int r, int half, const GuideRec& rec) {
     __nv_bfloat16* row = x + r * kLdIn;
-    auto st = [&](int i, float v) { row[i] = __float2bfloat16(v); };
-    if (position) guide_encode_position(v3(rec.p[0], rec.p[1], rec.p[2]), st);
-    else guide_encode_direction(v3(rec.n[0], rec.n[1], rec.n[2]), v3(rec.wo[0], rec.wo[1], rec.wo[2]), st);
+    guide_encode_half(v3(rec.p[0], rec.p[1], rec.p[2]), v3(rec.n[0], rec.n[1], rec.n[2]),
+                      v3(rec.wo[0], rec.wo[1], rec.wo[2]), half, [&](int i, float v) { row[i] = __float2bfloat16(v); });
 }
 
 __global__ void k_guide_coeff_sum(const GuideRec* recs, int n, float* sum) {
@@ -124,7 +145,7 @@ __global__ void k_guide_coeff_sum(const GuideRec* recs, int n, float* sum) {
 // with bulk async copies (double-buffered) and keeps its share of the
 // gradient in registers; the per-block partial gradients are summed by
 // k_guide_reduce in block order.
-constexpr int kFbWarps = 7;
+constexpr int kFbWarps = 14;
 constexpr size_t kFbSmem = sizeof(GuideSmemW) + kFbWarps * sizeof(TrainTile);
 // per-record offsets (BF16 elements) in a workspace row; every block starts
 // on a 16-byte boundary and the row (616 elements, 1232 bytes) is padded so
@@ -158,39 +179,45 @@ __global__ void __launch_bounds__(32 * kFbWarps) k_guide_fb(const GuideRec* recs
     const float inv_sum = *csum > 0.0f ? 1.0f / *csum : 0.0f;
     const int ntiles = (n + 15) / 16;
     for (int tile = blockIdx.x * kFbWarps + warp; tile < ntiles; tile += gridDim.x * kFbWarps) {
-        const int r0 = tile * 16, row = lane & 15, r = r0 + row;
+        const int r0 = tile * 16, row = lane & 15, r = r0 + row, half = lane >> 4;
         GuideRec rec{};
         const bool valid = r < n;
         if (valid) rec = recs[r];
-        if (valid) encode_row(T.t.x, row, lane < 16, rec);
+        if (valid) encode_row(T.x, row, half, rec);
         else
-            for (int i = (lane < 16 ? 0 : 96); i < (lane < 16 ? 96 : kGIn); ++i)
-                T.t.x[row * kLdIn + i] = __float2bfloat16(0.0f);
+            for (int i = half * 88; i < half * 88 + 88; ++i) T.x[row * kLdIn + i] = __float2bfloat16(0.0f);
         __syncwarp();
-        guide_forward_tile(W, T.t);
-        if (lane < 16) {
+        tile_layer<kGIn, kGHid, kLdIn, kLdIn, true>(T.x, W.w1, W.b1, T.h1, nullptr);
+        __syncwarp();
+        tile_store(T.x, kLdIn, kGIn, ws + kWsX, r0, n);
+        tile_layer<kGHid, kGHid, kLdH, kLdH, true>(T.h1, W.w2, W.b2, T.h2, nullptr);
+        __syncwarp();
+        tile_layer<kGHid, kGHid, kLdH, kLdH, true>(T.h2, W.w3, W.b3, T.h3, nullptr);
+        __syncwarp();
+        tile_layer<kGHid, kGOut, kLdH, kLdH, false>(T.h3, W.w4, W.b4, nullptr, T.raw());
+        __syncwarp();
+        {
             float F = 0.2126f * rec.L[0] + 0.7152f * rec.L[1] + 0.0722f * rec.L[2];
             float c = (valid && F > 0.0f && rec.pdf > 0.0f && isfinite(F)) ? F / rec.pdf * inv_sum : 0.0f;
-            float d[kGOut];
-            mixture_grad(T.t.raw + lane * kGOut, v3(rec.wi[0], rec.wi[1], rec.wi[2]), c, d);
-            for (int i = 0; i < kGOut; i += 2)
-                *reinterpret_cast<unsigned*>(T.dout + lane * kLdH + i) = pack_bf16(d[i], d[i + 1]);
+            __nv_bfloat16* drow = T.dout() + row * kLdH;
+            mixture_grad_half(T.raw() + row * kGOut, v3(rec.wi[0], rec.wi[1], rec.wi[2]), c, half,
+                              [&](int i, float v) { drow[i] = __float2bfloat16(v); });
         }
         __syncwarp();
-        tile_backprop<kGOut, kGHid, kLdH, kLdH>(T.dout, W.w4, T.t.h3, T.da);
+        tile_backprop<kGOut, kGHid, kLdH, kLdH>(T.dout(), W.w4, T.h3, T.da());
         __syncwarp();
-        tile_store(T.t.x, kLdIn, kGIn, ws + kWsX, r0, n);
-        tile_store(T.t.h1, kLdH, kGHid, ws + kWsH1, r0, n);
-        tile_store(T.t.h2, kLdH, kGHid, ws + kWsH2, r0, n);
-        tile_store(T.t.h3, kLdH, kGHid, ws + kWsH3, r0, n);
-        tile_store(T.dout, kLdH, kGOut, ws + kWsD4, r0, n);
-        tile_store(T.da, kLdH, kGHid, ws + kWsD3, r0, n);
-        tile_backprop<kGHid, kGHid, kLdH, kLdH>(T.da, W.w3, T.t.h2, T.db);
+        tile_store(T.h1, kLdH, kGHid, ws + kWsH1, r0, n);
+        tile_store(T.h2, kLdH, kGHid, ws + kWsH2, r0, n);
+        tile_store(T.h3, kLdH, kGHid, ws + kWsH3, r0, n);
+        tile_store(T.dout(), kLdH, kGOut, ws + kWsD4, r0, n);
+        tile_store(T.da(), kLdH, kGHid, ws + kWsD3, r0, n);
         __syncwarp();
-        tile_store(T.db, kLdH, kGHid, ws + kWsD2, r0, n);
-        tile_backprop<kGHid, kGHid, kLdH, kLdH>(T.db, W.w2, T.t.h1, T.da);
+        tile_backprop<kGHid, kGHid, kLdH, kLdH>(T.da(), W.w3, T.h2, T.db());
         __syncwarp();
-        tile_store(T.da, kLdH, kGHid, ws + kWsD1, r0, n);
+        tile_store(T.db(), kLdH, kGHid, ws + kWsD2, r0, n);
+        tile_backprop<kGHid, kGHid, kLdH, kLdH>(T.db(), W.w2, T.h1, T.da());
+        __syncwarp();
+        tile_store(T.da(), kLdH, kGHid, ws + kWsD1, r0, n);
         __syncwarp();
     }
 }
@@ -230,12 +257,6 @@ LD WgUnit wg_unit(int u) {
     return w;
 }
 
-LD unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-LD void ldsm_x4_trans(unsigned addr, unsigned* r) {
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0, %1, %2, %3}, [%4];\n"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(addr));
-}
 LD void mbar_init(unsigned bar, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count));
 }

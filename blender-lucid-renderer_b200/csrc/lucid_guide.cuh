@@ -79,6 +79,35 @@ LD void guide_encode(V3 p01, V3 n, V3 wo, Store&& st) {
     guide_encode_position(p01, st);
     guide_encode_direction(n, wo, st);
 }
+// The same features split over two lanes that run the same instructions:
+// half 0 writes frequencies 0..7, the normal and the cos-theta one-blob;
+// half 1 frequencies 8..15, the phi one-blob and the padding.
+template <class Store>
+LD void guide_encode_half(V3 p01, V3 n, V3 wo, int half, Store&& st) {
+    const float pc[3] = {p01.x, p01.y, p01.z};
+    const int j0 = half * (kGFreq / 2);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+#pragma unroll 2
+        for (int j = j0; j < j0 + kGFreq / 2; ++j) {
+            float s, c;
+            sincospif(pc[a] * (float)(1 << j), &s, &c);
+            st(a * 2 * kGFreq + 2 * j, s);
+            st(a * 2 * kGFreq + 2 * j + 1, c);
+        }
+    }
+    float x;
+    if (half == 0) {
+        st(96, n.x); st(97, n.y); st(98, n.z);
+        x = sclamp(0.5f * (wo.z + 1.0f), 0.0f, 1.0f);
+    } else {
+        x = atan2f(wo.y, wo.x) * (0.5f * kINV_PI) + 0.5f;
+        for (int i = kGInUsed; i < kGIn; ++i) st(i, 0.0f);
+    }
+    const int base = 99 + half * kGBins;
+#pragma unroll 4
+    for (int b = 0; b < kGBins; ++b) st(base + b, one_blob(x, b));
+}
 
 // ---- vMF mixture ----------------------------------------------------------------
 LD float softplusf(float x) { return x > 20.0f ? x : log1pf(__expf(x)); }
@@ -191,28 +220,56 @@ LD unsigned pair2(const __nv_bfloat16* a, const __nv_bfloat16* b) {
     return *reinterpret_cast<unsigned*>(&v);
 }
 
+// ldmatrix: four 8x8 BF16 matrices, one 16-byte row address per lane
+// (lanes 8j..8j+7 address the rows of matrix j); register j of a lane holds
+// the two elements of matrix j at row lane/4, columns 2(lane%4) and +1 (the
+// transposed variant: rows 2(lane%4) and +1 of column lane/4).
+LD unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+LD void ldsm_x4(unsigned addr, unsigned* r) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(addr));
+}
+LD void ldsm_x4_trans(unsigned addr, unsigned* r) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0, %1, %2, %3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(addr));
+}
+// Lane row addresses (element offsets) for a 16x16 row-major A block:
+// matrices (r0, k0), (r0 + 8, k0), (r0, k0 + 8), (r0 + 8, k0 + 8) = a0..a3.
+LD int ldsm_a_offset(int ld) {
+    const int lane = threadIdx.x & 31, j = lane >> 3, r = lane & 7;
+    return (r + ((j & 1) << 3)) * ld + ((j >> 1) << 3);
+}
+// ... and for the B fragments of two n-blocks of W stored [N][K]: matrices
+// (n0, k0), (n0, k0 + 8), (n0 + 8, k0), (n0 + 8, k0 + 8) = (b0, b1) of n0,
+// then of n0 + 8.
+LD int ldsm_b_offset(int ld) {
+    const int lane = threadIdx.x & 31, j = lane >> 3, r = lane & 7;
+    return (r + ((j >> 1) << 3)) * ld + ((j & 1) << 3);
+}
+
 // out[16 x N] = act(A[16 x K] W^T + b), W stored [N][K]: one warp.  With
 // RELU the result is stored as BF16 (ld kLdH); otherwise as FP32 (ld N).
 template <int K, int N, int LDA, int LDW, bool RELU>
 LD void tile_layer(const __nv_bfloat16* A, const __nv_bfloat16* W, const float* bias, __nv_bfloat16* outh,
                    float* outf) {
+    static_assert(N % 16 == 0 && K % 16 == 0, "tile shape");
     const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
     float acc[N / 8][4];
 #pragma unroll
     for (int nb = 0; nb < N / 8; ++nb) acc[nb][0] = acc[nb][1] = acc[nb][2] = acc[nb][3] = 0.0f;
+    const unsigned a_base = smem_u32(A + ldsm_a_offset(LDA)), w_base = smem_u32(W + ldsm_b_offset(LDW));
 #pragma unroll
     for (int kb = 0; kb < K / 16; ++kb) {
         unsigned a[4];
-        a[0] = ld_pair(A + g * LDA + kb * 16 + 2 * q);
-        a[1] = ld_pair(A + (g + 8) * LDA + kb * 16 + 2 * q);
-        a[2] = ld_pair(A + g * LDA + kb * 16 + 2 * q + 8);
-        a[3] = ld_pair(A + (g + 8) * LDA + kb * 16 + 2 * q + 8);
+        ldsm_x4(a_base + 32u * kb, a);
 #pragma unroll
-        for (int nb = 0; nb < N / 8; ++nb) {
-            unsigned b[2];
-            b[0] = ld_pair(W + (nb * 8 + g) * LDW + kb * 16 + 2 * q);
-            b[1] = ld_pair(W + (nb * 8 + g) * LDW + kb * 16 + 2 * q + 8);
+        for (int nb = 0; nb < N / 8; nb += 2) {
+            unsigned b[4];
+            ldsm_x4(w_base + 2u * (unsigned)(nb * 8 * LDW + kb * 16), b);
             mma16816(acc[nb], a, b);
+            mma16816(acc[nb + 1], a, b + 2);
         }
     }
 #pragma unroll
@@ -239,6 +296,25 @@ LD void guide_forward_tile(const GuideSmemW& w, GuideTile& t) {
     tile_layer<kGHid, kGHid, kLdH, kLdH, true>(t.h2, w.w3, w.b3, t.h3, nullptr);
     __syncwarp();
     tile_layer<kGHid, kGOut, kLdH, kLdH, false>(t.h3, w.w4, w.b4, nullptr, t.raw);
+    __syncwarp();
+}
+
+// Inference tile: the layers alternate between two activation buffers and
+// the raw outputs overwrite the inputs (10.25 KB per warp).
+struct GuideLeanTile {
+    __nv_bfloat16 x[16 * kLdIn];   // inputs, then the FP32 raw outputs (16 x kGOut)
+    __nv_bfloat16 ha[16 * kLdH], hb[16 * kLdH];
+    LD float* raw() { return reinterpret_cast<float*>(x); }
+};
+static_assert(sizeof(float) * 16 * kGOut <= sizeof(__nv_bfloat16) * 16 * kLdIn, "raw outputs fit the input rows");
+LD void guide_forward_lean(const GuideSmemW& w, GuideLeanTile& t) {
+    tile_layer<kGIn, kGHid, kLdIn, kLdIn, true>(t.x, w.w1, w.b1, t.ha, nullptr);
+    __syncwarp();
+    tile_layer<kGHid, kGHid, kLdH, kLdH, true>(t.ha, w.w2, w.b2, t.hb, nullptr);
+    __syncwarp();
+    tile_layer<kGHid, kGHid, kLdH, kLdH, true>(t.hb, w.w3, w.b3, t.ha, nullptr);
+    __syncwarp();
+    tile_layer<kGHid, kGOut, kLdH, kLdH, false>(t.ha, w.w4, w.b4, nullptr, t.raw());
     __syncwarp();
 }
 
