@@ -101,7 +101,7 @@ struct PathView {
     int4* rec_cnt;     // bounces, nee tests, nee occluded
     unsigned long long* rec_hash;
     // path guiding (null when off)
-    float* gmix;       // 40 raw network outputs per path (k_guide_infer)
+    float* gmix;       // compact guide mixture per path (k_guide_infer, kGMixFloats)
     int4* gslot;       // training records of the path's 3 latest guided vertices (-1: none)
     float4* ginv;      // 3 per path: 1 / throughput after each of those vertices
     GuideRec* grec;    // training records of this wave
@@ -550,17 +550,7 @@ LD ShadeResult shade_path(const DevScene& sc, const FrameParams& f, const PathVi
         }
         bool transmissive = m.transmission > 0.5f;
         const bool guided = GUIDE && guide_eligible(dm);
-        GuideMix gm;
-        if (guided) {
-            float raw[kGOut];
-            const float4* src = reinterpret_cast<const float4*>(pv.gmix + (size_t)id * 40);
-#pragma unroll
-            for (int k = 0; k < 10; ++k) {
-                float4 v = src[k];
-                raw[4 * k] = v.x; raw[4 * k + 1] = v.y; raw[4 * k + 2] = v.z; raw[4 * k + 3] = v.w;
-            }
-            guide_mix_from_raw(raw, gm);
-        }
+        const float* gm = GUIDE ? pv.gmix + (size_t)id * kGMixFloats : nullptr;
         if (nee && sc.num_lights > 0 && !has_em && !transmissive) {
             float usel = randf(rng);
             int li = select_light(sc, usel);
@@ -577,7 +567,7 @@ LD ShadeResult shade_path(const DevScene& sc, const FrameParams& f, const PathVi
                         RGB c;
                         if (mis) {
                             float pb = pdf_bsdf(m, wo, ls.dir, sn);
-                            if (guided) pb = 0.5f * pb + 0.5f * guide_pdf(gm, ls.dir);
+                            if (guided) pb = 0.5f * pb + 0.5f * guide_pdf_c(gm, ls.dir);
                             float mw = mis_power(pl, pb);
                             RGB bw = bsdf_weight(fb, nl, pl);
                             if (algo == ALGO_VOLUME_MIS) {
@@ -604,10 +594,10 @@ LD ShadeResult shade_path(const DevScene& sc, const FrameParams& f, const PathVi
             float usel = randf(rng);
             float u1 = randf(rng), u2 = randf(rng), u3 = randf(rng);
             if (usel < 0.5f) wi = sample_bsdf(m, wo, smp_n, u1, u2, u3, rng).wi;
-            else wi = guide_sample(gm, u1, u2, u3);
+            else wi = guide_sample_c(gm, u1, u2, u3);
             float c = dot(smp_n, wi);
             if (c <= 1e-6f) break;
-            gpdf = 0.5f * pdf_bsdf(m, wo, wi, smp_n) + 0.5f * guide_pdf(gm, wi);
+            gpdf = 0.5f * pdf_bsdf(m, wo, wi, smp_n) + 0.5f * guide_pdf_c(gm, wi);
             if (!(gpdf > MIN_PDF)) break;
             T = mul(T, bsdf_weight(eval_bsdf(m, wo, wi, smp_n), c, gpdf));
             last_pdf = gpdf;
@@ -636,10 +626,16 @@ LD ShadeResult shade_path(const DevScene& sc, const FrameParams& f, const PathVi
         new_o = p; new_d = wi;
         out.cont = true;
         if (guided) {
-            atomicAdd(&pv.gcount[1], 1);
+            // warp-aggregated counters: guided vertices, then record slots
+            unsigned am = __activemask();
+            int leader = __ffs(am) - 1;
+            if ((int)lane_id() == leader) atomicAdd(&pv.gcount[1], __popc(am));
             unsigned hsh = murmur3_finalize((unsigned)id * 0x9E3779B9u ^ (unsigned)(depth + 1) * 0x85EBCA6Bu);
             if (hsh < pv.gkeep) {
-                int r = atomicAdd(&pv.gcount[0], 1);
+                unsigned km = __activemask();
+                int kl = __ffs(km) - 1, rb = 0;
+                if ((int)lane_id() == kl) rb = atomicAdd(&pv.gcount[0], __popc(km));
+                int r = __shfl_sync(km, rb, kl) + __popc(km & lanemask_lt());
                 if (r < pv.gcap) {
                     GuideRec g;
                     g.p[0] = (p.x - pv.glo[0]) * pv.gscale[0];
@@ -846,12 +842,14 @@ __global__ void __launch_bounds__(32 * kInferWarps, 1) k_guide_infer(DevScene sc
             for (int k = half * 88; k < half * 88 + 88; ++k) row[k] = __float2bfloat16(0.0f);
         __syncwarp();
         guide_forward_lean(W, T);
-        // 40 raw outputs per path, 20 by each of its two lanes
+        // the compact mixture of each path, half by each of its two lanes
         if (elig) {
-            float4* dst = reinterpret_cast<float4*>(pv.gmix + (size_t)id * 40) + 5 * half;
-            const float* r = T.raw() + rl * kGOut + 20 * half;
+            float4 o[5];
+            guide_compact_half(T.raw() + rl * kGOut, half, o);
+            float4* dst = reinterpret_cast<float4*>(pv.gmix + (size_t)id * kGMixFloats);
 #pragma unroll
-            for (int k = 0; k < 5; ++k) dst[k] = make_float4(r[4 * k], r[4 * k + 1], r[4 * k + 2], r[4 * k + 3]);
+            for (int k = 0; k < 4; ++k) dst[4 * half + k] = o[k];
+            dst[8 + half] = o[4];
         }
         __syncwarp();
     }
@@ -2589,7 +2587,7 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
 int Engine::guide_buffers(long long paths) {
     GuideState& G = *guide_;
     if (G.cap < paths) {
-        CK(G.gmix.alloc((size_t)paths * 40));
+        CK(G.gmix.alloc((size_t)paths * kGMixFloats));
         CK(G.gslot.alloc((size_t)paths));
         CK(G.ginv.alloc((size_t)paths * 3));
         G.cap = paths;

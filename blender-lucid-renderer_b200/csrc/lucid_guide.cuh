@@ -159,6 +159,67 @@ LD V3 guide_sample(const GuideMix& g, float u0, float u1, float u2) {
     return make_dir_or(t * (r * cs) + b * (r * s) + g.mu[lobe] * w, g.mu[lobe]);
 }
 
+// ---- compact mixture (inference output, read by shading) ------------------------
+// 40 floats per vertex: per lobe l a float4 (kappa mu, log(w norm) - kappa),
+// so that the mixture density is sum_l exp(A_l.xyz . wi + A_l.w), then the
+// cumulative lobe weights.  Lanes h = 0, 1 of a row write lobes 4h..4h+3
+// (float4s h*4.. and the cumulative weights 4h..4h+3).
+constexpr int kGMixFloats = 40;
+LD void guide_compact_half(const float* raw, int half, float4* out) {
+    float mx = raw[0];
+    for (int i = 1; i < kGLobes; ++i) mx = fmaxf(mx, raw[i]);
+    float e[kGLobes], sum = 0.0f;
+#pragma unroll
+    for (int i = 0; i < kGLobes; ++i) { e[i] = __expf(raw[i] - mx); sum += e[i]; }
+    float cw[kGLobes], c = 0.0f;
+#pragma unroll
+    for (int i = 0; i < kGLobes; ++i) { c += e[i] / sum; cw[i] = c; }
+#pragma unroll
+    for (int j = 0; j < kGLobes / 2; ++j) {
+        const int l = half * (kGLobes / 2) + j;
+        const float w = e[l] / sum;
+        const float kappa = fminf(softplusf(raw[kGLobes + l]) + kGKappaMin, kGKappaMax);
+        V3 m = v3(raw[16 + 3 * l], raw[17 + 3 * l], raw[18 + 3 * l]);
+        const float len_m = len(m);
+        const V3 mu = len_m > 1e-6f ? m / len_m : v3(0.0f, 0.0f, 1.0f);
+        const float norm = kappa / (kTWO_PI * (1.0f - __expf(-2.0f * kappa)));
+        out[j] = make_float4(kappa * mu.x, kappa * mu.y, kappa * mu.z, logf(fmaxf(w * norm, 1e-30f)) - kappa);
+    }
+    out[4] = half ? make_float4(cw[4], cw[5], cw[6], cw[7]) : make_float4(cw[0], cw[1], cw[2], cw[3]);
+}
+LD float guide_pdf_c(const float* gm, V3 wi) {
+    const float4* A = reinterpret_cast<const float4*>(gm);
+    float p = 0.0f;
+#pragma unroll
+    for (int l = 0; l < kGLobes; ++l) {
+        const float4 a = A[l];
+        p += __expf(a.x * wi.x + a.y * wi.y + a.z * wi.z + a.w);
+    }
+    return p;
+}
+// Lobe by u0 from the cumulative weights, then the vMF inversion of
+// guide_sample on that lobe.
+LD V3 guide_sample_c(const float* gm, float u0, float u1, float u2) {
+    const float4* A = reinterpret_cast<const float4*>(gm);
+    const float4 c0 = A[8], c1 = A[9];
+    const float cw[kGLobes] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+    int lobe = kGLobes - 1;
+#pragma unroll
+    for (int i = kGLobes - 2; i >= 0; --i)
+        if (u0 < cw[i]) lobe = i;
+    const float4 a = A[lobe];
+    const float kappa = sqrtf(a.x * a.x + a.y * a.y + a.z * a.z);
+    const V3 mu = kappa > 0.0f ? v3(a.x, a.y, a.z) / kappa : v3(0.0f, 0.0f, 1.0f);
+    float w = 1.0f + logf(u1 + (1.0f - u1) * __expf(-2.0f * kappa)) / kappa;
+    w = sclamp(w, -1.0f, 1.0f);
+    float r = sqrtf(fmaxf(0.0f, 1.0f - w * w));
+    float s, cs;
+    sincospif(2.0f * u2, &s, &cs);
+    V3 t, b;
+    onb(mu, t, b);
+    return make_dir_or(t * (r * cs) + b * (r * s) + mu * w, mu);
+}
+
 // ---- tensor-core tiles ---------------------------------------------------------
 // mma.sync.m16n8k16 BF16 -> FP32.  Fragment ownership (PTX ISA, "Matrix
 // fragments for mma.m16n8k16"): with g = lane / 4 and q = lane % 4,
