@@ -156,7 +156,7 @@ struct GuideState {
     long long cap = 0;
     float keep = 1.0f;
     float lr = 1e-2f;
-    int steps = 4;   // Adam steps per wave, each on its own batch of records
+    int steps = 2;   // Adam steps per wave, each on its own batch of records
     bool on = false;
 };
 

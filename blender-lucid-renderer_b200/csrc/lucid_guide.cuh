@@ -47,6 +47,13 @@ LD float one_blob(float x, int b) {
     float d = (x - c) * (float)kGBins;
     return __expf(-0.5f * d * d);
 }
+// sin and cos of pi t: t reduced exactly to r = t - 2 rint(t / 2) in
+// [-1, 1], then the hardware approximations on [-pi, pi] (absolute error
+// below 1e-6, far under the BF16 rounding the features go through).
+LD void sincospi_fast(float t, float* s, float* c) {
+    const float r = t - 2.0f * rintf(0.5f * t);
+    __sincosf(kPI * r, s, c);
+}
 // Features [0, 96): the position frequencies.
 template <class Store>
 LD void guide_encode_position(V3 p01, Store&& st) {
@@ -56,7 +63,7 @@ LD void guide_encode_position(V3 p01, Store&& st) {
         float x = pc[a];
         for (int j = 0; j < kGFreq; ++j) {
             float s, c;
-            sincospif(x * (float)(1 << j), &s, &c);
+            sincospi_fast(x * (float)(1 << j), &s, &c);
             st(a * 2 * kGFreq + 2 * j, s);
             st(a * 2 * kGFreq + 2 * j + 1, c);
         }
@@ -91,7 +98,7 @@ LD void guide_encode_half(V3 p01, V3 n, V3 wo, int half, Store&& st) {
 #pragma unroll 2
         for (int j = j0; j < j0 + kGFreq / 2; ++j) {
             float s, c;
-            sincospif(pc[a] * (float)(1 << j), &s, &c);
+            sincospi_fast(pc[a] * (float)(1 << j), &s, &c);
             st(a * 2 * kGFreq + 2 * j, s);
             st(a * 2 * kGFreq + 2 * j + 1, c);
         }
@@ -171,19 +178,23 @@ LD void guide_compact_half(const float* raw, int half, float4* out) {
     float e[kGLobes], sum = 0.0f;
 #pragma unroll
     for (int i = 0; i < kGLobes; ++i) { e[i] = __expf(raw[i] - mx); sum += e[i]; }
+    const float inv = 1.0f / sum, lsum = __logf(sum);
     float cw[kGLobes], c = 0.0f;
 #pragma unroll
-    for (int i = 0; i < kGLobes; ++i) { c += e[i] / sum; cw[i] = c; }
+    for (int i = 0; i < kGLobes; ++i) { c += e[i] * inv; cw[i] = c; }
 #pragma unroll
     for (int j = 0; j < kGLobes / 2; ++j) {
         const int l = half * (kGLobes / 2) + j;
-        const float w = e[l] / sum;
-        const float kappa = fminf(softplusf(raw[kGLobes + l]) + kGKappaMin, kGKappaMax);
-        V3 m = v3(raw[16 + 3 * l], raw[17 + 3 * l], raw[18 + 3 * l]);
-        const float len_m = len(m);
-        const V3 mu = len_m > 1e-6f ? m / len_m : v3(0.0f, 0.0f, 1.0f);
-        const float norm = kappa / (kTWO_PI * (1.0f - __expf(-2.0f * kappa)));
-        out[j] = make_float4(kappa * mu.x, kappa * mu.y, kappa * mu.z, logf(fmaxf(w * norm, 1e-30f)) - kappa);
+        const float x = raw[kGLobes + l];
+        const float sp = x > 20.0f ? x : __logf(1.0f + __expf(x));
+        const float kappa = fminf(sp + kGKappaMin, kGKappaMax);
+        const V3 m = v3(raw[16 + 3 * l], raw[17 + 3 * l], raw[18 + 3 * l]);
+        const float l2 = dot(m, m);
+        const V3 mu = l2 > 1e-12f ? m * rsqrtf(l2) : v3(0.0f, 0.0f, 1.0f);
+        // log(w) + log(kappa / (2 pi (1 - e^{-2 kappa}))) - kappa
+        const float lw = raw[l] - mx - lsum;
+        const float ln = __logf(kappa) - __logf(kTWO_PI * (1.0f - __expf(-2.0f * kappa)));
+        out[j] = make_float4(kappa * mu.x, kappa * mu.y, kappa * mu.z, lw + ln - kappa);
     }
     out[4] = half ? make_float4(cw[4], cw[5], cw[6], cw[7]) : make_float4(cw[0], cw[1], cw[2], cw[3]);
 }

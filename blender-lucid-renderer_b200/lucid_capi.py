@@ -344,7 +344,7 @@ class Context:
     def guide_enable(self, on: bool = True, seed: int = 1):
         self._check(self.lib.lucid_cuda_guide_enable(self.h, int(on), seed))
 
-    def guide_config(self, steps_per_wave: int = 4, lr: float = 1e-2):
+    def guide_config(self, steps_per_wave: int = 2, lr: float = 1e-2):
         self._check(self.lib.lucid_cuda_guide_config(self.h, steps_per_wave, ctypes.c_float(lr)))
 
     def guide_steps(self) -> int:

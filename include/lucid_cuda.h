@@ -346,7 +346,7 @@ int lucid_guide_train(LucidGuide* guide, const float* records, int n, float lr);
 int lucid_cuda_guide_enable(LucidCudaCtx* ctx, int on, int seed);
 /* Training steps taken since the network was initialised. */
 int lucid_cuda_guide_steps(LucidCudaCtx* ctx);
-/* Adam steps per wave (1..64, each on up to 2^18 records; default 4) and
+/* Adam steps per wave (1..64, each on up to 2^18 records; default 2) and
  * the learning rate (default 1e-2). */
 int lucid_cuda_guide_config(LucidCudaCtx* ctx, int steps_per_wave, float lr);
 
