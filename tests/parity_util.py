@@ -23,6 +23,22 @@ def scene_and_camera(name: str, workdir: str):
         return ls.mirror_point_light_scene()
     if name == "procedural_small":
         return ls.procedural_scene(seed=5, n_spheres=6, levels=2, emissive_levels=1, workdir=workdir, extent=6.0)
+    if name == "empty_env":
+        # no geometry: every camera ray escapes to the environment
+        return ({"meshes": [], "native_lights": [], "environment": {"color": [0.3, 0.4, 0.5], "strength": 1.5}},
+                (0.0, 0.0, 3.0, 0.0, 0.0, -1.0, 0.0, 1.0, 0.0, 45.0))
+    if name == "two_small_quads":
+        # four triangles, none large against the scene: the whole BVH is one leaf
+        m = ls.material((0.7, 0.6, 0.5), 0.0, 0.4)
+        meshes = [ls.mesh(*ls.quad((-3, 0, 0), (-2, 0, 0), (-2, 1, 0), (-3, 1, 0)), m),
+                  ls.mesh(*ls.quad((2, 0, -4), (3, 0, -4), (3, 1, -4), (2, 1, -4)), ls.material((0.9, 0.9, 0.9), 1.0, 0.2))]
+        lights = [{"type": "POINT", "position": [0.0, 2.0, 2.0], "color": [1, 1, 1], "energy": 200.0, "radius": 0.0}]
+        return ({"meshes": meshes, "native_lights": lights, "environment": {"color": [0.05, 0.05, 0.08], "strength": 1.0}},
+                (0.0, 0.5, 6.0, 0.0, 0.0, -1.0, 0.0, 1.0, 0.0, 60.0))
+    if name == "material_preview":
+        return ls.material_preview_scene()
+    if name == "hard_indirect":
+        return ls.hard_indirect_scene()
     raise KeyError(name)
 
 

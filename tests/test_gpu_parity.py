@@ -25,6 +25,12 @@ CASES = [
     ("all_lights", "volume_simple", 32, 24, 2, 8),
     ("mirror", "mis", 32, 32, 4, 6),
     ("procedural_small", "volume_mis", 40, 24, 2, 12),
+    ("cornell", "mis", 37, 23, 3, 8),           # ragged frame: no multiple of the warp or block size
+    ("cornell", "mis", 32, 32, 2, 1),           # camera rays only
+    ("empty_env", "mis", 16, 16, 2, 4),         # no geometry
+    ("two_small_quads", "nee", 32, 24, 2, 6),   # single-leaf BVH
+    ("material_preview", "mis", 32, 32, 2, 8),
+    ("hard_indirect", "mis", 40, 24, 2, 8),
 ]
 
 
