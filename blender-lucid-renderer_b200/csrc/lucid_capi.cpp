@@ -306,6 +306,10 @@ int lucid_cuda_guide_config(LucidCudaCtx* ctx, int steps_per_wave, float lr) {
     return guarded(ctx, [&](lucid::Engine& e) { return e.guide_config(steps_per_wave, lr); });
 }
 
+int lucid_cuda_guide_max_depth(LucidCudaCtx* ctx, int max_depth) {
+    return guarded(ctx, [&](lucid::Engine& e) { return e.guide_max_depth(max_depth); });
+}
+
 int lucid_cuda_guide_steps(LucidCudaCtx* ctx) {
     return guarded(ctx, [&](lucid::Engine& e) { return e.guide_steps(); });
 }

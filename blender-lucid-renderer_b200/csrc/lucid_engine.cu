@@ -108,6 +108,7 @@ struct PathView {
     int* gcount;       // [0] records written, [1] guided vertices
     int gcap;
     unsigned gkeep;    // a guided vertex is recorded when its hash < gkeep
+    int gdepth;        // vertices at path depth < gdepth are guided
     float glo[3], gscale[3];   // scene box -> [0,1]^3
 };
 constexpr int kBins = 16;
@@ -157,6 +158,7 @@ struct GuideState {
     float keep = 1.0f;
     float lr = 1e-2f;
     int steps = 2;   // Adam steps per wave, each on its own batch of records
+    int max_depth = 1;   // vertices at path depth < max_depth are guided (camera hits: depth 0)
     bool on = false;
 };
 
@@ -549,7 +551,7 @@ LD ShadeResult shade_path(const DevScene& sc, const FrameParams& f, const PathVi
             if (GUIDE) guide_credit(pv, id, mul(T, em) * mw, 0);
         }
         bool transmissive = m.transmission > 0.5f;
-        const bool guided = GUIDE && guide_eligible(dm);
+        const bool guided = GUIDE && depth < pv.gdepth && guide_eligible(dm);
         const float* gm = GUIDE ? pv.gmix + (size_t)id * kGMixFloats : nullptr;
         if (nee && sc.num_lights > 0 && !has_em && !transmissive) {
             float usel = randf(rng);
@@ -2398,6 +2400,7 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
         GuideState& G = *guide_;
         gv.gmix = G.gmix.p; gv.gslot = G.gslot.p; gv.ginv = G.ginv.p; gv.grec = G.recs.p; gv.gcount = G.count.p;
         gv.gcap = G.steps * kGuideBatch;
+        gv.gdepth = G.max_depth;
         for (int k = 0; k < 3; ++k) {
             gv.glo[k] = scene_lo_[k];
             float ext = scene_hi_[k] - scene_lo_[k];
@@ -2467,7 +2470,7 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
                 k_trace<<<g_trace, 128, 0, st>>>(ds_->view, pv, cnt, 0, f.records);
             }
             ev_end(e);
-            if (guide) {
+            if (guide && depth < guide_->max_depth) {
                 e = ev_begin(K_GUIDE, depth);
                 k_guide_infer<<<num_sms_, 32 * kInferWarps, kInferSmem, st>>>(
                     ds_->view, pv, cnt, depth == 0, qin, static_cast<const __nv_bfloat16*>(guide_->net.weights_bf16()),
@@ -2622,6 +2625,14 @@ int Engine::guide_config(int steps_per_wave, float lr) {
     if (!guide_) guide_ = new GuideState();
     guide_->steps = steps_per_wave;
     guide_->lr = lr;
+    return LUCID_OK;
+}
+
+int Engine::guide_max_depth(int max_depth) {
+    GpuLock gl(*this);
+    if (max_depth < 1 || max_depth > kMaxDepth) return fail(LUCID_ERR_INVALID, "guide: bad guided depth");
+    if (!guide_) guide_ = new GuideState();
+    guide_->max_depth = max_depth;
     return LUCID_OK;
 }
 

@@ -56,6 +56,7 @@ public:
     int guide_enable(bool on, int seed);
     int guide_steps() const;
     int guide_config(int steps_per_wave, float lr);
+    int guide_max_depth(int max_depth);
     // Uses `owner`'s uploaded scene (BVH, materials, lights) without a copy.
     int share_scene(Engine& owner);
     // Progressive jobs (the request loop's unit of work).

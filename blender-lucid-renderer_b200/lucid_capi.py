@@ -151,6 +151,7 @@ SIGNATURES = {
     "lucid_cuda_guide_enable": (_I, [_P, _I, _I]),
     "lucid_cuda_guide_steps": (_I, [_P]),
     "lucid_cuda_guide_config": (_I, [_P, _I, ctypes.c_float]),
+    "lucid_cuda_guide_max_depth": (_I, [_P, _I]),
     "lucid_cuda_cancel": (_I, [_P]),
     "lucid_cuda_is_cancelled": (_I, [_P]),
     "lucid_cuda_reset_cancel": (_I, [_P]),
@@ -346,6 +347,9 @@ class Context:
 
     def guide_config(self, steps_per_wave: int = 2, lr: float = 1e-2):
         self._check(self.lib.lucid_cuda_guide_config(self.h, steps_per_wave, ctypes.c_float(lr)))
+
+    def guide_max_depth(self, max_depth: int = 1):
+        self._check(self.lib.lucid_cuda_guide_max_depth(self.h, max_depth))
 
     def guide_steps(self) -> int:
         return self._count(self.lib.lucid_cuda_guide_steps(self.h))

@@ -340,8 +340,8 @@ int lucid_guide_train(LucidGuide* guide, const float* records, int n, float lr);
  * not near-delta metal) from the BSDF or from the guide network with
  * probability 1/2 each, weighted by the balance heuristic (NEE's MIS weight
  * uses the same mixed pdf), records the guided vertices with the radiance
- * that arrives along their samples, and takes one Adam step (lr 1e-2, up to
- * 2^18 records) after each wave.  The estimator stays unbiased; its noise
+ * that arrives along their samples, and takes Adam steps (lr 1e-2, up to
+ * 2^18 records each) after each wave.  The estimator stays unbiased; its noise
  * changes.  Enabling (re)initialises the network from `seed`. */
 int lucid_cuda_guide_enable(LucidCudaCtx* ctx, int on, int seed);
 /* Training steps taken since the network was initialised. */
@@ -349,6 +349,11 @@ int lucid_cuda_guide_steps(LucidCudaCtx* ctx);
 /* Adam steps per wave (1..64, each on up to 2^18 records; default 2) and
  * the learning rate (default 1e-2). */
 int lucid_cuda_guide_config(LucidCudaCtx* ctx, int steps_per_wave, float lr);
+/* Guided vertices: those at path depth < max_depth (1..1024; default 1, the
+ * camera-ray hits only, which gave the best error at equal time on the
+ * hard-indirect test room); deeper vertices sample the BSDF as without
+ * guiding but still credit radiance to the guided vertices before them. */
+int lucid_cuda_guide_max_depth(LucidCudaCtx* ctx, int max_depth);
 
 /* ---- cancellation ---------------------------------------------------- */
 /* Replaces PyRenderer::cancel / is_cancelled / reset_cancel

@@ -22,11 +22,13 @@ def _ctx(scene, cam):
     return c
 
 
-def test_guided_render_is_unbiased():
+@pytest.mark.parametrize("guided_depth", [1, 8])
+def test_guided_render_is_unbiased(guided_depth):
     scene, cam = ls.cornell_box()
     ctx = _ctx(scene, cam)
     W = H = 64
     ref = lq.render_reference(ctx, W, H, spp=4096, max_depth=8, sample_offset=1 << 20)
+    ctx.guide_max_depth(guided_depth)
     ctx.guide_enable(True, 5)
     means = []
     for k in range(48):
@@ -49,6 +51,7 @@ def test_trained_guide_lowers_error_at_equal_samples():
     for guided in (False, True):
         if guided:
             ctx.guide_config(4, 1e-2)
+            ctx.guide_max_depth(8)
             ctx.guide_enable(True, 1)
         else:
             ctx.guide_enable(False, 0)
