@@ -156,6 +156,34 @@ def cpu_baseline(js: str, cam, steps: int = 1):
     return vals, threads, sample
 
 
+def scene_upload(device: int, js: str, cache_dir: str) -> dict:
+    """Time to a renderable scene for the benchmark scene in its two forms:
+    JSON text (parse + flatten + upload + BVH) and arrays
+    (lucid_cuda_load_scene_arrays: flatten + upload + BVH), each into a
+    fresh context, each followed by a one-sample 64x64 render."""
+    import lucid_capi
+    import lucid_scenes as ls
+    os.makedirs(cache_dir, exist_ok=True)
+    sc, cam = ls.procedural_scene(seed=SCENE_SEED, workdir=cache_dir)
+    arrays = ls.scene_arrays(sc, json_rounding=False)
+    out = {}
+    for form in ("json", "arrays"):
+        c = lucid_capi.Context(device)
+        t0 = time.perf_counter()
+        if form == "json":
+            c.load_scene_json(js)
+        else:
+            c.load_scene_arrays(arrays)
+        c.set_camera(*cam)
+        c.set_algorithm(ALGO)
+        c.render(64, 64, 64, 64, 1, 0, DEPTH)
+        out[f"{form}_s"] = round(time.perf_counter() - t0, 3)
+        c.close()
+    out["triangles"] = sum(len(m["triangles"]) // 3 for m in arrays["meshes"])
+    out["json_mb"] = round(len(js) / 1e6, 1)
+    return out
+
+
 def c1_quality(device: int) -> dict:
     """Cornell box (256x256, mis, depth 8): a 16-spp render's relMSE against
     an independent FP64-accumulated 4096-spp GPU reference, and the rate."""
@@ -303,6 +331,7 @@ def main():
     ap.add_argument("--cache", default="/tmp/lucid_bench")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-quality", action="store_true", help="skip the Cornell relMSE measurement")
+    ap.add_argument("--no-upload", action="store_true", help="skip the JSON vs array scene-upload timing")
     ap.add_argument("--no-serving", action="store_true", help="skip the request-loop job trace")
     ap.add_argument("--no-guiding", action="store_true", help="skip the guided-vs-plain equal-time comparison")
     ap.add_argument("--guiding-only", action="store_true", help="only the guided-vs-plain comparison")
@@ -412,6 +441,7 @@ def main():
     traffic = None if tpu is None else tpu * top[1]["units"] / max(1, top[1]["launches"])
     mrays = (segs + shadows) / (per_step_ms[-1] / 1000.0) / 1e6
 
+    upload = scene_upload(local_rank, js, args.cache) if rank == 0 and world == 1 and not args.no_upload else None
     quality = c1_quality(local_rank) if rank == 0 and not args.no_quality else None
     serve = serving(local_rank) if rank == 0 and world == 1 and not args.no_serving else None
     guide = (guiding(local_rank, args.guide_budget_ms, args.guide_width, args.guide_height)
@@ -443,7 +473,7 @@ def main():
                         for k, v in kern.items()},
             "mrays_per_s": mrays, "segments_per_step": segs, "shadow_rays_per_step": shadows,
             "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": cpu, "quality": quality,
-            "serving": serve, "guiding": guide,
+            "serving": serve, "guiding": guide, "scene_upload": upload,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -81,6 +81,11 @@ int lucid_cuda_load_scene_json(LucidCudaCtx* ctx, const char* json, size_t len) 
     return guarded(ctx, [&](lucid::Engine& e) { return e.load_scene_json(json, len); });
 }
 
+int lucid_cuda_load_scene_arrays(LucidCudaCtx* ctx, const LucidSceneDesc* scene) {
+    if (!scene) return LUCID_ERR_INVALID;
+    return guarded(ctx, [&](lucid::Engine& e) { return e.load_scene_arrays(*scene); });
+}
+
 int lucid_cuda_set_camera(LucidCudaCtx* ctx, float px, float py, float pz, float dx, float dy, float dz, float ux,
                           float uy, float uz, float fov_deg) {
     return guarded(ctx, [&](lucid::Engine& e) { return e.set_camera(px, py, pz, dx, dy, dz, ux, uy, uz, fov_deg); });
@@ -115,6 +120,20 @@ int lucid_cuda_inspect_scene(const char* json, size_t len, int counts8[8], float
             }
         }
         return (int)hs.lights.size();
+    } catch (...) {
+        return LUCID_ERR_INVALID;
+    }
+}
+
+int lucid_scene_digest(const char* json, size_t len, const LucidSceneDesc* arrays, uint64_t* digest) {
+    if (!digest || (json == nullptr) == (arrays == nullptr)) return LUCID_ERR_INVALID;
+    try {
+        lucid::HostScene hs;
+        std::string err;
+        const bool ok = json ? lucid::parse_scene_json(json, len, hs, err) : lucid::build_scene_arrays(*arrays, hs, err);
+        if (!ok) return LUCID_ERR_INVALID;
+        *digest = lucid::scene_digest(hs);
+        return LUCID_OK;
     } catch (...) {
         return LUCID_ERR_INVALID;
     }

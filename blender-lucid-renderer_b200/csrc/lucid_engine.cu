@@ -1701,6 +1701,27 @@ int Engine::load_scene_json(const char* json, size_t len) {
     std::string err;
     free_scene();
     if (!parse_scene_json(json, len, hs, err)) return fail(LUCID_ERR_INVALID, err);
+    return upload_scene(std::move(hs));
+}
+
+int Engine::load_scene_arrays(const LucidSceneDesc& desc) {
+    GpuLock gl(*this);
+    CK(cudaSetDevice(device_));
+    {
+        int rc = ensure_stream();
+        if (rc != LUCID_OK) return rc;
+    }
+    shared_ = false;
+    HostScene hs;
+    std::string err;
+    free_scene();
+    if (!build_scene_arrays(desc, hs, err)) return fail(LUCID_ERR_INVALID, err);
+    return upload_scene(std::move(hs));
+}
+
+// Uploads a flattened scene and builds its BVH (the caller holds the GPU
+// lock with the device current and the stream created).
+int Engine::upload_scene(HostScene&& hs) {
     host_ = std::move(hs);
     DeviceScene& D = *ds_;
     const HostScene& H = host_;

@@ -27,6 +27,7 @@ public:
     ~Engine();
 
     int load_scene_json(const char* json, size_t len);
+    int load_scene_arrays(const LucidSceneDesc& desc);
     int set_camera(float px, float py, float pz, float dx, float dy, float dz, float ux, float uy, float uz,
                    float fov_deg);
     int set_algorithm(const char* name);
@@ -87,6 +88,7 @@ private:
     int ensure_pool(long long paths, bool records);
     long long default_wave_paths(bool records) const;
     int build_bvh();
+    int upload_scene(HostScene&& hs);
     int ensure_stream();
     int guide_buffers(long long paths);
     void scene_stats_locked(int out8[8]) const;

@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "lucid_types.h"
+#include "../../include/lucid_cuda.h"
 
 namespace lucid {
 
@@ -38,6 +39,10 @@ struct HostScene {
 // Parses the reference's scene JSON (pybind_renderer.hpp:1258-1746).
 // Returns false and sets err on malformed input.
 bool parse_scene_json(const char* json, size_t len, HostScene& out, std::string& err);
+// The same scene from arrays (lucid_cuda_load_scene_arrays).
+bool build_scene_arrays(const LucidSceneDesc& desc, HostScene& out, std::string& err);
+// FNV-1a 64 over every uploaded array and count of a flattened scene.
+uint64_t scene_digest(const HostScene& s);
 
 struct HostCamera {
     float pos[3] = {0, 0, 0};

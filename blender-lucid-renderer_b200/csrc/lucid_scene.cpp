@@ -19,6 +19,10 @@
 #include "lucid_math.h"
 
 namespace lucid {
+static_assert(LUCID_LIGHT_POINT == LIGHT_POINT && LUCID_LIGHT_SUN == LIGHT_SUN && LUCID_LIGHT_SPOT == LIGHT_SPOT &&
+                  LUCID_LIGHT_AREA == LIGHT_AREA, "light type ids");
+static_assert(LUCID_AREA_SQUARE == AREA_SQUARE && LUCID_AREA_RECTANGLE == AREA_RECTANGLE && LUCID_AREA_DISK == AREA_DISK &&
+                  LUCID_AREA_ELLIPSE == AREA_ELLIPSE, "area shape ids");
 namespace {
 
 using json = nlohmann::json;
@@ -73,71 +77,95 @@ struct NativeLight {
     int shape = AREA_SQUARE;
 };
 
-// parseNativeLights (pybind_renderer.hpp:1544-1746), W -> radiance conversions.
-void parse_lights(const json& arr, std::vector<NativeLight>& out) {
+// One native light from its parameters (parseNativeLights,
+// pybind_renderer.hpp:1544-1746, W -> radiance conversions).  type: a
+// LightTypeId (0 for a name the reference does not know); dir, right and up
+// are null when the JSON omits them.
+NativeLight make_light(int type, F3 pos, const F3* dir, float cr, float cg, float cb, float energy, float radius,
+                       float spot_size, float spot_blend, float sx, float sy, int shape, const F3* right,
+                       const F3* up) {
     const double PI = M_PI;
     const float EPS = 1e-6f;
+    NativeLight L;
+    L.pos = pos;
+    if (dir) L.normal = dir_or(*dir, F3{0, 0, -1});
+    if (type == LIGHT_POINT) {
+        L.type = LIGHT_POINT;
+        L.radius = radius;
+        float area = 4.0f * PI * radius * radius;
+        if (area < EPS) area = 1.0f;
+        L.area = area;
+        if (radius > EPS) {
+            L.em[0] = (float)(cr * (energy / (PI * area)));
+            L.em[1] = (float)(cg * (energy / (PI * area)));
+            L.em[2] = (float)(cb * (energy / (PI * area)));
+        } else {
+            float factor = energy / (4.0f * PI);
+            L.em[0] = cr * factor; L.em[1] = cg * factor; L.em[2] = cb * factor;
+        }
+    } else if (type == LIGHT_SUN) {
+        L.type = LIGHT_SUN;
+        L.area = 1.0f;
+        L.em[0] = cr * energy; L.em[1] = cg * energy; L.em[2] = cb * energy;
+    } else if (type == LIGHT_SPOT) {
+        L.type = LIGHT_SPOT;
+        L.radius = radius;
+        L.spot_angle = spot_size;
+        L.spot_blend = spot_blend;
+        L.area = 1.0f;
+        float half = spot_size * 0.5f;
+        float solid = 2.0f * PI * (1.0f - std::cos(half));
+        float factor = energy / solid;
+        L.em[0] = cr * factor; L.em[1] = cg * factor; L.em[2] = cb * factor;
+    } else if (type == LIGHT_AREA) {
+        L.type = LIGHT_AREA;
+        L.sx = sx; L.sy = sy;
+        float area;
+        if (shape == AREA_DISK) { L.shape = AREA_DISK; float r = sx * 0.5f; area = PI * r * r; }
+        else if (shape == AREA_ELLIPSE) { L.shape = AREA_ELLIPSE; float rx = sx * 0.5f, ry = sy * 0.5f; area = PI * rx * ry; }
+        else if (shape == AREA_RECTANGLE) { L.shape = AREA_RECTANGLE; area = sx * sy; }
+        else { L.shape = AREA_SQUARE; area = sx * sy; }
+        L.area = area;
+        if (right) L.right = dir_or(*right, F3{1, 0, 0});
+        if (up) L.up = dir_or(*up, F3{0, 1, 0});
+        float factor = energy / (PI * area);
+        L.em[0] = cr * factor; L.em[1] = cg * factor; L.em[2] = cb * factor;
+    } else {
+        // An unknown type keeps the reference's default-constructed Light
+        // (EMISSIVE_MESH with zero area and emission).
+        L.type = LIGHT_EMISSIVE;
+        L.area = 0.0f;
+    }
+    return L;
+}
+
+// parseNativeLights (pybind_renderer.hpp:1544-1746): JSON keys and defaults.
+void parse_lights(const json& arr, std::vector<NativeLight>& out) {
     for (const auto& lj : arr) {
-        NativeLight L;
         std::string type = lj.value("type", "POINT");
-        if (lj.contains("position")) L.pos = arr3(lj["position"]);
-        if (lj.contains("direction")) L.normal = dir_or(arr3(lj["direction"]), F3{0, 0, -1});
+        int t = type == "POINT" ? LIGHT_POINT : type == "SUN" ? LIGHT_SUN : type == "SPOT" ? LIGHT_SPOT
+              : type == "AREA" ? LIGHT_AREA : LIGHT_EMISSIVE;
+        F3 pos{0, 0, 0}, dir{0, 0, -1}, right{1, 0, 0}, up{0, 1, 0};
+        if (lj.contains("position")) pos = arr3(lj["position"]);
+        const bool has_dir = lj.contains("direction");
+        if (has_dir) dir = arr3(lj["direction"]);
         float cr = 1, cg = 1, cb = 1;
         if (lj.contains("color")) { F3 c = arr3(lj["color"]); cr = c.x; cg = c.y; cb = c.z; }
         float energy = lj.value("energy", 1.0f);
-        if (type == "POINT") {
-            L.type = LIGHT_POINT;
-            float radius = lj.value("radius", 0.0f);
-            L.radius = radius;
-            float area = 4.0f * PI * radius * radius;
-            if (area < EPS) area = 1.0f;
-            L.area = area;
-            if (radius > EPS) {
-                L.em[0] = (float)(cr * (energy / (PI * area)));
-                L.em[1] = (float)(cg * (energy / (PI * area)));
-                L.em[2] = (float)(cb * (energy / (PI * area)));
-            } else {
-                float factor = energy / (4.0f * PI);
-                L.em[0] = cr * factor; L.em[1] = cg * factor; L.em[2] = cb * factor;
-            }
-        } else if (type == "SUN") {
-            L.type = LIGHT_SUN;
-            L.area = 1.0f;
-            L.em[0] = cr * energy; L.em[1] = cg * energy; L.em[2] = cb * energy;
-        } else if (type == "SPOT") {
-            L.type = LIGHT_SPOT;
-            L.radius = lj.value("radius", 0.0f);
-            float sa = lj.value("spot_size", static_cast<float>(M_PI / 4.0f));
-            L.spot_angle = sa;
-            L.spot_blend = lj.value("spot_blend", 0.0f);
-            L.area = 1.0f;
-            float half = sa * 0.5f;
-            float solid = 2.0f * PI * (1.0f - std::cos(half));
-            float factor = energy / solid;
-            L.em[0] = cr * factor; L.em[1] = cg * factor; L.em[2] = cb * factor;
-        } else if (type == "AREA") {
-            L.type = LIGHT_AREA;
-            float sx = lj.value("size", 1.0f);
-            float sy = lj.value("size_y", sx);
-            L.sx = sx; L.sy = sy;
-            float area;
-            std::string shape = lj.value("shape", "SQUARE");
-            if (shape == "DISK") { L.shape = AREA_DISK; float r = sx * 0.5f; area = PI * r * r; }
-            else if (shape == "ELLIPSE") { L.shape = AREA_ELLIPSE; float rx = sx * 0.5f, ry = sy * 0.5f; area = PI * rx * ry; }
-            else if (shape == "RECTANGLE") { L.shape = AREA_RECTANGLE; area = sx * sy; }
-            else { L.shape = AREA_SQUARE; area = sx * sy; }
-            L.area = area;
-            if (lj.contains("right")) L.right = dir_or(arr3(lj["right"]), F3{1, 0, 0});
-            if (lj.contains("up")) L.up = dir_or(arr3(lj["up"]), F3{0, 1, 0});
-            float factor = energy / (PI * area);
-            L.em[0] = cr * factor; L.em[1] = cg * factor; L.em[2] = cb * factor;
-        } else {
-            // An unknown type keeps the reference's default-constructed Light
-            // (EMISSIVE_MESH with zero area and emission).
-            L.type = LIGHT_EMISSIVE;
-            L.area = 0.0f;
-        }
-        out.push_back(L);
+        float radius = lj.value("radius", 0.0f);
+        float spot_size = lj.value("spot_size", static_cast<float>(M_PI / 4.0f));
+        float spot_blend = lj.value("spot_blend", 0.0f);
+        float sx = lj.value("size", 1.0f);
+        float sy = lj.value("size_y", sx);
+        std::string shape = lj.value("shape", "SQUARE");
+        int sh = shape == "DISK" ? AREA_DISK : shape == "ELLIPSE" ? AREA_ELLIPSE
+               : shape == "RECTANGLE" ? AREA_RECTANGLE : AREA_SQUARE;
+        const bool has_right = t == LIGHT_AREA && lj.contains("right");
+        const bool has_up = t == LIGHT_AREA && lj.contains("up");
+        if (has_right) right = arr3(lj["right"]);
+        if (has_up) up = arr3(lj["up"]);
+        out.push_back(make_light(t, pos, has_dir ? &dir : nullptr, cr, cg, cb, energy, radius, spot_size, spot_blend,
+                                 sx, sy, sh, has_right ? &right : nullptr, has_up ? &up : nullptr));
     }
 }
 
@@ -157,6 +185,110 @@ DevLight pack_native(const NativeLight& L) {
     return d;
 }
 
+// Scene assembly shared by the JSON and the array loaders: meshes in order,
+// then the native lights, then SceneLights (emissive triangles first).
+struct Assembly {
+    std::vector<DevLight> emissive_lights;
+    float total = 0.0f;
+    int mesh_index = 0;
+};
+
+// One mesh's material, prims, face/vertex normals and emissive-triangle
+// lights (pybind_renderer.hpp:1346-1503, scene.hpp:214-222,
+// scene_lights.hpp:79-101).  tn: normalised per-triangle vertex normals
+// (used when smooth), or empty.
+void emit_mesh(HostScene& S, Assembly& A, const std::vector<F3>& verts, const std::vector<std::array<int, 3>>& tris,
+               const std::vector<std::array<F3, 3>>& tn, bool has_tn, bool smooth, const float alb[3], float metallic,
+               float roughness, const float em[3], float transmission, float ior, bool boundary, DevVolume vol,
+               bool vol_has_grid, const std::vector<float>& grid) {
+    const int mesh_index = A.mesh_index;
+    for (const auto& t : tris)
+        for (int k = 0; k < 3; ++k)
+            if (t[k] < 0 || t[k] >= (int)verts.size())
+                throw std::runtime_error("mesh " + std::to_string(mesh_index) + ": triangle index out of range");
+    if (vol_has_grid) {
+        vol.grid_offset = (long long)S.grid.size();
+        S.grid.insert(S.grid.end(), grid.begin(), grid.end());
+        S.volumes.push_back(vol);
+    }
+    S.num_boundary_meshes += boundary;
+    bool emissive = (0.2126f * em[0] + 0.7152f * em[1] + 0.0722f * em[2]) > 1e-6f;
+    DevMaterial dm;
+    dm.albedo_metallic = f4(F3{alb[0], alb[1], alb[2]}, metallic);
+    dm.rough_trans_ior_flags.x = roughness;
+    dm.rough_trans_ior_flags.y = transmission;
+    dm.rough_trans_ior_flags.z = ior;
+    dm.rough_trans_ior_flags.w = ibits((emissive ? MAT_EMISSIVE : 0) | (boundary ? MAT_BOUNDARY_ONLY : 0));
+    dm.emission = f4(F3{em[0], em[1], em[2]}, emissive ? 1.0f : 0.0f);
+    S.materials.push_back(dm);
+    for (size_t ti = 0; ti < tris.size(); ++ti) {
+        const auto& t = tris[ti];
+        F3 a = verts[t[0]], b = verts[t[1]], c = verts[t[2]];
+        F3 e1 = sub(b, a), e2 = sub(c, a);
+        F3 fn = dir_or(cross3(e1, e2), F3{0, 1, 0});
+        int prim = S.num_prims++;
+        S.tri.push_back(f4(a, ibits(prim)));
+        S.tri.push_back(f4(e1, 0.0f));
+        S.tri.push_back(f4(e2, 0.0f));
+        S.verts.push_back(f4(a, 0.0f));
+        S.verts.push_back(f4(b, 0.0f));
+        S.verts.push_back(f4(c, 0.0f));
+        bool sm = has_tn && ti < tn.size() && smooth;
+        int light_index = -1;
+        if (emissive) {
+            float area = std::sqrt(len2(cross3(e1, e2))) * 0.5f;
+            if (area > 1e-6f) {
+                DevLight d;
+                std::memset(&d, 0, sizeof(d));
+                d.pos_type = f4(F3{0, 0, 0}, ibits(LIGHT_EMISSIVE));
+                d.normal_area = f4(fn, area);
+                d.emission_radius = f4(F3{em[0], em[1], em[2]}, 0.0f);
+                d.v0_shape = f4(a, ibits(0));
+                d.v1_cosc = f4(b, 0.0f);
+                d.v2_blend = f4(c, 0.0f);
+                light_index = (int)A.emissive_lights.size();
+                A.emissive_lights.push_back(d);
+                A.total += area;
+            }
+        }
+        int4 pi;
+        pi.x = mesh_index; pi.y = (int)ti; pi.z = light_index; pi.w = sm ? 1 : 0;
+        S.prim_info.push_back(pi);
+        S.prim_fn.push_back(f4(fn, 0.0f));
+        for (int k = 0; k < 3; ++k) S.prim_vn.push_back(sm ? f4(tn[ti][k], 0.0f) : f4(fn, 0.0f));
+        S.prim_boundary.push_back(boundary ? 1 : 0);
+    }
+    ++A.mesh_index;
+}
+
+// SceneLights: emissive triangles, then native lights; CDF by cumulative
+// area / total (scene_lights.hpp:103-121) and the CDF search guide.
+void finish_scene(HostScene& S, Assembly& A, const std::vector<NativeLight>& native, const float env[3]) {
+    S.num_meshes = A.mesh_index;
+    for (int k = 0; k < 3; ++k) S.env[k] = env[k];
+    float total = A.total;
+    S.lights = A.emissive_lights;
+    S.native_start = (int)S.lights.size();
+    S.num_native = (int)native.size();
+    for (const auto& L : native) {
+        DevLight d = pack_native(L);
+        S.lights.push_back(d);
+        total += d.normal_area.w;
+    }
+    S.total_light_area = total;
+    S.cdf.resize(S.lights.size());
+    float cum = 0.0f;
+    for (size_t i = 0; i < S.lights.size(); ++i) {
+        cum += S.lights[i].normal_area.w;
+        S.cdf[i] = (total < 1e-6f) ? 0.0f : cum / total;
+    }
+    S.light_guide.resize(kLightGuide + 1);
+    for (int k = 0; k <= kLightGuide; ++k) {
+        float x = (float)k / (float)kLightGuide;   // exact: power-of-two denominator
+        S.light_guide[k] = (int)(std::lower_bound(S.cdf.begin(), S.cdf.end(), x) - S.cdf.begin());
+    }
+}
+
 }  // namespace
 
 bool parse_scene_json(const char* text, size_t length, HostScene& S, std::string& err) {
@@ -169,10 +301,8 @@ bool parse_scene_json(const char* text, size_t length, HostScene& S, std::string
         return false;
     }
     try {
-        std::vector<DevLight> emissive_lights;
-        float total = 0.0f;
+        Assembly A;
         if (j.contains("meshes")) {
-            int mesh_index = 0;
             for (const auto& mj : j["meshes"]) {
                 std::vector<F3> verts;
                 if (mj.contains("vertices"))
@@ -193,10 +323,6 @@ bool parse_scene_json(const char* text, size_t length, HostScene& S, std::string
                 std::vector<std::array<int, 3>> tris;
                 if (mj.contains("triangles"))
                     for (const auto& t : mj["triangles"]) tris.push_back({t[0].get<int>(), t[1].get<int>(), t[2].get<int>()});
-                for (const auto& t : tris)
-                    for (int k = 0; k < 3; ++k)
-                        if (t[k] < 0 || t[k] >= (int)verts.size())
-                            throw std::runtime_error("mesh " + std::to_string(mesh_index) + ": triangle index out of range");
 
                 // material (pybind_renderer.hpp:1346-1503)
                 float alb[3] = {0.8f, 0.8f, 0.8f}, metallic = 0.0f, roughness = 0.5f, em[3] = {0, 0, 0};
@@ -260,104 +386,131 @@ bool parse_scene_json(const char* text, size_t length, HostScene& S, std::string
                     bool present = vol.density > 0.0f || vol_has_grid;
                     if (present && !surf) boundary = true;
                 }
-                if (vol_has_grid) {
-                    vol.grid_offset = (long long)S.grid.size();
-                    S.grid.insert(S.grid.end(), grid.begin(), grid.end());
-                    S.volumes.push_back(vol);
-                }
-                S.num_boundary_meshes += boundary;
-                bool emissive = (0.2126f * em[0] + 0.7152f * em[1] + 0.0722f * em[2]) > 1e-6f;
-                DevMaterial dm;
-                dm.albedo_metallic = f4(F3{alb[0], alb[1], alb[2]}, metallic);
-                dm.rough_trans_ior_flags.x = roughness;
-                dm.rough_trans_ior_flags.y = transmission;
-                dm.rough_trans_ior_flags.z = ior;
-                dm.rough_trans_ior_flags.w = ibits((emissive ? MAT_EMISSIVE : 0) | (boundary ? MAT_BOUNDARY_ONLY : 0));
-                dm.emission = f4(F3{em[0], em[1], em[2]}, emissive ? 1.0f : 0.0f);
-                S.materials.push_back(dm);
-
-                // triangles: face normals (scene.hpp:214-222) and emissive lights
-                for (size_t ti = 0; ti < tris.size(); ++ti) {
-                    const auto& t = tris[ti];
-                    F3 a = verts[t[0]], b = verts[t[1]], c = verts[t[2]];
-                    F3 e1 = sub(b, a), e2 = sub(c, a);
-                    F3 fn = dir_or(cross3(e1, e2), F3{0, 1, 0});
-                    int prim = S.num_prims++;
-                    S.tri.push_back(f4(a, ibits(prim)));
-                    S.tri.push_back(f4(e1, 0.0f));
-                    S.tri.push_back(f4(e2, 0.0f));
-                    S.verts.push_back(f4(a, 0.0f));
-                    S.verts.push_back(f4(b, 0.0f));
-                    S.verts.push_back(f4(c, 0.0f));
-                    bool sm = has_tn && ti < tn.size() && smooth;
-                    int light_index = -1;
-                    if (emissive) {
-                        // SceneLights::buildFromScene emissive triangles (scene_lights.hpp:79-101)
-                        float area = std::sqrt(len2(cross3(e1, e2))) * 0.5f;
-                        if (area > 1e-6f) {
-                            DevLight d;
-                            std::memset(&d, 0, sizeof(d));
-                            d.pos_type = f4(F3{0, 0, 0}, ibits(LIGHT_EMISSIVE));
-                            d.normal_area = f4(fn, area);
-                            d.emission_radius = f4(F3{em[0], em[1], em[2]}, 0.0f);
-                            d.v0_shape = f4(a, ibits(0));
-                            d.v1_cosc = f4(b, 0.0f);
-                            d.v2_blend = f4(c, 0.0f);
-                            light_index = (int)emissive_lights.size();
-                            emissive_lights.push_back(d);
-                            total += area;
-                        }
-                    }
-                    int4 pi;
-                    pi.x = mesh_index; pi.y = (int)ti; pi.z = light_index; pi.w = sm ? 1 : 0;
-                    S.prim_info.push_back(pi);
-                    S.prim_fn.push_back(f4(fn, 0.0f));
-                    for (int k = 0; k < 3; ++k) S.prim_vn.push_back(sm ? f4(tn[ti][k], 0.0f) : f4(fn, 0.0f));
-                    S.prim_boundary.push_back(boundary ? 1 : 0);
-                }
-                ++mesh_index;
+                emit_mesh(S, A, verts, tris, tn, has_tn, smooth, alb, metallic, roughness, em, transmission, ior,
+                          boundary, vol, vol_has_grid, grid);
             }
-            S.num_meshes = mesh_index;
         }
         std::vector<NativeLight> native;
         if (j.contains("native_lights") && j["native_lights"].is_array()) parse_lights(j["native_lights"], native);
         else if (j.contains("lights") && j["lights"].is_array()) parse_lights(j["lights"], native);
+        float env[3] = {0.05f * 1.0f, 0.05f * 1.0f, 0.05f * 1.0f};
         if (j.contains("environment") && j["environment"].is_object()) {
             const auto& e = j["environment"];
             float col[3] = {0.05f, 0.05f, 0.05f}, strength = 1.0f;
             if (e.contains("color") && e["color"].is_array()) { F3 c = arr3(e["color"]); col[0] = c.x; col[1] = c.y; col[2] = c.z; }
             if (e.contains("strength")) strength = e["strength"].get<float>();
-            for (int k = 0; k < 3; ++k) S.env[k] = col[k] * strength;
-        } else {
-            for (int k = 0; k < 3; ++k) S.env[k] = 0.05f * 1.0f;
+            for (int k = 0; k < 3; ++k) env[k] = col[k] * strength;
         }
-        // SceneLights: emissive triangles, then native lights; CDF by
-        // cumulative area / total (scene_lights.hpp:103-121).
-        S.lights = emissive_lights;
-        S.native_start = (int)S.lights.size();
-        S.num_native = (int)native.size();
-        for (const auto& L : native) {
-            DevLight d = pack_native(L);
-            S.lights.push_back(d);
-            total += d.normal_area.w;
-        }
-        S.total_light_area = total;
-        S.cdf.resize(S.lights.size());
-        float cum = 0.0f;
-        for (size_t i = 0; i < S.lights.size(); ++i) {
-            cum += S.lights[i].normal_area.w;
-            S.cdf[i] = (total < 1e-6f) ? 0.0f : cum / total;
-        }
-        S.light_guide.resize(kLightGuide + 1);
-        for (int k = 0; k <= kLightGuide; ++k) {
-            float x = (float)k / (float)kLightGuide;   // exact: power-of-two denominator
-            S.light_guide[k] = (int)(std::lower_bound(S.cdf.begin(), S.cdf.end(), x) - S.cdf.begin());
-        }
+        finish_scene(S, A, native, env);
     } catch (const std::exception& e) {
         err = std::string("malformed scene: ") + e.what();
         return false;
     }
     return true;
+}
+
+bool build_scene_arrays(const LucidSceneDesc& d, HostScene& S, std::string& err) {
+    S = HostScene();
+    try {
+        if (d.num_meshes < 0 || d.num_lights < 0) throw std::runtime_error("negative mesh or light count");
+        if ((d.num_meshes > 0 && !d.meshes) || (d.num_lights > 0 && !d.lights))
+            throw std::runtime_error("null mesh or light array");
+        Assembly A;
+        for (int mi = 0; mi < d.num_meshes; ++mi) {
+            const LucidMeshDesc& m = d.meshes[mi];
+            if (m.num_vertices < 0 || m.num_triangles < 0) throw std::runtime_error("negative vertex or triangle count");
+            if ((m.num_vertices > 0 && !m.vertices) || (m.num_triangles > 0 && !m.triangles))
+                throw std::runtime_error("mesh " + std::to_string(mi) + ": null vertex or triangle array");
+            std::vector<F3> verts((size_t)m.num_vertices);
+            for (int i = 0; i < m.num_vertices; ++i)
+                verts[i] = F3{m.vertices[3 * i], m.vertices[3 * i + 1], m.vertices[3 * i + 2]};
+            std::vector<std::array<int, 3>> tris((size_t)m.num_triangles);
+            for (int i = 0; i < m.num_triangles; ++i)
+                tris[i] = {m.triangles[3 * i], m.triangles[3 * i + 1], m.triangles[3 * i + 2]};
+            std::vector<std::array<F3, 3>> tn;
+            const bool has_tn = m.triangle_normals != nullptr;
+            if (has_tn) {
+                tn.resize((size_t)m.num_triangles);
+                for (int i = 0; i < m.num_triangles; ++i)
+                    for (int k = 0; k < 3; ++k) {
+                        const float* q = m.triangle_normals + 9 * i + 3 * k;
+                        tn[i][k] = dir_or(F3{q[0], q[1], q[2]}, F3{0, 0, 1});
+                    }
+            }
+            DevVolume vol;
+            std::memset(&vol, 0, sizeof(vol));
+            for (int k = 0; k < 3; ++k) {
+                vol.color[k] = m.volume_color[k];
+                vol.absorption[k] = m.volume_absorption[k];
+            }
+            vol.density = m.volume_density;
+            vol.anisotropy = m.volume_anisotropy;
+            bool vol_has_grid = false;
+            std::vector<float> grid;
+            if (m.volume_dims[0] != 0 || m.volume_dims[1] != 0 || m.volume_dims[2] != 0) {
+                for (int k = 0; k < 3; ++k) {
+                    vol.dims[k] = m.volume_dims[k];
+                    vol.wmin[k] = m.volume_world_min[k];
+                    vol.wmax[k] = m.volume_world_max[k];
+                }
+                if (vol.dims[0] < 2 || vol.dims[1] < 2 || vol.dims[2] < 2)
+                    throw std::runtime_error("volume grid dims must be >= 2 per axis");
+                if (m.volume_grid) {
+                    const size_t n = (size_t)vol.dims[0] * vol.dims[1] * vol.dims[2];
+                    grid.assign(m.volume_grid, m.volume_grid + n);
+                    float mx = 0.0f;
+                    for (float g : grid) if (g > mx) mx = g;
+                    vol.grid_max = mx;
+                    vol_has_grid = true;
+                } else {
+                    vol.dims[0] = vol.dims[1] = vol.dims[2] = 0;
+                }
+            }
+            const bool present = vol.density > 0.0f || vol_has_grid;
+            const bool boundary = present && !m.surface;
+            emit_mesh(S, A, verts, tris, tn, has_tn, m.smooth != 0, m.base_color, m.metallic, m.roughness, m.emission,
+                      m.transmission, m.ior, boundary, vol, vol_has_grid, grid);
+        }
+        std::vector<NativeLight> native;
+        for (int li = 0; li < d.num_lights; ++li) {
+            const LucidLightDesc& l = d.lights[li];
+            const int t = (l.type == LUCID_LIGHT_POINT || l.type == LUCID_LIGHT_SUN || l.type == LUCID_LIGHT_SPOT ||
+                           l.type == LUCID_LIGHT_AREA) ? l.type : LIGHT_EMISSIVE;
+            const F3 dir{l.direction[0], l.direction[1], l.direction[2]};
+            const F3 right{l.right[0], l.right[1], l.right[2]}, up{l.up[0], l.up[1], l.up[2]};
+            native.push_back(make_light(t, F3{l.position[0], l.position[1], l.position[2]}, &dir, l.color[0], l.color[1],
+                                        l.color[2], l.energy, l.radius, l.spot_size, l.spot_blend, l.size, l.size_y,
+                                        l.shape, t == LIGHT_AREA ? &right : nullptr, t == LIGHT_AREA ? &up : nullptr));
+        }
+        finish_scene(S, A, native, d.environment);
+    } catch (const std::exception& e) {
+        err = std::string("malformed scene arrays: ") + e.what();
+        return false;
+    }
+    return true;
+}
+
+namespace {
+template <class T>
+uint64_t fnv_bytes(const T* p, size_t n, uint64_t h) {
+    const unsigned char* b = reinterpret_cast<const unsigned char*>(p);
+    for (size_t i = 0; i < n * sizeof(T); ++i) h = (h ^ b[i]) * 1099511628211ull;
+    return h;
+}
+template <class T>
+uint64_t fnv_vec(const std::vector<T>& v, uint64_t h) { return fnv_bytes(v.data(), v.size(), h); }
+}  // namespace
+
+uint64_t scene_digest(const HostScene& S) {
+    uint64_t h = 1469598103934665603ull;
+    const int counts[6] = {S.num_meshes, S.num_prims, S.native_start, S.num_native, S.num_boundary_meshes, 0};
+    h = fnv_bytes(counts, 6, h);
+    h = fnv_bytes(S.env, 3, h);
+    h = fnv_bytes(&S.total_light_area, 1, h);
+    h = fnv_vec(S.tri, h); h = fnv_vec(S.verts, h); h = fnv_vec(S.prim_info, h); h = fnv_vec(S.prim_fn, h);
+    h = fnv_vec(S.prim_vn, h); h = fnv_vec(S.prim_boundary, h); h = fnv_vec(S.materials, h); h = fnv_vec(S.lights, h);
+    h = fnv_vec(S.cdf, h); h = fnv_vec(S.light_guide, h); h = fnv_vec(S.volumes, h); h = fnv_vec(S.grid, h);
+    return h;
 }
 
 void make_camera(HostCamera& c, float px, float py, float pz, float dx, float dy, float dz, float ux, float uy,

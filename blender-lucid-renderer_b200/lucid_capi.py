@@ -32,6 +32,77 @@ class RenderParams(ctypes.Structure):
                 ("flags", ctypes.c_int)]
 
 
+_F3 = ctypes.c_float * 3
+
+
+class MeshDesc(ctypes.Structure):
+    _fields_ = [("vertices", ctypes.c_void_p), ("num_vertices", ctypes.c_int32), ("triangles", ctypes.c_void_p),
+                ("num_triangles", ctypes.c_int32), ("triangle_normals", ctypes.c_void_p), ("smooth", ctypes.c_int32),
+                ("base_color", _F3), ("metallic", ctypes.c_float), ("roughness", ctypes.c_float), ("emission", _F3),
+                ("transmission", ctypes.c_float), ("ior", ctypes.c_float), ("surface", ctypes.c_int32),
+                ("volume_density", ctypes.c_float), ("volume_anisotropy", ctypes.c_float), ("volume_color", _F3),
+                ("volume_absorption", _F3), ("volume_dims", ctypes.c_int32 * 3), ("volume_world_min", _F3),
+                ("volume_world_max", _F3), ("volume_grid", ctypes.c_void_p)]
+
+
+class LightDesc(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int32), ("position", _F3), ("direction", _F3), ("color", _F3),
+                ("energy", ctypes.c_float), ("radius", ctypes.c_float), ("spot_size", ctypes.c_float),
+                ("spot_blend", ctypes.c_float), ("size", ctypes.c_float), ("size_y", ctypes.c_float),
+                ("shape", ctypes.c_int32), ("right", _F3), ("up", _F3)]
+
+
+class SceneDesc(ctypes.Structure):
+    _fields_ = [("meshes", ctypes.c_void_p), ("num_meshes", ctypes.c_int32), ("lights", ctypes.c_void_p),
+                ("num_lights", ctypes.c_int32), ("environment", _F3)]
+
+
+def _scene_desc(arrays: dict):
+    """ctypes descriptors for lucid_scenes.scene_arrays output; returns the
+    descriptor and the objects that must stay alive while it is used."""
+    keep = []
+
+    def ptr(a, dtype):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, dtype=dtype)
+        keep.append(a)
+        return a.ctypes.data
+
+    ms = (MeshDesc * max(1, len(arrays["meshes"])))()
+    for i, m in enumerate(arrays["meshes"]):
+        d = ms[i]
+        d.vertices = ptr(m["vertices"], np.float32)
+        d.num_vertices = len(m["vertices"]) // 3
+        d.triangles = ptr(m["triangles"], np.int32)
+        d.num_triangles = len(m["triangles"]) // 3
+        d.triangle_normals = ptr(m["triangle_normals"], np.float32)
+        d.smooth = int(m["smooth"])
+        d.base_color = _F3(*m["base_color"])
+        d.metallic, d.roughness = float(m["metallic"]), float(m["roughness"])
+        d.emission = _F3(*m["emission"])
+        d.transmission, d.ior = float(m["transmission"]), float(m["ior"])
+        d.surface = int(m["surface"])
+        d.volume_density, d.volume_anisotropy = float(m["volume_density"]), float(m["volume_anisotropy"])
+        d.volume_color, d.volume_absorption = _F3(*m["volume_color"]), _F3(*m["volume_absorption"])
+        d.volume_dims = (ctypes.c_int32 * 3)(*m["volume_dims"])
+        d.volume_world_min, d.volume_world_max = _F3(*m["volume_world_min"]), _F3(*m["volume_world_max"])
+        d.volume_grid = ptr(m["volume_grid"], np.float32)
+    ls_ = (LightDesc * max(1, len(arrays["lights"])))()
+    for i, l in enumerate(arrays["lights"]):
+        d = ls_[i]
+        d.type = int(l["type"])
+        d.position, d.direction, d.color = _F3(*l["position"]), _F3(*l["direction"]), _F3(*l["color"])
+        d.energy, d.radius = float(l["energy"]), float(l["radius"])
+        d.spot_size, d.spot_blend = float(l["spot_size"]), float(l["spot_blend"])
+        d.size, d.size_y, d.shape = float(l["size"]), float(l["size_y"]), int(l["shape"])
+        d.right, d.up = _F3(*l["right"]), _F3(*l["up"])
+    keep += [ms, ls_]
+    sd = SceneDesc(ctypes.addressof(ms), len(arrays["meshes"]), ctypes.addressof(ls_), len(arrays["lights"]),
+                   _F3(*arrays["environment"]))
+    return sd, keep
+
+
 class SampleRecord(ctypes.Structure):
     _fields_ = [("rgb", ctypes.c_float * 3), ("primary_mesh", ctypes.c_int32), ("primary_tri", ctypes.c_int32),
                 ("bounces", ctypes.c_uint32), ("nee_tests", ctypes.c_uint32), ("nee_occluded", ctypes.c_uint32),
@@ -102,6 +173,8 @@ SIGNATURES = {
     "lucid_cuda_last_error": (ctypes.c_char_p, [_P]),
     "lucid_cuda_device_info": (_I, [_P, ctypes.c_char_p, ctypes.c_size_t]),
     "lucid_cuda_load_scene_json": (_I, [_P, ctypes.c_char_p, ctypes.c_size_t]),
+    "lucid_cuda_load_scene_arrays": (_I, [_P, ctypes.c_void_p]),
+    "lucid_scene_digest": (_I, [ctypes.c_char_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p]),
     "lucid_cuda_set_camera": (_I, [_P] + [_F] * 10),
     "lucid_cuda_set_algorithm": (_I, [_P, ctypes.c_char_p]),
     "lucid_cuda_scene_stats": (_I, [_P, ctypes.POINTER(_I)]),
@@ -232,6 +305,12 @@ class Context:
     def load_scene_json(self, text: str) -> None:
         b = text.encode()
         self._check(self.lib.lucid_cuda_load_scene_json(self.h, b, len(b)))
+
+    def load_scene_arrays(self, arrays: dict) -> None:
+        """Upload a scene given as arrays (lucid_scenes.scene_arrays)."""
+        sd, keep = _scene_desc(arrays)
+        self._check(self.lib.lucid_cuda_load_scene_arrays(self.h, ctypes.byref(sd)))
+        del keep
 
     def set_camera(self, *cam) -> None:
         self._check(self.lib.lucid_cuda_set_camera(self.h, *[float(c) for c in cam]))
@@ -391,6 +470,22 @@ class Context:
         m = self._count(self.lib.lucid_cuda_diag_top_groups(self.h, n, int(by_mean), groups.ctypes.data,
                                                             xy.ctypes.data, groups.size))
         return groups[:m], xy[:m]
+
+
+def scene_digest(json_text: str | None = None, arrays: dict | None = None) -> int:
+    """Host-only digest of the scene either form would upload (no GPU)."""
+    lib = load_library()
+    out = ctypes.c_uint64(0)
+    if json_text is not None:
+        b = json_text.encode()
+        rc = lib.lucid_scene_digest(b, len(b), None, ctypes.byref(out))
+    else:
+        sd, keep = _scene_desc(arrays)
+        rc = lib.lucid_scene_digest(None, 0, ctypes.byref(sd), ctypes.byref(out))
+        del keep
+    if rc != LUCID_OK:
+        raise LucidError(rc, "invalid scene")
+    return out.value
 
 
 def admission_plan(budget: int, reserved: int, slots: int, job_bytes) -> list:

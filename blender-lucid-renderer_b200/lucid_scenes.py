@@ -422,3 +422,99 @@ def hard_indirect_scene():
 
 def scene_triangle_count(scene: dict) -> int:
     return int(sum(len(m["triangles"]) for m in scene["meshes"]))
+
+
+# ---------------------------------------------------------------------------
+# Array form of a scene (lucid_cuda_load_scene_arrays)
+# ---------------------------------------------------------------------------
+_JSON_ROUNDING = [True]
+
+
+def _json_f32(a) -> np.ndarray:
+    """float32 values exactly as the JSON loader reads this module's JSON
+    text: 9 significant digits, parsed as a double, then rounded to float
+    (with json_rounding off in scene_arrays: rounded to float directly)."""
+    a = np.asarray(a, dtype=np.float64)
+    if not _JSON_ROUNDING[0]:
+        return a.astype(np.float32)
+    return np.char.mod("%.9g", a).astype(np.float64).astype(np.float32)
+
+
+def _surface_linked(nt) -> bool:
+    """The loader's test for a linked Material Output Surface socket (a
+    node tree with no nodes, or no output node, counts as linked)."""
+    if not isinstance(nt, dict) or "nodes" not in nt or not nt["nodes"]:
+        return True
+    links = {(l["to_node"], l["to_socket"]) for l in nt.get("links", [])}
+    for n in nt["nodes"]:
+        if n.get("type", "") != "ShaderNodeOutputMaterial":
+            continue
+        for i in n.get("inputs", []):
+            if i.get("name", "") == "Surface":
+                return (n.get("name", ""), "Surface") in links
+        return False
+    return True
+
+
+def scene_arrays(scene: dict, json_rounding: bool = True) -> dict:
+    """The scene as plain arrays with every default filled in, read as the
+    JSON loader reads to_json(scene), so that both uploads give the same
+    scene bit for bit.  json_rounding=False rounds values to float32
+    directly (fast; a last-bit difference from the JSON form is possible)."""
+    _JSON_ROUNDING[0] = json_rounding
+    try:
+        return _scene_arrays(scene)
+    finally:
+        _JSON_ROUNDING[0] = True
+
+
+def _scene_arrays(scene: dict) -> dict:
+    meshes = []
+    for m in scene.get("meshes", []):
+        mat = m.get("material", {})
+        vol = mat.get("volume") or {}
+        sg = vol.get("smoke_grid") if isinstance(vol.get("smoke_grid"), dict) else None
+        grid = None
+        dims, wmin, wmax = (0, 0, 0), (0.0, 0.0, 0.0), (0.0, 0.0, 0.0)
+        if sg and all(k in sg for k in ("dims", "world_min", "world_max", "sidecar_path")):
+            dims, wmin, wmax = tuple(int(x) for x in sg["dims"]), sg["world_min"], sg["world_max"]
+            if os.path.exists(sg["sidecar_path"]):
+                grid = np.fromfile(sg["sidecar_path"], dtype=np.float32)[: int(np.prod(dims))].copy()
+        nt = mat.get("node_tree")
+        tn = m.get("triangle_normals")
+        meshes.append({
+            "vertices": _json_f32(np.asarray(m.get("vertices", np.zeros((0, 3)))).reshape(-1, 3)).ravel(),
+            "triangles": np.asarray(m.get("triangles", np.zeros((0, 3))), dtype=np.int32).reshape(-1).copy(),
+            "triangle_normals": None if tn is None else _json_f32(np.asarray(tn).reshape(-1, 9)).ravel(),
+            "smooth": bool(m.get("smooth", False)),
+            "base_color": _json_f32(mat.get("base_color", [0.8, 0.8, 0.8])),
+            "metallic": _json_f32(mat.get("metallic", 0.0)), "roughness": _json_f32(mat.get("roughness", 0.5)),
+            "emission": _json_f32(mat.get("emission", [0.0, 0.0, 0.0])),
+            "transmission": _json_f32(mat.get("transmission", 0.0)), "ior": _json_f32(mat.get("ior", 1.45)),
+            "surface": True if nt is None else _surface_linked(nt),
+            "volume_density": _json_f32(vol.get("density", 0.0)), "volume_anisotropy": _json_f32(vol.get("anisotropy", 0.0)),
+            "volume_color": _json_f32(vol.get("color", [1.0, 1.0, 1.0])),
+            "volume_absorption": _json_f32(vol.get("absorption_color", [0.0, 0.0, 0.0])),
+            "volume_dims": dims, "volume_world_min": _json_f32(wmin), "volume_world_max": _json_f32(wmax),
+            "volume_grid": grid})
+    lights = []
+    types = {"POINT": 1, "SUN": 2, "SPOT": 3, "AREA": 4}
+    shapes = {"SQUARE": 0, "RECTANGLE": 1, "DISK": 2, "ELLIPSE": 3}
+    for l in scene.get("native_lights", scene.get("lights", [])):
+        size = l.get("size", 1.0)
+        lights.append({
+            "type": types.get(l.get("type", "POINT"), 0), "position": _json_f32(l.get("position", [0.0, 0.0, 0.0])),
+            "direction": _json_f32(l.get("direction", [0.0, 0.0, 1.0])), "color": _json_f32(l.get("color", [1.0, 1.0, 1.0])),
+            "energy": _json_f32(l.get("energy", 1.0)), "radius": _json_f32(l.get("radius", 0.0)),
+            "spot_size": _json_f32(l.get("spot_size", np.float32(np.pi / 4.0))),
+            "spot_blend": _json_f32(l.get("spot_blend", 0.0)), "size": _json_f32(size),
+            "size_y": _json_f32(l.get("size_y", size)), "shape": shapes.get(l.get("shape", "SQUARE"), 0),
+            "right": _json_f32(l.get("right", [1.0, 0.0, 0.0])), "up": _json_f32(l.get("up", [0.0, 1.0, 0.0]))})
+    env = scene.get("environment")
+    if isinstance(env, dict):
+        col = _json_f32(env.get("color", [0.05, 0.05, 0.05])) if isinstance(env.get("color"), (list, tuple, np.ndarray)) \
+            else np.full(3, np.float32(0.05))
+        environment = (col * _json_f32(env.get("strength", 1.0))).astype(np.float32)
+    else:
+        environment = np.full(3, np.float32(0.05))
+    return {"meshes": meshes, "lights": lights, "environment": environment}

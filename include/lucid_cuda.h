@@ -97,6 +97,69 @@ int lucid_cuda_device_info(LucidCudaCtx* ctx, char* buf, size_t cap);
  * loadSceneFromJsonString (:1258-1746): parses the JSON scene, builds the
  * light CDF, uploads geometry and builds the device BVH. */
 int lucid_cuda_load_scene_json(LucidCudaCtx* ctx, const char* json, size_t len);
+
+/* Binary scene upload: the same scene as loadSceneFromJsonString
+ * (pybind_renderer.hpp:1258-1746) given as arrays instead of JSON text, so
+ * a host that already holds vertex buffers (Blender's depsgraph export,
+ * engine.py) skips formatting and parsing ~150 MB of JSON per million
+ * triangles.  A scene described the same way in both forms renders
+ * bit-identically.  Each field mirrors the JSON key named beside it; every
+ * field is required (the JSON loader's defaults for absent keys are the
+ * caller's to fill in). */
+typedef struct {
+    const float* vertices;          /* "vertices": 3 * num_vertices floats */
+    int32_t num_vertices;
+    const int32_t* triangles;       /* "triangles": 3 * num_triangles indices */
+    int32_t num_triangles;
+    const float* triangle_normals;  /* "triangle_normals": 9 * num_triangles floats, or NULL */
+    int32_t smooth;                 /* "smooth" */
+    float base_color[3];            /* "material": "base_color", "metallic", ... */
+    float metallic, roughness;
+    float emission[3];
+    float transmission, ior;
+    int32_t surface;                /* 0: the material's Surface output is unlinked (a volume domain) */
+    /* "material"."volume": density > 0 or a grid makes the mesh a medium */
+    float volume_density, volume_anisotropy;
+    float volume_color[3], volume_absorption[3];
+    int32_t volume_dims[3];         /* "smoke_grid": dims (0: no grid), world_min/max, the grid itself */
+    float volume_world_min[3], volume_world_max[3];
+    const float* volume_grid;       /* dims[0] * dims[1] * dims[2] densities, x fastest, or NULL */
+} LucidMeshDesc;
+
+/* One "native_lights" entry (parseNativeLights, pybind_renderer.hpp:1544-1746):
+ * energy in W, converted to radiance as the JSON loader does. */
+#define LUCID_LIGHT_POINT 1
+#define LUCID_LIGHT_SUN 2
+#define LUCID_LIGHT_SPOT 3
+#define LUCID_LIGHT_AREA 4
+#define LUCID_AREA_SQUARE 0
+#define LUCID_AREA_RECTANGLE 1
+#define LUCID_AREA_DISK 2
+#define LUCID_AREA_ELLIPSE 3
+typedef struct {
+    int32_t type;                   /* LUCID_LIGHT_*; any other value: a light with no area or emission */
+    float position[3];
+    float direction[3];             /* normalised, (0, 0, -1) when degenerate */
+    float color[3];
+    float energy;
+    float radius;                   /* point and spot */
+    float spot_size, spot_blend;    /* spot */
+    float size, size_y;             /* area */
+    int32_t shape;                  /* area: LUCID_AREA_* */
+    float right[3], up[3];          /* area */
+} LucidLightDesc;
+
+typedef struct {
+    const LucidMeshDesc* meshes;
+    int32_t num_meshes;
+    const LucidLightDesc* lights;
+    int32_t num_lights;
+    float environment[3];           /* "environment": color * strength */
+} LucidSceneDesc;
+
+/* Loads a scene given as arrays (no counterpart in the reference; the
+ * loadSceneFromJsonString semantics above).  Replaces the current scene. */
+int lucid_cuda_load_scene_arrays(LucidCudaCtx* ctx, const LucidSceneDesc* scene);
 /* Replaces PyRenderer::set_camera (pybind_renderer.hpp:131-160). */
 int lucid_cuda_set_camera(LucidCudaCtx* ctx, float pos_x, float pos_y, float pos_z, float dir_x, float dir_y,
                           float dir_z, float up_x, float up_y, float up_z, float fov_deg);
@@ -116,6 +179,12 @@ int lucid_cuda_scene_stats(LucidCudaCtx* ctx, int out8[8]);
  * negative status. */
 int lucid_cuda_inspect_scene(const char* json, size_t len, int counts8[8], float* cdf, float* area,
                              float* emission_rgb, int cap);
+/* Host-only (no GPU needed, no reference counterpart): a 64-bit FNV-1a digest
+ * of the device-ready scene that lucid_cuda_load_scene_json (json, len) or
+ * lucid_cuda_load_scene_arrays (arrays) would upload: geometry, per-prim
+ * normals, materials, lights and their CDF, volumes.  Give exactly one of
+ * json and arrays.  Equal digests mean identical uploads (and renders). */
+int lucid_scene_digest(const char* json, size_t len, const LucidSceneDesc* arrays, uint64_t* digest);
 
 /* ---- rendering ------------------------------------------------------- */
 /* Replaces PyRenderer::render_tile / render_tile_gpu
