@@ -267,6 +267,11 @@ int lucid_server_add_scene(LucidServer* srv, const char* json, size_t len, int* 
     return server_guarded(srv, [&](lucid::Server& s) { return s.add_scene(json, len, scene_id); });
 }
 
+int lucid_server_add_scene_arrays(LucidServer* srv, const LucidSceneDesc* scene, int* scene_id) {
+    if (!scene || !scene_id) return LUCID_ERR_INVALID;
+    return server_guarded(srv, [&](lucid::Server& s) { return s.add_scene_arrays(*scene, scene_id); });
+}
+
 int lucid_server_submit(LucidServer* srv, const LucidJobDesc* job, int* job_id) {
     if (!job || !job_id) return LUCID_ERR_INVALID;
     return server_guarded(srv, [&](lucid::Server& s) { return s.submit(*job, job_id); });

@@ -64,11 +64,22 @@ Server::~Server() {
 }
 
 int Server::add_scene(const char* json, size_t len, int* scene_id) {
+    return add_scene_with([&](Engine& e) { return e.load_scene_json(json, len); }, scene_id);
+}
+
+int Server::add_scene_arrays(const LucidSceneDesc& desc, int* scene_id) {
+    return add_scene_with([&](Engine& e) { return e.load_scene_arrays(desc); }, scene_id);
+}
+
+// Loads a scene into a new engine with `load` and registers it with the
+// device memory it took.
+template <class Load>
+int Server::add_scene_with(Load&& load, int* scene_id) {
     size_t f0 = 0, f1 = 0, tot = 0;
     cudaSetDevice(device_);
     cudaMemGetInfo(&f0, &tot);
     std::unique_ptr<Engine> e(new Engine(device_));
-    int rc = e->load_scene_json(json, len);
+    int rc = load(*e);
     if (rc != LUCID_OK) return fail(rc, e->last_error());
     cudaMemGetInfo(&f1, &tot);
     std::lock_guard<std::mutex> lk(mu_);

@@ -47,6 +47,7 @@ public:
     Server(int device, int slots, long long budget_bytes);
     ~Server();
     int add_scene(const char* json, size_t len, int* scene_id);
+    int add_scene_arrays(const LucidSceneDesc& desc, int* scene_id);
     int submit(const LucidJobDesc& d, int* job_id);
     int state(int job, int* samples_done);
     int wait(int job, int timeout_ms);
@@ -68,6 +69,8 @@ private:
         std::vector<float> image;
         std::string error;
     };
+    template <class Load>
+    int add_scene_with(Load&& load, int* scene_id);
     void slot_loop(int slot);
     int run_job(int slot, Job& j, int id);
     int pick_chunk(Engine& e, Job& j, int id, int& offset);

@@ -204,6 +204,7 @@ SIGNATURES = {
     "lucid_server_destroy": (None, [_P]),
     "lucid_server_last_error": (ctypes.c_char_p, [_P]),
     "lucid_server_add_scene": (_I, [_P, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(_I)]),
+    "lucid_server_add_scene_arrays": (_I, [_P, ctypes.c_void_p, ctypes.POINTER(_I)]),
     "lucid_server_submit": (_I, [_P, ctypes.POINTER(JobDesc), ctypes.POINTER(_I)]),
     "lucid_server_job_state": (_I, [_P, _I, ctypes.POINTER(_I)]),
     "lucid_server_wait": (_I, [_P, _I, _I]),
@@ -530,6 +531,15 @@ class Server:
         b = json_text.encode()
         sid = ctypes.c_int()
         rc = self.lib.lucid_server_add_scene(self.h, b, len(b), ctypes.byref(sid))
+        if rc != LUCID_OK:
+            self._err(rc)
+        return sid.value
+
+    def add_scene_arrays(self, arrays: dict) -> int:
+        sd, keep = _scene_desc(arrays)
+        sid = ctypes.c_int()
+        rc = self.lib.lucid_server_add_scene_arrays(self.h, ctypes.byref(sd), ctypes.byref(sid))
+        del keep
         if rc != LUCID_OK:
             self._err(rc)
         return sid.value

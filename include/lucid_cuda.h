@@ -357,6 +357,8 @@ void lucid_server_destroy(LucidServer* srv);
 const char* lucid_server_last_error(LucidServer* srv);
 /* Parses, uploads and builds the BVH once; jobs name the scene by its id. */
 int lucid_server_add_scene(LucidServer* srv, const char* json, size_t len, int* scene_id);
+/* The same from arrays (lucid_cuda_load_scene_arrays). */
+int lucid_server_add_scene_arrays(LucidServer* srv, const LucidSceneDesc* scene, int* scene_id);
 /* Queues a job (LUCID_ERR_OOM and state REFUSED when it can never fit). */
 int lucid_server_submit(LucidServer* srv, const LucidJobDesc* job, int* job_id);
 /* Returns the job's LUCID_JOB_* state; samples_done may be NULL. */

@@ -78,7 +78,8 @@ def test_jobs_equal_alone_in_a_mix_and_one_render_call(workdir):
     srv.close()
 
     srv = lucid_capi.Server(0, slots=3)
-    ids = {n: srv.add_scene(ls.to_json(scene_and_camera(n, workdir)[0])) for n in names}
+    # this server takes its scenes as arrays: the jobs must not change
+    ids = {n: srv.add_scene_arrays(ls.scene_arrays(scene_and_camera(n, workdir)[0])) for n in names}
     jids = _submit_all(srv, ids, workdir, JOBS + JOBS)   # every job twice, all at once
     for jid in jids:
         assert srv.wait(jid, 60000) == lucid_capi.JOB_DONE
