@@ -237,6 +237,27 @@ int lucid_cuda_diag_top_groups(LucidCudaCtx* ctx, int n, int by_mean, LucidDiagG
     return guarded(ctx, [&](lucid::Engine& e) { return e.diag_top(n, by_mean != 0, groups, xy, cap); });
 }
 
+int lucid_cuda_diag_coarse_stats(LucidCudaCtx* ctx, LucidDiagCoarse* out) {
+    if (!out) return LUCID_ERR_INVALID;
+    return guarded(ctx, [&](lucid::Engine& e) { return e.diag_coarse(out); });
+}
+
+int lucid_cuda_diag_suggestions(LucidCudaCtx* ctx, LucidDiagSuggestion* out, int cap) {
+    return guarded(ctx, [&](lucid::Engine& e) { return e.diag_suggestions(out, cap); });
+}
+
+long long lucid_cuda_diag_export_binary(LucidCudaCtx* ctx, uint8_t* out, size_t cap) {
+    long long n = LUCID_ERR_INVALID;
+    int rc = guarded(ctx, [&](lucid::Engine& e) { n = e.diag_export_binary(out, cap); return LUCID_OK; });
+    return rc == LUCID_OK ? n : rc;
+}
+
+long long lucid_cuda_diag_metadata_json(LucidCudaCtx* ctx, char* out, size_t cap) {
+    long long n = LUCID_ERR_INVALID;
+    int rc = guarded(ctx, [&](lucid::Engine& e) { n = e.diag_metadata_json(out, cap); return LUCID_OK; });
+    return rc == LUCID_OK ? n : rc;
+}
+
 // ---- request loop ----
 int lucid_server_create(int device, int slots, long long budget_bytes, LucidServer** out) {
     if (!out || slots <= 0 || slots > 64) return LUCID_ERR_INVALID;

@@ -233,3 +233,137 @@ int DiagFilm::export_top(int n, bool by_mean, LucidDiagGroup* groups, int32_t* x
 }
 
 }  // namespace lucid
+
+// ---- DiagnosticExporter (diagnostics/diagnostic_export.hpp:78-220) ----
+namespace lucid {
+
+namespace {
+const char* coarse_name(int t) {   // coarse_type_name (path_stats.hpp:26-40)
+    static const char* names[8] = {"Direct-NoDelta-BSDF",   "Direct-NoDelta-NEE",   "Direct-Delta-BSDF",
+                                   "Direct-Delta-NEE",      "Indirect-NoDelta-BSDF", "Indirect-NoDelta-NEE",
+                                   "Indirect-Delta-BSDF",   "Indirect-Delta-NEE"};
+    return names[t & 7];
+}
+void copy_str(char* dst, size_t cap, const char* src) {
+    std::strncpy(dst, src, cap - 1);
+    dst[cap - 1] = 0;
+}
+}  // namespace
+
+// get_coarse_stats: cells are read at film position (2 sx, 2 sy) for every
+// sampled (sx, sy), as the reference does whatever the subsample factor; a
+// cell's stats are merged with a sample-weighted mean and the largest
+// variance.
+void DiagFilm::coarse_export(LucidDiagCoarse* out) const {
+    struct Agg {
+        uint64_t count = 0;
+        float mean[3] = {0, 0, 0}, var[3] = {0, 0, 0};
+    } agg[8];
+    for (int sy = 0; sy < sh_; ++sy)
+        for (int sx = 0; sx < sw_; ++sx) {
+            const DiagPixel* px = at(sx * 2, sy * 2);
+            if (!px) continue;
+            for (int t = 0; t < 8; ++t) {
+                const DiagStats& cs = px->coarse[t];
+                if (cs.count == 0) continue;
+                agg[t].count += cs.count;
+                const float w = (float)cs.count / (float)agg[t].count;
+                for (int c = 0; c < 3; ++c) {
+                    agg[t].mean[c] = agg[t].mean[c] * (1.0f - w) + cs.mean[c] * w;
+                    agg[t].var[c] = std::max(agg[t].var[c], cs.var[c]);
+                }
+            }
+        }
+    for (int t = 0; t < 8; ++t) {
+        LucidDiagCoarse& o = out[t];
+        std::memset(&o, 0, sizeof(o));
+        o.type_id = t;
+        copy_str(o.name, sizeof(o.name), coarse_name(t));
+        o.sample_count = agg[t].count;
+        o.mean_luminance = 0.2126f * agg[t].mean[0] + 0.7152f * agg[t].mean[1] + 0.0722f * agg[t].mean[2];
+        o.variance_luminance = 0.2126f * 0.2126f * agg[t].var[0] + 0.7152f * 0.7152f * agg[t].var[1] +
+                               0.0722f * 0.0722f * agg[t].var[2];
+        for (int c = 0; c < 3; ++c) { o.mean_rgb[c] = agg[t].mean[c]; o.variance_rgb[c] = agg[t].var[c]; }
+    }
+}
+
+// generate_suggestions: patterns among the ten highest-variance groups, then
+// the share of cells that overflowed their group capacity.
+int DiagFilm::suggestions(LucidDiagSuggestion* out, int cap) const {
+    struct S {
+        const char *cat, *sev, *msg, *act;
+    };
+    std::vector<S> list;
+    std::vector<LucidDiagGroup> top(10);
+    const int n = export_top(10, false, top.data(), nullptr, 10);
+    if (n == 0) return 0;
+    size_t glossy = 0, diffuse = 0, indirect = 0;
+    for (int i = 0; i < n; ++i) {
+        bool has_glossy = false;
+        const bool has_indirect = top[i].depth > 2;
+        for (int v = 0; v < top[i].depth && v < kDiagMaxDepth; ++v)
+            if (top[i].bsdf[v] == 1) has_glossy = true;   // BsdfType::Glossy
+        if (has_glossy) ++glossy;
+        if (has_indirect) ++indirect;
+        if (!has_glossy && !has_indirect) ++diffuse;
+    }
+    if (glossy > 3)
+        list.push_back({"Settings", "warning", "High variance detected in glossy reflections",
+                        "Consider increasing samples or using adaptive sampling for glossy materials"});
+    if (indirect > 3)
+        list.push_back({"Algorithm", "info", "Significant variance from indirect illumination",
+                        "MIS algorithm recommended; consider path guiding for complex scenes"});
+    if (diffuse > 3)
+        list.push_back({"Scene", "info", "High variance in diffuse lighting",
+                        "Check for small or distant light sources; consider area lights"});
+    LucidDiagStats st;
+    stats(&st);
+    if (st.total_samples > 0 && (double)st.total_overflow > (double)st.active_pixels * 0.1)
+        list.push_back({"Settings", "warning", "Many path types exceeded tracking capacity",
+                        "Consider using 'Detailed' preset for more accurate analysis"});
+    for (int i = 0; i < (int)list.size() && i < cap; ++i) {
+        copy_str(out[i].category, sizeof(out[i].category), list[i].cat);
+        copy_str(out[i].severity, sizeof(out[i].severity), list[i].sev);
+        copy_str(out[i].message, sizeof(out[i].message), list[i].msg);
+        copy_str(out[i].action, sizeof(out[i].action), list[i].act);
+    }
+    return (int)list.size();
+}
+
+// export_binary: "PVAR", version 1, film and sampled sizes (uint32), the
+// subsample factor and capacities (one byte each, one zero byte), then per
+// cell in row order: group count (uint16), samples (uint32), mean rgb and
+// total variance (float32), all little-endian and unpadded.
+std::vector<uint8_t> DiagFilm::export_binary() const {
+    std::vector<uint8_t> b;
+    auto put = [&](const void* p, size_t n) {
+        const uint8_t* q = static_cast<const uint8_t*>(p);
+        b.insert(b.end(), q, q + n);
+    };
+    put("PVAR", 4);
+    const uint32_t hdr[5] = {1u, (uint32_t)w_, (uint32_t)h_, (uint32_t)sw_, (uint32_t)sh_};
+    put(hdr, sizeof(hdr));
+    const uint8_t cfg[4] = {(uint8_t)sf_, (uint8_t)max_groups_, (uint8_t)max_outliers_, 0};
+    put(cfg, 4);
+    b.reserve(b.size() + px_.size() * 22);
+    for (const DiagPixel& p : px_) {
+        const uint16_t gc = (uint16_t)p.num_groups;
+        const uint32_t ts = (uint32_t)p.total;
+        const float v = p.total_stats.total_variance();
+        put(&gc, 2);
+        put(&ts, 4);
+        put(p.total_stats.mean, 12);
+        put(&v, 4);
+    }
+    return b;
+}
+
+std::string DiagFilm::metadata_json() const {
+    return "{\n  \"width\": " + std::to_string(w_) + ",\n  \"height\": " + std::to_string(h_) +
+           ",\n  \"sampled_width\": " + std::to_string(sw_) + ",\n  \"sampled_height\": " + std::to_string(sh_) +
+           ",\n  \"subsample_factor\": " + std::to_string(sf_) + ",\n  \"max_groups\": " +
+           std::to_string(max_groups_) + ",\n  \"max_outliers\": " + std::to_string(max_outliers_) +
+           ",\n  \"total_samples\": " + std::to_string(recorded_) + "\n}\n";
+}
+
+}  // namespace lucid

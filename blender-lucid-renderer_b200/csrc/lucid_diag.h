@@ -14,6 +14,7 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include <string>
 #include <vector>
 
 #include "../../include/lucid_cuda.h"
@@ -83,6 +84,12 @@ public:
     int export_pixel(int x, int y, bool sort_by_mean, LucidDiagPixel* info, LucidDiagGroup* groups, int cap);
     int export_top(int n, bool by_mean, LucidDiagGroup* groups, int32_t* xy, int cap) const;
     static void export_group(const DiagGroup& g, LucidDiagGroup* o);
+    // DiagnosticExporter (diagnostic_export.hpp:78-220)
+    void coarse_export(LucidDiagCoarse* out) const;   // 8 entries
+    int suggestions(LucidDiagSuggestion* out, int cap) const;
+    std::vector<uint8_t> export_binary() const;
+    std::string metadata_json() const;
+    void set_limits(int max_groups, int max_outliers) { max_groups_ = max_groups; max_outliers_ = max_outliers; }
     int width() const { return w_; }
     int height() const { return h_; }
     bool valid() const { return valid_; }
@@ -90,7 +97,7 @@ public:
     static uint8_t coarse_type(const DiagRecord& r);
 
 private:
-    int w_ = 0, h_ = 0, sf_ = 2, sw_ = 0, sh_ = 0;
+    int w_ = 0, h_ = 0, sf_ = 2, sw_ = 0, sh_ = 0, max_groups_ = 16, max_outliers_ = 4;
     bool valid_ = false;
     size_t recorded_ = 0;
     std::vector<DiagPixel> px_;

@@ -2199,6 +2199,7 @@ int Engine::render_diag_impl(const LucidRenderParams& p, float* out_host, float*
     if (p.max_depth > kMaxDepth) return fail(LUCID_ERR_INVALID, "max_depth too large");
     if (np > (size_t)0x7fffffff / 2) return fail(LUCID_ERR_INVALID, "tile too large");
     diag_film_.init(p.tile_w, p.tile_h, diag_cfg_.subsample_factor);
+    diag_film_.set_limits(diag_cfg_.max_groups_per_pixel, diag_cfg_.max_outliers_per_pixel);
     cudaStream_t st = S(stream_);
     const long long wave = wave_cap_ > 0 ? std::min(wave_cap_, kDiagWavePaths) : kDiagWavePaths;
     const long long row_paths = (long long)p.tile_w * p.samples;
@@ -2341,6 +2342,38 @@ int Engine::diag_top(int n, bool by_mean, LucidDiagGroup* groups, int32_t* xy, i
     GpuLock gl(*this);
     if (!diag_film_.valid()) return 0;
     return diag_film_.export_top(n, by_mean, groups, xy, groups ? cap : 0);
+}
+
+int Engine::diag_coarse(LucidDiagCoarse* out) {
+    GpuLock gl(*this);
+    if (!diag_film_.valid()) {
+        DiagFilm empty;
+        empty.coarse_export(out);
+        return 8;
+    }
+    diag_film_.coarse_export(out);
+    return 8;
+}
+int Engine::diag_suggestions(LucidDiagSuggestion* out, int cap) {
+    GpuLock gl(*this);
+    if (!diag_film_.valid()) return 0;
+    return diag_film_.suggestions(out, out ? cap : 0);
+}
+long long Engine::diag_export_binary(uint8_t* out, size_t cap) {
+    GpuLock gl(*this);
+    const std::vector<uint8_t> b = diag_film_.export_binary();
+    if (out) std::memcpy(out, b.data(), std::min(cap, b.size()));
+    return (long long)b.size();
+}
+long long Engine::diag_metadata_json(char* out, size_t cap) {
+    GpuLock gl(*this);
+    const std::string m = diag_film_.metadata_json();
+    if (out && cap > 0) {
+        const size_t n = std::min(cap - 1, m.size());
+        std::memcpy(out, m.data(), n);
+        out[n] = 0;
+    }
+    return (long long)m.size();
 }
 
 // Adds one render's film into the async accumulator (float4 sum per pixel).

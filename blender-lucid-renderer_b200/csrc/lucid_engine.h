@@ -52,6 +52,10 @@ public:
     int diag_pixel(int x, int y, bool by_mean, LucidDiagPixel* info, LucidDiagGroup* groups, int cap);
     int diag_variance_map(float* out, size_t cap);
     int diag_top(int n, bool by_mean, LucidDiagGroup* groups, int32_t* xy, int cap);
+    int diag_coarse(LucidDiagCoarse* out);
+    int diag_suggestions(LucidDiagSuggestion* out, int cap);
+    long long diag_export_binary(uint8_t* out, size_t cap);
+    long long diag_metadata_json(char* out, size_t cap);
     int scene_stats(int out8[8]) const;
     // Online-trained path guiding for the `mis` integrator (reseeds the network).
     int guide_enable(bool on, int seed);

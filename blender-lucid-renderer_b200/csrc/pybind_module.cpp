@@ -74,6 +74,18 @@ struct GlobalDiagnosticStats {
     float total_variance = 0.0f;
 };
 
+// ExportedCoarseStats and DiagnosticSuggestion (diagnostic_export.hpp:45-72).
+struct ExportedCoarseStats {
+    uint8_t type_id = 0;
+    std::string name;
+    size_t sample_count = 0;
+    float mean_luminance = 0.0f, variance_luminance = 0.0f;
+    std::array<float, 3> mean_rgb{}, variance_rgb{};
+};
+struct DiagnosticSuggestion {
+    std::string category, severity, message, action;
+};
+
 // bsdf_type_short / bsdf_type_heckbert / light_source_heckbert
 // (diagnostics/path_types.hpp:56-157), coarse_type_name (path_stats.hpp:26-40).
 char bsdf_short(uint8_t t) { return t < 6 ? "DGMTLE"[t] : '?'; }
@@ -276,10 +288,11 @@ public:
         return j;
     }
     // DiagnosticExporter::convert_refs (diagnostic_export.hpp:257-285)
-    std::vector<ExportedGroupInfo> get_top_variance_groups(size_t count) {
+    std::vector<ExportedGroupInfo> get_top_variance_groups(size_t count) { return top_groups(count, false); }
+    std::vector<ExportedGroupInfo> top_groups(size_t count, bool by_mean) {
         std::vector<LucidDiagGroup> g(std::max<size_t>(count, 1));
         std::vector<int32_t> xy(2 * g.size());
-        int n = lucid_cuda_diag_top_groups(ctx_, (int)count, 0, g.data(), xy.data(), (int)g.size());
+        int n = lucid_cuda_diag_top_groups(ctx_, (int)count, by_mean ? 1 : 0, g.data(), xy.data(), (int)g.size());
         std::vector<ExportedGroupInfo> out;
         for (int i = 0; i < n; ++i) {
             ExportedGroupInfo e;
@@ -294,6 +307,42 @@ public:
             out.push_back(std::move(e));
         }
         return out;
+    }
+    // DiagnosticExporter queries (diagnostic_export.hpp:78-220)
+    std::vector<ExportedCoarseStats> coarse_stats() {
+        LucidDiagCoarse c[8];
+        std::vector<ExportedCoarseStats> out;
+        if (lucid_cuda_diag_coarse_stats(ctx_, c) != 8) return out;
+        for (int t = 0; t < 8; ++t) {
+            ExportedCoarseStats e;
+            e.type_id = (uint8_t)c[t].type_id; e.name = c[t].name; e.sample_count = (size_t)c[t].sample_count;
+            e.mean_luminance = c[t].mean_luminance; e.variance_luminance = c[t].variance_luminance;
+            for (int k = 0; k < 3; ++k) { e.mean_rgb[k] = c[t].mean_rgb[k]; e.variance_rgb[k] = c[t].variance_rgb[k]; }
+            out.push_back(std::move(e));
+        }
+        return out;
+    }
+    std::vector<DiagnosticSuggestion> suggestions() {
+        LucidDiagSuggestion sg[8];
+        int n = lucid_cuda_diag_suggestions(ctx_, sg, 8);
+        std::vector<DiagnosticSuggestion> out;
+        for (int i = 0; i < n && i < 8; ++i) out.push_back({sg[i].category, sg[i].severity, sg[i].message, sg[i].action});
+        return out;
+    }
+    py::bytes export_binary() {
+        long long n = lucid_cuda_diag_export_binary(ctx_, nullptr, 0);
+        if (n <= 0) return py::bytes("");
+        std::string b((size_t)n, '\0');
+        lucid_cuda_diag_export_binary(ctx_, reinterpret_cast<uint8_t*>(&b[0]), b.size());
+        return py::bytes(b);
+    }
+    std::string metadata_json() {
+        long long n = lucid_cuda_diag_metadata_json(ctx_, nullptr, 0);
+        if (n <= 0) return std::string();
+        std::string m((size_t)n + 1, '\0');
+        lucid_cuda_diag_metadata_json(ctx_, &m[0], m.size());
+        m.resize((size_t)n);
+        return m;
     }
     // get_pixel_diagnostic (pybind_renderer.hpp:1008-1102)
     PixelDiagnosticInfo get_pixel_diagnostic(size_t x, size_t y, TopGroupSortBy sort_by) {
@@ -380,6 +429,11 @@ std::string adapter_info() {
 }
 
 }  // namespace
+
+struct DiagnosticExporter {
+    explicit DiagnosticExporter(Renderer& renderer) : r(&renderer) {}
+    Renderer* r;
+};
 
 PYBIND11_MODULE(lucidrenderer, m) {
     m.doc() = "Lucid path tracer on NVIDIA B200 (sm_100a CUDA wavefront tracer)";
@@ -537,6 +591,37 @@ PYBIND11_MODULE(lucidrenderer, m) {
         .def_readonly("total_groups", &GlobalDiagnosticStats::total_groups)
         .def_readonly("total_overflow", &GlobalDiagnosticStats::total_overflow)
         .def_readonly("total_variance", &GlobalDiagnosticStats::total_variance);
+    py::class_<ExportedCoarseStats>(m, "ExportedCoarseStats")
+        .def(py::init<>())
+        .def_readonly("type_id", &ExportedCoarseStats::type_id)
+        .def_readonly("name", &ExportedCoarseStats::name)
+        .def_readonly("sample_count", &ExportedCoarseStats::sample_count)
+        .def_readonly("mean_luminance", &ExportedCoarseStats::mean_luminance)
+        .def_readonly("variance_luminance", &ExportedCoarseStats::variance_luminance)
+        .def_readonly("mean_rgb", &ExportedCoarseStats::mean_rgb)
+        .def_readonly("variance_rgb", &ExportedCoarseStats::variance_rgb);
+    py::class_<DiagnosticSuggestion>(m, "DiagnosticSuggestion")
+        .def(py::init<>())
+        .def_readonly("category", &DiagnosticSuggestion::category)
+        .def_readonly("severity", &DiagnosticSuggestion::severity)
+        .def_readonly("message", &DiagnosticSuggestion::message)
+        .def_readonly("action", &DiagnosticSuggestion::action)
+        .def("__repr__", [](const DiagnosticSuggestion& s) {
+            return "<DiagnosticSuggestion [" + s.severity + "] " + s.category + ": " + s.message + ">";
+        });
+    // DiagnosticExporter (diagnostic_export.hpp:78-220): the reference builds
+    // it from a DiagnosticFilm; here from the renderer that holds the film.
+    py::class_<DiagnosticExporter>(m, "DiagnosticExporter")
+        .def(py::init<Renderer&>(), py::arg("renderer"), py::keep_alive<1, 2>())
+        .def("get_global_stats", [](DiagnosticExporter& e) { return e.r->get_diagnostic_stats(); })
+        .def("get_top_variance_groups", [](DiagnosticExporter& e, size_t n) { return e.r->top_groups(n, false); },
+             py::arg("n") = 10)
+        .def("get_top_mean_groups", [](DiagnosticExporter& e, size_t n) { return e.r->top_groups(n, true); },
+             py::arg("n") = 10)
+        .def("get_coarse_stats", [](DiagnosticExporter& e) { return e.r->coarse_stats(); })
+        .def("generate_suggestions", [](DiagnosticExporter& e) { return e.r->suggestions(); })
+        .def("export_metadata_json", [](DiagnosticExporter& e) { return e.r->metadata_json(); })
+        .def("export_binary", [](DiagnosticExporter& e) { return e.r->export_binary(); });
     m.attr("__version__") = "1.0.0";
     m.attr("openmp_enabled") = false;
     m.attr("dawn_enabled") = false;

@@ -103,6 +103,17 @@ def _scene_desc(arrays: dict):
     return sd, keep
 
 
+class DiagCoarse(ctypes.Structure):
+    _fields_ = [("type_id", ctypes.c_int32), ("name", ctypes.c_char * 32), ("sample_count", ctypes.c_uint64),
+                ("mean_luminance", ctypes.c_float), ("variance_luminance", ctypes.c_float),
+                ("mean_rgb", ctypes.c_float * 3), ("variance_rgb", ctypes.c_float * 3)]
+
+
+class DiagSuggestion(ctypes.Structure):
+    _fields_ = [("category", ctypes.c_char * 16), ("severity", ctypes.c_char * 16), ("message", ctypes.c_char * 128),
+                ("action", ctypes.c_char * 128)]
+
+
 class SampleRecord(ctypes.Structure):
     _fields_ = [("rgb", ctypes.c_float * 3), ("primary_mesh", ctypes.c_int32), ("primary_tri", ctypes.c_int32),
                 ("bounces", ctypes.c_uint32), ("nee_tests", ctypes.c_uint32), ("nee_occluded", ctypes.c_uint32),
@@ -175,6 +186,10 @@ SIGNATURES = {
     "lucid_cuda_load_scene_json": (_I, [_P, ctypes.c_char_p, ctypes.c_size_t]),
     "lucid_cuda_load_scene_arrays": (_I, [_P, ctypes.c_void_p]),
     "lucid_scene_digest": (_I, [ctypes.c_char_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p]),
+    "lucid_cuda_diag_coarse_stats": (_I, [_P, ctypes.c_void_p]),
+    "lucid_cuda_diag_suggestions": (_I, [_P, ctypes.c_void_p, _I]),
+    "lucid_cuda_diag_export_binary": (ctypes.c_longlong, [_P, ctypes.c_void_p, ctypes.c_size_t]),
+    "lucid_cuda_diag_metadata_json": (ctypes.c_longlong, [_P, ctypes.c_void_p, ctypes.c_size_t]),
     "lucid_cuda_set_camera": (_I, [_P] + [_F] * 10),
     "lucid_cuda_set_algorithm": (_I, [_P, ctypes.c_char_p]),
     "lucid_cuda_scene_stats": (_I, [_P, ctypes.POINTER(_I)]),
@@ -464,6 +479,30 @@ class Context:
         out = np.zeros(w * h, np.float32)
         n = self._count(self.lib.lucid_cuda_diag_variance_map(self.h, out.ctypes.data, out.size))
         return out[:n]
+
+    def diag_coarse_stats(self) -> list:
+        out = (DiagCoarse * 8)()
+        self._count(self.lib.lucid_cuda_diag_coarse_stats(self.h, ctypes.addressof(out)))
+        return [(c.type_id, c.name.decode(), c.sample_count, c.mean_luminance, c.variance_luminance,
+                 tuple(c.mean_rgb), tuple(c.variance_rgb)) for c in out]
+
+    def diag_suggestions(self) -> list:
+        out = (DiagSuggestion * 8)()
+        n = self._count(self.lib.lucid_cuda_diag_suggestions(self.h, ctypes.addressof(out), 8))
+        return [(s.category.decode(), s.severity.decode(), s.message.decode(), s.action.decode())
+                for s in out[:min(n, 8)]]
+
+    def diag_export_binary(self) -> bytes:
+        n = self._count(self.lib.lucid_cuda_diag_export_binary(self.h, None, 0))
+        buf = ctypes.create_string_buffer(max(n, 1))
+        self.lib.lucid_cuda_diag_export_binary(self.h, buf, n)
+        return buf.raw[:n]
+
+    def diag_metadata_json(self) -> str:
+        n = self._count(self.lib.lucid_cuda_diag_metadata_json(self.h, None, 0))
+        buf = ctypes.create_string_buffer(n + 1)
+        self.lib.lucid_cuda_diag_metadata_json(self.h, buf, n + 1)
+        return buf.value.decode()
 
     def diag_top_groups(self, n, by_mean=False):
         groups = np.zeros(max(n, 1), DIAG_GROUP_DTYPE)

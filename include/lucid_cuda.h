@@ -322,6 +322,37 @@ int lucid_cuda_diag_variance_map(LucidCudaCtx* ctx, float* out, size_t cap);
  * number copied. */
 int lucid_cuda_diag_top_groups(LucidCudaCtx* ctx, int n, int by_mean, LucidDiagGroup* groups, int32_t* xy, int cap);
 
+/* DiagnosticExporter (diagnostics/diagnostic_export.hpp:78-220) over the
+ * current diagnostic film. */
+/* ExportedCoarseStats: one of the eight coarse path types aggregated over the
+ * film the way get_coarse_stats does it (:110-157, sample-weighted means,
+ * largest per-cell variance, cells read at (2 sx, 2 sy) as the reference
+ * reads them). */
+typedef struct LucidDiagCoarse {
+    int32_t type_id;
+    char name[32];
+    uint64_t sample_count;
+    float mean_luminance, variance_luminance;
+    float mean_rgb[3], variance_rgb[3];
+} LucidDiagCoarse;
+/* DiagnosticSuggestion (:62-72, generate_suggestions :178-248). */
+typedef struct LucidDiagSuggestion {
+    char category[16];
+    char severity[16];
+    char message[128];
+    char action[128];
+} LucidDiagSuggestion;
+/* Writes the eight coarse types (out[8]); returns 8. */
+int lucid_cuda_diag_coarse_stats(LucidCudaCtx* ctx, LucidDiagCoarse* out);
+/* Writes up to cap suggestions; returns how many there are. */
+int lucid_cuda_diag_suggestions(LucidCudaCtx* ctx, LucidDiagSuggestion* out, int cap);
+/* export_binary (diagnostic_film.hpp:243-299): the "PVAR" blob.  Copies
+ * min(size, cap) bytes and returns its size (out may be NULL to ask). */
+long long lucid_cuda_diag_export_binary(LucidCudaCtx* ctx, uint8_t* out, size_t cap);
+/* metadata_json (diagnostic_film.hpp:228-241): copies the text (NUL-
+ * terminated when it fits) and returns its length. */
+long long lucid_cuda_diag_metadata_json(LucidCudaCtx* ctx, char* out, size_t cap);
+
 /* ---- request loop (several jobs on one device) ------------------------- */
 /* No reference counterpart: the reference runs one Renderer per Blender
  * session (viewport, F12 render, material preview; render_session.py:77-106),

@@ -662,4 +662,109 @@ void orc_diag_stats(void* h, uint64_t* out5) {
     out5[0] = ts; out5[1] = act; out5[2] = grp; out5[3] = ovf; out5[4] = ds.film.recorded;
 }
 
+// DiagnosticExporter::get_coarse_stats (diagnostic_export.hpp:110-157): for
+// every sampled cell the film is read at (sx * 2, sy * 2) (the exporter's
+// fixed factor), and each coarse type is merged with a count-weighted mean and
+// the largest variance.  Layout shared with LucidDiagCoarse.
+struct OrcDiagCoarse {
+    int32_t type_id;
+    char name[32];
+    uint64_t sample_count;
+    float mean_luminance, variance_luminance;
+    float mean_rgb[3], variance_rgb[3];
+};
+void orc_diag_coarse(void* h, OrcDiagCoarse* out) {
+    static const char* names[8] = {"Direct-NoDelta-BSDF",   "Direct-NoDelta-NEE",   "Direct-Delta-BSDF",
+                                   "Direct-Delta-NEE",      "Indirect-NoDelta-BSDF", "Indirect-NoDelta-NEE",
+                                   "Indirect-Delta-BSDF",   "Indirect-Delta-NEE"};   // path_stats.hpp:26-40
+    DiagState& ds = diag_of(h);
+    const DiagFilm& f = ds.film;
+    size_t count[8] = {};
+    RGB mean[8], var[8];
+    for (size_t sy = 0; sy < f.shh; ++sy)
+        for (size_t sx = 0; sx < f.sw; ++sx) {
+            const PixelData* px = f.at(sx * 2, sy * 2);
+            if (!px) continue;
+            for (int t = 0; t < 8; ++t) {
+                const PStats& cs = px->coarse[t];
+                if (cs.count > 0) {
+                    count[t] += cs.count;
+                    float w = static_cast<float>(cs.count) / static_cast<float>(count[t]);
+                    mean[t].r = mean[t].r * (1.0f - w) + cs.mean.r * w;
+                    mean[t].g = mean[t].g * (1.0f - w) + cs.mean.g * w;
+                    mean[t].b = mean[t].b * (1.0f - w) + cs.mean.b * w;
+                    var[t].r = std::max(var[t].r, cs.variance.r);
+                    var[t].g = std::max(var[t].g, cs.variance.g);
+                    var[t].b = std::max(var[t].b, cs.variance.b);
+                }
+            }
+        }
+    for (int t = 0; t < 8; ++t) {
+        OrcDiagCoarse& o = out[t];
+        std::memset(&o, 0, sizeof(o));
+        o.type_id = t;
+        std::snprintf(o.name, sizeof(o.name), "%s", names[t]);
+        o.sample_count = count[t];
+        o.mean_luminance = 0.2126f * mean[t].r + 0.7152f * mean[t].g + 0.0722f * mean[t].b;   // path_stats.hpp:110-112
+        o.variance_luminance = 0.2126f * 0.2126f * var[t].r + 0.7152f * 0.7152f * var[t].g +
+                               0.0722f * 0.0722f * var[t].b;                                 // path_stats.hpp:117-123
+        o.mean_rgb[0] = mean[t].r; o.mean_rgb[1] = mean[t].g; o.mean_rgb[2] = mean[t].b;
+        o.variance_rgb[0] = var[t].r; o.variance_rgb[1] = var[t].g; o.variance_rgb[2] = var[t].b;
+    }
+}
+
+// DiagnosticExporter::generate_suggestions (diagnostic_export.hpp:178-248):
+// returns how many suggestions there are and, for up to cap of them, the
+// index of each (0 glossy, 1 indirect, 2 diffuse, 3 capacity) in order.
+int orc_diag_suggestions(void* h, int32_t* kinds, int cap) {
+    DiagState& ds = diag_of(h);
+    OrcDiagGroup top[10];
+    int32_t xy[20];
+    int n = orc_diag_top_groups(h, 10, 0, top, xy, 10);
+    if (n == 0) return 0;
+    size_t glossy = 0, indirect = 0, diffuse = 0;
+    for (int i = 0; i < n; ++i) {
+        bool has_glossy = false, has_indirect = top[i].depth > 2;
+        for (int v = 0; v < top[i].depth; ++v)
+            if (top[i].bsdf[v] == B_GLOSSY) has_glossy = true;
+        if (has_glossy) ++glossy;
+        if (has_indirect) ++indirect;
+        if (!has_glossy && !has_indirect) ++diffuse;
+    }
+    std::vector<int32_t> out;
+    if (glossy > 3) out.push_back(0);
+    if (indirect > 3) out.push_back(1);
+    if (diffuse > 3) out.push_back(2);
+    uint64_t st[5];
+    orc_diag_stats(h, st);
+    if (st[0] > 0 && st[3] > st[1] * 0.1) out.push_back(3);
+    for (int i = 0; i < (int)out.size() && i < cap; ++i) kinds[i] = out[i];
+    (void)ds;
+    return (int)out.size();
+}
+
+// DiagnosticFilm::export_binary (diagnostic_film.hpp:243-299); returns the
+// size and copies min(size, cap) bytes.
+long long orc_diag_export_binary(void* h, int max_groups, int max_outliers, uint8_t* out, size_t cap) {
+    DiagState& ds = diag_of(h);
+    const DiagFilm& f = ds.film;
+    std::string b;
+    auto w = [&](const void* p, size_t n) { b.append(static_cast<const char*>(p), n); };
+    w("PVAR", 4);
+    uint32_t version = 1, fw = (uint32_t)f.w, fh = (uint32_t)f.h, sw = (uint32_t)f.sw, sh = (uint32_t)f.shh;
+    w(&version, 4); w(&fw, 4); w(&fh, 4); w(&sw, 4); w(&sh, 4);
+    uint8_t sf = (uint8_t)f.sf, mg = (uint8_t)max_groups, mo = (uint8_t)max_outliers;
+    char padding = 0;
+    w(&sf, 1); w(&mg, 1); w(&mo, 1); w(&padding, 1);
+    for (const PixelData& px : f.px) {
+        uint16_t gc = (uint16_t)px.num_groups;
+        uint32_t ts = (uint32_t)px.total;
+        float mean[3] = {px.total_stats.mean.r, px.total_stats.mean.g, px.total_stats.mean.b};
+        float var = px.total_stats.total_variance();
+        w(&gc, 2); w(&ts, 4); w(mean, 12); w(&var, 4);
+    }
+    if (out) std::memcpy(out, b.data(), std::min(cap, b.size()));
+    return (long long)b.size();
+}
+
 }  // extern "C"

@@ -53,6 +53,8 @@ def load() -> ctypes.CDLL:
             "orc_render_tile_diag": (i, [p, i, i, i, i, i, i, i, i, i, i, p, i]),
             "orc_diag_pixel": (i, [p, i, i, i, p, p, i]), "orc_diag_stats": (None, [p, p]),
             "orc_diag_top_groups": (i, [p, i, i, p, p, i]),
+            "orc_diag_coarse": (None, [p, p]), "orc_diag_suggestions": (i, [p, p, i]),
+            "orc_diag_export_binary": (ctypes.c_longlong, [p, i, i, p, ctypes.c_size_t]),
             "orc_render_tile_f64": (i, [p, i, i, i, i, i, i, i, i, i, p, i]),
         }
         for name, (res, args) in sig.items():
@@ -78,6 +80,12 @@ DIAG_PIXEL_DTYPE = np.dtype([("valid", np.int32), ("sample_count", np.uint32), (
 
 def fptr(a: np.ndarray):
     return a.ctypes.data
+
+
+class OrcCoarse(ctypes.Structure):
+    _fields_ = [("type_id", ctypes.c_int32), ("name", ctypes.c_char * 32), ("sample_count", ctypes.c_uint64),
+                ("mean_luminance", ctypes.c_float), ("variance_luminance", ctypes.c_float),
+                ("mean_rgb", ctypes.c_float * 3), ("variance_rgb", ctypes.c_float * 3)]
 
 
 class Oracle:
@@ -154,6 +162,25 @@ class Oracle:
         xy = np.zeros((max(n, 1), 2), np.int32)
         m = self.lib.orc_diag_top_groups(self.h, n, int(by_mean), fptr(groups), fptr(xy), groups.size)
         return groups[:m], xy[:m]
+
+    def diag_coarse(self):
+        """get_coarse_stats: eight (type_id, name, count, mean_lum, var_lum, mean_rgb, var_rgb)."""
+        out = (OrcCoarse * 8)()
+        self.lib.orc_diag_coarse(self.h, ctypes.addressof(out))
+        return [(c.type_id, c.name.decode(), c.sample_count, c.mean_luminance, c.variance_luminance,
+                 tuple(c.mean_rgb), tuple(c.variance_rgb)) for c in out]
+
+    def diag_suggestion_kinds(self):
+        """generate_suggestions as kinds: 0 glossy, 1 indirect, 2 diffuse, 3 capacity."""
+        out = np.zeros(8, np.int32)
+        n = self.lib.orc_diag_suggestions(self.h, fptr(out), 8)
+        return out[:n].tolist()
+
+    def diag_export_binary(self, max_groups=16, max_outliers=4) -> bytes:
+        n = self.lib.orc_diag_export_binary(self.h, max_groups, max_outliers, None, 0)
+        buf = np.zeros(max(n, 1), np.uint8)
+        self.lib.orc_diag_export_binary(self.h, max_groups, max_outliers, fptr(buf), buf.size)
+        return buf[:n].tobytes()
 
     def diag_stats(self):
         out = np.zeros(5, np.uint64)

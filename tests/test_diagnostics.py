@@ -85,6 +85,39 @@ def test_oracle_diagnostic_render_matches_normal(oracle_lib, workdir, name, algo
     assert st[0] > 0 and st[0] == st[4] and st[1] > 0
 
 
+def test_oracle_exporter_restatement(oracle_lib, workdir):
+    """The oracle's DiagnosticExporter: the binary blob's cells are the
+    film's cells; at subsample 2 the coarse aggregation reads every cell once,
+    so its counts sum to the samples recorded; at subsample 4 it reads only the
+    cells at (2 sx, 2 sy) (the exporter's fixed factor)."""
+    scene, cam = scene_and_camera("all_lights_novol", workdir)
+    for sf in (2, 4):
+        o = oracle_for(scene, cam, "mis")
+        w, h = 16, 12
+        _, rc = o.render_diag(w, h, samples=8, max_depth=6, subsample=sf)
+        assert rc == 0
+        hdr, cells = parse_pvar(o.diag_export_binary())
+        assert hdr == (1, w, h, w // sf, h // sf, sf, 16, 4)
+        k = 0
+        for y in range(0, h // sf * sf, sf):
+            for x in range(0, w // sf * sf, sf):
+                info, _ = o.diag_pixel(x, y)
+                assert cells["gc"][k] == info["group_count"] and cells["ts"][k] == info["sample_count"]
+                np.testing.assert_array_equal(cells["mean"][k], info["mean_rgb"])
+                assert cells["var"][k] == info["variance"]
+                k += 1
+        coarse = o.diag_coarse()
+        assert [c[1] for c in coarse][:2] == ["Direct-NoDelta-BSDF", "Direct-NoDelta-NEE"]
+        want = 0
+        for sy in range(h // sf):
+            for sx in range(w // sf):
+                cx, cy = 2 * sx // sf, 2 * sy // sf          # the cell that film position (2 sx, 2 sy) falls in
+                if cx < w // sf and cy < h // sf:
+                    want += int(o.diag_pixel(cx * sf, cy * sf)[0]["sample_count"])
+        assert sum(c[2] for c in coarse) == want
+        assert set(o.diag_suggestion_kinds()) <= {0, 1, 2, 3}
+
+
 def test_oracle_film_invariants(oracle_lib, workdir):
     scene, cam = scene_and_camera("all_lights_novol", workdir)
     o = oracle_for(scene, cam, "mis")
@@ -136,6 +169,7 @@ def test_python_surface_without_gpu():
     assert (d.subsample_factor, d.max_groups_per_pixel, d.max_outliers_per_pixel) == (1, 32, 8)
     assert d.estimate_memory_bytes(1920, 1080) > s.estimate_memory_bytes(1920, 1080) > c.estimate_memory_bytes(1920, 1080)
     r = lr.Renderer()
+    assert hasattr(lr, "DiagnosticExporter") and hasattr(lr, "ExportedCoarseStats")
     assert not r.is_diagnostics_enabled()
     r.enable_diagnostics(c)
     assert r.is_diagnostics_enabled()
@@ -203,6 +237,43 @@ def _compare_films(ctx, o, w, h, sf):
                                          for y in range(0, h, sf)]), rtol=1e-4, atol=1e-7)
 
 
+def parse_pvar(blob: bytes):
+    """DiagnosticFilm::export_binary layout (diagnostic_film.hpp:243-299):
+    'PVAR', version, width, height, sampled width, sampled height (uint32),
+    subsample, max groups, max outliers, 0 (uint8), then per cell group count
+    (uint16), samples (uint32), mean rgb, total variance (float32)."""
+    import struct
+    assert blob[:4] == b"PVAR"
+    version, w, h, sw, sh = struct.unpack_from("<5I", blob, 4)
+    sf, mg, mo, pad = struct.unpack_from("<4B", blob, 24)
+    cells = np.frombuffer(blob, np.dtype([("gc", "<u2"), ("ts", "<u4"), ("mean", "<f4", 3), ("var", "<f4")]),
+                          offset=28)
+    assert len(blob) == 28 + 22 * sw * sh and pad == 0
+    return (version, w, h, sw, sh, sf, mg, mo), cells
+
+
+def _compare_exports(ctx, o, w, h, sf):
+    hdr, cells = parse_pvar(ctx.diag_export_binary())
+    ohdr, ocells = parse_pvar(o.diag_export_binary())
+    assert hdr == ohdr == (1, w, h, w // sf, h // sf, sf, 16, 4)
+    np.testing.assert_array_equal(cells["gc"], ocells["gc"])
+    np.testing.assert_array_equal(cells["ts"], ocells["ts"])
+    np.testing.assert_allclose(cells["mean"], ocells["mean"], rtol=1e-4, atol=1e-7)
+    np.testing.assert_allclose(cells["var"], ocells["var"], rtol=1e-4, atol=1e-7)
+    for a, b in zip(ctx.diag_coarse_stats(), o.diag_coarse()):
+        assert a[:3] == b[:3]
+        np.testing.assert_allclose(np.array(a[3:5]), np.array(b[3:5]), rtol=1e-4, atol=1e-7)
+        np.testing.assert_allclose(np.array(a[5] + a[6]), np.array(b[5] + b[6]), rtol=1e-4, atol=1e-7)
+    kinds = {"High variance detected in glossy reflections": 0,
+             "Significant variance from indirect illumination": 1,
+             "High variance in diffuse lighting": 2, "Many path types exceeded tracking capacity": 3}
+    assert [kinds[s[2]] for s in ctx.diag_suggestions()] == o.diag_suggestion_kinds()
+    st = ctx.diag_stats()
+    assert ctx.diag_metadata_json() == (
+        f'{{\n  "width": {w},\n  "height": {h},\n  "sampled_width": {w // sf},\n  "sampled_height": {h // sf},\n'
+        f'  "subsample_factor": {sf},\n  "max_groups": 16,\n  "max_outliers": 4,\n  "total_samples": {st[4]}\n}}\n')
+
+
 DIAG_CASES = [("cornell", "mis", 16, 16, 16), ("cornell", "nee", 16, 16, 8), ("cornell", "simple", 16, 16, 8),
               ("mirror", "mis", 16, 12, 8), ("all_lights_novol", "mis", 24, 16, 8),
               ("procedural_small", "nee", 16, 16, 4), ("octahedron", "mis", 16, 16, 8)]
@@ -219,6 +290,7 @@ def test_gpu_diagnostics_match_oracle(gpu_ctx, workdir, name, algo, w, h, spp):
     assert rc == 0
     np.testing.assert_allclose(img, oimg, rtol=1e-4, atol=1e-6)
     _compare_films(gpu_ctx, o, w, h, sf)
+    _compare_exports(gpu_ctx, o, w, h, sf)
     gpu_ctx.diag_disable()
 
 
@@ -238,6 +310,7 @@ def test_gpu_diagnostics_bands_waves_and_regrow(gpu_ctx, workdir):
     assert rc == 0
     np.testing.assert_allclose(img, oimg, rtol=1e-4, atol=1e-6)
     _compare_films(gpu_ctx, o, w, h, sf)
+    _compare_exports(gpu_ctx, o, w, h, sf)
     gpu_ctx.diag_disable()
 
 
@@ -276,6 +349,17 @@ def test_gpu_pyrenderer_diagnostics_workflow():
     groups = r.get_top_variance_groups(5)
     assert 0 < len(groups) <= 5
     assert all(g.sample_count >= 2 for g in groups)
+    ex = lr.DiagnosticExporter(r)                       # diagnostic_export.hpp:78-220
+    assert ex.get_global_stats().total_samples == r.get_diagnostic_stats().total_samples
+    assert [g.signature for g in ex.get_top_variance_groups(5)] == [g.signature for g in groups]
+    means = [g.mean_luminance for g in ex.get_top_mean_groups(5)]
+    assert means == sorted(means, reverse=True)
+    coarse = ex.get_coarse_stats()
+    assert [c.type_id for c in coarse] == list(range(8)) and coarse[0].name == "Direct-NoDelta-BSDF"
+    blob = ex.export_binary()
+    assert blob[:4] == b"PVAR" and len(blob) == 28 + 22 * 8 * 8
+    assert '"subsample_factor": 2' in ex.export_metadata_json()
+    assert all(s.severity in ("info", "warning", "critical") for s in ex.generate_suggestions())
     info = r.get_pixel_diagnostic(8, 8)
     assert info.valid and info.sample_count > 0 and len(info.top_groups) == info.group_count
     r.set_object_names(["Floor", "BackWall", "Sphere"])
