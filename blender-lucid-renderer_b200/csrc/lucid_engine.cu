@@ -67,13 +67,14 @@ struct DeviceScene {
     DBuf<DevNode4> nodes;
     DBuf<DevNode> nodes2;
     DBuf<DevMaterial> materials;
+    DBuf<float4> tex_ops, prim_uv;
     DBuf<DevLight> lights;
     DBuf<float> cdf, grid;
     DBuf<DevVolume> volumes;
     DevScene view{};
     void release() {
         bvh_tris.release(); bnd_tris.release(); big_tris.release(); prim_fn.release(); prim_vn.release(); prim_info.release();
-        nodes.release(); nodes2.release(); guide.release(); materials.release(); lights.release(); cdf.release(); grid.release(); volumes.release();
+        nodes.release(); nodes2.release(); guide.release(); materials.release(); tex_ops.release(); prim_uv.release(); lights.release(); cdf.release(); grid.release(); volumes.release();
     }
 };
 
@@ -384,6 +385,61 @@ LD void guide_credit(const PathView& pv, int id, RGB c, int from) {
     }
 }
 
+// Hit UV (bvh.hpp:67-72): the triangle's UVs at the hit's barycentrics,
+// (0, 0) when it has none.
+LD void hit_uv(const DevScene& sc, int prim, float bu, float bv, float& su, float& sv) {
+    su = 0.0f;
+    sv = 0.0f;
+    if (!sc.prim_uv) return;
+    const float4 a = sc.prim_uv[2 * prim], b = sc.prim_uv[2 * prim + 1];
+    if (b.z == 0.0f) return;
+    const float w = 1.0f - bu - bv;
+    su = a.x * w + a.z * bu + b.x * bv;
+    sv = a.y * w + a.w * bu + b.y * bv;
+}
+
+// A material node program (the loader's folding, lucid_nodes.cpp, in the
+// same float operations) at (u, v).  Out of line: only textured materials
+// run it, and its step array stays out of the shading kernels' frames.
+static __device__ __noinline__ RGB tex_eval(const float4* ops, int start, int n, float u, float v) {
+    float val[kTexMaxOps][3];
+    n = min(n, kTexMaxOps);
+    for (int i = 0; i < n; ++i) {
+        const float4 s0 = ops[2 * (start + i)], s1 = ops[2 * (start + i) + 1];
+        const int kind = __float_as_int(s0.x), a = __float_as_int(s0.y), b = __float_as_int(s0.z);
+        const float k = s0.w;
+        if (kind == TEX_CONST) {
+            val[i][0] = s1.x; val[i][1] = s1.y; val[i][2] = s1.z;
+        } else if (kind == TEX_CHECKER) {   // node_evaluator.cpp:385-396
+            int cu = (int)floorf(u * k) % 2, cv = (int)floorf(v * k) % 2;
+            if (cu < 0) cu += 2;
+            if (cv < 0) cv += 2;
+            const int src = (cu + cv) % 2 == 0 ? a : b;
+            for (int c = 0; c < 3; ++c) val[i][c] = val[src][c];
+        } else if (kind == TEX_MIX) {
+            for (int c = 0; c < 3; ++c) val[i][c] = val[a][c] * (1.0f - k) + val[b][c] * k;
+        } else {
+            for (int c = 0; c < 3; ++c) val[i][c] = val[a][c] * k;
+        }
+    }
+    return n > 0 ? rgb(val[n - 1][0], val[n - 1][1], val[n - 1][2]) : rgb(0.0f, 0.0f, 0.0f);
+}
+
+// Albedo and emission of a textured material at the hit (getMaterialParams
+// / getEmission, integrator/path_tracer.hpp:45-72); the other parameters
+// are constants of the material.
+LD void apply_textures(const DevScene& sc, const DevMaterial& dm, int prim, float bu, float bv, RGB& albedo, RGB& em,
+                       bool& has_em) {
+    if (!(__float_as_int(dm.rough_trans_ior_flags.w) & MAT_TEXTURED)) return;
+    float u, v;
+    hit_uv(sc, prim, bu, bv, u, v);
+    if (dm.program.y > 0) albedo = tex_eval(sc.tex_ops, dm.program.x, dm.program.y, u, v);
+    if (dm.program.w > 0) {
+        em = tex_eval(sc.tex_ops, dm.program.z, dm.program.w, u, v);
+        has_em = (0.2126f * em.r + 0.7152f * em.g + 0.0722f * em.b) > 1e-6f;
+    }
+}
+
 // A surface the guide may sample: no transmission lobe and not the
 // near-delta metal that sample_bsdf weights in closed form.
 LD bool guide_eligible(const DevMaterial& dm) {
@@ -529,6 +585,7 @@ LD ShadeResult shade_path(const DevScene& sc, const FrameParams& f, const PathVi
         m.ior = dm.rough_trans_ior_flags.z;
         RGB em = c3(dm.emission);
         bool has_em = dm.emission.w != 0.0f;
+        apply_textures(sc, dm, prim, hh.y, hh.z, m.albedo, em, has_em);
         V3 wo = -d;
         bool front = dot(wo, n) > 0;
         V3 sn = n;
@@ -1146,7 +1203,8 @@ __global__ void __launch_bounds__(128) k_diag_paths(DevScene sc, FrameParams f, 
         m.transmission = dm.rough_trans_ior_flags.y;
         m.ior = dm.rough_trans_ior_flags.z;
         RGB em = c3(dm.emission);
-        const bool has_em = dm.emission.w != 0.0f;
+        bool has_em = dm.emission.w != 0.0f;
+        apply_textures(sc, dm, h.prim, h.u, h.v, m.albedo, em, has_em);
         // classify_bsdf / is_delta_bsdf (diagnostic_integrator.hpp:25-60)
         uint8_t bt = m.transmission > 0.5f                       ? DB_GLASS
                      : (m.roughness < 0.01f && m.metallic > 0.5f) ? DB_MIRROR
@@ -1275,9 +1333,12 @@ __global__ void k_debug(DevScene sc, FrameParams f, int mode, float4* out, int* 
             n = make_dir_or(ni, fn);
         }
         const DevMaterial& dm = sc.materials[pi.x];
+        RGB alb = c3(dm.albedo_metallic), em = c3(dm.emission);
+        bool has_em = false;
+        apply_textures(sc, dm, h.prim, h.u, h.v, alb, em, has_em);
         if (mode == 0) c = make_float4(n.x * 0.5f + 0.5f, n.y * 0.5f + 0.5f, n.z * 0.5f + 0.5f, 1.0f);
-        else if (mode == 1) c = make_float4(dm.albedo_metallic.x, dm.albedo_metallic.y, dm.albedo_metallic.z, 1.0f);
-        else c = make_float4(dm.emission.x * 1.0f, dm.emission.y * 1.0f, dm.emission.z * 1.0f, 1.0f);
+        else if (mode == 1) c = make_float4(alb.r, alb.g, alb.b, 1.0f);
+        else c = make_float4(em.r * 1.0f, em.g * 1.0f, em.b * 1.0f, 1.0f);
     }
     out[(size_t)(f.tile_h - 1 - py) * f.tile_w + px] = c;
 }
@@ -1741,6 +1802,8 @@ int Engine::upload_scene(HostScene&& hs) {
     CK(up(D.prim_fn, H.prim_fn));
     CK(up(D.prim_vn, H.prim_vn));
     CK(up(D.materials, H.materials));
+    CK(up(D.tex_ops, H.tex_ops));
+    CK(up(D.prim_uv, H.prim_uv));
     CK(up(D.lights, H.lights));
     CK(up(D.cdf, H.cdf));
     CK(up(D.guide, H.light_guide));
@@ -1754,6 +1817,8 @@ int Engine::upload_scene(HostScene&& hs) {
     v.prim_fn = D.prim_fn.p;
     v.prim_vn = D.prim_vn.p;
     v.materials = D.materials.p;
+    v.tex_ops = H.tex_ops.empty() ? nullptr : D.tex_ops.p;
+    v.prim_uv = H.prim_uv.empty() ? nullptr : D.prim_uv.p;
     v.lights = D.lights.p;
     v.light_cdf = D.cdf.p;
     v.light_guide = D.guide.p;

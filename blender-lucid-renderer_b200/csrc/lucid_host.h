@@ -24,6 +24,8 @@ struct HostScene {
     std::vector<float4> prim_vn;    // 3 per prim: vertex normals
     std::vector<unsigned char> prim_boundary;
     std::vector<DevMaterial> materials;
+    std::vector<float4> tex_ops;    // node program steps of textured materials
+    std::vector<float4> prim_uv;    // 2 per prim when any mesh has UVs, else empty
     std::vector<DevLight> lights;
     std::vector<float> cdf;
     std::vector<int> light_guide;   // kLightGuide + 1 entries

@@ -17,6 +17,7 @@
 
 #include "lucid_host.h"
 #include "lucid_math.h"
+#include "lucid_nodes.h"
 
 namespace lucid {
 static_assert(LUCID_LIGHT_POINT == LIGHT_POINT && LUCID_LIGHT_SUN == LIGHT_SUN && LUCID_LIGHT_SPOT == LIGHT_SPOT &&
@@ -198,10 +199,19 @@ struct Assembly {
 // scene_lights.hpp:79-101).  tn: normalised per-triangle vertex normals
 // (used when smooth), or empty.
 void emit_mesh(HostScene& S, Assembly& A, const std::vector<F3>& verts, const std::vector<std::array<int, 3>>& tris,
-               const std::vector<std::array<F3, 3>>& tn, bool has_tn, bool smooth, const float alb[3], float metallic,
-               float roughness, const float em[3], float transmission, float ior, bool boundary, DevVolume vol,
-               bool vol_has_grid, const std::vector<float>& grid) {
+               const std::vector<std::array<F3, 3>>& tn, bool has_tn, bool smooth, const float alb_in[3],
+               float metallic, float roughness, const float em_in[3], float transmission, float ior, bool boundary,
+               DevVolume vol, bool vol_has_grid, const std::vector<float>& grid,
+               const std::vector<std::array<float, 6>>& uvs = {}, const NodeMaterial* nm = nullptr) {
     const int mesh_index = A.mesh_index;
+    // use_nodes: every parameter comes from the node graph
+    // (getMaterialParams / getEmission, integrator/path_tracer.hpp:45-72)
+    float alb[3] = {alb_in[0], alb_in[1], alb_in[2]}, em[3] = {em_in[0], em_in[1], em_in[2]};
+    if (nm) {
+        for (int c = 0; c < 3; ++c) { alb[c] = nm->albedo[c]; em[c] = nm->emission[c]; }
+        metallic = nm->metallic; roughness = nm->roughness; transmission = nm->transmission; ior = nm->ior;
+    }
+    const bool textured = nm && (nm->albedo_n > 0 || nm->emission_n > 0);
     for (const auto& t : tris)
         for (int k = 0; k < 3; ++k)
             if (t[k] < 0 || t[k] >= (int)verts.size())
@@ -218,8 +228,13 @@ void emit_mesh(HostScene& S, Assembly& A, const std::vector<F3>& verts, const st
     dm.rough_trans_ior_flags.x = roughness;
     dm.rough_trans_ior_flags.y = transmission;
     dm.rough_trans_ior_flags.z = ior;
-    dm.rough_trans_ior_flags.w = ibits((emissive ? MAT_EMISSIVE : 0) | (boundary ? MAT_BOUNDARY_ONLY : 0));
+    dm.rough_trans_ior_flags.w =
+        ibits((emissive ? MAT_EMISSIVE : 0) | (boundary ? MAT_BOUNDARY_ONLY : 0) | (textured ? MAT_TEXTURED : 0));
     dm.emission = f4(F3{em[0], em[1], em[2]}, emissive ? 1.0f : 0.0f);
+    dm.program.x = nm ? nm->albedo_start : 0;
+    dm.program.y = nm ? nm->albedo_n : 0;
+    dm.program.z = nm ? nm->emission_start : 0;
+    dm.program.w = nm ? nm->emission_n : 0;
     S.materials.push_back(dm);
     for (size_t ti = 0; ti < tris.size(); ++ti) {
         const auto& t = tris[ti];
@@ -257,6 +272,14 @@ void emit_mesh(HostScene& S, Assembly& A, const std::vector<F3>& verts, const st
         S.prim_fn.push_back(f4(fn, 0.0f));
         for (int k = 0; k < 3; ++k) S.prim_vn.push_back(sm ? f4(tn[ti][k], 0.0f) : f4(fn, 0.0f));
         S.prim_boundary.push_back(boundary ? 1 : 0);
+        // UVs (pybind_renderer.hpp:1296-1336); dropped in finish_scene when no prim has any
+        float4 u0 = {0, 0, 0, 0}, u1 = {0, 0, 0, 0};
+        if (ti < uvs.size()) {
+            const auto& q = uvs[ti];
+            u0.x = q[0]; u0.y = q[1]; u0.z = q[2]; u0.w = q[3]; u1.x = q[4]; u1.y = q[5]; u1.z = 1.0f;
+        }
+        S.prim_uv.push_back(u0);
+        S.prim_uv.push_back(u1);
     }
     ++A.mesh_index;
 }
@@ -265,6 +288,9 @@ void emit_mesh(HostScene& S, Assembly& A, const std::vector<F3>& verts, const st
 // area / total (scene_lights.hpp:103-121) and the CDF search guide.
 void finish_scene(HostScene& S, Assembly& A, const std::vector<NativeLight>& native, const float env[3]) {
     S.num_meshes = A.mesh_index;
+    bool any_uv = false;
+    for (size_t i = 1; i < S.prim_uv.size() && !any_uv; i += 2) any_uv = S.prim_uv[i].z != 0.0f;
+    if (!any_uv) std::vector<float4>().swap(S.prim_uv);
     for (int k = 0; k < 3; ++k) S.env[k] = env[k];
     float total = A.total;
     S.lights = A.emissive_lights;
@@ -323,6 +349,13 @@ bool parse_scene_json(const char* text, size_t length, HostScene& S, std::string
                 std::vector<std::array<int, 3>> tris;
                 if (mj.contains("triangles"))
                     for (const auto& t : mj["triangles"]) tris.push_back({t[0].get<int>(), t[1].get<int>(), t[2].get<int>()});
+                std::vector<std::array<float, 6>> uvs;
+                if (mj.contains("triangle_uvs"))
+                    for (const auto& t : mj["triangle_uvs"])
+                        uvs.push_back({t[0][0].get<float>(), t[0][1].get<float>(), t[1][0].get<float>(),
+                                       t[1][1].get<float>(), t[2][0].get<float>(), t[2][1].get<float>()});
+                bool use_nodes = false;
+                NodeMaterial nm;
 
                 // material (pybind_renderer.hpp:1346-1503)
                 float alb[3] = {0.8f, 0.8f, 0.8f}, metallic = 0.0f, roughness = 0.5f, em[3] = {0, 0, 0};
@@ -345,6 +378,8 @@ bool parse_scene_json(const char* text, size_t length, HostScene& S, std::string
                     if (mat.contains("node_tree") && !mat["node_tree"].is_null()) {
                         surf = surface_linked(mat["node_tree"], nt_valid);
                         if (!nt_valid) surf = true;
+                        use_nodes = nt_valid && mat.value("use_nodes", false);
+                        if (use_nodes) nm = compile_node_material(mat["node_tree"], S.tex_ops);
                     }
                     if (mat.contains("volume") && !mat["volume"].is_null()) {
                         const auto& v = mat["volume"];
@@ -387,7 +422,7 @@ bool parse_scene_json(const char* text, size_t length, HostScene& S, std::string
                     if (present && !surf) boundary = true;
                 }
                 emit_mesh(S, A, verts, tris, tn, has_tn, smooth, alb, metallic, roughness, em, transmission, ior,
-                          boundary, vol, vol_has_grid, grid);
+                          boundary, vol, vol_has_grid, grid, uvs, use_nodes ? &nm : nullptr);
             }
         }
         std::vector<NativeLight> native;
@@ -510,6 +545,7 @@ uint64_t scene_digest(const HostScene& S) {
     h = fnv_vec(S.tri, h); h = fnv_vec(S.verts, h); h = fnv_vec(S.prim_info, h); h = fnv_vec(S.prim_fn, h);
     h = fnv_vec(S.prim_vn, h); h = fnv_vec(S.prim_boundary, h); h = fnv_vec(S.materials, h); h = fnv_vec(S.lights, h);
     h = fnv_vec(S.cdf, h); h = fnv_vec(S.light_guide, h); h = fnv_vec(S.volumes, h); h = fnv_vec(S.grid, h);
+    h = fnv_vec(S.tex_ops, h); h = fnv_vec(S.prim_uv, h);
     return h;
 }
 

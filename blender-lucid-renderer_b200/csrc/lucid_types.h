@@ -34,8 +34,13 @@ struct alignas(16) DevMaterial {
     float4 albedo_metallic;        // albedo rgb, metallic
     float4 rough_trans_ior_flags;  // roughness, transmission, ior, flags (int bits)
     float4 emission;               // emission rgb, emissive flag
+    int4 program;                  // node programs: albedo start, steps, emission start, steps (0: constant)
 };
-enum MaterialFlags { MAT_EMISSIVE = 1, MAT_BOUNDARY_ONLY = 2 };
+enum MaterialFlags { MAT_EMISSIVE = 1, MAT_BOUNDARY_ONLY = 2, MAT_TEXTURED = 4 };
+// Steps of a material node program (two float4 each: {kind, operand a,
+// operand b, k}, {rgb, 0}; operands index earlier steps of the program).
+enum TexOpKind { TEX_CONST = 0, TEX_CHECKER = 1, TEX_MIX = 2, TEX_SCALE = 3 };
+constexpr int kTexMaxOps = 24;   // steps in one material program
 
 // A participating medium with a dense grid (material.hpp:149-188).
 struct DevVolume {
@@ -88,6 +93,8 @@ struct DevScene {
     const float4* prim_fn;          // face normal
     const float4* prim_vn;          // 3 vertex normals per prim (smooth prims)
     const DevMaterial* materials;   // per mesh
+    const float4* tex_ops;          // node program steps (two float4 each)
+    const float4* prim_uv;          // 2 per prim: (uv0, uv1), (uv2, has uv, 0); null without UVs
     // lights
     const DevLight* lights;
     const float* light_cdf;

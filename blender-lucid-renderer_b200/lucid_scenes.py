@@ -518,3 +518,97 @@ def _scene_arrays(scene: dict) -> dict:
     else:
         environment = np.full(3, np.float32(0.05))
     return {"meshes": meshes, "lights": lights, "environment": environment}
+
+
+# ---------------------------------------------------------------------------
+# Node-graph materials (use_nodes) with UV checker textures
+# ---------------------------------------------------------------------------
+def _sock(name, value=None):
+    s = {"name": name, "type": "RGBA" if isinstance(value, (list, tuple)) else "VALUE"}
+    if value is not None:
+        s["default_value"] = list(value) if isinstance(value, (list, tuple)) else float(value)
+    return s
+
+
+def _tree(nodes, links):
+    return {"nodes": nodes, "links": [{"from_node": a, "from_socket": b, "to_node": c, "to_socket": d}
+                                      for a, b, c, d in links]}
+
+
+def _out(surface_from, socket="BSDF"):
+    return ({"name": "Material Output", "type": "ShaderNodeOutputMaterial",
+             "inputs": [_sock("Surface"), _sock("Volume")]}, (surface_from, socket, "Material Output", "Surface"))
+
+
+def textured_scene():
+    """Quads whose materials come from node graphs: a checker floor (Base
+    Color <- Checker, UVs 0..4), a Mix of a checker and an RGB node on the back
+    wall (a Diffuse BSDF), an emissive checker panel (Emission <- Checker), a
+    Principled panel whose scalars come from the graph, and a box with a node
+    tree but use_nodes off; lit by a point light and the panel."""
+    meshes = []
+    uv = np.array([[[0, 0], [4, 0], [4, 4]], [[0, 0], [4, 4], [0, 4]]], dtype=np.float64)
+    # floor: Principled, Base Color <- Checker (Color1/Color2 constants, scale 2)
+    out, link = _out("Principled BSDF")
+    floor_mat = material((0.1, 0.1, 0.1))
+    floor_mat["use_nodes"] = True
+    floor_mat["node_tree"] = _tree([
+        out,
+        {"name": "Principled BSDF", "type": "ShaderNodeBsdfPrincipled",
+         "inputs": [_sock("Base Color", (0.5, 0.5, 0.5, 1.0)), _sock("Metallic", 0.0), _sock("Roughness", 0.7),
+                    _sock("IOR", 1.5), _sock("Transmission Weight", 0.0), _sock("Emission Color", (0, 0, 0, 1)),
+                    _sock("Emission Strength", 0.0)]},
+        {"name": "Checker Texture", "type": "ShaderNodeTexChecker",
+         "inputs": [_sock("Color1", (0.9, 0.8, 0.7, 1.0)), _sock("Color2", (0.1, 0.2, 0.3, 1.0)), _sock("Scale", 2.0)]}],
+        [link, ("Checker Texture", "Color", "Principled BSDF", "Base Color")])
+    m = mesh(*quad((-2, 0, -2), (2, 0, -2), (2, 0, 2), (-2, 0, 2)), floor_mat)
+    m["triangle_uvs"] = uv
+    meshes.append(m)
+    # back wall: Diffuse BSDF, Color <- Mix(Checker, RGB, fac 0.3)
+    out, link = _out("Diffuse BSDF")
+    wall_mat = material((0.5, 0.5, 0.5), 0.3, 0.2)
+    wall_mat["use_nodes"] = True
+    wall_mat["node_tree"] = _tree([
+        out,
+        {"name": "Diffuse BSDF", "type": "ShaderNodeBsdfDiffuse", "inputs": [_sock("Color", (0.8, 0.8, 0.8, 1.0))]},
+        {"name": "Mix", "type": "ShaderNodeMix", "inputs": [_sock("Fac", 0.3), _sock("A"), _sock("B")]},
+        {"name": "Checker Texture", "type": "ShaderNodeTexChecker", "inputs": [_sock("Scale", 3.0)]},
+        {"name": "RGB", "type": "ShaderNodeRGB", "inputs": [], "outputs": [{"name": "Color", "default_value": [0.2, 0.6, 0.3, 1.0]}]}],
+        [link, ("Mix", "Result", "Diffuse BSDF", "Color"), ("Checker Texture", "Color", "Mix", "A"),
+         ("RGB", "Color", "Mix", "B")])
+    m = mesh(*quad((-2, 0, -2), (-2, 2.5, -2), (2, 2.5, -2), (2, 0, -2)), wall_mat)
+    m["triangle_uvs"] = uv * 0.5
+    meshes.append(m)
+    # emissive panel: Emission shader, Color <- Checker, strength 4
+    out, link = _out("Emission", "Emission")
+    panel = material((0.0, 0.0, 0.0))
+    panel["use_nodes"] = True
+    panel["node_tree"] = _tree([
+        out,
+        {"name": "Emission", "type": "ShaderNodeEmission", "inputs": [_sock("Color"), _sock("Strength", 4.0)]},
+        {"name": "Checker Texture", "type": "ShaderNodeTexChecker",
+         "inputs": [_sock("Color1", (1.0, 0.9, 0.7, 1.0)), _sock("Color2", (0.0, 0.0, 0.0, 1.0)), _sock("Scale", 1.5)]}],
+        [link, ("Checker Texture", "Color", "Emission", "Color")])
+    m = mesh(*quad((-1.5, 1.0, -1.99), (-0.5, 1.0, -1.99), (-0.5, 2.0, -1.99), (-1.5, 2.0, -1.99)), panel)
+    m["triangle_uvs"] = np.array([[[0, 0], [1, 0], [1, 1]], [[0, 0], [1, 1], [0, 1]]], dtype=np.float64)
+    meshes.append(m)
+    # glossy Principled panel: all scalars from the graph (the JSON fields are ignored)
+    out, link = _out("Principled BSDF")
+    gl = material((0.9, 0.1, 0.1), 0.0, 0.9)
+    gl["use_nodes"] = True
+    gl["node_tree"] = _tree([
+        out,
+        {"name": "Principled BSDF", "type": "ShaderNodeBsdfPrincipled",
+         "inputs": [_sock("Base Color", (0.7, 0.75, 0.8, 1.0)), _sock("Metallic", 1.0), _sock("Roughness", 0.25),
+                    _sock("IOR", 1.45), _sock("Emission Color", (0.0, 0.0, 0.0, 1.0)), _sock("Emission Strength", 0.0)]}],
+        [link])
+    meshes.append(mesh(*quad((0.5, 0.2, -1.0), (1.8, 0.2, -1.0), (1.8, 1.5, -1.6), (0.5, 1.5, -1.6)), gl))
+    # a node tree present but use_nodes off: the JSON fields apply
+    bx = material((0.3, 0.5, 0.8), 0.0, 0.4)
+    bx["use_nodes"] = False
+    bx["node_tree"] = floor_mat["node_tree"]
+    meshes.append(mesh(*box((0.6, 0.6, 0.6), (-0.8, 0.0, 0.3), 20.0), bx))
+    lights = [{"type": "POINT", "position": [0.5, 2.2, 1.0], "color": [1, 1, 1], "energy": 150.0, "radius": 0.05}]
+    scene = {"meshes": meshes, "native_lights": lights, "environment": {"color": [0.05, 0.05, 0.06], "strength": 1.0}}
+    camera = (0.0, 1.2, 4.5, 0.0, -0.15, -1.0, 0.0, 1.0, 0.0, 50.0)
+    return scene, camera

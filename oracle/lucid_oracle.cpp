@@ -143,6 +143,13 @@ static Scene load_scene(const std::string& s) {
             }
         }
         bool smooth = mj.contains("smooth") && mj["smooth"].get<bool>();
+        std::vector<std::array<V2, 3>> tuv;
+        if (mj.contains("triangle_uvs"))
+            for (const auto& t : mj["triangle_uvs"]) {
+                std::array<V2, 3> a;
+                for (int k = 0; k < 3; ++k) a[k] = V2{t[k][0].get<float>(), t[k][1].get<float>()};
+                tuv.push_back(a);
+            }
         int ti = 0;
         if (mj.contains("triangles")) {
             for (const auto& t : mj["triangles"]) {
@@ -150,6 +157,7 @@ static Scene load_scene(const std::string& s) {
                 tr.i0 = t[0]; tr.i1 = t[1]; tr.i2 = t[2];
                 if (has_tn && (size_t)ti < tn.size()) { tr.n0 = tn[ti][0]; tr.n1 = tn[ti][1]; tr.n2 = tn[ti][2]; tr.smooth = smooth; }
                 else tr.smooth = false;
+                if ((size_t)ti < tuv.size()) { tr.uv0 = tuv[ti][0]; tr.uv1 = tuv[ti][1]; tr.uv2 = tuv[ti][2]; tr.has_uv = true; }
                 m.tris.push_back(tr);
                 ++ti;
             }
@@ -178,7 +186,8 @@ static Scene load_scene(const std::string& s) {
             if (mat.contains("node_tree") && !mat["node_tree"].is_null()) {
                 surf_linked = surface_socket_linked(mat["node_tree"], nt_valid);
                 if (!nt_valid) surf_linked = true;
-                m.mat.use_nodes = mat.value("use_nodes", false) && nt_valid;
+                m.mat.tree = parse_node_tree(mat["node_tree"]);
+                m.mat.use_nodes = mat.value("use_nodes", false) && m.mat.tree.valid;
             }
             if (mat.contains("volume") && !mat["volume"].is_null()) {
                 const auto& vol = mat["volume"];

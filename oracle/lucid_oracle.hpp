@@ -30,6 +30,7 @@
 #include <vector>
 
 #include "../blender-lucid-renderer_b200/csrc/lucid_math.h"
+#include "oracle_nodes.hpp"
 
 namespace orc {
 
@@ -192,16 +193,24 @@ struct Material {
     float metallic = 0, roughness = 0.5f;
     RGB emission{0, 0, 0};
     float transmission = 0, ior = 1.45f;
-    bool use_nodes = false;       // node-graph evaluation is not restated (see loader)
+    bool use_nodes = false;       // "use_nodes" and a valid node tree (pybind_renderer.hpp:1381-1384)
+    NodeTree tree;
     Volume volume;
     bool volume_boundary_only = false;
 };
+inline RGB mat_emission(const Material& m, V2 uv) {   // getEmission (path_tracer.hpp:67-72)
+    if (!m.use_nodes) return m.emission;
+    C3 e = node_emission(m.tree, uv);
+    return RGB(e.r, e.g, e.b);
+}
 struct Tri {
     int i0 = 0, i1 = 0, i2 = 0;
     V3 face_n{0, 1, 0};
     V3 n0{0, 1, 0}, n1{0, 1, 0}, n2{0, 1, 0};
     V3 centroid;
     bool smooth = false;
+    V2 uv0, uv1, uv2;             // "triangle_uvs" (pybind_renderer.hpp:1296-1336)
+    bool has_uv = false;
 };
 struct BNode { V3 bmin, bmax; int left = -1, right = -1, tri_start = 0, tri_count = 0; };
 struct Mesh {
@@ -373,6 +382,7 @@ struct Hit {
     V3 normal{0, 1, 0};
     const Material* mat = nullptr;
     int mesh = -1, tri = -1;
+    V2 uv;                        // (0, 0) when the hit triangle has no UVs
 };
 
 // geometry/bvh.hpp:34-142
@@ -407,6 +417,10 @@ inline void traverse(const Mesh& m, const Ray& r, V3 inv, Hit& res, int mi, floa
                 res.mat = &m.mat;
                 res.mesh = mi;
                 res.tri = ti;
+                // bvh.hpp:67-72 (the closest triangle's own UVs; the reference
+                // leaves an earlier candidate's uv in place when it has none)
+                res.uv = tr.has_uv ? V2{tr.uv0.x * w + tr.uv1.x * u + tr.uv2.x * v, tr.uv0.y * w + tr.uv1.y * u + tr.uv2.y * v}
+                                   : V2{};
             }
         } else {
             if (sp < 62) {
@@ -534,7 +548,7 @@ inline SceneLights build_lights(const Scene& s) {
     for (size_t mi = 0; mi < s.meshes.size(); ++mi) {
         const Mesh& m = s.meshes[mi];
         sl.tri_light[mi].assign(m.tris.size(), -1);
-        RGB e = m.mat.emission;
+        RGB e = mat_emission(m.mat, V2{});   // scene_lights.hpp:64-69: node emission at uv (0, 0)
         if (!is_emissive(e)) continue;
         for (size_t ti = 0; ti < m.tris.size(); ++ti) {
             const Tri& t = m.tris[ti];
@@ -801,10 +815,18 @@ struct BsdfSample {
     int type = ST_DIFFUSE;
     bool valid() const { return kind == KIND_PRECOMP ? true : pdf > MIN_PDF; }
 };
-inline MatParams mat_params(const Material& m) {   // path_tracer.hpp:45-64
+inline MatParams mat_params(const Material& m, V2 uv) {   // path_tracer.hpp:45-64
     MatParams p;
     p.albedo = m.albedo; p.metallic = m.metallic; p.roughness = m.roughness;
     p.transmission = m.transmission; p.ior = m.ior;
+    if (m.use_nodes) {
+        C3 a = node_albedo(m.tree, uv);
+        p.albedo = RGB(a.r, a.g, a.b);
+        p.metallic = node_scalar(m.tree, "Metallic", nullptr, 0.0f);
+        p.roughness = node_scalar(m.tree, "Roughness", nullptr, 0.5f);
+        p.transmission = node_scalar(m.tree, "Transmission", "Transmission Weight", 0.0f);
+        p.ior = node_scalar(m.tree, "IOR", nullptr, 1.45f);
+    }
     p.roughness = smax(p.roughness, MIN_ROUGHNESS);
     return p;
 }
@@ -1254,8 +1276,8 @@ inline RGB trace(const Scene& s, const SceneLights& sl, const Ray& ray, int max_
             result = result + mul(T, env);
             break;
         }
-        MatParams m = mat_params(*hit.mat);
-        RGB emission = hit.mat->emission;
+        MatParams m = mat_params(*hit.mat, hit.uv);
+        RGB emission = mat_emission(*hit.mat, hit.uv);
         V3 n = hit.normal;
         V3 wo = -cur.d;
         bool front = dot(wo, n) > 0;
@@ -1409,8 +1431,12 @@ inline RGB debug_pass(const Scene& s, const Ray& r, int mode) {
     Hit h = intersect_scene(s, r, 0.0f, RAY_T_MAX);
     if (!h.hit) return RGB(0, 0, 0);
     if (mode == 0) return RGB(h.normal.x, h.normal.y, h.normal.z) * 0.5f + RGB(0.5f, 0.5f, 0.5f);
-    if (mode == 1) return h.mat->albedo;
-    return h.mat->emission;   // apply_camera_sensitivity with the default sensitivity 1
+    if (mode == 1) {
+        if (!h.mat->use_nodes) return h.mat->albedo;
+        C3 a = node_albedo(h.mat->tree, h.uv);
+        return RGB(a.r, a.g, a.b);
+    }
+    return mat_emission(*h.mat, h.uv);   // apply_camera_sensitivity with the default sensitivity 1
 }
 
 }  // namespace orc

@@ -175,8 +175,8 @@ inline RGB trace_diag(const Scene& s, const SceneLights& sl, const Ray& ray, int
             }
             break;
         }
-        MatParams m = mat_params(*hit.mat);
-        RGB emission = hit.mat->emission;
+        MatParams m = mat_params(*hit.mat, hit.uv);
+        RGB emission = mat_emission(*hit.mat, hit.uv);
         uint8_t bt = classify_bsdf(m);
         bool delta = is_delta_bsdf(m);
         bool has_em = is_emissive(emission);

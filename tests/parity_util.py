@@ -39,6 +39,8 @@ def scene_and_camera(name: str, workdir: str):
         return ls.material_preview_scene()
     if name == "hard_indirect":
         return ls.hard_indirect_scene()
+    if name == "textured":
+        return ls.textured_scene()
     raise KeyError(name)
 
 

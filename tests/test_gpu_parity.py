@@ -31,6 +31,8 @@ CASES = [
     ("two_small_quads", "nee", 32, 24, 2, 6),   # single-leaf BVH
     ("material_preview", "mis", 32, 32, 2, 8),
     ("hard_indirect", "mis", 40, 24, 2, 8),
+    ("textured", "mis", 48, 36, 4, 8),          # node-graph materials with UV checker textures
+    ("textured", "nee", 40, 30, 2, 6),
 ]
 
 
@@ -68,10 +70,11 @@ def test_tile_equals_full_frame(ctx, workdir):
     assert np.array_equal(full_unflip[8:28, 16:40], tile_unflip)
 
 
-def test_debug_passes_match_oracle(ctx, workdir):
+@pytest.mark.parametrize("scene", ["all_lights", "textured"])
+def test_debug_passes_match_oracle(ctx, workdir, scene):
     import lucid_scenes as ls
     from oracle_ctypes import Oracle
-    sc, cam = scene_and_camera("all_lights", workdir)
+    sc, cam = scene_and_camera(scene, workdir)
     ctx.load_scene_json(ls.to_json(sc))
     ctx.set_camera(*cam)
     o = Oracle()
