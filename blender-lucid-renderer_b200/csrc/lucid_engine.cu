@@ -2155,6 +2155,35 @@ int Engine::build_bvh() {
     CK(D.nodes.alloc(n4.size()));
     CK(cudaMemcpyAsync(D.nodes.p, n4.data(), n4.size() * sizeof(DevNode4), cudaMemcpyHostToDevice, st));
     CK(cudaStreamSynchronize(st));
+    // Binary nodes in depth-first order (a node, its left subtree, its right
+    // subtree; root first): a ray's descent then reads nearby lines, and the
+    // top of the tree shares a few cache lines.
+    {
+        std::vector<int> order(n - 1, -1), stk{root};
+        std::vector<DevNode> dfs;
+        dfs.reserve(nodes);
+        while (!stk.empty()) {
+            int nd = stk.back();
+            stk.pop_back();
+            order[nd] = (int)dfs.size();
+            dfs.push_back(hn[nd]);
+            int c0, c1;
+            std::memcpy(&c0, &hn[nd].lmin_lc.w, 4);
+            std::memcpy(&c1, &hn[nd].lmax_rc.w, 4);
+            if (c1 >= 0) stk.push_back(c1);
+            if (c0 >= 0) stk.push_back(c0);
+        }
+        for (DevNode& d : dfs) {
+            int c0, c1;
+            std::memcpy(&c0, &d.lmin_lc.w, 4);
+            std::memcpy(&c1, &d.lmax_rc.w, 4);
+            if (c0 >= 0) { c0 = order[c0]; std::memcpy(&d.lmin_lc.w, &c0, 4); }
+            if (c1 >= 0) { c1 = order[c1]; std::memcpy(&d.lmax_rc.w, &c1, 4); }
+        }
+        CK(cudaMemcpyAsync(D.nodes2.p, dfs.data(), dfs.size() * sizeof(DevNode), cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+        root = 0;
+    }
     v.nodes = D.nodes.p;
     v.root = 0;
     v.nodes2 = D.nodes2.p;
