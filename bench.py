@@ -160,7 +160,8 @@ def scene_upload(device: int, js: str, cache_dir: str) -> dict:
     """Time to a renderable scene for the benchmark scene in its two forms:
     JSON text (parse + flatten + upload + BVH) and arrays
     (lucid_cuda_load_scene_arrays: flatten + upload + BVH), each into a
-    fresh context, each followed by a one-sample 64x64 render."""
+    fresh context, each followed by a one-sample 64x64 render (JSON meshes
+    are parsed on all host threads)."""
     import lucid_capi
     import lucid_scenes as ls
     os.makedirs(cache_dir, exist_ok=True)
@@ -168,17 +169,22 @@ def scene_upload(device: int, js: str, cache_dir: str) -> dict:
     arrays = ls.scene_arrays(sc, json_rounding=False)
     out = {}
     for form in ("json", "arrays"):
-        c = lucid_capi.Context(device)
-        t0 = time.perf_counter()
-        if form == "json":
-            c.load_scene_json(js)
-        else:
-            c.load_scene_arrays(arrays)
-        c.set_camera(*cam)
-        c.set_algorithm(ALGO)
-        c.render(64, 64, 64, 64, 1, 0, DEPTH)
-        out[f"{form}_s"] = round(time.perf_counter() - t0, 3)
-        c.close()
+        best = None
+        for _ in range(2):   # the better of two (host page cache and allocator warm)
+            c = lucid_capi.Context(device)
+            t0 = time.perf_counter()
+            if form == "json":
+                c.load_scene_json(js)
+            else:
+                c.load_scene_arrays(arrays)
+            c.set_camera(*cam)
+            c.set_algorithm(ALGO)
+            c.render(64, 64, 64, 64, 1, 0, DEPTH)
+            dt = time.perf_counter() - t0
+            best = dt if best is None else min(best, dt)
+            c.close()
+        out[f"{form}_s"] = round(best, 3)
+    out["host_threads"] = os.cpu_count()
     out["triangles"] = sum(len(m["triangles"]) // 3 for m in arrays["meshes"])
     out["json_mb"] = round(len(js) / 1e6, 1)
     return out

@@ -7,6 +7,8 @@
 // conversions, so the uploaded lights, CDF and normals equal the CPU
 // renderer's bit for bit.  Compiled with -ffp-contract=off.
 #include <algorithm>
+#include <atomic>
+#include <thread>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -315,114 +317,268 @@ void finish_scene(HostScene& S, Assembly& A, const std::vector<NativeLight>& nat
     }
 }
 
+// One "meshes" entry read as loadSceneFromJsonString reads it
+// (pybind_renderer.hpp:1266-1536): geometry, normals, UVs, the material (node
+// programs compiled into M.ops, offsets relative to M.ops) and the volume.
+struct MeshIn {
+    std::vector<F3> verts;
+    std::vector<std::array<F3, 3>> tn;
+    bool has_tn = false, smooth = false;
+    std::vector<std::array<int, 3>> tris;
+    std::vector<std::array<float, 6>> uvs;
+    bool use_nodes = false;
+    NodeMaterial nm;
+    std::vector<float4> ops;
+    float alb[3] = {0.8f, 0.8f, 0.8f}, metallic = 0.0f, roughness = 0.5f, em[3] = {0, 0, 0};
+    float transmission = 0.0f, ior = 1.45f;
+    bool boundary = false;
+    DevVolume vol;
+    bool vol_has_grid = false;
+    std::vector<float> grid;
+};
+
+void read_mesh(const json& mj, MeshIn& M) {
+    std::vector<F3> verts;
+    if (mj.contains("vertices"))
+        for (const auto& v : mj["vertices"]) verts.push_back(arr3(v));
+    std::vector<std::array<F3, 3>> tn;
+    bool has_tn = false;
+    if (mj.contains("triangle_normals")) {
+        has_tn = true;
+        for (const auto& t : mj["triangle_normals"]) {
+            std::array<F3, 3> a;
+            for (int k = 0; k < 3; ++k)
+                a[k] = dir_or(F3{static_cast<float>(t[k][0]), static_cast<float>(t[k][1]),
+                                 static_cast<float>(t[k][2])}, F3{0, 0, 1});
+            tn.push_back(a);
+        }
+    }
+    bool smooth = mj.contains("smooth") && mj["smooth"].get<bool>();
+    std::vector<std::array<int, 3>> tris;
+    if (mj.contains("triangles"))
+        for (const auto& t : mj["triangles"]) tris.push_back({t[0].get<int>(), t[1].get<int>(), t[2].get<int>()});
+    std::vector<std::array<float, 6>> uvs;
+    if (mj.contains("triangle_uvs"))
+        for (const auto& t : mj["triangle_uvs"])
+            uvs.push_back({t[0][0].get<float>(), t[0][1].get<float>(), t[1][0].get<float>(),
+                           t[1][1].get<float>(), t[2][0].get<float>(), t[2][1].get<float>()});
+    bool use_nodes = false;
+    NodeMaterial nm;
+
+    // material (pybind_renderer.hpp:1346-1503)
+    float alb[3] = {0.8f, 0.8f, 0.8f}, metallic = 0.0f, roughness = 0.5f, em[3] = {0, 0, 0};
+    float transmission = 0.0f, ior = 1.45f;
+    bool boundary = false;
+    DevVolume vol;
+    std::memset(&vol, 0, sizeof(vol));
+    vol.color[0] = vol.color[1] = vol.color[2] = 1.0f;
+    bool vol_has_grid = false;
+    std::vector<float> grid;
+    if (mj.contains("material")) {
+        const auto& mat = mj["material"];
+        if (mat.contains("base_color")) { F3 c = arr3(mat["base_color"]); alb[0] = c.x; alb[1] = c.y; alb[2] = c.z; }
+        if (mat.contains("metallic")) metallic = mat["metallic"];
+        if (mat.contains("roughness")) roughness = mat["roughness"];
+        if (mat.contains("emission")) { F3 c = arr3(mat["emission"]); em[0] = c.x; em[1] = c.y; em[2] = c.z; }
+        if (mat.contains("transmission")) transmission = mat["transmission"];
+        if (mat.contains("ior")) ior = mat["ior"];
+        bool nt_valid = false, surf = true;
+        if (mat.contains("node_tree") && !mat["node_tree"].is_null()) {
+            surf = surface_linked(mat["node_tree"], nt_valid);
+            if (!nt_valid) surf = true;
+            use_nodes = nt_valid && mat.value("use_nodes", false);
+            if (use_nodes) nm = compile_node_material(mat["node_tree"], M.ops);
+        }
+        if (mat.contains("volume") && !mat["volume"].is_null()) {
+            const auto& v = mat["volume"];
+            if (v.contains("color") && v["color"].is_array() && v["color"].size() >= 3) {
+                F3 c = arr3(v["color"]); vol.color[0] = c.x; vol.color[1] = c.y; vol.color[2] = c.z;
+            }
+            if (v.contains("absorption_color") && v["absorption_color"].is_array() && v["absorption_color"].size() >= 3) {
+                F3 c = arr3(v["absorption_color"]); vol.absorption[0] = c.x; vol.absorption[1] = c.y; vol.absorption[2] = c.z;
+            }
+            if (v.contains("density")) vol.density = v["density"].get<float>();
+            if (v.contains("anisotropy")) vol.anisotropy = v["anisotropy"].get<float>();
+            if (v.contains("smoke_grid") && v["smoke_grid"].is_object()) {
+                const auto& sg = v["smoke_grid"];
+                if (sg.contains("dims") && sg["dims"].is_array() && sg["dims"].size() == 3 && sg.contains("world_min") &&
+                    sg["world_min"].is_array() && sg.contains("world_max") && sg["world_max"].is_array() &&
+                    sg.contains("sidecar_path")) {
+                    for (int i = 0; i < 3; ++i) vol.dims[i] = sg["dims"][i].get<int>();
+                    for (int i = 0; i < 3; ++i) {
+                        vol.wmin[i] = sg["world_min"][i].get<float>();
+                        vol.wmax[i] = sg["world_max"][i].get<float>();
+                    }
+                    if (vol.dims[0] < 2 || vol.dims[1] < 2 || vol.dims[2] < 2)
+                        throw std::runtime_error("volume grid dims must be >= 2 per axis");
+                    size_t n = (size_t)vol.dims[0] * vol.dims[1] * vol.dims[2];
+                    std::ifstream f(sg["sidecar_path"].get<std::string>(), std::ios::binary);
+                    if (f) {
+                        grid.resize(n);
+                        f.read(reinterpret_cast<char*>(grid.data()), n * sizeof(float));
+                        float mx = 0.0f;
+                        for (float d : grid) if (d > mx) mx = d;
+                        vol.grid_max = mx;
+                        vol_has_grid = true;
+                    } else {
+                        vol.dims[0] = vol.dims[1] = vol.dims[2] = 0;
+                    }
+                }
+            }
+        }
+        bool present = vol.density > 0.0f || vol_has_grid;
+        if (present && !surf) boundary = true;
+    }
+    M.verts = std::move(verts); M.tn = std::move(tn); M.has_tn = has_tn; M.smooth = smooth; M.tris = std::move(tris);
+    M.uvs = std::move(uvs); M.use_nodes = use_nodes; M.nm = nm;
+    for (int c = 0; c < 3; ++c) { M.alb[c] = alb[c]; M.em[c] = em[c]; }
+    M.metallic = metallic; M.roughness = roughness; M.transmission = transmission; M.ior = ior;
+    M.boundary = boundary; M.vol = vol; M.vol_has_grid = vol_has_grid; M.grid = std::move(grid);
+}
+
+// Appends a read mesh (its node programs relocated after the scene's).
+void emit_read_mesh(HostScene& S, Assembly& A, MeshIn& M) {
+    const int base = (int)S.tex_ops.size() / 2;
+    if (M.use_nodes) {
+        if (M.nm.albedo_n) M.nm.albedo_start += base;
+        if (M.nm.emission_n) M.nm.emission_start += base;
+        S.tex_ops.insert(S.tex_ops.end(), M.ops.begin(), M.ops.end());
+    }
+    emit_mesh(S, A, M.verts, M.tris, M.tn, M.has_tn, M.smooth, M.alb, M.metallic, M.roughness, M.em, M.transmission,
+              M.ior, M.boundary, M.vol, M.vol_has_grid, M.grid, M.uvs, M.use_nodes ? &M.nm : nullptr);
+}
+
+// Byte ranges of the elements of the document's top-level "meshes" array
+// and of the array itself, found by a structural scan (strings and escapes
+// respected).  False when the text is not a plain object with exactly one
+// "meshes" array (the caller then parses it whole).
+bool scan_meshes(const char* t, size_t n, size_t& arr_begin, size_t& arr_end,
+                 std::vector<std::pair<size_t, size_t>>& elems) {
+    size_t i = 0;
+    auto ws = [&] { while (i < n && (t[i] == ' ' || t[i] == '\n' || t[i] == '\r' || t[i] == '\t')) ++i; };
+    auto skip_string = [&]() -> bool {   // at '"'
+        for (++i; i < n; ++i) {
+            if (t[i] == '\\') { ++i; continue; }
+            if (t[i] == '"') { ++i; return true; }
+        }
+        return false;
+    };
+    auto skip_value = [&]() -> bool {
+        ws();
+        if (i >= n) return false;
+        if (t[i] == '"') return skip_string();
+        if (t[i] == '{' || t[i] == '[') {
+            int depth = 0;
+            while (i < n) {
+                const char c = t[i];
+                if (c == '"') { if (!skip_string()) return false; continue; }
+                if (c == '{' || c == '[') ++depth;
+                else if (c == '}' || c == ']') { if (--depth == 0) { ++i; return true; } }
+                ++i;
+            }
+            return false;
+        }
+        while (i < n && t[i] != ',' && t[i] != '}' && t[i] != ']') ++i;   // number / literal
+        return true;
+    };
+    ws();
+    if (i >= n || t[i] != '{') return false;
+    ++i;
+    bool found = false;
+    for (;;) {
+        ws();
+        if (i < n && t[i] == '}') break;
+        if (i >= n || t[i] != '"') return false;
+        const size_t k0 = i;
+        if (!skip_string()) return false;
+        const bool is_meshes = (i - k0 == 8) && std::memcmp(t + k0, "\"meshes\"", 8) == 0;
+        ws();
+        if (i >= n || t[i] != ':') return false;
+        ++i;
+        ws();
+        if (is_meshes) {
+            if (found || i >= n || t[i] != '[') return false;
+            found = true;
+            arr_begin = i++;
+            for (;;) {
+                ws();
+                if (i < n && t[i] == ']') { ++i; break; }
+                const size_t e0 = i;
+                if (!skip_value()) return false;
+                elems.push_back({e0, i});
+                ws();
+                if (i < n && t[i] == ',') { ++i; continue; }
+                if (i < n && t[i] == ']') { ++i; break; }
+                return false;
+            }
+            arr_end = i;
+        } else if (!skip_value()) {
+            return false;
+        }
+        ws();
+        if (i < n && t[i] == ',') { ++i; continue; }
+        if (i < n && t[i] == '}') break;
+        return false;
+    }
+    return found;
+}
+
 }  // namespace
 
 bool parse_scene_json(const char* text, size_t length, HostScene& S, std::string& err) {
     S = HostScene();
+    // Large scenes: the mesh entries are parsed on all host threads, then
+    // assembled in order (the result is the same as one whole parse).
+    size_t ab = 0, ae = 0;
+    std::vector<std::pair<size_t, size_t>> elems;
+    std::vector<MeshIn> parsed;
+    bool split = length > (8u << 20) && scan_meshes(text, length, ab, ae, elems) && elems.size() > 1;
     json j;
     try {
-        j = json::parse(text, text + length);
+        if (split) {
+            std::string rest(text, ab);
+            rest += "[]";
+            rest.append(text + ae, length - ae);
+            j = json::parse(rest);
+        } else {
+            j = json::parse(text, text + length);
+        }
     } catch (const std::exception& e) {
         err = std::string("scene JSON parse error: ") + e.what();
         return false;
     }
+    if (split) {
+        parsed.resize(elems.size());
+        std::vector<std::string> errors(elems.size());
+        std::atomic<size_t> next{0};
+        auto work = [&] {
+            for (size_t k; (k = next.fetch_add(1)) < elems.size();) {
+                try {
+                    read_mesh(json::parse(text + elems[k].first, text + elems[k].second), parsed[k]);
+                } catch (const json::parse_error& e) {
+                    errors[k] = std::string("scene JSON parse error: ") + e.what();
+                } catch (const std::exception& e) {
+                    errors[k] = std::string("malformed scene: ") + e.what();
+                }
+            }
+        };
+        const unsigned nt = std::max(1u, std::min((unsigned)elems.size(), std::thread::hardware_concurrency()));
+        std::vector<std::thread> pool;
+        for (unsigned t = 1; t < nt; ++t) pool.emplace_back(work);
+        work();
+        for (auto& t : pool) t.join();
+        for (const auto& e : errors)
+            if (!e.empty()) { err = e; return false; }
+    }
     try {
         Assembly A;
-        if (j.contains("meshes")) {
+        if (split) {
+            for (auto& M : parsed) emit_read_mesh(S, A, M);
+        } else if (j.contains("meshes")) {
             for (const auto& mj : j["meshes"]) {
-                std::vector<F3> verts;
-                if (mj.contains("vertices"))
-                    for (const auto& v : mj["vertices"]) verts.push_back(arr3(v));
-                std::vector<std::array<F3, 3>> tn;
-                bool has_tn = false;
-                if (mj.contains("triangle_normals")) {
-                    has_tn = true;
-                    for (const auto& t : mj["triangle_normals"]) {
-                        std::array<F3, 3> a;
-                        for (int k = 0; k < 3; ++k)
-                            a[k] = dir_or(F3{static_cast<float>(t[k][0]), static_cast<float>(t[k][1]),
-                                             static_cast<float>(t[k][2])}, F3{0, 0, 1});
-                        tn.push_back(a);
-                    }
-                }
-                bool smooth = mj.contains("smooth") && mj["smooth"].get<bool>();
-                std::vector<std::array<int, 3>> tris;
-                if (mj.contains("triangles"))
-                    for (const auto& t : mj["triangles"]) tris.push_back({t[0].get<int>(), t[1].get<int>(), t[2].get<int>()});
-                std::vector<std::array<float, 6>> uvs;
-                if (mj.contains("triangle_uvs"))
-                    for (const auto& t : mj["triangle_uvs"])
-                        uvs.push_back({t[0][0].get<float>(), t[0][1].get<float>(), t[1][0].get<float>(),
-                                       t[1][1].get<float>(), t[2][0].get<float>(), t[2][1].get<float>()});
-                bool use_nodes = false;
-                NodeMaterial nm;
-
-                // material (pybind_renderer.hpp:1346-1503)
-                float alb[3] = {0.8f, 0.8f, 0.8f}, metallic = 0.0f, roughness = 0.5f, em[3] = {0, 0, 0};
-                float transmission = 0.0f, ior = 1.45f;
-                bool boundary = false;
-                DevVolume vol;
-                std::memset(&vol, 0, sizeof(vol));
-                vol.color[0] = vol.color[1] = vol.color[2] = 1.0f;
-                bool vol_has_grid = false;
-                std::vector<float> grid;
-                if (mj.contains("material")) {
-                    const auto& mat = mj["material"];
-                    if (mat.contains("base_color")) { F3 c = arr3(mat["base_color"]); alb[0] = c.x; alb[1] = c.y; alb[2] = c.z; }
-                    if (mat.contains("metallic")) metallic = mat["metallic"];
-                    if (mat.contains("roughness")) roughness = mat["roughness"];
-                    if (mat.contains("emission")) { F3 c = arr3(mat["emission"]); em[0] = c.x; em[1] = c.y; em[2] = c.z; }
-                    if (mat.contains("transmission")) transmission = mat["transmission"];
-                    if (mat.contains("ior")) ior = mat["ior"];
-                    bool nt_valid = false, surf = true;
-                    if (mat.contains("node_tree") && !mat["node_tree"].is_null()) {
-                        surf = surface_linked(mat["node_tree"], nt_valid);
-                        if (!nt_valid) surf = true;
-                        use_nodes = nt_valid && mat.value("use_nodes", false);
-                        if (use_nodes) nm = compile_node_material(mat["node_tree"], S.tex_ops);
-                    }
-                    if (mat.contains("volume") && !mat["volume"].is_null()) {
-                        const auto& v = mat["volume"];
-                        if (v.contains("color") && v["color"].is_array() && v["color"].size() >= 3) {
-                            F3 c = arr3(v["color"]); vol.color[0] = c.x; vol.color[1] = c.y; vol.color[2] = c.z;
-                        }
-                        if (v.contains("absorption_color") && v["absorption_color"].is_array() && v["absorption_color"].size() >= 3) {
-                            F3 c = arr3(v["absorption_color"]); vol.absorption[0] = c.x; vol.absorption[1] = c.y; vol.absorption[2] = c.z;
-                        }
-                        if (v.contains("density")) vol.density = v["density"].get<float>();
-                        if (v.contains("anisotropy")) vol.anisotropy = v["anisotropy"].get<float>();
-                        if (v.contains("smoke_grid") && v["smoke_grid"].is_object()) {
-                            const auto& sg = v["smoke_grid"];
-                            if (sg.contains("dims") && sg["dims"].is_array() && sg["dims"].size() == 3 && sg.contains("world_min") &&
-                                sg["world_min"].is_array() && sg.contains("world_max") && sg["world_max"].is_array() &&
-                                sg.contains("sidecar_path")) {
-                                for (int i = 0; i < 3; ++i) vol.dims[i] = sg["dims"][i].get<int>();
-                                for (int i = 0; i < 3; ++i) {
-                                    vol.wmin[i] = sg["world_min"][i].get<float>();
-                                    vol.wmax[i] = sg["world_max"][i].get<float>();
-                                }
-                                if (vol.dims[0] < 2 || vol.dims[1] < 2 || vol.dims[2] < 2)
-                                    throw std::runtime_error("volume grid dims must be >= 2 per axis");
-                                size_t n = (size_t)vol.dims[0] * vol.dims[1] * vol.dims[2];
-                                std::ifstream f(sg["sidecar_path"].get<std::string>(), std::ios::binary);
-                                if (f) {
-                                    grid.resize(n);
-                                    f.read(reinterpret_cast<char*>(grid.data()), n * sizeof(float));
-                                    float mx = 0.0f;
-                                    for (float d : grid) if (d > mx) mx = d;
-                                    vol.grid_max = mx;
-                                    vol_has_grid = true;
-                                } else {
-                                    vol.dims[0] = vol.dims[1] = vol.dims[2] = 0;
-                                }
-                            }
-                        }
-                    }
-                    bool present = vol.density > 0.0f || vol_has_grid;
-                    if (present && !surf) boundary = true;
-                }
-                emit_mesh(S, A, verts, tris, tn, has_tn, smooth, alb, metallic, roughness, em, transmission, ior,
-                          boundary, vol, vol_has_grid, grid, uvs, use_nodes ? &nm : nullptr);
+                MeshIn M;
+                read_mesh(mj, M);
+                emit_read_mesh(S, A, M);
             }
         }
         std::vector<NativeLight> native;

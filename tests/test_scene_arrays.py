@@ -62,3 +62,24 @@ def test_array_upload_renders_bit_identically(name, algo, workdir):
     c.close()
     assert stats[0] == stats[1]
     assert np.array_equal(imgs[0], imgs[1])
+
+
+def test_large_json_parsed_in_parallel_matches_the_arrays(workdir):
+    """Scenes above 8 MB of JSON are read mesh by mesh on all host threads;
+    the result is the scene the array form gives."""
+    sc, _ = ls.procedural_scene(seed=4, n_spheres=40, levels=4, emissive_levels=2, workdir=workdir, extent=20.0)
+    js = ls.to_json(sc)
+    assert len(js) > (8 << 20)
+    assert lucid_capi.scene_digest(json_text=js) == lucid_capi.scene_digest(arrays=ls.scene_arrays(sc))
+
+
+def test_large_json_errors_are_reported(workdir):
+    sc, _ = ls.procedural_scene(seed=4, n_spheres=40, levels=4, emissive_levels=2, workdir=workdir, extent=20.0)
+    sc["meshes"][5]["triangles"] = np.array(sc["meshes"][5]["triangles"])
+    sc["meshes"][5]["triangles"][3, 1] = 10 ** 7                # past the vertex array
+    js = ls.to_json(sc)
+    with pytest.raises(lucid_capi.LucidError):
+        lucid_capi.scene_digest(json_text=js)
+    bad = js.replace('"vertices"', '"vertices" x', 1)             # a syntax error inside one mesh
+    with pytest.raises(lucid_capi.LucidError):
+        lucid_capi.scene_digest(json_text=bad)
