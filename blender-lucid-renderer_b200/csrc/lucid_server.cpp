@@ -47,6 +47,8 @@ Server::Server(int device, int slots, long long budget_bytes) : device_(device) 
     for (int s = 0; s < slots; ++s) {
         slot_eng_.emplace_back(new Engine(device));
         slot_scene_.push_back(-1);
+        pre_eng_.emplace_back(nullptr);
+        pre_scene_.push_back(-1);
     }
     for (int s = 0; s < slots; ++s) threads_.emplace_back([this, s] { slot_loop(s); });
 }
@@ -59,6 +61,7 @@ Server::~Server() {
     }
     cv_.notify_all();
     for (auto& t : threads_) t.join();
+    pre_eng_.clear();
     slot_eng_.clear();
     scenes_.clear();
 }
@@ -156,21 +159,53 @@ void Server::slot_loop(int slot) {
             if (busy_from_ < 0) busy_from_ = j->t_start;
         }
         cv_.notify_all();   // another slot may start the next job too
-        int rc = run_job(slot, *j, id);
+        int rc = run_job(*slot_eng_[slot], slot_scene_[slot], *j, slot, false);
+        finish_job(*j, rc);
+    }
+}
+
+void Server::finish_job(Job& j, int rc) {
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        adm_.finish(j.bytes);
+        j.t_end = now();
+        busy_to_ = std::max(busy_to_, j.t_end);
+        if (rc == LUCID_OK && !j.cancel) {
+            j.state = LUCID_JOB_DONE;
+            samples_done_ += (long long)j.d.samples * j.d.width * j.d.height;
+        } else {
+            j.state = j.cancel ? LUCID_JOB_CANCELLED : LUCID_JOB_FAILED;
+        }
+    }
+    cv_.notify_all();
+    done_cv_.notify_all();
+}
+
+// Between two iterations of a batch job: while an interactive job waits at
+// the head of the queue and its memory fits, run it to completion on the
+// slot's second engine (the batch job's iterations in flight keep running on
+// their own stream), so interactive work never waits for a long render.
+void Server::run_waiting_interactive(int slot) {
+    for (;;) {
+        Job* j = nullptr;
         {
             std::lock_guard<std::mutex> lk(mu_);
-            adm_.finish(j->bytes);
-            j->t_end = now();
-            busy_to_ = std::max(busy_to_, j->t_end);
-            if (rc == LUCID_OK && !j->cancel) {
-                j->state = LUCID_JOB_DONE;
-                samples_done_ += (long long)j->d.samples * j->d.width * j->d.height;
-            } else {
-                j->state = j->cancel ? LUCID_JOB_CANCELLED : LUCID_JOB_FAILED;
-            }
+            if (stop_ || queue_.empty()) return;
+            Job& head = jobs_[queue_.front()];
+            if (!head.d.interactive || head.cancel) return;
+            if (adm_.reserved + adm_.running + head.bytes > adm_.budget) return;
+            queue_.pop_front();
+            j = &head;
+            adm_.running += j->bytes;   // admitted beside the slot's batch job (no slot of its own)
+            ++adm_.busy;
+            j->state = LUCID_JOB_RUNNING;
+            j->t_start = now();
         }
-        cv_.notify_all();
-        done_cv_.notify_all();
+        if (!pre_eng_[slot]) pre_eng_[slot].reset(new Engine(device_));
+        // the second engine keeps its path pool from one interactive job to the next
+        // (freeing device memory synchronises the device and would stall the batch job)
+        int rc = run_job(*pre_eng_[slot], pre_scene_[slot], *j, slot, true);
+        finish_job(*j, rc);
     }
 }
 
@@ -213,23 +248,22 @@ int Server::pick_chunk(Engine& e, Job& j, int id, int& offset) {
     return best;
 }
 
-int Server::run_job(int slot, Job& j, int id) {
-    Engine& e = *slot_eng_[slot];
+int Server::run_job(Engine& e, int& engine_scene, Job& j, int slot, bool keep_pool) {
     const LucidJobDesc& d = j.d;
     int rc = LUCID_OK;
-    if (slot_scene_[slot] != d.scene) {
+    if (engine_scene != d.scene) {
         rc = e.share_scene(*scenes_[d.scene]);
         if (rc != LUCID_OK) { j.error = e.last_error(); return rc; }
-        slot_scene_[slot] = d.scene;
+        engine_scene = d.scene;
     }
     const float* c = d.camera;
     e.set_camera(c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7], c[8], c[9]);
     e.set_algorithm(d.algorithm);
     rc = e.job_begin(d.width, d.height, d.samples, d.max_depth, j.chunk_max, false);
-    if (rc != LUCID_OK) { j.error = e.last_error(); e.job_end(); e.release_pool(); return rc; }
+    if (rc != LUCID_OK) { j.error = e.last_error(); e.job_end(); if (!keep_pool) e.release_pool(); return rc; }
     int offset = 0;
-    int chunk = pick_chunk(e, j, id, offset);
-    if (chunk < 0) { j.error = e.last_error(); e.job_end(); e.release_pool(); return -chunk; }
+    int chunk = pick_chunk(e, j, slot, offset);
+    if (chunk < 0) { j.error = e.last_error(); e.job_end(); if (!keep_pool) e.release_pool(); return -chunk; }
     if (offset < d.samples) {
         rc = e.job_set_chunk(chunk, d.samples - offset >= 2 * chunk);
         while (rc == LUCID_OK && offset < d.samples) {
@@ -237,10 +271,13 @@ int Server::run_job(int slot, Job& j, int id) {
             int n = std::min(chunk, d.samples - offset);
             rc = e.job_iterate(offset, n);
             offset += n;
-            std::lock_guard<std::mutex> lk(mu_);
-            // iteration k returns once iteration k - 2 has finished
-            j.done = std::max(j.done, std::max(0, offset - 2 * chunk));
-            if (j.t_first == 0 && offset > 2 * chunk) j.t_first = now();
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                // iteration k returns once iteration k - 2 has finished
+                j.done = std::max(j.done, std::max(0, offset - 2 * chunk));
+                if (j.t_first == 0 && offset > 2 * chunk) j.t_first = now();
+            }
+            if (!d.interactive && rc == LUCID_OK) run_waiting_interactive(slot);
         }
     }
     if (rc == LUCID_OK) rc = e.job_wait();
@@ -256,7 +293,7 @@ int Server::run_job(int slot, Job& j, int id) {
     }
     if (rc != LUCID_OK) j.error = e.last_error();
     e.job_end();
-    e.release_pool();
+    if (!keep_pool) e.release_pool();
     return rc;
 }
 

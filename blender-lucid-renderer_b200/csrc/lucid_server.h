@@ -6,7 +6,9 @@
 // slots; each slot is an engine with its own CUDA stream sharing the
 // uploaded scenes, so iterations of different jobs overlap on the device.
 // Jobs are admitted in arrival order (interactive jobs ahead of batch jobs)
-// as slots and device memory free up
+// as slots and device memory free up; a slot running a batch job also runs
+// waiting interactive jobs between the batch job's iterations, on a second
+// engine, so that they never wait for a long render
 // (HBM budget = uploaded scenes + every running job's path state and film);
 // a job that could never fit is refused at submission.  Each slot picks the
 // samples per iteration (the queue capacity of its waves) with a small
@@ -72,8 +74,10 @@ private:
     template <class Load>
     int add_scene_with(Load&& load, int* scene_id);
     void slot_loop(int slot);
-    int run_job(int slot, Job& j, int id);
-    int pick_chunk(Engine& e, Job& j, int id, int& offset);
+    int run_job(Engine& e, int& engine_scene, Job& j, int slot, bool keep_pool);
+    void finish_job(Job& j, int rc);
+    void run_waiting_interactive(int slot);
+    int pick_chunk(Engine& e, Job& j, int slot, int& offset);
     double now() const;
 
     int device_;
@@ -82,6 +86,8 @@ private:
     std::vector<long long> scene_bytes_;
     std::vector<std::unique_ptr<Engine>> slot_eng_;
     std::vector<int> slot_scene_;
+    std::vector<std::unique_ptr<Engine>> pre_eng_;   // per slot: interactive jobs run between batch iterations
+    std::vector<int> pre_scene_;
     std::vector<std::thread> threads_;
     std::mutex mu_;
     std::condition_variable cv_, done_cv_;

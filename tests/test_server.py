@@ -116,3 +116,28 @@ def test_budget_refusal_and_cancel(workdir):
     st = srv.stats()
     assert st["refused"] == 1 and st["done"] == 1
     srv.close()
+
+
+@pytest.mark.gpu
+def test_interactive_job_runs_between_the_iterations_of_a_long_batch_job(workdir):
+    """One slot busy with a long batch render: an interactive job submitted
+    meanwhile finishes well before it (it runs between the batch job's
+    iterations), and both images still equal single render calls."""
+    scene, cam = scene_and_camera("procedural_small", workdir)
+    big = ("procedural_small", "mis", 640, 480, 1024, 8)
+    small = ("procedural_small", "mis", 64, 48, 4, 8)
+    srv = lucid_capi.Server(0, slots=1)
+    sid = srv.add_scene(ls.to_json(scene))
+    b = srv.submit(sid, cam, big[2], big[3], big[4], big[5], big[1], False)
+    while srv.state(b)[0] != lucid_capi.JOB_RUNNING:
+        time.sleep(0.001)
+    time.sleep(0.05)
+    i = srv.submit(sid, cam, small[2], small[3], small[4], small[5], small[1], True)
+    assert srv.wait(i, 60000) == lucid_capi.JOB_DONE
+    batch_state_when_interactive_done = srv.state(b)[0]
+    assert srv.wait(b, 120000) == lucid_capi.JOB_DONE
+    img_i, img_b = srv.result(i), srv.result(b)
+    srv.close()
+    assert batch_state_when_interactive_done == lucid_capi.JOB_RUNNING
+    np.testing.assert_array_equal(img_i, _single_call(workdir, *small))
+    np.testing.assert_array_equal(img_b, _single_call(workdir, *big))
