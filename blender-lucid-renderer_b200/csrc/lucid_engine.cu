@@ -245,7 +245,7 @@ __global__ void k_raygen(FrameParams f, PathView pv) {
 
 // ---------------------------------------------------------------- trace
 constexpr int kRounds = 4;         // closest hit: descend/test rounds per lane between refills
-constexpr int kShadowSteps = 12;   // any hit: node visits per lane between refills
+constexpr int kShadowSteps = 24;   // any hit: node visits per lane between refills (6: 3x slower, 12: +1 %, 40: +5 %)
 
 LD unsigned lanemask_lt() { return (1u << lane_id()) - 1u; }
 
