@@ -2252,10 +2252,11 @@ static_assert(K_NUM <= LUCID_MAX_KERNEL_KINDS, "kernel kinds");
 // Default paths per wave: large waves keep every depth's launches full and
 // amortise each persistent kernel's tail (measured on the 1M-triangle
 // frame, samples/s: 4 Mi paths 287 M, 16 Mi 390 M, 64 Mi 429 M, the whole
-// 133 M-path frame 435 M), so up to 64 Mi paths, bounded to a fifth of the
-// free device memory (about 170 bytes of path state per path).
+// 133 M-path frame 435 M; with the current kernels 64 Mi 608 M against 622 M
+// for the whole frame), so up to 256 Mi paths (43 GB of path state), bounded
+// to a fifth of the free device memory (about 170 bytes per path).
 long long Engine::default_wave_paths(bool records) const {
-    constexpr long long kMaxWave = 1LL << 26;
+    constexpr long long kMaxWave = 1LL << 28;
     const long long per_path = 168 + (records ? 32 : 0);
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return 1LL << 22;
