@@ -190,6 +190,42 @@ def scene_upload(device: int, js: str, cache_dir: str) -> dict:
     return out
 
 
+def f12_loop(device: int, js: str, cam) -> dict:
+    """The add-on's progressive F12 render of the benchmark frame through
+    RenderSession (sample schedule 4, 8, 16, 32, then 64 per call; numpy
+    accumulation and display rectangle after every call), with the host
+    cost of the reference's per-float list loop for the same frame timed on
+    a 1/64 slice and scaled."""
+    from array import array
+    import lucid_session as lsn
+    os.environ["LUCID_CUDA_DEVICE"] = str(device)   # the device lucidrenderer.Renderer opens
+    s = lsn.RenderSession()
+    s.load_scene_json(js)
+    s.set_camera(lsn.CameraParams(pos=cam[0:3], dir=cam[3:6], up=cam[6:9], fov=cam[9]))
+    s.set_algorithm(ALGO)
+    s.render_tile(lsn.RenderParams(width=64, height=64, samples=1, max_bounces=DEPTH, algorithm=ALGO))
+    t0 = time.perf_counter()
+    res = lsn.render_f12(s, W, H, SPP, max_bounces=DEPTH, algorithm=ALGO, backend="gpu",
+                         on_result=lambda rect, n: None)
+    wall = time.perf_counter() - t0
+    s.shutdown()
+    n = W * H * 4 // 64
+    px = [0.25] * n
+    t1 = time.perf_counter()
+    acc = array("f", px)
+    for i in range(n):
+        acc[i] += px[i]
+    inv = 1.0 / SPP
+    rows = [[acc[i] * inv, acc[i + 1] * inv, acc[i + 2] * inv, 1.0] for i in range(0, n, 4)]
+    per_iter = (time.perf_counter() - t1) * 64
+    del rows
+    return {"frame": f"{W}x{H}, {SPP} spp, depth {DEPTH}, {ALGO}", "iterations": res.iterations,
+            "wall_s": round(wall, 3), "render_s": round(res.render_s, 3), "host_s": round(res.host_s, 3),
+            "samples_per_s": W * H * SPP / wall,
+            "reference_list_loop_s": round(per_iter * len(res.iterations), 2),
+            "reference_list_loop_sample": "array('f') accumulate + display lists on 1/64 of the frame, x64"}
+
+
 def c1_quality(device: int) -> dict:
     """Cornell box (256x256, mis, depth 8): a 16-spp render's relMSE against
     an independent FP64-accumulated 4096-spp GPU reference, and the rate."""
@@ -338,6 +374,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-quality", action="store_true", help="skip the Cornell relMSE measurement")
     ap.add_argument("--no-upload", action="store_true", help="skip the JSON vs array scene-upload timing")
+    ap.add_argument("--no-f12", action="store_true", help="skip the progressive F12 loop through RenderSession")
     ap.add_argument("--no-serving", action="store_true", help="skip the request-loop job trace")
     ap.add_argument("--no-guiding", action="store_true", help="skip the guided-vs-plain equal-time comparison")
     ap.add_argument("--guiding-only", action="store_true", help="only the guided-vs-plain comparison")
@@ -448,6 +485,7 @@ def main():
     mrays = (segs + shadows) / (per_step_ms[-1] / 1000.0) / 1e6
 
     upload = scene_upload(local_rank, js, args.cache) if rank == 0 and world == 1 and not args.no_upload else None
+    f12 = f12_loop(local_rank, js, cam) if rank == 0 and world == 1 and not args.no_f12 else None
     quality = c1_quality(local_rank) if rank == 0 and not args.no_quality else None
     serve = serving(local_rank) if rank == 0 and world == 1 and not args.no_serving else None
     guide = (guiding(local_rank, args.guide_budget_ms, args.guide_width, args.guide_height)
@@ -479,7 +517,7 @@ def main():
                         for k, v in kern.items()},
             "mrays_per_s": mrays, "segments_per_step": segs, "shadow_rays_per_step": shadows,
             "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": cpu, "quality": quality,
-            "serving": serve, "guiding": guide, "scene_upload": upload,
+            "serving": serve, "guiding": guide, "scene_upload": upload, "f12": f12,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -175,19 +175,25 @@ public:
     bool is_camera_set() const { return camera_set_; }
     int get_mesh_count() const { return scene_loaded_ ? mesh_count_ : 0; }
 
-    std::vector<float> render(int tx, int ty, int tw, int th, int fw, int fh, int samples, int offset, int depth) {
-        if (tw <= 0 || th <= 0) throw std::invalid_argument("tile size must be positive");
-        std::vector<float> px((size_t)tw * th * 4, 0.0f);
+    // Renders into `px` (tw * th * 4 floats, zeroed by the caller); the
+    // return-code handling of pybind_renderer.hpp:185-361 (no scene: a zero
+    // buffer and a message; cancelled: the partial sum).
+    void render_into(float* px, int tx, int ty, int tw, int th, int fw, int fh, int samples, int offset, int depth) {
         LucidRenderParams p{tx, ty, tw, th, fw, fh, samples, offset, depth, 0};
-        int rc = lucid_cuda_render(ctx_, &p, px.data(), nullptr);
+        int rc = lucid_cuda_render(ctx_, &p, px, nullptr);
         if (rc != LUCID_ERR_NO_SCENE) { last_tile_w_ = tw; last_tile_h_ = th; }
         if (rc == LUCID_ERR_NO_SCENE) {
             // the reference returns a zero buffer (pybind_renderer.hpp:200-203)
             std::fprintf(stderr, "[lucidrenderer] Scene or camera not set\n");
-            return px;
+            return;
         }
-        if (rc == LUCID_ERR_CANCELLED) return px;   // partial result, is_cancelled() stays true
+        if (rc == LUCID_ERR_CANCELLED) return;   // partial result, is_cancelled() stays true
         if (rc != LUCID_OK) throw std::runtime_error(std::string("render failed: ") + lucid_cuda_last_error(ctx_));
+    }
+    std::vector<float> render(int tx, int ty, int tw, int th, int fw, int fh, int samples, int offset, int depth) {
+        if (tw <= 0 || th <= 0) throw std::invalid_argument("tile size must be positive");
+        std::vector<float> px((size_t)tw * th * 4, 0.0f);
+        render_into(px.data(), tx, ty, tw, th, fw, fh, samples, offset, depth);
         return px;
     }
     std::vector<float> render_debug(int tx, int ty, int tw, int th, int fw, int fh, const std::string& mode) {
@@ -457,18 +463,34 @@ PYBIND11_MODULE(lucidrenderer, m) {
              py::arg("tile_y"), py::arg("tile_w"), py::arg("tile_h"), py::arg("full_w"), py::arg("full_h"),
              py::arg("samples") = 1, py::arg("sample_offset") = 0, py::arg("max_depth") = 8)
         .def("render_tile_numpy",
-             [](Renderer& self, int tx, int ty, int tw, int th, int fw, int fh, int samples, int offset, int depth) {
-                 std::vector<float> px;
+             [](Renderer& self, int tx, int ty, int tw, int th, int fw, int fh, int samples, int offset, int depth,
+                py::object out) {
+                 // the engine's film copy lands directly in the returned array
+                 if (tw <= 0 || th <= 0) throw std::invalid_argument("tile size must be positive");
+                 py::array_t<float, py::array::c_style> arr;
+                 if (out.is_none()) {
+                     arr = py::array_t<float, py::array::c_style>({th, tw, 4});
+                 } else {
+                     if (!py::isinstance<py::array_t<float>>(out))
+                         throw std::invalid_argument("out must be a float32 numpy array");
+                     arr = py::reinterpret_borrow<py::array_t<float, py::array::c_style>>(out);
+                     if (!(arr.flags() & py::array::c_style) || !arr.writeable() ||
+                         arr.size() != (py::ssize_t)tw * th * 4)
+                         throw std::invalid_argument("out must be a writable C-contiguous float32 array of "
+                                                     "tile_w * tile_h * 4 elements");
+                 }
+                 float* px = arr.mutable_data();
+                 std::memset(px, 0, (size_t)tw * th * 4 * sizeof(float));
                  {
                      py::gil_scoped_release release;
-                     px = self.render(tx, ty, tw, th, fw, fh, samples, offset, depth);
+                     self.render_into(px, tx, ty, tw, th, fw, fh, samples, offset, depth);
                  }
-                 py::array_t<float> arr({th, tw, 4});
-                 std::memcpy(arr.mutable_data(), px.data(), px.size() * sizeof(float));
                  return arr;
              },
              py::arg("tile_x"), py::arg("tile_y"), py::arg("tile_w"), py::arg("tile_h"), py::arg("full_w"),
-             py::arg("full_h"), py::arg("samples") = 1, py::arg("sample_offset") = 0, py::arg("max_depth") = 8)
+             py::arg("full_h"), py::arg("samples") = 1, py::arg("sample_offset") = 0, py::arg("max_depth") = 8,
+             py::arg("out") = py::none(),
+             "render_tile into a (tile_h, tile_w, 4) float32 array (or into `out`, reused between calls)")
         .def("render_debug", &Renderer::render_debug, py::call_guard<py::gil_scoped_release>(), py::arg("tile_x"),
              py::arg("tile_y"), py::arg("tile_w"), py::arg("tile_h"), py::arg("full_w"), py::arg("full_h"),
              py::arg("mode"))
