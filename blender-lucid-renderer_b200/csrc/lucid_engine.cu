@@ -2504,7 +2504,15 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
     if (guide) cap = std::min(cap, kGuideWave);
     int spw = (int)std::max<long long>(1, std::min<long long>(p.samples, cap / (long long)np));
     long long wave_paths = (long long)spw * (long long)np;
-    int rc = ensure_pool(wave_paths, records);
+    // A progressive caller (the add-on's F12 loop: 4, 8, 16, 32, then 64
+    // samples per call) grows the wave call by call; reserving 64 samples
+    // per pixel of the tile (within the cap) at the first multi-sample call
+    // keeps the later calls from reallocating the pool (50-60 ms each at
+    // 1920x1080).  Async dispatches (1 sample each) keep their small pool.
+    long long reserve = wave_paths;
+    if (!from_async && !records && p.samples > 1)
+        reserve = std::max(wave_paths, std::min(cap, 64LL * (long long)np));
+    int rc = ensure_pool(reserve, records);
     if (rc != LUCID_OK) return rc;
     PathPool& P = *pool_;
     if (P.film_n < np) {
