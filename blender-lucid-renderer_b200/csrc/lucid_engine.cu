@@ -2489,8 +2489,20 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
     if (p.tile_w <= 0 || p.tile_h <= 0 || p.full_w <= 0 || p.full_h <= 0)
         return fail(LUCID_ERR_INVALID, "tile and image sizes must be positive");
     size_t np = (size_t)p.tile_w * p.tile_h;
-    if (out_host) std::fill(out_host, out_host + np * 4, 0.0f);
-    if (out_f64) std::fill(out_f64, out_f64 + np * 4, 0.0);
+    // A call that returns before its image is copied out leaves a zero image
+    // (the reference's empty result); a finished copy is not written twice,
+    // which at 1920x1080 saves a 33 MB host fill per call.
+    struct ZeroUnlessCopied {
+        float* f;
+        double* d;
+        size_t n;
+        bool copied = false;
+        ~ZeroUnlessCopied() {
+            if (copied) return;
+            if (f) std::fill(f, f + n * 4, 0.0f);
+            if (d) std::fill(d, d + n * 4, 0.0);
+        }
+    } host_image{out_host, out_f64, np};
     if (!scene_loaded_ || !camera_set_) return fail(LUCID_ERR_NO_SCENE, "scene or camera not set");
     CK(cudaSetDevice(device_));
     if (p.samples <= 0) return fail(LUCID_ERR_INVALID, "samples must be >= 1");
@@ -2715,6 +2727,7 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
     if (records)
         CK(cudaMemcpyAsync(recs, d_recs.p, np * (size_t)p.samples * sizeof(LucidSampleRecord), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    host_image.copied = true;
     if (guide && guide_->net.failed(st) != 0) return fail(LUCID_ERR_TIMEOUT, guide_->net.error());
     float tot = 0.0f;
     cudaEventElapsedTime(&tot, t0, t1);

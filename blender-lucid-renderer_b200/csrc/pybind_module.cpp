@@ -175,7 +175,8 @@ public:
     bool is_camera_set() const { return camera_set_; }
     int get_mesh_count() const { return scene_loaded_ ? mesh_count_ : 0; }
 
-    // Renders into `px` (tw * th * 4 floats, zeroed by the caller); the
+    // Renders into `px` (tw * th * 4 floats; a zero image when the render
+    // fails before its copy, the library's own guarantee); the
     // return-code handling of pybind_renderer.hpp:185-361 (no scene: a zero
     // buffer and a message; cancelled: the partial sum).
     void render_into(float* px, int tx, int ty, int tw, int th, int fw, int fh, int samples, int offset, int depth) {
@@ -479,8 +480,7 @@ PYBIND11_MODULE(lucidrenderer, m) {
                          throw std::invalid_argument("out must be a writable C-contiguous float32 array of "
                                                      "tile_w * tile_h * 4 elements");
                  }
-                 float* px = arr.mutable_data();
-                 std::memset(px, 0, (size_t)tw * th * 4 * sizeof(float));
+                 float* px = arr.mutable_data();   // every return path of the render writes it
                  {
                      py::gil_scoped_release release;
                      self.render_into(px, tx, ty, tw, th, fw, fh, samples, offset, depth);

@@ -191,7 +191,9 @@ int lucid_scene_digest(const char* json, size_t len, const LucidSceneDesc* array
  * (pybind_renderer.hpp:185-361, 538-666).  out_rgba: host buffer of
  * tile_w*tile_h*4 floats: the SUM over the call's samples of each pixel's
  * radiance, camera sensitivity applied, clamped >= 0, alpha 1, rows
- * Y-flipped.  records (optional, may be NULL): tile_w*tile_h*samples entries
+ * Y-flipped; all zeros when the call fails before the image is copied out
+ * (no scene or camera, invalid samples / depth, device errors).
+ * records (optional, may be NULL): tile_w*tile_h*samples entries
  * in (row-major unflipped pixel, sample) order. */
 int lucid_cuda_render(LucidCudaCtx* ctx, const LucidRenderParams* params, float* out_rgba,
                       LucidSampleRecord* records);
