@@ -265,9 +265,63 @@ LD int refill(int* cursor, int n, bool need, bool& exhausted) {
     return r;
 }
 
+// ---------------------------------------------------------------- shading bins
+// The shading kernel is limited by instruction fetch: divergent warps run
+// different parts of it (light/environment hits, emitters, glass, near-delta
+// metal, general Principled lobes, volume delta tracking).  Before each
+// shading launch the queue is binned by that class — a counting sort whose
+// histogram the trace kernels build as each ray finishes (the hit, the
+// native-light hit and the ray are still in registers there) and whose
+// scatter pass is k_bin_scatter — so neighbouring warps shade the same kind
+// of event.  The order of paths in a queue does not change any result.
+LD int bin_class(const DevScene& sc, int prim, float t, int li, float lt, V3 o, V3 d, bool vol) {
+    int c = 0;   // light or environment reached
+    if (prim >= 0 && !(li >= 0 && lt < t)) {
+        const DevMaterial& dm = sc.materials[sc.prim_info[prim].x];
+        float rough = dm.rough_trans_ior_flags.x, trans = dm.rough_trans_ior_flags.y, metal = dm.albedo_metallic.w;
+        c = dm.emission.w != 0.0f ? 1 : trans > 0.5f ? 2 : (metal > 0.5f && rough < 0.05f) ? 3 : (metal > 0.5f ? 4 : 5);
+    }
+    if (vol && sc.num_volumes > 0) {
+        float ts = 1e6f;
+        if (prim >= 0) ts = smin(ts, t);
+        if (li >= 0) ts = smin(ts, lt);
+        for (int k = 0; k < sc.num_volumes && k < 4; ++k) {
+            float te, tx;
+            if (ray_aabb_segment(o, d, ts, sc.volumes[k], te, tx)) { c += 8; break; }
+        }
+    }
+    return c;
+}
+
+// Per-block class histogram of the rays a trace kernel finished
+// (bins < 0: no binning; else bins != 0 adds the volume bit), flushed to
+// the depth's class counters when the block ends.
+struct BinHist {
+    int* h;
+    LD void clear(int bins) {
+        if (bins >= 0 && threadIdx.x < kBins) h[threadIdx.x] = 0;
+        __syncthreads();
+    }
+    LD void add(const DevScene& sc, const PathView& pv, int id, int bins, int prim, float t, int li, float lt, V3 o,
+                V3 d) {
+        if (bins < 0) return;
+        int c = bin_class(sc, prim, t, li, lt, o, d, bins != 0);
+        pv.cls[id] = (unsigned char)c;
+        atomicAdd(&h[c], 1);
+    }
+    LD void flush(int bins, int* cnt) {
+        if (bins < 0) return;
+        __syncthreads();
+        if (threadIdx.x < kBins && h[threadIdx.x]) atomicAdd(&cnt[8 + threadIdx.x], h[threadIdx.x]);
+    }
+};
+
 // Closest hit of camera rays: neighbouring pixels trace similar paths, so a
 // warp claims 32 consecutive rays at a time and keeps them together.
-__global__ void __launch_bounds__(128) k_trace_primary(DevScene sc, PathView pv, int* cnt, int records) {
+__global__ void __launch_bounds__(128) k_trace_primary(DevScene sc, PathView pv, int* cnt, int records, int bins) {
+    __shared__ int hist[kBins];
+    BinHist bh{hist};
+    bh.clear(bins);
     const int n = *(volatile int*)&cnt[0];
     bool ok = true;
     for (;;) {
@@ -281,6 +335,7 @@ __global__ void __launch_bounds__(128) k_trace_primary(DevScene sc, PathView pv,
         if (h.prim < 0) { h.t = 1e30f; h.u = 0.0f; h.v = 0.0f; }
         pv.hit[id] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
         pv.lhit[id] = make_float2(__int_as_float(-1), 1e30f);   // native lights are invisible to camera rays
+        bh.add(sc, pv, id, bins, h.prim, h.t, -1, 1e30f, o, d);
         if (records) {
             int4 pi = h.prim >= 0 ? sc.prim_info[h.prim] : make_int4(-1, -1, -1, 0);
             pv.rec_prim[id] = make_int2(pi.x, pi.y);
@@ -292,6 +347,7 @@ __global__ void __launch_bounds__(128) k_trace_primary(DevScene sc, PathView pv,
             pv.rec_hash[id] = hs;
         }
     }
+    bh.flush(bins, cnt);
     if (!ok) atomicAdd(&pv.errors[0], 1);
 }
 
@@ -300,7 +356,11 @@ __global__ void __launch_bounds__(128) k_trace_primary(DevScene sc, PathView pv,
 // Nine resident CTAs per SM (at most 56 registers): one more warp group to
 // hide node-fetch latency than the unconstrained 61 registers allow
 // (1M-triangle scene: 8 CTAs 232 ms, 9 CTAs 221 ms, 10 CTAs 225 ms).
-__global__ void __launch_bounds__(128, 9) k_trace(DevScene sc, PathView pv, int* cnt, int identity, int records) {
+__global__ void __launch_bounds__(128, 9) k_trace(DevScene sc, PathView pv, int* cnt, int identity, int records,
+                                                 int bins) {
+    __shared__ int hist[kBins];
+    BinHist bh{hist};
+    bh.clear(bins);
     const int n = *(volatile int*)&cnt[0];
     const int* q = identity ? nullptr : pv.q0;
     int stack[kStack];
@@ -349,6 +409,7 @@ __global__ void __launch_bounds__(128, 9) k_trace(DevScene sc, PathView pv, int*
         int li = (depth == 0) ? -1 : native_lights_closest(sc, s.o, s.d, lt);
         pv.hit[id] = make_float4(res.t, res.u, res.v, __int_as_float(res.prim));
         pv.lhit[id] = make_float2(__int_as_float(li), lt);
+        bh.add(sc, pv, id, bins, res.prim, res.t, li, lt, s.o, s.d);
         if (records) {
             int4 pi = res.prim >= 0 ? sc.prim_info[res.prim] : make_int4(-1, -1, -1, 0);
             if (depth == 0) pv.rec_prim[id] = make_int2(pi.x, pi.y);
@@ -361,6 +422,7 @@ __global__ void __launch_bounds__(128, 9) k_trace(DevScene sc, PathView pv, int*
         }
         active = false;
     }
+    bh.flush(bins, cnt);
     if (!ok) atomicAdd(&pv.errors[0], 1);
 }
 
@@ -777,53 +839,9 @@ static ShadeKernel shade_kernel(int algo, bool guide = false) {
 }
 
 // ---------------------------------------------------------------- shading bins
-// The shading kernel is limited by instruction fetch: divergent warps run
-// different parts of it (light/environment hits, emitters, glass, near-delta
-// metal, general Principled lobes, volume delta tracking).  Before each
-// shading launch the queue is binned by that class (a counting sort: one
-// histogram pass, one scatter pass with one atomic per class per warp), so
-// neighbouring warps shade the same kind of event.  The order of paths in a
-// queue does not change any result.
-LD int shade_bin(const DevScene& sc, const PathView& pv, int id, bool vol) {
-    float4 hh = pv.hit[id];
-    int prim = __float_as_int(hh.w);
-    float2 lh = pv.lhit[id];
-    int li = __float_as_int(lh.x);
-    int c = 0;   // light or environment reached
-    if (prim >= 0 && !(li >= 0 && lh.y < hh.x)) {
-        const DevMaterial& dm = sc.materials[sc.prim_info[prim].x];
-        float rough = dm.rough_trans_ior_flags.x, trans = dm.rough_trans_ior_flags.y, metal = dm.albedo_metallic.w;
-        c = dm.emission.w != 0.0f ? 1 : trans > 0.5f ? 2 : (metal > 0.5f && rough < 0.05f) ? 3 : (metal > 0.5f ? 4 : 5);
-    }
-    if (vol && sc.num_volumes > 0) {
-        float ts = 1e6f;
-        if (prim >= 0) ts = smin(ts, hh.x);
-        if (li >= 0) ts = smin(ts, lh.y);
-        V3 o = f3(pv.ray_o[id]), d = f3(pv.ray_d[id]);
-        for (int k = 0; k < sc.num_volumes && k < 4; ++k) {
-            float te, tx;
-            if (ray_aabb_segment(o, d, ts, sc.volumes[k], te, tx)) { c += 8; break; }
-        }
-    }
-    return c;
-}
-
-__global__ void __launch_bounds__(256) k_bin_count(DevScene sc, PathView pv, int* cnt, int identity, const int* qin,
-                                                   int vol) {
-    __shared__ int h[kBins];
-    if (threadIdx.x < kBins) h[threadIdx.x] = 0;
-    __syncthreads();
-    const int n = *(volatile int*)&cnt[0];
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        int id = identity ? i : qin[i];
-        int c = shade_bin(sc, pv, id, vol != 0);
-        pv.cls[id] = (unsigned char)c;
-        atomicAdd(&h[c], 1);
-    }
-    __syncthreads();
-    if (threadIdx.x < kBins && h[threadIdx.x]) atomicAdd(&cnt[8 + threadIdx.x], h[threadIdx.x]);
-}
-
+// The scatter half of the counting sort whose histogram the trace kernels
+// build (bin_class): one atomic per class per warp, paths of a class kept
+// together so neighbouring warps shade the same kind of event.
 __global__ void __launch_bounds__(256) k_bin_scatter(PathView pv, int* cnt, int identity, const int* qin, int* qb) {
     __shared__ int base[kBins];
     if (threadIdx.x == 0) {
@@ -2227,7 +2245,8 @@ int Engine::ensure_pool(long long paths, bool records) {
 namespace {
 // Algorithmic bytes per unit of work (compulsory SoA traffic; BVH node and
 // triangle fetches are scene-dependent and excluded):
-//   trace : ray 32 + queue id 4 + hit 16 + light hit 8                  = 60 / ray
+//   trace : ray 32 + queue id 4 + hit 16 + light hit 8
+//           + the hit's prim info 16 and shading class 1 (binning)     = 77 / ray
 //   shade : queue 4 + hit 24 + ray 32 + throughput 16 + radiance 16 + rng 16
 //           + prim info/normal 32 + material 48  (reads)
 //           + rng 16 + radiance 16 + throughput 16 + ray 32 + queue 4
@@ -2235,10 +2254,9 @@ namespace {
 //   shadow: queue 4 + shadow record 48 + radiance 16 read + 16 write  = 84 / ray
 //   raygen: rng 16 + ray 32 + throughput 16 + radiance 16            = 80 / path
 //   film  : radiance 16 / path + film 32 / pixel
-//   bin   : queue id 2 x 4 + hit 16 + light hit 8 + class 1 w + 1 r
-//           + binned id 4                                            = 38 / path
-constexpr double kBytesTrace = 60, kBytesShade = 340, kBytesShadow = 84, kBytesRaygen = 80, kBytesFilm = 16,
-                 kBytesBin = 38;
+//   bin   : queue id 4 + class 1 + binned id 4 (scatter)             = 9 / path
+constexpr double kBytesTrace = 77, kBytesShade = 340, kBytesShadow = 84, kBytesRaygen = 80, kBytesFilm = 16,
+                 kBytesBin = 9;
 //   guide : queue 4 + hit 24 + ray 32 + raw outputs 160 w              = 220 / path
 //   train : one record 64 / record (weights are read from shared memory)
 enum Kind { K_RAYGEN, K_TRACE0, K_TRACE, K_SHADE, K_SHADOW, K_FILM, K_BIN, K_GUIDE, K_TRAIN, K_NUM };
@@ -2587,7 +2605,7 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
     }
     const char* sort_env = std::getenv("LUCID_SHADE_BINS");
     const bool bin = !(sort_env && sort_env[0] == '0');
-    const int vol_bins = (algo_ == ALGO_VOLUME_MIS || algo_ == ALGO_VOLUME_SIMPLE) ? 1 : 0;
+    const int bins = !bin ? -1 : (algo_ == ALGO_VOLUME_MIS || algo_ == ALGO_VOLUME_SIMPLE) ? 1 : 0;
 
     struct Launch { int kind; cudaEvent_t a, b; int depth; };
     std::vector<Launch> launches;
@@ -2637,10 +2655,10 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
             pv.q0 = qin;
             if (depth == 0) {
                 e = ev_begin(K_TRACE0, depth);
-                k_trace_primary<<<g_trace0, 128, 0, st>>>(ds_->view, pv, cnt, f.records);
+                k_trace_primary<<<g_trace0, 128, 0, st>>>(ds_->view, pv, cnt, f.records, bins);
             } else {
                 e = ev_begin(K_TRACE, depth);
-                k_trace<<<g_trace, 128, 0, st>>>(ds_->view, pv, cnt, 0, f.records);
+                k_trace<<<g_trace, 128, 0, st>>>(ds_->view, pv, cnt, 0, f.records, bins);
             }
             ev_end(e);
             if (guide && depth < guide_->max_depth) {
@@ -2652,7 +2670,6 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
             }
             if (bin) {
                 e = ev_begin(K_BIN, depth);
-                k_bin_count<<<g_bin, 256, 0, st>>>(ds_->view, pv, cnt, depth == 0, qin, vol_bins);
                 k_bin_scatter<<<g_bin, 256, 0, st>>>(pv, cnt, depth == 0, qin, P.qb.p);
                 ev_end(e);
             }
@@ -2847,7 +2864,7 @@ void Engine::enqueue_iteration(void* fp, int n) {
     f.samples = n;
     f.n_wave = n * f.npix;
     const ShadeKernel shade = shade_kernel(algo_);
-    const int vol_bins = (algo_ == ALGO_VOLUME_MIS || algo_ == ALGO_VOLUME_SIMPLE) ? 1 : 0;
+    const int bins = (algo_ == ALGO_VOLUME_MIS || algo_ == ALGO_VOLUME_SIMPLE) ? 1 : 0;
     cudaMemsetAsync(P.counters.p, 0, sizeof(int) * kCountersPerDepth * (J.depth + 1), st);
     k_raygen<<<(f.n_wave + 255) / 256, 256, 0, st>>>(f, P.view);
     for (int depth = 0; depth < J.depth; ++depth) {
@@ -2857,9 +2874,8 @@ void Engine::enqueue_iteration(void* fp, int n) {
         int* qin = (depth & 1) ? P.q1.p : P.q0.p;
         int* qout = (depth & 1) ? P.q0.p : P.q1.p;
         pv.q0 = qin;
-        if (depth == 0) k_trace_primary<<<J.g_trace0, 128, 0, st>>>(ds_->view, pv, cnt, 0);
-        else k_trace<<<J.g_trace, 128, 0, st>>>(ds_->view, pv, cnt, 0, 0);
-        k_bin_count<<<J.g_bin, 256, 0, st>>>(ds_->view, pv, cnt, depth == 0, qin, vol_bins);
+        if (depth == 0) k_trace_primary<<<J.g_trace0, 128, 0, st>>>(ds_->view, pv, cnt, 0, bins);
+        else k_trace<<<J.g_trace, 128, 0, st>>>(ds_->view, pv, cnt, 0, 0, bins);
         k_bin_scatter<<<J.g_bin, 256, 0, st>>>(pv, cnt, depth == 0, qin, P.qb.p);
         shade<<<J.g_shade, 128, 0, st>>>(ds_->view, f, pv, cnt, cnt_next, 0, P.qb.p, qout);
         k_shadow<<<J.g_shadow, 128, 0, st>>>(ds_->view, pv, cnt, 0);
@@ -3259,8 +3275,8 @@ int Engine::render_noalloc(const LucidRenderParams& p, float* d_out) {
             int* qin = (depth & 1) ? q1 : q0;
             int* qout = (depth & 1) ? q0 : q1;
             pv.q0 = qin;
-            if (depth == 0) k_trace_primary<<<g_trace0, 128, 0, st>>>(ds_->view, pv, cnt, 0);
-            else k_trace<<<g_trace, 128, 0, st>>>(ds_->view, pv, cnt, 0, 0);
+            if (depth == 0) k_trace_primary<<<g_trace0, 128, 0, st>>>(ds_->view, pv, cnt, 0, -1);
+            else k_trace<<<g_trace, 128, 0, st>>>(ds_->view, pv, cnt, 0, 0, -1);
             shade<<<g_shade, 128, 0, st>>>(ds_->view, f, pv, cnt, cnt_next, depth == 0, qin, qout);
             k_shadow<<<g_shadow, 128, 0, st>>>(ds_->view, pv, cnt, 0);
         }
