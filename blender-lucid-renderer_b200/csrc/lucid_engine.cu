@@ -63,6 +63,7 @@ struct DBuf {
 struct DeviceScene {
     DBuf<float4> bvh_tris, bnd_tris, big_tris, prim_fn, prim_vn;
     DBuf<int4> prim_info;
+    DBuf<unsigned char> prim_cls;
     DBuf<int> guide;
     DBuf<DevNode4> nodes;
     DBuf<DevNode> nodes2;
@@ -74,7 +75,7 @@ struct DeviceScene {
     DevScene view{};
     void release() {
         bvh_tris.release(); bnd_tris.release(); big_tris.release(); prim_fn.release(); prim_vn.release(); prim_info.release();
-        nodes.release(); nodes2.release(); guide.release(); materials.release(); tex_ops.release(); prim_uv.release(); lights.release(); cdf.release(); grid.release(); volumes.release();
+        prim_cls.release(); nodes.release(); nodes2.release(); guide.release(); materials.release(); tex_ops.release(); prim_uv.release(); lights.release(); cdf.release(); grid.release(); volumes.release();
     }
 };
 
@@ -275,12 +276,9 @@ LD int refill(int* cursor, int n, bool need, bool& exhausted) {
 // scatter pass is k_bin_scatter — so neighbouring warps shade the same kind
 // of event.  The order of paths in a queue does not change any result.
 LD int bin_class(const DevScene& sc, int prim, float t, int li, float lt, V3 o, V3 d, bool vol) {
-    int c = 0;   // light or environment reached
-    if (prim >= 0 && !(li >= 0 && lt < t)) {
-        const DevMaterial& dm = sc.materials[sc.prim_info[prim].x];
-        float rough = dm.rough_trans_ior_flags.x, trans = dm.rough_trans_ior_flags.y, metal = dm.albedo_metallic.w;
-        c = dm.emission.w != 0.0f ? 1 : trans > 0.5f ? 2 : (metal > 0.5f && rough < 0.05f) ? 3 : (metal > 0.5f ? 4 : 5);
-    }
+    // 0: light or environment reached; else the prim's material class
+    // (emitter, glass, near-delta metal, metal, dielectric), set at upload
+    int c = (prim >= 0 && !(li >= 0 && lt < t)) ? (int)__ldg(sc.prim_cls + prim) : 0;
     if (vol && sc.num_volumes > 0) {
         float ts = 1e6f;
         if (prim >= 0) ts = smin(ts, t);
@@ -1819,8 +1817,17 @@ int Engine::upload_scene(HostScene&& hs) {
         if (vec.empty()) return cudaSuccess;
         return cudaMemcpyAsync(buf.p, vec.data(), vec.size() * sizeof(vec[0]), cudaMemcpyHostToDevice, S(stream_));
     };
+    // each prim's shading class for a surface hit (the material part of
+    // bin_class, decided once here instead of per hit)
+    std::vector<unsigned char> cls(H.prim_info.size());
+    for (size_t p = 0; p < cls.size(); ++p) {
+        const DevMaterial& dm = H.materials[H.prim_info[p].x];
+        const float rough = dm.rough_trans_ior_flags.x, trans = dm.rough_trans_ior_flags.y, metal = dm.albedo_metallic.w;
+        cls[p] = dm.emission.w != 0.0f ? 1 : trans > 0.5f ? 2 : (metal > 0.5f && rough < 0.05f) ? 3 : (metal > 0.5f ? 4 : 5);
+    }
     CK(up(D.bnd_tris, bnd));
     CK(up(D.prim_info, H.prim_info));
+    CK(up(D.prim_cls, cls));
     CK(up(D.prim_fn, H.prim_fn));
     CK(up(D.prim_vn, H.prim_vn));
     CK(up(D.materials, H.materials));
@@ -1836,6 +1843,7 @@ int Engine::upload_scene(HostScene&& hs) {
     v.bnd_tris = D.bnd_tris.p;
     v.num_bnd_tris = (int)(bnd.size() / 3);
     v.prim_info = D.prim_info.p;
+    v.prim_cls = D.prim_cls.p;
     v.prim_fn = D.prim_fn.p;
     v.prim_vn = D.prim_vn.p;
     v.materials = D.materials.p;
@@ -2246,7 +2254,7 @@ namespace {
 // Algorithmic bytes per unit of work (compulsory SoA traffic; BVH node and
 // triangle fetches are scene-dependent and excluded):
 //   trace : ray 32 + queue id 4 + hit 16 + light hit 8
-//           + the hit's prim info 16 and shading class 1 (binning)     = 77 / ray
+//           + the hit prim's class 1 and the shading class 1 (binning) = 62 / ray
 //   shade : queue 4 + hit 24 + ray 32 + throughput 16 + radiance 16 + rng 16
 //           + prim info/normal 32 + material 48  (reads)
 //           + rng 16 + radiance 16 + throughput 16 + ray 32 + queue 4
@@ -2255,7 +2263,7 @@ namespace {
 //   raygen: rng 16 + ray 32 + throughput 16 + radiance 16            = 80 / path
 //   film  : radiance 16 / path + film 32 / pixel
 //   bin   : queue id 4 + class 1 + binned id 4 (scatter)             = 9 / path
-constexpr double kBytesTrace = 77, kBytesShade = 340, kBytesShadow = 84, kBytesRaygen = 80, kBytesFilm = 16,
+constexpr double kBytesTrace = 62, kBytesShade = 340, kBytesShadow = 84, kBytesRaygen = 80, kBytesFilm = 16,
                  kBytesBin = 9;
 //   guide : queue 4 + hit 24 + ray 32 + raw outputs 160 w              = 220 / path
 //   train : one record 64 / record (weights are read from shared memory)

@@ -90,6 +90,7 @@ struct DevScene {
     int num_big_tris;
     // per global prim (mesh-major order)
     const int4* prim_info;          // mesh, local tri, light index (-1), smooth flag
+    const unsigned char* prim_cls;  // shading class of a surface hit on the prim (1..5)
     const float4* prim_fn;          // face normal
     const float4* prim_vn;          // 3 vertex normals per prim (smooth prims)
     const DevMaterial* materials;   // per mesh
