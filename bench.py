@@ -10,8 +10,9 @@ reference's `volume_mis` integrator.  Synthetic data: no public dataset.
 
 value   : samples/s over the whole job, device-timed (CUDA events on the
           renderer's stream) with the image left in device memory.
-e2e     : samples/s through the C ABI call lucid_cuda_render with a host
-          output buffer (device->host copy of the image inside the timing).
+e2e     : samples/s through the C ABI call lucid_cuda_render with a pinned
+          host output buffer (device->host copy of the image inside the
+          timing).
 roofline: the dominant kernel's algorithmic bytes / its measured time,
           against the measured HBM copy bandwidth.
 cpu_baseline: the CPU oracle (a restatement of the reference CPU path) on a
@@ -454,8 +455,8 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
 
-    # e2e: the reference-facing C ABI call with a host output buffer
-    host = np.zeros((H, W, 4), np.float32)
+    # e2e: the reference-facing C ABI call with a (pinned) host output buffer
+    host = torch.zeros((H, W, 4), dtype=torch.float32, pin_memory=True).numpy()
     if dist:
         dist.barrier()
     e2e_ms = []
