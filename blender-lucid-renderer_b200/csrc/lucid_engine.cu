@@ -212,12 +212,11 @@ LD V3 primary_dir(const FrameParams& f, float nx, float ny) {
     return make_dir_or(v, v3(f.fwd[0], f.fwd[1], f.fwd[2]));
 }
 
-// Primary rays (pybind_renderer.hpp:250-293): NDC, seed (x, y, offset + s),
-// two jitter draws when the call has more than one sample.
-__global__ void k_raygen(FrameParams f, PathView pv) {
-    int id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (id == 0) pv.counters[0] = f.n_wave;
-    if (id >= f.n_wave) return;
+// Primary ray of wave path `id` (pybind_renderer.hpp:250-293): NDC, seed
+// (x, y, offset + s), two jitter draws when the call has more than one
+// sample; writes the path's initial state and returns the direction (the
+// origin is the camera position, tMin 0).
+LD V3 camera_ray(const FrameParams& f, const PathView& pv, int id) {
     int p = id % f.npix, sl = id / f.npix;
     int gx = f.tile_x + p % f.tile_w, gy = f.tile_y + p / f.tile_w;
     float nx = (2.0f * ((float)gx + 0.5f) / (float)f.full_w - 1.0f) * f.aspect;
@@ -242,6 +241,15 @@ __global__ void k_raygen(FrameParams f, PathView pv) {
         pv.rec_cnt[id] = make_int4(0, 0, 0, 0);
         pv.rec_hash[id] = 1469598103934665603ULL;
     }
+    return d;
+}
+
+// Primary rays alone, for the passes that do not trace them at once.
+__global__ void k_raygen(FrameParams f, PathView pv) {
+    int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id == 0) pv.counters[0] = f.n_wave;
+    if (id >= f.n_wave) return;
+    camera_ray(f, pv, id);
 }
 
 // ---------------------------------------------------------------- trace
@@ -314,22 +322,26 @@ struct BinHist {
     }
 };
 
-// Closest hit of camera rays: neighbouring pixels trace similar paths, so a
-// warp claims 32 consecutive rays at a time and keeps them together.
-__global__ void __launch_bounds__(128) k_trace_primary(DevScene sc, PathView pv, int* cnt, int records, int bins) {
+// Camera rays, generated and traced in one pass: neighbouring pixels trace
+// similar paths, so a warp claims 32 consecutive rays at a time and keeps
+// them together.  Also publishes the wave's path count as the depth-0 queue
+// length for the kernels after it.
+__global__ void __launch_bounds__(128) k_trace_primary(DevScene sc, FrameParams f, PathView pv, int* cnt,
+                                                       int records, int bins) {
     __shared__ int hist[kBins];
     BinHist bh{hist};
     bh.clear(bins);
-    const int n = *(volatile int*)&cnt[0];
+    const int n = f.n_wave;
+    if (blockIdx.x == 0 && threadIdx.x == 0) cnt[0] = n;
+    const V3 o = v3(f.pos[0], f.pos[1], f.pos[2]);
     bool ok = true;
     for (;;) {
         int base = warp_fetch(&cnt[2]);
         if (base >= n) break;
         int id = base + (int)lane_id();
         if (id >= n) continue;
-        float4 ro = pv.ray_o[id], rd = pv.ray_d[id];
-        V3 o = f3(ro), d = f3(rd);
-        HitRec h = closest_skip_boundaries(sc, o, d, ro.w, ok);
+        const V3 d = camera_ray(f, pv, id);
+        HitRec h = closest_skip_boundaries(sc, o, d, 0.0f, ok);
         if (h.prim < 0) { h.t = 1e30f; h.u = 0.0f; h.v = 0.0f; }
         pv.hit[id] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
         pv.lhit[id] = make_float2(__int_as_float(-1), 1e30f);   // native lights are invisible to camera rays
@@ -2261,16 +2273,18 @@ namespace {
 //           + shadow record 48 + shadow queue 4  (writes)           = 340 / path
 //   shadow: queue 4 + shadow record 48 + radiance 16 read + 16 write  = 84 / ray
 //   raygen: rng 16 + ray 32 + throughput 16 + radiance 16            = 80 / path
+//   camera trace (generates its rays): the raygen writes 80 + hit 16
+//           + light hit 8 + prim class 1 + shading class 1             = 106 / ray
 //   film  : radiance 16 / path + film 32 / pixel
 //   bin   : queue id 4 + class 1 + binned id 4 (scatter)             = 9 / path
-constexpr double kBytesTrace = 62, kBytesShade = 340, kBytesShadow = 84, kBytesRaygen = 80, kBytesFilm = 16,
+constexpr double kBytesTrace0 = 106, kBytesTrace = 62, kBytesShade = 340, kBytesShadow = 84, kBytesRaygen = 80, kBytesFilm = 16,
                  kBytesBin = 9;
 //   guide : queue 4 + hit 24 + ray 32 + raw outputs 160 w              = 220 / path
 //   train : one record 64 / record (weights are read from shared memory)
 enum Kind { K_RAYGEN, K_TRACE0, K_TRACE, K_SHADE, K_SHADOW, K_FILM, K_BIN, K_GUIDE, K_TRAIN, K_NUM };
 const char* kKindNames[K_NUM] = {"k_raygen", "k_trace_primary", "k_trace", "k_shade", "k_shadow", "k_film", "k_bin",
                                  "k_guide_infer", "k_guide_train"};
-const double kKindBytes[K_NUM] = {kBytesRaygen, kBytesTrace, kBytesTrace, kBytesShade, kBytesShadow, kBytesFilm,
+const double kKindBytes[K_NUM] = {kBytesRaygen, kBytesTrace0, kBytesTrace, kBytesShade, kBytesShadow, kBytesFilm,
                                   kBytesBin, 220, 64};
 static_assert(K_NUM <= LUCID_MAX_KERNEL_KINDS, "kernel kinds");
 }  // namespace
@@ -2650,9 +2664,7 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
             CK(cudaMemsetAsync(G.gslot.p, 0xff, (size_t)f.n_wave * sizeof(int4), st));
             CK(cudaMemsetAsync(G.count.p, 0, 2 * sizeof(int), st));
         }
-        int e = ev_begin(K_RAYGEN, 0);
-        k_raygen<<<(f.n_wave + 255) / 256, 256, 0, st>>>(f, P.view);
-        ev_end(e);
+        int e = 0;
         for (int depth = 0; depth < p.max_depth; ++depth) {
             int* cnt = P.counters.p + kCountersPerDepth * depth;
             int* cnt_next = P.counters.p + kCountersPerDepth * (depth + 1);
@@ -2663,7 +2675,7 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
             pv.q0 = qin;
             if (depth == 0) {
                 e = ev_begin(K_TRACE0, depth);
-                k_trace_primary<<<g_trace0, 128, 0, st>>>(ds_->view, pv, cnt, f.records, bins);
+                k_trace_primary<<<g_trace0, 128, 0, st>>>(ds_->view, f, pv, cnt, f.records, bins);
             } else {
                 e = ev_begin(K_TRACE, depth);
                 k_trace<<<g_trace, 128, 0, st>>>(ds_->view, pv, cnt, 0, f.records, bins);
@@ -2722,7 +2734,6 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
             shadows += hcnt[kCountersPerDepth * d + 1];
         }
         if (profile) {
-            kind_units[K_RAYGEN] += f.n_wave;
             kind_units[K_FILM] += f.n_wave;
             for (int d = 0; d < p.max_depth; ++d) {
                 kind_units[d == 0 ? K_TRACE0 : K_TRACE] += hcnt[kCountersPerDepth * d];
@@ -2874,7 +2885,6 @@ void Engine::enqueue_iteration(void* fp, int n) {
     const ShadeKernel shade = shade_kernel(algo_);
     const int bins = (algo_ == ALGO_VOLUME_MIS || algo_ == ALGO_VOLUME_SIMPLE) ? 1 : 0;
     cudaMemsetAsync(P.counters.p, 0, sizeof(int) * kCountersPerDepth * (J.depth + 1), st);
-    k_raygen<<<(f.n_wave + 255) / 256, 256, 0, st>>>(f, P.view);
     for (int depth = 0; depth < J.depth; ++depth) {
         int* cnt = P.counters.p + kCountersPerDepth * depth;
         int* cnt_next = P.counters.p + kCountersPerDepth * (depth + 1);
@@ -2882,7 +2892,7 @@ void Engine::enqueue_iteration(void* fp, int n) {
         int* qin = (depth & 1) ? P.q1.p : P.q0.p;
         int* qout = (depth & 1) ? P.q0.p : P.q1.p;
         pv.q0 = qin;
-        if (depth == 0) k_trace_primary<<<J.g_trace0, 128, 0, st>>>(ds_->view, pv, cnt, 0, bins);
+        if (depth == 0) k_trace_primary<<<J.g_trace0, 128, 0, st>>>(ds_->view, f, pv, cnt, 0, bins);
         else k_trace<<<J.g_trace, 128, 0, st>>>(ds_->view, pv, cnt, 0, 0, bins);
         k_bin_scatter<<<J.g_bin, 256, 0, st>>>(pv, cnt, depth == 0, qin, P.qb.p);
         shade<<<J.g_shade, 128, 0, st>>>(ds_->view, f, pv, cnt, cnt_next, 0, P.qb.p, qout);
@@ -3275,7 +3285,6 @@ int Engine::render_noalloc(const LucidRenderParams& p, float* d_out) {
         f.s0 = s0;
         f.n_wave = (int)(this_spw * np);
         CK(cudaMemsetAsync(v.counters, 0, sizeof(int) * kCountersPerDepth * (p.max_depth + 1), st));
-        k_raygen<<<(f.n_wave + 255) / 256, 256, 0, st>>>(f, v);
         for (int depth = 0; depth < p.max_depth; ++depth) {
             int* cnt = v.counters + kCountersPerDepth * depth;
             int* cnt_next = v.counters + kCountersPerDepth * (depth + 1);
@@ -3283,7 +3292,7 @@ int Engine::render_noalloc(const LucidRenderParams& p, float* d_out) {
             int* qin = (depth & 1) ? q1 : q0;
             int* qout = (depth & 1) ? q0 : q1;
             pv.q0 = qin;
-            if (depth == 0) k_trace_primary<<<g_trace0, 128, 0, st>>>(ds_->view, pv, cnt, 0, -1);
+            if (depth == 0) k_trace_primary<<<g_trace0, 128, 0, st>>>(ds_->view, f, pv, cnt, 0, -1);
             else k_trace<<<g_trace, 128, 0, st>>>(ds_->view, pv, cnt, 0, 0, -1);
             shade<<<g_shade, 128, 0, st>>>(ds_->view, f, pv, cnt, cnt_next, depth == 0, qin, qout);
             k_shadow<<<g_shadow, 128, 0, st>>>(ds_->view, pv, cnt, 0);
