@@ -2552,7 +2552,17 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
     const bool profile = (p.flags & LUCID_RENDER_PROFILE) != 0;
     const bool records = recs != nullptr;
     const bool guide = guide_ && guide_->on && algo_ == ALGO_MIS && !from_async;
-    long long cap = wave_cap_ > 0 ? wave_cap_ : default_wave_paths(records);
+    // The wave cap needs a device memory query (a driver call that other
+    // processes' driver traffic can hold up for tens of milliseconds); a
+    // call that fits the path pool it already has skips it.
+    const PathPool& P0 = *pool_;
+    long long cap;
+    if (wave_cap_ > 0)
+        cap = wave_cap_;
+    else if (P0.cap >= (long long)p.samples * (long long)np && (!records || P0.records))
+        cap = P0.cap;
+    else
+        cap = default_wave_paths(records);
     if (guide) cap = std::min(cap, kGuideWave);
     int spw = (int)std::max<long long>(1, std::min<long long>(p.samples, cap / (long long)np));
     long long wave_paths = (long long)spw * (long long)np;
