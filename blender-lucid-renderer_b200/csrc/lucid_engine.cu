@@ -3219,6 +3219,9 @@ namespace {
 // address).
 std::mutex g_noalloc_mu;
 unsigned char* g_noalloc_addr[64] = {};
+// Grid sizes (blocks) of the four wave kernels per device and integrator,
+// from the occupancy queries made on that device's first call.
+int g_noalloc_grid[64][5][4] = {};
 }  // namespace
 
 int Engine::render_noalloc(const LucidRenderParams& p, float* d_out) {
@@ -3236,8 +3239,20 @@ int Engine::render_noalloc(const LucidRenderParams& p, float* d_out) {
         return fail(LUCID_ERR_INVALID, "render_noalloc: max_depth must be in [1, " + std::to_string(kNoAllocMaxDepth) + "]");
     if (p.samples <= 0) return fail(LUCID_ERR_INVALID, "samples must be >= 1");
     if (device_ < 0 || device_ >= 64) return fail(LUCID_ERR_INVALID, "device index out of range");
+    if (algo_ < 0 || algo_ > 4) return fail(LUCID_ERR_INVALID, "unknown integrator");
+    // Diagnostics and path guiding keep per-render buffers that this entry
+    // point cannot allocate; rendering without them would give a different
+    // image than lucid_cuda_render_device, so refuse instead.
+    if (diag_enabled_)
+        return fail(LUCID_ERR_INVALID, "render_noalloc: path diagnostics are enabled; they need allocated record "
+                                       "buffers (disable them or use lucid_cuda_render_device)");
+    if (guide_ && guide_->on && algo_ == ALGO_MIS)
+        return fail(LUCID_ERR_INVALID, "render_noalloc: path guiding is on; it needs allocated training and "
+                                       "inference buffers (turn it off or use lucid_cuda_render_device)");
     CK(cudaSetDevice(device_));
+    const ShadeKernel shade = shade_kernel(algo_);
     unsigned char* base;
+    int grid[4];
     {
         std::lock_guard<std::mutex> lk(g_noalloc_mu);
         if (!g_noalloc_addr[device_]) {
@@ -3248,6 +3263,16 @@ int Engine::render_noalloc(const LucidRenderParams& p, float* d_out) {
             g_noalloc_addr[device_] = (unsigned char*)ptr;
         }
         base = g_noalloc_addr[device_];
+        int* g = g_noalloc_grid[device_][algo_];
+        if (g[0] == 0) {
+            int occ[4] = {1, 1, 1, 1};
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], k_trace_primary, 128, 0);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], k_trace, 128, 0);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], shade, 128, 0);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[3], k_shadow, 128, 0);
+            for (int k = 0; k < 4; ++k) g[k] = num_sms_ * std::max(1, occ[k]);
+        }
+        for (int k = 0; k < 4; ++k) grid[k] = g[k];
     }
     PathView v{};
     size_t off = 0;
@@ -3279,14 +3304,7 @@ int Engine::render_noalloc(const LucidRenderParams& p, float* d_out) {
     f.samples = p.samples; f.sample_offset = p.sample_offset; f.max_depth = p.max_depth; f.algo = algo_;
     f.npix = (int)np;
     f.records = 0;
-    int occ_t = 1, occ_s = 1, occ_h = 1, occ_t0 = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t0, k_trace_primary, 128, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t, k_trace, 128, 0);
-    const ShadeKernel shade = shade_kernel(algo_);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, shade, 128, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, k_shadow, 128, 0);
-    const int g_trace0 = num_sms_ * std::max(1, occ_t0), g_trace = num_sms_ * std::max(1, occ_t);
-    const int g_shade = num_sms_ * std::max(1, occ_s), g_shadow = num_sms_ * std::max(1, occ_h);
+    const int g_trace0 = grid[0], g_trace = grid[1], g_shade = grid[2], g_shadow = grid[3];
     const int spw = (int)std::max<long long>(1, std::min<long long>(p.samples, kNoAllocPaths / np));
     int status = LUCID_OK;
     for (int s0 = 0; s0 < p.samples; s0 += spw) {
@@ -3309,7 +3327,7 @@ int Engine::render_noalloc(const LucidRenderParams& p, float* d_out) {
         }
         k_film<<<(f.npix + 255) / 256, 256, 0, st>>>(f.npix, this_spw, v.rad, film);
         CK(cudaGetLastError());
-        CK(cudaStreamSynchronize(st));
+        // no wait here: stream order keeps the next wave behind this film sum
     }
     k_output<<<(f.npix + 255) / 256, 256, 0, st>>>(p.tile_w, p.tile_h, film, (float4*)d_out);
     int herr[4] = {0, 0, 0, 0};

@@ -12,7 +12,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.environ.get("LUCID_CUDA_LIB") or os.path.join(HERE, "liblucid_cuda.so")
+LIB_PATH = os.path.join(HERE, "liblucid_cuda.so")
 
 LUCID_OK = 0
 LUCID_ERR_NO_SCENE = -1

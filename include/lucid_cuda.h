@@ -209,7 +209,9 @@ int lucid_cuda_render_device(LucidCudaCtx* ctx, const LucidRenderParams* params,
  * floats), but all working memory sits in one fixed static device array of
  * about 12 MB that every GPU loading this library holds until exit.
  * Limits: tile_w*tile_h <= 65536 pixels, 1 <= max_depth <= 64, no sample
- * records; larger requests return LUCID_ERR_INVALID.  The first call on a
+ * records; larger requests return LUCID_ERR_INVALID.  Path diagnostics and
+ * path guiding keep buffers of their own: while either is on for the
+ * context, the call returns LUCID_ERR_INVALID.  The first call on a
  * device looks up the array's device address (cudaGetSymbolAddress) with
  * that device current; make that first call before any stream capture.
  * Every call on a device shares the array: calls that overlap on the GPU
