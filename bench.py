@@ -15,8 +15,10 @@ e2e     : samples/s through the C ABI call lucid_cuda_render with a pinned
           timing).
 roofline: the dominant kernel's algorithmic bytes / its measured time,
           against the measured HBM copy bandwidth.
-cpu_baseline: the CPU oracle (a restatement of the reference CPU path) on a
-          stratified 2% pixel crop at full spp, all host cores.
+cpu_baseline: the reference's own CPU render path (built from its sources
+          with its module's flags, oracle/_ref) on a stratified 2% pixel
+          crop at full spp, all host cores; the oracle restatement where
+          that build is missing.
 Multi-GPU (torchrun): each rank renders the frame with its own sample range
 (sample_offset = rank * 64); no collective on the data path ("weak").
 """
@@ -133,15 +135,36 @@ class ClockSampler:
 
 
 def cpu_baseline(js: str, cam, steps: int = 1):
-    """Oracle (CPU restatement of the reference path) on the stratified crop."""
+    """The reference's own CPU render path on the stratified crop: its
+    PyRenderer::render_tile built from the reference sources with the
+    reference module's flags (oracle/_ref, `make -C oracle ref`), one
+    render_tile call per tile on all host cores (OpenMP), as the add-on calls
+    it.  Where that build is missing, the oracle restatement run the same way
+    (libm, literal traversal order) stands in (kind "port")."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
-    from oracle_ctypes import Oracle
-    o = Oracle(device_math=False, canonical_ties=False)   # libm + literal traversal order, as the reference
-    assert o.load_scene_json(js)
-    o.set_camera(*cam)
-    o.set_algorithm(ALGO)
+    import ref_ctypes
+    path = ref_ctypes.bench_library_path()
+    if path:
+        r = ref_ctypes.ReferenceRenderer(path)
+        kind, threads = "reference", r.threads()
+        build = (f"reference PyRenderer::render_tile ({os.path.basename(path)}: -O3 "
+                 f"{'-march=native' if path.endswith('libref_bench.so') else '-march=x86-64-v3'} "
+                 f"-ffast-math -flto -fopenmp, the flags of CMakeLists.txt:90)")
+
+        def render(tx, ty, tw, th):
+            r.render(tw, th, W, H, SPP, 0, DEPTH, tile_x=tx, tile_y=ty)
+    else:
+        from oracle_ctypes import Oracle
+        r = Oracle(device_math=False, canonical_ties=False)   # libm + literal traversal order, as the reference
+        kind, threads = "port", os.cpu_count() or 1
+        build = "oracle restatement (-O2, no fast math), libm and literal traversal order"
+
+        def render(tx, ty, tw, th):
+            r.render(tw, th, W, H, SPP, 0, DEPTH, tile_x=tx, tile_y=ty, threads=threads)
+    assert r.load_scene_json(js)
+    r.set_camera(*cam)
+    r.set_algorithm(ALGO)
     nx, ny, tw, th = CPU_TILES
-    threads = os.cpu_count() or 1
     vals = []
     for _ in range(steps):
         t0 = time.perf_counter()
@@ -149,12 +172,12 @@ def cpu_baseline(js: str, cam, steps: int = 1):
             for i in range(nx):
                 tx = (i * W) // nx + (W // nx - tw) // 2
                 ty = (j * H) // ny + (H // ny - th) // 2
-                o.render(tw, th, W, H, SPP, 0, DEPTH, tile_x=tx, tile_y=ty, threads=threads)
+                render(tx, ty, tw, th)
         dt = time.perf_counter() - t0
         vals.append(nx * ny * tw * th * SPP / dt)
     sample = f"{nx * ny} stratified tiles of {tw}x{th} px ({nx * ny * tw * th} px, " \
-             f"{100.0 * nx * ny * tw * th / (W * H):.2f}% of the frame) at {SPP} spp, depth {DEPTH}, {ALGO}"
-    return vals, threads, sample
+             f"{100.0 * nx * ny * tw * th / (W * H):.2f}% of the frame) at {SPP} spp, depth {DEPTH}, {ALGO}; {build}"
+    return vals, threads, sample, kind
 
 
 def scene_upload(device: int, js: str, cache_dir: str) -> dict:
@@ -351,7 +374,7 @@ def run_reference(args, rank: int):
         return 0
     js, cam = scene_json(args.cache)
     cpu_baseline(js, cam, steps=max(0, min(args.warmup, 1)))   # warm caches (bounded)
-    vals, threads, sample = cpu_baseline(js, cam, steps=args.steps)
+    vals, threads, sample, kind = cpu_baseline(js, cam, steps=args.steps)
     v = float(np.mean(vals))
     line = {"impl": "reference", "metric": "samples/s", "value": v, "unit": "samples/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * (42240 * SPP) / v,
@@ -359,7 +382,7 @@ def run_reference(args, rank: int):
             "data": "synthetic (seeded procedural scene)",
             "config": {"workload": WORKLOAD, "triangles": 1026574, "width": W, "height": H, "spp": SPP,
                        "max_depth": DEPTH, "integrator": ALGO, "cpu_sample": sample},
-            "cpu_baseline": {"value": v, "unit": "samples/s", "cores": threads, "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": v, "unit": "samples/s", "cores": threads, "kind": kind, "sample": sample},
             "e2e": {"value": v, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -494,8 +517,8 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        vals, threads, sample = cpu_baseline(js, cam, steps=1)
-        cpu = {"value": float(vals[0]), "unit": "samples/s", "cores": threads, "kind": "port", "sample": sample}
+        vals, threads, sample, kind = cpu_baseline(js, cam, steps=1)
+        cpu = {"value": float(vals[0]), "unit": "samples/s", "cores": threads, "kind": kind, "sample": sample}
 
     if rank == 0:
         line = {

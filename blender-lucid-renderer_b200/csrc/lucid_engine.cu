@@ -1353,7 +1353,9 @@ __global__ void k_debug(DevScene sc, FrameParams f, int mode, float4* out, int* 
     bool ok = true;
     HitRec h = scene_closest(sc, v3(f.pos[0], f.pos[1], f.pos[2]), d, 0.0f, 1e30f, ok);
     if (!ok) atomicAdd(&errors[0], 1);
-    float4 c = make_float4(0.f, 0.f, 0.f, 1.f);
+    // a miss is black, except in the normal pass, which maps its colour to
+    // 0..1 after the lookup (pybind_renderer.hpp:412-415): grey
+    float4 c = mode == 0 ? make_float4(0.5f, 0.5f, 0.5f, 1.f) : make_float4(0.f, 0.f, 0.f, 1.f);
     if (h.prim >= 0) {
         int4 pi = sc.prim_info[h.prim];
         V3 fn = f3(sc.prim_fn[h.prim]);

@@ -258,6 +258,8 @@ void orc_set_options(int device_math, int canonical_ties) {
     opts().canonical_ties = canonical_ties != 0;
 }
 
+void orc_set_draw_order(int right_to_left) { opts().draw_rtl = right_to_left != 0; }
+
 int orc_load_scene_json(void* h, const char* js) {
     Renderer* r = static_cast<Renderer*>(h);
     try {

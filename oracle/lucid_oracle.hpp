@@ -38,6 +38,11 @@ namespace orc {
 struct Options {
     bool device_math = true;      // lucid_math.h instead of libm
     bool canonical_ties = true;   // see header comment
+    // Draws passed together as call arguments (sampleBSDF's three, sampleLight's
+    // and hg_sample's two: path_tracer.hpp:533,503,683) taken right to left, the
+    // order g++ gives the reference when it is built here; false = left to
+    // right, the reference's own toolchain and the product.
+    bool draw_rtl = false;
 };
 inline Options& opts() { static Options o; return o; }
 
@@ -175,6 +180,15 @@ inline uint32_t pcg32(Rng& s) {
     return (xs >> rot) | (xs << ((-rot) & 31));
 }
 inline float randf(Rng& s) { return std::ldexp((float)(pcg32(s) >> 9), -23); }
+// Two / three draws that the reference passes as arguments of one call.
+inline void draw2(Rng& s, float& u1, float& u2) {
+    if (opts().draw_rtl) { u2 = randf(s); u1 = randf(s); }
+    else { u1 = randf(s); u2 = randf(s); }
+}
+inline void draw3(Rng& s, float& u1, float& u2, float& u3) {
+    if (opts().draw_rtl) { u3 = randf(s); u2 = randf(s); u1 = randf(s); }
+    else { u1 = randf(s); u2 = randf(s); u3 = randf(s); }
+}
 
 // ------------------------------------------------------------------ scene
 // core/material.hpp, core/scene.hpp, light/light.hpp
@@ -1217,7 +1231,7 @@ inline RGB trace(const Scene& s, const SceneLights& sl, const Ray& ray, int max_
                     float lsp;
                     int li = select_light(sl, usel, lsp);
                     if (li >= 0 && lsp > 1e-6f) {
-                        float u1 = randf(rng), u2 = randf(rng);
+                        float u1, u2; draw2(rng, u1, u2);
                         LightSample ls = sample_light(sl.lights[li], x, u1, u2);
                         if (ls.pdf > MIN_PDF) {
                             Ray sr{x, ls.dir};
@@ -1237,7 +1251,7 @@ inline RGB trace(const Scene& s, const SceneLights& sl, const Ray& ray, int max_
                         }
                     }
                 }
-                float u1 = randf(rng), u2 = randf(rng);
+                float u1, u2; draw2(rng, u1, u2);
                 float ppdf;
                 V3 wi = hg_sample(g, wo, u1, u2, ppdf);
                 last_pdf = ppdf;
@@ -1308,7 +1322,7 @@ inline RGB trace(const Scene& s, const SceneLights& sl, const Ray& ray, int max_
             float lsp;
             int li = select_light(sl, usel, lsp);
             if (li >= 0 && lsp > 1e-6f) {
-                float u1 = randf(rng), u2 = randf(rng);
+                float u1, u2; draw2(rng, u1, u2);
                 LightSample ls = sample_light(sl.lights[li], hit.point, u1, u2);
                 if (ls.pdf > MIN_PDF) {
                     float NdotL = dot(sn, ls.dir);
@@ -1347,7 +1361,8 @@ inline RGB trace(const Scene& s, const SceneLights& sl, const Ray& ray, int max_
             }
         }
         V3 smp_n = (m.transmission > 0.5f) ? n : sn;
-        float u1 = randf(rng), u2 = randf(rng), u3 = randf(rng);   // left-to-right pin
+        float u1, u2, u3;
+        draw3(rng, u1, u2, u3);   // left-to-right pin (right to left when draw_rtl)
         BsdfSample bs = sample_bsdf(m, wo, smp_n, u1, u2, u3, rng);
         if (!bs.valid()) break;
         RGB w;
@@ -1429,7 +1444,9 @@ inline RGB render_pixel(const Scene& s, const SceneLights& sl, const Camera& cam
 // render_debug's primary-hit passes (renderer.hpp:59-93).
 inline RGB debug_pass(const Scene& s, const Ray& r, int mode) {
     Hit h = intersect_scene(s, r, 0.0f, RAY_T_MAX);
-    if (!h.hit) return RGB(0, 0, 0);
+    // render_debug maps the normal pass to 0..1 after traceNormal, so a miss
+    // (black) comes out grey (pybind_renderer.hpp:412-415)
+    if (!h.hit) return mode == 0 ? RGB(0, 0, 0) * 0.5f + RGB(0.5f, 0.5f, 0.5f) : RGB(0, 0, 0);
     if (mode == 0) return RGB(h.normal.x, h.normal.y, h.normal.z) * 0.5f + RGB(0.5f, 0.5f, 0.5f);
     if (mode == 1) {
         if (!h.mat->use_nodes) return h.mat->albedo;

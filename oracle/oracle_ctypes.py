@@ -36,6 +36,7 @@ def load() -> ctypes.CDLL:
         f, i, p, u = ctypes.c_float, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint32
         sig = {
             "orc_create": (p, []), "orc_destroy": (None, [p]), "orc_set_options": (None, [i, i]),
+            "orc_set_draw_order": (None, [i]),
             "orc_load_scene_json": (i, [p, ctypes.c_char_p]), "orc_set_camera": (None, [p] + [f] * 10),
             "orc_set_algorithm": (None, [p, ctypes.c_char_p]),
             "orc_render_tile": (i, [p, i, i, i, i, i, i, i, i, i, p, p, i]),
@@ -91,9 +92,10 @@ class OrcCoarse(ctypes.Structure):
 class Oracle:
     """The reference's PyRenderer surface, restated on the CPU."""
 
-    def __init__(self, device_math: bool = True, canonical_ties: bool = True):
+    def __init__(self, device_math: bool = True, canonical_ties: bool = True, draw_rtl: bool = False):
         self.lib = load()
         self.lib.orc_set_options(int(device_math), int(canonical_ties))
+        self.lib.orc_set_draw_order(int(draw_rtl))
         self.h = self.lib.orc_create()
 
     def __del__(self):

@@ -221,7 +221,7 @@ inline RGB trace_diag(const Scene& s, const SceneLights& sl, const Ray& ray, int
                 int li = select_light(sl, usel, lsp);
                 if (li >= 0 && lsp > 1e-6f) {
                     const Light& L = sl.lights[li];
-                    float u1 = randf(rng), u2 = randf(rng);
+                    float u1, u2; draw2(rng, u1, u2);
                     LightSample ls = sample_light(L, hit.point, u1, u2);
                     if (ls.pdf > MIN_PDF) {
                         float NdotL = dot(sn, ls.dir);
@@ -250,7 +250,8 @@ inline RGB trace_diag(const Scene& s, const SceneLights& sl, const Ray& ray, int
             }
         }
         V3 smp_n = (m.transmission > 0.5f) ? n : sn;
-        float u1 = randf(rng), u2 = randf(rng), u3 = randf(rng);
+        float u1, u2, u3;
+        draw3(rng, u1, u2, u3);
         BsdfSample bs = sample_bsdf(m, wo, smp_n, u1, u2, u3, rng);
         if (!bs.valid()) break;
         RGB w;
