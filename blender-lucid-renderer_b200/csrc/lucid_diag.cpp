@@ -27,11 +27,19 @@ void DiagStats::add(const float* v) {   // path_stats.hpp:63-100
 // vertex's (object id, material id 0 or -1, BSDF class, flags), with the
 // signed ids sign-extended to 64 bits.
 uint64_t DiagFilm::hash(const DiagRecord& r) {
+    // the diagnostic integrators record material 0 on surfaces and -1 on the
+    // final light vertex, the only Emission vertex of their paths
+    int16_t material[kDiagMaxDepth];
+    for (int i = 0; i < kDiagMaxDepth; ++i) material[i] = r.bsdf[i] == 4 ? -1 : 0;
+    return hash(r, material);
+}
+
+uint64_t DiagFilm::hash(const DiagRecord& r, const int16_t* material_ids) {
     uint64_t h = 14695981039346656037ULL;
     h ^= (uint64_t)r.depth;
     h *= 1099511628211ULL;
     for (int i = 0; i < r.depth; ++i) {
-        const int16_t material = r.bsdf[i] == 4 ? -1 : 0;   // only the final light vertex is Emission
+        const int16_t material = material_ids[i];
         h ^= (uint64_t)(int64_t)r.object_id[i];
         h *= 1099511628211ULL;
         h ^= (uint64_t)(int64_t)material;
@@ -136,6 +144,14 @@ void DiagFilm::replay(std::vector<DiagRecord>& recs, int tile_w) {
         px_[(size_t)sy * sw_ + sx].record(r, hash(r), coarse_type(r));
         ++recorded_;
     }
+}
+
+void DiagFilm::record_path(long long x, long long y, const DiagRecord& r, const int16_t* material) {
+    if (!valid_ || x < 0 || y < 0) return;
+    const long long sx = x / sf_, sy = y / sf_;
+    if (sx >= sw_ || sy >= sh_) return;
+    px_[(size_t)sy * sw_ + sx].record(r, hash(r, material), coarse_type(r));
+    ++recorded_;
 }
 
 const DiagPixel* DiagFilm::at(int x, int y) const {

@@ -76,6 +76,10 @@ public:
     void reset() { px_.clear(); valid_ = false; w_ = h_ = sw_ = sh_ = 0; recorded_ = 0; }
     // Sorts the records into the reference's loop order and replays them.
     void replay(std::vector<DiagRecord>& records, int tile_w);
+    // DiagnosticFilm::record_path (diagnostic_film.hpp:94-106): one path at
+    // film pixel (x, y); out-of-range pixels are ignored.  material: the
+    // vertices' material ids (the path hash includes them).
+    void record_path(long long x, long long y, const DiagRecord& r, const int16_t* material);
     const DiagPixel* at(int x, int y) const;
     DiagPixel* at_mut(int x, int y);
     void stats(LucidDiagStats* out) const;
@@ -92,8 +96,14 @@ public:
     void set_limits(int max_groups, int max_outliers) { max_groups_ = max_groups; max_outliers_ = max_outliers; }
     int width() const { return w_; }
     int height() const { return h_; }
+    int sampled_width() const { return sw_; }
+    int sampled_height() const { return sh_; }
+    int subsample() const { return sf_; }
+    size_t total_recorded() const { return recorded_; }
     bool valid() const { return valid_; }
     static uint64_t hash(const DiagRecord& r);
+    // PathTrace::hash (path_types.hpp:321-343) with explicit material ids
+    static uint64_t hash(const DiagRecord& r, const int16_t* material);
     static uint8_t coarse_type(const DiagRecord& r);
 
 private:

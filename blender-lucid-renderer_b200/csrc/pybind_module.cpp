@@ -59,6 +59,10 @@ struct ExportedGroupInfo {
 };
 
 enum class TopGroupSortBy { Variance, Mean };
+// BsdfType and LightSourceType (diagnostics/path_types.hpp:28-120)
+enum class BsdfType : uint8_t { Diffuse = 0, Glossy = 1, Mirror = 2, Glass = 3, Emission = 4, Environment = 5 };
+enum class LightSourceType : uint8_t { Unknown = 0, Point = 1, Area = 2, Directional = 3, Spot = 4, Environment = 5,
+                                       Emissive = 6 };
 
 struct PixelDiagnosticInfo {
     bool valid = false;
@@ -129,6 +133,93 @@ std::string heckbert_of(const LucidDiagGroup& g) {   // PathGroup::signature_hec
 float variance_luminance(const LucidDiagGroup& g) {   // PathStatistics::variance_luminance (path_stats.hpp:117-123)
     return 0.2126f * 0.2126f * g.variance_rgb[0] + 0.7152f * 0.7152f * g.variance_rgb[1] +
            0.0722f * 0.0722f * g.variance_rgb[2];
+}
+
+// The film an exporter reads: a renderer's (lucid_cuda_diag_*) or a
+// standalone DiagnosticFilm (lucid_diag_film_*).
+struct FilmRef {
+    LucidCudaCtx* ctx = nullptr;
+    LucidDiagFilm* film = nullptr;
+    int stats(LucidDiagStats* s) const { return film ? lucid_diag_film_stats(film, s) : lucid_cuda_diag_stats(ctx, s); }
+    int top(int n, int by_mean, LucidDiagGroup* g, int32_t* xy, int cap) const {
+        return film ? lucid_diag_film_top_groups(film, n, by_mean, g, xy, cap)
+                    : lucid_cuda_diag_top_groups(ctx, n, by_mean, g, xy, cap);
+    }
+    int coarse(LucidDiagCoarse* c) const { return film ? lucid_diag_film_coarse_stats(film, c) : lucid_cuda_diag_coarse_stats(ctx, c); }
+    int suggestions(LucidDiagSuggestion* o, int cap) const {
+        return film ? lucid_diag_film_suggestions(film, o, cap) : lucid_cuda_diag_suggestions(ctx, o, cap);
+    }
+    long long binary(uint8_t* o, size_t cap) const {
+        return film ? lucid_diag_film_export_binary(film, o, cap) : lucid_cuda_diag_export_binary(ctx, o, cap);
+    }
+    long long metadata(char* o, size_t cap) const {
+        return film ? lucid_diag_film_metadata_json(film, o, cap) : lucid_cuda_diag_metadata_json(ctx, o, cap);
+    }
+};
+
+GlobalDiagnosticStats global_stats_of(const FilmRef& f) {   // DiagnosticFilm::global_stats (diagnostic_film.hpp:130-154)
+    LucidDiagStats st{};
+    GlobalDiagnosticStats out;
+    if (f.stats(&st) != LUCID_OK) return out;
+    out.total_samples = st.total_samples; out.active_pixels = st.active_pixels;
+    out.total_groups = st.total_groups; out.total_overflow = st.total_overflow;
+    return out;
+}
+// DiagnosticExporter::convert_refs (diagnostic_export.hpp:257-285)
+std::vector<ExportedGroupInfo> top_groups_of(const FilmRef& f, size_t count, bool by_mean) {
+    std::vector<LucidDiagGroup> g(std::max<size_t>(count, 1));
+    std::vector<int32_t> xy(2 * g.size());
+    int n = f.top((int)count, by_mean ? 1 : 0, g.data(), xy.data(), (int)g.size());
+    std::vector<ExportedGroupInfo> out;
+    for (int i = 0; i < n; ++i) {
+        ExportedGroupInfo e;
+        e.pixel_x = (size_t)xy[2 * i]; e.pixel_y = (size_t)xy[2 * i + 1];
+        e.signature = signature_of(g[i]);
+        e.sample_count = g[i].count;
+        e.mean_luminance = g[i].mean_luminance;
+        e.variance_luminance = variance_luminance(g[i]);
+        for (int c = 0; c < 3; ++c) { e.mean_rgb[c] = g[i].mean_rgb[c]; e.variance_rgb[c] = g[i].variance_rgb[c]; }
+        e.depth = g[i].depth; e.coarse_type = g[i].coarse_type;
+        e.coarse_type_name = coarse_name(g[i].coarse_type);
+        out.push_back(std::move(e));
+    }
+    return out;
+}
+// DiagnosticExporter queries (diagnostic_export.hpp:78-220)
+std::vector<ExportedCoarseStats> coarse_stats_of(const FilmRef& f) {
+    LucidDiagCoarse c[8];
+    std::vector<ExportedCoarseStats> out;
+    if (f.coarse(c) != 8) return out;
+    for (int t = 0; t < 8; ++t) {
+        ExportedCoarseStats e;
+        e.type_id = (uint8_t)c[t].type_id; e.name = c[t].name; e.sample_count = (size_t)c[t].sample_count;
+        e.mean_luminance = c[t].mean_luminance; e.variance_luminance = c[t].variance_luminance;
+        for (int k = 0; k < 3; ++k) { e.mean_rgb[k] = c[t].mean_rgb[k]; e.variance_rgb[k] = c[t].variance_rgb[k]; }
+        out.push_back(std::move(e));
+    }
+    return out;
+}
+std::vector<DiagnosticSuggestion> suggestions_of(const FilmRef& f) {
+    LucidDiagSuggestion sg[8];
+    int n = f.suggestions(sg, 8);
+    std::vector<DiagnosticSuggestion> out;
+    for (int i = 0; i < n && i < 8; ++i) out.push_back({sg[i].category, sg[i].severity, sg[i].message, sg[i].action});
+    return out;
+}
+py::bytes binary_of(const FilmRef& f) {
+    long long n = f.binary(nullptr, 0);
+    if (n <= 0) return py::bytes("");
+    std::string b((size_t)n, '\0');
+    f.binary(reinterpret_cast<uint8_t*>(&b[0]), b.size());
+    return py::bytes(b);
+}
+std::string metadata_of(const FilmRef& f) {
+    long long n = f.metadata(nullptr, 0);
+    if (n <= 0) return std::string();
+    std::string m((size_t)n + 1, '\0');
+    f.metadata(&m[0], m.size());
+    m.resize((size_t)n);
+    return m;
 }
 
 class Renderer {
@@ -260,14 +351,7 @@ public:
     void disable_diagnostics() { lucid_cuda_diag_disable(ctx_); }
     bool is_diagnostics_enabled() { return lucid_cuda_diag_enabled(ctx_) == 1; }
     void clear_diagnostics() { lucid_cuda_diag_clear(ctx_); }
-    GlobalDiagnosticStats get_diagnostic_stats() {
-        LucidDiagStats st{};
-        GlobalDiagnosticStats out;
-        if (lucid_cuda_diag_stats(ctx_, &st) != LUCID_OK) return out;
-        out.total_samples = st.total_samples; out.active_pixels = st.active_pixels;
-        out.total_groups = st.total_groups; out.total_overflow = st.total_overflow;
-        return out;
-    }
+    GlobalDiagnosticStats get_diagnostic_stats() { return global_stats_of(FilmRef{ctx_, nullptr}); }
     size_t diag_paths_recorded() {
         LucidDiagStats st{};
         return lucid_cuda_diag_stats(ctx_, &st) == LUCID_OK ? (size_t)st.paths_recorded : 0;
@@ -297,60 +381,9 @@ public:
     // DiagnosticExporter::convert_refs (diagnostic_export.hpp:257-285)
     std::vector<ExportedGroupInfo> get_top_variance_groups(size_t count) { return top_groups(count, false); }
     std::vector<ExportedGroupInfo> top_groups(size_t count, bool by_mean) {
-        std::vector<LucidDiagGroup> g(std::max<size_t>(count, 1));
-        std::vector<int32_t> xy(2 * g.size());
-        int n = lucid_cuda_diag_top_groups(ctx_, (int)count, by_mean ? 1 : 0, g.data(), xy.data(), (int)g.size());
-        std::vector<ExportedGroupInfo> out;
-        for (int i = 0; i < n; ++i) {
-            ExportedGroupInfo e;
-            e.pixel_x = (size_t)xy[2 * i]; e.pixel_y = (size_t)xy[2 * i + 1];
-            e.signature = signature_of(g[i]);
-            e.sample_count = g[i].count;
-            e.mean_luminance = g[i].mean_luminance;
-            e.variance_luminance = variance_luminance(g[i]);
-            for (int c = 0; c < 3; ++c) { e.mean_rgb[c] = g[i].mean_rgb[c]; e.variance_rgb[c] = g[i].variance_rgb[c]; }
-            e.depth = g[i].depth; e.coarse_type = g[i].coarse_type;
-            e.coarse_type_name = coarse_name(g[i].coarse_type);
-            out.push_back(std::move(e));
-        }
-        return out;
+        return top_groups_of(FilmRef{ctx_, nullptr}, count, by_mean);
     }
-    // DiagnosticExporter queries (diagnostic_export.hpp:78-220)
-    std::vector<ExportedCoarseStats> coarse_stats() {
-        LucidDiagCoarse c[8];
-        std::vector<ExportedCoarseStats> out;
-        if (lucid_cuda_diag_coarse_stats(ctx_, c) != 8) return out;
-        for (int t = 0; t < 8; ++t) {
-            ExportedCoarseStats e;
-            e.type_id = (uint8_t)c[t].type_id; e.name = c[t].name; e.sample_count = (size_t)c[t].sample_count;
-            e.mean_luminance = c[t].mean_luminance; e.variance_luminance = c[t].variance_luminance;
-            for (int k = 0; k < 3; ++k) { e.mean_rgb[k] = c[t].mean_rgb[k]; e.variance_rgb[k] = c[t].variance_rgb[k]; }
-            out.push_back(std::move(e));
-        }
-        return out;
-    }
-    std::vector<DiagnosticSuggestion> suggestions() {
-        LucidDiagSuggestion sg[8];
-        int n = lucid_cuda_diag_suggestions(ctx_, sg, 8);
-        std::vector<DiagnosticSuggestion> out;
-        for (int i = 0; i < n && i < 8; ++i) out.push_back({sg[i].category, sg[i].severity, sg[i].message, sg[i].action});
-        return out;
-    }
-    py::bytes export_binary() {
-        long long n = lucid_cuda_diag_export_binary(ctx_, nullptr, 0);
-        if (n <= 0) return py::bytes("");
-        std::string b((size_t)n, '\0');
-        lucid_cuda_diag_export_binary(ctx_, reinterpret_cast<uint8_t*>(&b[0]), b.size());
-        return py::bytes(b);
-    }
-    std::string metadata_json() {
-        long long n = lucid_cuda_diag_metadata_json(ctx_, nullptr, 0);
-        if (n <= 0) return std::string();
-        std::string m((size_t)n + 1, '\0');
-        lucid_cuda_diag_metadata_json(ctx_, &m[0], m.size());
-        m.resize((size_t)n);
-        return m;
-    }
+    FilmRef film_ref() { return FilmRef{ctx_, nullptr}; }
     // get_pixel_diagnostic (pybind_renderer.hpp:1008-1102)
     PixelDiagnosticInfo get_pixel_diagnostic(size_t x, size_t y, TopGroupSortBy sort_by) {
         PixelDiagnosticInfo info;
@@ -437,9 +470,109 @@ std::string adapter_info() {
 
 }  // namespace
 
+// ---- standalone diagnostics (src/pybind_module.cpp:433-539) ----
+// PathTrace (diagnostics/path_types.hpp:249-372)
+struct PathTrace {
+    LucidPathTrace t{};
+    size_t depth() const { return t.depth; }
+};
+
+// PathDiagnosticRecorder (diagnostics/diagnostic_integrator.hpp:87-248):
+// builds one PathTrace vertex by vertex.
+class PathDiagnosticRecorder {
+public:
+    // begin_path: PathTrace::clear (path_types.hpp:272-278); the vertex
+    // positions and normals are left as they were, as there
+    void begin_path() {
+        cur_.depth = 0;
+        cur_.contribution[0] = cur_.contribution[1] = cur_.contribution[2] = 0.0f;
+        cur_.light_type = 0;
+        cur_.strategy = 0;
+    }
+    void record_vertex(int32_t object_id, int16_t material_id, uint8_t type, bool is_delta, bool is_light_sampled) {
+        push(object_id, material_id, type, (uint8_t)((is_delta ? 1 : 0) | (is_light_sampled ? 2 : 0)));
+    }
+    void record_environment_hit() {
+        if (push(-1, -1, 5, 0)) cur_.light_type = 5;
+    }
+    void record_light_hit(int32_t light_id, uint8_t light_source_type) {
+        if (push(-(light_id + 2), -1, 4, 0)) cur_.light_type = light_source_type;
+    }
+    void record_emissive_hit(int32_t object_id, int16_t material_id) {
+        if (push(object_id, material_id, 4, 0)) cur_.light_type = 6;
+    }
+    size_t current_depth() const { return cur_.depth; }
+    PathTrace end_path(float r, float g, float b) {
+        cur_.contribution[0] = r; cur_.contribution[1] = g; cur_.contribution[2] = b;
+        PathTrace p;
+        p.t = cur_;
+        return p;
+    }
+
+private:
+    bool push(int32_t obj, int16_t mat, uint8_t type, uint8_t flags) {
+        if (cur_.depth >= 16) return false;
+        LucidPathVertex& v = cur_.vertices[cur_.depth++];
+        v.object_id = obj; v.material_id = mat; v.bsdf_type = type; v.flags = flags;
+        return true;
+    }
+    LucidPathTrace cur_{};
+};
+
+// DiagnosticFilm (diagnostics/diagnostic_film.hpp:59-313) over a host film
+// of the C ABI.
+class DiagnosticFilm {
+public:
+    DiagnosticFilm(size_t width, size_t height, const PathRecordingConfig& c) : cfg_(c) {
+        LucidDiagConfig cfg{c.subsample_factor, c.max_groups_per_pixel, c.max_outliers_per_pixel, c.max_depth,
+                            c.variance_threshold, c.outlier_threshold, 0};
+        if (lucid_diag_film_create((long long)width, (long long)height, &cfg, &f_) != LUCID_OK)
+            throw std::invalid_argument("DiagnosticFilm: invalid size or subsample_factor");
+    }
+    ~DiagnosticFilm() { lucid_diag_film_destroy(f_); }
+    DiagnosticFilm(const DiagnosticFilm&) = delete;
+    DiagnosticFilm& operator=(const DiagnosticFilm&) = delete;
+    size_t info(int k) const {
+        long long v[5] = {0, 0, 0, 0, 0};
+        lucid_diag_film_info(f_, v);
+        return (size_t)v[k];
+    }
+    void record_path(size_t x, size_t y, const PathTrace& t) { lucid_diag_film_record_path(f_, (long long)x, (long long)y, &t.t); }
+    void clear() { lucid_diag_film_clear(f_); }
+    FilmRef ref() const { return FilmRef{nullptr, f_}; }
+
+private:
+    LucidDiagFilm* f_ = nullptr;
+    PathRecordingConfig cfg_;
+};
+
+// DiagnosticPathTracer (diagnostic_integrator.hpp:408-463): a film plus an
+// enabled flag and the subsampling test.
+class DiagnosticPathTracer {
+public:
+    DiagnosticPathTracer(size_t w, size_t h, const PathRecordingConfig& c) : film_(w, h, c), cfg_(c) {}
+    void set_enabled(bool e) { enabled_ = e; }
+    bool is_enabled() const { return enabled_; }
+    bool should_record(size_t x, size_t y) const {
+        const size_t sf = (size_t)std::max(1, cfg_.subsample_factor);
+        return enabled_ && x % sf == 0 && y % sf == 0;
+    }
+    void record_path(size_t x, size_t y, const PathTrace& t) {
+        if (enabled_) film_.record_path(x, y, t);
+    }
+    void clear() { film_.clear(); }
+    DiagnosticFilm& film() { return film_; }
+
+private:
+    DiagnosticFilm film_;
+    PathRecordingConfig cfg_;
+    bool enabled_ = true;
+};
+
+// DiagnosticExporter (diagnostic_export.hpp:78-285) over a DiagnosticFilm,
+// as in the reference, or over a Renderer's film (an addition).
 struct DiagnosticExporter {
-    explicit DiagnosticExporter(Renderer& renderer) : r(&renderer) {}
-    Renderer* r;
+    FilmRef f;
 };
 
 PYBIND11_MODULE(lucidrenderer, m) {
@@ -631,19 +764,86 @@ PYBIND11_MODULE(lucidrenderer, m) {
         .def("__repr__", [](const DiagnosticSuggestion& s) {
             return "<DiagnosticSuggestion [" + s.severity + "] " + s.category + ": " + s.message + ">";
         });
-    // DiagnosticExporter (diagnostic_export.hpp:78-220): the reference builds
-    // it from a DiagnosticFilm; here from the renderer that holds the film.
+    // DiagnosticFilm / DiagnosticPathTracer / DiagnosticExporter / enums /
+    // PathTrace / PathDiagnosticRecorder (src/pybind_module.cpp:433-539)
+    py::class_<DiagnosticFilm>(m, "DiagnosticFilm")
+        .def(py::init<size_t, size_t, const PathRecordingConfig&>(), py::arg("width"), py::arg("height"),
+             py::arg("config"), "Create diagnostic film for given dimensions")
+        .def("width", [](const DiagnosticFilm& f) { return f.info(0); })
+        .def("height", [](const DiagnosticFilm& f) { return f.info(1); })
+        .def("sampled_width", [](const DiagnosticFilm& f) { return f.info(2); })
+        .def("sampled_height", [](const DiagnosticFilm& f) { return f.info(3); })
+        .def("total_paths_recorded", [](const DiagnosticFilm& f) { return f.info(4); })
+        .def("global_stats", [](const DiagnosticFilm& f) { return global_stats_of(f.ref()); })
+        .def("metadata_json", [](const DiagnosticFilm& f) { return metadata_of(f.ref()); })
+        .def("record_path", &DiagnosticFilm::record_path, py::arg("x"), py::arg("y"), py::arg("trace"),
+             "Record a path trace at pixel (x, y)")
+        .def("clear", &DiagnosticFilm::clear);
+    py::class_<DiagnosticPathTracer>(m, "DiagnosticPathTracer")
+        .def(py::init<size_t, size_t, const PathRecordingConfig&>(), py::arg("width"), py::arg("height"),
+             py::arg("config"), "Create diagnostic path tracer")
+        .def("is_enabled", &DiagnosticPathTracer::is_enabled)
+        .def("set_enabled", &DiagnosticPathTracer::set_enabled)
+        .def("film", &DiagnosticPathTracer::film, py::return_value_policy::reference_internal);
     py::class_<DiagnosticExporter>(m, "DiagnosticExporter")
-        .def(py::init<Renderer&>(), py::arg("renderer"), py::keep_alive<1, 2>())
-        .def("get_global_stats", [](DiagnosticExporter& e) { return e.r->get_diagnostic_stats(); })
-        .def("get_top_variance_groups", [](DiagnosticExporter& e, size_t n) { return e.r->top_groups(n, false); },
+        .def(py::init([](const DiagnosticFilm& f) { return DiagnosticExporter{f.ref()}; }), py::arg("film"),
+             py::keep_alive<1, 2>(), "Create exporter for a diagnostic film")
+        .def(py::init([](Renderer& r) { return DiagnosticExporter{r.film_ref()}; }), py::arg("renderer"),
+             py::keep_alive<1, 2>(), "Create exporter for the film of a Renderer's last diagnostic render")
+        .def("get_global_stats", [](const DiagnosticExporter& e) { return global_stats_of(e.f); })
+        .def("get_top_variance_groups", [](const DiagnosticExporter& e, size_t n) { return top_groups_of(e.f, n, false); },
              py::arg("n") = 10)
-        .def("get_top_mean_groups", [](DiagnosticExporter& e, size_t n) { return e.r->top_groups(n, true); },
+        .def("get_top_mean_groups", [](const DiagnosticExporter& e, size_t n) { return top_groups_of(e.f, n, true); },
              py::arg("n") = 10)
-        .def("get_coarse_stats", [](DiagnosticExporter& e) { return e.r->coarse_stats(); })
-        .def("generate_suggestions", [](DiagnosticExporter& e) { return e.r->suggestions(); })
-        .def("export_metadata_json", [](DiagnosticExporter& e) { return e.r->metadata_json(); })
-        .def("export_binary", [](DiagnosticExporter& e) { return e.r->export_binary(); });
+        .def("get_coarse_stats", [](const DiagnosticExporter& e) { return coarse_stats_of(e.f); })
+        .def("generate_suggestions", [](const DiagnosticExporter& e) { return suggestions_of(e.f); })
+        .def("export_metadata_json", [](const DiagnosticExporter& e) { return metadata_of(e.f); })
+        .def("export_binary", [](const DiagnosticExporter& e) { return binary_of(e.f); });
+    py::enum_<BsdfType>(m, "BsdfType")
+        .value("Diffuse", BsdfType::Diffuse)
+        .value("Glossy", BsdfType::Glossy)
+        .value("Mirror", BsdfType::Mirror)
+        .value("Glass", BsdfType::Glass)
+        .value("Emission", BsdfType::Emission)
+        .value("Environment", BsdfType::Environment)
+        .export_values();
+    py::enum_<LightSourceType>(m, "LightSourceType")
+        .value("Unknown", LightSourceType::Unknown)
+        .value("Point", LightSourceType::Point)
+        .value("Area", LightSourceType::Area)
+        .value("Directional", LightSourceType::Directional)
+        .value("Spot", LightSourceType::Spot)
+        .value("Environment", LightSourceType::Environment)
+        .value("Emissive", LightSourceType::Emissive)
+        .export_values();
+    py::class_<PathTrace>(m, "PathTrace")
+        .def(py::init<>(), "Create empty path trace")
+        .def_property_readonly("depth", &PathTrace::depth)
+        .def("get_contribution", [](const PathTrace& p) {
+            return std::array<float, 3>{p.t.contribution[0], p.t.contribution[1], p.t.contribution[2]};
+        });
+    py::class_<PathDiagnosticRecorder>(m, "PathDiagnosticRecorder")
+        .def(py::init<>(), "Create a new path recorder")
+        .def("begin_path", &PathDiagnosticRecorder::begin_path, "Start recording a new path")
+        .def("record_vertex", [](PathDiagnosticRecorder& r, int32_t object_id, int16_t material_id, BsdfType t,
+                                 bool is_delta, bool is_light_sampled) {
+                 r.record_vertex(object_id, material_id, (uint8_t)t, is_delta, is_light_sampled);
+             },
+             py::arg("object_id"), py::arg("material_id"), py::arg("bsdf_type"), py::arg("is_delta"),
+             py::arg("is_light_sampled"), "Record a surface interaction vertex")
+        .def("record_environment_hit", &PathDiagnosticRecorder::record_environment_hit, "Record environment map hit")
+        .def("record_light_hit", [](PathDiagnosticRecorder& r, int32_t light_id, LightSourceType t) {
+                 r.record_light_hit(light_id, (uint8_t)t);
+             },
+             py::arg("light_id"), py::arg("light_source_type") = LightSourceType::Unknown,
+             "Record light hit with optional light source type for Heckbert notation")
+        .def("record_emissive_hit", &PathDiagnosticRecorder::record_emissive_hit, py::arg("object_id"),
+             py::arg("material_id"), "Record emissive mesh hit")
+        .def("current_depth", &PathDiagnosticRecorder::current_depth, "Get current path depth")
+        .def("end_path", &PathDiagnosticRecorder::end_path, py::arg("r"), py::arg("g"), py::arg("b"),
+             "Finalize path and return PathTrace")
+        .def("end_path_lum", [](PathDiagnosticRecorder& r, float l) { return r.end_path(l, l, l); },
+             py::arg("luminance"), "Finalize path with grayscale luminance");
     m.attr("__version__") = "1.0.0";
     m.attr("openmp_enabled") = false;
     m.attr("dawn_enabled") = false;

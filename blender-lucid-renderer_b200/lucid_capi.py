@@ -144,6 +144,19 @@ class DiagConfig(ctypes.Structure):
                 ("record_capacity", ctypes.c_longlong)]
 
 
+class PathVertex(ctypes.Structure):
+    _fields_ = [("object_id", ctypes.c_int32), ("material_id", ctypes.c_int16), ("bsdf_type", ctypes.c_uint8),
+                ("flags", ctypes.c_uint8)]
+
+
+class PathTrace(ctypes.Structure):
+    """LucidPathTrace (include/lucid_cuda.h): PathTrace of path_types.hpp:249-257."""
+    _fields_ = [("vertices", PathVertex * 16), ("positions", (ctypes.c_float * 3) * 16),
+                ("normals", (ctypes.c_float * 3) * 16), ("depth", ctypes.c_uint32),
+                ("contribution", ctypes.c_float * 3), ("light_type", ctypes.c_uint8), ("strategy", ctypes.c_uint8),
+                ("pad", ctypes.c_uint8 * 2)]
+
+
 # LucidDiagGroup / LucidDiagPixel / LucidDiagStats (include/lucid_cuda.h).
 DIAG_GROUP_DTYPE = np.dtype([("hash", np.uint64), ("count", np.uint32), ("depth", np.uint8),
                              ("coarse_type", np.uint8), ("light_type", np.uint8), ("strategy", np.uint8),
@@ -215,6 +228,21 @@ SIGNATURES = {
     "lucid_cuda_diag_pixel": (_I, [_P, _I, _I, _I, _P, _P, _I]),
     "lucid_cuda_diag_variance_map": (_I, [_P, _P, ctypes.c_size_t]),
     "lucid_cuda_diag_top_groups": (_I, [_P, _I, _I, _P, _P, _I]),
+    "lucid_diag_film_create": (_I, [ctypes.c_longlong, ctypes.c_longlong, ctypes.POINTER(DiagConfig),
+                                    ctypes.POINTER(_P)]),
+    "lucid_diag_film_destroy": (None, [_P]),
+    "lucid_diag_film_record_path": (_I, [_P, ctypes.c_longlong, ctypes.c_longlong, ctypes.POINTER(PathTrace)]),
+    "lucid_diag_film_clear": (_I, [_P]),
+    "lucid_diag_film_info": (_I, [_P, ctypes.POINTER(ctypes.c_longlong)]),
+    "lucid_diag_film_stats": (_I, [_P, _P]),
+    "lucid_diag_film_pixel": (_I, [_P, ctypes.c_longlong, ctypes.c_longlong, _I, _P, _P, _I]),
+    "lucid_diag_film_top_groups": (_I, [_P, _I, _I, _P, _P, _I]),
+    "lucid_diag_film_coarse_stats": (_I, [_P, ctypes.c_void_p]),
+    "lucid_diag_film_suggestions": (_I, [_P, ctypes.c_void_p, _I]),
+    "lucid_diag_film_export_binary": (ctypes.c_longlong, [_P, ctypes.c_void_p, ctypes.c_size_t]),
+    "lucid_diag_film_metadata_json": (ctypes.c_longlong, [_P, ctypes.c_void_p, ctypes.c_size_t]),
+    "lucid_path_trace_hash": (ctypes.c_uint64, [ctypes.POINTER(PathTrace)]),
+    "lucid_path_trace_coarse_type": (_I, [ctypes.POINTER(PathTrace)]),
     "lucid_server_create": (_I, [_I, _I, ctypes.c_longlong, ctypes.POINTER(_P)]),
     "lucid_server_destroy": (None, [_P]),
     "lucid_server_last_error": (ctypes.c_char_p, [_P]),
@@ -619,3 +647,50 @@ class Server:
         if rc != LUCID_OK:
             self._err(rc)
         return {f: getattr(st, f) for f, _ in ServerStats._fields_}
+
+
+class DiagFilm:
+    """A standalone DiagnosticFilm (lucid_diag_film_*, host only: no GPU)."""
+
+    def __init__(self, width: int, height: int, subsample: int = 2, max_groups: int = 16, max_outliers: int = 4,
+                 max_depth: int = 16, variance_threshold: float = 0.001, outlier_threshold: float = 3.0):
+        self.lib = load_library()
+        cfg = DiagConfig(subsample, max_groups, max_outliers, max_depth, variance_threshold, outlier_threshold, 0)
+        h = ctypes.c_void_p()
+        rc = self.lib.lucid_diag_film_create(width, height, ctypes.byref(cfg), ctypes.byref(h))
+        if rc != LUCID_OK:
+            raise LucidError(rc, "lucid_diag_film_create failed")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.lucid_diag_film_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def record_path(self, x: int, y: int, trace: PathTrace):
+        rc = self.lib.lucid_diag_film_record_path(self.h, x, y, ctypes.byref(trace))
+        if rc != LUCID_OK:
+            raise LucidError(rc, "record_path failed")
+
+    def clear(self):
+        self.lib.lucid_diag_film_clear(self.h)
+
+    def info(self) -> list:
+        v = (ctypes.c_longlong * 5)()
+        self.lib.lucid_diag_film_info(self.h, v)
+        return list(v)
+
+    def pixel(self, x, y, sort_by_mean=False, cap=32):
+        info = np.zeros(1, DIAG_PIXEL_DTYPE)
+        groups = np.zeros(cap, DIAG_GROUP_DTYPE)
+        n = self.lib.lucid_diag_film_pixel(self.h, x, y, int(sort_by_mean), info.ctypes.data, groups.ctypes.data, cap)
+        if n < 0:
+            raise LucidError(n, "pixel query failed")
+        return info[0], groups[:n]
+

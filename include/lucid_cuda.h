@@ -357,6 +357,63 @@ long long lucid_cuda_diag_export_binary(LucidCudaCtx* ctx, uint8_t* out, size_t 
  * terminated when it fits) and returns its length. */
 long long lucid_cuda_diag_metadata_json(LucidCudaCtx* ctx, char* out, size_t cap);
 
+/* ---- standalone diagnostic films (host only, no device) ---------------- */
+/* The reference module's DiagnosticFilm / DiagnosticPathTracer /
+ * DiagnosticExporter / PathTrace / PathDiagnosticRecorder classes
+ * (src/pybind_module.cpp:433-539): a film built by the caller and fed one
+ * completed path at a time, as the add-on's DiagnosticsManager does
+ * (LucidRenderer/diagnostics.py:111-330).  These calls need no GPU. */
+typedef struct LucidDiagFilm LucidDiagFilm;
+/* PathVertex (diagnostics/path_types.hpp:195-246): object id (mesh index,
+ * -1 environment, -(light + 2) a light), material id, BsdfType (0 Diffuse,
+ * 1 Glossy, 2 Mirror, 3 Glass, 4 Emission, 5 Environment), flags (1 delta,
+ * 2 light sampled). */
+typedef struct LucidPathVertex {
+    int32_t object_id;
+    int16_t material_id;
+    uint8_t bsdf_type, flags;
+} LucidPathVertex;
+/* PathTrace (path_types.hpp:249-257): up to 16 vertices with positions and
+ * normals, the contribution, LightSourceType (0 Unknown, 1 Point, 2 Area,
+ * 3 Directional, 4 Spot, 5 Environment, 6 Emissive) and SamplingStrategy
+ * (0 BSDF, 1 NEE, 2 MIS_BSDF, 3 MIS_NEE). */
+typedef struct LucidPathTrace {
+    LucidPathVertex vertices[16];
+    float positions[16][3];
+    float normals[16][3];
+    uint32_t depth;
+    float contribution[3];
+    uint8_t light_type, strategy, pad[2];
+} LucidPathTrace;
+/* DiagnosticFilm(width, height, config) (diagnostic_film.hpp:66-75);
+ * config may be NULL (standard preset).  Free with lucid_diag_film_destroy. */
+int lucid_diag_film_create(long long width, long long height, const LucidDiagConfig* config, LucidDiagFilm** out);
+void lucid_diag_film_destroy(LucidDiagFilm* film);
+/* DiagnosticFilm::record_path (diagnostic_film.hpp:94-106): pixel (x, y) of
+ * the film (cells of subsample_factor^2 pixels; pixels outside are ignored). */
+int lucid_diag_film_record_path(LucidDiagFilm* film, long long x, long long y, const LucidPathTrace* trace);
+/* DiagnosticFilm::clear (:308-313). */
+int lucid_diag_film_clear(LucidDiagFilm* film);
+/* width, height, sampled_width, sampled_height, total_paths_recorded
+ * (diagnostic_film.hpp:80-113) into out[5]. */
+int lucid_diag_film_info(LucidDiagFilm* film, long long* out5);
+/* global_stats (:130-154) + paths recorded. */
+int lucid_diag_film_stats(LucidDiagFilm* film, LucidDiagStats* out);
+/* PixelPathData of film pixel (x, y), groups sorted by variance (or mean
+ * luminance), as lucid_cuda_diag_pixel. */
+int lucid_diag_film_pixel(LucidDiagFilm* film, long long x, long long y, int sort_by_mean, LucidDiagPixel* info,
+                          LucidDiagGroup* groups, int cap);
+/* DiagnosticExporter over the film (diagnostic_export.hpp:78-220), as the
+ * lucid_cuda_diag_* exporter calls over a renderer's film. */
+int lucid_diag_film_top_groups(LucidDiagFilm* film, int n, int by_mean, LucidDiagGroup* groups, int32_t* xy, int cap);
+int lucid_diag_film_coarse_stats(LucidDiagFilm* film, LucidDiagCoarse* out);
+int lucid_diag_film_suggestions(LucidDiagFilm* film, LucidDiagSuggestion* out, int cap);
+long long lucid_diag_film_export_binary(LucidDiagFilm* film, uint8_t* out, size_t cap);
+long long lucid_diag_film_metadata_json(LucidDiagFilm* film, char* out, size_t cap);
+/* PathTrace::hash and coarse_type (path_types.hpp:321-372). */
+uint64_t lucid_path_trace_hash(const LucidPathTrace* trace);
+int lucid_path_trace_coarse_type(const LucidPathTrace* trace);
+
 /* ---- request loop (several jobs on one device) ------------------------- */
 /* No reference counterpart: the reference runs one Renderer per Blender
  * session (viewport, F12 render, material preview; render_session.py:77-106),

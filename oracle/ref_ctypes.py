@@ -65,6 +65,13 @@ def load(path: str) -> ctypes.CDLL:
             "ref_set_camera": (None, [p] + [f] * 10), "ref_set_algorithm": (None, [p, ctypes.c_char_p]),
             "ref_render_tile": (i, [p] + [i] * 9 + [p]),
             "ref_render_debug": (i, [p] + [i] * 6 + [ctypes.c_char_p, p]), "ref_max_threads": (i, []),
+            "ref_film_create": (p, [ctypes.c_longlong, ctypes.c_longlong, i, i, i, i, f, f]),
+            "ref_film_destroy": (None, [p]), "ref_film_clear": (None, [p]),
+            "ref_recorder_create": (p, []), "ref_recorder_destroy": (None, [p]), "ref_recorder_begin": (None, [p]),
+            "ref_recorder_vertex": (None, [p, i, i, i, i, i]), "ref_recorder_environment": (None, [p]),
+            "ref_recorder_light": (None, [p, i, i]), "ref_recorder_emissive": (None, [p, i, i]),
+            "ref_recorder_end_into": (ctypes.c_ulonglong, [p, p, ctypes.c_longlong, ctypes.c_longlong, f, f, f]),
+            "ref_film_report": (ctypes.c_void_p, [p, i, i]), "ref_free": (None, [ctypes.c_void_p]),
         }.items():
             fn = getattr(lib, name)
             fn.restype = res
@@ -123,3 +130,55 @@ class ReferenceRenderer:
         if rc != 0:
             raise RuntimeError("reference render_debug returned a buffer of the wrong size")
         return out
+
+
+class ReferenceFilm:
+    """The reference's DiagnosticFilm with a PathDiagnosticRecorder feeding it
+    and a DiagnosticExporter reading it (diagnostics/*.hpp)."""
+
+    def __init__(self, width, height, subsample=2, max_groups=16, max_outliers=4, max_depth=16,
+                 variance_threshold=0.001, outlier_threshold=3.0, path: str | None = None):
+        path = path or os.path.join(REF_DIR, "libref_check.so")
+        self.lib = load(path)
+        self.subsample = subsample
+        self.f = self.lib.ref_film_create(width, height, subsample, max_groups, max_outliers, max_depth,
+                                          variance_threshold, outlier_threshold)
+        self.r = self.lib.ref_recorder_create()
+
+    def __del__(self):
+        try:
+            self.lib.ref_recorder_destroy(self.r)
+            self.lib.ref_film_destroy(self.f)
+        except Exception:
+            pass
+
+    # PathDiagnosticRecorder calls
+    def begin_path(self):
+        self.lib.ref_recorder_begin(self.r)
+
+    def record_vertex(self, obj, mat, bsdf, delta, light_sampled):
+        self.lib.ref_recorder_vertex(self.r, obj, mat, bsdf, int(delta), int(light_sampled))
+
+    def record_environment_hit(self):
+        self.lib.ref_recorder_environment(self.r)
+
+    def record_light_hit(self, light_id, light_type):
+        self.lib.ref_recorder_light(self.r, light_id, light_type)
+
+    def record_emissive_hit(self, obj, mat):
+        self.lib.ref_recorder_emissive(self.r, obj, mat)
+
+    def end_path_into_film(self, x, y, r, g, b) -> int:
+        return int(self.lib.ref_recorder_end_into(self.r, self.f, x, y, r, g, b))
+
+    def clear(self):
+        self.lib.ref_film_clear(self.f)
+
+    def report(self, top_n: int = 10) -> dict:
+        import json
+        c = self.lib.ref_film_report(self.f, top_n, self.subsample)
+        try:
+            return json.loads(ctypes.string_at(c).decode())
+        finally:
+            self.lib.ref_free(c)
+
