@@ -72,6 +72,8 @@ def load(path: str) -> ctypes.CDLL:
             "ref_recorder_light": (None, [p, i, i]), "ref_recorder_emissive": (None, [p, i, i]),
             "ref_recorder_end_into": (ctypes.c_ulonglong, [p, p, ctypes.c_longlong, ctypes.c_longlong, f, f, f]),
             "ref_film_report": (ctypes.c_void_p, [p, i, i]), "ref_free": (None, [ctypes.c_void_p]),
+            "ref_enable_diagnostics": (None, [p, i, i, i, i, f, f]), "ref_disable_diagnostics": (None, [p]),
+            "ref_diag_report": (ctypes.c_void_p, [p, i, i, i]), "ref_set_threads": (None, [i]),
         }.items():
             fn = getattr(lib, name)
             fn.restype = res
@@ -101,6 +103,10 @@ class ReferenceRenderer:
     def threads(self) -> int:
         return int(self.lib.ref_max_threads())
 
+    def set_threads(self, n: int):
+        """OpenMP threads of the render loops (0: all processors); process-wide."""
+        self.lib.ref_set_threads(n)
+
     def load_scene_json(self, text: str) -> bool:
         return bool(self.lib.ref_load_scene_json(self.h, text.encode()))
 
@@ -120,6 +126,25 @@ class ReferenceRenderer:
         if rc != 0:
             raise RuntimeError("reference render_tile returned a buffer of the wrong size")
         return out
+
+    def enable_diagnostics(self, subsample=2, max_groups=16, max_outliers=4, max_depth=16,
+                           variance_threshold=0.001, outlier_threshold=3.0):
+        self.lib.ref_enable_diagnostics(self.h, subsample, max_groups, max_outliers, max_depth,
+                                        variance_threshold, outlier_threshold)
+
+    def disable_diagnostics(self):
+        self.lib.ref_disable_diagnostics(self.h)
+
+    def diag_report(self, tile_w, tile_h, top_n=10) -> dict:
+        """get_diagnostic_stats, get_pixel_diagnostic of every tile pixel (groups
+        sorted by variance), get_top_variance_groups and export_diagnostic_json
+        of the last diagnostic render."""
+        import json
+        c = self.lib.ref_diag_report(self.h, tile_w, tile_h, top_n)
+        try:
+            return json.loads(ctypes.string_at(c).decode())
+        finally:
+            self.lib.ref_free(c)
 
     def render_debug(self, mode: str, tile_w, tile_h, full_w=None, full_h=None, tile_x=0, tile_y=0) -> np.ndarray:
         full_w = tile_w if full_w is None else full_w

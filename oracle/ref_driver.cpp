@@ -134,6 +134,66 @@ char* ref_film_report(void* fp, int top_n, int subsample) {
 }
 void ref_free(char* p) { std::free(p); }
 
+// ---- PyRenderer's own diagnostics (pybind_renderer.hpp:893-1102)
+void ref_enable_diagnostics(void* r, int subsample, int max_groups, int max_outliers, int max_depth,
+                            float variance_threshold, float outlier_threshold) {
+    render::diagnostics::PathRecordingConfig c;
+    c.subsample_factor = subsample;
+    c.max_groups_per_pixel = max_groups;
+    c.max_outliers_per_pixel = max_outliers;
+    c.max_depth = max_depth;
+    c.variance_threshold = variance_threshold;
+    c.outlier_threshold = outlier_threshold;
+    static_cast<PyRenderer*>(r)->enable_diagnostics(c);
+}
+void ref_disable_diagnostics(void* r) { static_cast<PyRenderer*>(r)->disable_diagnostics(); }
+
+// get_diagnostic_stats, every pixel's get_pixel_diagnostic (by variance),
+// get_top_variance_groups, export_diagnostic_json, as JSON.
+char* ref_diag_report(void* rp, int tile_w, int tile_h, int top_n) {
+    PyRenderer& r = *static_cast<PyRenderer*>(rp);
+    nlohmann::json j;
+    auto st = r.get_diagnostic_stats();
+    j["stats"] = nlohmann::json::array({st.total_samples, st.active_pixels, st.total_groups, st.total_overflow});
+    auto group = [](const render::diagnostics::ExportedGroupInfo& g) {
+        return nlohmann::json{{"signature", g.signature}, {"heckbert", g.signature_heckbert},
+                              {"object_ids", g.object_ids}, {"count", g.sample_count},
+                              {"mean_luminance", g.mean_luminance}, {"variance_luminance", g.variance_luminance},
+                              {"mean_rgb", g.mean_rgb}, {"variance_rgb", g.variance_rgb}, {"depth", g.depth},
+                              {"coarse_type", g.coarse_type}, {"strategy", g.strategy_name},
+                              {"object_path", g.object_path}, {"positions", g.positions}, {"normals", g.normals},
+                              {"x", g.pixel_x}, {"y", g.pixel_y}};
+    };
+    nlohmann::json px = nlohmann::json::array();
+    for (int y = 0; y < tile_h; ++y)
+        for (int x = 0; x < tile_w; ++x) {
+            auto info = r.get_pixel_diagnostic((size_t)x, (size_t)y);
+            nlohmann::json gs = nlohmann::json::array();
+            for (const auto& g : info.top_groups) gs.push_back(group(g));
+            px.push_back({{"valid", info.valid}, {"samples", info.sample_count}, {"variance", info.variance},
+                          {"groups", info.group_count}, {"outliers", info.outlier_count}, {"mean_rgb", info.mean_rgb},
+                          {"top", gs}});
+        }
+    j["pixels"] = px;
+    nlohmann::json tv = nlohmann::json::array();
+    for (const auto& g : r.get_top_variance_groups((size_t)top_n)) tv.push_back(group(g));
+    j["top_variance"] = tv;
+    j["json"] = r.export_diagnostic_json();
+    std::string out = j.dump();
+    char* c = static_cast<char*>(std::malloc(out.size() + 1));
+    std::memcpy(c, out.c_str(), out.size() + 1);
+    return c;
+}
+
+// OpenMP threads of the reference's render loops (omp_set_num_threads).
+void ref_set_threads(int n) {
+#ifdef _OPENMP
+    omp_set_num_threads(n > 0 ? n : omp_get_num_procs());
+#else
+    (void)n;
+#endif
+}
+
 int ref_max_threads() {
 #ifdef _OPENMP
     return omp_get_max_threads();

@@ -162,3 +162,72 @@ def test_oracle_reproduces_reference_golden_images(workdir, name):
         got, _, rc = o.render(w, h, w, h, spp, off, depth)
         assert rc == 0
     _assert_bit_equal(got, want, name)
+
+
+DIAG_CASES = [
+    ("cornell", "mis", 24, 24, 4, 8, 2),
+    ("cornell", "nee", 16, 16, 3, 8, 1),
+    ("cornell", "simple", 16, 16, 2, 6, 2),
+    ("all_lights_novol", "mis", 24, 16, 2, 8, 2),
+    ("mirror", "mis", 16, 16, 4, 6, 1),
+]
+
+
+@pytest.mark.parametrize("scene,algo,w,h,spp,depth,sf", DIAG_CASES)
+def test_oracle_reproduces_reference_diagnostic_render(ref_lib, workdir, scene, algo, w, h, spp, depth, sf):
+    """render_tile with diagnostics enabled (the reference's diagnostic
+    integrators, path_tracer.hpp:880-1514, recording into a fresh
+    DiagnosticFilm per call, pybind_renderer.hpp:205-316): the image, the
+    global stats and every pixel's get_pixel_diagnostic (sample / group /
+    outlier counts, variance, mean, and each group's object ids, counts,
+    mean and variance, depth, coarse type, strategy, vertex positions and
+    normals) equal the oracle's restatement.
+
+    The reference parallelises the pixels of each 8x8 micro-tile over
+    OpenMP threads, so with a subsample factor above 1 several threads
+    update one film cell at once (a data race: samples counted, groups
+    lost).  It runs single-threaded here, in the loop order the oracle and
+    the CUDA film replay follow."""
+    import lucid_scenes as ls
+    sc, cam = scene_and_camera(scene, workdir)
+    r, o = _pair(ref_lib, ls.to_json(sc), cam, algo)
+    r.enable_diagnostics(subsample=sf)
+    r.set_threads(1)
+    try:
+        want_img = r.render(w, h, w, h, spp, 2, depth)
+    finally:
+        r.set_threads(0)
+    want = r.diag_report(w, h, top_n=8)
+    got_img, rc = o.render_diag(w, h, w, h, spp, 2, depth, subsample=sf)
+    assert rc == 0
+    _assert_bit_equal(got_img, want_img, f"{scene}/{algo} diagnostic image")
+    assert o.diag_stats()[:4] == want["stats"]
+    f32 = np.float32
+    n_groups = 0
+    for y in range(h):
+        for x in range(w):
+            wp = want["pixels"][y * w + x]
+            info, groups = o.diag_pixel(x, y)
+            assert bool(info["valid"]) == wp["valid"]
+            if not wp["valid"]:
+                continue
+            assert (int(info["sample_count"]), int(info["group_count"]), int(info["outlier_count"])) == \
+                (wp["samples"], wp["groups"], wp["outliers"]), (x, y)
+            assert f32(info["variance"]) == f32(wp["variance"])
+            assert [f32(v) for v in info["mean_rgb"]] == [f32(v) for v in wp["mean_rgb"]]
+            assert len(groups) == len(wp["top"])
+            for g, wg in zip(groups, wp["top"]):
+                d = int(g["depth"])
+                assert d == wg["depth"] and int(g["count"]) == wg["count"]
+                assert [int(v) for v in g["object_ids"][:d]] == wg["object_ids"]
+                assert int(g["coarse_type"]) == wg["coarse_type"]
+                assert ["BSDF", "NEE", "MIS_BSDF", "MIS_NEE"][int(g["strategy"])] == wg["strategy"]
+                assert [f32(v) for v in g["mean_rgb"]] == [f32(v) for v in wg["mean_rgb"]]
+                assert [f32(v) for v in g["variance_rgb"]] == [f32(v) for v in wg["variance_rgb"]]
+                assert f32(g["mean_luminance"]) == f32(wg["mean_luminance"])
+                assert g["positions"][:d].astype(np.float32).tolist() == \
+                    np.asarray(wg["positions"][1:], np.float32).tolist()
+                assert g["normals"][:d].astype(np.float32).tolist() == np.asarray(wg["normals"], np.float32).tolist()
+                n_groups += 1
+    assert n_groups > 0
+    r.disable_diagnostics()
