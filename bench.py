@@ -369,6 +369,26 @@ def guiding(device: int, budget_ms: float = 1000.0, width: int = 1280, height: i
     return out
 
 
+def guide_profile(device: int, calls: int) -> int:
+    """N guided renders of the hard-indirect room, 640x360, 4 spp per call,
+    mis, depth 8 (guide_config(2, 1e-2), guiding on): each call runs the
+    guide's inference, forward/backward and weight-gradient kernels once per
+    wave."""
+    import lucid_capi
+    import lucid_scenes as ls
+    scene, cam = ls.hard_indirect_scene()
+    c = lucid_capi.Context(device)
+    c.load_scene_json(ls.to_json(scene))
+    c.set_camera(*cam)
+    c.set_algorithm("mis")
+    c.guide_config(2, 1e-2)
+    c.guide_enable(True, 1)
+    for k in range(calls):
+        c.render(640, 360, 640, 360, 4, 4 * k, 8)
+    c.close()
+    return 0
+
+
 def run_reference(args, rank: int):
     if rank != 0:
         return 0
@@ -405,6 +425,9 @@ def main():
     ap.add_argument("--guide-budget-ms", type=float, default=1000.0)
     ap.add_argument("--guide-width", type=int, default=1280)
     ap.add_argument("--guide-height", type=int, default=720)
+    ap.add_argument("--guide-profile", type=int, default=0, metavar="N",
+                    help="only N guided 640x360 renders of the hard-indirect room (a target for ncu captures of "
+                         "the guide kernels); prints no bench line")
     ap.add_argument("--wave", type=int, default=0, help="paths per wave (0: the engine's default)")
     ap.add_argument("--width", type=int, default=W, help="smaller frames for profiling captures")
     ap.add_argument("--height", type=int, default=H)
@@ -417,6 +440,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank)
+    if args.guide_profile:
+        return guide_profile(int(os.environ.get("LOCAL_RANK", "0")), args.guide_profile)
     if args.guiding_only:
         print(json.dumps(guiding(int(os.environ.get("LOCAL_RANK", "0")), args.guide_budget_ms, args.guide_width,
                                  args.guide_height)), flush=True)

@@ -1,6 +1,8 @@
 // lucid_guide.cu — training of the path-guiding network (forward/backward
-// pass and split-K weight-gradient GEMMs on the tensor cores; Adam on FP32
-// masters).
+// pass, then every weight gradient as tcgen05 GEMMs over the records with
+// TMA-fed shared memory and TMEM accumulators; Adam on FP32 masters).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -138,37 +140,48 @@ __global__ void k_guide_coeff_sum(const GuideRec* recs, int n, float* sum) {
 // ---- training in two passes ---------------------------------------------------
 // Pass 1 (k_guide_fb): per warp tile of 16 records, forward, mixture
 // gradient and backpropagation through the layers; the layer inputs
-// (x, h1..h3) and the gradients of the layer outputs (d4..d1) go to a
-// per-record BF16 workspace row.  Pass 2 (k_guide_wgrad): every weight and
-// bias gradient, dW = D^T H and db = D^T 1, as one split-K GEMM over the
-// records: each block streams chunks of workspace rows into shared memory
-// with bulk async copies (double-buffered) and keeps its share of the
-// gradient in registers; the per-block partial gradients are summed by
-// k_guide_reduce in block order.
+// (x, h1..h3) and the gradients of the layer outputs (d4..d1) go to a BF16
+// workspace stored feature-major (one row of records per feature).  Pass 2
+// (k_guide_wgrad_tc): every weight and bias gradient, dW = D^T H and
+// db = D^T 1, as two tcgen05 GEMMs contracting over the records: TMA streams
+// 64-record chunks of the feature rows into swizzled shared memory, one
+// thread issues the MMAs into TMEM accumulators, and each block writes its
+// partial gradient; k_guide_reduce_tc sums the partials in block order.
 constexpr int kFbWarps = 14;
 constexpr size_t kFbSmem = sizeof(GuideSmemW) + kFbWarps * sizeof(TrainTile);
-// per-record offsets (BF16 elements) in a workspace row; every block starts
-// on a 16-byte boundary and the row (616 elements, 1232 bytes) is padded so
-// that eight consecutive rows fall in different shared-memory banks
-constexpr int kWsX = 0, kWsH1 = kGIn, kWsH2 = kWsH1 + kGHid, kWsH3 = kWsH2 + kGHid, kWsD4 = kWsH3 + kGHid,
-              kWsD3 = kWsD4 + kGOut, kWsD2 = kWsD3 + kGHid, kWsD1 = kWsD2 + kGHid, kWsRow = kWsD1 + kGHid + 8;
-static_assert(kWsRow * 2 % 16 == 0 && kWsH1 % 8 == 0 && kWsD4 % 8 == 0 && kWsD1 % 8 == 0, "workspace alignment");
+// Feature rows of the workspace, in the order the GEMMs read them:
+//   A_a = [d1 | d4] (112 rows)   B_a = [x | h3] (240 rows)
+//   A_b = [d2 | d3] (128 rows)   B_b = [h1 | h2] (128 rows)
+// GEMM a: rows 0..63 of A_a against rows 0..175 of B_a give dW1, rows 64..111
+// against rows 176..239 give dW4; GEMM b: d2 x h1 = dW2, d3 x h2 = dW3 (the
+// off-diagonal blocks are computed and discarded).  A ones row after each B
+// block gives the bias gradients in the same accumulators.
+constexpr int kTD1 = 0, kTD4 = kTD1 + kGHid, kTX = kTD4 + kGOut, kTH3 = kTX + kGIn, kTD2 = kTH3 + kGHid,
+              kTD3 = kTD2 + kGHid, kTH1 = kTD3 + kGHid, kTH2 = kTH1 + kGHid, kTFeat = kTH2 + kGHid;
+static_assert(kTD4 + kGOut == kTX && kTX - kTD1 == 112 && kTD2 - kTX == 240 && kTFeat == 608, "workspace rows");
 
-// Copies a 16-row tile (ld `ld` in shared memory) to rows r0.. of the
-// workspace column block at `dst` (16-byte vectors).
-LD void tile_store(const __nv_bfloat16* src, int ld, int cols, __nv_bfloat16* dst, int r0, int n) {
-    const int lane = threadIdx.x & 31, vec = cols / 8;
-    for (int e = lane; e < 16 * vec; e += 32) {
-        int r = e / vec, c = 8 * (e % vec);
-        if (r0 + r < n)
-            *reinterpret_cast<uint4*>(dst + (size_t)(r0 + r) * kWsRow + c) =
-                *reinterpret_cast<const uint4*>(src + r * ld + c);
+// Copies a 16-record tile (row r = record r0 + r, ld `ld` in shared memory)
+// into feature rows f0.. of the feature-major workspace (rcap records per
+// row): 8 records (16 bytes) per lane and store.
+LD void tile_store_t(const __nv_bfloat16* src, int ld, int cols, __nv_bfloat16* ws, int f0, int r0, int n, int rcap) {
+    const int lane = threadIdx.x & 31;
+    for (int e = lane; e < 2 * cols; e += 32) {
+        const int f = e >> 1, h = e & 1, rb = r0 + 8 * h;
+        __nv_bfloat16* dst = ws + (size_t)(f0 + f) * rcap + rb;
+        if (rb + 8 <= n) {
+            __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) v[k] = src[(8 * h + k) * ld + f];
+            *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(v);
+        } else {
+            for (int k = 0; k < 8 && rb + k < n; ++k) dst[k] = src[(8 * h + k) * ld + f];
+        }
     }
 }
 
 __global__ void __launch_bounds__(32 * kFbWarps) k_guide_fb(const GuideRec* recs, int n, const __nv_bfloat16* wq,
                                                            const float* master, const float* csum,
-                                                           __nv_bfloat16* ws) {
+                                                           __nv_bfloat16* ws, int rcap) {
     extern __shared__ __align__(16) unsigned char smem[];
     GuideSmemW& W = *reinterpret_cast<GuideSmemW*>(smem);
     TrainTile* tiles = reinterpret_cast<TrainTile*>(smem + sizeof(GuideSmemW));
@@ -189,7 +202,7 @@ __global__ void __launch_bounds__(32 * kFbWarps) k_guide_fb(const GuideRec* recs
         __syncwarp();
         tile_layer<kGIn, kGHid, kLdIn, kLdIn, true>(T.x, W.w1, W.b1, T.h1, nullptr);
         __syncwarp();
-        tile_store(T.x, kLdIn, kGIn, ws + kWsX, r0, n);
+        tile_store_t(T.x, kLdIn, kGIn, ws, kTX, r0, n, rcap);
         tile_layer<kGHid, kGHid, kLdH, kLdH, true>(T.h1, W.w2, W.b2, T.h2, nullptr);
         __syncwarp();
         tile_layer<kGHid, kGHid, kLdH, kLdH, true>(T.h2, W.w3, W.b3, T.h3, nullptr);
@@ -206,64 +219,40 @@ __global__ void __launch_bounds__(32 * kFbWarps) k_guide_fb(const GuideRec* recs
         __syncwarp();
         tile_backprop<kGOut, kGHid, kLdH, kLdH>(T.dout(), W.w4, T.h3, T.da());
         __syncwarp();
-        tile_store(T.h1, kLdH, kGHid, ws + kWsH1, r0, n);
-        tile_store(T.h2, kLdH, kGHid, ws + kWsH2, r0, n);
-        tile_store(T.h3, kLdH, kGHid, ws + kWsH3, r0, n);
-        tile_store(T.dout(), kLdH, kGOut, ws + kWsD4, r0, n);
-        tile_store(T.da(), kLdH, kGHid, ws + kWsD3, r0, n);
+        tile_store_t(T.h1, kLdH, kGHid, ws, kTH1, r0, n, rcap);
+        tile_store_t(T.h2, kLdH, kGHid, ws, kTH2, r0, n, rcap);
+        tile_store_t(T.h3, kLdH, kGHid, ws, kTH3, r0, n, rcap);
+        tile_store_t(T.dout(), kLdH, kGOut, ws, kTD4, r0, n, rcap);
+        tile_store_t(T.da(), kLdH, kGHid, ws, kTD3, r0, n, rcap);
         __syncwarp();
         tile_backprop<kGHid, kGHid, kLdH, kLdH>(T.da(), W.w3, T.h2, T.db());
         __syncwarp();
-        tile_store(T.db(), kLdH, kGHid, ws + kWsD2, r0, n);
+        tile_store_t(T.db(), kLdH, kGHid, ws, kTD2, r0, n, rcap);
         tile_backprop<kGHid, kGHid, kLdH, kLdH>(T.db(), W.w2, T.h1, T.da());
         __syncwarp();
-        tile_store(T.da(), kLdH, kGHid, ws + kWsD1, r0, n);
+        tile_store_t(T.da(), kLdH, kGHid, ws, kTD1, r0, n, rcap);
         __syncwarp();
     }
 }
 
-// Pass 2 work units: a 16 x 16 block of one weight gradient (two m16n8
-// fragments) or a 16-row block of one bias gradient (one fragment against a
-// column of ones).  Units 0..87 are the weight blocks (W1 44, W2 16, W3 16,
-// W4 12), units 88..102 the bias blocks (b1 4, b2 4, b3 4, b4 3).
-constexpr int kWgRows = 64, kWgWarps = 16, kWgUnits = 103, kWgMaxUnits = (kWgUnits + kWgWarps - 1) / kWgWarps;
-constexpr size_t kWgChunkBytes = (size_t)kWgRows * kWsRow * 2;
-constexpr size_t kWgSmem = 2 * kWgChunkBytes;
-constexpr long long kWgSpin = 1ll << 24;   // bound on the polls of one chunk's arrival
-
-struct WgUnit {
-    int a_off, b_off;   // workspace column of the A block (D^T) and B block (H^T); b_off < 0: bias
-    int goff, cols;     // gradient offset of the block's first element and the row length
-};
-LD WgUnit wg_unit(int u) {
-    // per layer: D column, H column, weight offset, bias offset, outputs, inputs
-    const int dcol[4] = {kWsD1, kWsD2, kWsD3, kWsD4}, hcol[4] = {kWsX, kWsH1, kWsH2, kWsH3};
-    const int wofs[4] = {kGW1, kGW2, kGW3, kGW4}, bofs[4] = {kGB1, kGB2, kGB3, kGB4};
-    const int outs[4] = {kGHid, kGHid, kGHid, kGOut}, ins[4] = {kGIn, kGHid, kGHid, kGHid};
-    WgUnit w{};
-    if (u < 88) {
-        int l = 0;
-        while (u >= (outs[l] / 16) * (ins[l] / 16)) { u -= (outs[l] / 16) * (ins[l] / 16); ++l; }
-        const int pb = ins[l] / 16, m0 = (u / pb) * 16, n0 = (u % pb) * 16;
-        w.a_off = dcol[l] + m0; w.b_off = hcol[l] + n0;
-        w.goff = wofs[l] + m0 * ins[l] + n0; w.cols = ins[l];
-    } else {
-        u -= 88;
-        int l = 0;
-        while (u >= outs[l] / 16) { u -= outs[l] / 16; ++l; }
-        w.a_off = dcol[l] + u * 16; w.b_off = -1;
-        w.goff = bofs[l] + u * 16; w.cols = 1;
-    }
-    return w;
-}
+// ---- pass 2: tcgen05 weight-gradient GEMMs ----------------------------------------
+// Each stage holds 64 records of every operand block, K-major with the
+// 128-byte swizzle TMA writes (one 128-byte row per feature, 8-row groups
+// 1024 bytes apart).  Rows past a block's TMA box are written once at
+// start: zeros, and a row of ones at B_a row 240 and B_b row 128.
+constexpr int kTcK = 64;                                     // records per stage
+constexpr int kTcNa = 256, kTcNb = 144;                      // GEMM N (B rows incl. ones row + zeros)
+constexpr unsigned kTcAa = 0, kTcBa = kTcAa + 128 * 128, kTcAb = kTcBa + kTcNa * 128, kTcBb = kTcAb + 128 * 128,
+                   kTcStage = kTcBb + kTcNb * 128;           // 83,968 bytes
+constexpr unsigned kTcTx = (112 + 240 + 128 + 128) * 128;     // TMA bytes per stage
+constexpr size_t kTcSmem = 2 * (size_t)kTcStage + 1024;      // two stages + alignment
+constexpr int kTcSlots = 128 * (kTcNa + kTcNb);              // partial floats per block
+constexpr unsigned kTcCols = 512;                            // TMEM columns allocated
+static_assert(kTcStage % 1024 == 0 && kTcBa % 1024 == 0 && kTcAb % 1024 == 0 && kTcBb % 1024 == 0, "1024-B stages");
+constexpr long long kWgSpin = 1ll << 24;   // bound on the polls of one barrier phase
 
 LD void mbar_init(unsigned bar, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count));
-}
-LD void bulk_load(unsigned dst, const void* src, unsigned bytes, unsigned bar) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
-                 ::"r"(dst), "l"(src), "r"(bytes), "r"(bar) : "memory");
 }
 // Polls the barrier's phase `parity` at most kWgSpin times; false if it
 // never completed.
@@ -277,116 +266,177 @@ LD bool mbar_wait(unsigned bar, unsigned parity) {
     }
     return false;
 }
+LD void tma_load_2d(unsigned dst, const CUtensorMap* map, int x, int y, unsigned bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n"
+        ::"r"(dst), "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(bar) : "memory");
+}
+// Shared-memory matrix descriptor (sm100): start address, leading offset
+// 16 B (unused by swizzled K-major layouts), 8-row groups 1024 B apart,
+// descriptor version 1, 128-byte swizzle.
+LD unsigned long long tc_desc(unsigned saddr) {
+    return (unsigned long long)((saddr >> 4) & 0x3FFFu) | (1ull << 16) | ((unsigned long long)(1024 >> 4) << 32) |
+           (1ull << 46) | (2ull << 61);
+}
+// Instruction descriptor, kind::f16: FP32 accumulate, BF16 A and B, both
+// K-major, N >> 3 at bit 17, M >> 4 at bit 24.
+constexpr unsigned tc_idesc(int m, int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(n >> 3) << 17) | ((unsigned)(m >> 4) << 24);
+}
+LD void tc_mma(unsigned d_tmem, unsigned long long a, unsigned long long b, unsigned idesc, unsigned acc) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+        ::"r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc) : "memory");
+}
+// The barrier's arrival once every tcgen05.mma this thread issued so far has
+// completed.
+LD void tc_commit(unsigned bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar)
+                 : "memory");
+}
+LD void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+LD void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+// 32 lanes x 16 consecutive columns of FP32 from TMEM (this warp's lanes).
+LD void tmem_ld16(unsigned taddr, float* v) {
+    unsigned r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15},"
+        " [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
 
-__global__ void __launch_bounds__(32 * kWgWarps, 1) k_guide_wgrad(const __nv_bfloat16* ws, int chunks, float* part,
-                                                                  int* flag) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ __align__(8) unsigned long long bars[2];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
-    const unsigned buf0 = smem_u32(smem), bar0 = smem_u32(&bars[0]);
+// One block per SM (its shared memory and 512 TMEM columns leave room for no
+// second one).  Warp 0 lane 0 feeds the stages by TMA, warp 1 lane 0 issues
+// the MMAs; all four warps then move the accumulators (TMEM lanes = GEMM
+// rows) to this block's partial, column-major so the stores coalesce.
+__global__ void __launch_bounds__(128, 1)
+    k_guide_wgrad_tc(const __grid_constant__ CUtensorMap m112, const __grid_constant__ CUtensorMap m240,
+                     const __grid_constant__ CUtensorMap m128, int chunks, float* part, int* flag) {
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ __align__(8) unsigned long long bars[5];   // full[2], empty[2], done
+    __shared__ unsigned tmem_base_s;
+    __shared__ int abort_s;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned base = (smem_u32(smem_raw) + 1023u) & ~1023u;
+    const unsigned full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[2]), done = smem_u32(&bars[4]);
+    const int iters = chunks > (int)blockIdx.x ? (chunks - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x : 0;
+
+    // constant rows of both stages: zeros, and the ones rows of the B blocks
+    unsigned char* gbase = smem_raw + (base - smem_u32(smem_raw));
+    for (int s = 0; s < 2; ++s) {
+        unsigned char* st = gbase + s * kTcStage;
+        for (int e = threadIdx.x; e < 3 * 16 * 8; e += blockDim.x) {   // 3 blocks x 16 rows x 8 vectors
+            const int blk = e / 128, row = (e / 8) % 16, vec = e % 8;
+            const unsigned off = blk == 0 ? kTcAa + (112 + row) * 128 : blk == 1 ? kTcBa + (240 + row) * 128
+                                                                                : kTcBb + (128 + row) * 128;
+            const unsigned one = row == 0 && blk > 0 ? 0x3F803F80u : 0u;   // BF16 1.0 pairs
+            *reinterpret_cast<uint4*>(st + off + vec * 16) = make_uint4(one, one, one, one);
+        }
+    }
     if (threadIdx.x == 0) {
-        mbar_init(bar0, 1);
-        mbar_init(bar0 + 8, 1);
-        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        for (int i = 0; i < 5; ++i) mbar_init(full0 + 8 * i, 1);
+        abort_s = 0;
     }
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");   // the MMAs read the rows written above
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"
+                     ::"r"(smem_u32(&tmem_base_s)), "r"(kTcCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+    }
+    tc_fence_before();
     __syncthreads();
-    // this warp's units
-    const int u_lo = warp * kWgUnits / kWgWarps, u_hi = (warp + 1) * kWgUnits / kWgWarps;
-    int a_off[kWgMaxUnits], b_off[kWgMaxUnits];
+    tc_fence_after();
+    const unsigned tmem = tmem_base_s;
+
+    if (warp == 0 && lane == 0) {
+        // producer
+        for (int it = 0; it < iters; ++it) {
+            const int s = it & 1;
+            if (it >= 2 && !mbar_wait(empty0 + 8 * s, ((it >> 1) - 1) & 1)) { abort_s = 1; break; }
+            if (*(volatile int*)&abort_s) break;
+            const int x = (blockIdx.x + it * gridDim.x) * kTcK;
+            const unsigned sb = base + s * kTcStage, fb = full0 + 8 * s;
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fb), "r"(kTcTx) : "memory");
+            tma_load_2d(sb + kTcAa, &m112, x, kTD1, fb);
+            tma_load_2d(sb + kTcBa, &m240, x, kTX, fb);
+            tma_load_2d(sb + kTcAb, &m128, x, kTD2, fb);
+            tma_load_2d(sb + kTcBb, &m128, x, kTH1, fb);
+        }
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer: D_a = A_a B_a^T in TMEM columns [0, 256), D_b in [256, 400)
+        const unsigned ida = tc_idesc(128, kTcNa), idb = tc_idesc(128, kTcNb);
+        for (int it = 0; it < iters; ++it) {
+            const int s = it & 1;
+            if (!mbar_wait(full0 + 8 * s, (it >> 1) & 1)) { abort_s = 1; break; }
+            tc_fence_after();
+            const unsigned sb = base + s * kTcStage;
+            const unsigned long long da = tc_desc(sb + kTcAa), db = tc_desc(sb + kTcBa), dc = tc_desc(sb + kTcAb),
+                                     dd = tc_desc(sb + kTcBb);
 #pragma unroll
-    for (int j = 0; j < kWgMaxUnits; ++j) {
-        WgUnit w = wg_unit(min(u_lo + j, kWgUnits - 1));
-        a_off[j] = w.a_off; b_off[j] = w.b_off;
-    }
-    float acc[kWgMaxUnits][8];
-#pragma unroll
-    for (int j = 0; j < kWgMaxUnits; ++j)
-#pragma unroll
-        for (int i = 0; i < 8; ++i) acc[j][i] = 0.0f;
-    // ldmatrix row addresses: A = D^T blocks (matrices k0|m0, k0|m0+8,
-    // k0+8|m0, k0+8|m0+8), B = H^T blocks (k0|n0, k0+8|n0, k0|n0+8, k0+8|n0+8)
-    const int mi = lane >> 3, ri = lane & 7;
-    const int a_lane = (ri + ((mi >> 1) << 3)) * kWsRow + ((mi & 1) << 3);
-    const int b_lane = (ri + ((mi & 1) << 3)) * kWsRow + ((mi >> 1) << 3);
-    const unsigned ones = pack_bf16(1.0f, 1.0f);
-    bool ok = true;
-    if (threadIdx.x == 0 && (int)blockIdx.x < chunks)
-        bulk_load(buf0, ws + (size_t)blockIdx.x * kWgRows * kWsRow, (unsigned)kWgChunkBytes, bar0);
-    int it = 0;
-    for (int c = blockIdx.x; c < chunks; c += gridDim.x, ++it) {
-        const int b = it & 1;
-        const int nxt = c + gridDim.x;
-        if (threadIdx.x == 0 && nxt < chunks)
-            bulk_load(buf0 + (unsigned)((b ^ 1) * kWgChunkBytes), ws + (size_t)nxt * kWgRows * kWsRow,
-                      (unsigned)kWgChunkBytes, bar0 + 8 * (b ^ 1));
-        ok = mbar_wait(bar0 + 8 * b, (it >> 1) & 1);
-        if (!__syncthreads_and(ok)) break;
-        const unsigned base = buf0 + (unsigned)(b * kWgChunkBytes);
-#pragma unroll
-        for (int ks = 0; ks < kWgRows; ks += 16) {
-            const unsigned kb = base + 2u * (unsigned)(ks * kWsRow);
-            int a_cur = -1;
-            unsigned a[4] = {0, 0, 0, 0};
-#pragma unroll
-            for (int j = 0; j < kWgMaxUnits; ++j) {
-                if (u_lo + j < u_hi) {
-                    if (a_off[j] != a_cur) {
-                        ldsm_x4_trans(kb + 2u * (unsigned)(a_lane + a_off[j]), a);
-                        a_cur = a_off[j];
-                    }
-                    if (b_off[j] >= 0) {
-                        unsigned bb[4];
-                        ldsm_x4_trans(kb + 2u * (unsigned)(b_lane + b_off[j]), bb);
-                        mma16816(acc[j], a, bb);
-                        mma16816(acc[j] + 4, a, bb + 2);
-                    } else {
-                        const unsigned bo[2] = {ones, ones};
-                        mma16816(acc[j], a, bo);
-                    }
-                }
+            for (int k = 0; k < kTcK / 16; ++k) {   // 16 records (32 bytes) per MMA
+                const unsigned acc = (it > 0 || k > 0) ? 1u : 0u;
+                tc_mma(tmem, da + 2 * k, db + 2 * k, ida, acc);
+                tc_mma(tmem + kTcNa, dc + 2 * k, dd + 2 * k, idb, acc);
             }
+            tc_commit(empty0 + 8 * s);
         }
-        __syncthreads();
+        tc_commit(done);
     }
-    if (!ok) {
-        // give the copies still in flight (this chunk's, the prefetched
-        // one's) a bounded time to land before the shared memory goes away
-        if (threadIdx.x == 0) {
-            atomicExch(flag, 1);
-            const int c = blockIdx.x + it * gridDim.x;
-            mbar_wait(bar0 + 8 * (it & 1), (it >> 1) & 1);
-            if (c + (int)gridDim.x < chunks) mbar_wait(bar0 + 8 * ((it + 1) & 1), ((it + 1) >> 1) & 1);
-        }
-        return;
-    }
-    float* dst = part + (size_t)blockIdx.x * kGParams;
+    __syncwarp();
+    // epilogue: every thread waits for the last MMAs (bounded)
+    const bool ok = __all_sync(0xffffffffu, mbar_wait(done, 0) && !*(volatile int*)&abort_s);
+    tc_fence_after();
+    if (ok && iters > 0) {
+        float* dst = part + (size_t)blockIdx.x * kTcSlots + warp * 32 + lane;
+        const unsigned lane_base = tmem + ((unsigned)(warp * 32) << 16);
+        for (int c0 = 0; c0 < kTcNa + kTcNb; c0 += 16) {
+            float v[16];
+            tmem_ld16(lane_base + (unsigned)c0, v);
 #pragma unroll
-    for (int j = 0; j < kWgMaxUnits; ++j) {
-        if (u_lo + j < u_hi) {
-            const WgUnit w = wg_unit(u_lo + j);
-            if (w.b_off >= 0) {
-                float* o = dst + w.goff;
-                o[g * w.cols + 2 * q] = acc[j][0];
-                o[g * w.cols + 2 * q + 1] = acc[j][1];
-                o[(g + 8) * w.cols + 2 * q] = acc[j][2];
-                o[(g + 8) * w.cols + 2 * q + 1] = acc[j][3];
-                o[g * w.cols + 8 + 2 * q] = acc[j][4];
-                o[g * w.cols + 8 + 2 * q + 1] = acc[j][5];
-                o[(g + 8) * w.cols + 8 + 2 * q] = acc[j][6];
-                o[(g + 8) * w.cols + 8 + 2 * q + 1] = acc[j][7];
-            } else if (q == 0) {
-                dst[w.goff + g] = acc[j][0];
-                dst[w.goff + g + 8] = acc[j][2];
-            }
+            for (int i = 0; i < 16; ++i) dst[(size_t)(c0 + i) * 128] = v[i];
         }
+    } else if (threadIdx.x == 0) {
+        atomicExch(flag, 1);
+    }
+    if (!ok && threadIdx.x == 0) {
+        // give the loads still in flight a bounded time to land before the
+        // shared memory goes away
+        for (int s = 0; s < 2; ++s) mbar_wait(full0 + 8 * s, 0), mbar_wait(full0 + 8 * s, 1);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kTcCols));
     }
 }
 
-// grad[i] += sum over blocks of part[block][i], in block order.
-__global__ void k_guide_reduce(const float* part, int blocks, float* grad) {
+// Slot of parameter i in a block's partial: D_a(row, col) at col * 128 + row
+// (cols 0..255), D_b(row, col) at 128 * 256 + col * 128 + row.
+LD int tc_slot(int i) {
+    constexpr int Db = 128 * kTcNa;
+    if (i < kGB1) return (i % kGIn) * 128 + i / kGIn;                                     // W1: D_a(o, x)
+    if (i < kGW2) return 240 * 128 + (i - kGB1);                                          // b1: D_a(o, ones)
+    if (i < kGB2) { const int j = i - kGW2; return Db + (j % kGHid) * 128 + j / kGHid; }  // W2: D_b(o, h1)
+    if (i < kGW3) return Db + 128 * 128 + (i - kGB2);                                     // b2: D_b(o, ones)
+    if (i < kGB3) { const int j = i - kGW3; return Db + (64 + j % kGHid) * 128 + 64 + j / kGHid; }   // W3
+    if (i < kGW4) return Db + 128 * 128 + 64 + (i - kGB3);                                // b3
+    if (i < kGB4) { const int j = i - kGW4; return (kGIn + j % kGHid) * 128 + 64 + j / kGHid; }      // W4
+    return 240 * 128 + 64 + (i - kGB4);                                                    // b4
+}
+
+// grad[i] += sum over blocks of the block partials, in block order.
+__global__ void k_guide_reduce_tc(const float* part, int blocks, float* grad) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kGParams; i += gridDim.x * blockDim.x) {
+        const int slot = tc_slot(i);
         float s = 0.0f;
-        for (int b = 0; b < blocks; ++b) s += part[(size_t)b * kGParams + i];
+        for (int b = 0; b < blocks; ++b) s += part[(size_t)b * kTcSlots + slot];
         grad[i] += s;
     }
 }
@@ -512,6 +562,35 @@ int GuideNet::get_params(float* w, cudaStream_t st) {
     return 0;
 }
 
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime
+// (no link-time dependency on libcuda).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// 2-D map over the feature-major workspace: n records (x, innermost) by
+// kTFeat feature rows (y), rows rcap records apart; boxes of 64 records by
+// `rows` features, 128-byte swizzle; records past n read as zeros.
+static bool workspace_map(CUtensorMap* m, void* ws, int n, int rcap, int rows) {
+    auto enc = tensor_map_encoder();
+    if (!enc) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)n, (cuuint64_t)kTFeat};
+    cuuint64_t strides[1] = {(cuuint64_t)rcap * sizeof(__nv_bfloat16)};
+    cuuint32_t box[2] = {(cuuint32_t)kTcK, (cuuint32_t)rows};
+    cuuint32_t estr[2] = {1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, ws, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 int GuideNet::gradient(const GuideRec* recs, int n, cudaStream_t st) {
     GCK(cudaMemsetAsync(csum_, 0, sizeof(float), st));
     if (n <= 0) return 0;
@@ -522,29 +601,35 @@ int GuideNet::gradient(const GuideRec* recs, int n, cudaStream_t st) {
     static bool attr = false;
     if (!attr) {
         GCK(cudaFuncSetAttribute(k_guide_fb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFbSmem));
-        GCK(cudaFuncSetAttribute(k_guide_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWgSmem));
+        GCK(cudaFuncSetAttribute(k_guide_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
         attr = true;
     }
-    // workspace rows for whole chunks; rows past n stay zero
-    const int chunks = (n + kWgRows - 1) / kWgRows, rows = chunks * kWgRows;
+    // feature rows of whole 64-record chunks (the GEMM reads records past n
+    // as zeros through the tensor map)
+    const int chunks = (n + kTcK - 1) / kTcK, rcap_need = chunks * kTcK;
     const int wblocks = std::min(chunks, sms);
-    if (ws_rows_ < rows || part_blocks_ < wblocks) {
+    if (ws_rows_ < rcap_need || part_blocks_ < sms) {
         if (ws_) cudaFree(ws_);
         if (part_) cudaFree(part_);
         ws_ = nullptr;
         part_ = nullptr;
         ws_rows_ = part_blocks_ = 0;
-        GCK(cudaMalloc(&ws_, (size_t)rows * kWsRow * sizeof(__nv_bfloat16)));
-        GCK(cudaMalloc(&part_, (size_t)sms * kGParams * sizeof(float)));
-        ws_rows_ = rows;
+        GCK(cudaMalloc(&ws_, (size_t)kTFeat * rcap_need * sizeof(__nv_bfloat16)));
+        GCK(cudaMalloc(&part_, (size_t)sms * kTcSlots * sizeof(float)));
+        ws_rows_ = rcap_need;
         part_blocks_ = sms;
     }
-    __nv_bfloat16* ws = WQ(ws_);
-    if (rows > n) GCK(cudaMemsetAsync(ws + (size_t)n * kWsRow, 0, (size_t)(rows - n) * kWsRow * sizeof(__nv_bfloat16), st));
+    const int rcap = ws_rows_;
+    CUtensorMap m112, m240, m128;
+    if (!workspace_map(&m112, ws_, n, rcap, 112) || !workspace_map(&m240, ws_, n, rcap, 240) ||
+        !workspace_map(&m128, ws_, n, rcap, 128)) {
+        err_ = "guide training: cuTensorMapEncodeTiled failed for the workspace";
+        return -6;
+    }
     int blocks = std::max(1, std::min(sms, (n + 16 * kFbWarps - 1) / (16 * kFbWarps)));
-    k_guide_fb<<<blocks, 32 * kFbWarps, kFbSmem, st>>>(recs, n, WQ(wq_), master_, csum_, ws);
-    k_guide_wgrad<<<wblocks, 32 * kWgWarps, kWgSmem, st>>>(ws, chunks, part_, flag_);
-    k_guide_reduce<<<(kGParams + 255) / 256, 256, 0, st>>>(part_, wblocks, grad_);
+    k_guide_fb<<<blocks, 32 * kFbWarps, kFbSmem, st>>>(recs, n, WQ(wq_), master_, csum_, WQ(ws_), rcap);
+    k_guide_wgrad_tc<<<wblocks, 128, kTcSmem, st>>>(m112, m240, m128, chunks, part_, flag_);
+    k_guide_reduce_tc<<<(kGParams + 255) / 256, 256, 0, st>>>(part_, wblocks, grad_);
     GCK(cudaGetLastError());
     return 0;
 }

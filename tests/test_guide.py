@@ -153,3 +153,32 @@ def test_gpu_adam_step_matches_fp64(guide):
     np.testing.assert_allclose(after, want, rtol=1e-5, atol=1e-4)
     # a step against its own gradient lowers the loss
     assert go.loss(after.astype(np.float64), recs) < go.loss(theta.astype(np.float64), recs)
+
+
+@pytest.mark.gpu
+def test_gpu_gradient_over_many_chunks_and_a_ragged_tail(guide):
+    """The weight-gradient GEMMs stream 64-record chunks through a two-stage
+    pipeline, several chunks per block: 65,573 records (1,025 chunks, the
+    last one 37 records long and read as zeros past its end) against the FP64
+    gradient, and the sum of two calls equals one call on the concatenation."""
+    lib, h = guide
+    rng = np.random.default_rng(8)
+    theta = rng.normal(0, 0.15, go.N_PARAMS).astype(np.float32)
+    assert lib.lucid_guide_set_params(h, theta.ctypes.data, theta.size) == 0
+    tq = go.bf16_weights(theta)
+    recs = go.coherent_records(rng, 65573).astype(np.float32)
+    g = np.zeros(go.N_PARAMS, np.float32)
+    assert lib.lucid_guide_gradient(h, recs.ctypes.data, len(recs), g.ctypes.data) == 0
+    ref = go.gradient(tq, recs.astype(np.float64), bf16_inputs=True)
+    o = 0
+    for name, shape in go.SHAPES:
+        n = int(np.prod(shape))
+        t = RTOL_BF16_W1 if name in ("W1", "b1") else RTOL_BF16
+        assert _rel(g[o:o + n], ref[o:o + n]) < t, (name, t)
+        o += n
+    # 37 records alone: one ragged chunk
+    small = np.ascontiguousarray(recs[:37])
+    gs = np.zeros(go.N_PARAMS, np.float32)
+    assert lib.lucid_guide_gradient(h, small.ctypes.data, 37, gs.ctypes.data) == 0
+    refs = go.gradient(tq, small.astype(np.float64), bf16_inputs=True)
+    assert _rel(gs, refs) < 0.1
