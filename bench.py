@@ -361,11 +361,32 @@ def guiding(device: int, budget_ms: float = 1000.0, width: int = 1280, height: i
         out["guided" if guided else "plain"] = {"relmse": lq.relmse(lq.mean_image(acc, k * spp), ref),
                                                 "spp": k * spp, "device_ms": ms}
     out["training_steps"] = c.guide_steps()
+    # the fit of the trained guide at probe points on camera-visible surfaces
+    # (camera hits are the guided vertices): KL of the guide and of cosine
+    # sampling against the incident radiance rendered in FP64 at the probe
+    import lucid_guide_probe as lgp
+    eye = np.asarray(cam[:3], np.float64)
+    probes = {"floor, middle of the room": ((4.0, 0.0, 6.0), (0.0, 1.0, 0.0)),
+              "floor, 1.5 m from the door gap": ((10.5, 0.0, 6.5), (0.0, 1.0, 0.0)),
+              "floor, far corner": ((6.0, 0.0, 10.5), (0.0, 1.0, 0.0)),
+              "side wall z = 12": ((8.0, 1.5, 12.0), (0.0, 0.0, -1.0))}
+    out["probes"] = {}
+    weights, box = c.guide_params()
     c.guide_enable(False, 0)
+    for name, (pp, nn) in probes.items():
+        r = lgp.probe(c, weights, box, pp, nn, eye - np.asarray(pp), res=32, spp=256, max_depth=D)
+        out["probes"][name] = {k: round(v, 4) for k, v in r.items()}
+    c.set_camera(*cam)
     c.close()
+    # the reference's own noise is in both relMSEs: relMSE falls as 1/spp, so
+    # the reference (4096 spp) adds about plain * spp_plain / 4096 to each
+    floor = out["plain"]["relmse"] * out["plain"]["spp"] / lq.REFERENCE_SPP
     out.update({"scene": f"hard-indirect room, 20,828 triangles, {W}x{H}, mis, depth 8",
                 "reference": f"FP64-accumulated {lq.REFERENCE_SPP} spp on the GPU", "reference_s": round(ref_s, 2),
-                "equal_time_relmse_ratio": out["guided"]["relmse"] / out["plain"]["relmse"]})
+                "equal_time_relmse_ratio": out["guided"]["relmse"] / out["plain"]["relmse"],
+                "reference_noise_relmse": floor,
+                "equal_time_relmse_ratio_less_reference_noise":
+                    (out["guided"]["relmse"] - floor) / (out["plain"]["relmse"] - floor)})
     return out
 
 

@@ -355,6 +355,11 @@ int lucid_cuda_guide_max_depth(LucidCudaCtx* ctx, int max_depth) {
     return guarded(ctx, [&](lucid::Engine& e) { return e.guide_max_depth(max_depth); });
 }
 
+int lucid_cuda_guide_params(LucidCudaCtx* ctx, float* out, size_t cap, float* box6) {
+    if (!out) return LUCID_ERR_INVALID;
+    return guarded(ctx, [&](lucid::Engine& e) { return e.guide_params(out, cap, box6); });
+}
+
 int lucid_cuda_guide_steps(LucidCudaCtx* ctx) {
     return guarded(ctx, [&](lucid::Engine& e) { return e.guide_steps(); });
 }

@@ -2841,6 +2841,17 @@ int Engine::guide_enable(bool on, int seed) {
 
 int Engine::guide_steps() const { return guide_ ? guide_->net.steps() : 0; }
 
+int Engine::guide_params(float* out, size_t cap, float* box6) {
+    GpuLock gl(*this);
+    if (!guide_) return fail(LUCID_ERR_INVALID, "guide: not enabled on this context");
+    if (cap < (size_t)kGuideParams) return fail(LUCID_ERR_INVALID, "guide: output buffer too small");
+    CK(cudaSetDevice(device_));
+    if (guide_->net.get_params(out, S(stream_)) != 0) return fail(LUCID_ERR_CUDA, guide_->net.error());
+    if (box6)
+        for (int k = 0; k < 3; ++k) { box6[k] = scene_lo_[k]; box6[3 + k] = scene_hi_[k]; }
+    return kGuideParams;
+}
+
 int Engine::guide_config(int steps_per_wave, float lr) {
     GpuLock gl(*this);
     if (steps_per_wave < 1 || steps_per_wave > 64 || !(lr > 0.0f)) return fail(LUCID_ERR_INVALID, "guide: bad config");

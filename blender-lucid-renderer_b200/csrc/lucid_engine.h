@@ -62,6 +62,7 @@ public:
     int guide_steps() const;
     int guide_config(int steps_per_wave, float lr);
     int guide_max_depth(int max_depth);
+    int guide_params(float* out, size_t cap, float* box6);
     // Uses `owner`'s uploaded scene (BVH, materials, lights) without a copy.
     int share_scene(Engine& owner);
     // Progressive jobs (the request loop's unit of work).

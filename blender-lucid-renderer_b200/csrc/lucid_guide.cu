@@ -160,21 +160,31 @@ constexpr int kTD1 = 0, kTD4 = kTD1 + kGHid, kTX = kTD4 + kGOut, kTH3 = kTX + kG
               kTD3 = kTD2 + kGHid, kTH1 = kTD3 + kGHid, kTH2 = kTH1 + kGHid, kTFeat = kTH2 + kGHid;
 static_assert(kTD4 + kGOut == kTX && kTX - kTD1 == 112 && kTD2 - kTX == 240 && kTFeat == 608, "workspace rows");
 
-// Copies a 16-record tile (row r = record r0 + r, ld `ld` in shared memory)
-// into feature rows f0.. of the feature-major workspace (rcap records per
-// row): 8 records (16 bytes) per lane and store.
+// Copies a 16-record tile (row r = record r0 + r, ld `ld` in shared memory,
+// ld and cols even) into feature rows f0.. of the feature-major workspace
+// (rcap records per row).  Each lane takes two features of 8 records: eight
+// 32-bit reads of feature pairs, regrouped by byte permutes into one 16-byte
+// vector per feature.
 LD void tile_store_t(const __nv_bfloat16* src, int ld, int cols, __nv_bfloat16* ws, int f0, int r0, int n, int rcap) {
     const int lane = threadIdx.x & 31;
-    for (int e = lane; e < 2 * cols; e += 32) {
-        const int f = e >> 1, h = e & 1, rb = r0 + 8 * h;
-        __nv_bfloat16* dst = ws + (size_t)(f0 + f) * rcap + rb;
-        if (rb + 8 <= n) {
-            __align__(16) __nv_bfloat16 v[8];
+    for (int e = lane; e < cols; e += 32) {   // cols / 2 feature pairs x 2 record halves
+        const int f = 2 * (e >> 1), h = e & 1, rb = r0 + 8 * h;
+        const unsigned* s32 = reinterpret_cast<const unsigned*>(src + 8 * h * ld + f);
+        unsigned w[8];
 #pragma unroll
-            for (int k = 0; k < 8; ++k) v[k] = src[(8 * h + k) * ld + f];
-            *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(v);
+        for (int k = 0; k < 8; ++k) w[k] = s32[k * (ld >> 1)];
+        __nv_bfloat16* d0 = ws + (size_t)(f0 + f) * rcap + rb;
+        __nv_bfloat16* d1 = d0 + rcap;
+        if (rb + 8 <= n) {
+            *reinterpret_cast<uint4*>(d0) = make_uint4(__byte_perm(w[0], w[1], 0x5410), __byte_perm(w[2], w[3], 0x5410),
+                                                       __byte_perm(w[4], w[5], 0x5410), __byte_perm(w[6], w[7], 0x5410));
+            *reinterpret_cast<uint4*>(d1) = make_uint4(__byte_perm(w[0], w[1], 0x7632), __byte_perm(w[2], w[3], 0x7632),
+                                                       __byte_perm(w[4], w[5], 0x7632), __byte_perm(w[6], w[7], 0x7632));
         } else {
-            for (int k = 0; k < 8 && rb + k < n; ++k) dst[k] = src[(8 * h + k) * ld + f];
+            for (int k = 0; k < 8 && rb + k < n; ++k) {
+                d0[k] = src[(8 * h + k) * ld + f];
+                d1[k] = src[(8 * h + k) * ld + f + 1];
+            }
         }
     }
 }

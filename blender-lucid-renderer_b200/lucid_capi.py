@@ -269,6 +269,7 @@ SIGNATURES = {
     "lucid_cuda_guide_steps": (_I, [_P]),
     "lucid_cuda_guide_config": (_I, [_P, _I, ctypes.c_float]),
     "lucid_cuda_guide_max_depth": (_I, [_P, _I]),
+    "lucid_cuda_guide_params": (_I, [_P, _P, ctypes.c_size_t, _P]),
     "lucid_cuda_cancel": (_I, [_P]),
     "lucid_cuda_is_cancelled": (_I, [_P]),
     "lucid_cuda_reset_cancel": (_I, [_P]),
@@ -473,6 +474,14 @@ class Context:
 
     def guide_max_depth(self, max_depth: int = 1):
         self._check(self.lib.lucid_cuda_guide_max_depth(self.h, max_depth))
+
+    def guide_params(self):
+        """(FP32 weights, scene box (lo, hi)) of this context's guide network."""
+        n = self.lib.lucid_guide_num_params()
+        w = np.zeros(n, np.float32)
+        box = np.zeros(6, np.float32)
+        self._count(self.lib.lucid_cuda_guide_params(self.h, w.ctypes.data, w.size, box.ctypes.data))
+        return w, (box[:3].copy(), box[3:].copy())
 
     def guide_steps(self) -> int:
         return self._count(self.lib.lucid_cuda_guide_steps(self.h))

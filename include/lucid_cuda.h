@@ -517,6 +517,11 @@ int lucid_cuda_guide_config(LucidCudaCtx* ctx, int steps_per_wave, float lr);
  * hard-indirect test room); deeper vertices sample the BSDF as without
  * guiding but still credit radiance to the guided vertices before them. */
 int lucid_cuda_guide_max_depth(LucidCudaCtx* ctx, int max_depth);
+/* The context's guide network as trained so far: its FP32 master weights
+ * (out: cap >= lucid_guide_num_params() floats, the layout lucid_guide_*
+ * uses) and the scene box its position encoding maps to [0,1]^3 (box6: lo
+ * x y z, hi x y z; may be NULL).  Returns the number of weights copied. */
+int lucid_cuda_guide_params(LucidCudaCtx* ctx, float* out, size_t cap, float* box6);
 
 /* ---- cancellation ---------------------------------------------------- */
 /* Replaces PyRenderer::cancel / is_cancelled / reset_cancel
