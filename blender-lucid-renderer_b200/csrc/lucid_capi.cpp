@@ -293,6 +293,10 @@ int lucid_server_add_scene_arrays(LucidServer* srv, const LucidSceneDesc* scene,
     return server_guarded(srv, [&](lucid::Server& s) { return s.add_scene_arrays(*scene, scene_id); });
 }
 
+int lucid_server_update_scene(LucidServer* srv, int scene_id, const LucidSceneEdit* edits, int count) {
+    return server_guarded(srv, [&](lucid::Server& s) { return s.update_scene(scene_id, edits, count); });
+}
+
 int lucid_server_submit(LucidServer* srv, const LucidJobDesc* job, int* job_id) {
     if (!job || !job_id) return LUCID_ERR_INVALID;
     return server_guarded(srv, [&](lucid::Server& s) { return s.submit(*job, job_id); });
@@ -353,6 +357,10 @@ int lucid_cuda_guide_config(LucidCudaCtx* ctx, int steps_per_wave, float lr) {
 
 int lucid_cuda_guide_max_depth(LucidCudaCtx* ctx, int max_depth) {
     return guarded(ctx, [&](lucid::Engine& e) { return e.guide_max_depth(max_depth); });
+}
+
+int lucid_cuda_update_scene(LucidCudaCtx* ctx, const LucidSceneEdit* edits, int count) {
+    return guarded(ctx, [&](lucid::Engine& e) { return e.update_scene(edits, count); });
 }
 
 int lucid_cuda_guide_params(LucidCudaCtx* ctx, float* out, size_t cap, float* box6) {

@@ -73,7 +73,11 @@ struct DeviceScene {
     DBuf<float> cdf, grid;
     DBuf<DevVolume> volumes;
     DevScene view{};
+    // an edited version (Engine::update_scene) owns only its material, light
+    // and class arrays and keeps the version whose geometry it renders alive
+    std::shared_ptr<DeviceScene> base;
     void release() {
+        base.reset();
         bvh_tris.release(); bnd_tris.release(); big_tris.release(); prim_fn.release(); prim_vn.release(); prim_info.release();
         prim_cls.release(); nodes.release(); nodes2.release(); guide.release(); materials.release(); tex_ops.release(); prim_uv.release(); lights.release(); cdf.release(); grid.release(); volumes.release();
     }
@@ -1691,6 +1695,7 @@ Engine::~Engine() {
     cudaSetDevice(device_);
     if (async_acc_) cudaFree(async_acc_);
     if (async_pinned_) cudaFreeHost(async_pinned_);
+    if (jacc_) cudaFree(jacc_);
     job_end();
     delete guide_;
     ds_.reset();   // the device scene is freed with its last sharing engine
@@ -1765,22 +1770,71 @@ int Engine::ensure_stream() {
 }
 
 int Engine::share_scene(Engine& owner) {
-    std::shared_ptr<DeviceScene> ds;
-    int stats[8];
-    {
-        GpuLock ol(owner);
-        if (!owner.scene_loaded_) return fail(LUCID_ERR_NO_SCENE, "the sharing source has no scene");
-        ds = owner.ds_;
-        owner.scene_stats_locked(stats);
-    }
+    SceneSnapshot snap;
+    int rc = owner.snapshot_scene(snap);
+    if (rc != LUCID_OK) return fail(rc, owner.last_error());
+    return use_snapshot(snap);
+}
+
+int Engine::snapshot_scene(SceneSnapshot& out) {
+    GpuLock gl(*this);
+    if (!scene_loaded_) return fail(LUCID_ERR_NO_SCENE, "the sharing source has no scene");
+    out.ds = ds_;
+    scene_stats_locked(out.stats);
+    for (int k = 0; k < 3; ++k) { out.lo[k] = scene_lo_[k]; out.hi[k] = scene_hi_[k]; }
+    return LUCID_OK;
+}
+
+int Engine::use_snapshot(const SceneSnapshot& snap) {
+    if (!snap.ds) return fail(LUCID_ERR_NO_SCENE, "empty scene snapshot");
     GpuLock gl(*this);
     CK(cudaSetDevice(device_));
     int rc = ensure_stream();
     if (rc != LUCID_OK) return rc;
-    ds_ = ds;
-    std::memcpy(shared_stats_, stats, sizeof(stats));
+    ds_ = snap.ds;
+    std::memcpy(shared_stats_, snap.stats, sizeof(shared_stats_));
+    for (int k = 0; k < 3; ++k) { scene_lo_[k] = snap.lo[k]; scene_hi_[k] = snap.hi[k]; }
     shared_ = true;
     scene_loaded_ = true;
+    return LUCID_OK;
+}
+
+// A new scene version: the edited materials, lights, light CDF and guide,
+// and per-prim shading classes in buffers of its own; the BVH, triangles and
+// everything else are the current version's, which it keeps alive.  Engines
+// rendering the current version keep it until they take the new one.
+int Engine::update_scene(const LucidSceneEdit* edits, int count) {
+    GpuLock gl(*this);
+    if (!scene_loaded_) return fail(LUCID_ERR_NO_SCENE, "no scene loaded");
+    if (shared_) return fail(LUCID_ERR_INVALID, "this context renders a scene it does not own; edit the owner");
+    CK(cudaSetDevice(device_));
+    std::string err;
+    if (!apply_scene_edits(host_, edits, count, err)) return fail(LUCID_ERR_INVALID, err);
+    const HostScene& H = host_;
+    std::vector<unsigned char> cls(H.prim_info.size());
+    for (size_t p = 0; p < cls.size(); ++p) cls[p] = prim_shading_class(H.materials[H.prim_info[p].x]);
+    auto nv = std::make_shared<DeviceScene>();
+    cudaStream_t st = S(stream_);
+    auto up = [&](auto& buf, const auto& vec) -> cudaError_t {
+        cudaError_t e = buf.alloc(vec.size());
+        if (e != cudaSuccess || vec.empty()) return e;
+        return cudaMemcpyAsync(buf.p, vec.data(), vec.size() * sizeof(vec[0]), cudaMemcpyHostToDevice, st);
+    };
+    CK(up(nv->materials, H.materials));
+    CK(up(nv->lights, H.lights));
+    CK(up(nv->cdf, H.cdf));
+    CK(up(nv->guide, H.light_guide));
+    CK(up(nv->prim_cls, cls));
+    CK(cudaStreamSynchronize(st));   // complete before any other stream reads the version
+    nv->view = ds_->view;
+    nv->view.materials = nv->materials.p;
+    nv->view.lights = nv->lights.p;
+    nv->view.light_cdf = nv->cdf.p;
+    nv->view.light_guide = nv->guide.p;
+    nv->view.prim_cls = nv->prim_cls.p;
+    nv->view.total_light_area = H.total_light_area;
+    nv->base = ds_;
+    ds_ = nv;
     return LUCID_OK;
 }
 
@@ -1834,11 +1888,7 @@ int Engine::upload_scene(HostScene&& hs) {
     // each prim's shading class for a surface hit (the material part of
     // bin_class, decided once here instead of per hit)
     std::vector<unsigned char> cls(H.prim_info.size());
-    for (size_t p = 0; p < cls.size(); ++p) {
-        const DevMaterial& dm = H.materials[H.prim_info[p].x];
-        const float rough = dm.rough_trans_ior_flags.x, trans = dm.rough_trans_ior_flags.y, metal = dm.albedo_metallic.w;
-        cls[p] = dm.emission.w != 0.0f ? 1 : trans > 0.5f ? 2 : (metal > 0.5f && rough < 0.05f) ? 3 : (metal > 0.5f ? 4 : 5);
-    }
+    for (size_t p = 0; p < cls.size(); ++p) cls[p] = prim_shading_class(H.materials[H.prim_info[p].x]);
     CK(up(D.bnd_tris, bnd));
     CK(up(D.prim_info, H.prim_info));
     CK(up(D.prim_cls, cls));
@@ -3051,6 +3101,73 @@ int Engine::job_output(float* out_host) {
     CK(cudaMemcpyAsync(out_host, pool_->out.p, (size_t)np * sizeof(float4), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     return LUCID_OK;
+}
+
+long long Engine::guide_job_bytes(long long paths) {
+    // per path: compact mixture (40 floats), slot and inverse-throughput
+    // entries; fixed: two batches of records, the feature-major training
+    // workspace and the per-block partial gradients
+    return paths * (kGMixFloats * 4 + 16 + 48) + 2LL * kGuideBatch * (long long)sizeof(GuideRec) +
+           608LL * kGuideBatch * 2 + 148LL * 51200 * 4 + (1 << 20);
+}
+
+int Engine::accum_begin(int w, int h) {
+    GpuLock gl(*this);
+    if (w <= 0 || h <= 0) return fail(LUCID_ERR_INVALID, "accumulator: sizes must be positive");
+    CK(cudaSetDevice(device_));
+    int rc = ensure_stream();
+    if (rc != LUCID_OK) return rc;
+    const size_t np = (size_t)w * h;
+    if (jacc_n_ < np) {
+        if (jacc_) cudaFree(jacc_);
+        jacc_ = nullptr;
+        jacc_n_ = 0;
+        CK(cudaMalloc(&jacc_, np * sizeof(float4)));
+        jacc_n_ = np;
+    }
+    jacc_w_ = w;
+    jacc_h_ = h;
+    CK(cudaMemsetAsync(jacc_, 0, np * sizeof(float4), S(stream_)));
+    return LUCID_OK;
+}
+
+int Engine::render_accumulate(const LucidRenderParams& p) {
+    GpuLock gl(*this);
+    if (!jacc_ || p.tile_w != jacc_w_ || p.tile_h != jacc_h_) return fail(LUCID_ERR_INVALID, "accumulator size mismatch");
+    return render_impl(p, nullptr, nullptr, nullptr, jacc_, false);
+}
+
+int Engine::accum_output(float* out_host) {
+    GpuLock gl(*this);
+    if (!jacc_) return fail(LUCID_ERR_INVALID, "no accumulator");
+    CK(cudaSetDevice(device_));
+    cudaStream_t st = S(stream_);
+    const int np = jacc_w_ * jacc_h_;
+    PathPool& P = *pool_;
+    if (P.film_n < (size_t)np) { CK(P.film.alloc(np)); CK(P.out.alloc(np)); P.film_n = np; }
+    k_output<<<(np + 255) / 256, 256, 0, st>>>(jacc_w_, jacc_h_, (const float4*)jacc_, P.out.p);
+    CK(cudaMemcpyAsync(out_host, P.out.p, (size_t)np * sizeof(float4), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return LUCID_OK;
+}
+
+void Engine::accum_end() {
+    GpuLock gl(*this);
+    if (!jacc_) return;
+    cudaSetDevice(device_);
+    if (stream_) cudaStreamSynchronize(S(stream_));
+    cudaFree(jacc_);
+    jacc_ = nullptr;
+    jacc_n_ = 0;
+}
+
+void Engine::guide_free() {
+    GpuLock gl(*this);
+    if (!guide_) return;
+    cudaSetDevice(device_);
+    if (stream_) cudaStreamSynchronize(S(stream_));
+    delete guide_;
+    guide_ = nullptr;
 }
 
 void Engine::job_end_locked() {

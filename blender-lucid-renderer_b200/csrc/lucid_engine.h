@@ -21,6 +21,14 @@ struct DiagDevice;    // device record buffer of the path diagnostics
 struct JobState;      // progressive job (film, captured iteration graph)
 struct GuideState;    // path-guiding network and its per-path buffers
 
+// One version of an uploaded scene, as other engines share it: the device
+// scene and the counts and bounds that go with it.
+struct SceneSnapshot {
+    std::shared_ptr<DeviceScene> ds;
+    int stats[8] = {};
+    float lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+};
+
 class Engine {
 public:
     explicit Engine(int device);
@@ -65,6 +73,22 @@ public:
     int guide_params(float* out, size_t cap, float* box6);
     // Uses `owner`'s uploaded scene (BVH, materials, lights) without a copy.
     int share_scene(Engine& owner);
+    // The current version of this engine's scene, and rendering a version
+    // taken from another engine.
+    int snapshot_scene(SceneSnapshot& out);
+    int use_snapshot(const SceneSnapshot& snap);
+    const void* scene_ptr() const { return ds_.get(); }
+    // Parameter edits (lucid_cuda_update_scene): a new scene version that
+    // shares the geometry of the current one.
+    int update_scene(const LucidSceneEdit* edits, int count);
+    // Guided progressive jobs: render_impl iterations (guiding and training
+    // per wave) summed into a per-pixel accumulator.
+    static long long guide_job_bytes(long long paths);
+    int accum_begin(int w, int h);
+    int render_accumulate(const LucidRenderParams& p);
+    int accum_output(float* out_host);
+    void accum_end();          // frees the accumulator
+    void guide_free();         // frees the guide network and its buffers
     // Progressive jobs (the request loop's unit of work).
     static long long job_bytes(int w, int h, int chunk);
     int job_begin(int w, int h, int spp, int max_depth, int chunk, bool use_graph);
@@ -116,6 +140,9 @@ private:
     int shared_stats_[8] = {};
     JobState* job_ = nullptr;
     GuideState* guide_ = nullptr;
+    void* jacc_ = nullptr;        // device float4 accumulator of a guided job
+    size_t jacc_n_ = 0;
+    int jacc_w_ = 0, jacc_h_ = 0;
     float scene_lo_[3] = {0, 0, 0}, scene_hi_[3] = {1, 1, 1};
     PathPool* pool_ = nullptr;
     long long wave_cap_ = 0;  // 0 = automatic

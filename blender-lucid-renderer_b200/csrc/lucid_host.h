@@ -45,6 +45,16 @@ bool parse_scene_json(const char* json, size_t len, HostScene& out, std::string&
 bool build_scene_arrays(const LucidSceneDesc& desc, HostScene& out, std::string& err);
 // FNV-1a 64 over every uploaded array and count of a flattened scene.
 uint64_t scene_digest(const HostScene& s);
+// Parameter edits of a flattened scene (lucid_cuda_update_scene), all or
+// none: materials and native lights, no geometry.  False (err set, scene
+// unchanged) for an index out of range, a material that varies over its
+// surface (a textured node graph), or an edit that would add or remove an
+// emitting mesh.
+bool apply_scene_edits(HostScene& s, const LucidSceneEdit* edits, int count, std::string& err);
+// The shading class of a surface hit on a prim with this material (the
+// material part of the shading-queue bins): 1 emitter, 2 glass, 3 near-delta
+// metal, 4 metal, 5 other.
+unsigned char prim_shading_class(const DevMaterial& dm);
 
 struct HostCamera {
     float pos[3] = {0, 0, 0};

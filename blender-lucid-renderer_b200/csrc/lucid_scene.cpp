@@ -188,6 +188,57 @@ DevLight pack_native(const NativeLight& L) {
     return d;
 }
 
+// is_emissive (render_units.hpp:1200-1202): luminance above 1e-6.
+bool is_emissive(const float em[3]) { return (0.2126f * em[0] + 0.7152f * em[1] + 0.0722f * em[2]) > 1e-6f; }
+
+// A mesh's material record (getMaterialParams / getEmission inputs,
+// integrator/path_tracer.hpp:45-72); node programs are set by the caller.
+DevMaterial make_material(const float alb[3], float metallic, float roughness, const float em[3], float transmission,
+                          float ior, bool boundary, bool textured) {
+    const bool emissive = is_emissive(em);
+    DevMaterial dm;
+    std::memset(&dm, 0, sizeof(dm));
+    dm.albedo_metallic = f4(F3{alb[0], alb[1], alb[2]}, metallic);
+    dm.rough_trans_ior_flags.x = roughness;
+    dm.rough_trans_ior_flags.y = transmission;
+    dm.rough_trans_ior_flags.z = ior;
+    dm.rough_trans_ior_flags.w =
+        ibits((emissive ? MAT_EMISSIVE : 0) | (boundary ? MAT_BOUNDARY_ONLY : 0) | (textured ? MAT_TEXTURED : 0));
+    dm.emission = f4(F3{em[0], em[1], em[2]}, emissive ? 1.0f : 0.0f);
+    return dm;
+}
+
+// One native light of the array form (LucidLightDesc).
+NativeLight light_from_desc(const LucidLightDesc& l) {
+    const int t = (l.type == LUCID_LIGHT_POINT || l.type == LUCID_LIGHT_SUN || l.type == LUCID_LIGHT_SPOT ||
+                   l.type == LUCID_LIGHT_AREA) ? l.type : LIGHT_EMISSIVE;
+    const F3 dir{l.direction[0], l.direction[1], l.direction[2]};
+    const F3 right{l.right[0], l.right[1], l.right[2]}, up{l.up[0], l.up[1], l.up[2]};
+    return make_light(t, F3{l.position[0], l.position[1], l.position[2]}, &dir, l.color[0], l.color[1], l.color[2],
+                      l.energy, l.radius, l.spot_size, l.spot_blend, l.size, l.size_y, l.shape,
+                      t == LIGHT_AREA ? &right : nullptr, t == LIGHT_AREA ? &up : nullptr);
+}
+
+// SceneLights' CDF over the light list by cumulative area / total
+// (scene_lights.hpp:103-121; the total summed in list order, as
+// buildFromScene sums it) and the CDF search guide.
+void light_cdf(HostScene& S) {
+    float total = 0.0f;
+    for (const auto& d : S.lights) total += d.normal_area.w;
+    S.total_light_area = total;
+    S.cdf.resize(S.lights.size());
+    float cum = 0.0f;
+    for (size_t i = 0; i < S.lights.size(); ++i) {
+        cum += S.lights[i].normal_area.w;
+        S.cdf[i] = (total < 1e-6f) ? 0.0f : cum / total;
+    }
+    S.light_guide.resize(kLightGuide + 1);
+    for (int k = 0; k <= kLightGuide; ++k) {
+        float x = (float)k / (float)kLightGuide;   // exact: power-of-two denominator
+        S.light_guide[k] = (int)(std::lower_bound(S.cdf.begin(), S.cdf.end(), x) - S.cdf.begin());
+    }
+}
+
 // Scene assembly shared by the JSON and the array loaders: meshes in order,
 // then the native lights, then SceneLights (emissive triangles first).
 struct Assembly {
@@ -224,15 +275,8 @@ void emit_mesh(HostScene& S, Assembly& A, const std::vector<F3>& verts, const st
         S.volumes.push_back(vol);
     }
     S.num_boundary_meshes += boundary;
-    bool emissive = (0.2126f * em[0] + 0.7152f * em[1] + 0.0722f * em[2]) > 1e-6f;
-    DevMaterial dm;
-    dm.albedo_metallic = f4(F3{alb[0], alb[1], alb[2]}, metallic);
-    dm.rough_trans_ior_flags.x = roughness;
-    dm.rough_trans_ior_flags.y = transmission;
-    dm.rough_trans_ior_flags.z = ior;
-    dm.rough_trans_ior_flags.w =
-        ibits((emissive ? MAT_EMISSIVE : 0) | (boundary ? MAT_BOUNDARY_ONLY : 0) | (textured ? MAT_TEXTURED : 0));
-    dm.emission = f4(F3{em[0], em[1], em[2]}, emissive ? 1.0f : 0.0f);
+    const bool emissive = is_emissive(em);
+    DevMaterial dm = make_material(alb, metallic, roughness, em, transmission, ior, boundary, textured);
     dm.program.x = nm ? nm->albedo_start : 0;
     dm.program.y = nm ? nm->albedo_n : 0;
     dm.program.z = nm ? nm->emission_start : 0;
@@ -294,27 +338,11 @@ void finish_scene(HostScene& S, Assembly& A, const std::vector<NativeLight>& nat
     for (size_t i = 1; i < S.prim_uv.size() && !any_uv; i += 2) any_uv = S.prim_uv[i].z != 0.0f;
     if (!any_uv) std::vector<float4>().swap(S.prim_uv);
     for (int k = 0; k < 3; ++k) S.env[k] = env[k];
-    float total = A.total;
     S.lights = A.emissive_lights;
     S.native_start = (int)S.lights.size();
     S.num_native = (int)native.size();
-    for (const auto& L : native) {
-        DevLight d = pack_native(L);
-        S.lights.push_back(d);
-        total += d.normal_area.w;
-    }
-    S.total_light_area = total;
-    S.cdf.resize(S.lights.size());
-    float cum = 0.0f;
-    for (size_t i = 0; i < S.lights.size(); ++i) {
-        cum += S.lights[i].normal_area.w;
-        S.cdf[i] = (total < 1e-6f) ? 0.0f : cum / total;
-    }
-    S.light_guide.resize(kLightGuide + 1);
-    for (int k = 0; k <= kLightGuide; ++k) {
-        float x = (float)k / (float)kLightGuide;   // exact: power-of-two denominator
-        S.light_guide[k] = (int)(std::lower_bound(S.cdf.begin(), S.cdf.end(), x) - S.cdf.begin());
-    }
+    for (const auto& L : native) S.lights.push_back(pack_native(L));
+    light_cdf(S);
 }
 
 // One "meshes" entry read as loadSceneFromJsonString reads it
@@ -663,21 +691,72 @@ bool build_scene_arrays(const LucidSceneDesc& d, HostScene& S, std::string& err)
                       m.transmission, m.ior, boundary, vol, vol_has_grid, grid);
         }
         std::vector<NativeLight> native;
-        for (int li = 0; li < d.num_lights; ++li) {
-            const LucidLightDesc& l = d.lights[li];
-            const int t = (l.type == LUCID_LIGHT_POINT || l.type == LUCID_LIGHT_SUN || l.type == LUCID_LIGHT_SPOT ||
-                           l.type == LUCID_LIGHT_AREA) ? l.type : LIGHT_EMISSIVE;
-            const F3 dir{l.direction[0], l.direction[1], l.direction[2]};
-            const F3 right{l.right[0], l.right[1], l.right[2]}, up{l.up[0], l.up[1], l.up[2]};
-            native.push_back(make_light(t, F3{l.position[0], l.position[1], l.position[2]}, &dir, l.color[0], l.color[1],
-                                        l.color[2], l.energy, l.radius, l.spot_size, l.spot_blend, l.size, l.size_y,
-                                        l.shape, t == LIGHT_AREA ? &right : nullptr, t == LIGHT_AREA ? &up : nullptr));
-        }
+        for (int li = 0; li < d.num_lights; ++li) native.push_back(light_from_desc(d.lights[li]));
         finish_scene(S, A, native, d.environment);
     } catch (const std::exception& e) {
         err = std::string("malformed scene arrays: ") + e.what();
         return false;
     }
+    return true;
+}
+
+unsigned char prim_shading_class(const DevMaterial& dm) {
+    const float rough = dm.rough_trans_ior_flags.x, trans = dm.rough_trans_ior_flags.y, metal = dm.albedo_metallic.w;
+    return dm.emission.w != 0.0f ? 1 : trans > 0.5f ? 2 : (metal > 0.5f && rough < 0.05f) ? 3 : (metal > 0.5f ? 4 : 5);
+}
+
+bool apply_scene_edits(HostScene& S, const LucidSceneEdit* e, int n, std::string& err) {
+    if (n < 0 || (n > 0 && !e)) { err = "scene edit: bad edit list"; return false; }
+    // check every edit first: all or none
+    for (int i = 0; i < n; ++i) {
+        const LucidSceneEdit& x = e[i];
+        if (x.kind == LUCID_EDIT_MATERIAL) {
+            if (x.index < 0 || x.index >= (int)S.materials.size()) {
+                err = "scene edit: no mesh " + std::to_string(x.index);
+                return false;
+            }
+            int fl;
+            std::memcpy(&fl, &S.materials[x.index].rough_trans_ior_flags.w, 4);
+            if (fl & MAT_TEXTURED) {
+                err = "scene edit: mesh " + std::to_string(x.index) + " has a textured node-graph material";
+                return false;
+            }
+            if (((fl & MAT_EMISSIVE) != 0) != is_emissive(x.emission)) {
+                err = "scene edit: mesh " + std::to_string(x.index) +
+                      " would start or stop emitting, which changes the light list; reload the scene";
+                return false;
+            }
+        } else if (x.kind == LUCID_EDIT_LIGHT) {
+            if (x.index < 0 || x.index >= S.num_native) {
+                err = "scene edit: no native light " + std::to_string(x.index);
+                return false;
+            }
+        } else {
+            err = "scene edit: unknown kind " + std::to_string(x.kind);
+            return false;
+        }
+    }
+    for (int i = 0; i < n; ++i) {
+        const LucidSceneEdit& x = e[i];
+        if (x.kind == LUCID_EDIT_MATERIAL) {
+            DevMaterial& dm = S.materials[x.index];
+            int fl;
+            std::memcpy(&fl, &dm.rough_trans_ior_flags.w, 4);
+            DevMaterial nd = make_material(x.base_color, x.metallic, x.roughness, x.emission, x.transmission, x.ior,
+                                           (fl & MAT_BOUNDARY_ONLY) != 0, false);
+            nd.program = dm.program;
+            dm = nd;
+            if (fl & MAT_EMISSIVE)   // the mesh's emissive-triangle lights carry its emission
+                for (size_t p = 0; p < S.prim_info.size(); ++p)
+                    if (S.prim_info[p].x == x.index && S.prim_info[p].z >= 0) {
+                        float4& er = S.lights[S.prim_info[p].z].emission_radius;
+                        er.x = x.emission[0]; er.y = x.emission[1]; er.z = x.emission[2];
+                    }
+        } else {
+            S.lights[S.native_start + x.index] = pack_native(light_from_desc(x.light));
+        }
+    }
+    light_cdf(S);
     return true;
 }
 

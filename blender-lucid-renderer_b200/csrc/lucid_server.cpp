@@ -46,9 +46,7 @@ Server::Server(int device, int slots, long long budget_bytes) : device_(device) 
     t0_ = now();
     for (int s = 0; s < slots; ++s) {
         slot_eng_.emplace_back(new Engine(device));
-        slot_scene_.push_back(-1);
         pre_eng_.emplace_back(nullptr);
-        pre_scene_.push_back(-1);
     }
     for (int s = 0; s < slots; ++s) threads_.emplace_back([this, s] { slot_loop(s); });
 }
@@ -94,22 +92,43 @@ int Server::add_scene_with(Load&& load, int* scene_id) {
     return LUCID_OK;
 }
 
+int Server::update_scene(int scene_id, const LucidSceneEdit* edits, int count) {
+    std::lock_guard<std::mutex> lk(mu_);   // ordered with submissions: later jobs see the edit
+    if (scene_id < 0 || scene_id >= (int)scenes_.size()) return fail(LUCID_ERR_INVALID, "update: unknown scene");
+    int rc = scenes_[scene_id]->update_scene(edits, count);
+    if (rc != LUCID_OK) return fail(rc, scenes_[scene_id]->last_error());
+    return LUCID_OK;
+}
+
+// Bytes of a job: path state and film for `chunk` samples per iteration,
+// plus the guide's buffers for a guided job.
+static long long job_total_bytes(const LucidJobDesc& d, int chunk) {
+    long long b = Engine::job_bytes(d.width, d.height, chunk);
+    if (d.guided) b += Engine::guide_job_bytes((long long)d.width * d.height * chunk);
+    return b;
+}
+
 int Server::submit(const LucidJobDesc& d, int* job_id) {
     if (d.width <= 0 || d.height <= 0 || d.samples <= 0 || d.max_depth <= 0 || d.max_depth > 1024)
         return fail(LUCID_ERR_INVALID, "job: sizes must be positive (max_depth <= 1024)");
+    if (d.guided && std::string(d.algorithm, strnlen(d.algorithm, sizeof(d.algorithm))) != "mis")
+        return fail(LUCID_ERR_INVALID, "job: path guiding needs the \"mis\" integrator");
     std::unique_lock<std::mutex> lk(mu_);
     if (d.scene < 0 || d.scene >= (int)scenes_.size()) return fail(LUCID_ERR_INVALID, "job: unknown scene");
+    auto snap = std::make_shared<SceneSnapshot>();
+    if (scenes_[d.scene]->snapshot_scene(*snap) != LUCID_OK) return fail(LUCID_ERR_NO_SCENE, "job: scene not loaded");
     int id = next_id_++;
     Job& j = jobs_[id];
     j.d = d;
     j.d.algorithm[sizeof(j.d.algorithm) - 1] = 0;
+    j.snap = std::move(snap);
     j.t_submit = now();
     const long long np = (long long)d.width * d.height;
     // the largest samples per iteration within the wave limit and the budget
     int cmax = (int)std::max(1LL, std::min<long long>(d.samples, kJobWavePaths / std::max(1LL, np)));
-    while (cmax > 1 && adm_.never_fits(Engine::job_bytes(d.width, d.height, cmax))) cmax /= 2;
+    while (cmax > 1 && adm_.never_fits(job_total_bytes(d, cmax))) cmax /= 2;
     j.chunk_max = cmax;
-    j.bytes = Engine::job_bytes(d.width, d.height, j.chunk_max);
+    j.bytes = job_total_bytes(d, j.chunk_max);
     *job_id = id;
     if (adm_.never_fits(j.bytes)) {
         j.state = LUCID_JOB_REFUSED;
@@ -159,7 +178,7 @@ void Server::slot_loop(int slot) {
             if (busy_from_ < 0) busy_from_ = j->t_start;
         }
         cv_.notify_all();   // another slot may start the next job too
-        int rc = run_job(*slot_eng_[slot], slot_scene_[slot], *j, slot, false);
+        int rc = run_job(*slot_eng_[slot], *j, slot, false);
         finish_job(*j, rc);
     }
 }
@@ -176,6 +195,7 @@ void Server::finish_job(Job& j, int rc) {
         } else {
             j.state = j.cancel ? LUCID_JOB_CANCELLED : LUCID_JOB_FAILED;
         }
+        j.snap.reset();   // the scene version may go once no job needs it
     }
     cv_.notify_all();
     done_cv_.notify_all();
@@ -204,7 +224,7 @@ void Server::run_waiting_interactive(int slot) {
         if (!pre_eng_[slot]) pre_eng_[slot].reset(new Engine(device_));
         // the second engine keeps its path pool from one interactive job to the next
         // (freeing device memory synchronises the device and would stall the batch job)
-        int rc = run_job(*pre_eng_[slot], pre_scene_[slot], *j, slot, true);
+        int rc = run_job(*pre_eng_[slot], *j, slot, true);
         finish_job(*j, rc);
     }
 }
@@ -248,17 +268,17 @@ int Server::pick_chunk(Engine& e, Job& j, int id, int& offset) {
     return best;
 }
 
-int Server::run_job(Engine& e, int& engine_scene, Job& j, int slot, bool keep_pool) {
+int Server::run_job(Engine& e, Job& j, int slot, bool keep_pool) {
     const LucidJobDesc& d = j.d;
     int rc = LUCID_OK;
-    if (engine_scene != d.scene) {
-        rc = e.share_scene(*scenes_[d.scene]);
+    if (e.scene_ptr() != j.snap->ds.get()) {   // another scene, or another version of it
+        rc = e.use_snapshot(*j.snap);
         if (rc != LUCID_OK) { j.error = e.last_error(); return rc; }
-        engine_scene = d.scene;
     }
     const float* c = d.camera;
     e.set_camera(c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7], c[8], c[9]);
     e.set_algorithm(d.algorithm);
+    if (d.guided) return run_guided_job(e, j, slot, keep_pool);
     rc = e.job_begin(d.width, d.height, d.samples, d.max_depth, j.chunk_max, false);
     if (rc != LUCID_OK) { j.error = e.last_error(); e.job_end(); if (!keep_pool) e.release_pool(); return rc; }
     int offset = 0;
@@ -293,6 +313,42 @@ int Server::run_job(Engine& e, int& engine_scene, Job& j, int slot, bool keep_po
     }
     if (rc != LUCID_OK) j.error = e.last_error();
     e.job_end();
+    if (!keep_pool) e.release_pool();
+    return rc;
+}
+
+// A guided job: iterations of chunk_max samples through the engine's render
+// path (guided sampling, and training after every wave, on the job's own
+// network), summed per pixel; batch jobs let waiting interactive jobs run
+// between their iterations as unguided jobs do.
+int Server::run_guided_job(Engine& e, Job& j, int slot, bool keep_pool) {
+    const LucidJobDesc& d = j.d;
+    int rc = e.guide_enable(true, d.guide_seed);
+    if (rc == LUCID_OK) rc = e.accum_begin(d.width, d.height);
+    int offset = 0;
+    while (rc == LUCID_OK && offset < d.samples) {
+        if (j.cancel) break;
+        const int n = std::min(j.chunk_max, d.samples - offset);
+        LucidRenderParams p{0, 0, d.width, d.height, d.width, d.height, n, offset, d.max_depth, 0};
+        rc = e.render_accumulate(p);
+        offset += n;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            j.done = offset;
+            if (j.t_first == 0) j.t_first = now();
+        }
+        if (!d.interactive && rc == LUCID_OK) run_waiting_interactive(slot);
+    }
+    if (rc == LUCID_OK && !j.cancel) {
+        std::vector<float> img((size_t)d.width * d.height * 4);
+        rc = e.accum_output(img.data());
+        std::lock_guard<std::mutex> lk(mu_);
+        if (rc == LUCID_OK) j.image.swap(img);
+    }
+    if (rc != LUCID_OK) j.error = e.last_error();
+    // the guide's buffers and the accumulator were counted in this job's bytes
+    e.guide_free();
+    e.accum_end();
     if (!keep_pool) e.release_pool();
     return rc;
 }

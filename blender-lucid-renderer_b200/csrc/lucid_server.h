@@ -10,7 +10,10 @@
 // waiting interactive jobs between the batch job's iterations, on a second
 // engine, so that they never wait for a long render
 // (HBM budget = uploaded scenes + every running job's path state and film);
-// a job that could never fit is refused at submission.  Each slot picks the
+// a job that could never fit is refused at submission.  Scene edits make a
+// new scene version; a job renders the version current when it was
+// submitted.  Guided jobs (the "mis" integrator with online path guiding)
+// train their own guide and count its buffers in their bytes.  Each slot picks the
 // samples per iteration (the queue capacity of its waves) with a small
 // autotuner and replays the iteration as a CUDA graph.  A job's image
 // depends only on its own sample indices, so it is the same alone and in
@@ -31,6 +34,7 @@
 namespace lucid {
 
 class Engine;
+struct SceneSnapshot;
 
 // FIFO admission under a byte budget: the head job starts when a slot is
 // free and reserved + running + its bytes fit; a job larger than budget -
@@ -50,6 +54,7 @@ public:
     ~Server();
     int add_scene(const char* json, size_t len, int* scene_id);
     int add_scene_arrays(const LucidSceneDesc& desc, int* scene_id);
+    int update_scene(int scene_id, const LucidSceneEdit* edits, int count);
     int submit(const LucidJobDesc& d, int* job_id);
     int state(int job, int* samples_done);
     int wait(int job, int timeout_ms);
@@ -70,11 +75,13 @@ private:
         double t_submit = 0, t_start = 0, t_first = 0, t_end = 0;
         std::vector<float> image;
         std::string error;
+        std::shared_ptr<SceneSnapshot> snap;   // the scene version current at submission
     };
     template <class Load>
     int add_scene_with(Load&& load, int* scene_id);
     void slot_loop(int slot);
-    int run_job(Engine& e, int& engine_scene, Job& j, int slot, bool keep_pool);
+    int run_job(Engine& e, Job& j, int slot, bool keep_pool);
+    int run_guided_job(Engine& e, Job& j, int slot, bool keep_pool);
     void finish_job(Job& j, int rc);
     void run_waiting_interactive(int slot);
     int pick_chunk(Engine& e, Job& j, int slot, int& offset);
@@ -85,9 +92,7 @@ private:
     std::vector<std::unique_ptr<Engine>> scenes_;
     std::vector<long long> scene_bytes_;
     std::vector<std::unique_ptr<Engine>> slot_eng_;
-    std::vector<int> slot_scene_;
     std::vector<std::unique_ptr<Engine>> pre_eng_;   // per slot: interactive jobs run between batch iterations
-    std::vector<int> pre_scene_;
     std::vector<std::thread> threads_;
     std::mutex mu_;
     std::condition_variable cv_, done_cv_;

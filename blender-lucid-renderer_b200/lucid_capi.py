@@ -52,6 +52,44 @@ class LightDesc(ctypes.Structure):
                 ("shape", ctypes.c_int32), ("right", _F3), ("up", _F3)]
 
 
+LUCID_EDIT_MATERIAL = 1
+LUCID_EDIT_LIGHT = 2
+
+
+class SceneEdit(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("index", ctypes.c_int32), ("base_color", _F3), ("metallic", ctypes.c_float),
+                ("roughness", ctypes.c_float), ("emission", _F3), ("transmission", ctypes.c_float),
+                ("ior", ctypes.c_float), ("light", LightDesc)]
+
+
+def _light_desc(l: dict, d: LightDesc) -> None:
+    d.type = int(l["type"])
+    d.position, d.direction, d.color = _F3(*l["position"]), _F3(*l["direction"]), _F3(*l["color"])
+    d.energy, d.radius = float(l["energy"]), float(l["radius"])
+    d.spot_size, d.spot_blend = float(l["spot_size"]), float(l["spot_blend"])
+    d.size, d.size_y, d.shape = float(l["size"]), float(l["size_y"]), int(l["shape"])
+    d.right, d.up = _F3(*l["right"]), _F3(*l["up"])
+
+
+def scene_edits(edits) -> ctypes.Array:
+    """LucidSceneEdit array from dicts: {"mesh": i, "material": {base_color,
+    metallic, roughness, emission, transmission, ior}} or {"light": j,
+    "desc": a light of lucid_scenes.scene_arrays(...)["lights"]}."""
+    arr = (SceneEdit * max(1, len(edits)))()
+    for i, e in enumerate(edits):
+        x = arr[i]
+        if "mesh" in e:
+            m = e["material"]
+            x.kind, x.index = LUCID_EDIT_MATERIAL, int(e["mesh"])
+            x.base_color, x.emission = _F3(*m["base_color"]), _F3(*m["emission"])
+            x.metallic, x.roughness = float(m["metallic"]), float(m["roughness"])
+            x.transmission, x.ior = float(m["transmission"]), float(m["ior"])
+        else:
+            x.kind, x.index = LUCID_EDIT_LIGHT, int(e["light"])
+            _light_desc(e["desc"], x.light)
+    return arr
+
+
 class SceneDesc(ctypes.Structure):
     _fields_ = [("meshes", ctypes.c_void_p), ("num_meshes", ctypes.c_int32), ("lights", ctypes.c_void_p),
                 ("num_lights", ctypes.c_int32), ("environment", _F3)]
@@ -90,13 +128,7 @@ def _scene_desc(arrays: dict):
         d.volume_grid = ptr(m["volume_grid"], np.float32)
     ls_ = (LightDesc * max(1, len(arrays["lights"])))()
     for i, l in enumerate(arrays["lights"]):
-        d = ls_[i]
-        d.type = int(l["type"])
-        d.position, d.direction, d.color = _F3(*l["position"]), _F3(*l["direction"]), _F3(*l["color"])
-        d.energy, d.radius = float(l["energy"]), float(l["radius"])
-        d.spot_size, d.spot_blend = float(l["spot_size"]), float(l["spot_blend"])
-        d.size, d.size_y, d.shape = float(l["size"]), float(l["size_y"]), int(l["shape"])
-        d.right, d.up = _F3(*l["right"]), _F3(*l["up"])
+        _light_desc(l, ls_[i])
     keep += [ms, ls_]
     sd = SceneDesc(ctypes.addressof(ms), len(arrays["meshes"]), ctypes.addressof(ls_), len(arrays["lights"]),
                    _F3(*arrays["environment"]))
@@ -173,7 +205,8 @@ DIAG_STATS_FIELDS = ("total_samples", "active_pixels", "total_groups", "total_ov
 class JobDesc(ctypes.Structure):
     _fields_ = [("scene", ctypes.c_int), ("camera", ctypes.c_float * 10), ("algorithm", ctypes.c_char * 16),
                 ("width", ctypes.c_int), ("height", ctypes.c_int), ("samples", ctypes.c_int),
-                ("max_depth", ctypes.c_int), ("interactive", ctypes.c_int)]
+                ("max_depth", ctypes.c_int), ("interactive", ctypes.c_int), ("guided", ctypes.c_int),
+                ("guide_seed", ctypes.c_int)]
 
 
 class ServerStats(ctypes.Structure):
@@ -243,6 +276,8 @@ SIGNATURES = {
     "lucid_diag_film_metadata_json": (ctypes.c_longlong, [_P, ctypes.c_void_p, ctypes.c_size_t]),
     "lucid_path_trace_hash": (ctypes.c_uint64, [ctypes.POINTER(PathTrace)]),
     "lucid_path_trace_coarse_type": (_I, [ctypes.POINTER(PathTrace)]),
+    "lucid_cuda_update_scene": (_I, [_P, _P, _I]),
+    "lucid_server_update_scene": (_I, [_P, _I, _P, _I]),
     "lucid_server_create": (_I, [_I, _I, ctypes.c_longlong, ctypes.POINTER(_P)]),
     "lucid_server_destroy": (None, [_P]),
     "lucid_server_last_error": (ctypes.c_char_p, [_P]),
@@ -356,6 +391,12 @@ class Context:
         sd, keep = _scene_desc(arrays)
         self._check(self.lib.lucid_cuda_load_scene_arrays(self.h, ctypes.byref(sd)))
         del keep
+
+    def update_scene(self, edits, check=True) -> int:
+        """lucid_cuda_update_scene with scene_edits(edits)."""
+        arr = scene_edits(edits)
+        rc = self.lib.lucid_cuda_update_scene(self.h, ctypes.addressof(arr), len(edits))
+        return self._check(rc) if check else rc
 
     def set_camera(self, *cam) -> None:
         self._check(self.lib.lucid_cuda_set_camera(self.h, *[float(c) for c in cam]))
@@ -620,10 +661,19 @@ class Server:
             self._err(rc)
         return sid.value
 
+    def update_scene(self, scene: int, edits, check=True) -> int:
+        """lucid_server_update_scene: jobs submitted afterwards see the edits."""
+        arr = scene_edits(edits)
+        rc = self.lib.lucid_server_update_scene(self.h, scene, ctypes.addressof(arr), len(edits))
+        if rc != LUCID_OK and check:
+            self._err(rc)
+        return rc
+
     def submit(self, scene: int, camera, width: int, height: int, samples: int, max_depth: int = 8,
-               algorithm: str = "mis", interactive: bool = False, check: bool = True):
+               algorithm: str = "mis", interactive: bool = False, check: bool = True, guided: bool = False,
+               guide_seed: int = 1):
         d = JobDesc(scene, (ctypes.c_float * 10)(*[float(c) for c in camera]), algorithm.encode(), width, height,
-                    samples, max_depth, int(interactive))
+                    samples, max_depth, int(interactive), int(guided), guide_seed)
         jid = ctypes.c_int()
         rc = self.lib.lucid_server_submit(self.h, ctypes.byref(d), ctypes.byref(jid))
         self._sizes[jid.value] = (height, width)

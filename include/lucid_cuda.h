@@ -160,6 +160,30 @@ typedef struct {
 /* Loads a scene given as arrays (no counterpart in the reference; the
  * loadSceneFromJsonString semantics above).  Replaces the current scene. */
 int lucid_cuda_load_scene_arrays(LucidCudaCtx* ctx, const LucidSceneDesc* scene);
+
+/* Parameter edits of the loaded scene without a re-upload or BVH rebuild.
+ * The reference has no such call: every scene change re-exports, re-parses
+ * and re-packs the whole scene (PyRenderer keys its packed GPU scene on
+ * scene_version_, pybind_renderer.hpp:116, 502-504; the viewport pushes
+ * edits through scene_update_pending, LucidRenderer/viewport.py:108-111).
+ * An edited scene renders bit-identically to loading the edited scene. */
+#define LUCID_EDIT_MATERIAL 1   /* mesh `index` ("meshes" order) gets the material fields below */
+#define LUCID_EDIT_LIGHT 2      /* native light `index` ("native_lights" order) becomes `light` */
+typedef struct {
+    int32_t kind, index;
+    /* LUCID_EDIT_MATERIAL: the Principled fields of a LucidMeshDesc */
+    float base_color[3], metallic, roughness, emission[3], transmission, ior;
+    /* LUCID_EDIT_LIGHT: the whole light, as lucid_cuda_load_scene_arrays takes it */
+    LucidLightDesc light;
+} LucidSceneEdit;
+/* Applies `count` edits in order, all or none: LUCID_ERR_INVALID (nothing
+ * changed) when an index is out of range, a material varies over its
+ * surface (a node graph with a texture), or an edit would add or remove an
+ * emitting mesh (that changes
+ * the light list: reload the scene instead).  Renders and jobs started
+ * after the call see the edited scene; a context rendering another
+ * context's scene (the request loop's slots) keeps the version it took. */
+int lucid_cuda_update_scene(LucidCudaCtx* ctx, const LucidSceneEdit* edits, int count);
 /* Replaces PyRenderer::set_camera (pybind_renderer.hpp:131-160). */
 int lucid_cuda_set_camera(LucidCudaCtx* ctx, float pos_x, float pos_y, float pos_z, float dir_x, float dir_y,
                           float dir_z, float up_x, float up_y, float up_z, float fov_deg);
@@ -429,6 +453,8 @@ typedef struct LucidJobDesc {
     char algorithm[16];   /* "simple", "nee", "mis", "volume_simple", "volume_mis" */
     int width, height, samples, max_depth;
     int interactive;      /* 1: keep each iteration short (viewport); 0: throughput */
+    int guided;           /* 1: "mis" with online path guiding (lucid_cuda_guide_enable), trained per job */
+    int guide_seed;       /* the guide network's initialisation seed */
 } LucidJobDesc;
 
 enum { LUCID_JOB_QUEUED = 0, LUCID_JOB_RUNNING = 1, LUCID_JOB_DONE = 2, LUCID_JOB_REFUSED = 3,
@@ -451,6 +477,10 @@ const char* lucid_server_last_error(LucidServer* srv);
 int lucid_server_add_scene(LucidServer* srv, const char* json, size_t len, int* scene_id);
 /* The same from arrays (lucid_cuda_load_scene_arrays). */
 int lucid_server_add_scene_arrays(LucidServer* srv, const LucidSceneDesc* scene, int* scene_id);
+/* lucid_cuda_update_scene on a server scene: jobs submitted after the call
+ * render the edited scene; jobs already queued or running keep the version
+ * they were submitted with. */
+int lucid_server_update_scene(LucidServer* srv, int scene_id, const LucidSceneEdit* edits, int count);
 /* Queues a job (LUCID_ERR_OOM and state REFUSED when it can never fit). */
 int lucid_server_submit(LucidServer* srv, const LucidJobDesc* job, int* job_id);
 /* Returns the job's LUCID_JOB_* state; samples_done may be NULL. */
