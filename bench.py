@@ -273,63 +273,145 @@ def c1_quality(device: int) -> dict:
             "reference_s": round(ref_s, 3), "samples_per_s": 256 * 256 * 16 / (ms / 1000.0)}
 
 
-def serving(device: int, seed: int = 7, slots: int = 2) -> dict:
-    """The request loop on a seeded job trace: Poisson arrivals (mean 40 per
-    second for one second) of viewport sessions (800x600, 16 one-sample
-    ticks, interactive), material previews (256x256, 32 spp) and F12 renders
-    (1920x1080, 256 spp) of the Cornell box.  Latencies come from the trace
-    on 2 slots; aggregate samples/s from the same jobs submitted at once, on
-    2 slots and on 1 slot (one after another).  (Measured: 2 slots beat 4
-    and 8, whose persistent kernels contend for the same SMs.)"""
+def serving(device: int, seed: int = 7, slots: int = 2, seconds: float = 2.0) -> dict:
+    """The request loop on a seeded job trace (the serving configuration):
+    Poisson arrivals (mean 40 per second for two seconds) of viewport
+    sessions (800x600, 16 one-sample ticks, interactive), material previews
+    (256x256, 32 spp) and F12 renders (1920x1080, 256 spp) over two Cornell
+    scenes and a preview scene; jobs on the second Cornell scene are guided
+    (online path guiding, trained per job); every 0.5 s an edit perturbs one
+    material colour (1 % of the parameters, rounded up) and the light of both
+    Cornell scenes, through lucid_server_update_scene, while jobs run.
+    Latencies come from the trace on 2 slots; aggregate samples/s from the
+    same jobs submitted at once, on 2 slots and on 1 slot (one after
+    another).  (Measured: 2 slots beat 4 and 8, whose persistent kernels
+    contend for the same SMs.)"""
     import lucid_capi
     import lucid_scenes as ls
     rng = np.random.default_rng(seed)
     cornell, ccam = ls.cornell_box()
+    cornell_b, _ = ls.cornell_variant(seed, 36)
     preview, pcam = ls.material_preview_scene(seed)
     t, jobs = 0.0, []
     while True:
         t += rng.exponential(1.0 / 40.0)
-        if t > 1.0:
+        if t > seconds:
             break
-        u = rng.random()
+        u, sc = rng.random(), ("cornell", "cornell_b")[int(rng.random() < 0.5)]
         if u < 0.6:
-            jobs.append((t, "cornell", 800, 600, 16, True))
+            jobs.append((t, sc, 800, 600, 16, True))
         elif u < 0.95:
             jobs.append((t, "preview", 256, 256, 32, False))
         else:
-            jobs.append((t, "cornell", 1920, 1080, 256, False))
+            jobs.append((t, sc, 1920, 1080, 256, False))
     if not any(j[2] == 1920 for j in jobs):
-        jobs.append((0.5, "cornell", 1920, 1080, 256, False))
-    cams = {"cornell": ccam, "preview": pcam}
+        jobs.append((0.5, "cornell_b", 1920, 1080, 256, False))
+    edit_times = [0.5 * (k + 1) for k in range(int(seconds / 0.5)) if 0.5 * (k + 1) < seconds]
+    cams = {"cornell": ccam, "cornell_b": ccam, "preview": pcam}
+    arr = {"cornell": ls.scene_arrays(cornell), "cornell_b": ls.scene_arrays(cornell_b)}
 
-    def run(slots, timed):
-        srv = lucid_capi.Server(device, slots=slots)
-        ids = {"cornell": srv.add_scene(ls.to_json(cornell)), "preview": srv.add_scene(ls.to_json(preview))}
+    def edits_at(k, name):
+        m = dict(arr[name]["meshes"][k % 7])
+        mat = {key: m[key] for key in ("base_color", "metallic", "roughness", "emission", "transmission", "ior")}
+        mat["base_color"] = [float(c) * (0.9 + 0.2 * ((k * 7 + i) % 5) / 4.0) for i, c in enumerate(mat["base_color"])]
+        light = dict(arr[name]["meshes"][7])
+        lmat = {key: light[key] for key in ("base_color", "metallic", "roughness", "emission", "transmission", "ior")}
+        lmat["emission"] = [float(c) * (0.95 + 0.1 * (k % 3) / 2.0) for c in lmat["emission"]]
+        return [{"mesh": k % 7, "material": mat}, {"mesh": 7, "material": lmat}]
+
+    def run(n_slots, timed):
+        srv = lucid_capi.Server(device, slots=n_slots)
+        ids = {"cornell": srv.add_scene(ls.to_json(cornell)), "cornell_b": srv.add_scene(ls.to_json(cornell_b)),
+               "preview": srv.add_scene(ls.to_json(preview))}
         t0 = time.perf_counter()
-        jids = []
+        jids, edit_ms, e = [], [], 0
         for (ta, name, w, h, spp, inter) in jobs:
             if timed:
+                while e < len(edit_times) and edit_times[e] <= ta:
+                    dt = edit_times[e] - (time.perf_counter() - t0)
+                    if dt > 0:
+                        time.sleep(dt)
+                    for sc in ("cornell", "cornell_b"):
+                        te = time.perf_counter()
+                        srv.update_scene(ids[sc], edits_at(e, sc))
+                        edit_ms.append(1000.0 * (time.perf_counter() - te))
+                    e += 1
                 dt = ta - (time.perf_counter() - t0)
                 if dt > 0:
                     time.sleep(dt)
-            jids.append(srv.submit(ids[name], cams[name], w, h, spp, 8, "mis", inter))
+            jids.append(srv.submit(ids[name], cams[name], w, h, spp, 8, "mis", inter, guided=(name == "cornell_b"),
+                                   guide_seed=len(jids) + 1))
         for j in jids:
             srv.wait(j, -1)
         wall = time.perf_counter() - t0
         st = srv.stats()
         srv.close()
-        return st, wall
+        return st, wall, edit_ms
 
     total = sum(w * h * spp for (_, _, w, h, spp, _) in jobs)
-    st_trace, _ = run(slots, True)
-    _, wall_mix = run(slots, False)
-    _, wall_seq = run(1, False)
-    return {"trace": "Poisson 40/s for 1 s, seed %d: 60%% viewport 800x600x16 (interactive), 35%% preview "
-                     "256x256x32, 5%% F12 1920x1080x256, mis depth 8" % seed,
-            "jobs": len(jobs), "samples": total,
+    st_trace, _, edit_ms = run(slots, True)
+    _, wall_mix, _ = run(slots, False)
+    _, wall_seq, _ = run(1, False)
+    return {"trace": "Poisson 40/s for %.0f s, seed %d: 60%% viewport 800x600x16 (interactive), 35%% preview "
+                     "256x256x32, 5%% F12 1920x1080x256, mis depth 8; two Cornell scenes, jobs on the second "
+                     "guided; a material and light edit of both every 0.5 s" % (seconds, seed),
+            "jobs": len(jobs), "guided_jobs": sum(1 for j in jobs if j[1] == "cornell_b"), "samples": total,
+            "edits": len(edit_ms), "edit_ms_max": round(max(edit_ms), 3) if edit_ms else None,
             "latency_p50_ms": st_trace["latency_p50_ms"], "latency_p99_ms": st_trace["latency_p99_ms"],
             "first_frame_p50_ms": st_trace["first_p50_ms"], "first_frame_p99_ms": st_trace["first_p99_ms"],
             "slots": slots, "samples_per_s": total / wall_mix, "samples_per_s_sequential": total / wall_seq}
+
+
+def batch_mix(device: int, seed: int = 11, slots: int = 4) -> dict:
+    """The batched configuration: 48 render jobs, each on its own seeded
+    variant of the Cornell box tessellated to 10k-500k triangles
+    (log-uniform), at log-uniform 128-1024 px with aspect 1:1, 4:3 or 16:9
+    and 1, 4, 16 or 64 spp, plus 8 material previews (256x256, 32 spp),
+    submitted at once to the request loop (scenes uploaded as arrays):
+    aggregate samples/s on `slots` slots against the same jobs one after
+    another on one slot."""
+    import lucid_capi
+    import lucid_scenes as ls
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for i in range(48):
+        side = float(np.exp(rng.uniform(np.log(128), np.log(1024))))
+        aspect = (1.0, 4.0 / 3.0, 16.0 / 9.0)[int(rng.integers(0, 3))]
+        w, h = int(round(side)), max(1, int(round(side / aspect)))
+        spp = int((1, 4, 16, 64)[int(rng.integers(0, 4))])
+        tris = int(np.exp(rng.uniform(np.log(10_000), np.log(500_000))))
+        jobs.append(("variant", seed * 1000 + i, tris, w, h, spp))
+    for i in range(8):
+        jobs.append(("preview", seed * 1000 + 100 + i, 5122, 256, 256, 32))
+    scenes = []
+    for kind, sd, tris, *_ in jobs:
+        sc, cam = ls.cornell_variant(sd, tris) if kind == "variant" else ls.material_preview_scene(sd)
+        scenes.append((ls.scene_arrays(sc, json_rounding=False), cam, ls.scene_triangle_count(sc)))
+    total = sum(w * h * spp for (*_, w, h, spp) in jobs)
+
+    def run(n_slots):
+        srv = lucid_capi.Server(device, slots=n_slots)
+        tu = time.perf_counter()
+        ids = [srv.add_scene_arrays(a) for (a, _, _) in scenes]
+        upload = time.perf_counter() - tu
+        t0 = time.perf_counter()
+        jids = [srv.submit(ids[k], scenes[k][1], w, h, spp, 8, "mis") for k, (*_, w, h, spp) in enumerate(jobs)]
+        for j in jids:
+            srv.wait(j, -1)
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
+        return wall, upload, st
+
+    run(1)   # first use of every kernel and allocation
+    wall_mix, upload, st = run(slots)
+    wall_seq, _, _ = run(1)
+    return {"jobs": len(jobs), "scenes": len(scenes), "triangles": int(sum(s[2] for s in scenes)),
+            "samples": total, "slots": slots, "upload_s": round(upload, 3),
+            "samples_per_s": total / wall_mix, "samples_per_s_sequential": total / wall_seq,
+            "latency_p50_ms": st["latency_p50_ms"], "latency_p99_ms": st["latency_p99_ms"],
+            "launch": "per-slot streams over shared scenes; each job its own wavefront launches (no single "
+                      "launch across jobs)"}
 
 
 def guiding(device: int, budget_ms: float = 1000.0, width: int = 1280, height: int = 720) -> dict:
@@ -443,6 +525,7 @@ def main():
     ap.add_argument("--no-serving", action="store_true", help="skip the request-loop job trace")
     ap.add_argument("--no-guiding", action="store_true", help="skip the guided-vs-plain equal-time comparison")
     ap.add_argument("--guiding-only", action="store_true", help="only the guided-vs-plain comparison")
+    ap.add_argument("--serving-only", action="store_true", help="only the request-loop traces")
     ap.add_argument("--guide-budget-ms", type=float, default=1000.0)
     ap.add_argument("--guide-width", type=int, default=1280)
     ap.add_argument("--guide-height", type=int, default=720)
@@ -463,6 +546,10 @@ def main():
         return run_reference(args, rank)
     if args.guide_profile:
         return guide_profile(int(os.environ.get("LOCAL_RANK", "0")), args.guide_profile)
+    if args.serving_only:
+        dev = int(os.environ.get("LOCAL_RANK", "0"))
+        print(json.dumps({"serving": serving(dev), "batch": batch_mix(dev)}), flush=True)
+        return 0
     if args.guiding_only:
         print(json.dumps(guiding(int(os.environ.get("LOCAL_RANK", "0")), args.guide_budget_ms, args.guide_width,
                                  args.guide_height)), flush=True)
@@ -558,6 +645,7 @@ def main():
     f12 = f12_loop(local_rank, js, cam) if rank == 0 and world == 1 and not args.no_f12 else None
     quality = c1_quality(local_rank) if rank == 0 and not args.no_quality else None
     serve = serving(local_rank) if rank == 0 and world == 1 and not args.no_serving else None
+    batch = batch_mix(local_rank) if rank == 0 and world == 1 and not args.no_serving else None
     guide = (guiding(local_rank, args.guide_budget_ms, args.guide_width, args.guide_height)
              if rank == 0 and world == 1 and not args.no_guiding else None)
 
@@ -587,7 +675,7 @@ def main():
                         for k, v in kern.items()},
             "mrays_per_s": mrays, "segments_per_step": segs, "shadow_rays_per_step": shadows,
             "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": cpu, "quality": quality,
-            "serving": serve, "guiding": guide, "scene_upload": upload, "f12": f12,
+            "serving": serve, "batch": batch, "guiding": guide, "scene_upload": upload, "f12": f12,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -383,6 +383,42 @@ def _grid_quad(origin, du, dv, nu, nv, skip=None):
     return np.array(verts), np.array(tris, dtype=np.int64)
 
 
+def _grid_quad_fast(origin, du, dv, nu, nv):
+    """_grid_quad without openings, vectorised: (nu + 1) x (nv + 1) shared
+    vertices, two triangles per cell."""
+    o, du, dv = (np.asarray(a, np.float64) for a in (origin, du, dv))
+    i, j = np.meshgrid(np.arange(nu + 1) / nu, np.arange(nv + 1) / nv)
+    verts = o + i.reshape(-1, 1) * du + j.reshape(-1, 1) * dv
+    ci, cj = np.meshgrid(np.arange(nu), np.arange(nv))
+    a = (cj * (nu + 1) + ci).reshape(-1)
+    b, c, d = a + 1, a + nu + 2, a + nu + 1
+    tris = np.stack([np.stack([a, b, c], 1), np.stack([a, c, d], 1)], 1).reshape(-1, 3)
+    return verts, tris.astype(np.int64)
+
+
+def cornell_variant(seed: int, triangles: int):
+    """A seeded variant of the Cornell box with about `triangles` triangles:
+    the five walls split into k x k grids, wall colours and box rotations
+    varied, the same two boxes, ceiling light and camera."""
+    rng = np.random.default_rng(seed)
+    k = max(1, int(round(np.sqrt(max(triangles - 26, 10) / 10.0))))
+    jitter = lambda c: tuple(float(x) for x in np.clip(np.asarray(c) * rng.uniform(0.8, 1.2, 3), 0.0, 0.95))
+    white, red, green = jitter((0.73, 0.73, 0.73)), jitter((0.63, 0.065, 0.05)), jitter((0.14, 0.45, 0.09))
+    wall = lambda col: material(col, 0.0, 1.0)
+    meshes = [mesh(*_grid_quad_fast((0, 0, 0), (0, 0, 1), (1, 0, 0), k, k), wall(white)),   # floor
+              mesh(*_grid_quad_fast((0, 1, 0), (1, 0, 0), (0, 0, 1), k, k), wall(white)),   # ceiling
+              mesh(*_grid_quad_fast((0, 0, 0), (1, 0, 0), (0, 1, 0), k, k), wall(white)),   # back
+              mesh(*_grid_quad_fast((0, 0, 0), (0, 1, 0), (0, 0, 1), k, k), wall(red)),     # left
+              mesh(*_grid_quad_fast((1, 0, 0), (0, 0, 1), (0, 1, 0), k, k), wall(green)),   # right
+              mesh(*box((0.3, 0.3, 0.3), (0.66, 0.0, 0.62), float(rng.uniform(-30, 0))), wall(white)),
+              mesh(*box((0.3, 0.6, 0.3), (0.34, 0.0, 0.36), float(rng.uniform(0, 30))), wall(white))]
+    lv, lt = quad((0.375, 0.999, 0.4), (0.625, 0.999, 0.4), (0.625, 0.999, 0.6), (0.375, 0.999, 0.6))
+    meshes.append(mesh(lv, lt, material((0.78, 0.78, 0.78), 0.0, 1.0, emission=(17.0, 12.0, 4.0))))
+    scene = {"meshes": meshes, "native_lights": [], "environment": {"color": [0.0, 0.0, 0.0], "strength": 1.0}}
+    camera = (0.5, 0.5, 1.95, 0.0, 0.0, -1.0, 0.0, 1.0, 0.0, 40.0)
+    return scene, camera
+
+
 def hard_indirect_scene():
     """A 12 x 12 x 4 m room (diffuse walls, albedo 0.6; glossy floor,
     roughness 0.2) lit only through a 0.5 m wide, 2.25 m high door gap from
