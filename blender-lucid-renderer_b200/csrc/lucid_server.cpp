@@ -35,9 +35,11 @@ double Server::now() const {
 Server::Server(int device, int slots, long long budget_bytes) : device_(device) {
     slots = std::max(1, slots);
     if (budget_bytes <= 0) {
+        // 70 % of the free memory: the rest holds the path pools slots keep
+        // between jobs
         size_t free_b = 0, total_b = 0;
         cudaSetDevice(device);
-        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) budget_bytes = (long long)(free_b * 0.8);
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) budget_bytes = (long long)(free_b * 0.7);
         else budget_bytes = 1LL << 30;
     }
     budget_ = budget_bytes;
@@ -178,7 +180,21 @@ void Server::slot_loop(int slot) {
             if (busy_from_ < 0) busy_from_ = j->t_start;
         }
         cv_.notify_all();   // another slot may start the next job too
-        int rc = run_job(*slot_eng_[slot], *j, slot, false);
+        // the slot keeps its path pool (and a guided job's buffers) for the
+        // next job: freeing device memory synchronises the whole device and
+        // would stall every other slot's work
+        int rc = run_job(*slot_eng_[slot], *j, slot, true);
+        if (rc == LUCID_ERR_OOM) {   // a pool grown by earlier jobs may be in the way: release it and retry once
+            slot_eng_[slot]->guide_free();
+            slot_eng_[slot]->accum_end();
+            slot_eng_[slot]->release_pool();
+            if (pre_eng_[slot]) pre_eng_[slot]->release_pool();
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                j->error.clear();
+            }
+            rc = run_job(*slot_eng_[slot], *j, slot, true);
+        }
         finish_job(*j, rc);
     }
 }
@@ -346,10 +362,12 @@ int Server::run_guided_job(Engine& e, Job& j, int slot, bool keep_pool) {
         if (rc == LUCID_OK) j.image.swap(img);
     }
     if (rc != LUCID_OK) j.error = e.last_error();
-    // the guide's buffers and the accumulator were counted in this job's bytes
-    e.guide_free();
-    e.accum_end();
-    if (!keep_pool) e.release_pool();
+    e.guide_enable(false, 0);
+    if (!keep_pool) {
+        e.guide_free();
+        e.accum_end();
+        e.release_pool();
+    }
     return rc;
 }
 

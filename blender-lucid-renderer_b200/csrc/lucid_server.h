@@ -9,7 +9,9 @@
 // as slots and device memory free up; a slot running a batch job also runs
 // waiting interactive jobs between the batch job's iterations, on a second
 // engine, so that they never wait for a long render
-// (HBM budget = uploaded scenes + every running job's path state and film);
+// (HBM budget = uploaded scenes + every running job's path state and film;
+// slots keep their path pools between jobs, since freeing device memory
+// synchronises the device, and the default budget leaves room for them);
 // a job that could never fit is refused at submission.  Scene edits make a
 // new scene version; a job renders the version current when it was
 // submitted.  Guided jobs (the "mis" integrator with online path guiding)

@@ -468,8 +468,9 @@ typedef struct LucidServerStats {
     long long bytes_reserved, bytes_running, budget_bytes;
 } LucidServerStats;
 
-/* slots: concurrent jobs; budget_bytes: device memory the server may use
- * (0 = 80 % of the free memory). */
+/* slots: concurrent jobs; budget_bytes: device memory the jobs may use
+ * (0 = 70 % of the free memory; slots keep their path pools between jobs
+ * outside this budget). */
 int lucid_server_create(int device, int slots, long long budget_bytes, LucidServer** out);
 void lucid_server_destroy(LucidServer* srv);
 const char* lucid_server_last_error(LucidServer* srv);
