@@ -362,6 +362,42 @@ def serving(device: int, seed: int = 7, slots: int = 2, seconds: float = 2.0) ->
             "slots": slots, "samples_per_s": total / wall_mix, "samples_per_s_sequential": total / wall_seq}
 
 
+def diagnostics(device: int) -> dict:
+    """Path diagnostics at scale (render_tile with diagnostics enabled: the
+    diagnostic integrators, device path records, the film replayed on the
+    host in the reference's loop order): the Cornell configuration's 16x16
+    recording window at 16 spp, and a 1920x1080 Cornell frame at 4 spp with
+    the standard preset (subsample 2), each against the same render without
+    diagnostics."""
+    import lucid_capi
+    import lucid_scenes as ls
+    sc, cam = ls.cornell_box()
+    c = lucid_capi.Context(device)
+    c.load_scene_json(ls.to_json(sc))
+    c.set_camera(*cam)
+    c.set_algorithm("mis")
+    out = {}
+    for name, (tx, ty, tw, th, fw, fh, spp) in {"cornell_window_16x16_16spp": (120, 120, 16, 16, 256, 256, 16),
+                                               "cornell_1920x1080_4spp_standard": (0, 0, 1920, 1080, 1920, 1080, 4)}.items():
+        c.diag_disable()
+        c.render(tw, th, fw, fh, spp, 0, 8, tile_x=tx, tile_y=ty)   # warm
+        t0 = time.perf_counter()
+        c.render(tw, th, fw, fh, spp, 0, 8, tile_x=tx, tile_y=ty)
+        plain = time.perf_counter() - t0
+        c.diag_enable(subsample=2)
+        c.render(tw, th, fw, fh, spp, 0, 8, tile_x=tx, tile_y=ty)   # warm (record buffer sized)
+        t0 = time.perf_counter()
+        c.render(tw, th, fw, fh, spp, 0, 8, tile_x=tx, tile_y=ty)
+        wall = time.perf_counter() - t0
+        st = c.diag_stats()
+        out[name] = {"paths": tw * th * spp, "records": int(st[4]) if len(st) > 4 else None,
+                     "film_groups": int(st[2]), "wall_ms": round(1000 * wall, 2),
+                     "plain_wall_ms": round(1000 * plain, 2)}
+    c.diag_disable()
+    c.close()
+    return out
+
+
 def batch_mix(device: int, seed: int = 11, slots: int = 4) -> dict:
     """The batched configuration: 48 render jobs, each on its own seeded
     variant of the Cornell box tessellated to 10k-500k triangles
@@ -548,7 +584,8 @@ def main():
         return guide_profile(int(os.environ.get("LOCAL_RANK", "0")), args.guide_profile)
     if args.serving_only:
         dev = int(os.environ.get("LOCAL_RANK", "0"))
-        print(json.dumps({"serving": serving(dev), "batch": batch_mix(dev)}), flush=True)
+        print(json.dumps({"serving": serving(dev), "batch": batch_mix(dev), "diagnostics": diagnostics(dev)}),
+              flush=True)
         return 0
     if args.guiding_only:
         print(json.dumps(guiding(int(os.environ.get("LOCAL_RANK", "0")), args.guide_budget_ms, args.guide_width,
@@ -646,6 +683,7 @@ def main():
     quality = c1_quality(local_rank) if rank == 0 and not args.no_quality else None
     serve = serving(local_rank) if rank == 0 and world == 1 and not args.no_serving else None
     batch = batch_mix(local_rank) if rank == 0 and world == 1 and not args.no_serving else None
+    diag = diagnostics(local_rank) if rank == 0 and world == 1 and not args.no_serving else None
     guide = (guiding(local_rank, args.guide_budget_ms, args.guide_width, args.guide_height)
              if rank == 0 and world == 1 and not args.no_guiding else None)
 
@@ -675,7 +713,8 @@ def main():
                         for k, v in kern.items()},
             "mrays_per_s": mrays, "segments_per_step": segs, "shadow_rays_per_step": shadows,
             "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": cpu, "quality": quality,
-            "serving": serve, "batch": batch, "guiding": guide, "scene_upload": upload, "f12": f12,
+            "serving": serve, "batch": batch, "diagnostics": diag, "guiding": guide, "scene_upload": upload,
+            "f12": f12,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -11,6 +11,7 @@
 //   k_film                        per-pixel sum in sample order (deterministic)
 // Queues are compacted with warp ballots + one atomic per warp.  Work counts
 // stay on the device; the host enqueues a whole wave without synchronising.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -32,6 +33,7 @@
 #include "lucid_kernels.cuh"
 
 namespace lucid {
+namespace cg = cooperative_groups;
 
 #define CK(call)                                                                              \
     do {                                                                                      \
@@ -1139,9 +1141,20 @@ LD void diag_vertex(DiagPath& P, int32_t obj, uint8_t type, bool delta, V3 p, V3
 // record_completed_path_with_geometry (diagnostic_integrator.hpp:349-389):
 // the path plus a final Emission vertex (object -1 for the environment, else
 // -(light + 2)) when there is room.
+// A record slot per calling thread with one atomic per group of converged
+// lanes (the lanes that complete a path at the same point of the loop);
+// each thread's slots still increase in its own program order, which the
+// host's sort uses to keep records of one (pixel, sample, bounce) in order.
+LD unsigned long long warp_append(unsigned long long* count) {
+    cg::coalesced_group g = cg::coalesced_threads();
+    unsigned long long base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(count, (unsigned long long)g.size());
+    return g.shfl(base, 0) + g.thread_rank();
+}
+
 LD void diag_complete(const DiagOut& o, const DiagPath& P, uint32_t pixel, uint32_t sample, uint32_t seq,
                       uint8_t strategy, int light_id, uint8_t ltype, RGB c, V3 lpos) {
-    unsigned long long slot = atomicAdd(o.count, 1ull);
+    unsigned long long slot = warp_append(o.count);
     if ((long long)slot >= o.cap) return;   // the host grows the buffer and runs the wave again
     DiagRecord* r = o.recs + slot;
     int d = P.depth;
