@@ -390,9 +390,10 @@ def diagnostics(device: int) -> dict:
         c.render(tw, th, fw, fh, spp, 0, 8, tile_x=tx, tile_y=ty)
         wall = time.perf_counter() - t0
         st = c.diag_stats()
+        parts = {k: round(v["total_ms"], 2) for k, v in c.stats()["kernels"].items()}
         out[name] = {"paths": tw * th * spp, "records": int(st[4]) if len(st) > 4 else None,
-                     "film_groups": int(st[2]), "wall_ms": round(1000 * wall, 2),
-                     "plain_wall_ms": round(1000 * plain, 2)}
+                     "record_bytes": 512, "film_groups": int(st[2]), "wall_ms": round(1000 * wall, 2),
+                     "plain_wall_ms": round(1000 * plain, 2), "parts_ms": parts}
     c.diag_disable()
     c.close()
     return out

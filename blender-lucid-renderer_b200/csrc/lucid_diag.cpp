@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <thread>
 
 namespace lucid {
 
@@ -126,24 +127,57 @@ void DiagFilm::clear() {
 
 void DiagFilm::replay(std::vector<DiagRecord>& recs, int tile_w) {
     // the reference's single-threaded loop order: 8x8 micro-tiles row-major,
-    // pixels row-major inside one, samples, records along the path
+    // pixels row-major inside one, samples, records along the path.  Cells
+    // are independent, so the records are bucketed by cell (a stable
+    // counting sort), each cell's bucket is put in that order (ties keep
+    // the records' arrival order, which is each thread's program order), and
+    // the cells are replayed on all host threads.
+    const size_t n = recs.size();
+    if (n == 0 || px_.empty()) return;
     const int nmx = (tile_w + 7) / 8;
+    const size_t ncell = px_.size();
     auto key = [&](const DiagRecord& r) {
         int x = (int)(r.pixel % (uint32_t)tile_w), y = (int)(r.pixel / (uint32_t)tile_w);
         uint64_t order = (uint64_t)((y / 8) * nmx + x / 8) * 64u + (uint64_t)((y % 8) * 8 + (x % 8));
         return (order << 40) | ((uint64_t)r.sample << 16) | (uint64_t)r.seq;
     };
-    std::vector<std::pair<uint64_t, uint32_t>> idx(recs.size());
-    for (size_t i = 0; i < recs.size(); ++i) idx[i] = {key(recs[i]), (uint32_t)i};
-    std::sort(idx.begin(), idx.end());
-    for (const auto& e : idx) {
-        const DiagRecord& r = recs[e.second];
+    auto cell_of = [&](const DiagRecord& r) -> size_t {
         int x = (int)(r.pixel % (uint32_t)tile_w), y = (int)(r.pixel / (uint32_t)tile_w);
         int sx = x / sf_, sy = y / sf_;
-        if (sx >= sw_ || sy >= sh_) continue;
-        px_[(size_t)sy * sw_ + sx].record(r, hash(r), coarse_type(r));
-        ++recorded_;
+        return (sx >= sw_ || sy >= sh_) ? ncell : (size_t)sy * sw_ + sx;
+    };
+    std::vector<uint32_t> start(ncell + 2, 0);
+    std::vector<uint32_t> cell(n);
+    for (size_t i = 0; i < n; ++i) {
+        cell[i] = (uint32_t)cell_of(recs[i]);
+        ++start[cell[i] + 1];
     }
+    for (size_t c = 0; c <= ncell; ++c) start[c + 1] += start[c];
+    std::vector<std::pair<uint64_t, uint32_t>> order(n);
+    {
+        std::vector<uint32_t> fill(start.begin(), start.end() - 1);
+        for (size_t i = 0; i < n; ++i) order[fill[cell[i]]++] = {key(recs[i]), (uint32_t)i};
+    }
+    recorded_ += start[ncell];
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned nt = (unsigned)std::min<size_t>(hw, std::max<size_t>(1, n / 4096));
+    auto work = [&](size_t c0, size_t c1) {
+        for (size_t c = c0; c < c1; ++c) {
+            auto b = order.begin() + start[c], e = order.begin() + start[c + 1];
+            if (e - b > 1) std::sort(b, e);   // (key, arrival index): unique
+            for (auto it = b; it != e; ++it) {
+                const DiagRecord& r = recs[it->second];
+                px_[c].record(r, hash(r), coarse_type(r));
+            }
+        }
+    };
+    if (nt <= 1) {
+        work(0, ncell);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nt; ++t) th.emplace_back(work, ncell * t / nt, ncell * (t + 1) / nt);
+    for (auto& t : th) t.join();
 }
 
 void DiagFilm::record_path(long long x, long long y, const DiagRecord& r, const int16_t* material) {

@@ -2436,12 +2436,14 @@ int Engine::render_diag_impl(const LucidRenderParams& p, float* out_host, float*
     f.records = 0;
 
     stats_ = LucidRenderStats{};
-    cudaEvent_t t0, t1;
+    cudaEvent_t t0, t1, ka, kb, ca, cb;
     cudaEventCreate(&t0);
     cudaEventCreate(&t1);
+    for (cudaEvent_t* e : {&ka, &kb, &ca, &cb}) cudaEventCreate(e);
     cudaEventRecord(t0, st);
     int status = LUCID_OK;
     int waves = 0;
+    double kernel_ms = 0.0, copy_ms = 0.0, replay_ms = 0.0, records_total = 0.0;
     std::vector<DiagRecord> band;
     for (int y0 = 0; y0 < p.tile_h && status == LUCID_OK; y0 += band_rows) {
         const int bh = std::min(band_rows, p.tile_h - y0);
@@ -2457,12 +2459,17 @@ int Engine::render_diag_impl(const LucidRenderParams& p, float* out_host, float*
             unsigned long long produced = 0;
             for (;;) {
                 CK(cudaMemsetAsync(D.count.p, 0, sizeof(unsigned long long), st));
+                cudaEventRecord(ka, st);
                 k_raygen<<<(f.n_wave + 255) / 256, 256, 0, st>>>(f, P.view);
                 DiagOut o{D.recs.p, D.count.p, (long long)D.recs.n};
                 k_diag_paths<<<(f.n_wave + 127) / 128, 128, 0, st>>>(ds_->view, f, P.view, o, y0 * p.tile_w);
+                cudaEventRecord(kb, st);
                 CK(cudaGetLastError());
                 CK(cudaMemcpyAsync(&produced, D.count.p, sizeof(produced), cudaMemcpyDeviceToHost, st));
                 CK(cudaStreamSynchronize(st));
+                float kms = 0.0f;
+                cudaEventElapsedTime(&kms, ka, kb);
+                kernel_ms += kms;
                 if (produced <= (unsigned long long)D.recs.n) break;
                 // the wave is deterministic: grow the buffer and run it again
                 CK(D.recs.alloc((size_t)(produced + produced / 4)));
@@ -2470,13 +2477,36 @@ int Engine::render_diag_impl(const LucidRenderParams& p, float* out_host, float*
             k_film<<<(f.npix + 255) / 256, 256, 0, st>>>(f.npix, this_spw, P.rad.p, P.film.p + (size_t)y0 * p.tile_w);
             const size_t old = band.size();
             band.resize(old + (size_t)produced);
+            cudaEventRecord(ca, st);
             if (produced)
                 CK(cudaMemcpyAsync(band.data() + old, D.recs.p, (size_t)produced * sizeof(DiagRecord),
                                    cudaMemcpyDeviceToHost, st));
+            cudaEventRecord(cb, st);
             CK(cudaStreamSynchronize(st));
+            float cms = 0.0f;
+            cudaEventElapsedTime(&cms, ca, cb);
+            copy_ms += cms;
+            records_total += (double)produced;
             ++waves;
         }
-        if (status == LUCID_OK) diag_film_.replay(band, p.tile_w);
+        if (status == LUCID_OK) {
+            const auto h0 = std::chrono::steady_clock::now();
+            diag_film_.replay(band, p.tile_w);
+            replay_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - h0).count();
+        }
+    }
+    for (cudaEvent_t e : {ka, kb, ca, cb}) cudaEventDestroy(e);
+    // where a diagnostic render's time goes: the path kernel (raygen
+    // included), the record copies to the host, and the host replay
+    const char* names[3] = {"k_diag_paths", "diag_record_copy", "diag_replay_host"};
+    const double ms3[3] = {kernel_ms, copy_ms, replay_ms};
+    stats_.num_kinds = 3;
+    for (int k = 0; k < 3; ++k) {
+        std::snprintf(stats_.kinds[k].name, sizeof(stats_.kinds[k].name), "%s", names[k]);
+        stats_.kinds[k].launches = waves;
+        stats_.kinds[k].total_ms = ms3[k];
+        stats_.kinds[k].units = k == 0 ? (double)np * p.samples : records_total;
+        stats_.kinds[k].algo_bytes = k == 1 ? records_total * sizeof(DiagRecord) : 0.0;
     }
     const int np_i = (int)np;
     k_output<<<(np_i + 255) / 256, 256, 0, st>>>(p.tile_w, p.tile_h, P.film.p, out_device ? (float4*)out_device : P.out.p);
