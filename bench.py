@@ -563,6 +563,7 @@ def main():
     ap.add_argument("--no-guiding", action="store_true", help="skip the guided-vs-plain equal-time comparison")
     ap.add_argument("--guiding-only", action="store_true", help="only the guided-vs-plain comparison")
     ap.add_argument("--serving-only", action="store_true", help="only the request-loop traces")
+    ap.add_argument("--diagnostics-only", action="store_true", help="only the path-diagnostics timings")
     ap.add_argument("--guide-budget-ms", type=float, default=1000.0)
     ap.add_argument("--guide-width", type=int, default=1280)
     ap.add_argument("--guide-height", type=int, default=720)
@@ -583,6 +584,9 @@ def main():
         return run_reference(args, rank)
     if args.guide_profile:
         return guide_profile(int(os.environ.get("LOCAL_RANK", "0")), args.guide_profile)
+    if args.diagnostics_only:
+        print(json.dumps({"diagnostics": diagnostics(int(os.environ.get("LOCAL_RANK", "0")))}), flush=True)
+        return 0
     if args.serving_only:
         dev = int(os.environ.get("LOCAL_RANK", "0"))
         print(json.dumps({"serving": serving(dev), "batch": batch_mix(dev), "diagnostics": diagnostics(dev)}),

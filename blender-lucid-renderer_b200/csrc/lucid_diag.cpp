@@ -112,27 +112,41 @@ void DiagPixel::record(const DiagRecord& r, uint64_t h, uint8_t coarse_t) {
     init_from(groups[mi]);
 }
 
+// A film of the same cell count as the last one only resets the cells that
+// recorded paths since (a 1080p film at subsample 2 holds 4 GB of cells).
 void DiagFilm::init(int tile_w, int tile_h, int subsample) {
     w_ = tile_w; h_ = tile_h; sf_ = std::max(1, subsample);
     sw_ = w_ / sf_; sh_ = h_ / sf_;
-    px_.assign((size_t)sw_ * sh_, DiagPixel());
+    const size_t n = (size_t)sw_ * sh_;
+    if (px_.size() == n && dirty_.size() == n) {
+        clear();
+    } else {
+        px_.assign(n, DiagPixel());
+        dirty_.assign(n, 0);
+    }
     recorded_ = 0;
     valid_ = true;
 }
 
 void DiagFilm::clear() {
-    for (auto& p : px_) p = DiagPixel();
+    if (dirty_.size() != px_.size()) {
+        for (auto& p : px_) p = DiagPixel();
+        dirty_.assign(px_.size(), 0);
+    } else {
+        const DiagPixel empty;
+        for (size_t c = 0; c < px_.size(); ++c)
+            if (dirty_[c]) { px_[c] = empty; dirty_[c] = 0; }
+    }
     recorded_ = 0;
 }
 
-void DiagFilm::replay(std::vector<DiagRecord>& recs, int tile_w) {
+void DiagFilm::replay(const DiagRecord* recs, size_t n, int tile_w) {
     // the reference's single-threaded loop order: 8x8 micro-tiles row-major,
     // pixels row-major inside one, samples, records along the path.  Cells
     // are independent, so the records are bucketed by cell (a stable
     // counting sort), each cell's bucket is put in that order (ties keep
     // the records' arrival order, which is each thread's program order), and
     // the cells are replayed on all host threads.
-    const size_t n = recs.size();
     if (n == 0 || px_.empty()) return;
     const int nmx = (tile_w + 7) / 8;
     const size_t ncell = px_.size();
@@ -158,12 +172,17 @@ void DiagFilm::replay(std::vector<DiagRecord>& recs, int tile_w) {
         std::vector<uint32_t> fill(start.begin(), start.end() - 1);
         for (size_t i = 0; i < n; ++i) order[fill[cell[i]]++] = {key(recs[i]), (uint32_t)i};
     }
-    recorded_ += start[ncell];
+    const size_t in_film = start[ncell];
+    recorded_ += in_film;
+    if (in_film == 0) return;
+    if (dirty_.size() != ncell) dirty_.assign(ncell, 1);
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const unsigned nt = (unsigned)std::min<size_t>(hw, std::max<size_t>(1, n / 4096));
+    const unsigned nt = (unsigned)std::min<size_t>(hw, std::max<size_t>(1, in_film / 4096));
     auto work = [&](size_t c0, size_t c1) {
         for (size_t c = c0; c < c1; ++c) {
             auto b = order.begin() + start[c], e = order.begin() + start[c + 1];
+            if (b == e) continue;
+            dirty_[c] = 1;
             if (e - b > 1) std::sort(b, e);   // (key, arrival index): unique
             for (auto it = b; it != e; ++it) {
                 const DiagRecord& r = recs[it->second];
@@ -175,8 +194,18 @@ void DiagFilm::replay(std::vector<DiagRecord>& recs, int tile_w) {
         work(0, ncell);
         return;
     }
+    // split the cells so that each thread gets about the same number of
+    // records (a band's records fill only the band's rows of cells)
+    std::vector<size_t> cut(nt + 1, ncell);
+    cut[0] = 0;
+    for (unsigned t = 1; t < nt; ++t) {
+        const uint32_t target = (uint32_t)(in_film * t / nt);
+        cut[t] = (size_t)(std::upper_bound(start.begin(), start.begin() + ncell + 1, target) - start.begin()) - 1;
+        cut[t] = std::max(cut[t], cut[t - 1]);
+    }
     std::vector<std::thread> th;
-    for (unsigned t = 0; t < nt; ++t) th.emplace_back(work, ncell * t / nt, ncell * (t + 1) / nt);
+    for (unsigned t = 0; t < nt; ++t)
+        if (cut[t + 1] > cut[t]) th.emplace_back(work, cut[t], cut[t + 1]);
     for (auto& t : th) t.join();
 }
 
@@ -184,7 +213,9 @@ void DiagFilm::record_path(long long x, long long y, const DiagRecord& r, const 
     if (!valid_ || x < 0 || y < 0) return;
     const long long sx = x / sf_, sy = y / sf_;
     if (sx >= sw_ || sy >= sh_) return;
-    px_[(size_t)sy * sw_ + sx].record(r, hash(r, material), coarse_type(r));
+    const size_t c = (size_t)sy * sw_ + sx;
+    px_[c].record(r, hash(r, material), coarse_type(r));
+    if (c < dirty_.size()) dirty_[c] = 1;
     ++recorded_;
 }
 

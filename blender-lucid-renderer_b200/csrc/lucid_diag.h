@@ -73,9 +73,9 @@ class DiagFilm {
 public:
     void init(int tile_w, int tile_h, int subsample);
     void clear();
-    void reset() { px_.clear(); valid_ = false; w_ = h_ = sw_ = sh_ = 0; recorded_ = 0; }
+    void reset() { px_.clear(); dirty_.clear(); valid_ = false; w_ = h_ = sw_ = sh_ = 0; recorded_ = 0; }
     // Sorts the records into the reference's loop order and replays them.
-    void replay(std::vector<DiagRecord>& records, int tile_w);
+    void replay(const DiagRecord* records, size_t n, int tile_w);
     // DiagnosticFilm::record_path (diagnostic_film.hpp:94-106): one path at
     // film pixel (x, y); out-of-range pixels are ignored.  material: the
     // vertices' material ids (the path hash includes them).
@@ -111,6 +111,7 @@ private:
     bool valid_ = false;
     size_t recorded_ = 0;
     std::vector<DiagPixel> px_;
+    std::vector<unsigned char> dirty_;   // cells that recorded a path since they were last reset
 };
 
 }  // namespace lucid

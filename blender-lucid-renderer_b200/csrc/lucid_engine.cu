@@ -174,6 +174,23 @@ struct GuideState {
 struct DiagDevice {
     DBuf<DiagRecord> recs;
     DBuf<unsigned long long> count;
+    // pinned host copy of one band's records (kept between calls: page-locked
+    // copies run at full link speed and the buffer is not zero-filled)
+    DiagRecord* host = nullptr;
+    size_t host_cap = 0;
+    ~DiagDevice() { if (host) cudaFreeHost(host); }
+    cudaError_t reserve_host(size_t n, size_t keep) {
+        if (n <= host_cap) return cudaSuccess;
+        const size_t cap = n + n / 4;
+        DiagRecord* h = nullptr;
+        cudaError_t e = cudaHostAlloc(reinterpret_cast<void**>(&h), cap * sizeof(DiagRecord), cudaHostAllocDefault);
+        if (e != cudaSuccess) return e;
+        if (host && keep) std::memcpy(h, host, keep * sizeof(DiagRecord));
+        if (host) cudaFreeHost(host);
+        host = h;
+        host_cap = cap;
+        return cudaSuccess;
+    }
 };
 
 struct FrameParams {
@@ -2444,13 +2461,13 @@ int Engine::render_diag_impl(const LucidRenderParams& p, float* out_host, float*
     int status = LUCID_OK;
     int waves = 0;
     double kernel_ms = 0.0, copy_ms = 0.0, replay_ms = 0.0, records_total = 0.0;
-    std::vector<DiagRecord> band;
+    size_t band_n = 0;
     for (int y0 = 0; y0 < p.tile_h && status == LUCID_OK; y0 += band_rows) {
         const int bh = std::min(band_rows, p.tile_h - y0);
         f.tile_y = p.tile_y + y0;
         f.tile_h = bh;
         f.npix = bh * p.tile_w;
-        band.clear();
+        band_n = 0;
         for (int s0 = 0; s0 < p.samples; s0 += spw) {
             if (is_cancelled()) { status = LUCID_ERR_CANCELLED; break; }
             const int this_spw = std::min(spw, p.samples - s0);
@@ -2475,12 +2492,12 @@ int Engine::render_diag_impl(const LucidRenderParams& p, float* out_host, float*
                 CK(D.recs.alloc((size_t)(produced + produced / 4)));
             }
             k_film<<<(f.npix + 255) / 256, 256, 0, st>>>(f.npix, this_spw, P.rad.p, P.film.p + (size_t)y0 * p.tile_w);
-            const size_t old = band.size();
-            band.resize(old + (size_t)produced);
+            CK(D.reserve_host(band_n + (size_t)produced, band_n));
             cudaEventRecord(ca, st);
             if (produced)
-                CK(cudaMemcpyAsync(band.data() + old, D.recs.p, (size_t)produced * sizeof(DiagRecord),
+                CK(cudaMemcpyAsync(D.host + band_n, D.recs.p, (size_t)produced * sizeof(DiagRecord),
                                    cudaMemcpyDeviceToHost, st));
+            band_n += (size_t)produced;
             cudaEventRecord(cb, st);
             CK(cudaStreamSynchronize(st));
             float cms = 0.0f;
@@ -2491,7 +2508,7 @@ int Engine::render_diag_impl(const LucidRenderParams& p, float* out_host, float*
         }
         if (status == LUCID_OK) {
             const auto h0 = std::chrono::steady_clock::now();
-            diag_film_.replay(band, p.tile_w);
+            diag_film_.replay(D.host, band_n, p.tile_w);
             replay_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - h0).count();
         }
     }
