@@ -571,6 +571,7 @@ def main():
                     help="only N guided 640x360 renders of the hard-indirect room (a target for ncu captures of "
                          "the guide kernels); prints no bench line")
     ap.add_argument("--wave", type=int, default=0, help="paths per wave (0: the engine's default)")
+    ap.add_argument("--launch-profile", type=int, default=0, help="resident-CTA profile of the wavefront kernels")
     ap.add_argument("--width", type=int, default=W, help="smaller frames for profiling captures")
     ap.add_argument("--height", type=int, default=H)
     ap.add_argument("--spp", type=int, default=SPP)
@@ -615,6 +616,8 @@ def main():
     ctx.set_algorithm(ALGO)
     if args.wave:
         ctx.set_wave_capacity(args.wave)
+    if args.launch_profile:
+        ctx.set_launch_profile(args.launch_profile)
     stats0 = ctx.scene_stats()
     log(f"[rank {rank}] {ctx.device_info()} scene {stats0} load {load_s:.2f}s")
     dev = torch.device("cuda", local_rank)

@@ -359,6 +359,10 @@ int lucid_cuda_guide_max_depth(LucidCudaCtx* ctx, int max_depth) {
     return guarded(ctx, [&](lucid::Engine& e) { return e.guide_max_depth(max_depth); });
 }
 
+int lucid_cuda_set_launch_profile(LucidCudaCtx* ctx, int profile) {
+    return guarded(ctx, [&](lucid::Engine& e) { return e.set_launch_profile(profile); });
+}
+
 int lucid_cuda_update_scene(LucidCudaCtx* ctx, const LucidSceneEdit* edits, int count) {
     return guarded(ctx, [&](lucid::Engine& e) { return e.update_scene(edits, count); });
 }

@@ -133,9 +133,8 @@ void DiagFilm::clear() {
         for (auto& p : px_) p = DiagPixel();
         dirty_.assign(px_.size(), 0);
     } else {
-        const DiagPixel empty;
         for (size_t c = 0; c < px_.size(); ++c)
-            if (dirty_[c]) { px_[c] = empty; dirty_[c] = 0; }
+            if (dirty_[c]) { px_[c].reset(); dirty_[c] = 0; }
     }
     recorded_ = 0;
 }

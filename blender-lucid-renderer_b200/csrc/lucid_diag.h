@@ -67,6 +67,13 @@ struct DiagPixel {   // PixelPathData<16, 4>
     size_t num_groups = 0, num_outliers = 0, total = 0, overflow = 0;
     DiagStats total_stats;
     void record(const DiagRecord& r, uint64_t hash, uint8_t coarse_type);
+    // Back to an empty cell: counters and statistics (group and outlier
+    // entries past the counts are never read, so they are left as they are).
+    void reset() {
+        num_groups = num_outliers = total = overflow = 0;
+        total_stats = DiagStats();
+        for (auto& c : coarse) c = DiagStats();
+    }
 };
 
 class DiagFilm {

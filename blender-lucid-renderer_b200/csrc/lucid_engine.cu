@@ -389,8 +389,9 @@ __global__ void __launch_bounds__(128) k_trace_primary(DevScene sc, FrameParams 
 // Nine resident CTAs per SM (at most 56 registers): one more warp group to
 // hide node-fetch latency than the unconstrained 61 registers allow
 // (1M-triangle scene: 8 CTAs 232 ms, 9 CTAs 221 ms, 10 CTAs 225 ms).
-__global__ void __launch_bounds__(128, 9) k_trace(DevScene sc, PathView pv, int* cnt, int identity, int records,
-                                                 int bins) {
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) k_trace_lb(DevScene sc, PathView pv, int* cnt, int identity, int records,
+                                                      int bins) {
     __shared__ int hist[kBins];
     BinHist bh{hist};
     bh.clear(bins);
@@ -838,9 +839,9 @@ LD ShadeResult shade_path(const DevScene& sc, const FrameParams& f, const PathVi
 // hundred bytes of spills): the extra warps hide more of the shading
 // kernel's instruction-fetch and memory latency than the spills cost
 // (measured on the 1M-triangle scene: 4, 5, 6, 7, 8 CTAs per SM).
-template <int ALGO, bool GUIDE = false>
-__global__ void __launch_bounds__(128, 8) k_shade(DevScene sc, FrameParams f, PathView pv, int* cnt, int* cnt_next,
-                                               int identity, int* qin, int* qout) {
+template <int ALGO, bool GUIDE = false, int MINB = 8>
+__global__ void __launch_bounds__(128, MINB) k_shade(DevScene sc, FrameParams f, PathView pv, int* cnt, int* cnt_next,
+                                                  int identity, int* qin, int* qout) {
     const int n = *(volatile int*)&cnt[0];
     for (;;) {
         int base = warp_fetch(&cnt[3]);
@@ -860,16 +861,18 @@ __global__ void __launch_bounds__(128, 8) k_shade(DevScene sc, FrameParams f, Pa
 }
 
 using ShadeKernel = void (*)(DevScene, FrameParams, PathView, int*, int*, int, int*, int*);
-static ShadeKernel shade_kernel(int algo, bool guide = false) {
-    if (guide && algo == ALGO_MIS) return k_shade<ALGO_MIS, true>;
+template <int MINB>
+static ShadeKernel shade_kernel_lb(int algo, bool guide) {
+    if (guide && algo == ALGO_MIS) return k_shade<ALGO_MIS, true, MINB>;
     switch (algo) {
-        case ALGO_SIMPLE: return k_shade<ALGO_SIMPLE>;
-        case ALGO_MIS: return k_shade<ALGO_MIS>;
-        case ALGO_VOLUME_SIMPLE: return k_shade<ALGO_VOLUME_SIMPLE>;
-        case ALGO_VOLUME_MIS: return k_shade<ALGO_VOLUME_MIS>;
-        default: return k_shade<ALGO_NEE>;
+        case ALGO_SIMPLE: return k_shade<ALGO_SIMPLE, false, MINB>;
+        case ALGO_MIS: return k_shade<ALGO_MIS, false, MINB>;
+        case ALGO_VOLUME_SIMPLE: return k_shade<ALGO_VOLUME_SIMPLE, false, MINB>;
+        case ALGO_VOLUME_MIS: return k_shade<ALGO_VOLUME_MIS, false, MINB>;
+        default: return k_shade<ALGO_NEE, false, MINB>;
     }
 }
+static ShadeKernel shade_kernel(int algo, bool guide = false) { return shade_kernel_lb<8>(algo, guide); }
 
 // ---------------------------------------------------------------- shading bins
 // The scatter half of the counting sort whose histogram the trace kernels
@@ -973,7 +976,8 @@ __global__ void __launch_bounds__(32 * kInferWarps, 1) k_guide_infer(DevScene sc
 // boundaries (path_tracer.hpp:103-119) with any-hit BVH queries; a segment
 // ends at the nearest boundary-only hit, past which the probe advances 1 mm.
 // Nine resident CTAs per SM as for k_trace (shadow time -0.7 %; 10: +4 %).
-__global__ void __launch_bounds__(128, 9) k_shadow(DevScene sc, PathView pv, int* cnt, int records) {
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) k_shadow_lb(DevScene sc, PathView pv, int* cnt, int records) {
     const int n = *(volatile int*)&cnt[1];
     int stack[kStack];
     Trav s;
@@ -1046,6 +1050,25 @@ __global__ void __launch_bounds__(128, 9) k_shadow(DevScene sc, PathView pv, int
         active = false;
     }
     if (!ok) atomicAdd(&pv.errors[0], 1);
+}
+
+// ---------------------------------------------------------------- launch profiles
+// Resident CTAs per SM of the wavefront kernels (their register caps):
+// profile 0 is the measured optimum on the 1M-triangle scene (closest hit 9,
+// shading 8, shadow 9); profile 1 gives each kernel more registers and fewer
+// spills (8, 6, 8), which scenes with short paths or few triangles can
+// prefer.  The request loop's autotuner picks per job shape.
+using TraceKernel = void (*)(DevScene, PathView, int*, int, int, int);
+using ShadowKernel = void (*)(DevScene, PathView, int*, int);
+struct LaunchSet {
+    TraceKernel trace;
+    ShadeKernel shade;
+    ShadowKernel shadow;
+};
+constexpr int kLaunchProfiles = 2;
+static LaunchSet launch_set(int algo, bool guide, int profile) {
+    if (profile == 1) return {k_trace_lb<8>, shade_kernel_lb<6>(algo, guide), k_shadow_lb<8>};
+    return {k_trace_lb<9>, shade_kernel_lb<8>(algo, guide), k_shadow_lb<9>};
 }
 
 // ---------------------------------------------------------------- film
@@ -2719,9 +2742,12 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
 
     // persistent grids: a whole number of CTAs per SM
     int occ_t = 1, occ_s = 1, occ_h = 1, occ_t0 = 1;
+    const LaunchSet ks = launch_set(algo_, guide, launch_profile_);
+    const TraceKernel k_trace = ks.trace;
+    const ShadowKernel k_shadow = ks.shadow;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t0, k_trace_primary, 128, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t, k_trace, 128, 0);
-    const ShadeKernel shade = shade_kernel(algo_, guide);
+    const ShadeKernel shade = ks.shade;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, shade, 128, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, k_shadow, 128, 0);
     const int g_trace0 = num_sms_ * std::max(1, occ_t0);
@@ -3000,6 +3026,7 @@ struct JobState {
     DBuf<int> dyn;
     FrameParams f{};
     int g_trace0 = 0, g_trace = 0, g_shade = 0, g_shadow = 0, g_bin = 0;
+    int profile = 0;   // launch profile of the job's kernels
 };
 
 long long Engine::job_bytes(int w, int h, int chunk) {
@@ -3015,7 +3042,10 @@ void Engine::enqueue_iteration(void* fp, int n) {
     f.s0 = 0;
     f.samples = n;
     f.n_wave = n * f.npix;
-    const ShadeKernel shade = shade_kernel(algo_);
+    const LaunchSet ks = launch_set(algo_, false, J.profile);
+    const ShadeKernel shade = ks.shade;
+    const TraceKernel k_trace = ks.trace;
+    const ShadowKernel k_shadow = ks.shadow;
     const int bins = (algo_ == ALGO_VOLUME_MIS || algo_ == ALGO_VOLUME_SIMPLE) ? 1 : 0;
     cudaMemsetAsync(P.counters.p, 0, sizeof(int) * kCountersPerDepth * (J.depth + 1), st);
     for (int depth = 0; depth < J.depth; ++depth) {
@@ -3067,17 +3097,8 @@ int Engine::job_begin(int w, int h, int spp, int max_depth, int chunk, bool use_
     f.max_depth = max_depth; f.algo = algo_;
     f.npix = (int)np;
     f.jitter = spp > 1 ? 1 : 0;
-    int occ_t = 1, occ_s = 1, occ_h = 1, occ_t0 = 1;
-    const ShadeKernel shade = shade_kernel(algo_);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t0, k_trace_primary, 128, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t, k_trace, 128, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, shade, 128, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, k_shadow, 128, 0);
-    J.g_trace0 = num_sms_ * std::max(1, occ_t0);
-    J.g_trace = num_sms_ * std::max(1, occ_t);
-    J.g_shade = num_sms_ * std::max(1, occ_s);
-    J.g_shadow = num_sms_ * std::max(1, occ_h);
-    J.g_bin = num_sms_ * 8;
+    J.profile = launch_profile_;
+    job_grids_locked();
     for (int k = 0; k < 2; ++k)
         if (!J.ev[k]) CK(cudaEventCreateWithFlags(&J.ev[k], cudaEventDisableTiming));
     J.issued = 0;
@@ -3102,6 +3123,44 @@ int Engine::capture_locked(int chunk) {
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) { J.graph = nullptr; return fail(LUCID_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e)); }
     J.chunk = chunk;
+    return LUCID_OK;
+}
+
+// Persistent grids of the job's kernels for its launch profile: a whole
+// number of CTAs per SM.
+void Engine::job_grids_locked() {
+    JobState& J = *job_;
+    const LaunchSet ks = launch_set(algo_, false, J.profile);
+    int occ_t = 1, occ_s = 1, occ_h = 1, occ_t0 = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t0, k_trace_primary, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t, ks.trace, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, ks.shade, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, ks.shadow, 128, 0);
+    J.g_trace0 = num_sms_ * std::max(1, occ_t0);
+    J.g_trace = num_sms_ * std::max(1, occ_t);
+    J.g_shade = num_sms_ * std::max(1, occ_s);
+    J.g_shadow = num_sms_ * std::max(1, occ_h);
+    J.g_bin = num_sms_ * 8;
+}
+
+int Engine::set_launch_profile(int profile) {
+    GpuLock gl(*this);
+    if (profile < 0 || profile >= kLaunchProfiles) return fail(LUCID_ERR_INVALID, "unknown launch profile");
+    launch_profile_ = profile;
+    return LUCID_OK;
+}
+
+int Engine::job_set_profile(int profile, bool use_graph) {
+    GpuLock gl(*this);
+    if (!job_ || !job_->active) return fail(LUCID_ERR_INVALID, "no job");
+    if (profile < 0 || profile >= kLaunchProfiles) return fail(LUCID_ERR_INVALID, "unknown launch profile");
+    CK(cudaSetDevice(device_));
+    // iterations in flight were enqueued with the old grids; they finish first
+    CK(cudaStreamSynchronize(S(stream_)));
+    job_->profile = profile;
+    job_grids_locked();
+    if (use_graph) return capture_locked(job_->chunk);
+    if (job_->graph) { cudaGraphExecDestroy(job_->graph); job_->graph = nullptr; }
     return LUCID_OK;
 }
 
@@ -3457,9 +3516,9 @@ int Engine::render_noalloc(const LucidRenderParams& p, float* d_out) {
         if (g[0] == 0) {
             int occ[4] = {1, 1, 1, 1};
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], k_trace_primary, 128, 0);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], k_trace, 128, 0);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], k_trace_lb<9>, 128, 0);
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], shade, 128, 0);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[3], k_shadow, 128, 0);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[3], k_shadow_lb<9>, 128, 0);
             for (int k = 0; k < 4; ++k) g[k] = num_sms_ * std::max(1, occ[k]);
         }
         for (int k = 0; k < 4; ++k) grid[k] = g[k];
@@ -3511,9 +3570,9 @@ int Engine::render_noalloc(const LucidRenderParams& p, float* d_out) {
             int* qout = (depth & 1) ? q0 : q1;
             pv.q0 = qin;
             if (depth == 0) k_trace_primary<<<g_trace0, 128, 0, st>>>(ds_->view, f, pv, cnt, 0, -1);
-            else k_trace<<<g_trace, 128, 0, st>>>(ds_->view, pv, cnt, 0, 0, -1);
+            else k_trace_lb<9><<<g_trace, 128, 0, st>>>(ds_->view, pv, cnt, 0, 0, -1);
             shade<<<g_shade, 128, 0, st>>>(ds_->view, f, pv, cnt, cnt_next, depth == 0, qin, qout);
-            k_shadow<<<g_shadow, 128, 0, st>>>(ds_->view, pv, cnt, 0);
+            k_shadow_lb<9><<<g_shadow, 128, 0, st>>>(ds_->view, pv, cnt, 0);
         }
         k_film<<<(f.npix + 255) / 256, 256, 0, st>>>(f.npix, this_spw, v.rad, film);
         CK(cudaGetLastError());

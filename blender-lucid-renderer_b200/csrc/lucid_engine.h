@@ -93,6 +93,11 @@ public:
     static long long job_bytes(int w, int h, int chunk);
     int job_begin(int w, int h, int spp, int max_depth, int chunk, bool use_graph);
     int job_set_chunk(int chunk, bool use_graph);
+    // Launch profile (resident CTAs per SM of the wavefront kernels; 0 the
+    // default, 1 more registers per thread) of renders and of the job.
+    int set_launch_profile(int profile);
+    int job_set_profile(int profile, bool use_graph);
+    int launch_profile() const { return launch_profile_; }
     int job_iterate(int sample_offset, int n);
     int job_wait();
     int job_output(float* out_host);
@@ -124,6 +129,7 @@ private:
     void enqueue_iteration(void* frame_params, int n);
     void job_end_locked();
     int capture_locked(int chunk);
+    void job_grids_locked();
     int build_ploc(const float4* verts, const int* sorted_ids, int n, int2* child, int2* range, float* nbox,
                    int* slot_ids, int& root);
     void free_scene();
@@ -146,6 +152,7 @@ private:
     float scene_lo_[3] = {0, 0, 0}, scene_hi_[3] = {1, 1, 1};
     PathPool* pool_ = nullptr;
     long long wave_cap_ = 0;  // 0 = automatic
+    int launch_profile_ = 0;
     std::atomic<bool> cancel_{false};
     std::string err_;
     LucidRenderStats stats_{};

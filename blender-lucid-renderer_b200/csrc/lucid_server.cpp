@@ -257,30 +257,56 @@ int Server::pick_chunk(Engine& e, Job& j, int id, int& offset) {
     {
         std::lock_guard<std::mutex> lk(mu_);
         auto it = tuned_.find(key);
-        if (it != tuned_.end()) return std::min(it->second, j.chunk_max);
+        if (it != tuned_.end()) {
+            if (it->second.second != 0) {
+                int rc = e.job_set_profile(it->second.second, false);
+                if (rc != LUCID_OK) return -rc;
+            }
+            return std::min(it->second.first, j.chunk_max);
+        }
     }
-    int best = 1;
-    double best_rate = -1.0;
-    for (int c = 1; c <= j.chunk_max && offset + c <= d.samples; c *= 2) {
+    auto timed = [&](int c, double& ms) {
         auto t = std::chrono::steady_clock::now();
         int rc = e.job_iterate(offset, c);
         if (rc == LUCID_OK) rc = e.job_wait();
-        if (rc != LUCID_OK) return -rc;
-        double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
+        if (rc != LUCID_OK) return rc;
+        ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
         offset += c;
-        {
-            std::lock_guard<std::mutex> lk(mu_);
-            j.done = offset;
-            if (j.t_first == 0) j.t_first = now();
-        }
+        std::lock_guard<std::mutex> lk(mu_);
+        j.done = offset;
+        if (j.t_first == 0) j.t_first = now();
+        return LUCID_OK;
+    };
+    int best = 1;
+    double best_rate = -1.0, best_ms = 0.0;
+    for (int c = 1; c <= j.chunk_max && offset + c <= d.samples; c *= 2) {
+        double ms = 0.0;
+        int rc = timed(c, ms);
+        if (rc != LUCID_OK) return -rc;
         double rate = c / std::max(ms, 1e-3);
         bool ok = !d.interactive || ms <= kInteractiveMs || c == 1;
-        if (ok && rate > best_rate) { best_rate = rate; best = c; }
+        if (ok && rate > best_rate) { best_rate = rate; best = c; best_ms = ms; }
         if (d.interactive && ms > kInteractiveMs) break;
+    }
+    // then the launch profiles (resident CTAs per SM) at that size, when the
+    // job has samples left for a trial of each
+    int best_profile = 0, cur_profile = 0;
+    for (int prof = 1; prof < 2 && offset + best <= d.samples; ++prof) {
+        int rc = e.job_set_profile(prof, false);
+        if (rc != LUCID_OK) return -rc;
+        cur_profile = prof;
+        double ms = 0.0;
+        rc = timed(best, ms);
+        if (rc != LUCID_OK) return -rc;
+        if (ms < best_ms) { best_ms = ms; best_profile = prof; }
+    }
+    if (cur_profile != best_profile) {
+        int rc = e.job_set_profile(best_profile, false);
+        if (rc != LUCID_OK) return -rc;
     }
     (void)id;
     std::lock_guard<std::mutex> lk(mu_);
-    tuned_[key] = best;
+    tuned_[key] = {best, best_profile};
     return best;
 }
 

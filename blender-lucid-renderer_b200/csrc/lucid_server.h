@@ -12,7 +12,8 @@
 // (HBM budget = uploaded scenes + every running job's path state and film;
 // slots keep their path pools between jobs, since freeing device memory
 // synchronises the device, and the default budget leaves room for them);
-// a job that could never fit is refused at submission.  Scene edits make a
+// a job that could never fit is refused at submission.  The autotuner also
+// picks the kernels' launch profile (resident CTAs per SM).  Scene edits make a
 // new scene version; a job renders the version current when it was
 // submitted.  Guided jobs (the "mis" integrator with online path guiding)
 // train their own guide and count its buffers in their bytes.  Each slot picks the
@@ -100,7 +101,7 @@ private:
     std::condition_variable cv_, done_cv_;
     std::deque<int> queue_;
     std::map<int, Job> jobs_;
-    std::map<std::string, int> tuned_;   // autotuned samples per iteration
+    std::map<std::string, std::pair<int, int>> tuned_;   // autotuned samples per iteration and launch profile
     Admission adm_;
     int next_id_ = 1;
     bool stop_ = false;

@@ -277,6 +277,7 @@ SIGNATURES = {
     "lucid_path_trace_hash": (ctypes.c_uint64, [ctypes.POINTER(PathTrace)]),
     "lucid_path_trace_coarse_type": (_I, [ctypes.POINTER(PathTrace)]),
     "lucid_cuda_update_scene": (_I, [_P, _P, _I]),
+    "lucid_cuda_set_launch_profile": (_I, [_P, _I]),
     "lucid_server_update_scene": (_I, [_P, _I, _P, _I]),
     "lucid_server_create": (_I, [_I, _I, ctypes.c_longlong, ctypes.POINTER(_P)]),
     "lucid_server_destroy": (None, [_P]),
@@ -391,6 +392,9 @@ class Context:
         sd, keep = _scene_desc(arrays)
         self._check(self.lib.lucid_cuda_load_scene_arrays(self.h, ctypes.byref(sd)))
         del keep
+
+    def set_launch_profile(self, profile: int) -> None:
+        self._check(self.lib.lucid_cuda_set_launch_profile(self.h, profile))
 
     def update_scene(self, edits, check=True) -> int:
         """lucid_cuda_update_scene with scene_edits(edits)."""

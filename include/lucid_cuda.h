@@ -248,6 +248,12 @@ int lucid_cuda_render_noalloc(LucidCudaCtx* ctx, const LucidRenderParams* params
  * the primary hit, no jitter, Y-flipped RGBA. */
 int lucid_cuda_render_debug(LucidCudaCtx* ctx, int tile_x, int tile_y, int tile_w, int tile_h, int full_w,
                             int full_h, const char* mode, float* out_rgba);
+/* Launch profile of the wavefront kernels for this context's renders
+ * (no counterpart in the reference): 0 (default) runs closest-hit, shading
+ * and shadow kernels at 9 / 8 / 9 resident CTAs per SM, the measured optimum
+ * on large scenes; 1 at 8 / 6 / 8, more registers per thread and fewer
+ * spills.  Images are identical under both. */
+int lucid_cuda_set_launch_profile(LucidCudaCtx* ctx, int profile);
 /* Statistics of the last render (kernel times need LUCID_RENDER_PROFILE). */
 int lucid_cuda_get_stats(LucidCudaCtx* ctx, LucidRenderStats* out);
 /* Path-pool capacity in paths (0 = automatic).  A render processes

@@ -98,3 +98,18 @@ def test_against_golden_fixtures(ctx, workdir, name):
     r = compare_records(grec, frec)
     assert r["primary"] == 0 and r["hash"] == 0 and r["counts"] == 0 and r["rgb"] == 0, r
     np.testing.assert_allclose(gimg, fimg, rtol=1e-4, atol=1e-5)
+
+
+@pytest.mark.parametrize("scene,algo", [("cornell", "mis"), ("all_lights", "volume_mis"), ("procedural_small", "nee")])
+def test_launch_profiles_give_identical_samples(ctx, workdir, scene, algo):
+    """The launch profiles change only the kernels' resident CTAs per SM (and
+    so their register caps): every sample stays bit-identical."""
+    sc, cam = scene_and_camera(scene, workdir)
+    out = []
+    for prof in (0, 1):
+        ctx.set_launch_profile(prof)
+        out.append(render_gpu(ctx, sc, cam, algo, 40, 30, 4, 8, offset=2))
+    ctx.set_launch_profile(0)
+    (i0, r0), (i1, r1) = out
+    assert np.array_equal(r0["hash"], r1["hash"])
+    assert np.array_equal(i0.view(np.uint32), i1.view(np.uint32))
