@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <atomic>
 #include <thread>
 
 namespace lucid {
@@ -142,10 +143,10 @@ void DiagFilm::clear() {
 void DiagFilm::replay(const DiagRecord* recs, size_t n, int tile_w) {
     // the reference's single-threaded loop order: 8x8 micro-tiles row-major,
     // pixels row-major inside one, samples, records along the path.  Cells
-    // are independent, so the records are bucketed by cell (a stable
-    // counting sort), each cell's bucket is put in that order (ties keep
-    // the records' arrival order, which is each thread's program order), and
-    // the cells are replayed on all host threads.
+    // are independent, so the records are bucketed by cell, each cell's
+    // bucket is sorted by (order key, arrival index) -- unique, and the
+    // arrival index keeps each thread's program order for ties -- and the
+    // cells are replayed, all on the host's threads.
     if (n == 0 || px_.empty()) return;
     const int nmx = (tile_w + 7) / 8;
     const size_t ncell = px_.size();
@@ -154,35 +155,48 @@ void DiagFilm::replay(const DiagRecord* recs, size_t n, int tile_w) {
         uint64_t order = (uint64_t)((y / 8) * nmx + x / 8) * 64u + (uint64_t)((y % 8) * 8 + (x % 8));
         return (order << 40) | ((uint64_t)r.sample << 16) | (uint64_t)r.seq;
     };
-    auto cell_of = [&](const DiagRecord& r) -> size_t {
+    auto cell_of = [&](const DiagRecord& r) -> uint32_t {
         int x = (int)(r.pixel % (uint32_t)tile_w), y = (int)(r.pixel / (uint32_t)tile_w);
         int sx = x / sf_, sy = y / sf_;
-        return (sx >= sw_ || sy >= sh_) ? ncell : (size_t)sy * sw_ + sx;
+        return (sx >= sw_ || sy >= sh_) ? (uint32_t)ncell : (uint32_t)((size_t)sy * sw_ + sx);
     };
-    std::vector<uint32_t> start(ncell + 2, 0);
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned nt = (unsigned)std::min<size_t>(hw, std::max<size_t>(1, n / 4096));
+    auto parallel = [&](auto&& fn) {   // fn(t, i0, i1) over the records
+        if (nt <= 1) { fn(0u, (size_t)0, n); return; }
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t < nt; ++t) th.emplace_back(fn, t, n * t / nt, n * (t + 1) / nt);
+        for (auto& x : th) x.join();
+    };
+    // counting sort by cell (bucket order inside a cell does not matter: the
+    // per-cell sort below fixes it)
+    std::vector<std::atomic<uint32_t>> count(ncell + 1);
+    for (auto& c : count) c.store(0, std::memory_order_relaxed);
     std::vector<uint32_t> cell(n);
-    for (size_t i = 0; i < n; ++i) {
-        cell[i] = (uint32_t)cell_of(recs[i]);
-        ++start[cell[i] + 1];
-    }
-    for (size_t c = 0; c <= ncell; ++c) start[c + 1] += start[c];
+    parallel([&](unsigned, size_t i0, size_t i1) {
+        for (size_t i = i0; i < i1; ++i) {
+            cell[i] = cell_of(recs[i]);
+            count[cell[i]].fetch_add(1, std::memory_order_relaxed);
+        }
+    });
+    std::vector<uint32_t> start(ncell + 2, 0);
+    for (size_t c = 0; c <= ncell; ++c) start[c + 1] = start[c] + count[c].load(std::memory_order_relaxed);
+    for (size_t c = 0; c <= ncell; ++c) count[c].store(start[c], std::memory_order_relaxed);
     std::vector<std::pair<uint64_t, uint32_t>> order(n);
-    {
-        std::vector<uint32_t> fill(start.begin(), start.end() - 1);
-        for (size_t i = 0; i < n; ++i) order[fill[cell[i]]++] = {key(recs[i]), (uint32_t)i};
-    }
+    parallel([&](unsigned, size_t i0, size_t i1) {
+        for (size_t i = i0; i < i1; ++i)
+            order[count[cell[i]].fetch_add(1, std::memory_order_relaxed)] = {key(recs[i]), (uint32_t)i};
+    });
     const size_t in_film = start[ncell];
     recorded_ += in_film;
     if (in_film == 0) return;
     if (dirty_.size() != ncell) dirty_.assign(ncell, 1);
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const unsigned nt = (unsigned)std::min<size_t>(hw, std::max<size_t>(1, in_film / 4096));
     auto work = [&](size_t c0, size_t c1) {
         for (size_t c = c0; c < c1; ++c) {
             auto b = order.begin() + start[c], e = order.begin() + start[c + 1];
             if (b == e) continue;
             dirty_[c] = 1;
-            if (e - b > 1) std::sort(b, e);   // (key, arrival index): unique
+            if (e - b > 1) std::sort(b, e);
             for (auto it = b; it != e; ++it) {
                 const DiagRecord& r = recs[it->second];
                 px_[c].record(r, hash(r), coarse_type(r));
