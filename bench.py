@@ -75,9 +75,9 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def profile_traffic(kernel: str):
-    """DRAM bytes per unit of work of `kernel` from the committed ncu summary
-    (profiles/*.md lines 'traffic_bytes_per_unit <kernel> <bytes>')."""
+def profile_figure(name: str, kernel: str):
+    """A per-unit figure of `kernel` from the committed ncu summaries
+    (profiles/*.md lines '<name> <kernel> <value>')."""
     d = os.path.join(REPO, "profiles")
     if not os.path.isdir(d):
         return None
@@ -87,9 +87,39 @@ def profile_traffic(kernel: str):
         with open(os.path.join(d, fn)) as f:
             for line in f:
                 parts = line.strip().strip("`").split()
-                if len(parts) == 3 and parts[0] == "traffic_bytes_per_unit" and parts[1] == kernel:
+                if len(parts) == 3 and parts[0] == name and parts[1] == kernel:
                     return float(parts[2])
     return None
+
+
+def profile_traffic(kernel: str):
+    """DRAM bytes per unit of work of `kernel` (traffic_bytes_per_unit)."""
+    return profile_figure("traffic_bytes_per_unit", kernel)
+
+
+SM_COUNT, SCHEDULERS_PER_SM = 148, 4
+
+
+def issue_roofline(kern: dict, sm_mhz):
+    """Issue-slot roofline of the traversal and shading kernels: warp
+    instructions per unit of work (ncu smsp__inst_executed.sum over a whole
+    render, divided by its units; profiles/*.md 'inst_per_unit' lines) times
+    the kernel's live unit rate, against one warp instruction per scheduler
+    per cycle (148 SMs x 4 schedulers x the median SM clock sampled during
+    the timed region).  'lanes' is the mean active lanes per issued
+    instruction from the same capture (SIMT efficiency = lanes / 32)."""
+    if not sm_mhz:
+        return None
+    peak = SM_COUNT * SCHEDULERS_PER_SM * sm_mhz * 1e6
+    out = {}
+    for k, v in kern.items():
+        ipu = profile_figure("inst_per_unit", k)
+        if ipu is None or not v["total_ms"]:
+            continue
+        rate = ipu * v["units"] / (v["total_ms"] / 1000.0)
+        out[k] = {"inst_per_unit": ipu, "achieved_ginst_s": rate / 1e9, "peak_ginst_s": peak / 1e9,
+                  "frac": rate / peak, "lanes": profile_figure("lanes_per_inst", k)}
+    return out or None
 
 
 class ClockSampler:
@@ -701,6 +731,7 @@ def main():
         cpu = {"value": float(vals[0]), "unit": "samples/s", "cores": threads, "kind": kind, "sample": sample}
 
     if rank == 0:
+        clocks = clk.summary()
         line = {
             "metric": "samples/s", "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -719,8 +750,9 @@ def main():
             "kernels": {k: {"launches": v["launches"], "ms": round(v["total_ms"], 3), "units": v["units"],
                             "share": round(v["total_ms"] / sum(x["total_ms"] for x in kern.values()), 4)}
                         for k, v in kern.items()},
+            "issue": issue_roofline(kern, clocks["sm_mhz"]),
             "mrays_per_s": mrays, "segments_per_step": segs, "shadow_rays_per_step": shadows,
-            "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": cpu, "quality": quality,
+            "gpu_launches": launches, "clocks": clocks, "cpu_baseline": cpu, "quality": quality,
             "serving": serve, "batch": batch, "diagnostics": diag, "guiding": guide, "scene_upload": upload,
             "f12": f12,
         }

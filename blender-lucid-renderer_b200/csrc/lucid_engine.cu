@@ -101,9 +101,9 @@ struct PathView {
     int* q1;
     int* qs;
     int* qb;           // shading queue binned by event / material class
-    unsigned char* cls;   // class of each path's pending event
+    unsigned short* cls;  // shading bin of each path's pending event
     int* counters;     // per depth: [0] active, [1] shadow, [2..4] fetch cursors,
-                       // [8, 8 + kBins) class counts, then kBins class cursors
+                       // [8, 8 + kBins) bin counts, then kBins bin cursors
     int* errors;       // [0] traversal stack overflow
     int2* rec_prim;
     int4* rec_cnt;     // bounces, nee tests, nee occluded
@@ -119,7 +119,13 @@ struct PathView {
     int gdepth;        // vertices at path depth < gdepth are guided
     float glo[3], gscale[3];   // scene box -> [0,1]^3
 };
-constexpr int kBins = 16;
+// Shading bins: the event / material class (bin_class, 16 values) times
+// the cell of the hit point in a 4 x 4 x 4 grid over the scene box.
+constexpr int kClassBins = 16;
+constexpr int kCellBits = 2;                       // per axis
+constexpr int kCellDim = 1 << kCellBits;
+constexpr int kCells = 1 << (3 * kCellBits);
+constexpr int kBins = kClassBins * kCells;
 constexpr int kCountersPerDepth = 8 + 2 * kBins;
 constexpr int kMaxDepth = 1024;
 
@@ -130,7 +136,7 @@ struct PathPool {
     DBuf<float4> ray_o, ray_d, thr, rad, hit, sh_o, sh_d, sh_c;
     DBuf<float2> lhit;
     DBuf<int> q0, q1, qs, qb, counters, errors;
-    DBuf<unsigned char> cls;
+    DBuf<unsigned short> cls;
     DBuf<int2> rec_prim;
     DBuf<int4> rec_cnt;
     DBuf<unsigned long long> rec_hash;
@@ -322,26 +328,46 @@ LD int bin_class(const DevScene& sc, int prim, float t, int li, float lt, V3 o, 
     return c;
 }
 
-// Per-block class histogram of the rays a trace kernel finished
-// (bins < 0: no binning; else bins != 0 adds the volume bit), flushed to
-// the depth's class counters when the block ends.
+// Cell of a surface hit point: its Morton index in the kCellDim^3 grid over
+// the scene box, so that neighbouring bins hold neighbouring cells.  Paths
+// shaded in bin order hand the trace and shadow kernels rays whose origins
+// lie close together (neighbouring lanes then walk similar BVH nodes).
+LD int bin_cell(const DevScene& sc, V3 p) {
+    const float c[3] = {p.x, p.y, p.z};
+    int m = 0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        int q = (int)((c[a] - sc.bin_lo[a]) * sc.bin_scale[a]);
+        q = min(max(q, 0), kCellDim - 1);
+#pragma unroll
+        for (int b = 0; b < kCellBits; ++b) m |= ((q >> b) & 1) << (3 * b + a);
+    }
+    return m;
+}
+
+// Per-block histogram of the shading bins of the rays a trace kernel
+// finished (bins < 0: no binning; else bins != 0 adds the volume bit),
+// flushed to the depth's bin counters when the block ends.
 struct BinHist {
     int* h;
     LD void clear(int bins) {
-        if (bins >= 0 && threadIdx.x < kBins) h[threadIdx.x] = 0;
+        if (bins >= 0)
+            for (int i = threadIdx.x; i < kBins; i += blockDim.x) h[i] = 0;
         __syncthreads();
     }
     LD void add(const DevScene& sc, const PathView& pv, int id, int bins, int prim, float t, int li, float lt, V3 o,
                 V3 d) {
         if (bins < 0) return;
-        int c = bin_class(sc, prim, t, li, lt, o, d, bins != 0);
-        pv.cls[id] = (unsigned char)c;
-        atomicAdd(&h[c], 1);
+        const int c = bin_class(sc, prim, t, li, lt, o, d, bins != 0);
+        const int key = c * kCells + ((c & 7) != 0 ? bin_cell(sc, o + d * t) : 0);
+        pv.cls[id] = (unsigned short)key;
+        atomicAdd(&h[key], 1);
     }
     LD void flush(int bins, int* cnt) {
         if (bins < 0) return;
         __syncthreads();
-        if (threadIdx.x < kBins && h[threadIdx.x]) atomicAdd(&cnt[8 + threadIdx.x], h[threadIdx.x]);
+        for (int i = threadIdx.x; i < kBins; i += blockDim.x)
+            if (h[i]) atomicAdd(&cnt[8 + i], h[i]);
     }
 };
 
@@ -878,11 +904,33 @@ static ShadeKernel shade_kernel(int algo, bool guide = false) { return shade_ker
 // The scatter half of the counting sort whose histogram the trace kernels
 // build (bin_class): one atomic per class per warp, paths of a class kept
 // together so neighbouring warps shade the same kind of event.
-__global__ void __launch_bounds__(256) k_bin_scatter(PathView pv, int* cnt, int identity, const int* qin, int* qb) {
+constexpr int kBinThreads = 256;
+static_assert(kBins % kBinThreads == 0, "bins per scatter thread");
+__global__ void __launch_bounds__(kBinThreads) k_bin_scatter(PathView pv, int* cnt, int identity, const int* qin,
+                                                             int* qb) {
     __shared__ int base[kBins];
-    if (threadIdx.x == 0) {
-        int sum = 0;
-        for (int c = 0; c < kBins; ++c) { base[c] = sum; sum += cnt[8 + c]; }
+    __shared__ int wsum[kBinThreads / 32];
+    {
+        // exclusive prefix sum of the bin counts: kPer bins per thread, then a
+        // block scan of the per-thread sums
+        constexpr int kPer = kBins / kBinThreads;
+        int loc[kPer], sum = 0;
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) { loc[j] = sum; sum += cnt[8 + threadIdx.x * kPer + j]; }
+        const int lane = (int)(threadIdx.x & 31), w = (int)(threadIdx.x >> 5);
+        int x = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[w] = x;
+        __syncthreads();
+        int before = 0;
+        for (int k = 0; k < w; ++k) before += wsum[k];
+        const int excl = before + x - sum;
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) base[threadIdx.x * kPer + j] = excl + loc[j];
     }
     __syncthreads();
     const int n = *(volatile int*)&cnt[0];
@@ -2106,6 +2154,11 @@ int Engine::build_bvh() {
         if (!H.prim_boundary[p] && !is_big[p]) real.push_back(p);
     int n = (int)real.size();
     DevScene& v = D.view;
+    for (int a = 0; a < 3; ++a) {
+        const float ext = hi[a] - lo[a];
+        v.bin_lo[a] = ext > 0.0f ? lo[a] : 0.0f;
+        v.bin_scale[a] = ext > 0.0f ? (float)kCellDim / ext : 0.0f;
+    }
     {
         cudaError_t e = D.big_tris.alloc(big.size());
         if (e != cudaSuccess) return fail(LUCID_ERR_OOM, "big triangle list allocation failed");

@@ -113,6 +113,8 @@ struct DevScene {
     int num_volumes;
     const float* grid;
     int has_boundary;
+    // scene box -> shading-bin cells (the spatial part of the shading sort)
+    float bin_lo[3], bin_scale[3];
 };
 
 }  // namespace lucid
