@@ -63,7 +63,7 @@ struct DBuf {
 };
 
 struct DeviceScene {
-    DBuf<float4> bvh_tris, bnd_tris, big_tris, prim_fn, prim_vn;
+    DBuf<float4> bvh_tris, bnd_tris, bnd_box, big_tris, prim_fn, prim_vn, light_bsph;
     DBuf<int4> prim_info;
     DBuf<unsigned char> prim_cls;
     DBuf<int> guide;
@@ -80,7 +80,7 @@ struct DeviceScene {
     std::shared_ptr<DeviceScene> base;
     void release() {
         base.reset();
-        bvh_tris.release(); bnd_tris.release(); big_tris.release(); prim_fn.release(); prim_vn.release(); prim_info.release();
+        bvh_tris.release(); bnd_tris.release(); bnd_box.release(); light_bsph.release(); big_tris.release(); prim_fn.release(); prim_vn.release(); prim_info.release();
         prim_cls.release(); nodes.release(); nodes2.release(); guide.release(); materials.release(); tex_ops.release(); prim_uv.release(); lights.release(); cdf.release(); grid.release(); volumes.release();
     }
 };
@@ -451,7 +451,7 @@ __global__ void __launch_bounds__(128, MINB) k_trace_lb(DevScene sc, PathView pv
                 HitRec real = s.h;
                 HitRec b = real;
                 if (real.prim < 0) b.t = 1e30f;
-                boundary_closest(sc, s.o, s.d, search, b);
+                boundary_closest<true>(sc, s.o, s.d, s.inv, search, b);
                 if (b.prim < 0) { res.prim = -1; res.t = 1e30f; break; }
                 if (b.prim == real.prim) { res = real; break; }
                 search = b.t + 1e-3f;
@@ -466,7 +466,9 @@ __global__ void __launch_bounds__(128, MINB) k_trace_lb(DevScene sc, PathView pv
         }
         if (res.prim < 0) { res.t = 1e30f; res.u = 0.0f; res.v = 0.0f; }
         float lt = 1e30f;
-        int li = (depth == 0) ? -1 : native_lights_closest(sc, s.o, s.d, lt);
+        // a native light counts only in front of the surface hit (the shading
+        // kernel's `lh.y < hh.x`): lights beyond it are not tested
+        int li = (depth == 0) ? -1 : native_lights_closest(sc, s.o, s.d, res.t, lt);
         pv.hit[id] = make_float4(res.t, res.u, res.v, __int_as_float(res.prim));
         pv.lhit[id] = make_float2(__int_as_float(li), lt);
         bh.add(sc, pv, id, bins, res.prim, res.t, li, lt, s.o, s.d);
@@ -1023,6 +1025,10 @@ __global__ void __launch_bounds__(32 * kInferWarps, 1) k_guide_infer(DevScene sc
 // Shadow rays (persistent, dynamic refill): is_shadowed_skipping_volume_
 // boundaries (path_tracer.hpp:103-119) with any-hit BVH queries; a segment
 // ends at the nearest boundary-only hit, past which the probe advances 1 mm.
+// The boundary triangles are tested one after another, without the group
+// boxes the closest-hit kernels use: on the 1M-triangle scene the box tests
+// made this kernel 4 % slower (more registers at its 56-register cap),
+// while they save the closest-hit kernels 7 %.
 // Nine resident CTAs per SM as for k_trace (shadow time -0.7 %; 10: +4 %).
 template <int MINB>
 __global__ void __launch_bounds__(128, MINB) k_shadow_lb(DevScene sc, PathView pv, int* cnt, int records) {
@@ -1048,7 +1054,7 @@ __global__ void __launch_bounds__(128, MINB) k_shadow_lb(DevScene sc, PathView p
                 bt = -1.0f;
                 if (sc.num_bnd_tris) {
                     HitRec b; b.t = rem; b.u = 0.f; b.v = 0.f; b.prim = -1;
-                    boundary_closest(sc, po, d, RAY_T_MIN, b);
+                    boundary_closest_all(sc, po, d, RAY_T_MIN, b);
                     if (b.prim >= 0) bt = b.t;
                 }
                 trav_begin<true>(s, sc, po, d, RAY_T_MIN, bt >= 0.0f ? bt : rem);
@@ -1073,7 +1079,7 @@ __global__ void __launch_bounds__(128, MINB) k_shadow_lb(DevScene sc, PathView p
                     else {
                         bt = -1.0f;
                         HitRec b; b.t = rem; b.u = 0.f; b.v = 0.f; b.prim = -1;
-                        boundary_closest(sc, po, d, RAY_T_MIN, b);
+                        boundary_closest_all(sc, po, d, RAY_T_MIN, b);
                         if (b.prim >= 0) bt = b.t;
                         trav_begin<true>(s, sc, po, d, RAY_T_MIN, bt >= 0.0f ? bt : rem);
                         if (s.any_hit) outcome = 1;
@@ -1287,7 +1293,7 @@ __global__ void __launch_bounds__(128) k_diag_paths(DevScene sc, FrameParams f, 
         const uint32_t seq = (uint32_t)depth * 2u;
         HitRec h = scene_closest(sc, o, d, tmin, 1e30f, ok);
         float lt = 1e30f;
-        int li = (depth == 0) ? -1 : native_lights_closest(sc, o, d, lt);
+        int li = (depth == 0) ? -1 : native_lights_closest(sc, o, d, 1e30f, lt);
         if (li >= 0 && (h.prim < 0 || lt < h.t)) {
             if (!nee_only || depth == 0) {
                 const DevLight& L = sc.lights[sc.native_start + li];
@@ -1923,6 +1929,7 @@ int Engine::update_scene(const LucidSceneEdit* edits, int count) {
     };
     CK(up(nv->materials, H.materials));
     CK(up(nv->lights, H.lights));
+    CK(up(nv->light_bsph, native_light_bounds(H)));
     CK(up(nv->cdf, H.cdf));
     CK(up(nv->guide, H.light_guide));
     CK(up(nv->prim_cls, cls));
@@ -1930,6 +1937,7 @@ int Engine::update_scene(const LucidSceneEdit* edits, int count) {
     nv->view = ds_->view;
     nv->view.materials = nv->materials.p;
     nv->view.lights = nv->lights.p;
+    nv->view.light_bsph = H.num_native > 0 ? nv->light_bsph.p : nullptr;
     nv->view.light_cdf = nv->cdf.p;
     nv->view.light_guide = nv->guide.p;
     nv->view.prim_cls = nv->prim_cls.p;
@@ -1999,6 +2007,7 @@ int Engine::upload_scene(HostScene&& hs) {
     CK(up(D.tex_ops, H.tex_ops));
     CK(up(D.prim_uv, H.prim_uv));
     CK(up(D.lights, H.lights));
+    CK(up(D.light_bsph, native_light_bounds(H)));
     CK(up(D.cdf, H.cdf));
     CK(up(D.guide, H.light_guide));
     CK(up(D.volumes, H.volumes));
@@ -2020,6 +2029,7 @@ int Engine::upload_scene(HostScene&& hs) {
     v.num_lights = (int)H.lights.size();
     v.native_start = H.native_start;
     v.num_native = H.num_native;
+    v.light_bsph = H.num_native > 0 ? D.light_bsph.p : nullptr;
     v.total_light_area = H.total_light_area;
     for (int k = 0; k < 3; ++k) v.env[k] = H.env[k];
     v.volumes = D.volumes.p;
@@ -2131,6 +2141,59 @@ int Engine::build_bvh() {
         for (int a = 0; a < 3; ++a)
             maxabs = std::max(maxabs, std::max(std::fabs(vol.wmin[a]), std::fabs(vol.wmax[a])));
     for (int a = 0; a < 3; ++a) { scene_lo_[a] = lo[a]; scene_hi_[a] = hi[a]; }
+    {
+        // boundary-only triangles grouped by mesh (they are stored in prim
+        // order), each group with its bounding box padded as the BVH's boxes
+        std::vector<float4> boxes;
+        const float bpad = maxabs * 9.5367431640625e-07f + 1e-30f;
+        int k = 0;
+        for (int p = 0; p < H.num_prims; ++p) {
+            if (!H.prim_boundary[p]) continue;
+            const int mesh = H.prim_info[(size_t)p].x;
+            bool fresh = boxes.empty();
+            if (!fresh) {
+                int last_mesh;
+                std::memcpy(&last_mesh, &boxes[boxes.size() - 1].w, 4);   // scratch: mesh id of the open group
+                fresh = last_mesh != mesh;
+            }
+            if (fresh) {
+                float first;
+                std::memcpy(&first, &k, 4);
+                float m;
+                std::memcpy(&m, &mesh, 4);
+                boxes.push_back(make_float4(1e30f, 1e30f, 1e30f, first));
+                boxes.push_back(make_float4(-1e30f, -1e30f, -1e30f, m));
+            }
+            float4& blo = boxes[boxes.size() - 2];
+            float4& bhi = boxes[boxes.size() - 1];
+            for (int c = 0; c < 3; ++c) {
+                const float4& q = H.verts[3 * p + c];
+                blo.x = std::min(blo.x, q.x); blo.y = std::min(blo.y, q.y); blo.z = std::min(blo.z, q.z);
+                bhi.x = std::max(bhi.x, q.x); bhi.y = std::max(bhi.y, q.y); bhi.z = std::max(bhi.z, q.z);
+            }
+            ++k;
+        }
+        // close the groups: pad the boxes, replace the mesh id by the count
+        for (size_t g = 0; g < boxes.size(); g += 2) {
+            int first, next;
+            std::memcpy(&first, &boxes[g].w, 4);
+            if (g + 2 < boxes.size()) std::memcpy(&next, &boxes[g + 2].w, 4);
+            else next = k;
+            const int count = next - first;
+            boxes[g].x -= bpad; boxes[g].y -= bpad; boxes[g].z -= bpad;
+            boxes[g + 1].x += bpad; boxes[g + 1].y += bpad; boxes[g + 1].z += bpad;
+            std::memcpy(&boxes[g + 1].w, &count, 4);
+        }
+        DeviceScene& Db = D;
+        cudaError_t e = Db.bnd_box.alloc(std::max<size_t>(1, boxes.size()));
+        if (e != cudaSuccess) return fail(LUCID_ERR_OOM, "boundary box allocation failed");
+        if (!boxes.empty())
+            CK(cudaMemcpyAsync(Db.bnd_box.p, boxes.data(), boxes.size() * sizeof(float4), cudaMemcpyHostToDevice,
+                               S(stream_)));
+        Db.view.bnd_box = boxes.empty() ? nullptr : Db.bnd_box.p;
+        Db.view.num_bnd_groups = (int)(boxes.size() / 2);
+        if (k != Db.view.num_bnd_tris) return fail(LUCID_ERR_CUDA, "boundary triangle groups do not cover the list");
+    }
     float sdiag = std::sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
                             (hi[2] - lo[2]) * (hi[2] - lo[2]));
     const int kMaxBig = 32;
@@ -2424,7 +2487,7 @@ namespace {
 // Algorithmic bytes per unit of work (compulsory SoA traffic; BVH node and
 // triangle fetches are scene-dependent and excluded):
 //   trace : ray 32 + queue id 4 + hit 16 + light hit 8
-//           + the hit prim's class 1 and the shading class 1 (binning) = 62 / ray
+//           + the hit prim's class 1 and the shading bin 2 (binning)   = 63 / ray
 //   shade : queue 4 + hit 24 + ray 32 + throughput 16 + radiance 16 + rng 16
 //           + prim info/normal 32 + material 48  (reads)
 //           + rng 16 + radiance 16 + throughput 16 + ray 32 + queue 4
@@ -2432,11 +2495,11 @@ namespace {
 //   shadow: queue 4 + shadow record 48 + radiance 16 read + 16 write  = 84 / ray
 //   raygen: rng 16 + ray 32 + throughput 16 + radiance 16            = 80 / path
 //   camera trace (generates its rays): the raygen writes 80 + hit 16
-//           + light hit 8 + prim class 1 + shading class 1             = 106 / ray
+//           + light hit 8 + prim class 1 + shading bin 2               = 107 / ray
 //   film  : radiance 16 / path + film 32 / pixel
-//   bin   : queue id 4 + class 1 + binned id 4 (scatter)             = 9 / path
-constexpr double kBytesTrace0 = 106, kBytesTrace = 62, kBytesShade = 340, kBytesShadow = 84, kBytesRaygen = 80, kBytesFilm = 16,
-                 kBytesBin = 9;
+//   bin   : queue id 4 + shading bin 2 + binned id 4 (scatter)       = 10 / path
+constexpr double kBytesTrace0 = 107, kBytesTrace = 63, kBytesShade = 340, kBytesShadow = 84, kBytesRaygen = 80, kBytesFilm = 16,
+                 kBytesBin = 10;
 //   guide : queue 4 + hit 24 + ray 32 + raw outputs 160 w              = 220 / path
 //   train : one record 64 / record (weights are read from shared memory)
 enum Kind { K_RAYGEN, K_TRACE0, K_TRACE, K_SHADE, K_SHADOW, K_FILM, K_BIN, K_GUIDE, K_TRAIN, K_NUM };

@@ -55,6 +55,11 @@ bool apply_scene_edits(HostScene& s, const LucidSceneEdit* edits, int count, std
 // material part of the shading-queue bins): 1 emitter, 2 glass, 3 near-delta
 // metal, 4 metal, 5 other.
 unsigned char prim_shading_class(const DevMaterial& dm);
+// Bounding spheres of the native lights a ray can hit (centre, radius; a
+// negative radius for lights the camera-side intersection skips: spot, sun
+// and point lights without a radius), one per native light: the cheap
+// rejection before the exact native-light tests.
+std::vector<float4> native_light_bounds(const HostScene& s);
 
 struct HostCamera {
     float pos[3] = {0, 0, 0};

@@ -419,9 +419,9 @@ LD bool trav_run(Trav& s, int* stack, float* stack_t, const DevScene& sc, bool& 
     return false;
 }
 
-// Closest boundary-only triangle in [tmin, h.t] by brute force (these are the
-// few triangles of volume-domain cubes).
-LD void boundary_closest(const DevScene& sc, V3 o, V3 d, float tmin, HitRec& h) {
+// Closest boundary-only triangle in [tmin, h.t] over the whole list, one
+// triangle after another.
+LD void boundary_closest_all(const DevScene& sc, V3 o, V3 d, float tmin, HitRec& h) {
     for (int k = 0; k < sc.num_bnd_tris; ++k) {
         V3 v0, e1, e2;
         int prim;
@@ -433,12 +433,35 @@ LD void boundary_closest(const DevScene& sc, V3 o, V3 d, float tmin, HitRec& h) 
     }
 }
 
+// Closest boundary-only triangle in [tmin, h.t] by brute force (these are the
+// few triangles of volume-domain cubes), one mesh's group at a time; with
+// BOXES, behind the conservative test of the group's padded box (inv = the
+// componentwise reciprocal of d).
+template <bool BOXES>
+LD void boundary_closest(const DevScene& sc, V3 o, V3 d, V3 inv, float tmin, HitRec& h) {
+    for (int g = 0; g < sc.num_bnd_groups; ++g) {
+        const float4 lo = __ldg(&sc.bnd_box[2 * g]), hi = __ldg(&sc.bnd_box[2 * g + 1]);
+        float tn;
+        if (BOXES && !box_hit(lo, hi, o, inv, tmin, h.t, tn)) continue;
+        const int first = __float_as_int(lo.w), end = first + __float_as_int(hi.w);
+        for (int k = first; k < end; ++k) {
+            V3 v0, e1, e2;
+            int prim;
+            load_tri(sc.bnd_tris, k, v0, e1, e2, prim);
+            float t, u, v;
+            if (isect_tri(o, d, v0, e1, e2, tmin, h.t, t, u, v)) {
+                if (t < h.t || prim > h.prim) { h.t = t; h.u = u; h.v = v; h.prim = prim; }
+            }
+        }
+    }
+}
+
 // intersectScene over every triangle (geometry/bvh.hpp:155-177).
 LD HitRec scene_closest(const DevScene& sc, V3 o, V3 d, float tmin, float tmax, bool& ok) {
     HitRec h;
     h.t = tmax; h.u = 0.0f; h.v = 0.0f; h.prim = -1;
     ok &= bvh_closest(sc, o, d, tmin, h);
-    if (sc.num_bnd_tris) boundary_closest(sc, o, d, tmin, h);
+    if (sc.num_bnd_tris) boundary_closest<true>(sc, o, d, v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z), tmin, h);
     return h;
 }
 
@@ -451,6 +474,7 @@ LD HitRec closest_skip_boundaries(const DevScene& sc, V3 o, V3 d, float tmin, bo
     real.t = 1e30f; real.u = 0.0f; real.v = 0.0f; real.prim = -1;
     ok &= bvh_closest(sc, o, d, tmin, real);
     if (!sc.num_bnd_tris) return real;
+    const V3 inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
     float search = tmin;
     HitRec none;
     none.t = 1e30f; none.u = 0.0f; none.v = 0.0f; none.prim = -1;
@@ -463,7 +487,7 @@ LD HitRec closest_skip_boundaries(const DevScene& sc, V3 o, V3 d, float tmin, bo
         b.t = (real.prim >= 0) ? real.t : 1e30f; b.u = 0.0f; b.v = 0.0f;
         b.prim = (real.prim >= 0) ? real.prim : -1;
         int real_prim = b.prim;
-        boundary_closest(sc, o, d, search, b);
+        boundary_closest<true>(sc, o, d, inv, search, b);
         if (b.prim < 0) return none;                 // no hit at all
         if (b.prim == real_prim) return real;        // the real surface is closest
         search = b.t + 1e-3f;                        // skip the boundary hit
@@ -477,6 +501,7 @@ LD bool shadowed_skip_boundaries(const DevScene& sc, V3 o, V3 d, float tmax, boo
         if (tmax <= 0.0f) return false;
         return bvh_any(sc, o, d, RAY_T_MIN, tmax, ok);
     }
+    const V3 inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
     V3 po = o;
     float off = 0.0f;
     for (int peek = 0; peek < 8; ++peek) {
@@ -484,7 +509,7 @@ LD bool shadowed_skip_boundaries(const DevScene& sc, V3 o, V3 d, float tmax, boo
         if (rem <= 0.0f) return false;
         HitRec b;
         b.t = rem; b.u = 0.0f; b.v = 0.0f; b.prim = -1;
-        boundary_closest(sc, po, d, RAY_T_MIN, b);
+        boundary_closest<true>(sc, po, d, inv, RAY_T_MIN, b);
         if (b.prim < 0) return bvh_any(sc, po, d, RAY_T_MIN, rem, ok);
         if (bvh_any(sc, po, d, RAY_T_MIN, b.t, ok)) return true;
         float skip = b.t + 1e-3f;
@@ -523,11 +548,25 @@ LD bool isect_planar(V3 o, V3 d, V3 c, V3 n, V3 right, V3 up, float& t, float& x
 }
 
 // intersectNativeLights (scene_lights.hpp:176-246): index into the native
-// light list and distance, or -1.
-LD int native_lights_closest(const DevScene& sc, V3 o, V3 d, float& t_out) {
+// light list and distance of the closest light hit nearer than `bound`, or
+// -1 (bound 1e30: every hit).  Each light is first tested against its
+// bounding sphere (light_bsph): skipped when the ray's line passes farther
+// than the radius from the centre, or when the whole sphere lies behind the
+// ray or beyond the nearest hit so far.  Both rejections keep a relative
+// margin of 1e-5 over the few-ulp rounding of the exact tests below (whose
+// accepted points lie on the light, inside the sphere), so they only skip
+// lights the exact test would reject.
+LD int native_lights_closest(const DevScene& sc, V3 o, V3 d, float bound, float& t_out) {
     int best = -1;
-    float bt = 1e30f;
+    float bt = bound;
     for (int i = 0; i < sc.num_native; ++i) {
+        const float4 bs = __ldg(&sc.light_bsph[i]);
+        if (!(bs.w >= 0.0f)) continue;
+        const V3 oc = v3(bs.x - o.x, bs.y - o.y, bs.z - o.z);
+        const float tca = dot(oc, d), oc2 = dot(oc, oc), r = bs.w;
+        if (oc2 - tca * tca > r * r + 1e-5f * oc2) continue;                  // the line misses the sphere
+        const float slack = 1e-5f * (fabsf(tca) + r) + 1e-30f;
+        if (tca + r < RAY_T_MIN - slack || tca - r > bt + slack) continue;   // behind the ray / beyond bt
         const DevLight& L = sc.lights[sc.native_start + i];
         int type = __float_as_int(L.pos_type.w);
         float t;

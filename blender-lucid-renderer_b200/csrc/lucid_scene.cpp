@@ -17,6 +17,8 @@
 #include <nlohmann/json.hpp>
 #include <stdexcept>
 
+#include <vector_functions.h>
+
 #include "lucid_host.h"
 #include "lucid_math.h"
 #include "lucid_nodes.h"
@@ -795,6 +797,26 @@ void make_camera(HostCamera& c, float px, float py, float pz, float dx, float dy
     c.forward[0] = dir.x; c.forward[1] = dir.y; c.forward[2] = dir.z;
     c.right[0] = right.x; c.right[1] = right.y; c.right[2] = right.z;
     c.up[0] = upc.x; c.up[1] = upc.y; c.up[2] = upc.z;
+}
+
+std::vector<float4> native_light_bounds(const HostScene& S) {
+    std::vector<float4> out((size_t)std::max(0, S.num_native));
+    for (int i = 0; i < S.num_native; ++i) {
+        const DevLight& L = S.lights[(size_t)(S.native_start + i)];
+        int type;
+        std::memcpy(&type, &L.pos_type.w, 4);
+        float r = -1.0f;
+        if (type == LIGHT_POINT && L.emission_radius.w > 1e-6f) {   // the device's MIN_LENGTH test
+            r = L.emission_radius.w;
+        } else if (type == LIGHT_AREA) {
+            // circumscribed radius of the rectangle / ellipse, widened by
+            // 0.1 % for the rounding of the unit right / up vectors
+            const double hx = 0.5 * (double)L.right_sx.w, hy = 0.5 * (double)L.up_sy.w;
+            r = (float)(std::sqrt(hx * hx + hy * hy) * 1.001);
+        }
+        out[(size_t)i] = make_float4(L.pos_type.x, L.pos_type.y, L.pos_type.z, r);
+    }
+    return out;
 }
 
 }  // namespace lucid

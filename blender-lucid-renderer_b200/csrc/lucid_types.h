@@ -79,9 +79,13 @@ struct DevScene {
     int root2;
     int num_bvh_tris;
     int root;                       // root child code (node index or leaf code)
-    // boundary-only triangles (tested by brute force): 3 float4 each
+    // boundary-only triangles (tested by brute force): 3 float4 each, in
+    // groups of one mesh each with a padded bounding box (2 float4 per
+    // group: min xyz | first triangle, max xyz | triangle count)
     const float4* bnd_tris;
     int num_bnd_tris;
+    const float4* bnd_box;
+    int num_bnd_groups;
     // the few triangles whose bounds span a large part of the scene (ground
     // planes, walls) are kept out of the BVH and tested first by brute force:
     // in a Morton-ordered hierarchy they would inflate every box on their
@@ -105,6 +109,7 @@ struct DevScene {
     int num_lights;
     int native_start;
     int num_native;
+    const float4* light_bsph;       // per native light: bounding sphere (radius < 0: never hit by rays)
     float total_light_area;
     // environment
     float env[3];

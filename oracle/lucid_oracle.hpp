@@ -1202,7 +1202,9 @@ inline RGB trace(const Scene& s, const SceneLights& sl, const Ray& ray, int max_
             if (depth == 0) { rec->primary_mesh = hit.hit ? hit.mesh : -1; rec->primary_tri = hit.hit ? hit.tri : -1; }
             hpush(rec, (uint32_t)(hit.hit ? hit.mesh : -1));
             hpush(rec, (uint32_t)(hit.hit ? hit.tri : -1));
-            hpush(rec, (uint32_t)(lh.hit ? lh.index : -1));
+            // the native light hit that takes effect: nearer than the surface
+            // hit (the light branch below and the CUDA trace kernel's bound)
+            hpush(rec, (uint32_t)(lh.hit && (!hit.hit || lh.t < hit.t) ? lh.index : -1));
         }
         if (algo == Algo::VOLUME_SIMPLE) {
             float ts = 1e6f;
