@@ -2274,16 +2274,15 @@ int Engine::build_bvh() {
         return LUCID_OK;
     }
     CK(d_child.alloc(n - 1)); CK(d_range.alloc(n - 1)); CK(d_nbox.alloc((size_t)6 * (n - 1)));
-    const char* builder = std::getenv("LUCID_BVH");
     int root = -1;
     DBuf<int> d_slot;
-    if (!(builder && std::string(builder) == "lbvh")) {
+    {
         CK(d_slot.alloc(n));
         int rc = build_ploc(d_verts.p, d_vals_sorted.p, n, d_child.p, d_range.p, d_nbox.p, d_slot.p, root);
         if (rc != LUCID_OK) return rc;
     }
     const int* slot_ids = root >= 0 ? d_slot.p : d_vals_sorted.p;
-    if (root < 0) {   // Karras LBVH (also the fallback when clustering does not converge)
+    if (root < 0) {   // Karras LBVH: the fallback when clustering does not converge
         CK(d_parent.alloc(n - 1)); CK(d_leaf_parent.alloc(n)); CK(d_arrive.alloc(n - 1));
         CK(cudaMemsetAsync(d_parent.p, 0xff, (n - 1) * sizeof(int), st));   // root's parent = -1
         CK(cudaMemsetAsync(d_arrive.p, 0, (n - 1) * sizeof(int), st));
@@ -2889,9 +2888,9 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
             attr = true;
         }
     }
-    const char* sort_env = std::getenv("LUCID_SHADE_BINS");
-    const bool bin = !(sort_env && sort_env[0] == '0');
-    const int bins = !bin ? -1 : (algo_ == ALGO_VOLUME_MIS || algo_ == ALGO_VOLUME_SIMPLE) ? 1 : 0;
+    // the shading queue is binned at every depth (the volume bit only for
+    // the integrators with media)
+    const int bins = (algo_ == ALGO_VOLUME_MIS || algo_ == ALGO_VOLUME_SIMPLE) ? 1 : 0;
 
     struct Launch { int kind; cudaEvent_t a, b; int depth; };
     std::vector<Launch> launches;
@@ -2952,16 +2951,11 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
                     guide_->net.master());
                 ev_end(e);
             }
-            if (bin) {
-                e = ev_begin(K_BIN, depth);
-                k_bin_scatter<<<g_bin, 256, 0, st>>>(pv, cnt, depth == 0, qin, P.qb.p);
-                ev_end(e);
-            }
+            e = ev_begin(K_BIN, depth);
+            k_bin_scatter<<<g_bin, 256, 0, st>>>(pv, cnt, depth == 0, qin, P.qb.p);
+            ev_end(e);
             e = ev_begin(K_SHADE, depth);
-            if (bin)
-                shade<<<g_shade, 128, 0, st>>>(ds_->view, f, pv, cnt, cnt_next, 0, P.qb.p, qout);
-            else
-                shade<<<g_shade, 128, 0, st>>>(ds_->view, f, pv, cnt, cnt_next, depth == 0, qin, qout);
+            shade<<<g_shade, 128, 0, st>>>(ds_->view, f, pv, cnt, cnt_next, 0, P.qb.p, qout);
             ev_end(e);
             e = ev_begin(K_SHADOW, depth);
             k_shadow<<<g_shadow, 128, 0, st>>>(ds_->view, pv, cnt, f.records);
@@ -3002,7 +2996,7 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
             for (int d = 0; d < p.max_depth; ++d) {
                 kind_units[d == 0 ? K_TRACE0 : K_TRACE] += hcnt[kCountersPerDepth * d];
                 kind_units[K_SHADE] += hcnt[kCountersPerDepth * d];
-                if (bin) kind_units[K_BIN] += hcnt[kCountersPerDepth * d];
+                kind_units[K_BIN] += hcnt[kCountersPerDepth * d];
                 if (guide) kind_units[K_GUIDE] += hcnt[kCountersPerDepth * d];
                 kind_units[K_SHADOW] += hcnt[kCountersPerDepth * d + 1];
             }
