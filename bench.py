@@ -421,8 +421,12 @@ def diagnostics(device: int) -> dict:
         wall = time.perf_counter() - t0
         st = c.diag_stats()
         parts = {k: round(v["total_ms"], 2) for k, v in c.stats()["kernels"].items()}
+        kinds = c.stats()["kernels"]
+        copy = kinds.get("diag_record_copy", {})
+        rb = copy.get("algo_bytes", 0.0) / copy["units"] if copy.get("units") else None
         out[name] = {"paths": tw * th * spp, "records": int(st[4]) if len(st) > 4 else None,
-                     "record_bytes": 512, "film_groups": int(st[2]), "wall_ms": round(1000 * wall, 2),
+                     "record_bytes": None if rb is None else round(rb, 1), "film_groups": int(st[2]),
+                     "wall_ms": round(1000 * wall, 2),
                      "plain_wall_ms": round(1000 * plain, 2), "parts_ms": parts}
     c.diag_disable()
     c.close()

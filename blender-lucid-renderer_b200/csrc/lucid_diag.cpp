@@ -140,7 +140,7 @@ void DiagFilm::clear() {
     recorded_ = 0;
 }
 
-void DiagFilm::replay(const DiagRecord* recs, size_t n, int tile_w) {
+void DiagFilm::replay(const uint8_t* units, const uint32_t* index, size_t n, int tile_w) {
     // the reference's single-threaded loop order: 8x8 micro-tiles row-major,
     // pixels row-major inside one, samples, records along the path.  Cells
     // are independent, so the records are bucketed by cell, each cell's
@@ -150,12 +150,15 @@ void DiagFilm::replay(const DiagRecord* recs, size_t n, int tile_w) {
     if (n == 0 || px_.empty()) return;
     const int nmx = (tile_w + 7) / 8;
     const size_t ncell = px_.size();
-    auto key = [&](const DiagRecord& r) {
+    auto head = [&](size_t i) {
+        return reinterpret_cast<const DiagRecHead*>(units + (size_t)index[i] * kDiagUnitBytes);
+    };
+    auto key = [&](const DiagRecHead& r) {
         int x = (int)(r.pixel % (uint32_t)tile_w), y = (int)(r.pixel / (uint32_t)tile_w);
         uint64_t order = (uint64_t)((y / 8) * nmx + x / 8) * 64u + (uint64_t)((y % 8) * 8 + (x % 8));
         return (order << 40) | ((uint64_t)r.sample << 16) | (uint64_t)r.seq;
     };
-    auto cell_of = [&](const DiagRecord& r) -> uint32_t {
+    auto cell_of = [&](const DiagRecHead& r) -> uint32_t {
         int x = (int)(r.pixel % (uint32_t)tile_w), y = (int)(r.pixel / (uint32_t)tile_w);
         int sx = x / sf_, sy = y / sf_;
         return (sx >= sw_ || sy >= sh_) ? (uint32_t)ncell : (uint32_t)((size_t)sy * sw_ + sx);
@@ -175,7 +178,7 @@ void DiagFilm::replay(const DiagRecord* recs, size_t n, int tile_w) {
     std::vector<uint32_t> cell(n);
     parallel([&](unsigned, size_t i0, size_t i1) {
         for (size_t i = i0; i < i1; ++i) {
-            cell[i] = cell_of(recs[i]);
+            cell[i] = cell_of(*head(i));
             count[cell[i]].fetch_add(1, std::memory_order_relaxed);
         }
     });
@@ -185,7 +188,7 @@ void DiagFilm::replay(const DiagRecord* recs, size_t n, int tile_w) {
     std::vector<std::pair<uint64_t, uint32_t>> order(n);
     parallel([&](unsigned, size_t i0, size_t i1) {
         for (size_t i = i0; i < i1; ++i)
-            order[count[cell[i]].fetch_add(1, std::memory_order_relaxed)] = {key(recs[i]), (uint32_t)i};
+            order[count[cell[i]].fetch_add(1, std::memory_order_relaxed)] = {key(*head(i)), (uint32_t)i};
     });
     const size_t in_film = start[ncell];
     recorded_ += in_film;
@@ -197,8 +200,9 @@ void DiagFilm::replay(const DiagRecord* recs, size_t n, int tile_w) {
             if (b == e) continue;
             dirty_[c] = 1;
             if (e - b > 1) std::sort(b, e);
+            DiagRecord r;
             for (auto it = b; it != e; ++it) {
-                const DiagRecord& r = recs[it->second];
+                diag_expand(head(it->second), r);
                 px_[c].record(r, hash(r), coarse_type(r));
             }
         }

@@ -39,6 +39,37 @@ struct DiagRecord {
 };
 static_assert(sizeof(DiagRecord) == 512, "DiagRecord layout");
 
+// The compact form the diagnostic kernel writes: a 32-B head and one 32-B
+// entry per vertex, in 16-B units, found through an index of unit offsets
+// (a Cornell path of a few bounces takes 100-200 B instead of 512).  The
+// replay expands each one into a DiagRecord.
+struct DiagRecHead {
+    uint32_t pixel, sample, seq;
+    uint8_t strategy, light_type, depth, pad;
+    float contrib[3];
+    uint32_t pad2;
+};
+struct DiagRecVertex {
+    int32_t object_id;
+    uint8_t bsdf, flags, pad0, pad1;
+    float pos[3];
+    float nrm[3];
+};
+static_assert(sizeof(DiagRecHead) == 32 && sizeof(DiagRecVertex) == 32, "compact record layout");
+constexpr size_t kDiagUnitBytes = 16;
+inline unsigned diag_record_units(int depth) { return 2u + 2u * (unsigned)depth; }
+inline void diag_expand(const DiagRecHead* h, DiagRecord& r) {
+    r.pixel = h->pixel; r.sample = h->sample; r.seq = h->seq;
+    r.strategy = h->strategy; r.light_type = h->light_type; r.depth = h->depth; r.pad = 0;
+    r.contrib[0] = h->contrib[0]; r.contrib[1] = h->contrib[1]; r.contrib[2] = h->contrib[2];
+    const DiagRecVertex* v = reinterpret_cast<const DiagRecVertex*>(h + 1);
+    const int d = h->depth < kDiagMaxDepth ? h->depth : kDiagMaxDepth;
+    for (int k = 0; k < d; ++k) {
+        r.object_id[k] = v[k].object_id; r.bsdf[k] = v[k].bsdf; r.flags[k] = v[k].flags;
+        for (int a = 0; a < 3; ++a) { r.pos[k][a] = v[k].pos[a]; r.nrm[k][a] = v[k].nrm[a]; }
+    }
+}
+
 struct DiagStats {   // PathStatistics (path_stats.hpp:63-100)
     uint32_t count = 0;
     float mean[3] = {0, 0, 0}, m2[3] = {0, 0, 0}, var[3] = {0, 0, 0};
@@ -81,8 +112,9 @@ public:
     void init(int tile_w, int tile_h, int subsample);
     void clear();
     void reset() { px_.clear(); dirty_.clear(); valid_ = false; w_ = h_ = sw_ = sh_ = 0; recorded_ = 0; }
-    // Sorts the records into the reference's loop order and replays them.
-    void replay(const DiagRecord* records, size_t n, int tile_w);
+    // Sorts the records (compact form: record i starts at unit index[i] of
+    // `units`) into the reference's loop order and replays them.
+    void replay(const uint8_t* units, const uint32_t* index, size_t n, int tile_w);
     // DiagnosticFilm::record_path (diagnostic_film.hpp:94-106): one path at
     // film pixel (x, y); out-of-range pixels are ignored.  material: the
     // vertices' material ids (the path hash includes them).

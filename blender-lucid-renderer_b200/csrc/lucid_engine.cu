@@ -12,6 +12,7 @@
 // Queues are compacted with warp ballots + one atomic per warp.  Work counts
 // stay on the device; the host enqueues a whole wave without synchronising.
 #include <cooperative_groups.h>
+#include <cooperative_groups/scan.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -176,26 +177,39 @@ struct GuideState {
     bool on = false;
 };
 
-// Completed-path records of the path diagnostics and their count.
+// Completed-path records of the path diagnostics (compact form: 16-B units
+// and an index of each record's first unit) and their counts.
 struct DiagDevice {
-    DBuf<DiagRecord> recs;
-    DBuf<unsigned long long> count;
+    DBuf<uint4> units;
+    DBuf<uint32_t> index;
+    DBuf<unsigned long long> count;   // [0] records, [1] units
     // pinned host copy of one band's records (kept between calls: page-locked
-    // copies run at full link speed and the buffer is not zero-filled)
-    DiagRecord* host = nullptr;
-    size_t host_cap = 0;
-    ~DiagDevice() { if (host) cudaFreeHost(host); }
-    cudaError_t reserve_host(size_t n, size_t keep) {
-        if (n <= host_cap) return cudaSuccess;
-        const size_t cap = n + n / 4;
-        DiagRecord* h = nullptr;
-        cudaError_t e = cudaHostAlloc(reinterpret_cast<void**>(&h), cap * sizeof(DiagRecord), cudaHostAllocDefault);
+    // copies run at full link speed and the buffers are not zero-filled)
+    uint8_t* host_units = nullptr;
+    uint32_t* host_index = nullptr;
+    size_t host_units_cap = 0, host_index_cap = 0;
+    ~DiagDevice() {
+        if (host_units) cudaFreeHost(host_units);
+        if (host_index) cudaFreeHost(host_index);
+    }
+    // grows a pinned buffer of `elem`-byte entries to hold n, keeping the first `keep`
+    template <typename T>
+    static cudaError_t grow(T*& buf, size_t& cap, size_t n, size_t keep, size_t elem) {
+        if (n <= cap) return cudaSuccess;
+        const size_t c = n + n / 4;
+        T* h = nullptr;
+        cudaError_t e = cudaHostAlloc(reinterpret_cast<void**>(&h), c * elem, cudaHostAllocDefault);
         if (e != cudaSuccess) return e;
-        if (host && keep) std::memcpy(h, host, keep * sizeof(DiagRecord));
-        if (host) cudaFreeHost(host);
-        host = h;
-        host_cap = cap;
+        if (buf && keep) std::memcpy(h, buf, keep * elem);
+        if (buf) cudaFreeHost(buf);
+        buf = h;
+        cap = c;
         return cudaSuccess;
+    }
+    cudaError_t reserve_host(size_t n_rec, size_t keep_rec, size_t n_units, size_t keep_units) {
+        cudaError_t e = grow(host_index, host_index_cap, n_rec, keep_rec, sizeof(uint32_t));
+        if (e != cudaSuccess) return e;
+        return grow(host_units, host_units_cap, n_units, keep_units, kDiagUnitBytes);
     }
 };
 
@@ -1220,9 +1234,11 @@ struct DiagPath {   // the recorder's current PathTrace
 };
 
 struct DiagOut {
-    DiagRecord* recs;
-    unsigned long long* count;
-    long long cap;
+    uint4* units;
+    uint32_t* index;
+    unsigned long long* count;   // [0] records, [1] units
+    long long cap, cap_units;
+    uint32_t unit_base;          // the band's units before this wave (index entries are band offsets)
 };
 
 LD void diag_vertex(DiagPath& P, int32_t obj, uint8_t type, bool delta, V3 p, V3 n) {
@@ -1234,39 +1250,43 @@ LD void diag_vertex(DiagPath& P, int32_t obj, uint8_t type, bool delta, V3 p, V3
 
 // record_completed_path_with_geometry (diagnostic_integrator.hpp:349-389):
 // the path plus a final Emission vertex (object -1 for the environment, else
-// -(light + 2)) when there is room.
-// A record slot per calling thread with one atomic per group of converged
-// lanes (the lanes that complete a path at the same point of the loop);
-// each thread's slots still increase in its own program order, which the
-// host's sort uses to keep records of one (pixel, sample, bounce) in order.
-LD unsigned long long warp_append(unsigned long long* count) {
-    cg::coalesced_group g = cg::coalesced_threads();
-    unsigned long long base = 0;
-    if (g.thread_rank() == 0) base = atomicAdd(count, (unsigned long long)g.size());
-    return g.shfl(base, 0) + g.thread_rank();
+// -(light + 2)) when there is room, in the compact form (lucid_diag.h).
+// A record slot and its units per calling thread with one atomic each per
+// group of converged lanes (the lanes that complete a path at the same point
+// of the loop; the units by an exclusive scan of the record sizes); each
+// thread's slots still increase in its own program order, which the host's
+// sort uses to keep records of one (pixel, sample, bounce) in order.
+LD void diag_vertex_store(uint4* u, int32_t obj, uint32_t bsdf, uint32_t flags, V3 p, V3 n) {
+    u[0] = make_uint4((uint32_t)obj, bsdf | (flags << 8), __float_as_uint(p.x), __float_as_uint(p.y));
+    u[1] = make_uint4(__float_as_uint(p.z), __float_as_uint(n.x), __float_as_uint(n.y), __float_as_uint(n.z));
 }
 
 LD void diag_complete(const DiagOut& o, const DiagPath& P, uint32_t pixel, uint32_t sample, uint32_t seq,
                       uint8_t strategy, int light_id, uint8_t ltype, RGB c, V3 lpos) {
-    unsigned long long slot = warp_append(o.count);
-    if ((long long)slot >= o.cap) return;   // the host grows the buffer and runs the wave again
-    DiagRecord* r = o.recs + slot;
-    int d = P.depth;
-    for (int k = 0; k < d; ++k) {
-        r->object_id[k] = P.obj[k]; r->bsdf[k] = P.bsdf[k]; r->flags[k] = P.flags[k];
-        r->pos[k][0] = P.pos[k].x; r->pos[k][1] = P.pos[k].y; r->pos[k][2] = P.pos[k].z;
-        r->nrm[k][0] = P.nrm[k].x; r->nrm[k][1] = P.nrm[k].y; r->nrm[k][2] = P.nrm[k].z;
+    const int d = P.depth;
+    const bool emission = d < kDiagMaxDepth;
+    const int dv = d + (emission ? 1 : 0);
+    const unsigned size = 2u + 2u * (unsigned)dv;
+    cg::coalesced_group g = cg::coalesced_threads();
+    const unsigned before = cg::exclusive_scan(g, size);
+    const unsigned total = g.shfl(before + size, g.size() - 1);
+    unsigned long long rb = 0, ub = 0;
+    if (g.thread_rank() == 0) {
+        rb = atomicAdd(&o.count[0], (unsigned long long)g.size());
+        ub = atomicAdd(&o.count[1], (unsigned long long)total);
     }
-    if (d < kDiagMaxDepth) {
-        r->object_id[d] = (ltype == DL_ENV) ? -1 : -(light_id + 2);
-        r->bsdf[d] = DB_EMISSION; r->flags[d] = 0;
-        r->pos[d][0] = lpos.x; r->pos[d][1] = lpos.y; r->pos[d][2] = lpos.z;
-        r->nrm[d][0] = 0.0f; r->nrm[d][1] = 0.0f; r->nrm[d][2] = 0.0f;
-        ++d;
-    }
-    r->pixel = pixel; r->sample = sample; r->seq = seq;
-    r->strategy = strategy; r->light_type = ltype; r->depth = (uint8_t)d; r->pad = 0;
-    r->contrib[0] = c.r; r->contrib[1] = c.g; r->contrib[2] = c.b;
+    const unsigned long long slot = g.shfl(rb, 0) + g.thread_rank();
+    const unsigned long long uoff = g.shfl(ub, 0) + before;
+    // past either capacity the host grows the buffers and runs the wave again
+    if ((long long)slot >= o.cap || (long long)(uoff + size) > o.cap_units) return;
+    o.index[slot] = o.unit_base + (uint32_t)uoff;
+    uint4* u = o.units + uoff;
+    u[0] = make_uint4(pixel, sample, seq, (uint32_t)strategy | ((uint32_t)ltype << 8) | ((uint32_t)dv << 16));
+    u[1] = make_uint4(__float_as_uint(c.r), __float_as_uint(c.g), __float_as_uint(c.b), 0u);
+    for (int k = 0; k < d; ++k) diag_vertex_store(u + 2 + 2 * k, P.obj[k], P.bsdf[k], P.flags[k], P.pos[k], P.nrm[k]);
+    if (emission)
+        diag_vertex_store(u + 2 + 2 * d, (ltype == DL_ENV) ? -1 : -(light_id + 2), DB_EMISSION, 0u, lpos,
+                          v3(0.0f, 0.0f, 0.0f));
 }
 
 __global__ void __launch_bounds__(128) k_diag_paths(DevScene sc, FrameParams f, PathView pv, DiagOut out,
@@ -1293,8 +1313,8 @@ __global__ void __launch_bounds__(128) k_diag_paths(DevScene sc, FrameParams f, 
         const uint32_t seq = (uint32_t)depth * 2u;
         HitRec h = scene_closest(sc, o, d, tmin, 1e30f, ok);
         float lt = 1e30f;
-        int li = (depth == 0) ? -1 : native_lights_closest(sc, o, d, 1e30f, lt);
-        if (li >= 0 && (h.prim < 0 || lt < h.t)) {
+        int li = (depth == 0) ? -1 : native_lights_closest(sc, o, d, h.prim >= 0 ? h.t : 1e30f, lt);
+        if (li >= 0) {   // in front of the surface hit (the bound above)
             if (!nee_only || depth == 0) {
                 const DevLight& L = sc.lights[sc.native_start + li];
                 uint8_t ltype = diag_light_type(__float_as_int(L.pos_type.w));
@@ -2577,8 +2597,9 @@ int Engine::render_diag_impl(const LucidRenderParams& p, float* out_host, float*
     if (!diag_dev_) diag_dev_ = new DiagDevice();
     DiagDevice& D = *diag_dev_;
     const long long want = diag_cfg_.record_capacity > 0 ? diag_cfg_.record_capacity : (1LL << 20);
-    if ((long long)D.recs.n < want) CK(D.recs.alloc((size_t)want));
-    if (!D.count.p) CK(D.count.alloc(1));
+    if ((long long)D.index.n < want) CK(D.index.alloc((size_t)want));
+    if ((long long)D.units.n < 8 * want) CK(D.units.alloc((size_t)(8 * want)));   // a few bounces per record
+    if (!D.count.p) CK(D.count.alloc(2));
     CK(cudaMemsetAsync(P.film.p, 0, np * sizeof(float4), st));
     CK(cudaMemsetAsync(P.errors.p, 0, 4 * sizeof(int), st));
 
@@ -2598,55 +2619,65 @@ int Engine::render_diag_impl(const LucidRenderParams& p, float* out_host, float*
     cudaEventRecord(t0, st);
     int status = LUCID_OK;
     int waves = 0;
-    double kernel_ms = 0.0, copy_ms = 0.0, replay_ms = 0.0, records_total = 0.0;
-    size_t band_n = 0;
+    double kernel_ms = 0.0, copy_ms = 0.0, replay_ms = 0.0, records_total = 0.0, record_bytes = 0.0;
+    size_t band_n = 0, band_units = 0;
     for (int y0 = 0; y0 < p.tile_h && status == LUCID_OK; y0 += band_rows) {
         const int bh = std::min(band_rows, p.tile_h - y0);
         f.tile_y = p.tile_y + y0;
         f.tile_h = bh;
         f.npix = bh * p.tile_w;
         band_n = 0;
+        band_units = 0;
         for (int s0 = 0; s0 < p.samples; s0 += spw) {
             if (is_cancelled()) { status = LUCID_ERR_CANCELLED; break; }
             const int this_spw = std::min(spw, p.samples - s0);
             f.s0 = s0;
             f.n_wave = this_spw * f.npix;
-            unsigned long long produced = 0;
+            unsigned long long produced[2] = {0, 0};
             for (;;) {
-                CK(cudaMemsetAsync(D.count.p, 0, sizeof(unsigned long long), st));
+                CK(cudaMemsetAsync(D.count.p, 0, 2 * sizeof(unsigned long long), st));
                 cudaEventRecord(ka, st);
                 k_raygen<<<(f.n_wave + 255) / 256, 256, 0, st>>>(f, P.view);
-                DiagOut o{D.recs.p, D.count.p, (long long)D.recs.n};
+                DiagOut o{D.units.p, D.index.p, D.count.p, (long long)D.index.n, (long long)D.units.n,
+                          (uint32_t)band_units};
                 k_diag_paths<<<(f.n_wave + 127) / 128, 128, 0, st>>>(ds_->view, f, P.view, o, y0 * p.tile_w);
                 cudaEventRecord(kb, st);
                 CK(cudaGetLastError());
-                CK(cudaMemcpyAsync(&produced, D.count.p, sizeof(produced), cudaMemcpyDeviceToHost, st));
+                CK(cudaMemcpyAsync(produced, D.count.p, sizeof(produced), cudaMemcpyDeviceToHost, st));
                 CK(cudaStreamSynchronize(st));
                 float kms = 0.0f;
                 cudaEventElapsedTime(&kms, ka, kb);
                 kernel_ms += kms;
-                if (produced <= (unsigned long long)D.recs.n) break;
-                // the wave is deterministic: grow the buffer and run it again
-                CK(D.recs.alloc((size_t)(produced + produced / 4)));
+                if (band_units + produced[1] >= (1ULL << 32))
+                    return fail(LUCID_ERR_OVERFLOW, "path diagnostics: a band's records exceed 64 GB");
+                if (produced[0] <= (unsigned long long)D.index.n && produced[1] <= (unsigned long long)D.units.n) break;
+                // the wave is deterministic: grow the buffers and run it again
+                if (produced[0] > (unsigned long long)D.index.n) CK(D.index.alloc((size_t)(produced[0] + produced[0] / 4)));
+                if (produced[1] > (unsigned long long)D.units.n) CK(D.units.alloc((size_t)(produced[1] + produced[1] / 4)));
             }
             k_film<<<(f.npix + 255) / 256, 256, 0, st>>>(f.npix, this_spw, P.rad.p, P.film.p + (size_t)y0 * p.tile_w);
-            CK(D.reserve_host(band_n + (size_t)produced, band_n));
+            CK(D.reserve_host(band_n + (size_t)produced[0], band_n, band_units + (size_t)produced[1], band_units));
             cudaEventRecord(ca, st);
-            if (produced)
-                CK(cudaMemcpyAsync(D.host + band_n, D.recs.p, (size_t)produced * sizeof(DiagRecord),
+            if (produced[0]) {
+                CK(cudaMemcpyAsync(D.host_index + band_n, D.index.p, (size_t)produced[0] * sizeof(uint32_t),
                                    cudaMemcpyDeviceToHost, st));
-            band_n += (size_t)produced;
+                CK(cudaMemcpyAsync(D.host_units + band_units * kDiagUnitBytes, D.units.p,
+                                   (size_t)produced[1] * kDiagUnitBytes, cudaMemcpyDeviceToHost, st));
+            }
+            band_n += (size_t)produced[0];
+            band_units += (size_t)produced[1];
+            record_bytes += (double)produced[0] * sizeof(uint32_t) + (double)produced[1] * kDiagUnitBytes;
             cudaEventRecord(cb, st);
             CK(cudaStreamSynchronize(st));
             float cms = 0.0f;
             cudaEventElapsedTime(&cms, ca, cb);
             copy_ms += cms;
-            records_total += (double)produced;
+            records_total += (double)produced[0];
             ++waves;
         }
         if (status == LUCID_OK) {
             const auto h0 = std::chrono::steady_clock::now();
-            diag_film_.replay(D.host, band_n, p.tile_w);
+            diag_film_.replay(D.host_units, D.host_index, band_n, p.tile_w);
             replay_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - h0).count();
         }
     }
@@ -2661,7 +2692,7 @@ int Engine::render_diag_impl(const LucidRenderParams& p, float* out_host, float*
         stats_.kinds[k].launches = waves;
         stats_.kinds[k].total_ms = ms3[k];
         stats_.kinds[k].units = k == 0 ? (double)np * p.samples : records_total;
-        stats_.kinds[k].algo_bytes = k == 1 ? records_total * sizeof(DiagRecord) : 0.0;
+        stats_.kinds[k].algo_bytes = k == 1 ? record_bytes : 0.0;
     }
     const int np_i = (int)np;
     k_output<<<(np_i + 255) / 256, 256, 0, st>>>(p.tile_w, p.tile_h, P.film.p, out_device ? (float4*)out_device : P.out.p);
