@@ -85,7 +85,7 @@ void DiagPixel::record(const DiagRecord& r, uint64_t h, uint8_t coarse_t) {
         }
     }
     for (size_t i = 0; i < num_groups; ++i)
-        if (groups[i].hash == h) { groups[i].stats.add(r.contrib); return; }
+        if (ghash[i] == h) { groups[i].stats.add(r.contrib); return; }
     auto init_from = [&](DiagGroup& g) {   // PathGroup::init_from (path_stats.hpp:161-178)
         g.hash = h;
         g.depth = (uint8_t)std::min<int>(r.depth, kDiagMaxDepth);
@@ -99,7 +99,11 @@ void DiagPixel::record(const DiagRecord& r, uint64_t h, uint8_t coarse_t) {
         g.stats = DiagStats();
         g.stats.add(r.contrib);
     };
-    if (num_groups < (size_t)kGroups) { init_from(groups[num_groups++]); return; }
+    if (num_groups < (size_t)kGroups) {
+        ghash[num_groups] = h;
+        init_from(groups[num_groups++]);
+        return;
+    }
     // evict_and_add (:203-220)
     size_t mi = 0;
     float mv = groups[0].stats.total_variance();
@@ -110,6 +114,7 @@ void DiagPixel::record(const DiagRecord& r, uint64_t h, uint8_t coarse_t) {
         if (adj < madj) { mi = i; mv = var; }
     }
     ++overflow;
+    ghash[mi] = h;
     init_from(groups[mi]);
 }
 
@@ -172,23 +177,30 @@ void DiagFilm::replay(const uint8_t* units, const uint32_t* index, size_t n, int
         for (auto& x : th) x.join();
     };
     // counting sort by cell (bucket order inside a cell does not matter: the
-    // per-cell sort below fixes it)
-    std::vector<std::atomic<uint32_t>> count(ncell + 1);
-    for (auto& c : count) c.store(0, std::memory_order_relaxed);
-    std::vector<uint32_t> cell(n);
+    // per-cell sort below fixes it); the scratch arrays are kept between
+    // calls, since first-touch page faults on fresh ones cost as much as the
+    // sort itself
+    if (scr_count_.size() < ncell + 1) scr_count_.resize(ncell + 1);
+    if (scr_start_.size() < ncell + 2) scr_start_.resize(ncell + 2);
+    if (scr_cell_.size() < n) scr_cell_.resize(n);
+    if (scr_order_.size() < n) scr_order_.resize(n);
+    uint32_t* count = scr_count_.data();
+    uint32_t* start = scr_start_.data();
+    uint32_t* cell = scr_cell_.data();
+    std::pair<uint64_t, uint32_t>* order = scr_order_.data();
+    std::memset(count, 0, (ncell + 1) * sizeof(uint32_t));
     parallel([&](unsigned, size_t i0, size_t i1) {
         for (size_t i = i0; i < i1; ++i) {
             cell[i] = cell_of(*head(i));
-            count[cell[i]].fetch_add(1, std::memory_order_relaxed);
+            __atomic_fetch_add(&count[cell[i]], 1u, __ATOMIC_RELAXED);
         }
     });
-    std::vector<uint32_t> start(ncell + 2, 0);
-    for (size_t c = 0; c <= ncell; ++c) start[c + 1] = start[c] + count[c].load(std::memory_order_relaxed);
-    for (size_t c = 0; c <= ncell; ++c) count[c].store(start[c], std::memory_order_relaxed);
-    std::vector<std::pair<uint64_t, uint32_t>> order(n);
+    start[0] = 0;
+    for (size_t c = 0; c <= ncell; ++c) start[c + 1] = start[c] + count[c];
+    for (size_t c = 0; c <= ncell; ++c) count[c] = start[c];
     parallel([&](unsigned, size_t i0, size_t i1) {
         for (size_t i = i0; i < i1; ++i)
-            order[count[cell[i]].fetch_add(1, std::memory_order_relaxed)] = {key(*head(i)), (uint32_t)i};
+            order[__atomic_fetch_add(&count[cell[i]], 1u, __ATOMIC_RELAXED)] = {key(*head(i)), (uint32_t)i};
     });
     const size_t in_film = start[ncell];
     recorded_ += in_film;
@@ -196,7 +208,7 @@ void DiagFilm::replay(const uint8_t* units, const uint32_t* index, size_t n, int
     if (dirty_.size() != ncell) dirty_.assign(ncell, 1);
     auto work = [&](size_t c0, size_t c1) {
         for (size_t c = c0; c < c1; ++c) {
-            auto b = order.begin() + start[c], e = order.begin() + start[c + 1];
+            auto b = order + start[c], e = order + start[c + 1];
             if (b == e) continue;
             dirty_[c] = 1;
             if (e - b > 1) std::sort(b, e);
@@ -217,7 +229,7 @@ void DiagFilm::replay(const uint8_t* units, const uint32_t* index, size_t n, int
     cut[0] = 0;
     for (unsigned t = 1; t < nt; ++t) {
         const uint32_t target = (uint32_t)(in_film * t / nt);
-        cut[t] = (size_t)(std::upper_bound(start.begin(), start.begin() + ncell + 1, target) - start.begin()) - 1;
+        cut[t] = (size_t)(std::upper_bound(start, start + ncell + 1, target) - start) - 1;
         cut[t] = std::max(cut[t], cut[t - 1]);
     }
     std::vector<std::thread> th;
@@ -290,6 +302,7 @@ int DiagFilm::export_pixel(int x, int y, bool sort_by_mean, LucidDiagPixel* info
         std::sort(p->groups, p->groups + p->num_groups, [](const DiagGroup& a, const DiagGroup& b) {
             return a.stats.total_variance() > b.stats.total_variance();
         });
+    for (size_t i = 0; i < p->num_groups; ++i) p->ghash[i] = p->groups[i].hash;   // keep the lookup array in step
     info->valid = 1;
     info->sample_count = (uint32_t)p->total;
     info->group_count = (uint32_t)p->num_groups;

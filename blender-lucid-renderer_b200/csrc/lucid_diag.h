@@ -15,6 +15,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/lucid_cuda.h"
@@ -91,6 +92,9 @@ struct DiagGroup {   // PathGroup (path_stats.hpp:142-232)
 
 struct DiagPixel {   // PixelPathData<16, 4>
     static constexpr int kGroups = 16, kOutliers = 4;
+    // the groups' hashes side by side (the lookup of every recorded path
+    // reads two cache lines instead of one per ~540-B group)
+    uint64_t ghash[kGroups] = {};
     DiagGroup groups[kGroups];
     DiagStats coarse[8];
     uint64_t outlier_hash[kOutliers] = {};
@@ -150,6 +154,10 @@ private:
     bool valid_ = false;
     size_t recorded_ = 0;
     std::vector<DiagPixel> px_;
+    // replay scratch (counts per cell, bucket starts, each record's cell, the
+    // (order key, record) pairs), kept between calls
+    std::vector<uint32_t> scr_count_, scr_start_, scr_cell_;
+    std::vector<std::pair<uint64_t, uint32_t>> scr_order_;
     std::vector<unsigned char> dirty_;   // cells that recorded a path since they were last reset
 };
 
