@@ -389,7 +389,8 @@ struct BinHist {
 // similar paths, so a warp claims 32 consecutive rays at a time and keeps
 // them together.  Also publishes the wave's path count as the depth-0 queue
 // length for the kernels after it.
-__global__ void __launch_bounds__(128) k_trace_primary(DevScene sc, FrameParams f, PathView pv, int* cnt,
+template <bool FMA>
+__global__ void __launch_bounds__(128) k_trace_primary_t(DevScene sc, FrameParams f, PathView pv, int* cnt,
                                                        int records, int bins) {
     __shared__ int hist[kBins];
     BinHist bh{hist};
@@ -404,7 +405,7 @@ __global__ void __launch_bounds__(128) k_trace_primary(DevScene sc, FrameParams 
         int id = base + (int)lane_id();
         if (id >= n) continue;
         const V3 d = camera_ray(f, pv, id);
-        HitRec h = closest_skip_boundaries(sc, o, d, 0.0f, ok);
+        HitRec h = closest_skip_boundaries<FMA>(sc, o, d, 0.0f, ok);
         if (h.prim < 0) { h.t = 1e30f; h.u = 0.0f; h.v = 0.0f; }
         pv.hit[id] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
         pv.lhit[id] = make_float2(__int_as_float(-1), 1e30f);   // native lights are invisible to camera rays
@@ -422,6 +423,15 @@ __global__ void __launch_bounds__(128) k_trace_primary(DevScene sc, FrameParams 
     }
     bh.flush(bins, cnt);
     if (!ok) atomicAdd(&pv.errors[0], 1);
+}
+
+// Camera rays take the FMA slab test when the camera lies within the
+// scene's coordinate bound (its error analysis then holds as for secondary
+// rays), else the subtraction form.
+using PrimaryKernel = void (*)(DevScene, FrameParams, PathView, int*, int, int);
+static PrimaryKernel k_trace_primary_for(const DevScene& sc, const float pos[3]) {
+    const float m = std::max(std::fabs(pos[0]), std::max(std::fabs(pos[1]), std::fabs(pos[2])));
+    return m <= sc.coord_bound ? k_trace_primary_t<true> : k_trace_primary_t<false>;
 }
 
 // Closest hit of extension rays (persistent, dynamic refill), including the
@@ -2237,6 +2247,7 @@ int Engine::build_bvh() {
         if (!H.prim_boundary[p] && !is_big[p]) real.push_back(p);
     int n = (int)real.size();
     DevScene& v = D.view;
+    v.coord_bound = maxabs;
     for (int a = 0; a < 3; ++a) {
         const float ext = hi[a] - lo[a];
         v.bin_lo[a] = ext > 0.0f ? lo[a] : 0.0f;
@@ -2891,7 +2902,7 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
     const LaunchSet ks = launch_set(algo_, guide, launch_profile_);
     const TraceKernel k_trace = ks.trace;
     const ShadowKernel k_shadow = ks.shadow;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t0, k_trace_primary, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t0, k_trace_primary_t<false>, 128, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t, k_trace, 128, 0);
     const ShadeKernel shade = ks.shade;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, shade, 128, 0);
@@ -2969,7 +2980,7 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
             pv.q0 = qin;
             if (depth == 0) {
                 e = ev_begin(K_TRACE0, depth);
-                k_trace_primary<<<g_trace0, 128, 0, st>>>(ds_->view, f, pv, cnt, f.records, bins);
+                k_trace_primary_for(ds_->view, f.pos)<<<g_trace0, 128, 0, st>>>(ds_->view, f, pv, cnt, f.records, bins);
             } else {
                 e = ev_begin(K_TRACE, depth);
                 k_trace<<<g_trace, 128, 0, st>>>(ds_->view, pv, cnt, 0, f.records, bins);
@@ -3196,7 +3207,7 @@ void Engine::enqueue_iteration(void* fp, int n) {
         int* qin = (depth & 1) ? P.q1.p : P.q0.p;
         int* qout = (depth & 1) ? P.q0.p : P.q1.p;
         pv.q0 = qin;
-        if (depth == 0) k_trace_primary<<<J.g_trace0, 128, 0, st>>>(ds_->view, f, pv, cnt, 0, bins);
+        if (depth == 0) k_trace_primary_for(ds_->view, f.pos)<<<J.g_trace0, 128, 0, st>>>(ds_->view, f, pv, cnt, 0, bins);
         else k_trace<<<J.g_trace, 128, 0, st>>>(ds_->view, pv, cnt, 0, 0, bins);
         k_bin_scatter<<<J.g_bin, 256, 0, st>>>(pv, cnt, depth == 0, qin, P.qb.p);
         shade<<<J.g_shade, 128, 0, st>>>(ds_->view, f, pv, cnt, cnt_next, 0, P.qb.p, qout);
@@ -3273,7 +3284,7 @@ void Engine::job_grids_locked() {
     JobState& J = *job_;
     const LaunchSet ks = launch_set(algo_, false, J.profile);
     int occ_t = 1, occ_s = 1, occ_h = 1, occ_t0 = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t0, k_trace_primary, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t0, k_trace_primary_t<false>, 128, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t, ks.trace, 128, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, ks.shade, 128, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, ks.shadow, 128, 0);
@@ -3656,7 +3667,7 @@ int Engine::render_noalloc(const LucidRenderParams& p, float* d_out) {
         int* g = g_noalloc_grid[device_][algo_];
         if (g[0] == 0) {
             int occ[4] = {1, 1, 1, 1};
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], k_trace_primary, 128, 0);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], k_trace_primary_t<false>, 128, 0);
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], k_trace_lb<9>, 128, 0);
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], shade, 128, 0);
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[3], k_shadow_lb<9>, 128, 0);
@@ -3710,7 +3721,7 @@ int Engine::render_noalloc(const LucidRenderParams& p, float* d_out) {
             int* qin = (depth & 1) ? q1 : q0;
             int* qout = (depth & 1) ? q0 : q1;
             pv.q0 = qin;
-            if (depth == 0) k_trace_primary<<<g_trace0, 128, 0, st>>>(ds_->view, f, pv, cnt, 0, -1);
+            if (depth == 0) k_trace_primary_for(ds_->view, f.pos)<<<g_trace0, 128, 0, st>>>(ds_->view, f, pv, cnt, 0, -1);
             else k_trace_lb<9><<<g_trace, 128, 0, st>>>(ds_->view, pv, cnt, 0, 0, -1);
             shade<<<g_shade, 128, 0, st>>>(ds_->view, f, pv, cnt, cnt_next, depth == 0, qin, qout);
             k_shadow_lb<9><<<g_shadow, 128, 0, st>>>(ds_->view, pv, cnt, 0);

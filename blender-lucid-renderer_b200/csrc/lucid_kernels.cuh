@@ -209,11 +209,15 @@ LD void node_hits(const Node4& q, V3 o, V3 ooi, V3 inv, float tmin, float tfar, 
 
 // Closest hit over the BVH (non-boundary triangles) in [tmin, h.t].
 // Returns false when the traversal stack overflowed (a hit may be missed).
+// FMA: the origin lies within the scene's coordinate bound (DevScene::
+// coord_bound), so the FMA slab form is conservative (box_hit_fma).
+template <bool FMA = false>
 LD bool bvh_closest(const DevScene& sc, V3 o, V3 d, float tmin, HitRec& h) {
     if (sc.num_big_tris) list_closest(sc.big_tris, sc.num_big_tris, o, d, tmin, h);
     if (sc.num_bvh_tris == 0) return true;
     if (sc.root2 < 0) { test_leaf_closest(sc.bvh_tris, sc.root2, o, d, tmin, h); return true; }
     V3 inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    const V3 ooi = v3(-o.x * inv.x, -o.y * inv.y, -o.z * inv.z);
     int stack[kStack];
     int sp = 0;
     int node = sc.root2;
@@ -223,8 +227,8 @@ LD bool bvh_closest(const DevScene& sc, V3 o, V3 d, float tmin, HitRec& h) {
         float4 a = __ldg(&n->lmin_lc), b = __ldg(&n->lmax_rc), c = __ldg(&n->rmin), e = __ldg(&n->rmax);
         int cl = __float_as_int(a.w), cr = __float_as_int(b.w);
         float tl, tr;
-        bool hl = box_hit(a, b, o, inv, tmin, h.t, tl);
-        bool hr = box_hit(c, e, o, inv, tmin, h.t, tr);
+        bool hl = FMA ? box_hit_fma(a, b, ooi, inv, tmin, h.t, tl) : box_hit(a, b, o, inv, tmin, h.t, tl);
+        bool hr = FMA ? box_hit_fma(c, e, ooi, inv, tmin, h.t, tr) : box_hit(c, e, o, inv, tmin, h.t, tr);
         if (hl && cl < 0) { test_leaf_closest(sc.bvh_tris, cl, o, d, tmin, h); hl = false; }
         if (hr && cr < 0) { test_leaf_closest(sc.bvh_tris, cr, o, d, tmin, h); hr = false; }
         if (hl && hr) {
@@ -469,10 +473,11 @@ LD HitRec scene_closest(const DevScene& sc, V3 o, V3 d, float tmin, float tmax, 
 // non-boundary hit after skipping at most 8 boundary hits, each skip moving
 // the search start 1 mm past the boundary.  The real-surface BVH query is
 // reused while its hit stays beyond the advanced search start.
+template <bool FMA = false>
 LD HitRec closest_skip_boundaries(const DevScene& sc, V3 o, V3 d, float tmin, bool& ok) {
     HitRec real;
     real.t = 1e30f; real.u = 0.0f; real.v = 0.0f; real.prim = -1;
-    ok &= bvh_closest(sc, o, d, tmin, real);
+    ok &= bvh_closest<FMA>(sc, o, d, tmin, real);
     if (!sc.num_bnd_tris) return real;
     const V3 inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
     float search = tmin;
@@ -481,7 +486,7 @@ LD HitRec closest_skip_boundaries(const DevScene& sc, V3 o, V3 d, float tmin, bo
     for (int peek = 0; peek < 8; ++peek) {
         if (real.prim >= 0 && real.t < search) {
             real = none;
-            ok &= bvh_closest(sc, o, d, search, real);
+            ok &= bvh_closest<FMA>(sc, o, d, search, real);
         }
         HitRec b;
         b.t = (real.prim >= 0) ? real.t : 1e30f; b.u = 0.0f; b.v = 0.0f;

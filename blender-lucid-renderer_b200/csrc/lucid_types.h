@@ -120,6 +120,9 @@ struct DevScene {
     int has_boundary;
     // scene box -> shading-bin cells (the spatial part of the shading sort)
     float bin_lo[3], bin_scale[3];
+    // the largest coordinate magnitude of the scene (the BVH boxes' padding
+    // is 2^-20 of it): rays starting within it may use the FMA slab test
+    float coord_bound;
 };
 
 }  // namespace lucid
