@@ -296,8 +296,12 @@ __global__ void k_raygen(FrameParams f, PathView pv) {
 }
 
 // ---------------------------------------------------------------- trace
-constexpr int kRounds = 4;         // closest hit: descend/test rounds per lane between refills
-constexpr int kShadowSteps = 24;   // any hit: node visits per lane between refills (6: 3x slower, 12: +1 %, 40: +5 %)
+// closest hit: descend/test rounds per lane between refills (five frames on
+// the 1M-triangle scene: 3 -> 321 ms, 4 -> 317 ms, 6 -> 362 ms)
+constexpr int kRounds = 4;
+// any hit: node visits per lane between refills (6: 3x slower; five frames:
+// 16 -> 229.7 ms, 24 -> 231.9 ms, 32 -> 240.4 ms)
+constexpr int kShadowSteps = 16;
 
 LD unsigned lanemask_lt() { return (1u << lane_id()) - 1u; }
 
@@ -2548,7 +2552,9 @@ static_assert(K_NUM <= LUCID_MAX_KERNEL_KINDS, "kernel kinds");
 // to a fifth of the free device memory (about 170 bytes per path).
 long long Engine::default_wave_paths(bool records) const {
     constexpr long long kMaxWave = 1LL << 28;
-    const long long per_path = 168 + (records ? 32 : 0);
+    // path state: 8 float4 arrays, the PCG state 16, the native-light hit 8,
+    // four int queues 16 and the shading bin 2 = 170 B (+ 32 B of records)
+    const long long per_path = 170 + (records ? 32 : 0);
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return 1LL << 22;
     long long fit = (long long)(free_b / 5) / per_path;
@@ -3183,7 +3189,7 @@ struct JobState {
 
 long long Engine::job_bytes(int w, int h, int chunk) {
     const long long np = (long long)w * h;
-    return (long long)chunk * np * (168 + 5) + np * 32 + (1 << 20);
+    return (long long)chunk * np * 176 + np * 32 + (1 << 20);   // path state (170 B) with slack
 }
 
 void Engine::enqueue_iteration(void* fp, int n) {

@@ -292,8 +292,10 @@ int lucid_cuda_render_f64(LucidCudaCtx* ctx, const LucidRenderParams* params, do
 /* ---- path diagnostics (DiagnosticFilm) ---------------------------------- */
 /* PathRecordingConfig (diagnostics/path_stats_config.hpp:24-105).  The film
  * uses subsample_factor; the others are carried for the caller, as in the
- * reference.  record_capacity bounds the device record buffer (completed
- * paths per render call; 0 = 1,048,576). */
+ * reference.  record_capacity is the initial size of the device record
+ * buffer in completed paths per wave (0 = 1,048,576, with eight 16-byte
+ * units per path for their vertices); a wave that produces more grows the
+ * buffers and runs again. */
 typedef struct LucidDiagConfig {
     int subsample_factor, max_groups_per_pixel, max_outliers_per_pixel, max_depth;
     float variance_threshold, outlier_threshold;

@@ -19,6 +19,16 @@ def scene_and_camera(name: str, workdir: str):
         return ls.all_lights_scene(workdir=workdir)
     if name == "all_lights_novol":
         return ls.all_lights_scene(workdir=workdir, with_volume=False)
+    if name == "two_volumes":
+        # a second volume box (a second group of boundary triangles, each
+        # group behind its own box test in the closest-hit kernels)
+        import os
+        sc, cam = ls.all_lights_scene(workdir=workdir)
+        sidecar = os.path.join(workdir, "second_volume_grid.f32")
+        ls.write_constant_grid(sidecar, (4, 4, 4), 1.0)
+        sc["meshes"].append(ls.volume_box_mesh((-2.2, 0.0, -2.0), (-1.0, 1.2, -0.8), 0.8, (0.6, 0.8, 0.9), -0.2,
+                                               sidecar, (4, 4, 4)))
+        return sc, cam
     if name == "mirror":
         return ls.mirror_point_light_scene()
     if name == "procedural_small":

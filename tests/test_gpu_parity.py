@@ -23,6 +23,7 @@ CASES = [
     ("all_lights_novol", "nee", 32, 24, 2, 8),
     ("all_lights", "volume_mis", 48, 36, 4, 8),
     ("all_lights", "volume_simple", 32, 24, 2, 8),
+    ("two_volumes", "volume_mis", 40, 30, 2, 8),   # two boundary meshes (two culling groups)
     ("mirror", "mis", 32, 32, 4, 6),
     ("procedural_small", "volume_mis", 40, 24, 2, 12),
     ("cornell", "mis", 37, 23, 3, 8),           # ragged frame: no multiple of the warp or block size
