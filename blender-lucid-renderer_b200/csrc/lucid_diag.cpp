@@ -145,7 +145,7 @@ void DiagFilm::clear() {
     recorded_ = 0;
 }
 
-void DiagFilm::replay(const uint8_t* units, const uint32_t* index, size_t n, int tile_w) {
+void DiagFilm::replay(const uint8_t* units, const uint32_t* index, size_t n, int tile_w, unsigned threads) {
     // the reference's single-threaded loop order: 8x8 micro-tiles row-major,
     // pixels row-major inside one, samples, records along the path.  Cells
     // are independent, so the records are bucketed by cell, each cell's
@@ -168,7 +168,7 @@ void DiagFilm::replay(const uint8_t* units, const uint32_t* index, size_t n, int
         int sx = x / sf_, sy = y / sf_;
         return (sx >= sw_ || sy >= sh_) ? (uint32_t)ncell : (uint32_t)((size_t)sy * sw_ + sx);
     };
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned hw = threads ? threads : std::max(1u, std::thread::hardware_concurrency());
     const unsigned nt = (unsigned)std::min<size_t>(hw, std::max<size_t>(1, n / 4096));
     auto parallel = [&](auto&& fn) {   // fn(t, i0, i1) over the records
         if (nt <= 1) { fn(0u, (size_t)0, n); return; }

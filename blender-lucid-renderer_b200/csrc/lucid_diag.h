@@ -118,7 +118,8 @@ public:
     void reset() { px_.clear(); dirty_.clear(); valid_ = false; w_ = h_ = sw_ = sh_ = 0; recorded_ = 0; }
     // Sorts the records (compact form: record i starts at unit index[i] of
     // `units`) into the reference's loop order and replays them.
-    void replay(const uint8_t* units, const uint32_t* index, size_t n, int tile_w);
+    // threads: host threads to use (0: all).
+    void replay(const uint8_t* units, const uint32_t* index, size_t n, int tile_w, unsigned threads = 0);
     // DiagnosticFilm::record_path (diagnostic_film.hpp:94-106): one path at
     // film pixel (x, y); out-of-range pixels are ignored.  material: the
     // vertices' material ids (the path hash includes them).

@@ -21,6 +21,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <chrono>
+#include <future>
 #include <cub/cub.cuh>
 #include <mutex>
 #include <thread>
@@ -183,14 +184,18 @@ struct DiagDevice {
     DBuf<uint4> units;
     DBuf<uint32_t> index;
     DBuf<unsigned long long> count;   // [0] records, [1] units
-    // pinned host copy of one band's records (kept between calls: page-locked
-    // copies run at full link speed and the buffers are not zero-filled)
-    uint8_t* host_units = nullptr;
-    uint32_t* host_index = nullptr;
-    size_t host_units_cap = 0, host_index_cap = 0;
+    // pinned host copies of a band's records, two of them: the host replays
+    // one band while the device renders the next into the other (kept
+    // between calls: page-locked copies run at full link speed and the
+    // buffers are not zero-filled)
+    uint8_t* host_units[2] = {nullptr, nullptr};
+    uint32_t* host_index[2] = {nullptr, nullptr};
+    size_t host_units_cap[2] = {0, 0}, host_index_cap[2] = {0, 0};
     ~DiagDevice() {
-        if (host_units) cudaFreeHost(host_units);
-        if (host_index) cudaFreeHost(host_index);
+        for (int b = 0; b < 2; ++b) {
+            if (host_units[b]) cudaFreeHost(host_units[b]);
+            if (host_index[b]) cudaFreeHost(host_index[b]);
+        }
     }
     // grows a pinned buffer of `elem`-byte entries to hold n, keeping the first `keep`
     template <typename T>
@@ -206,10 +211,10 @@ struct DiagDevice {
         cap = c;
         return cudaSuccess;
     }
-    cudaError_t reserve_host(size_t n_rec, size_t keep_rec, size_t n_units, size_t keep_units) {
-        cudaError_t e = grow(host_index, host_index_cap, n_rec, keep_rec, sizeof(uint32_t));
+    cudaError_t reserve_host(int b, size_t n_rec, size_t keep_rec, size_t n_units, size_t keep_units) {
+        cudaError_t e = grow(host_index[b], host_index_cap[b], n_rec, keep_rec, sizeof(uint32_t));
         if (e != cudaSuccess) return e;
-        return grow(host_units, host_units_cap, n_units, keep_units, kDiagUnitBytes);
+        return grow(host_units[b], host_units_cap[b], n_units, keep_units, kDiagUnitBytes);
     }
 };
 
@@ -2646,6 +2651,12 @@ int Engine::render_diag_impl(const LucidRenderParams& p, float* out_host, float*
     int waves = 0;
     double kernel_ms = 0.0, copy_ms = 0.0, replay_ms = 0.0, records_total = 0.0, record_bytes = 0.0;
     size_t band_n = 0, band_units = 0;
+    // the host replays band k (in band order) while the device renders band
+    // k + 1 into the other pinned buffer; the film is touched by the replay
+    // alone.  A pending replay is waited for before the next starts, and on
+    // every return (the future's destructor).
+    int hb = 0;
+    std::future<double> replay;
     for (int y0 = 0; y0 < p.tile_h && status == LUCID_OK; y0 += band_rows) {
         const int bh = std::min(band_rows, p.tile_h - y0);
         f.tile_y = p.tile_y + y0;
@@ -2681,12 +2692,12 @@ int Engine::render_diag_impl(const LucidRenderParams& p, float* out_host, float*
                 if (produced[1] > (unsigned long long)D.units.n) CK(D.units.alloc((size_t)(produced[1] + produced[1] / 4)));
             }
             k_film<<<(f.npix + 255) / 256, 256, 0, st>>>(f.npix, this_spw, P.rad.p, P.film.p + (size_t)y0 * p.tile_w);
-            CK(D.reserve_host(band_n + (size_t)produced[0], band_n, band_units + (size_t)produced[1], band_units));
+            CK(D.reserve_host(hb, band_n + (size_t)produced[0], band_n, band_units + (size_t)produced[1], band_units));
             cudaEventRecord(ca, st);
             if (produced[0]) {
-                CK(cudaMemcpyAsync(D.host_index + band_n, D.index.p, (size_t)produced[0] * sizeof(uint32_t),
+                CK(cudaMemcpyAsync(D.host_index[hb] + band_n, D.index.p, (size_t)produced[0] * sizeof(uint32_t),
                                    cudaMemcpyDeviceToHost, st));
-                CK(cudaMemcpyAsync(D.host_units + band_units * kDiagUnitBytes, D.units.p,
+                CK(cudaMemcpyAsync(D.host_units[hb] + band_units * kDiagUnitBytes, D.units.p,
                                    (size_t)produced[1] * kDiagUnitBytes, cudaMemcpyDeviceToHost, st));
             }
             band_n += (size_t)produced[0];
@@ -2701,11 +2712,27 @@ int Engine::render_diag_impl(const LucidRenderParams& p, float* out_host, float*
             ++waves;
         }
         if (status == LUCID_OK) {
-            const auto h0 = std::chrono::steady_clock::now();
-            diag_film_.replay(D.host_units, D.host_index, band_n, p.tile_w);
-            replay_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - h0).count();
+            if (replay.valid()) replay_ms += replay.get();
+            const uint8_t* units = D.host_units[hb];
+            const uint32_t* index = D.host_index[hb];
+            const size_t n_rec = band_n;
+            const int tw = p.tile_w;
+            const bool last = y0 + band_rows >= p.tile_h;
+            // while the device renders the next band, this thread waits on it:
+            // the replay leaves it a core
+            const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+            const unsigned nt = last ? hw : std::max(1u, hw - 1);
+            auto run = [this, units, index, n_rec, tw, nt]() {
+                const auto h0 = std::chrono::steady_clock::now();
+                diag_film_.replay(units, index, n_rec, tw, nt);
+                return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - h0).count();
+            };
+            if (last) replay_ms += run();   // the last band: nothing left to overlap
+            else replay = std::async(std::launch::async, run);
+            hb ^= 1;
         }
     }
+    if (replay.valid()) replay_ms += replay.get();
     for (cudaEvent_t e : {ka, kb, ca, cb}) cudaEventDestroy(e);
     // where a diagnostic render's time goes: the path kernel (raygen
     // included), the record copies to the host, and the host replay
