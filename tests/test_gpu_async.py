@@ -76,3 +76,29 @@ def test_pybind_async_surface():
     assert r.render_snapshot_revision_async() >= 3
     r.render_stop_async()
     assert not r.is_render_async_running()
+
+
+def test_async_snapshot_equals_the_oracle():
+    """The accumulator checked against the CPU oracle directly: a snapshot
+    after n samples equals the oracle's one-sample renders at sample offsets
+    0..n-1, summed in order and divided by n."""
+    import lucid_capi
+    import lucid_scenes as ls
+    from parity_util import render_oracle
+    sc, cam = ls.cornell_box()
+    ctx = lucid_capi.Context(0)
+    ctx.load_scene_json(ls.to_json(sc))
+    ctx.set_camera(*cam)
+    ctx.set_algorithm("mis")
+    ctx.async_start(W, H, DEPTH)
+    assert _wait(lambda: ctx.async_poll()[0] >= 8)
+    ctx.async_stop()
+    n, img = ctx.async_poll()
+    ctx.close()
+    acc = np.zeros((H, W, 4), np.float32)
+    for k in range(n):
+        one, _ = render_oracle(sc, cam, "mis", W, H, 1, DEPTH, offset=k)
+        acc = acc + one.astype(np.float32)
+    want = acc / np.float32(n)
+    want[..., 3] = 1.0
+    np.testing.assert_allclose(img, want, rtol=1e-6, atol=1e-7)

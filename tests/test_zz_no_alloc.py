@@ -74,6 +74,22 @@ def test_noalloc_matches_render_device_other_integrators(torch_mod, tmp_path_fac
         ctx.close()
 
 
+def test_noalloc_matches_the_oracle(torch_mod):
+    """The no-allocation render checked against the CPU oracle directly
+    (Cornell, mis, two waves' worth of samples at 96x80)."""
+    import lucid_scenes as ls
+    from parity_util import render_oracle
+    sc, cam = ls.cornell_box()
+    w, h, spp = 96, 80, 12
+    ctx = _ctx("cornell", "mis")
+    out = torch_mod.full((h, w, 4), -1.0, dtype=torch_mod.float32, device="cuda")
+    ctx.render_noalloc(out.data_ptr(), w, h, spp, 0, DEPTH)
+    torch_mod.cuda.synchronize()
+    ctx.close()
+    want, _ = render_oracle(sc, cam, "mis", w, h, spp, DEPTH)
+    np.testing.assert_allclose(out.cpu().numpy(), want, rtol=1e-6, atol=1e-7)
+
+
 def test_noalloc_rejects_requests_beyond_its_scratch(torch_mod):
     import lucid_capi
     torch = torch_mod
