@@ -415,12 +415,23 @@ __global__ void __launch_bounds__(128) k_trace_primary_t(DevScene sc, FrameParam
     const int n = f.n_wave;
     if (blockIdx.x == 0 && threadIdx.x == 0) cnt[0] = n;
     const V3 o = v3(f.pos[0], f.pos[1], f.pos[2]);
+    // a warp traces the 8 x 4 pixels of one screen tile (one sample each):
+    // a compact footprint keeps its lanes on the same BVH nodes longer than
+    // a 32-pixel row.  Slots run over the tiles of the first sample, then of
+    // the next; lanes past the tile's edge idle.
+    const int tiles_x = (f.tile_w + 7) / 8, tiles_y = (f.tile_h + 3) / 4;
+    const long long per_sample = (long long)tiles_x * tiles_y * 32;
+    const long long slots = per_sample * (long long)(n / max(f.npix, 1));
+    const int lane = (int)lane_id();
     bool ok = true;
     for (;;) {
-        int base = warp_fetch(&cnt[2]);
-        if (base >= n) break;
-        int id = base + (int)lane_id();
-        if (id >= n) continue;
+        const int base = warp_fetch(&cnt[2]);
+        if (base >= slots) break;
+        const long long slot = (long long)base + lane;
+        const int sl = (int)(slot / per_sample), tile = (int)((slot % per_sample) >> 5);
+        const int px = (tile % tiles_x) * 8 + (lane & 7), py = (tile / tiles_x) * 4 + (lane >> 3);
+        if (slot >= slots || px >= f.tile_w || py >= f.tile_h) continue;
+        const int id = sl * f.npix + py * f.tile_w + px;
         const V3 d = camera_ray(f, pv, id);
         HitRec h = closest_skip_boundaries<FMA>(sc, o, d, 0.0f, ok);
         if (h.prim < 0) { h.t = 1e30f; h.u = 0.0f; h.v = 0.0f; }
