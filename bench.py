@@ -439,7 +439,9 @@ def batch_mix(device: int, seed: int = 11, slots: int = 4) -> dict:
     (log-uniform), at log-uniform 128-1024 px with aspect 1:1, 4:3 or 16:9
     and 1, 4, 16 or 64 spp, plus 8 material previews (256x256, 32 spp),
     submitted at once to the request loop (scenes uploaded as arrays):
-    aggregate samples/s on `slots` slots against the same jobs one after
+    aggregate samples/s on `slots` slots with the jobs batched (one set of
+    wavefront launches over a device job table per batch), against the same
+    slots with every job in its own launches and against the jobs one after
     another on one slot."""
     import lucid_capi
     import lucid_scenes as ls
@@ -460,8 +462,9 @@ def batch_mix(device: int, seed: int = 11, slots: int = 4) -> dict:
         scenes.append((ls.scene_arrays(sc, json_rounding=False), cam, ls.scene_triangle_count(sc)))
     total = sum(w * h * spp for (*_, w, h, spp) in jobs)
 
-    def run(n_slots):
+    def run(n_slots, batching):
         srv = lucid_capi.Server(device, slots=n_slots)
+        srv.set_batching(batching)
         tu = time.perf_counter()
         ids = [srv.add_scene_arrays(a) for (a, _, _) in scenes]
         upload = time.perf_counter() - tu
@@ -474,17 +477,23 @@ def batch_mix(device: int, seed: int = 11, slots: int = 4) -> dict:
         srv.close()
         return wall, upload, st
 
-    run(1)   # first use of every kernel and allocation
-    wall_mix, upload, st = run(slots)
+    batch_paths = 1 << 26
+    run(slots, batch_paths)   # first use of every kernel and allocation
+    wall_batched, upload, st = run(slots, batch_paths)
+    wall_mix = run(slots, 0)[0]
     # the one-slot figure varies from run to run (host threads, allocations):
     # the better of two runs
-    wall_seq = min(run(1)[0], run(1)[0])
+    wall_seq = min(run(1, 0)[0], run(1, 0)[0])
     return {"jobs": len(jobs), "scenes": len(scenes), "triangles": int(sum(s[2] for s in scenes)),
             "samples": total, "slots": slots, "upload_s": round(upload, 3),
-            "samples_per_s": total / wall_mix, "samples_per_s_sequential": total / wall_seq,
+            "samples_per_s": total / wall_batched, "batches": st["batches"], "batched_jobs": st["batched_jobs"],
+            "batch_paths": batch_paths,
+            "samples_per_s_per_job_launches": total / wall_mix, "samples_per_s_sequential": total / wall_seq,
             "latency_p50_ms": st["latency_p50_ms"], "latency_p99_ms": st["latency_p99_ms"],
-            "launch": "per-slot streams over shared scenes; each job its own wavefront launches (no single "
-                      "launch across jobs)"}
+            "launch": "throughput jobs batched up to 2^26 paths: one set of wavefront launches over a device "
+                      "job table per batch (each path carries its scene index), batches on per-slot streams; "
+                      "per_job_launches: the same slots with batching off (each job its own launches); "
+                      "sequential: one slot, batching off"}
 
 
 def guiding(device: int, budget_ms: float = 1000.0, width: int = 1280, height: int = 720) -> dict:

@@ -4,6 +4,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "../../include/lucid_cuda.h"
 #include "lucid_engine.h"
@@ -152,6 +153,34 @@ int lucid_cuda_render_device(LucidCudaCtx* ctx, const LucidRenderParams* params,
 int lucid_cuda_render_noalloc(LucidCudaCtx* ctx, const LucidRenderParams* params, float* d_out_rgba) {
     if (!params || !d_out_rgba) return LUCID_ERR_INVALID;
     return guarded(ctx, [&](lucid::Engine& e) { return e.render_noalloc(*params, d_out_rgba); });
+}
+
+int lucid_cuda_render_batch(LucidCudaCtx* ctx, const LucidBatchJob* jobs, int n, const char* algorithm) {
+    if (!jobs || n <= 0) return LUCID_ERR_INVALID;
+    return guarded(ctx, [&](lucid::Engine& e) {
+        // each distinct scene context's current version, held for the call
+        std::vector<LucidCudaCtx*> owners;
+        std::vector<lucid::SceneSnapshot> snaps;
+        std::vector<lucid::Engine::BatchItem> items((size_t)n);
+        for (int j = 0; j < n; ++j) {
+            LucidCudaCtx* sc = jobs[j].scene;
+            if (!sc || !sc->engine) return e.fail(LUCID_ERR_INVALID, "batch: job " + std::to_string(j) + " has no scene context");
+            size_t k = 0;
+            while (k < owners.size() && owners[k] != sc) ++k;
+            if (k == owners.size()) {
+                snaps.emplace_back();
+                if (sc->engine->snapshot_scene(snaps.back()) != LUCID_OK)
+                    return e.fail(LUCID_ERR_NO_SCENE, "batch: job " + std::to_string(j) + ": " + sc->engine->last_error());
+                owners.push_back(sc);
+            }
+            lucid::Engine::BatchItem& it = items[(size_t)j];
+            it.scene = snaps[k].ds.get();
+            std::memcpy(it.camera, jobs[j].camera, sizeof(it.camera));
+            it.p = jobs[j].params;
+            it.out_host = jobs[j].out_rgba;
+        }
+        return e.render_batch(items.data(), n, algorithm, 0);
+    });
 }
 
 int lucid_cuda_render_debug(LucidCudaCtx* ctx, int tile_x, int tile_y, int tile_w, int tile_h, int full_w, int full_h,
@@ -317,6 +346,10 @@ int lucid_server_result(LucidServer* srv, int job_id, float* out_rgba, size_t ca
 
 int lucid_server_cancel(LucidServer* srv, int job_id) {
     return server_guarded(srv, [&](lucid::Server& s) { return s.cancel(job_id); });
+}
+
+int lucid_server_set_batching(LucidServer* srv, long long max_paths) {
+    return server_guarded(srv, [&](lucid::Server& s) { return s.set_batching(max_paths); });
 }
 
 int lucid_server_stats(LucidServer* srv, LucidServerStats* out) {

@@ -120,6 +120,10 @@ struct PathView {
     unsigned gkeep;    // a guided vertex is recorded when its hash < gkeep
     int gdepth;        // vertices at path depth < gdepth are guided
     float glo[3], gscale[3];   // scene box -> [0,1]^3
+    // batched jobs (null otherwise): the device table of the batch's scenes
+    // and each path's index into it, set with its camera ray
+    const DevScene* scenes;
+    unsigned short* sid;
 };
 // Shading bins: the event / material class (bin_class, 16 values) times
 // the cell of the hit point in a 4 x 4 x 4 grid over the scene box.
@@ -147,8 +151,12 @@ struct PathPool {
     size_t film_n = 0;
     DBuf<double> film64, out64;   // FP64 accumulation (converged references)
     size_t film64_n = 0;
+    DBuf<unsigned short> sid;     // batched jobs: scene index per path (render_batch)
+    DBuf<unsigned char> btab;     // batched jobs: the scene table, then a wave's job table
     PathView view{};
     void release() {
+        sid.release();
+        btab.release();
         rng.release(); ray_o.release(); ray_d.release(); thr.release(); rad.release(); hit.release();
         sh_o.release(); sh_d.release(); sh_c.release(); lhit.release(); q0.release(); q1.release(); qs.release();
         qb.release(); cls.release();
@@ -264,8 +272,13 @@ LD V3 primary_dir(const FrameParams& f, float nx, float ny) {
 // (x, y, offset + s), two jitter draws when the call has more than one
 // sample; writes the path's initial state and returns the direction (the
 // origin is the camera position, tMin 0).
-LD V3 camera_ray(const FrameParams& f, const PathView& pv, int id) {
-    int p = id % f.npix, sl = id / f.npix;
+LD V3 camera_ray_at(const FrameParams& f, const PathView& pv, int local, int id);
+LD V3 camera_ray(const FrameParams& f, const PathView& pv, int id) { return camera_ray_at(f, pv, id, id); }
+
+// The same for path `local` of the frame `f` stored at wave path `id`
+// (a batched job's paths start at its base in the wave).
+LD V3 camera_ray_at(const FrameParams& f, const PathView& pv, int local, int id) {
+    int p = local % f.npix, sl = local / f.npix;
     int gx = f.tile_x + p % f.tile_w, gy = f.tile_y + p / f.tile_w;
     float nx = (2.0f * ((float)gx + 0.5f) / (float)f.full_w - 1.0f) * f.aspect;
     float ny = 1.0f - 2.0f * ((float)gy + 0.5f) / (float)f.full_h;
@@ -462,13 +475,89 @@ static PrimaryKernel k_trace_primary_for(const DevScene& sc, const float pos[3])
     return m <= sc.coord_bound ? k_trace_primary_t<true> : k_trace_primary_t<false>;
 }
 
+// ---------------------------------------------------------------- batched jobs
+// One entry of the device job table of a batch wave: a piece of one job (a
+// range of its samples) with its camera and image (f: s0 = the piece's first
+// sample, n_wave = its paths), the scene it renders (index into the wave's
+// scene table), where its paths start in the wave, and where its camera-ray
+// slots start (each piece has whole warps of slots: 8 x 4 pixel tiles per
+// sample).
+struct BatchJob {
+    FrameParams f;
+    int sid;
+    int path_base;
+    int slot_base;
+    int pad;
+};
+constexpr int kMaxBatchPieces = 1024;
+
+// Camera rays of a batch wave, generated and traced in one pass over every
+// piece: a warp's 32 slots lie in one piece (found by binary search over the
+// slot bases, staged in shared memory), whose camera and sample range give
+// the rays and whose scene the rays are traced in.  Each path's scene index
+// is stored for the kernels after this one.  The subtraction form of the
+// slab test is used throughout (the FMA form's error bound needs the camera
+// inside its scene's coordinate bound, which varies from job to job); both
+// give the same hits.
+__global__ void __launch_bounds__(128) k_trace_primary_batch(PathView pv, const BatchJob* jobs, int njobs, int slots,
+                                                           int n, int* cnt, int bins) {
+    __shared__ int hist[kBins];
+    __shared__ int sbase[kMaxBatchPieces];
+    for (int i = threadIdx.x; i < njobs; i += blockDim.x) sbase[i] = jobs[i].slot_base;
+    BinHist bh{hist};
+    bh.clear(bins);   // ends with a block barrier, which also publishes sbase
+    if (blockIdx.x == 0 && threadIdx.x == 0) cnt[0] = n;
+    const int lane = (int)lane_id();
+    bool ok = true;
+    for (;;) {
+        const int base = warp_fetch(&cnt[2]);
+        if (base >= slots) break;
+        int lo = 0, hi = njobs - 1;   // the last piece whose slots start at or before base
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (sbase[mid] <= base) lo = mid; else hi = mid - 1;
+        }
+        const BatchJob& J = jobs[lo];
+        const FrameParams& f = J.f;
+        const int tw = f.tile_w, th = f.tile_h;
+        const int tiles_x = (tw + 7) / 8, tiles_y = (th + 3) / 4;
+        const int per_sample = tiles_x * tiles_y * 32;
+        const int slot = base - sbase[lo] + lane;
+        const int sl = slot / per_sample, tile = (slot % per_sample) >> 5;
+        const int px = (tile % tiles_x) * 8 + (lane & 7), py = (tile / tiles_x) * 4 + (lane >> 3);
+        if (px >= tw || py >= th) continue;
+        const int local = sl * f.npix + py * tw + px;
+        const int id = J.path_base + local;
+        const int sid = J.sid;
+        const DevScene& sc = pv.scenes[sid];
+        const V3 d = camera_ray_at(f, pv, local, id);
+        const V3 o = v3(f.pos[0], f.pos[1], f.pos[2]);
+        pv.sid[id] = (unsigned short)sid;
+        HitRec h = closest_skip_boundaries<false>(sc, o, d, 0.0f, ok);
+        if (h.prim < 0) { h.t = 1e30f; h.u = 0.0f; h.v = 0.0f; }
+        pv.hit[id] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
+        pv.lhit[id] = make_float2(__int_as_float(-1), 1e30f);   // native lights are invisible to camera rays
+        bh.add(sc, pv, id, bins, h.prim, h.t, -1, 1e30f, o, d);
+    }
+    bh.flush(bins, cnt);
+    if (!ok) atomicAdd(&pv.errors[0], 1);
+}
+
+// The scene of path `id`: the kernel's scene, or in a batch wave the entry
+// of the wave's scene table the path's camera ray chose.
+template <bool MULTI>
+LD const DevScene& path_scene(const DevScene& sc, const PathView& pv, int id) {
+    if constexpr (MULTI) return pv.scenes[pv.sid[id]];
+    else return sc;
+}
+
 // Closest hit of extension rays (persistent, dynamic refill), including the
 // skip-volume-boundary rule (path_tracer.hpp:82-95) and native lights.
 // Nine resident CTAs per SM (at most 56 registers): one more warp group to
 // hide node-fetch latency than the unconstrained 61 registers allow
 // (1M-triangle scene: 8 CTAs 232 ms, 9 CTAs 221 ms, 10 CTAs 225 ms).
-template <int MINB>
-__global__ void __launch_bounds__(128, MINB) k_trace_lb(DevScene sc, PathView pv, int* cnt, int identity, int records,
+template <int MINB, bool MULTI = false>
+__global__ void __launch_bounds__(128, MINB) k_trace_lb(DevScene sc0, PathView pv, int* cnt, int identity, int records,
                                                       int bins) {
     __shared__ int hist[kBins];
     BinHist bh{hist};
@@ -479,12 +568,20 @@ __global__ void __launch_bounds__(128, MINB) k_trace_lb(DevScene sc, PathView pv
     float stack_t[kStack];
     Trav s;
     bool active = false, exhausted = false, ok = true;
-    int id = 0, depth = 0, peek = 0;
+    int id = 0, depth = 0, peek = 0, sid = 0;
     float search = 0.0f;
+    // the lane's scene: the kernel's, or in a batch wave its ray's entry of
+    // the wave's scene table (kept in a register between refills)
+    auto scene = [&]() -> const DevScene& {
+        if constexpr (MULTI) return pv.scenes[sid];
+        else return sc0;
+    };
     for (;;) {
         int r = refill(&cnt[2], n, !active, exhausted);
         if (r >= 0) {
             id = q ? q[r] : r;
+            if constexpr (MULTI) sid = pv.sid[id];
+            const DevScene& sc = scene();
             float4 ro = pv.ray_o[id], rd = pv.ray_d[id];
             depth = __float_as_int(rd.w);
             trav_begin<false>(s, sc, f3(ro), f3(rd), ro.w, 1e30f);
@@ -494,6 +591,7 @@ __global__ void __launch_bounds__(128, MINB) k_trace_lb(DevScene sc, PathView pv
         }
         if (__ballot_sync(0xffffffffu, active) == 0) break;
         if (!active) continue;
+        const DevScene& sc = scene();
         if (!trav_run<false>(s, stack, stack_t, sc, ok, kRounds)) continue;
         HitRec res = s.h;
         if (sc.num_bnd_tris) {
@@ -919,7 +1017,7 @@ LD ShadeResult shade_path(const DevScene& sc, const FrameParams& f, const PathVi
 // hundred bytes of spills): the extra warps hide more of the shading
 // kernel's instruction-fetch and memory latency than the spills cost
 // (measured on the 1M-triangle scene: 4, 5, 6, 7, 8 CTAs per SM).
-template <int ALGO, bool GUIDE = false, int MINB = 8>
+template <int ALGO, bool GUIDE = false, int MINB = 8, bool MULTI = false>
 __global__ void __launch_bounds__(128, MINB) k_shade(DevScene sc, FrameParams f, PathView pv, int* cnt, int* cnt_next,
                                                   int identity, int* qin, int* qout) {
     const int n = *(volatile int*)&cnt[0];
@@ -933,7 +1031,7 @@ __global__ void __launch_bounds__(128, MINB) k_shade(DevScene sc, FrameParams f,
         r.shadow = false;
         if (i < n) {
             id = identity ? i : qin[i];
-            r = shade_path<ALGO, GUIDE>(sc, f, pv, id);
+            r = shade_path<ALGO, GUIDE>(path_scene<MULTI>(sc, pv, id), f, pv, id);
         }
         warp_append(qout, &cnt_next[0], id, r.cont);
         warp_append(pv.qs, &cnt[1], id, r.shadow);
@@ -953,6 +1051,16 @@ static ShadeKernel shade_kernel_lb(int algo, bool guide) {
     }
 }
 static ShadeKernel shade_kernel(int algo, bool guide = false) { return shade_kernel_lb<8>(algo, guide); }
+// Batch waves (unguided): each path shaded in its own job's scene.
+static ShadeKernel shade_kernel_batch(int algo) {
+    switch (algo) {
+        case ALGO_SIMPLE: return k_shade<ALGO_SIMPLE, false, 8, true>;
+        case ALGO_MIS: return k_shade<ALGO_MIS, false, 8, true>;
+        case ALGO_VOLUME_SIMPLE: return k_shade<ALGO_VOLUME_SIMPLE, false, 8, true>;
+        case ALGO_VOLUME_MIS: return k_shade<ALGO_VOLUME_MIS, false, 8, true>;
+        default: return k_shade<ALGO_NEE, false, 8, true>;
+    }
+}
 
 // ---------------------------------------------------------------- shading bins
 // The scatter half of the counting sort whose histogram the trace kernels
@@ -1082,20 +1190,27 @@ __global__ void __launch_bounds__(32 * kInferWarps, 1) k_guide_infer(DevScene sc
 // made this kernel 4 % slower (more registers at its 56-register cap),
 // while they save the closest-hit kernels 7 %.
 // Nine resident CTAs per SM as for k_trace (shadow time -0.7 %; 10: +4 %).
-template <int MINB>
-__global__ void __launch_bounds__(128, MINB) k_shadow_lb(DevScene sc, PathView pv, int* cnt, int records) {
+template <int MINB, bool MULTI = false>
+__global__ void __launch_bounds__(128, MINB) k_shadow_lb(DevScene sc0, PathView pv, int* cnt, int records) {
     const int n = *(volatile int*)&cnt[1];
     int stack[kStack];
     Trav s;
     bool active = false, exhausted = false, ok = true;
-    int id = 0, peek = 0;
+    int id = 0, peek = 0, sid = 0;
     float tmax = 0.0f, off = 0.0f, bt = -1.0f;
     V3 po = v3(0.f, 0.f, 0.f), d = v3(0.f, 0.f, 1.f);
+    // the lane's scene (a batch wave: its ray's entry of the scene table)
+    auto scene = [&]() -> const DevScene& {
+        if constexpr (MULTI) return pv.scenes[sid];
+        else return sc0;
+    };
     for (;;) {
         int r = refill(&cnt[4], n, !active, exhausted);
         int outcome = -1;   // -1 running, 0 unoccluded, 1 occluded
         if (r >= 0) {
             id = pv.qs[r];
+            if constexpr (MULTI) sid = pv.sid[id];
+            const DevScene& sc = scene();
             float4 so = pv.sh_o[id], sd = pv.sh_d[id];
             po = f3(so); d = f3(sd); tmax = so.w; off = 0.0f; peek = 0;
             active = true;
@@ -1116,6 +1231,7 @@ __global__ void __launch_bounds__(128, MINB) k_shadow_lb(DevScene sc, PathView p
         if (__ballot_sync(0xffffffffu, active) == 0) break;
         if (!active) continue;
         if (outcome < 0) {
+            const DevScene& sc = scene();
             if (!trav_run_any(s, stack, sc, ok, kShadowSteps)) continue;
             if (s.any_hit) outcome = 1;
             else if (bt < 0.0f) outcome = 0;
@@ -1175,6 +1291,11 @@ constexpr int kLaunchProfiles = 2;
 static LaunchSet launch_set(int algo, bool guide, int profile) {
     if (profile == 1) return {k_trace_lb<8>, shade_kernel_lb<6>(algo, guide), k_shadow_lb<8>};
     return {k_trace_lb<9>, shade_kernel_lb<8>(algo, guide), k_shadow_lb<9>};
+}
+// Batch waves: the same kernels reading each path's scene from the wave's
+// scene table (profile 0's resident CTAs).
+static LaunchSet launch_set_batch(int algo) {
+    return {k_trace_lb<9, true>, shade_kernel_batch(algo), k_shadow_lb<9, true>};
 }
 
 // ---------------------------------------------------------------- film
@@ -3144,6 +3265,230 @@ int Engine::render_impl(const LucidRenderParams& p, float* out_host, LucidSample
         }
         stats_.kinds[K_FILM].algo_bytes += (double)np * 32.0 * waves;
     }
+    if (herr[0] != 0) return fail(LUCID_ERR_OVERFLOW, "BVH traversal stack overflow");
+    if (status == LUCID_ERR_CANCELLED) return fail(LUCID_ERR_CANCELLED, "render cancelled");
+    return LUCID_OK;
+}
+
+// ---------------------------------------------------------------- batched jobs (host)
+static int algo_from_name(const char* name) {
+    std::string a = name ? name : "";
+    if (a == "simple") return ALGO_SIMPLE;
+    if (a == "mis") return ALGO_MIS;
+    if (a == "volume_simple") return ALGO_VOLUME_SIMPLE;
+    if (a == "volume_mis") return ALGO_VOLUME_MIS;
+    return ALGO_NEE;   // the reference's dispatch falls through to traceNEE
+}
+
+long long Engine::batch_bytes(long long pixels, long long wave_paths) {
+    // path state (170 B) and scene index (2 B) per path with slack, film and
+    // output per pixel, the job and scene tables
+    return wave_paths * 178 + pixels * 32 + (2 << 20);
+}
+
+// Jobs on different scenes (and cameras, image sizes, sample counts) in one
+// set of wavefront launches: the jobs' samples are cut into pieces that fill
+// waves of up to `wave_paths` paths in job order (a job larger than a wave
+// continues in the next one, in sample order); a wave's device job table
+// gives the camera-ray kernel each piece's camera, image, sample range,
+// scene and first path, and every later kernel reads a path's scene from the
+// wave's scene table.  Each job's film sums its samples in sample order, so
+// its image is the one lucid_cuda_render gives for the same call on its own
+// scene, bit for bit.
+int Engine::render_batch(const BatchItem* items, int n, const char* algorithm, long long wave_paths) {
+    GpuLock gl(*this);
+    reset_cancel();
+    if (n <= 0 || !items) return fail(LUCID_ERR_INVALID, "batch: no jobs");
+    const int algo = algo_from_name(algorithm);
+    const int depth = items[0].p.max_depth;
+    if (depth < 1 || depth > kMaxDepth) return fail(LUCID_ERR_INVALID, "batch: max_depth must be 1..1024");
+    std::vector<const DeviceScene*> scenes;
+    std::vector<int> job_sid((size_t)n);
+    std::vector<size_t> film_off((size_t)n + 1, 0);
+    long long total_paths = 0, max_np = 1;
+    for (int j = 0; j < n; ++j) {
+        const LucidRenderParams& p = items[j].p;
+        if (!items[j].scene || !items[j].out_host) return fail(LUCID_ERR_INVALID, "batch: a job has no scene or output");
+        if (p.tile_w <= 0 || p.tile_h <= 0 || p.full_w <= 0 || p.full_h <= 0)
+            return fail(LUCID_ERR_INVALID, "batch: tile and image sizes must be positive");
+        if (p.samples <= 0) return fail(LUCID_ERR_INVALID, "batch: samples must be >= 1");
+        if (p.max_depth != depth) return fail(LUCID_ERR_INVALID, "batch: every job needs the same max_depth");
+        const long long np = (long long)p.tile_w * p.tile_h;
+        if (np > (1LL << 28)) return fail(LUCID_ERR_INVALID, "batch: tile too large");
+        const DeviceScene* ds = static_cast<const DeviceScene*>(items[j].scene);
+        int k = 0;
+        while (k < (int)scenes.size() && scenes[k] != ds) ++k;
+        if (k == (int)scenes.size()) {
+            if (scenes.size() >= 65535) return fail(LUCID_ERR_INVALID, "batch: more than 65535 scenes");
+            scenes.push_back(ds);
+        }
+        job_sid[j] = k;
+        film_off[j + 1] = film_off[j] + (size_t)np;
+        total_paths += np * p.samples;
+        max_np = std::max(max_np, np);
+    }
+    CK(cudaSetDevice(device_));
+    int rc = ensure_stream();
+    if (rc != LUCID_OK) return rc;
+    cudaStream_t st = S(stream_);
+    long long cap = wave_paths > 0 ? wave_paths : wave_cap_;
+    if (cap <= 0) cap = pool_->cap >= total_paths ? pool_->cap : default_wave_paths(false);
+    cap = std::max(cap, max_np);                 // one sample of the largest tile per wave at least
+    cap = std::min(cap, std::max(total_paths, max_np));
+    if (cap >= (1LL << 31) - 64) return fail(LUCID_ERR_INVALID, "batch: wave too large");
+    rc = ensure_pool(cap, false);
+    if (rc != LUCID_OK) return rc;
+    PathPool& P = *pool_;
+    if (P.sid.n < (size_t)P.cap) CK(P.sid.alloc((size_t)P.cap));
+    const size_t npix_all = film_off[(size_t)n];
+    if (P.film_n < npix_all) {
+        CK(P.film.alloc(npix_all));
+        CK(P.out.alloc(npix_all));
+        P.film_n = npix_all;
+    }
+    CK(cudaMemsetAsync(P.film.p, 0, npix_all * sizeof(float4), st));
+    CK(cudaMemsetAsync(P.errors.p, 0, 4 * sizeof(int), st));
+
+    // the scene table, then room for the largest wave's job table
+    std::vector<DevScene> scene_tab(scenes.size());
+    for (size_t k = 0; k < scenes.size(); ++k) scene_tab[k] = scenes[k]->view;
+    const size_t tab_off = (scene_tab.size() * sizeof(DevScene) + 255) & ~(size_t)255;
+    const size_t tab_bytes = tab_off + (size_t)kMaxBatchPieces * sizeof(BatchJob);
+    if (P.btab.n < tab_bytes) CK(P.btab.alloc(tab_bytes));
+    CK(cudaMemcpyAsync(P.btab.p, scene_tab.data(), scene_tab.size() * sizeof(DevScene), cudaMemcpyHostToDevice, st));
+    const DevScene* d_scenes = reinterpret_cast<const DevScene*>(P.btab.p);
+    const BatchJob* d_jobs = reinterpret_cast<const BatchJob*>(P.btab.p + tab_off);
+
+    std::vector<HostCamera> cams((size_t)n);
+    for (int j = 0; j < n; ++j) {
+        const float* c = items[j].camera;
+        make_camera(cams[j], c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7], c[8], c[9]);
+    }
+    auto frame_of = [&](int j, int s0, int spw) {
+        const LucidRenderParams& p = items[j].p;
+        const HostCamera& cam = cams[j];
+        FrameParams f{};
+        for (int k = 0; k < 3; ++k) { f.pos[k] = cam.pos[k]; f.fwd[k] = cam.forward[k]; f.right[k] = cam.right[k]; f.up[k] = cam.up[k]; }
+        f.aspect = (float)p.full_w / (float)p.full_h;
+        f.scale = std::tan(cam.fov * 0.5f);
+        f.tile_x = p.tile_x; f.tile_y = p.tile_y; f.tile_w = p.tile_w; f.tile_h = p.tile_h;
+        f.full_w = p.full_w; f.full_h = p.full_h;
+        f.samples = p.samples; f.sample_offset = p.sample_offset; f.max_depth = depth; f.algo = algo;
+        f.npix = p.tile_w * p.tile_h;
+        f.s0 = s0;
+        f.n_wave = spw * f.npix;
+        return f;
+    };
+
+    const LaunchSet ks = launch_set_batch(algo);
+    int occ_t0 = 1, occ_t = 1, occ_s = 1, occ_h = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t0, k_trace_primary_batch, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t, ks.trace, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, ks.shade, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, ks.shadow, 128, 0);
+    const int g_trace0 = num_sms_ * std::max(1, occ_t0), g_trace = num_sms_ * std::max(1, occ_t),
+              g_shade = num_sms_ * std::max(1, occ_s), g_shadow = num_sms_ * std::max(1, occ_h);
+    const int g_bin = num_sms_ * 8;
+    FrameParams fshade{};
+    fshade.max_depth = depth;
+    fshade.algo = algo;
+
+    stats_ = LucidRenderStats{};
+    double seg = 0, shadows = 0;
+    std::vector<int> hcnt((size_t)kCountersPerDepth * (depth + 1));
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    cudaEventRecord(t0, st);
+    int waves = 0, status = LUCID_OK;
+    std::vector<BatchJob> tab;
+    struct PieceFilm { int job, spw, path_base; };
+    std::vector<PieceFilm> films;
+    int j = 0, s = 0;   // next sample s of job j still to render
+    while (j < n) {
+        if (is_cancelled()) { status = LUCID_ERR_CANCELLED; break; }
+        // fill one wave with pieces, in job order
+        tab.clear();
+        films.clear();
+        long long used = 0, slots = 0;
+        while (j < n && (int)tab.size() < kMaxBatchPieces) {
+            const LucidRenderParams& p = items[j].p;
+            const long long np = (long long)p.tile_w * p.tile_h;
+            const int take = (int)std::min<long long>(p.samples - s, (cap - used) / np);
+            if (take < 1) break;
+            const long long per_sample = (long long)((p.tile_w + 7) / 8) * ((p.tile_h + 3) / 4) * 32;
+            if (slots + per_sample * take >= (1LL << 31) - 64) break;
+            BatchJob b{};
+            b.f = frame_of(j, s, take);
+            b.sid = job_sid[j];
+            b.path_base = (int)used;
+            b.slot_base = (int)slots;
+            tab.push_back(b);
+            films.push_back({j, take, (int)used});
+            used += np * take;
+            slots += per_sample * take;
+            s += take;
+            if (s >= p.samples) { ++j; s = 0; }
+        }
+        if (tab.empty()) return fail(LUCID_ERR_INVALID, "batch: a job piece does not fit a wave");
+        CK(cudaMemcpyAsync(const_cast<BatchJob*>(d_jobs), tab.data(), tab.size() * sizeof(BatchJob),
+                           cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(P.counters.p, 0, sizeof(int) * kCountersPerDepth * (depth + 1), st));
+        const int n_wave = (int)used;
+        const int bins = ((algo == ALGO_VOLUME_MIS || algo == ALGO_VOLUME_SIMPLE) ? kBinVolume : 0) |
+                         (n_wave >= kCellBinPaths ? kBinCells : 0);
+        PathView pv = P.view;
+        pv.scenes = d_scenes;
+        pv.sid = P.sid.p;
+        for (int dd = 0; dd < depth; ++dd) {
+            int* cnt = P.counters.p + kCountersPerDepth * dd;
+            int* cnt_next = P.counters.p + kCountersPerDepth * (dd + 1);
+            int* qin = (dd & 1) ? P.q1.p : P.q0.p;
+            int* qout = (dd & 1) ? P.q0.p : P.q1.p;
+            pv.q0 = qin;
+            if (dd == 0)
+                k_trace_primary_batch<<<g_trace0, 128, 0, st>>>(pv, d_jobs, (int)tab.size(), (int)slots, n_wave, cnt, bins);
+            else
+                ks.trace<<<g_trace, 128, 0, st>>>(scene_tab[0], pv, cnt, 0, 0, bins);
+            k_bin_scatter<<<g_bin, 256, 0, st>>>(pv, cnt, dd == 0, qin, P.qb.p);
+            ks.shade<<<g_shade, 128, 0, st>>>(scene_tab[0], fshade, pv, cnt, cnt_next, 0, P.qb.p, qout);
+            ks.shadow<<<g_shadow, 128, 0, st>>>(scene_tab[0], pv, cnt, 0);
+        }
+        for (const PieceFilm& pf : films) {
+            const int np_j = (int)(film_off[(size_t)pf.job + 1] - film_off[(size_t)pf.job]);
+            k_film<<<(np_j + 255) / 256, 256, 0, st>>>(np_j, pf.spw, P.rad.p + pf.path_base, P.film.p + film_off[pf.job]);
+        }
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(hcnt.data(), P.counters.p, hcnt.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (int d = 0; d < depth; ++d) {
+            seg += hcnt[kCountersPerDepth * d];
+            shadows += hcnt[kCountersPerDepth * d + 1];
+        }
+        ++waves;
+    }
+    for (int k = 0; k < n && status == LUCID_OK; ++k) {
+        const LucidRenderParams& p = items[k].p;
+        const int np_k = p.tile_w * p.tile_h;
+        k_output<<<(np_k + 255) / 256, 256, 0, st>>>(p.tile_w, p.tile_h, P.film.p + film_off[k], P.out.p + film_off[k]);
+    }
+    cudaEventRecord(t1, st);
+    int herr[4] = {0, 0, 0, 0};
+    CK(cudaMemcpyAsync(herr, P.errors.p, sizeof(herr), cudaMemcpyDeviceToHost, st));
+    if (status == LUCID_OK)
+        for (int k = 0; k < n; ++k)
+            CK(cudaMemcpyAsync(items[k].out_host, P.out.p + film_off[k],
+                               (film_off[(size_t)k + 1] - film_off[k]) * sizeof(float4), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    float tot = 0.0f;
+    cudaEventElapsedTime(&tot, t0, t1);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    stats_.total_ms = tot;
+    stats_.paths = (double)total_paths;
+    stats_.segments = seg;
+    stats_.shadow_rays = shadows;
+    stats_.waves = waves;
     if (herr[0] != 0) return fail(LUCID_ERR_OVERFLOW, "BVH traversal stack overflow");
     if (status == LUCID_ERR_CANCELLED) return fail(LUCID_ERR_CANCELLED, "render cancelled");
     return LUCID_OK;

@@ -50,6 +50,18 @@ public:
     int async_revision() const { return async_revision_.load(); }
     bool async_running() const { return async_run_.load(); }
     int render_noalloc(const LucidRenderParams& p, float* d_out);
+    // Jobs on other engines' scenes in one set of wavefront launches over a
+    // device job table (lucid_cuda_render_batch); the scenes must stay
+    // loaded until the call returns.
+    struct BatchItem {
+        const void* scene;        // DeviceScene: scene_ptr() of the engine or snapshot holding it
+        float camera[10];         // position, direction, up, vertical fov (degrees)
+        LucidRenderParams p;      // the same max_depth for every job
+        float* out_host;          // tile_w * tile_h * 4 floats (the layout of render)
+    };
+    int render_batch(const BatchItem* items, int n, const char* algorithm, long long wave_paths);
+    // Device memory of a batch: path state for wave_paths paths and films of `pixels`.
+    static long long batch_bytes(long long pixels, long long wave_paths);
     int render_debug(int tx, int ty, int tw, int th, int fw, int fh, const char* mode, float* out_host);
     // Path diagnostics (PyRenderer's diagnostics API, pybind_renderer.hpp:893-1102).
     int diag_enable(const LucidDiagConfig* cfg);

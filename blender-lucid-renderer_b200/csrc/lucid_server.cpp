@@ -17,6 +17,11 @@ namespace {
 // an interactive job aims for.
 constexpr long long kJobWavePaths = 1LL << 24;
 constexpr double kInteractiveMs = 33.0;
+// Default paths per batch (one wave: 64 Mi paths, 11 GB of path state) and
+// the most jobs one batch takes.
+constexpr long long kBatchPaths = 1LL << 26;
+constexpr int kBatchJobs = 256;
+long long job_paths(const LucidJobDesc& d) { return (long long)d.width * d.height * d.samples; }
 
 double percentile(std::vector<double> v, double q) {
     if (v.empty()) return 0.0;
@@ -32,7 +37,7 @@ double Server::now() const {
     return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
 }
 
-Server::Server(int device, int slots, long long budget_bytes) : device_(device) {
+Server::Server(int device, int slots, long long budget_bytes) : device_(device), batch_paths_(kBatchPaths) {
     slots = std::max(1, slots);
     if (budget_bytes <= 0) {
         // 70 % of the free memory: the rest holds the path pools slots keep
@@ -157,6 +162,8 @@ void Server::slot_loop(int slot) {
     for (;;) {
         int id = -1;
         Job* j = nullptr;
+        std::vector<Job*> batch;
+        long long batch_bytes = 0;
         {
             std::unique_lock<std::mutex> lk(mu_);
             cv_.wait(lk, [&] {
@@ -174,12 +181,60 @@ void Server::slot_loop(int slot) {
             id = queue_.front();
             queue_.pop_front();
             j = &jobs_[id];
-            adm_.start(j->bytes);
-            j->state = LUCID_JOB_RUNNING;
-            j->t_start = now();
-            if (busy_from_ < 0) busy_from_ = j->t_start;
+            // a throughput job takes the compatible jobs waiting behind it
+            // (same integrator and depth, in queue order) into one batch
+            // while the batch stays within a wave and the budget
+            std::vector<Job*> members{j};
+            long long paths = job_paths(j->d), pixels = (long long)j->d.width * j->d.height;
+            long long bbytes = Engine::batch_bytes(pixels, paths);
+            const bool batchable = batch_paths_ > 0 && !j->d.interactive && !j->d.guided;
+            if (batchable && paths < batch_paths_) {
+                for (auto it = queue_.begin(); it != queue_.end() && (int)members.size() < kBatchJobs;) {
+                    Job& c = jobs_[*it];
+                    const long long p2 = paths + job_paths(c.d), px2 = pixels + (long long)c.d.width * c.d.height;
+                    const long long b2 = Engine::batch_bytes(px2, p2);
+                    if (c.cancel || c.d.interactive || c.d.guided || c.d.max_depth != j->d.max_depth ||
+                        std::strcmp(c.d.algorithm, j->d.algorithm) != 0 || p2 > batch_paths_ ||
+                        adm_.reserved + adm_.running + b2 > adm_.budget) {
+                        ++it;
+                        continue;
+                    }
+                    members.push_back(&c);
+                    paths = p2;
+                    pixels = px2;
+                    bbytes = b2;
+                    it = queue_.erase(it);
+                }
+            }
+            const double t = now();
+            if (busy_from_ < 0) busy_from_ = t;
+            if (members.size() > 1) {
+                adm_.start(bbytes);
+                for (Job* m : members) {
+                    m->state = LUCID_JOB_RUNNING;
+                    m->t_start = t;
+                }
+                batch = std::move(members);
+            } else {
+                adm_.start(j->bytes);
+                j->state = LUCID_JOB_RUNNING;
+                j->t_start = t;
+            }
+            batch_bytes = bbytes;
         }
         cv_.notify_all();   // another slot may start the next job too
+        if (!batch.empty()) {
+            int rc = run_batch(*slot_eng_[slot], batch);
+            if (rc == LUCID_ERR_OOM) {   // retained pools may be in the way: release them and retry once
+                slot_eng_[slot]->guide_free();
+                slot_eng_[slot]->accum_end();
+                slot_eng_[slot]->release_pool();
+                if (pre_eng_[slot]) pre_eng_[slot]->release_pool();
+                rc = run_batch(*slot_eng_[slot], batch);
+            }
+            finish_batch(batch, batch_bytes, rc);
+            continue;
+        }
         // the slot keeps its path pool (and a guided job's buffers) for the
         // next job: freeing device memory synchronises the whole device and
         // would stall every other slot's work
@@ -397,6 +452,63 @@ int Server::run_guided_job(Engine& e, Job& j, int slot, bool keep_pool) {
     return rc;
 }
 
+// A batch: every member's whole image in one Engine::render_batch call on
+// the slot's engine (each member on the scene version of its submission).
+int Server::run_batch(Engine& e, const std::vector<Job*>& members) {
+    std::vector<Engine::BatchItem> items(members.size());
+    for (size_t k = 0; k < members.size(); ++k) {
+        Job& j = *members[k];
+        const LucidJobDesc& d = j.d;
+        j.image.assign((size_t)d.width * d.height * 4, 0.0f);
+        Engine::BatchItem& it = items[k];
+        it.scene = j.snap->ds.get();
+        std::memcpy(it.camera, d.camera, sizeof(it.camera));
+        it.p = LucidRenderParams{0, 0, d.width, d.height, d.width, d.height, d.samples, 0, d.max_depth, 0};
+        it.out_host = j.image.data();
+    }
+    int rc = e.render_batch(items.data(), (int)items.size(), members[0]->d.algorithm, batch_paths_);
+    if (rc != LUCID_OK) {
+        std::lock_guard<std::mutex> lk(mu_);
+        for (Job* m : members) m->error = e.last_error();
+    }
+    return rc;
+}
+
+void Server::finish_batch(const std::vector<Job*>& members, long long bytes, int rc) {
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        adm_.finish(bytes);
+        ++batches_;
+        batched_jobs_ += (int)members.size();
+        const double t = now();
+        busy_to_ = std::max(busy_to_, t);
+        for (Job* m : members) {
+            Job& j = *m;
+            j.t_end = t;
+            if (rc == LUCID_OK && !j.cancel) {
+                j.state = LUCID_JOB_DONE;
+                j.done = j.d.samples;
+                j.t_first = t;
+                j.error.clear();
+                samples_done_ += (long long)j.d.samples * j.d.width * j.d.height;
+            } else {
+                j.state = j.cancel ? LUCID_JOB_CANCELLED : LUCID_JOB_FAILED;
+                j.image.clear();
+            }
+            j.snap.reset();
+        }
+    }
+    cv_.notify_all();
+    done_cv_.notify_all();
+}
+
+int Server::set_batching(long long max_paths) {
+    if (max_paths < 0) return fail(LUCID_ERR_INVALID, "batching: max_paths must be >= 0");
+    std::lock_guard<std::mutex> lk(mu_);
+    batch_paths_ = max_paths;
+    return LUCID_OK;
+}
+
 int Server::state(int job, int* samples_done) {
     std::lock_guard<std::mutex> lk(mu_);
     auto it = jobs_.find(job);
@@ -463,6 +575,8 @@ int Server::stats(LucidServerStats* out) {
     out->bytes_reserved = adm_.reserved;
     out->bytes_running = adm_.running;
     out->budget_bytes = adm_.budget;
+    out->batches = batches_;
+    out->batched_jobs = batched_jobs_;
     return LUCID_OK;
 }
 

@@ -12,7 +12,10 @@
 // (HBM budget = uploaded scenes + every running job's path state and film;
 // slots keep their path pools between jobs, since freeing device memory
 // synchronises the device, and the default budget leaves room for them);
-// a job that could never fit is refused at submission.  The autotuner also
+// a job that could never fit is refused at submission.  Throughput jobs
+// (not interactive, not guided) waiting together with the same integrator
+// and depth run as one batch: one set of wavefront launches over a device
+// job table (Engine::render_batch), up to a wave of paths.  The autotuner also
 // picks the kernels' launch profile (resident CTAs per SM).  Scene edits make a
 // new scene version; a job renders the version current when it was
 // submitted.  Guided jobs (the "mis" integrator with online path guiding)
@@ -64,6 +67,9 @@ public:
     int result(int job, float* out, size_t cap_floats);
     int cancel(int job);
     int stats(LucidServerStats* out);
+    // Batched throughput jobs: at most `max_paths` paths (samples x pixels)
+    // per batch, 0 = every job its own launches.
+    int set_batching(long long max_paths);
     const std::string& last_error() const { return err_; }
     int fail(int code, const std::string& m) { err_ = m; return code; }
 
@@ -85,6 +91,8 @@ private:
     void slot_loop(int slot);
     int run_job(Engine& e, Job& j, int slot, bool keep_pool);
     int run_guided_job(Engine& e, Job& j, int slot, bool keep_pool);
+    int run_batch(Engine& e, const std::vector<Job*>& members);
+    void finish_batch(const std::vector<Job*>& members, long long bytes, int rc);
     void finish_job(Job& j, int rc);
     void run_waiting_interactive(int slot);
     int pick_chunk(Engine& e, Job& j, int slot, int& offset);
@@ -107,6 +115,8 @@ private:
     bool stop_ = false;
     double t0_ = 0, busy_from_ = -1, busy_to_ = 0;
     long long samples_done_ = 0;
+    long long batch_paths_;
+    int batches_ = 0, batched_jobs_ = 0;
     std::string err_;
 };
 

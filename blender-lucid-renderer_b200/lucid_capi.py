@@ -209,13 +209,19 @@ class JobDesc(ctypes.Structure):
                 ("guide_seed", ctypes.c_int)]
 
 
+class BatchJob(ctypes.Structure):
+    _fields_ = [("scene", ctypes.c_void_p), ("camera", ctypes.c_float * 10), ("params", RenderParams),
+                ("out_rgba", ctypes.c_void_p)]
+
+
 class ServerStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_int), ("done", ctypes.c_int), ("refused", ctypes.c_int),
                 ("running", ctypes.c_int), ("queued", ctypes.c_int),
                 ("latency_p50_ms", ctypes.c_double), ("latency_p99_ms", ctypes.c_double),
                 ("first_p50_ms", ctypes.c_double), ("first_p99_ms", ctypes.c_double),
                 ("samples_per_s", ctypes.c_double), ("bytes_reserved", ctypes.c_longlong),
-                ("bytes_running", ctypes.c_longlong), ("budget_bytes", ctypes.c_longlong)]
+                ("bytes_running", ctypes.c_longlong), ("budget_bytes", ctypes.c_longlong),
+                ("batches", ctypes.c_int), ("batched_jobs", ctypes.c_int)]
 
 
 JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_REFUSED, JOB_FAILED, JOB_CANCELLED = range(6)
@@ -243,6 +249,7 @@ SIGNATURES = {
     "lucid_cuda_render": (_I, [_P, ctypes.POINTER(RenderParams), _P, _P]),
     "lucid_cuda_render_device": (_I, [_P, ctypes.POINTER(RenderParams), _P]),
     "lucid_cuda_render_noalloc": (_I, [_P, ctypes.POINTER(RenderParams), _P]),
+    "lucid_cuda_render_batch": (_I, [_P, _P, _I, ctypes.c_char_p]),
     "lucid_cuda_render_debug": (_I, [_P, _I, _I, _I, _I, _I, _I, ctypes.c_char_p, _P]),
     "lucid_cuda_get_stats": (_I, [_P, ctypes.POINTER(RenderStats)]),
     "lucid_cuda_set_wave_capacity": (_I, [_P, ctypes.c_longlong]),
@@ -290,6 +297,7 @@ SIGNATURES = {
     "lucid_server_result": (_I, [_P, _I, _P, ctypes.c_size_t]),
     "lucid_server_cancel": (_I, [_P, _I]),
     "lucid_server_stats": (_I, [_P, ctypes.POINTER(ServerStats)]),
+    "lucid_server_set_batching": (_I, [_P, ctypes.c_longlong]),
     "lucid_admission_plan": (_I, [ctypes.c_longlong, ctypes.c_longlong, _I, _P, _I, _P]),
     "lucid_guide_create": (_I, [_I, _I, ctypes.POINTER(_P)]),
     "lucid_guide_destroy": (None, [_P]),
@@ -450,6 +458,29 @@ class Context:
         p = RenderParams(0, 0, tile_w, tile_h, tile_w, tile_h, samples, sample_offset, max_depth, 0)
         rc = self.lib.lucid_cuda_render_noalloc(self.h, ctypes.byref(p), ctypes.c_void_p(d_out_ptr))
         return self._check(rc) if check else rc
+
+    def render_batch(self, jobs, algorithm: str = "mis", check=True):
+        """lucid_cuda_render_batch: `jobs` is a list of dicts with `scene` (a
+        Context with a loaded scene), `camera` (10 floats), `width`, `height`
+        and optionally `samples`, `sample_offset`, `max_depth` (8), `tile_x`,
+        `tile_y`, `full_w`, `full_h` (a tile of a larger image).  Returns
+        ([image per job], status); each image is (height, width, 4) float32."""
+        arr = (BatchJob * len(jobs))()
+        imgs = []
+        for k, j in enumerate(jobs):
+            w, h = int(j["width"]), int(j["height"])
+            img = np.zeros((h, w, 4), np.float32)
+            imgs.append(img)
+            arr[k].scene = j["scene"].h
+            arr[k].camera = (ctypes.c_float * 10)(*[float(c) for c in j["camera"]])
+            arr[k].params = RenderParams(int(j.get("tile_x", 0)), int(j.get("tile_y", 0)), w, h,
+                                         int(j.get("full_w", w)), int(j.get("full_h", h)), int(j.get("samples", 1)),
+                                         int(j.get("sample_offset", 0)), int(j.get("max_depth", 8)), 0)
+            arr[k].out_rgba = img.ctypes.data
+        rc = self.lib.lucid_cuda_render_batch(self.h, ctypes.addressof(arr), len(jobs), algorithm.encode())
+        if check:
+            self._check(rc)
+        return imgs, rc
 
     def render_debug(self, mode: str, tile_w, tile_h, full_w=None, full_h=None, tile_x=0, tile_y=0):
         full_w = tile_w if full_w is None else full_w
@@ -703,6 +734,12 @@ class Server:
 
     def cancel(self, job: int):
         self.lib.lucid_server_cancel(self.h, job)
+
+    def set_batching(self, max_paths: int) -> None:
+        """lucid_server_set_batching: batches of at most max_paths paths (0: off)."""
+        rc = self.lib.lucid_server_set_batching(self.h, int(max_paths))
+        if rc != LUCID_OK:
+            self._err(rc)
 
     def stats(self) -> dict:
         st = ServerStats()

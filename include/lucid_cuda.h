@@ -243,6 +243,26 @@ int lucid_cuda_render_device(LucidCudaCtx* ctx, const LucidRenderParams* params,
  * caller.  The scene must already be loaded (lucid_cuda_load_scene_json
  * allocates). */
 int lucid_cuda_render_noalloc(LucidCudaCtx* ctx, const LucidRenderParams* params, float* d_out_rgba);
+/* Batched jobs.  No counterpart in the reference: the add-on gives every
+ * session its own Renderer and renders each job with its own calls
+ * (LucidRenderer/render_session.py:77-106, pybind_renderer.hpp:185-361).
+ * Renders n jobs, each on the scene of its own context (`scene`: that
+ * context's scene version current at the call; `ctx` may be one of them),
+ * with its own camera, tile, image size, samples and sample offset, in one
+ * set of wavefront launches over a device job table: the jobs' samples fill
+ * waves of up to the context's wave capacity in job order, every path
+ * carries its job's scene index, and each kernel launch of a wave serves all
+ * its jobs.  Every job's image (out_rgba: host, tile_w*tile_h*4 floats) is
+ * bit for bit the lucid_cuda_render of the same params on its own context
+ * with that camera and `algorithm`.  All jobs need the same max_depth.  No
+ * sample records, path diagnostics or path guiding. */
+typedef struct LucidBatchJob {
+    LucidCudaCtx* scene;        /* context whose loaded scene the job renders */
+    float camera[10];           /* position, direction, up, vertical fov (degrees) */
+    LucidRenderParams params;   /* tile, image size, samples, sample_offset, max_depth */
+    float* out_rgba;            /* host image, the layout of lucid_cuda_render */
+} LucidBatchJob;
+int lucid_cuda_render_batch(LucidCudaCtx* ctx, const LucidBatchJob* jobs, int n, const char* algorithm);
 /* Replaces PyRenderer::render_debug / render_debug_gpu
  * (pybind_renderer.hpp:371-525): mode "normal", "albedo" or "emission" at
  * the primary hit, no jitter, Y-flipped RGBA. */
@@ -474,6 +494,7 @@ typedef struct LucidServerStats {
     double first_p50_ms, first_p99_ms;       /* submit -> first iteration finished */
     double samples_per_s;                    /* samples of finished jobs / busy wall time */
     long long bytes_reserved, bytes_running, budget_bytes;
+    int batches, batched_jobs;               /* batches run (lucid_server_set_batching) and the jobs in them */
 } LucidServerStats;
 
 /* slots: concurrent jobs; budget_bytes: device memory the jobs may use
@@ -501,6 +522,14 @@ int lucid_server_wait(LucidServer* srv, int job_id, int timeout_ms);
 int lucid_server_result(LucidServer* srv, int job_id, float* out_rgba, size_t cap_floats);
 int lucid_server_cancel(LucidServer* srv, int job_id);
 int lucid_server_stats(LucidServer* srv, LucidServerStats* out);
+/* Batched throughput jobs (no counterpart in the reference).  Jobs that are
+ * neither interactive nor guided and wait in the queue together with the
+ * same algorithm and max_depth run as one batch (lucid_cuda_render_batch:
+ * one set of wavefront launches over a device job table) of at most
+ * max_paths paths (width * height * samples summed over the batch; default
+ * 2^26); a job of max_paths paths or more runs on its own.  A batch's jobs
+ * finish together, each image unchanged.  0 turns batching off. */
+int lucid_server_set_batching(LucidServer* srv, long long max_paths);
 /* The server's admission policy on its own (host only, no GPU): n jobs of
  * job_bytes[i] arrive in order; decision[i] = the start order of job i
  * (0, 1, ...) when jobs finish in start order, or -1 when it is refused. */
