@@ -477,20 +477,34 @@ def batch_mix(device: int, seed: int = 11, slots: int = 4) -> dict:
         srv.close()
         return wall, upload, st
 
-    batch_paths = 1 << 26
+    batch_paths = 1 << 25
     run(slots, batch_paths)   # first use of every kernel and allocation
     wall_batched, upload, st = run(slots, batch_paths)
     wall_mix = run(slots, 0)[0]
     # the one-slot figure varies from run to run (host threads, allocations):
     # the better of two runs
     wall_seq = min(run(1, 0)[0], run(1, 0)[0])
+    # what one large render reaches on these scenes: 1024x1024 at 16 spp on
+    # the most detailed variant (the batch cannot beat its scenes' own rate)
+    k_big = max(range(48), key=lambda k: jobs[k][2])
+    ctx = lucid_capi.Context(device)
+    ctx.load_scene_arrays(scenes[k_big][0])
+    ctx.set_camera(*scenes[k_big][1])
+    ctx.set_algorithm("mis")
+    ctx.render(1024, 1024, 1024, 1024, 16, 0, 8)
+    t0 = time.perf_counter()
+    ctx.render(1024, 1024, 1024, 1024, 16, 0, 8)
+    single_rate = 1024 * 1024 * 16 / (time.perf_counter() - t0)
+    ctx.close()
     return {"jobs": len(jobs), "scenes": len(scenes), "triangles": int(sum(s[2] for s in scenes)),
             "samples": total, "slots": slots, "upload_s": round(upload, 3),
             "samples_per_s": total / wall_batched, "batches": st["batches"], "batched_jobs": st["batched_jobs"],
             "batch_paths": batch_paths,
             "samples_per_s_per_job_launches": total / wall_mix, "samples_per_s_sequential": total / wall_seq,
+            "single_large_job": {"scene_triangles": int(scenes[k_big][2]), "frame": "1024x1024, 16 spp, mis depth 8",
+                                 "samples_per_s": single_rate},
             "latency_p50_ms": st["latency_p50_ms"], "latency_p99_ms": st["latency_p99_ms"],
-            "launch": "throughput jobs batched up to 2^26 paths: one set of wavefront launches over a device "
+            "launch": "throughput jobs batched up to 2^25 paths: one set of wavefront launches over a device "
                       "job table per batch (each path carries its scene index), batches on per-slot streams; "
                       "per_job_launches: the same slots with batching off (each job its own launches); "
                       "sequential: one slot, batching off"}

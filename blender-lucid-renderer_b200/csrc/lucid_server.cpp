@@ -17,9 +17,13 @@ namespace {
 // an interactive job aims for.
 constexpr long long kJobWavePaths = 1LL << 24;
 constexpr double kInteractiveMs = 33.0;
-// Default paths per batch (one wave: 64 Mi paths, 11 GB of path state) and
-// the most jobs one batch takes.
-constexpr long long kBatchPaths = 1LL << 26;
+// Default paths per batch (one wave: 32 Mi paths, 6 GB of path state) and
+// the most jobs one batch takes.  On the batched configuration (56 jobs on
+// 56 scenes, 175 M samples), same box: 2^25 455 M samples/s on 4 slots,
+// 2^26 398 M, 2^27 379 M, 2^28 362 M (two or more smaller batches in flight
+// overlap each other's wave tails and host gaps; large retained pools crowd
+// the device).
+constexpr long long kBatchPaths = 1LL << 25;
 constexpr int kBatchJobs = 256;
 long long job_paths(const LucidJobDesc& d) { return (long long)d.width * d.height * d.samples; }
 

@@ -527,7 +527,7 @@ int lucid_server_stats(LucidServer* srv, LucidServerStats* out);
  * same algorithm and max_depth run as one batch (lucid_cuda_render_batch:
  * one set of wavefront launches over a device job table) of at most
  * max_paths paths (width * height * samples summed over the batch; default
- * 2^26); a job of max_paths paths or more runs on its own.  A batch's jobs
+ * 2^25); a job of max_paths paths or more runs on its own.  A batch's jobs
  * finish together, each image unchanged.  0 turns batching off. */
 int lucid_server_set_batching(LucidServer* srv, long long max_paths);
 /* The server's admission policy on its own (host only, no GPU): n jobs of
