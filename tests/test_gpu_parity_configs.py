@@ -161,3 +161,36 @@ def test_reference_literal_mode_mismatch_rate(ctx, c2_scene):
     assert r1["primary_mismatch"] <= 0.01 * r1["samples"] and r2["primary_mismatch"] <= 0.01 * r2["samples"]
     assert r1["hash_mismatch_rate"] < 0.15 and r2["hash_mismatch_rate"] < 0.25
     assert r1["image_rel_l1"] < 0.05
+
+
+def test_c2_crop_in_a_batch_equals_its_own_renders(c2_scene, tmp_path):
+    """The bench scene's stratified crop rendered as tiles inside one batch
+    (lucid_cuda_render_batch) beside a Cornell job: the kernels that read
+    each path's scene from the batch's scene table give every tile the image
+    of its own render call on the 1M-triangle BVH, bit for bit."""
+    import lucid_capi
+    import lucid_scenes as ls
+    js, cam = c2_scene
+    c2 = lucid_capi.Context(0)
+    c2.load_scene_json(js)
+    c2.set_camera(*cam)
+    c2.set_algorithm(C2_ALGO)
+    cb_scene, cb_cam = ls.cornell_box()
+    cb = lucid_capi.Context(0)
+    cb.load_scene_json(ls.to_json(cb_scene))
+    jobs, want = [], []
+    for k, (tx, ty, tw, th) in enumerate(_c2_tiles()[:8]):
+        jobs.append({"scene": c2, "camera": cam, "tile_x": tx, "tile_y": ty, "width": tw, "height": th,
+                     "full_w": C2_W, "full_h": C2_H, "samples": 4, "sample_offset": 64 * k, "max_depth": C2_DEPTH})
+        want.append(c2.render(tw, th, C2_W, C2_H, 4, 64 * k, C2_DEPTH, tile_x=tx, tile_y=ty)[0])
+        if k == 3:
+            jobs.append({"scene": cb, "camera": cb_cam, "width": 64, "height": 64, "samples": 4,
+                         "max_depth": C2_DEPTH})
+            cb.set_camera(*cb_cam)
+            cb.set_algorithm(C2_ALGO)
+            want.append(cb.render(64, 64, 64, 64, 4, 0, C2_DEPTH)[0])
+    got, _ = c2.render_batch(jobs, C2_ALGO)
+    for k in range(len(jobs)):
+        np.testing.assert_array_equal(got[k], want[k], err_msg="job %d" % k)
+    c2.close()
+    cb.close()
