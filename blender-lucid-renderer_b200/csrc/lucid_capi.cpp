@@ -158,19 +158,28 @@ int lucid_cuda_render_noalloc(LucidCudaCtx* ctx, const LucidRenderParams* params
 int lucid_cuda_render_batch(LucidCudaCtx* ctx, const LucidBatchJob* jobs, int n, const char* algorithm) {
     if (!jobs || n <= 0) return LUCID_ERR_INVALID;
     return guarded(ctx, [&](lucid::Engine& e) {
+        // a job that cannot start leaves every image zero, as a failed render does
+        auto refuse = [&](int code, const std::string& msg) {
+            for (int j = 0; j < n; ++j) {
+                const LucidRenderParams& p = jobs[j].params;
+                if (jobs[j].out_rgba && p.tile_w > 0 && p.tile_h > 0)
+                    std::memset(jobs[j].out_rgba, 0, (size_t)p.tile_w * p.tile_h * 4 * sizeof(float));
+            }
+            return e.fail(code, msg);
+        };
         // each distinct scene context's current version, held for the call
         std::vector<LucidCudaCtx*> owners;
         std::vector<lucid::SceneSnapshot> snaps;
         std::vector<lucid::Engine::BatchItem> items((size_t)n);
         for (int j = 0; j < n; ++j) {
             LucidCudaCtx* sc = jobs[j].scene;
-            if (!sc || !sc->engine) return e.fail(LUCID_ERR_INVALID, "batch: job " + std::to_string(j) + " has no scene context");
+            if (!sc || !sc->engine) return refuse(LUCID_ERR_INVALID, "batch: job " + std::to_string(j) + " has no scene context");
             size_t k = 0;
             while (k < owners.size() && owners[k] != sc) ++k;
             if (k == owners.size()) {
                 snaps.emplace_back();
                 if (sc->engine->snapshot_scene(snaps.back()) != LUCID_OK)
-                    return e.fail(LUCID_ERR_NO_SCENE, "batch: job " + std::to_string(j) + ": " + sc->engine->last_error());
+                    return refuse(LUCID_ERR_NO_SCENE, "batch: job " + std::to_string(j) + ": " + sc->engine->last_error());
                 owners.push_back(sc);
             }
             lucid::Engine::BatchItem& it = items[(size_t)j];

@@ -3299,6 +3299,19 @@ int Engine::render_batch(const BatchItem* items, int n, const char* algorithm, l
     GpuLock gl(*this);
     reset_cancel();
     if (n <= 0 || !items) return fail(LUCID_ERR_INVALID, "batch: no jobs");
+    // a call that returns before the images are copied out leaves every
+    // job's image zero, as a single render call does
+    struct ZeroUnlessCopied {
+        const BatchItem* it;
+        int n;
+        bool copied = false;
+        ~ZeroUnlessCopied() {
+            if (copied) return;
+            for (int j = 0; j < n; ++j)
+                if (it[j].out_host && it[j].p.tile_w > 0 && it[j].p.tile_h > 0)
+                    std::fill(it[j].out_host, it[j].out_host + (size_t)it[j].p.tile_w * it[j].p.tile_h * 4, 0.0f);
+        }
+    } host_images{items, n};
     const int algo = algo_from_name(algorithm);
     const int depth = items[0].p.max_depth;
     if (depth < 1 || depth > kMaxDepth) return fail(LUCID_ERR_INVALID, "batch: max_depth must be 1..1024");
@@ -3480,6 +3493,7 @@ int Engine::render_batch(const BatchItem* items, int n, const char* algorithm, l
             CK(cudaMemcpyAsync(items[k].out_host, P.out.p + film_off[k],
                                (film_off[(size_t)k + 1] - film_off[k]) * sizeof(float4), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    host_images.copied = status == LUCID_OK;
     float tot = 0.0f;
     cudaEventElapsedTime(&tot, t0, t1);
     cudaEventDestroy(t0);

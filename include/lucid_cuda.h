@@ -255,7 +255,9 @@ int lucid_cuda_render_noalloc(LucidCudaCtx* ctx, const LucidRenderParams* params
  * its jobs.  Every job's image (out_rgba: host, tile_w*tile_h*4 floats) is
  * bit for bit the lucid_cuda_render of the same params on its own context
  * with that camera and `algorithm`.  All jobs need the same max_depth.  No
- * sample records, path diagnostics or path guiding. */
+ * sample records, path diagnostics or path guiding.  A call that fails or
+ * is cancelled (lucid_cuda_cancel on ctx, checked between waves) leaves
+ * every job's image zero. */
 typedef struct LucidBatchJob {
     LucidCudaCtx* scene;        /* context whose loaded scene the job renders */
     float camera[10];           /* position, direction, up, vertical fov (degrees) */

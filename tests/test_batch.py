@@ -6,6 +6,8 @@ its own scene, whatever the batch around it and however its samples are cut
 across waves; one batch is also checked against the CPU oracle directly."""
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -43,6 +45,17 @@ def test_batch_rejects_bad_jobs_without_a_gpu():
     assert lib.lucid_cuda_render_batch(ctx.h, None, 0, b"mis") == lucid_capi.LUCID_ERR_INVALID
     assert lib.lucid_cuda_render_batch(None, None, 1, b"mis") == lucid_capi.LUCID_ERR_INVALID
     job = {"scene": ctx, "camera": (0, 0, 3, 0, 0, -1, 0, 1, 0, 45), "width": 4, "height": 4}
+    # the binding hands the library non-zero buffers here: a refused batch
+    # must leave every image zero
+    arr = (lucid_capi.BatchJob * 2)()
+    imgs = [np.full((4, 4, 4), 7.0, np.float32), np.full((2, 3, 4), 7.0, np.float32)]
+    for k, img in enumerate(imgs):
+        arr[k].scene = ctx.h
+        arr[k].params = lucid_capi.RenderParams(0, 0, img.shape[1], img.shape[0], img.shape[1], img.shape[0],
+                                                1, 0, 8, 0)
+        arr[k].out_rgba = img.ctypes.data
+    assert lib.lucid_cuda_render_batch(ctx.h, ctypes.addressof(arr), 2, b"mis") == lucid_capi.LUCID_ERR_NO_SCENE
+    assert not any(img.any() for img in imgs)
     _, rc = ctx.render_batch([job], check=False)
     assert rc == lucid_capi.LUCID_ERR_NO_SCENE
     ctx.close()
