@@ -510,6 +510,61 @@ def batch_mix(device: int, seed: int = 11, slots: int = 4) -> dict:
                       "sequential: one slot, batching off"}
 
 
+def sessions(device: int, n_sessions: int = 8, calls: int = 8) -> dict:
+    """Concurrent sessions: n_sessions contexts, each on its own material
+    preview scene and its own host thread, render `calls` calls of
+    256x256 at 8 spp (mis, depth 8) at the same time, as the add-on's
+    material previews do, with the device's combiner of concurrent small
+    renders on (the calls meet in batches) and off (each call its own
+    launches on its own stream): aggregate samples/s."""
+    import threading
+
+    import lucid_capi
+    import lucid_scenes as ls
+    ctxs = []
+    for k in range(n_sessions):
+        sc, cam = ls.material_preview_scene(500 + k)
+        c = lucid_capi.Context(device)
+        c.load_scene_json(ls.to_json(sc))
+        c.set_camera(*cam)
+        c.set_algorithm("mis")
+        ctxs.append(c)
+    w = h = 256
+    spp = 8
+
+    def run(on):
+        for c in ctxs:
+            c.set_combining(on)
+        start = threading.Barrier(n_sessions + 1)
+
+        def body(c):
+            start.wait()
+            for i in range(calls):
+                c.render(w, h, w, h, spp, spp * i, 8)
+
+        ts = [threading.Thread(target=body, args=(c,)) for c in ctxs]
+        for t in ts:
+            t.start()
+        start.wait()
+        t0 = time.perf_counter()
+        for t in ts:
+            t.join()
+        return time.perf_counter() - t0
+
+    total = n_sessions * calls * w * h * spp
+    run(True)
+    run(False)   # first use of every path pool and kernel
+    b0, c0 = lucid_capi.combine_stats(device)
+    on = min(run(True), run(True))
+    b1, c1 = lucid_capi.combine_stats(device)
+    off = min(run(False), run(False))
+    for c in ctxs:
+        c.close()
+    return {"sessions": n_sessions, "calls_per_session": calls, "call": "256x256, 8 spp, mis depth 8",
+            "samples": total, "samples_per_s_combined": total / on, "samples_per_s_separate": total / off,
+            "batches": (b1 - b0) // 2, "calls_in_batches": (c1 - c0) // 2}
+
+
 def guiding(device: int, budget_ms: float = 1000.0, width: int = 1280, height: int = 720) -> dict:
     """Equal-time relMSE on the hard-indirect room (1280x720, mis, depth 8)
     against an independent FP64-accumulated 4096-spp reference: plain and
@@ -649,8 +704,8 @@ def main():
         return 0
     if args.serving_only:
         dev = int(os.environ.get("LOCAL_RANK", "0"))
-        print(json.dumps({"serving": serving(dev), "batch": batch_mix(dev), "diagnostics": diagnostics(dev)}),
-              flush=True)
+        print(json.dumps({"serving": serving(dev), "batch": batch_mix(dev), "sessions": sessions(dev),
+                          "diagnostics": diagnostics(dev)}), flush=True)
         return 0
     if args.guiding_only:
         print(json.dumps(guiding(int(os.environ.get("LOCAL_RANK", "0")), args.guide_budget_ms, args.guide_width,
@@ -750,6 +805,7 @@ def main():
     quality = c1_quality(local_rank) if rank == 0 and not args.no_quality else None
     serve = serving(local_rank) if rank == 0 and world == 1 and not args.no_serving else None
     batch = batch_mix(local_rank) if rank == 0 and world == 1 and not args.no_serving else None
+    sess = sessions(local_rank) if rank == 0 and world == 1 and not args.no_serving else None
     diag = diagnostics(local_rank) if rank == 0 and world == 1 and not args.no_serving else None
     guide = (guiding(local_rank, args.guide_budget_ms, args.guide_width, args.guide_height)
              if rank == 0 and world == 1 and not args.no_guiding else None)
@@ -782,7 +838,7 @@ def main():
             "issue": issue_roofline(kern, clocks["sm_mhz"]),
             "mrays_per_s": mrays, "segments_per_step": segs, "shadow_rays_per_step": shadows,
             "gpu_launches": launches, "clocks": clocks, "cpu_baseline": cpu, "quality": quality,
-            "serving": serve, "batch": batch, "diagnostics": diag, "guiding": guide, "scene_upload": upload,
+            "serving": serve, "batch": batch, "sessions": sess, "diagnostics": diag, "guiding": guide, "scene_upload": upload,
             "f12": f12,
         }
         print(json.dumps(line), flush=True)

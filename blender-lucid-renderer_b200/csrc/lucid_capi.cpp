@@ -155,6 +155,15 @@ int lucid_cuda_render_noalloc(LucidCudaCtx* ctx, const LucidRenderParams* params
     return guarded(ctx, [&](lucid::Engine& e) { return e.render_noalloc(*params, d_out_rgba); });
 }
 
+int lucid_cuda_set_combining(LucidCudaCtx* ctx, int on) {
+    return guarded(ctx, [&](lucid::Engine& e) { e.set_combining(on != 0); return LUCID_OK; });
+}
+
+int lucid_cuda_combine_stats(int device, long long* batches, long long* calls) {
+    lucid::Engine::combine_stats(device, batches, calls);
+    return LUCID_OK;
+}
+
 int lucid_cuda_render_batch(LucidCudaCtx* ctx, const LucidBatchJob* jobs, int n, const char* algorithm) {
     if (!jobs || n <= 0) return LUCID_ERR_INVALID;
     return guarded(ctx, [&](lucid::Engine& e) {

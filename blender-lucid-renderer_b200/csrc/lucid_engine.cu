@@ -21,8 +21,10 @@
 #include <cstdlib>
 #include <cstring>
 #include <chrono>
+#include <condition_variable>
 #include <future>
 #include <cub/cub.cuh>
+#include <map>
 #include <mutex>
 #include <thread>
 #include <string>
@@ -2001,6 +2003,8 @@ int Engine::set_camera(float px, float py, float pz, float dx, float dy, float d
                        float fov_deg) {
     GpuLock gl(*this);
     make_camera(cam_, px, py, pz, dx, dy, dz, ux, uy, uz, fov_deg);
+    const float raw[10] = {px, py, pz, dx, dy, dz, ux, uy, uz, fov_deg};
+    std::memcpy(cam_raw_, raw, sizeof(cam_raw_));
     camera_set_ = true;
     return LUCID_OK;
 }
@@ -2712,7 +2716,131 @@ int Engine::render(const LucidRenderParams& p, float* out_host, LucidSampleRecor
         if (recs) return fail(LUCID_ERR_INVALID, "per-sample records are not produced while diagnostics are enabled");
         return render_diag_impl(p, out_host, out_device);
     }
+    const long long paths = (long long)std::max(0, p.tile_w) * std::max(0, p.tile_h) * std::max(0, p.samples);
+    if (combine_ && out_host && !recs && !out_device && !(guide_ && guide_->on) && scene_loaded_ && camera_set_ &&
+        paths > 0 && paths <= kCombinePaths && p.full_w > 0 && p.full_h > 0 && p.max_depth >= 1 &&
+        p.max_depth <= kMaxDepth)
+        return render_combined(p, out_host);
     return render_impl(p, out_host, recs, out_device, nullptr, false);
+}
+
+// ---------------------------------------------------------------- combining concurrent small renders
+// Concurrent sessions (the add-on's viewport, material previews and F12
+// renders each own a Renderer) meet on one device.  Small render calls
+// (at most kCombinePaths paths, image to host memory, no records,
+// diagnostics or guiding) pass through a process-wide combiner per device:
+// a call that finds no other small call running renders on its own
+// context exactly as without the combiner; calls that arrive while one
+// runs wait, and the first of them to find the device free renders every
+// waiting call with the same integrator and depth as one batch
+// (render_batch on the combiner's own engine), each call's image bit for
+// bit its own render.  Large calls never wait here: they overlap on their
+// own streams as before.
+namespace {
+const char* const kAlgoNames[5] = {"simple", "nee", "mis", "volume_simple", "volume_mis"};
+struct CombineReq {
+    Engine* e;
+    Engine::BatchItem item;
+    int algo;
+    int rc = LUCID_OK;
+    bool done = false;
+    std::string err;
+    LucidRenderStats stats{};
+};
+struct Combiner {
+    std::mutex mu;
+    std::condition_variable cv;
+    bool busy = false;
+    std::vector<CombineReq*> pending;
+    std::unique_ptr<Engine> runner;   // renders the batches (its own stream and path pool)
+    long long batches = 0, calls = 0;
+};
+// One per device for the life of the process (never destroyed, so no CUDA
+// call runs from a static destructor at exit).
+Combiner& combiner_for(int device) {
+    static std::mutex mu;
+    static std::map<int, Combiner*>* all = new std::map<int, Combiner*>();
+    std::lock_guard<std::mutex> lk(mu);
+    Combiner*& c = (*all)[device];
+    if (!c) c = new Combiner();
+    return *c;
+}
+}  // namespace
+
+int Engine::render_combined(const LucidRenderParams& p, float* out_host) {
+    reset_cancel();
+    Combiner& C = combiner_for(device_);
+    CombineReq r;
+    r.e = this;
+    r.item.scene = ds_.get();
+    std::memcpy(r.item.camera, cam_raw_, sizeof(cam_raw_));
+    r.item.p = p;
+    r.item.p.flags = 0;
+    r.item.out_host = out_host;
+    r.algo = algo_;
+    std::shared_ptr<DeviceScene> keep = ds_;   // this call's scene version, whoever renders it
+    std::unique_lock<std::mutex> lk(C.mu);
+    C.pending.push_back(&r);
+    while (!r.done) {
+        if (C.busy) {
+            C.cv.wait(lk);
+            continue;
+        }
+        // lead: every waiting call with this call's integrator and depth
+        C.busy = true;
+        std::vector<CombineReq*> group;
+        for (auto it = C.pending.begin(); it != C.pending.end();) {
+            CombineReq* q = *it;
+            if (q->algo == r.algo && q->item.p.max_depth == r.item.p.max_depth && group.size() < 256) {
+                group.push_back(q);
+                it = C.pending.erase(it);
+            } else {
+                ++it;
+            }
+        }
+        lk.unlock();
+        if (group.size() == 1) {
+            // alone: this context's own render, as without the combiner
+            r.rc = render_impl(p, out_host, nullptr, nullptr, nullptr, false);
+            if (r.rc != LUCID_OK) r.err = err_;
+            r.stats = stats_;
+        } else {
+            int rc = LUCID_OK;
+            if (!C.runner) C.runner.reset(new Engine(device_));
+            std::vector<BatchItem> items;
+            items.reserve(group.size());
+            for (CombineReq* q : group) items.push_back(q->item);
+            rc = C.runner->render_batch(items.data(), (int)items.size(), kAlgoNames[r.algo], kCombinePaths * 8);
+            LucidRenderStats bst{};
+            C.runner->stats(&bst);
+            for (CombineReq* q : group) {
+                q->rc = rc;
+                if (rc != LUCID_OK) q->err = C.runner->last_error();
+                q->stats = bst;
+                q->stats.paths = (double)q->item.p.tile_w * q->item.p.tile_h * q->item.p.samples;
+            }
+        }
+        lk.lock();
+        for (CombineReq* q : group) q->done = true;
+        if (group.size() > 1) {
+            ++C.batches;
+            C.calls += (long long)group.size();
+        }
+        C.busy = false;
+        C.cv.notify_all();
+    }
+    lk.unlock();
+    stats_ = r.stats;
+    if (r.rc == LUCID_OK && is_cancelled()) return fail(LUCID_ERR_CANCELLED, "render cancelled");
+    if (r.rc != LUCID_OK) return fail(r.rc, r.err);
+    return LUCID_OK;
+}
+
+void Engine::combine_stats(int device, long long* batches, long long* calls) {
+    Combiner& C = combiner_for(device);
+    std::lock_guard<std::mutex> lk(C.mu);
+    if (batches) *batches = C.batches;
+    if (calls) *calls = C.calls;
 }
 
 int Engine::render_f64(const LucidRenderParams& p, double* out_host) {

@@ -60,6 +60,11 @@ public:
         float* out_host;          // tile_w * tile_h * 4 floats (the layout of render)
     };
     int render_batch(const BatchItem* items, int n, const char* algorithm, long long wave_paths);
+    // Small render calls of concurrent contexts combined into batches
+    // (lucid_cuda_set_combining); on by default.
+    void set_combining(bool on) { combine_ = on; }
+    static void combine_stats(int device, long long* batches, long long* calls);
+    static constexpr long long kCombinePaths = 1LL << 22;
     // Device memory of a batch: path state for wave_paths paths and films of `pixels`.
     static long long batch_bytes(long long pixels, long long wave_paths);
     int render_debug(int tx, int ty, int tw, int th, int fw, int fh, const char* mode, float* out_host);
@@ -130,6 +135,7 @@ private:
     int render_impl(const LucidRenderParams& p, float* out_host, LucidSampleRecord* recs, float* out_device,
                     void* accumulate, bool from_async, double* out_f64 = nullptr);
     int render_diag_impl(const LucidRenderParams& p, float* out_host, float* out_device);
+    int render_combined(const LucidRenderParams& p, float* out_host);
     void async_worker();
     int ensure_pool(long long paths, bool records);
     long long default_wave_paths(bool records) const;
@@ -151,6 +157,8 @@ private:
     int num_sms_ = 0;
     HostScene host_;
     HostCamera cam_;
+    float cam_raw_[10] = {};   // set_camera's arguments (batched renders rebuild the camera from them)
+    bool combine_ = true;
     bool scene_loaded_ = false, camera_set_ = false;
     int algo_ = 1;            // "nee": PyRenderer's default (pybind_renderer.hpp:68)
     std::shared_ptr<DeviceScene> ds_;

@@ -250,6 +250,8 @@ SIGNATURES = {
     "lucid_cuda_render_device": (_I, [_P, ctypes.POINTER(RenderParams), _P]),
     "lucid_cuda_render_noalloc": (_I, [_P, ctypes.POINTER(RenderParams), _P]),
     "lucid_cuda_render_batch": (_I, [_P, _P, _I, ctypes.c_char_p]),
+    "lucid_cuda_set_combining": (_I, [_P, _I]),
+    "lucid_cuda_combine_stats": (_I, [_I, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
     "lucid_cuda_render_debug": (_I, [_P, _I, _I, _I, _I, _I, _I, ctypes.c_char_p, _P]),
     "lucid_cuda_get_stats": (_I, [_P, ctypes.POINTER(RenderStats)]),
     "lucid_cuda_set_wave_capacity": (_I, [_P, ctypes.c_longlong]),
@@ -459,6 +461,11 @@ class Context:
         rc = self.lib.lucid_cuda_render_noalloc(self.h, ctypes.byref(p), ctypes.c_void_p(d_out_ptr))
         return self._check(rc) if check else rc
 
+    def set_combining(self, on: bool) -> None:
+        """lucid_cuda_set_combining: take part in (or stay out of) the
+        device's combining of concurrent small renders."""
+        self._check(self.lib.lucid_cuda_set_combining(self.h, int(bool(on))))
+
     def render_batch(self, jobs, algorithm: str = "mis", check=True):
         """lucid_cuda_render_batch: `jobs` is a list of dicts with `scene` (a
         Context with a loaded scene), `camera` (10 floats), `width`, `height`
@@ -651,6 +658,14 @@ def admission_plan(budget: int, reserved: int, slots: int, job_bytes) -> list:
     if rc != LUCID_OK:
         raise LucidError(rc, "admission plan")
     return out.tolist()
+
+
+def combine_stats(device: int = 0):
+    """(batches, calls) the device's combiner of concurrent small renders has run."""
+    lib = load_library()
+    b, c = ctypes.c_longlong(), ctypes.c_longlong()
+    lib.lucid_cuda_combine_stats(device, ctypes.byref(b), ctypes.byref(c))
+    return b.value, c.value
 
 
 class Server:

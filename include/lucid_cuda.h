@@ -265,6 +265,22 @@ typedef struct LucidBatchJob {
     float* out_rgba;            /* host image, the layout of lucid_cuda_render */
 } LucidBatchJob;
 int lucid_cuda_render_batch(LucidCudaCtx* ctx, const LucidBatchJob* jobs, int n, const char* algorithm);
+/* Concurrent small renders.  The reference gives each Blender session its
+ * own Renderer (render_session.py:77-106), so a viewport, several material
+ * previews and an F12 render call render_tile at the same time.  Here every
+ * context of a device meets in one process-wide combiner: a
+ * lucid_cuda_render call of at most 2^22 paths (tile_w * tile_h * samples)
+ * with a host image, no sample records, diagnostics or guiding, made while
+ * no other such call runs, renders on its own context as before; calls made
+ * while one runs wait, and the first of them to find the device free renders
+ * all waiting calls with its integrator and max_depth as one batch
+ * (lucid_cuda_render_batch), every image unchanged bit for bit.  Larger
+ * calls never wait for the combiner.  lucid_cuda_get_stats after a combined
+ * call describes its batch (paths: this call's).  On by default;
+ * on = 0 takes this context's calls out. */
+int lucid_cuda_set_combining(LucidCudaCtx* ctx, int on);
+/* Batches the combiner of `device` has run and the render calls in them. */
+int lucid_cuda_combine_stats(int device, long long* batches, long long* calls);
 /* Replaces PyRenderer::render_debug / render_debug_gpu
  * (pybind_renderer.hpp:371-525): mode "normal", "albedo" or "emission" at
  * the primary hit, no jitter, Y-flipped RGBA. */
