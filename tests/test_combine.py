@@ -14,7 +14,7 @@ import pytest
 
 import lucid_capi
 import lucid_scenes as ls
-from parity_util import scene_and_camera
+from parity_util import ATOL, RTOL, render_oracle, scene_and_camera
 
 
 def test_combining_calls_without_a_gpu():
@@ -95,6 +95,11 @@ def test_concurrent_sessions_equal_their_calls_alone(workdir):
                                               err_msg="%s %s call %d round %d" % (name, algo, i, r))
     # 21 small calls per round over five threads: some ran inside batches
     assert b1 - b0 >= 1 and c1 - c0 >= 2 * (b1 - b0)
+    # and directly against the CPU oracle: the first Cornell call of every round
+    scene, cam = scene_and_camera("cornell", workdir)
+    ref, _ = render_oracle(scene, cam, "mis", 96, 96, 8, 8, offset=0)
+    for r in range(rounds):
+        np.testing.assert_allclose(got[0][r * len(SESSIONS[0][2])], ref, rtol=RTOL, atol=ATOL)
     for c in ctxs:
         c.close()
 
