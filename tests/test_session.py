@@ -84,6 +84,21 @@ def test_display_pixels_match_reference_conversion():
         assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
 
 
+def test_display_pixels_on_the_host_threads_match_reference_conversion():
+    """A frame larger than one host-thread chunk (ragged last chunk):
+    every float of the threaded conversion, into a new array and into a
+    reused one, equals the reference's per-value conversion."""
+    rng = np.random.default_rng(5)
+    n_px = 3 * (1 << 16) + 37          # 786,580 floats: four chunks of 2^18 floats, the last one short
+    acc = (rng.random(n_px * 4) * 10.0 ** rng.integers(-8, 5, n_px * 4)).astype(np.float32)
+    out = np.full(n_px * 4, np.nan, np.float32)
+    for total in (3, 60):
+        ref = _reference_display(acc.tolist(), total)
+        for got in (lsn.display_pixels(acc, total), lsn.display_pixels(acc, total, out=out)):
+            assert got.shape == (n_px, 4)
+            assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+
+
 def test_session_without_scene():
     s = lsn.RenderSession()
     assert s.is_available and "available" in repr(s)
