@@ -398,6 +398,26 @@ int lucid_admission_plan(long long budget, long long reserved, int slots, const 
     return LUCID_OK;
 }
 
+int lucid_batch_plan(long long max_paths, long long room_bytes, const LucidJobDesc* jobs, const int* cancelled, int n,
+                     int* member) {
+    if (n <= 0 || !jobs || !member) return LUCID_ERR_INVALID;
+    try {
+        std::vector<const LucidJobDesc*> waiting;
+        std::vector<char> canc;
+        for (int i = 1; i < n; ++i) {
+            waiting.push_back(&jobs[i]);
+            canc.push_back(cancelled && cancelled[i] ? 1 : 0);
+        }
+        std::vector<int> take = lucid::plan_batch(jobs[0], waiting, canc, max_paths, room_bytes, 256, nullptr);
+        for (int i = 0; i < n; ++i) member[i] = 0;
+        for (int k : take) member[k + 1] = 1;
+        member[0] = take.empty() ? 0 : 1;
+        return (int)take.size() + 1;
+    } catch (...) {
+        return LUCID_ERR_INVALID;
+    }
+}
+
 int lucid_cuda_guide_enable(LucidCudaCtx* ctx, int on, int seed) {
     return guarded(ctx, [&](lucid::Engine& e) { return e.guide_enable(on != 0, seed); });
 }

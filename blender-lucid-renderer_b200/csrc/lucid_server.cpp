@@ -36,6 +36,30 @@ double percentile(std::vector<double> v, double q) {
 }
 }  // namespace
 
+std::vector<int> plan_batch(const LucidJobDesc& head, const std::vector<const LucidJobDesc*>& queue,
+                            const std::vector<char>& cancelled, long long max_paths, long long room_bytes,
+                            int max_jobs, long long* bytes) {
+    std::vector<int> take;
+    long long paths = job_paths(head), pixels = (long long)head.width * head.height;
+    long long bb = Engine::batch_bytes(pixels, paths);
+    if (max_paths > 0 && !head.interactive && !head.guided && paths < max_paths) {
+        for (int k = 0; k < (int)queue.size() && (int)take.size() + 1 < max_jobs; ++k) {
+            const LucidJobDesc& c = *queue[(size_t)k];
+            const long long p2 = paths + job_paths(c), px2 = pixels + (long long)c.width * c.height;
+            const long long b2 = Engine::batch_bytes(px2, p2);
+            if (cancelled[(size_t)k] || c.interactive || c.guided || c.max_depth != head.max_depth ||
+                std::strncmp(c.algorithm, head.algorithm, sizeof(c.algorithm)) != 0 || p2 > max_paths || b2 > room_bytes)
+                continue;
+            take.push_back(k);
+            paths = p2;
+            pixels = px2;
+            bb = b2;
+        }
+    }
+    if (bytes) *bytes = bb;
+    return take;
+}
+
 double Server::now() const {
     using namespace std::chrono;
     return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
@@ -189,26 +213,22 @@ void Server::slot_loop(int slot) {
             // (same integrator and depth, in queue order) into one batch
             // while the batch stays within a wave and the budget
             std::vector<Job*> members{j};
-            long long paths = job_paths(j->d), pixels = (long long)j->d.width * j->d.height;
-            long long bbytes = Engine::batch_bytes(pixels, paths);
-            const bool batchable = batch_paths_ > 0 && !j->d.interactive && !j->d.guided;
-            if (batchable && paths < batch_paths_) {
-                for (auto it = queue_.begin(); it != queue_.end() && (int)members.size() < kBatchJobs;) {
-                    Job& c = jobs_[*it];
-                    const long long p2 = paths + job_paths(c.d), px2 = pixels + (long long)c.d.width * c.d.height;
-                    const long long b2 = Engine::batch_bytes(px2, p2);
-                    if (c.cancel || c.d.interactive || c.d.guided || c.d.max_depth != j->d.max_depth ||
-                        std::strcmp(c.d.algorithm, j->d.algorithm) != 0 || p2 > batch_paths_ ||
-                        adm_.reserved + adm_.running + b2 > adm_.budget) {
-                        ++it;
-                        continue;
-                    }
-                    members.push_back(&c);
-                    paths = p2;
-                    pixels = px2;
-                    bbytes = b2;
-                    it = queue_.erase(it);
+            long long bbytes = 0;
+            {
+                std::vector<const LucidJobDesc*> waiting;
+                std::vector<char> cancelled;
+                for (int q : queue_) {
+                    waiting.push_back(&jobs_[q].d);
+                    cancelled.push_back(jobs_[q].cancel ? 1 : 0);
                 }
+                std::vector<int> take = plan_batch(j->d, waiting, cancelled, batch_paths_,
+                                                   adm_.budget - adm_.reserved - adm_.running, kBatchJobs, &bbytes);
+                for (int k = (int)take.size() - 1; k >= 0; --k) {   // erase from the back: indices stay valid
+                    auto it = queue_.begin() + take[(size_t)k];
+                    members.push_back(&jobs_[*it]);
+                    queue_.erase(it);
+                }
+                std::reverse(members.begin() + 1, members.end());   // queue order
             }
             const double t = now();
             if (busy_from_ < 0) busy_from_ = t;

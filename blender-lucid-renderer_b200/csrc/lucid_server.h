@@ -54,6 +54,18 @@ struct Admission {
     void finish(long long bytes) { running -= bytes; --busy; }
 };
 
+// The batch a slot forms when it takes `head` from the queue: the indices
+// of the jobs of `queue` (the jobs waiting behind it, in queue order) that
+// join it — throughput jobs (not interactive, not guided, not cancelled)
+// with the head's integrator and depth, taken in order while the batch
+// stays within max_paths paths (width * height * samples), the byte room
+// left in the budget (Engine::batch_bytes) and max_jobs jobs.  An empty
+// result: the head runs on its own.  `bytes` receives the batch's bytes.
+// Shared by the server and by the host-only planner (lucid_batch_plan).
+std::vector<int> plan_batch(const LucidJobDesc& head, const std::vector<const LucidJobDesc*>& queue,
+                            const std::vector<char>& cancelled, long long max_paths, long long room_bytes,
+                            int max_jobs, long long* bytes);
+
 class Server {
 public:
     Server(int device, int slots, long long budget_bytes);

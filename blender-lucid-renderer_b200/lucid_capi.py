@@ -301,6 +301,7 @@ SIGNATURES = {
     "lucid_server_stats": (_I, [_P, ctypes.POINTER(ServerStats)]),
     "lucid_server_set_batching": (_I, [_P, ctypes.c_longlong]),
     "lucid_admission_plan": (_I, [ctypes.c_longlong, ctypes.c_longlong, _I, _P, _I, _P]),
+    "lucid_batch_plan": (_I, [ctypes.c_longlong, ctypes.c_longlong, _P, _P, _I, _P]),
     "lucid_guide_create": (_I, [_I, _I, ctypes.POINTER(_P)]),
     "lucid_guide_destroy": (None, [_P]),
     "lucid_guide_last_error": (ctypes.c_char_p, [_P]),
@@ -646,6 +647,32 @@ def scene_digest(json_text: str | None = None, arrays: dict | None = None) -> in
     if rc != LUCID_OK:
         raise LucidError(rc, "invalid scene")
     return out.value
+
+
+def batch_plan(max_paths: int, room_bytes: int, jobs, cancelled=None) -> list:
+    """The server's batching policy run on the host (no GPU): `jobs` is a
+    list of dicts (scene, width, height, samples, max_depth, algorithm,
+    interactive, guided), the first taken from the head of the queue, the
+    rest waiting behind it; returns the 0/1 membership of each in the
+    head's batch."""
+    lib = load_library()
+    arr = (JobDesc * len(jobs))()
+    for k, j in enumerate(jobs):
+        arr[k] = JobDesc(int(j.get("scene", 0)), (ctypes.c_float * 10)(), j.get("algorithm", "mis").encode(),
+                         int(j["width"]), int(j["height"]), int(j["samples"]), int(j.get("max_depth", 8)),
+                         int(j.get("interactive", 0)), int(j.get("guided", 0)), 1)
+    canc = (ctypes.c_int * len(jobs))(*[int(c) for c in (cancelled or [0] * len(jobs))])
+    member = (ctypes.c_int * len(jobs))()
+    rc = lib.lucid_batch_plan(int(max_paths), int(room_bytes), ctypes.addressof(arr), ctypes.addressof(canc),
+                              len(jobs), ctypes.addressof(member))
+    if rc < 0:
+        raise LucidError(rc, "batch_plan failed")
+    return list(member)
+
+
+def batch_bytes(pixels: int, paths: int) -> int:
+    """Device bytes of a batch of `pixels` image pixels and `paths` paths in one wave."""
+    return paths * 178 + pixels * 32 + (2 << 20)
 
 
 def admission_plan(budget: int, reserved: int, slots: int, job_bytes) -> list:

@@ -548,6 +548,15 @@ int lucid_server_stats(LucidServer* srv, LucidServerStats* out);
  * 2^25); a job of max_paths paths or more runs on its own.  A batch's jobs
  * finish together, each image unchanged.  0 turns batching off. */
 int lucid_server_set_batching(LucidServer* srv, long long max_paths);
+/* The server's batching policy on its own (host only, no GPU; no
+ * counterpart in the reference): jobs[0] is the job a slot takes from the
+ * head of the queue, jobs[1..n-1] the jobs waiting behind it in queue order,
+ * cancelled[i] (may be NULL) marks jobs cancelled while queued, room_bytes
+ * is the device-memory budget left.  member[i] = 1 for every job of the
+ * batch the head forms (member[0] = 1 when one forms); returns the number of
+ * jobs the head runs with (1: alone) or a negative status. */
+int lucid_batch_plan(long long max_paths, long long room_bytes, const LucidJobDesc* jobs, const int* cancelled, int n,
+                     int* member);
 /* The server's admission policy on its own (host only, no GPU): n jobs of
  * job_bytes[i] arrive in order; decision[i] = the start order of job i
  * (0, 1, ...) when jobs finish in start order, or -1 when it is refused. */

@@ -28,6 +28,48 @@ def test_admission_is_first_come_first_served_within_slots_and_budget():
     assert lucid_capi.admission_plan(100, 0, 2, []) == []
 
 
+def _job(w, h, spp, algo="mis", depth=8, interactive=0, guided=0):
+    return {"width": w, "height": h, "samples": spp, "algorithm": algo, "max_depth": depth,
+            "interactive": interactive, "guided": guided}
+
+
+def test_batch_plan_takes_compatible_jobs_in_queue_order():
+    big_room = 1 << 40
+    head = _job(64, 64, 4)
+    queue = [_job(32, 32, 8), _job(32, 32, 8, algo="nee"), _job(16, 16, 4, depth=6), _job(8, 8, 1, interactive=1),
+             _job(8, 8, 1, guided=1), _job(48, 48, 2)]
+    # other integrators, other depths, interactive and guided jobs stay queued
+    assert lucid_capi.batch_plan(1 << 25, big_room, [head] + queue) == [1, 1, 0, 0, 0, 0, 1]
+    # cancelled jobs are skipped
+    assert lucid_capi.batch_plan(1 << 25, big_room, [head] + queue, [0, 1, 0, 0, 0, 0, 0]) == [1, 0, 0, 0, 0, 0, 1]
+    # nothing compatible behind it: the head runs alone
+    assert lucid_capi.batch_plan(1 << 25, big_room, [head, _job(8, 8, 1, algo="simple")]) == [0, 0]
+    # batching off, an interactive or guided head, or a head at the path limit: alone
+    assert lucid_capi.batch_plan(0, big_room, [head] + queue) == [0] * 7
+    assert lucid_capi.batch_plan(1 << 25, big_room, [_job(64, 64, 4, interactive=1)] + queue) == [0] * 7
+    assert lucid_capi.batch_plan(1 << 25, big_room, [_job(64, 64, 4, guided=1)] + queue) == [0] * 7
+    assert lucid_capi.batch_plan(64 * 64 * 4, big_room, [head] + queue) == [0] * 7
+
+
+def test_batch_plan_respects_the_path_limit_and_the_budget():
+    head = _job(100, 100, 1)                      # 10,000 paths
+    queue = [_job(100, 100, 3), _job(50, 50, 4), _job(100, 100, 2), _job(10, 10, 1)]
+    # 40,000-path limit: 10k + 30k fits, the 10k job would exceed it, the
+    # 20k job too; the last 100 paths still fit after the first
+    assert lucid_capi.batch_plan(40_000, 1 << 40, [head] + queue) == [1, 1, 0, 0, 0]
+    assert lucid_capi.batch_plan(40_100, 1 << 40, [head] + queue) == [1, 1, 0, 0, 1]
+    # bytes: room for exactly the head and the 50x50x4 job (the 30k-path
+    # job before it needs more, the 100-path job after it does not fit
+    # beside them); one byte less and the 100-path job joins instead
+    room = lucid_capi.batch_bytes(100 * 100 + 50 * 50, 10_000 + 10_000)
+    assert lucid_capi.batch_plan(1 << 25, room, [head] + queue) == [1, 0, 1, 0, 0]
+    assert lucid_capi.batch_plan(1 << 25, room - 1, [head] + queue) == [1, 0, 0, 0, 1]
+    assert lucid_capi.batch_plan(1 << 25, room + 100 * (178 + 32), [head] + queue) == [1, 0, 1, 0, 1]
+    # at most 256 jobs in one batch
+    many = [_job(4, 4, 1)] * 300
+    assert sum(lucid_capi.batch_plan(1 << 25, 1 << 40, many)) == 256
+
+
 def test_server_rejects_bad_arguments_without_a_gpu():
     lib = lucid_capi.load_library()
     assert lib.lucid_server_create(0, 0, 0, None) == lucid_capi.LUCID_ERR_INVALID
