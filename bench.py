@@ -433,17 +433,13 @@ def diagnostics(device: int) -> dict:
     return out
 
 
-def batch_mix(device: int, seed: int = 11, slots: int = 4) -> dict:
-    """The batched configuration: 48 render jobs, each on its own seeded
-    variant of the Cornell box tessellated to 10k-500k triangles
-    (log-uniform), at log-uniform 128-1024 px with aspect 1:1, 4:3 or 16:9
-    and 1, 4, 16 or 64 spp, plus 8 material previews (256x256, 32 spp),
-    submitted at once to the request loop (scenes uploaded as arrays):
-    aggregate samples/s on `slots` slots with the jobs batched (one set of
-    wavefront launches over a device job table per batch), against the same
-    slots with every job in its own launches and against the jobs one after
-    another on one slot."""
-    import lucid_capi
+def batch_workload(seed: int = 11):
+    """The batched configuration's jobs and scenes: 48 render jobs, each on
+    its own seeded variant of the Cornell box tessellated to 10k-500k
+    triangles (log-uniform), at log-uniform 128-1024 px with aspect 1:1,
+    4:3 or 16:9 and 1, 4, 16 or 64 spp, plus 8 material previews (256x256,
+    32 spp).  Returns (jobs, scenes): jobs as (kind, seed, triangles, width,
+    height, spp), scenes as (arrays, camera, triangle count)."""
     import lucid_scenes as ls
     rng = np.random.default_rng(seed)
     jobs = []
@@ -460,6 +456,41 @@ def batch_mix(device: int, seed: int = 11, slots: int = 4) -> dict:
     for kind, sd, tris, *_ in jobs:
         sc, cam = ls.cornell_variant(sd, tris) if kind == "variant" else ls.material_preview_scene(sd)
         scenes.append((ls.scene_arrays(sc, json_rounding=False), cam, ls.scene_triangle_count(sc)))
+    return jobs, scenes
+
+
+def batch_profile(device: int) -> int:
+    """The batched configuration's 56 jobs rendered by one
+    lucid_cuda_render_batch call (one context per scene, waves of 2^25
+    paths): a target for ncu launch lists of the batch kernels; prints no
+    bench line."""
+    import lucid_capi
+    jobs, scenes = batch_workload()
+    ctxs = []
+    for a, _, _ in scenes:
+        c = lucid_capi.Context(device)
+        c.load_scene_arrays(a)
+        ctxs.append(c)
+    runner = lucid_capi.Context(device)
+    runner.set_wave_capacity(1 << 25)
+    runner.render_batch([{"scene": ctxs[k], "camera": scenes[k][1], "width": w, "height": h, "samples": spp,
+                          "max_depth": 8} for k, (*_, w, h, spp) in enumerate(jobs)], "mis")
+    st = runner.stats()
+    log("batch profile: %d jobs, %.0f paths, %d waves, %.1f ms" % (len(jobs), st["paths"], st["waves"],
+                                                                   st["total_ms"]))
+    for c in ctxs + [runner]:
+        c.close()
+    return 0
+
+
+def batch_mix(device: int, seed: int = 11, slots: int = 4) -> dict:
+    """The batched configuration (batch_workload) submitted at once to the
+    request loop (scenes uploaded as arrays): aggregate samples/s on `slots`
+    slots with the jobs batched (one set of wavefront launches over a device
+    job table per batch), against the same slots with every job in its own
+    launches and against the jobs one after another on one slot."""
+    import lucid_capi
+    jobs, scenes = batch_workload(seed)
     total = sum(w * h * spp for (*_, w, h, spp) in jobs)
 
     def run(n_slots, batching):
@@ -684,6 +715,9 @@ def main():
     ap.add_argument("--guide-profile", type=int, default=0, metavar="N",
                     help="only N guided 640x360 renders of the hard-indirect room (a target for ncu captures of "
                          "the guide kernels); prints no bench line")
+    ap.add_argument("--batch-profile", action="store_true",
+                    help="only one render_batch call over the batched configuration's 56 jobs (a target for ncu "
+                         "launch lists of the batch kernels); prints no bench line")
     ap.add_argument("--wave", type=int, default=0, help="paths per wave (0: the engine's default)")
     ap.add_argument("--launch-profile", type=int, default=0, help="resident-CTA profile of the wavefront kernels")
     ap.add_argument("--width", type=int, default=W, help="smaller frames for profiling captures")
@@ -699,6 +733,8 @@ def main():
         return run_reference(args, rank)
     if args.guide_profile:
         return guide_profile(int(os.environ.get("LOCAL_RANK", "0")), args.guide_profile)
+    if args.batch_profile:
+        return batch_profile(int(os.environ.get("LOCAL_RANK", "0")))
     if args.diagnostics_only:
         print(json.dumps({"diagnostics": diagnostics(int(os.environ.get("LOCAL_RANK", "0")))}), flush=True)
         return 0
